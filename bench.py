@@ -1,0 +1,399 @@
+"""All-pairs exact intersection cardinality on B200: the benchmark.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload (one "step"): every pair i <= j of the large dense configuration --
+N = 65536 rows x M = 262144 bits, bit iid Bernoulli(p) with p drawn per row
+uniformly in [0.05, 0.5], packed as u64 (2 GiB in), u32 |Xi & Xj| for all
+i <= j out (2,147,516,416 pairs, 8.6 GB) -- through the STORM_contiguous_t
+interface of libstorm_b200.so.  Inputs are seeded synthetic data generated
+on the GPU.  Metric: exact pairs per second (and ns per pair).
+
+    value  device-resident: rows already in HBM, output stays in HBM; the
+           timed region is the all-pairs call (CUDA events, max over ranks).
+    e2e    through the C ABI with HOST buffers: each step ingests the rows
+           from pinned host memory (STORM_contig_add_bitmaps), computes and
+           copies the whole triangle back into pinned host memory.
+
+Multi-GPU (torchrun): every rank runs its own instance (seed + rank); the
+rows of different ranks are independent, so there is no data-path
+collective ("scaling": "weak").  `--impl reference` times the reference's own
+CPU kernel (oracle/_ref, built from the reference sources) on the host cores,
+on a bounded row sample of the same workload, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_ROWS, M_BITS, P_RANGE, SEED = 65536, 262144, (0.05, 0.5), 0x5EED2
+METRIC = "exact pairs/sec & ns/pair on 1 B200: learned-batched vs plain GPU vs CPU"
+
+
+# --------------------------------------------------------------- workload
+def bernoulli_rows_gpu(n, m, p, seed, device, chunk=1024):
+    """[n, ceil(m/64)] int64 rows (bit patterns of u64 words) generated on the
+    GPU: row r's bits are iid Bernoulli(p_r), p_r = p or U[p[0], p[1]]."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    w = (m + 63) // 64
+    out = torch.empty((n, w), dtype=torch.int64, device=device)
+    shifts = torch.arange(64, device=device, dtype=torch.int64)
+    for r0 in range(0, n, chunk):
+        r1 = min(n, r0 + chunk)
+        if isinstance(p, tuple):
+            pr = p[0] + (p[1] - p[0]) * torch.rand((r1 - r0, 1), generator=g, device=device)
+        else:
+            pr = torch.full((r1 - r0, 1), float(p), device=device)
+        bits = torch.rand((r1 - r0, w * 64), generator=g, device=device) < pr
+        if w * 64 > m:
+            bits[:, m:] = False
+        out[r0:r1] = (bits.view(r1 - r0, w, 64).to(torch.int64) << shifts).sum(dim=-1)
+        del bits
+    return out
+
+
+def pairs_of(n):
+    return n * (n + 1) // 2
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region (200 ms period)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, name in enumerate(names):
+                if len(s) > 5 + k and s[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+# ------------------------------------------------------ distributed setup
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def init_dist(world, backend):
+    import torch.distributed as dist
+    if world > 1 and not dist.is_initialized():
+        import datetime
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+    return dist if world > 1 else None
+
+
+def max_over_ranks(value, dist, device):
+    """Max of a float over ranks (all ranks call it in the same order)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(value, dist, device):
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ------------------------------------------------------------ CPU baseline
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def reference_sample(host_rows: np.ndarray, target_s: float, threads: int):
+    """Time the reference's AND+popcount kernel (oracle/_ref) over whole rows
+    of the triangle, starting at row 0, sized to ~target_s seconds.
+    Returns (pairs/s, pairs, seconds, rows)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as ol
+    R = ol.reference()
+    if R is None:
+        return None
+    n, w = host_rows.shape
+    rows = np.ascontiguousarray(host_rows)
+    ptr = rows.ctypes.data_as(ol.u64p)
+    # calibrate on a few rows
+    r1 = max(1, min(n, 2 * threads))
+    t0 = time.perf_counter()
+    R.ref_contig_matrix_mt(ptr, n, w, 0, r1, None, threads)
+    dt = time.perf_counter() - t0
+    pairs_cal = sum(n - i for i in range(r1))
+    rate = pairs_cal / max(dt, 1e-9)
+    want_pairs = rate * target_s
+    rows_needed = max(1, min(n, int(want_pairs / n) + 1))
+    t0 = time.perf_counter()
+    R.ref_contig_matrix_mt(ptr, n, w, 0, rows_needed, None, threads)
+    dt = time.perf_counter() - t0
+    pairs = sum(n - i for i in range(rows_needed))
+    return pairs / dt, pairs, dt, rows_needed
+
+
+# ------------------------------------------------------------------ arms
+def run_reference_arm(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    import torch
+    threads = cpu_threads()
+    device = torch.device("cuda", 0) if torch.cuda.is_available() else None
+    if device is not None:
+        rows = bernoulli_rows_gpu(N_ROWS, M_BITS, P_RANGE, SEED, device).cpu().numpy().view(np.uint64)
+    else:
+        import gen  # noqa  (CPU-only fallback for the input generator only)
+        rows = None
+    if rows is None:
+        print(json.dumps({"impl": "reference", "unavailable": "no CUDA device to generate the workload"}))
+        return 0
+    per_step_s = max(2.0, 60.0 / max(1, args.steps + args.warmup))
+    for _ in range(args.warmup):
+        if reference_sample(rows, min(per_step_s, 3.0), threads) is None:
+            print(json.dumps({"impl": "reference",
+                              "unavailable": "oracle/_ref/libstorm_ref.so was not built from the reference"}))
+            return 0
+    rates, total_pairs, total_s, last_rows = [], 0, 0.0, 0
+    for _ in range(args.steps):
+        rate, pairs, dt, nrows = reference_sample(rows, per_step_s, threads)
+        rates.append(rate)
+        total_pairs += pairs
+        total_s += dt
+        last_rows = nrows
+    value = total_pairs / total_s
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * pairs_of(N_ROWS) / value,
+        "ns_per_pair": 1e9 / value, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u64 (AND + popcount)", "data": "synthetic (seeded, generated on the GPU, copied to host)",
+        "config": {"workload": "dense all-bitmap XX^T: 65536 rows x 262144 bits, p~U[0.05,0.5], u32 i<=j out",
+                   "rows": N_ROWS, "bits": M_BITS, "pairs": pairs_of(N_ROWS),
+                   "sampled": f"rows 0..{last_rows} of the triangle per step (every j >= i)"},
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": "reference",
+                         "sample": f"{last_rows} rows x all j>=i per step, reference kernel "
+                                   f"STORM_get_intersect_count_func({M_BITS // 64}) on {threads} threads"},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200_arm(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    dist = init_dist(world, "nccl")
+    sb = importlib.import_module("stormbitmaps-internal_b200")
+
+    n, m = args.rows, args.bits
+    tri = pairs_of(n)
+    rows_d = bernoulli_rows_gpu(n, m, P_RANGE, SEED + rank, device)
+    w = rows_d.shape[1]
+    c = sb.StormContig(m)
+    c.set_kernel({"auto": sb.KERNEL_AUTO, "popc": sb.KERNEL_POPC, "mma": sb.KERNEL_MMA}[args.kernel])
+    rc = sb.lib().STORM_contig_add_bitmaps(c.h, C.cast(rows_d.data_ptr(), sb.u64p), n, w)
+    if rc < 0:
+        raise sb.StormError(rc, "STORM_contig_add_bitmaps")
+    c.upload()
+    out_d = torch.empty(tri, dtype=torch.int32, device=device)
+    stream = torch.cuda.ExternalStream(c.stream(), device=device)
+
+    # ---- device-resident timing ----
+    for _ in range(args.warmup):
+        c.matrix_device(out_d.data_ptr(), tri)
+    kernel_ms = []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            s = c.matrix_device(out_d.data_ptr(), tri)
+            kernel_ms.append(c.last_kernel_ms())
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    elapsed_ms = ev0.elapsed_time(ev1)
+    elapsed_ms = max_over_ranks(elapsed_ms, dist, device)
+    launches = args.steps * c.last_launches()
+    kernel_used = {sb.KERNEL_POPC: "bb_popc_kernel", sb.KERNEL_MMA: "bb_mma_kernel"}.get(c.last_kernel(), "?")
+    ms_per_step = elapsed_ms / args.steps
+    value = world * tri / (ms_per_step / 1e3)
+
+    # ---- end to end through the C ABI with host buffers ----
+    host_in = torch.empty((n, w), dtype=torch.int64, pin_memory=True)
+    host_in.copy_(rows_d)
+    del rows_d
+    host_out = torch.empty(tri, dtype=torch.int32, pin_memory=True)
+    e2e_ms = []
+    L = sb.lib()
+    for it in range(1 + args.e2e_steps):
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        L.STORM_contig_clear(c.h)
+        rc = L.STORM_contig_add_bitmaps(c.h, C.cast(host_in.data_ptr(), sb.u64p), n, w)
+        if rc < 0:
+            raise sb.StormError(rc, "STORM_contig_add_bitmaps")
+        ssum = C.c_uint64(0)
+        rc = L.STORM_contig_pairw_intersect_matrix(c.h, C.cast(host_out.data_ptr(), sb.u32p), tri, C.byref(ssum))
+        if rc < 0:
+            raise sb.StormError(rc, "STORM_contig_pairw_intersect_matrix")
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) * 1e3
+        if it > 0:   # first iteration re-allocates the handle's buffers
+            e2e_ms.append(dt)
+    e2e_step_ms = max_over_ranks(statistics.median(e2e_ms), dist, device)
+    e2e_value = world * tri / (e2e_step_ms / 1e3)
+    assert int(ssum.value) == s, "device and host runs disagree"
+
+    # ---- roofline of the dominant kernel ----
+    peaks, peak_src = measured_peaks()
+    k_ms = statistics.median(kernel_ms)
+    if kernel_used == "bb_mma_kernel":
+        ops = 2.0 * tri * m                      # u8 MACs = pairs x row bits, 2 ops each
+        achieved = ops / (k_ms / 1e3) / 1e12
+        peak = 2.0 * peaks["bf16_tflops"]        # dense int8 rate = 2 x dense bf16 on sm_100
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOPS (int8)",
+                "frac": achieved / peak,
+                "peak_source": f"2 x bf16_tflops {peak_src} ({peaks['bf16_tflops']}); int8 dense = 2 x bf16",
+                "algorithmic": f"pairs(i<=j) x {m} bit-MACs x 2 ops", "traffic": args.traffic}
+    else:
+        ops = 2.0 * tri * m
+        achieved = ops / (k_ms / 1e3) / 1e12
+        roof = {"bound": "alu", "achieved": achieved, "peak": None, "unit": "Tbit-ops/s", "frac": None,
+                "traffic": args.traffic}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "ns_per_pair": 1e9 / (value / world),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8 (tcgen05 kind::i8, s32 acc)"
+        if kernel_used == "bb_mma_kernel" else "u64 (AND + POPC)",
+        "data": "synthetic (seeded Bernoulli rows generated on the GPU)",
+        "config": {"workload": "dense all-bitmap XX^T: 65536 rows x 262144 bits, p~U[0.05,0.5], u32 i<=j out",
+                   "rows": n, "bits": m, "pairs_per_gpu": tri, "kernel": kernel_used,
+                   "l2": "inputs (2 GiB) and outputs (8.6 GB) exceed L2 (126 MB); no flush needed",
+                   "parallelism": f"{world} independent instances (weak)"},
+        "kernel_ms_median": k_ms,
+        "gpu_launches": launches,
+        "roofline": roof,
+        "clocks": clocks.summary(),
+        "e2e": {"value": e2e_value, "unit": "pairs/s", "ms_per_step": e2e_step_ms,
+                "h2d_bytes_per_step": int(n * w * 8), "d2h_bytes_per_step": int(tri * 4)},
+    }
+    if rank == 0 and args.cpu_baseline:
+        r = reference_sample(host_in.numpy().view(np.uint64), args.cpu_seconds, cpu_threads())
+        if r is not None:
+            rate, pairs, dt, nrows = r
+            line["cpu_baseline"] = {"value": rate, "unit": "pairs/s", "cores": cpu_threads(), "kind": "reference",
+                                    "sample": f"rows 0..{nrows} x all j>=i ({pairs} pairs, {dt:.1f} s), reference "
+                                              f"AND+popcount kernel via oracle/_ref"}
+        else:
+            line["cpu_baseline"] = {"value": None, "unit": "pairs/s", "cores": 0, "kind": "reference",
+                                    "sample": "oracle/_ref not built"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma"])
+    ap.add_argument("--rows", type=int, default=N_ROWS)
+    ap.add_argument("--bits", type=int, default=M_BITS)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--traffic", type=float, default=None,
+                    help="dram bytes per launch of the dominant kernel from an ncu capture")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_b200_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

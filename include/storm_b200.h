@@ -1,0 +1,117 @@
+/*
+ * storm_b200.h -- extensions of the drop-in interface.
+ *
+ * The reference interface (storm.h) only returns the SUM of |Xi & Xj| over
+ * i < j.  An all-pairs user almost always wants the individual counts, which
+ * the reference's C++ kernel layer hands out tile by tile
+ * (kernels/storm_allpairs.h:206-214, `allpairs_tiles` + `TileCallback`).
+ * The entry points below expose that per-pair output through the C ABI, plus
+ * bulk ingest and device-resident variants used for measurement.
+ *
+ * Conventions shared by every entry point in this file:
+ *   - int returns: 0 (or a count) on success, a negative STORM_B200_E* code
+ *     on failure; STORM_b200_strerror() names it.
+ *   - "matrix" outputs are the packed upper triangle INCLUDING the diagonal,
+ *     in original row order: entry (i, j), i <= j, lives at
+ *     STORM_tri_index(n, i, j); n*(n+1)/2 entries in total.  The diagonal is
+ *     the row cardinality.
+ *   - the optional `sum` out-parameter receives the reference's own result,
+ *     the sum over i < j (storm.cpp:1232-1240, 927-945).
+ *   - every call is synchronous: results are on the host (or, for *_device
+ *     calls, complete in device memory) when it returns.
+ */
+#ifndef STORM_B200_EXT_H_
+#define STORM_B200_EXT_H_
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct STORM_s STORM_t;
+typedef struct STORM_contiguous_s STORM_contiguous_t;
+
+/* ---- status codes ----------------------------------------------------- */
+#define STORM_B200_OK          0
+#define STORM_B200_ENULL      (-1)   /* NULL handle (reference code -1)            */
+#define STORM_B200_EVALUES    (-2)   /* NULL values pointer (reference code -2)    */
+#define STORM_B200_EARG       (-3)   /* argument out of range / unsorted input     */
+#define STORM_B200_ENOMEM     (-4)   /* host or device allocation failed (ref -4)  */
+#define STORM_B200_ECUDA      (-5)   /* no usable sm_100 device, or a CUDA error   */
+#define STORM_B200_ETIMEOUT   (-6)   /* a bounded device-side wait gave up         */
+#define STORM_B200_ESIZE      (-7)   /* output buffer smaller than required        */
+#define STORM_B200_ELIMIT     (-8)   /* problem exceeds a documented size limit    */
+
+const char* STORM_b200_strerror(int status);
+/* Status of the last call on this thread that returned a sentinel instead of
+ * a status (the uint64_t-returning reference calls return 0, or (uint64_t)-1
+ * for a NULL STORM_t, exactly as the reference does). */
+int STORM_b200_last_status(void);
+
+/* Packed upper-triangle index of pair (i, j), i <= j < n. */
+static inline uint64_t STORM_tri_index(uint64_t n, uint64_t i, uint64_t j) {
+    /* rows 0..i-1 hold n, n-1, ..., n-i+1 entries; i*(i-1) is even */
+    return i * n - (i * (i - 1)) / 2 + (j - i);
+}
+static inline uint64_t STORM_tri_size(uint64_t n) { return n * (n + 1) / 2; }
+
+/* Tile visitor, shaped like storm::TileCallback (storm_allpairs.h:206-208):
+ * `counts` is a tile x tile buffer, row stride `tile`, of which the nr x nc
+ * block is live.  On diagonal tiles only j > i is filled (the reference's
+ * allpairs_tiles convention, storm_allpairs.cpp:709); other entries are 0.
+ * Rows/columns are ORIGINAL row indices i0.., j0.. */
+typedef void (*STORM_tile_callback)(uint32_t i0, uint32_t j0, uint32_t nr, uint32_t nc,
+                                    const uint32_t* counts, void* ctx);
+
+/* ---- STORM_contiguous_t extensions ------------------------------------ */
+/* Bitmap x bitmap kernel used by the contiguous all-pairs calls. */
+#define STORM_B200_KERNEL_AUTO  0   /* tensor-core kernel where exact, else POPC   */
+#define STORM_B200_KERNEL_POPC  1   /* CUDA-core AND + POPC tiles                  */
+#define STORM_B200_KERNEL_MMA   2   /* tcgen05 kind::i8 tensor-core tiles          */
+
+/* Append n_rows rows given as packed little-endian bitmaps of
+ * words_per_row 64-bit words each, in host memory or (unified addressing)
+ * device memory (bit b of row r = word b/64, bit b%64).
+ * words_per_row must equal ceil(vector_length/64).  Bits at or above
+ * vector_length must be zero (STORM_B200_EARG otherwise).  Equivalent to one
+ * STORM_contig_add per row with that row's set positions, except that empty
+ * rows are kept (STORM_contig_add drops n_values == 0 calls).  Returns
+ * n_rows. */
+int STORM_contig_add_bitmaps(STORM_contiguous_t* c, const uint64_t* words,
+                             uint32_t n_rows, uint32_t words_per_row);
+/* Number of rows held. */
+uint64_t STORM_contig_size(const STORM_contiguous_t* c);
+int STORM_contig_set_kernel(STORM_contiguous_t* c, int kernel);
+/* Pack the rows into HBM now (otherwise done by the first all-pairs call). */
+int STORM_contig_upload(STORM_contiguous_t* c);
+/* Per-pair counts into a HOST buffer of out_len >= n*(n+1)/2 entries. */
+int STORM_contig_pairw_intersect_matrix(STORM_contiguous_t* c, uint32_t* out,
+                                        uint64_t out_len, uint64_t* sum);
+/* Same, into a DEVICE buffer on the current device (d_out may be NULL to
+ * compute only the sum).  Rows must already be resident (upload). */
+int STORM_contig_pairw_intersect_matrix_device(STORM_contiguous_t* c, uint32_t* d_out,
+                                               uint64_t out_len, uint64_t* sum);
+int STORM_contig_pairw_intersect_tiles(STORM_contiguous_t* c, uint32_t tile,
+                                       STORM_tile_callback cb, void* ctx);
+/* CUDA stream the handle launches on (a cudaStream_t), for event timing. */
+void* STORM_contig_stream(STORM_contiguous_t* c);
+/* Device time of the kernels of the last all-pairs call (CUDA events on the
+ * handle's stream) and how many kernels it launched. */
+float STORM_contig_last_kernel_ms(const STORM_contiguous_t* c);
+uint32_t STORM_contig_last_launches(const STORM_contiguous_t* c);
+/* Which kernel the last call ran (STORM_B200_KERNEL_POPC or _MMA). */
+int STORM_contig_last_kernel(const STORM_contiguous_t* c);
+
+/* ---- STORM_t extensions ----------------------------------------------- */
+int STORM_upload(STORM_t* s);
+int STORM_pairw_intersect_matrix(STORM_t* s, uint32_t* out, uint64_t out_len, uint64_t* sum);
+int STORM_pairw_intersect_tiles(STORM_t* s, uint32_t tile, STORM_tile_callback cb, void* ctx);
+float STORM_last_kernel_ms(const STORM_t* s);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* STORM_B200_EXT_H_ */

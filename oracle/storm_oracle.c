@@ -1,0 +1,270 @@
+/*
+ * storm_oracle.c -- CPU ORACLE for the all-pairs intersection path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the shipped library links, loads or
+ * calls this file; only tests/, __graft_entry__.smoke() and bench.py's
+ * CPU-baseline leg use it, and only as the checker.
+ *
+ * It restates, in plain C, what the StormBitmaps reference computes on this
+ * path, each function citing the reference code it follows:
+ *
+ *   - per-pair |Xi & Xj| over packed bitmap rows: the contiguous container's
+ *     dispatch (storm.cpp:1144-1156) and libalgebra's AND+popcount kernels
+ *     (libalgebra.h:2996 scalar form).  All dispatch branches compute the same
+ *     set-intersection cardinality, so one AND+popcount loop restates them.
+ *   - per-pair |Xi & Xj| over sorted position lists: kernels/oracle.cpp:28-38
+ *     (rebuild both sides from positions, count common bits) -- restated as a
+ *     two-pointer merge over the sorted distinct lists.
+ *   - the STORM_t chunk split (storm.cpp:737-803): chunk = value / 65536,
+ *     list chunk when fewer than 4096 values, bitmap chunk otherwise.
+ *   - representation builders of kernels/storm_repr.cpp: maximal runs
+ *     (:118-128), EWAH-64 (:78-100, marker layout storm_repr.h:28-31),
+ *     rank9 (:25-45), zone map (:47-59), complement (:139-154) and RowMeta
+ *     (:186-206).
+ *
+ * The popcount here is a SWAR bit count (no compiler builtin), so a broken
+ * intrinsic path in a build cannot also break the checker -- the same
+ * independence rule as kernels/oracle.cpp:17-24.
+ *
+ * Parity pinning: tests/golden/ holds outputs of the reference itself,
+ * compiled from its own sources (oracle/Makefile) and run on seeded inputs
+ * (tests/golden/make_golden.py); tests/test_oracle.py checks this file
+ * against every one of them.
+ */
+#include <stdint.h>
+#include <stddef.h>
+#include <string.h>
+#include <stdlib.h>
+
+static uint32_t oracle_popcount64(uint64_t x) {
+    x = x - ((x >> 1) & 0x5555555555555555ull);
+    x = (x & 0x3333333333333333ull) + ((x >> 2) & 0x3333333333333333ull);
+    x = (x + (x >> 4)) & 0x0F0F0F0F0F0F0F0Full;
+    return (uint32_t)((x * 0x0101010101010101ull) >> 56);
+}
+
+/* |A & B| over nw words (libalgebra.h:2996, storm.cpp:1155). */
+uint64_t oracle_and_popcount(const uint64_t* a, const uint64_t* b, uint64_t nw) {
+    uint64_t c = 0;
+    for (uint64_t k = 0; k < nw; ++k) c += oracle_popcount64(a[k] & b[k]);
+    return c;
+}
+
+/* Packed upper triangle (i <= j, diagonal included) of per-pair counts over
+ * n packed bitmap rows of nw words, plus the reference's sum over i < j
+ * (storm.cpp:1232-1240).  `out` may be NULL.  Rows [r0, r1) only, so a
+ * caller can sample a bounded slice; rows outside contribute nothing. */
+uint64_t oracle_contig_matrix(const uint64_t* words, uint64_t n, uint64_t nw,
+                              uint64_t r0, uint64_t r1, uint32_t* out) {
+    uint64_t sum = 0;
+    for (uint64_t i = r0; i < r1 && i < n; ++i) {
+        const uint64_t* a = words + i * nw;
+        const uint64_t base = i * n - (i * (i - 1)) / 2 - i;
+        for (uint64_t j = i; j < n; ++j) {
+            const uint64_t c = oracle_and_popcount(a, words + j * nw, nw);
+            if (out) out[base + j] = (uint32_t)c;
+            if (j > i) sum += c;
+        }
+    }
+    return sum;
+}
+
+/* |A & B| of two sorted, distinct position lists (kernels/oracle.cpp:28-38:
+ * the set intersection of the two rows). */
+uint64_t oracle_list_intersect(const uint32_t* a, uint64_t na,
+                               const uint32_t* b, uint64_t nb) {
+    uint64_t i = 0, j = 0, c = 0;
+    while (i < na && j < nb) {
+        if (a[i] < b[j]) ++i;
+        else if (b[j] < a[i]) ++j;
+        else { ++c; ++i; ++j; }
+    }
+    return c;
+}
+
+/* Per-pair counts over n rows given as sorted distinct lists in CSR form
+ * (values[offsets[r] .. offsets[r+1])).  Same output convention as
+ * oracle_contig_matrix.  This is the count every STORM_t and kernel-layer
+ * all-pairs call must reproduce (storm.cpp:927-945; storm_allpairs.cpp:677-732). */
+uint64_t oracle_sets_matrix(const uint32_t* values, const uint64_t* offsets, uint64_t n,
+                            uint64_t r0, uint64_t r1, uint32_t* out) {
+    uint64_t sum = 0;
+    for (uint64_t i = r0; i < r1 && i < n; ++i) {
+        const uint64_t base = i * n - (i * (i - 1)) / 2 - i;
+        for (uint64_t j = i; j < n; ++j) {
+            const uint64_t c = oracle_list_intersect(values + offsets[i], offsets[i + 1] - offsets[i],
+                                                     values + offsets[j], offsets[j + 1] - offsets[j]);
+            if (out) out[base + j] = (uint32_t)c;
+            if (j > i) sum += c;
+        }
+    }
+    return sum;
+}
+
+/* Rectangular form: sum over all (i in X, j in Y) (storm.cpp:1027-1046). */
+uint64_t oracle_sets_square(const uint32_t* xv, const uint64_t* xo, uint64_t nx,
+                            const uint32_t* yv, const uint64_t* yo, uint64_t ny) {
+    uint64_t sum = 0;
+    for (uint64_t i = 0; i < nx; ++i)
+        for (uint64_t j = 0; j < ny; ++j)
+            sum += oracle_list_intersect(xv + xo[i], xo[i + 1] - xo[i], yv + yo[j], yo[j + 1] - yo[j]);
+    return sum;
+}
+
+/* ---- STORM_t chunk split (storm.cpp:737-803) ----------------------------
+ * For one sorted row, writes per chunk: id, kind (0 = list, 1 = bitmap) and
+ * value count.  Returns the number of chunks. */
+uint64_t oracle_chunk_split(const uint32_t* v, uint64_t n, uint32_t* ids, uint8_t* kinds,
+                            uint32_t* counts) {
+    uint64_t k = 0, s = 0;
+    while (s < n) {
+        const uint32_t id = v[s] / 65536u;
+        uint64_t e = s;
+        while (e < n && v[e] / 65536u == id) ++e;
+        ids[k] = id;
+        counts[k] = (uint32_t)(e - s);
+        kinds[k] = (e - s) < 4096 ? 0 : 1;
+        ++k;
+        s = e;
+    }
+    return k;
+}
+
+/* ---- representation builders (kernels/storm_repr.cpp) ------------------ */
+
+/* Maximal runs [start, end) of a sorted distinct list (storm_repr.cpp:118-128). */
+uint64_t oracle_runs(const uint32_t* v, uint64_t n, uint32_t* start, uint32_t* end) {
+    uint64_t r = 0;
+    for (uint64_t i = 0; i < n;) {
+        uint64_t j = i;
+        while (j + 1 < n && v[j + 1] == v[j] + 1) ++j;
+        start[r] = v[i];
+        end[r] = v[j] + 1;
+        ++r;
+        i = j + 1;
+    }
+    return r;
+}
+
+/* EWAH-64 encoding of a bitmap (storm_repr.cpp:78-100).  Marker: bit 0 fill
+ * value, bits 1..31 fill length, bits 32..63 literal count
+ * (storm_repr.h:28-31).  A maximal stretch of all-zero or all-one words (at
+ * most 2^31-1) is a fill; the non-fill words after it are literals.  `out`
+ * must hold 2*nw+1 words.  Returns the stream length. */
+uint64_t oracle_ewah(const uint64_t* w, uint64_t nw, uint64_t* out) {
+    uint64_t o = 0, i = 0;
+    while (i < nw) {
+        uint64_t fv = (w[i] == ~0ull) ? 1 : 0;
+        uint64_t fl = 0;
+        if (w[i] == 0 || fv) {
+            const uint64_t pat = fv ? ~0ull : 0ull;
+            while (i < nw && w[i] == pat && fl < 0x7FFFFFFFull) { ++i; ++fl; }
+        } else {
+            fv = 0;
+        }
+        const uint64_t l0 = i;
+        while (i < nw && w[i] != 0 && w[i] != ~0ull) ++i;
+        const uint64_t ll = i - l0;
+        out[o++] = fv | (fl << 1) | (ll << 32);
+        for (uint64_t k = 0; k < ll; ++k) out[o++] = w[l0 + k];
+    }
+    if (o == 0) out[o++] = 0;
+    return o;
+}
+
+/* Decode EWAH-64 back to nw words (storm_repr.cpp:61-74). */
+void oracle_ewah_decode(const uint64_t* buf, uint64_t n, uint64_t* out) {
+    uint64_t i = 0, o = 0;
+    while (i < n) {
+        const uint64_t m = buf[i++];
+        const uint64_t fl = (m >> 1) & 0x7FFFFFFFull, ll = m >> 32;
+        const uint64_t fv = (m & 1) ? ~0ull : 0ull;
+        for (uint64_t k = 0; k < fl; ++k) out[o++] = fv;
+        for (uint64_t k = 0; k < ll; ++k) out[o++] = buf[i++];
+    }
+}
+
+/* rank9 index, 2*(nblk+1) words (storm_repr.cpp:25-45; layout storm_repr.h:78-93). */
+void oracle_rank9(const uint64_t* w, uint64_t nw, uint64_t* out) {
+    const uint64_t nblk = (nw + 7) / 8;
+    uint64_t acc = 0;
+    for (uint64_t b = 0; b < nblk; ++b) {
+        uint64_t rel = 0, sub = 0;
+        out[2 * b] = acc;
+        for (uint64_t k = 0; k < 8; ++k) {
+            if (k >= 1) sub |= (rel & 0x1FFull) << (9 * (k - 1));
+            if (b * 8 + k < nw) rel += oracle_popcount64(w[b * 8 + k]);
+        }
+        out[2 * b + 1] = sub;
+        acc += rel;
+    }
+    out[2 * nblk] = acc;
+    out[2 * nblk + 1] = 0;
+}
+
+/* Zone map: one bit per bin of `bin` words, set when the bin is non-zero
+ * (storm_repr.cpp:47-59).  out holds ceil(ceil(nw/bin)/64) words. */
+void oracle_occ(const uint64_t* w, uint64_t nw, uint64_t bin, uint64_t* out) {
+    const uint64_t bins = (nw + bin - 1) / bin;
+    memset(out, 0, ((bins + 63) / 64) * 8);
+    for (uint64_t b = 0; b < bins; ++b) {
+        uint64_t any = 0;
+        for (uint64_t k = b * bin; k < (b + 1) * bin && k < nw; ++k) any |= w[k];
+        if (any) out[b >> 6] |= 1ull << (b & 63);
+    }
+}
+
+/* RowMeta of a sorted distinct list over `universe` bits
+ * (storm_repr.cpp:186-206, storm_repr.h:213-231).  meta[0..7] =
+ * cardinality, n_runs, n_words, n_nonzero_w, first_set, last_set, has_rank,
+ * has_occ. */
+void oracle_row_meta(const uint32_t* v, uint64_t n, uint32_t universe, uint32_t* meta) {
+    const uint32_t nw = (universe + 63u) / 64u;
+    uint32_t runs = 0, nnz = 0;
+    int64_t last_word = -1;
+    for (uint64_t i = 0; i < n; ++i) {
+        if (i == 0 || v[i] != v[i - 1] + 1) ++runs;
+        if ((int64_t)(v[i] >> 6) != last_word) { ++nnz; last_word = v[i] >> 6; }
+    }
+    meta[0] = (uint32_t)n;
+    meta[1] = runs;
+    meta[2] = nw;
+    meta[3] = nnz;
+    meta[4] = n ? v[0] : 0xFFFFFFFFu;
+    meta[5] = n ? v[n - 1] : 0;
+    meta[6] = (runs && n / runs >= 512) ? 1 : 0;
+    meta[7] = ((uint64_t)n * 512 > (uint64_t)universe) ? 1 : 0;
+}
+
+/* Complement positions of a sorted distinct list (storm_repr.cpp:139-146). */
+uint64_t oracle_complement(const uint32_t* v, uint64_t n, uint32_t universe, uint32_t* out) {
+    uint64_t o = 0;
+    uint32_t prev = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        for (uint32_t p = prev; p < v[i]; ++p) out[o++] = p;
+        prev = v[i] + 1;
+    }
+    for (uint32_t p = prev; p < universe; ++p) out[o++] = p;
+    return o;
+}
+
+/* One row's strip of the packed triangle: out[j - i] = |Xi & Xj| for
+ * j in [i, n).  Same counts as oracle_contig_matrix, without the n^2 buffer. */
+uint64_t oracle_contig_row(const uint64_t* words, uint64_t n, uint64_t nw, uint64_t i, uint32_t* out) {
+    uint64_t sum = 0;
+    for (uint64_t j = i; j < n; ++j) {
+        const uint64_t c = oracle_and_popcount(words + i * nw, words + j * nw, nw);
+        out[j - i] = (uint32_t)c;
+        if (j > i) sum += c;
+    }
+    return sum;
+}
+
+/* Cardinality of each packed row (the diagonal of the all-pairs matrix). */
+void oracle_row_popcounts(const uint64_t* words, uint64_t n, uint64_t nw, uint32_t* out) {
+    for (uint64_t r = 0; r < n; ++r) {
+        uint64_t c = 0;
+        for (uint64_t k = 0; k < nw; ++k) c += oracle_popcount64(words[r * nw + k]);
+        out[r] = (uint32_t)c;
+    }
+}

@@ -1,0 +1,352 @@
+"""Python mirror of the storm.h interface, over libstorm_b200.so (ctypes).
+
+The shipped product is the C-ABI library; this module is the host-side view
+that tests and bench.py use.  Class and method names follow the reference's
+C entry points (storm.h:214-231):
+
+    StormContig(vector_length)      STORM_contig_new / add / pairw_* / clear
+    Storm()                         STORM_new / add / pairw_* / clear / square
+
+Every all-pairs method runs on the GPU through the library.  There is no
+host fallback: if libstorm_b200.so is missing this module fails to import,
+and on a machine without an sm_100 device the calls raise StormError
+(STORM_B200_ECUDA).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libstorm_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"{LIB_PATH} is not built; run `python stormbitmaps-internal_b200/build.py` "
+        "(or __graft_entry__.build())"
+    )
+
+_lib = C.CDLL(LIB_PATH)
+
+u8p = C.POINTER(C.c_uint8)
+u16p = C.POINTER(C.c_uint16)
+u32p = C.POINTER(C.c_uint32)
+u64p = C.POINTER(C.c_uint64)
+TILE_CB = C.CFUNCTYPE(None, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, u32p, C.c_void_p)
+
+KERNEL_AUTO, KERNEL_POPC, KERNEL_MMA = 0, 1, 2
+OK, ENULL, EVALUES, EARG, ENOMEM, ECUDA, ETIMEOUT, ESIZE, ELIMIT = 0, -1, -2, -3, -4, -5, -6, -7, -8
+
+
+def _sig(name, res, args):
+    f = getattr(_lib, name)
+    f.restype = res
+    f.argtypes = args
+    return f
+
+
+# --- declarations (include/storm.h, include/storm_b200.h) ----------------
+_sig("STORM_b200_strerror", C.c_char_p, [C.c_int])
+_sig("STORM_b200_last_status", C.c_int, [])
+_sig("STORM_intersect_vector16_cardinality", C.c_uint64, [u16p, u16p, C.c_uint32, C.c_uint32])
+_sig("STORM_intersect_vector32_unsafe", C.c_uint64, [u32p, u32p, C.c_uint32, C.c_uint32, u32p])
+_sig("STORM_intersect_bitmaps_scalar_list", C.c_uint64, [u64p, u64p, u32p, u32p, C.c_uint32, C.c_uint32])
+_sig("STORM_wrapper_diag", C.c_uint64, [C.c_uint32, u64p, C.c_uint32, C.c_void_p])
+_sig("STORM_wrapper_diag_blocked", C.c_uint64, [C.c_uint32, u64p, C.c_uint32, C.c_void_p, C.c_uint32])
+_sig("STORM_wrapper_square", C.c_uint64, [C.c_uint32, u64p, C.c_uint32, u64p, C.c_uint32, C.c_void_p])
+_sig("STORM_contig_new", C.c_void_p, [C.c_size_t])
+_sig("STORM_contig_free", None, [C.c_void_p])
+_sig("STORM_contig_add", C.c_int, [C.c_void_p, u32p, C.c_uint32])
+_sig("STORM_contig_clear", C.c_int, [C.c_void_p])
+_sig("STORM_contig_pairw_intersect_cardinality", C.c_uint64, [C.c_void_p])
+_sig("STORM_contig_pairw_intersect_cardinality_blocked", C.c_uint64, [C.c_void_p, C.c_uint32])
+_sig("STORM_contig_pairw_intersect_cardinality_list", C.c_uint64, [C.c_void_p])
+_sig("STORM_contig_pairw_intersect_cardinality_blocked_list", C.c_uint64, [C.c_void_p, C.c_uint32])
+_sig("STORM_contig_add_bitmaps", C.c_int, [C.c_void_p, u64p, C.c_uint32, C.c_uint32])
+_sig("STORM_contig_size", C.c_uint64, [C.c_void_p])
+_sig("STORM_contig_set_kernel", C.c_int, [C.c_void_p, C.c_int])
+_sig("STORM_contig_upload", C.c_int, [C.c_void_p])
+_sig("STORM_contig_pairw_intersect_matrix", C.c_int, [C.c_void_p, u32p, C.c_uint64, u64p])
+_sig("STORM_contig_pairw_intersect_matrix_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, u64p])
+_sig("STORM_contig_pairw_intersect_tiles", C.c_int, [C.c_void_p, C.c_uint32, TILE_CB, C.c_void_p])
+_sig("STORM_contig_stream", C.c_void_p, [C.c_void_p])
+_sig("STORM_contig_last_kernel_ms", C.c_float, [C.c_void_p])
+_sig("STORM_contig_last_launches", C.c_uint32, [C.c_void_p])
+_sig("STORM_contig_last_kernel", C.c_int, [C.c_void_p])
+_sig("STORM_new", C.c_void_p, [])
+_sig("STORM_free", None, [C.c_void_p])
+_sig("STORM_add", C.c_int, [C.c_void_p, u32p, C.c_uint32])
+_sig("STORM_clear", C.c_int, [C.c_void_p])
+_sig("STORM_pairw_intersect_cardinality", C.c_uint64, [C.c_void_p])
+_sig("STORM_pairw_intersect_cardinality_blocked", C.c_uint64, [C.c_void_p, C.c_uint32])
+_sig("STORM_intersect_cardinality_square", C.c_uint64, [C.c_void_p, C.c_void_p])
+_sig("STORM_serialized_size", C.c_uint64, [C.c_void_p])
+_sig("STORM_upload", C.c_int, [C.c_void_p])
+_sig("STORM_pairw_intersect_matrix", C.c_int, [C.c_void_p, u32p, C.c_uint64, u64p])
+_sig("STORM_pairw_intersect_tiles", C.c_int, [C.c_void_p, C.c_uint32, TILE_CB, C.c_void_p])
+_sig("STORM_last_kernel_ms", C.c_float, [C.c_void_p])
+
+
+class StormError(RuntimeError):
+    def __init__(self, code: int, where: str = ""):
+        self.code = code
+        msg = _lib.STORM_b200_strerror(code).decode()
+        super().__init__(f"{where}: {msg} ({code})" if where else f"{msg} ({code})")
+
+
+def lib():
+    """The loaded ctypes library (for calling entry points directly)."""
+    return _lib
+
+
+def _check(rc: int, where: str) -> int:
+    if rc < 0:
+        raise StormError(rc, where)
+    return rc
+
+
+def _check_status(where: str):
+    s = _lib.STORM_b200_last_status()
+    if s < 0:
+        raise StormError(s, where)
+
+
+def _p(a: np.ndarray, t):
+    return a.ctypes.data_as(t)
+
+
+def tri_size(n: int) -> int:
+    return n * (n + 1) // 2
+
+
+def tri_index(n: int, i, j):
+    """Packed upper-triangle index of (i, j), i <= j (storm_b200.h)."""
+    i = np.asarray(i, dtype=np.uint64)
+    j = np.asarray(j, dtype=np.uint64)
+    n = np.uint64(n)
+    return i * n - (i * (i - np.uint64(1))) // np.uint64(2) * (i > 0) + (j - i)
+
+
+def unpack_triangle(tri: np.ndarray, n: int) -> np.ndarray:
+    """Dense symmetric n x n matrix from a packed upper triangle."""
+    m = np.zeros((n, n), dtype=tri.dtype)
+    iu = np.triu_indices(n)
+    m[iu] = tri
+    m.T[iu] = tri
+    return m
+
+
+def _u32(values) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(values, dtype=np.uint32))
+
+
+# --- single-pair kernels (storm.h:56-61) ---------------------------------
+def intersect_vector16(a, b) -> int:
+    a = np.ascontiguousarray(a, dtype=np.uint16)
+    b = np.ascontiguousarray(b, dtype=np.uint16)
+    r = _lib.STORM_intersect_vector16_cardinality(_p(a, u16p), _p(b, u16p), len(a), len(b))
+    _check_status("STORM_intersect_vector16_cardinality")
+    return int(r)
+
+
+def intersect_vector32(a, b):
+    """Matched index pairs of two sorted u32 arrays (STORM_intersect_vector32_unsafe)."""
+    a, b = _u32(a), _u32(b)
+    out = np.zeros(2 * max(1, min(len(a), len(b))), dtype=np.uint32)
+    k = _lib.STORM_intersect_vector32_unsafe(_p(a, u32p), _p(b, u32p), len(a), len(b), _p(out, u32p))
+    _check_status("STORM_intersect_vector32_unsafe")
+    return out[: int(k)].reshape(-1, 2)
+
+
+def intersect_bitmaps_scalar_list(b1, b2, l1, l2) -> int:
+    b1 = np.ascontiguousarray(b1, dtype=np.uint64)
+    b2 = np.ascontiguousarray(b2, dtype=np.uint64)
+    l1, l2 = _u32(l1), _u32(l2)
+    r = _lib.STORM_intersect_bitmaps_scalar_list(_p(b1, u64p), _p(b2, u64p), _p(l1, u32p), _p(l2, u32p),
+                                                 len(l1), len(l2))
+    _check_status("STORM_intersect_bitmaps_scalar_list")
+    return int(r)
+
+
+def wrapper_diag(vals: np.ndarray, blocked: int = 0) -> int:
+    vals = np.ascontiguousarray(vals, dtype=np.uint64)
+    n, w = vals.shape
+    if blocked:
+        r = _lib.STORM_wrapper_diag_blocked(n, _p(vals, u64p), w, None, blocked)
+    else:
+        r = _lib.STORM_wrapper_diag(n, _p(vals, u64p), w, None)
+    _check_status("STORM_wrapper_diag")
+    return int(r)
+
+
+def wrapper_square(v1: np.ndarray, v2: np.ndarray) -> int:
+    v1 = np.ascontiguousarray(v1, dtype=np.uint64)
+    v2 = np.ascontiguousarray(v2, dtype=np.uint64)
+    r = _lib.STORM_wrapper_square(v1.shape[0], _p(v1, u64p), v2.shape[0], _p(v2, u64p), v1.shape[1], None)
+    _check_status("STORM_wrapper_square")
+    return int(r)
+
+
+class _TileCollector:
+    def __init__(self, n: int, tile: int):
+        self.n, self.tile = n, tile
+        self.out = np.zeros(tri_size(n), dtype=np.uint32)
+        self.calls = []
+
+    def __call__(self, i0, j0, nr, nc, counts, ctx):
+        buf = np.ctypeslib.as_array(counts, shape=(self.tile * self.tile,)).reshape(self.tile, self.tile)
+        self.calls.append((i0, j0, nr, nc, int(buf[:nr, :nc].astype(np.uint64).sum())))
+        for a in range(nr):
+            i = i0 + a
+            js = np.arange(j0, j0 + nc, dtype=np.uint64)
+            keep = js > i
+            if keep.any():
+                self.out[tri_index(self.n, i, js[keep])] = buf[a, :nc][keep]
+
+
+class StormContig:
+    """STORM_contiguous_t (storm.h:224-231)."""
+
+    def __init__(self, vector_length: int):
+        self.h = _lib.STORM_contig_new(vector_length)
+        if not self.h:
+            raise StormError(ENOMEM, "STORM_contig_new")
+        self.vector_length = vector_length
+        self.n_words = (vector_length + 63) // 64
+
+    def close(self):
+        if self.h:
+            _lib.STORM_contig_free(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def add(self, values) -> int:
+        v = _u32(values)
+        return _check(_lib.STORM_contig_add(self.h, _p(v, u32p), len(v)), "STORM_contig_add")
+
+    def add_bitmaps(self, words: np.ndarray) -> int:
+        words = np.ascontiguousarray(words, dtype=np.uint64)
+        return _check(_lib.STORM_contig_add_bitmaps(self.h, _p(words, u64p), words.shape[0], words.shape[1]),
+                      "STORM_contig_add_bitmaps")
+
+    def clear(self):
+        return _lib.STORM_contig_clear(self.h)
+
+    def __len__(self):
+        return int(_lib.STORM_contig_size(self.h))
+
+    def set_kernel(self, kernel: int):
+        _check(_lib.STORM_contig_set_kernel(self.h, kernel), "STORM_contig_set_kernel")
+
+    def upload(self):
+        _check(_lib.STORM_contig_upload(self.h), "STORM_contig_upload")
+
+    def pairw_intersect_cardinality(self, blocked: int = 0) -> int:
+        if blocked:
+            r = _lib.STORM_contig_pairw_intersect_cardinality_blocked(self.h, blocked)
+        else:
+            r = _lib.STORM_contig_pairw_intersect_cardinality(self.h)
+        _check_status("STORM_contig_pairw_intersect_cardinality")
+        return int(r)
+
+    def matrix(self, out: np.ndarray | None = None):
+        n = len(self)
+        if out is None:
+            out = np.zeros(max(1, tri_size(n)), dtype=np.uint32)
+        s = C.c_uint64(0)
+        _check(_lib.STORM_contig_pairw_intersect_matrix(self.h, _p(out, u32p), out.size, C.byref(s)),
+               "STORM_contig_pairw_intersect_matrix")
+        return out[: tri_size(n)], int(s.value)
+
+    def matrix_device(self, d_out_ptr: int, out_len: int) -> int:
+        s = C.c_uint64(0)
+        _check(_lib.STORM_contig_pairw_intersect_matrix_device(self.h, C.c_void_p(d_out_ptr), out_len, C.byref(s)),
+               "STORM_contig_pairw_intersect_matrix_device")
+        return int(s.value)
+
+    def tiles(self, tile: int = 64):
+        col = _TileCollector(len(self), tile)
+        cb = TILE_CB(col)
+        _check(_lib.STORM_contig_pairw_intersect_tiles(self.h, tile, cb, None), "STORM_contig_pairw_intersect_tiles")
+        return col
+
+    def stream(self) -> int:
+        return _lib.STORM_contig_stream(self.h) or 0
+
+    def last_kernel_ms(self) -> float:
+        return float(_lib.STORM_contig_last_kernel_ms(self.h))
+
+    def last_launches(self) -> int:
+        return int(_lib.STORM_contig_last_launches(self.h))
+
+    def last_kernel(self) -> int:
+        return int(_lib.STORM_contig_last_kernel(self.h))
+
+
+class Storm:
+    """STORM_t (storm.h:214-221): rows split into 65536-bit chunks."""
+
+    def __init__(self):
+        self.h = _lib.STORM_new()
+        if not self.h:
+            raise StormError(ENOMEM, "STORM_new")
+        self.n = 0
+
+    def close(self):
+        if self.h:
+            _lib.STORM_free(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def add(self, values) -> int:
+        v = _u32(values)
+        rc = _lib.STORM_add(self.h, _p(v, u32p), len(v))
+        _check(rc, "STORM_add")
+        self.n += 1
+        return rc
+
+    def clear(self):
+        self.n = 0
+        return _lib.STORM_clear(self.h)
+
+    def __len__(self):
+        return self.n
+
+    def upload(self):
+        _check(_lib.STORM_upload(self.h), "STORM_upload")
+
+    def pairw_intersect_cardinality(self, blocked: int = 0) -> int:
+        if blocked:
+            r = _lib.STORM_pairw_intersect_cardinality_blocked(self.h, blocked)
+        else:
+            r = _lib.STORM_pairw_intersect_cardinality(self.h)
+        _check_status("STORM_pairw_intersect_cardinality")
+        return int(r)
+
+    def square(self, other: "Storm") -> int:
+        r = _lib.STORM_intersect_cardinality_square(self.h, other.h)
+        _check_status("STORM_intersect_cardinality_square")
+        return int(r)
+
+    def serialized_size(self) -> int:
+        return int(_lib.STORM_serialized_size(self.h))
+
+    def matrix(self):
+        out = np.zeros(max(1, tri_size(self.n)), dtype=np.uint32)
+        s = C.c_uint64(0)
+        _check(_lib.STORM_pairw_intersect_matrix(self.h, _p(out, u32p), out.size, C.byref(s)),
+               "STORM_pairw_intersect_matrix")
+        return out[: tri_size(self.n)], int(s.value)
+
+    def tiles(self, tile: int = 64):
+        col = _TileCollector(self.n, tile)
+        cb = TILE_CB(col)
+        _check(_lib.STORM_pairw_intersect_tiles(self.h, tile, cb, None), "STORM_pairw_intersect_tiles")
+        return col
+
+    def last_kernel_ms(self) -> float:
+        return float(_lib.STORM_last_kernel_ms(self.h))

@@ -1,0 +1,541 @@
+// storm_t.cu -- the chunked container (STORM_t and its parts) behind the
+// reference's public layout.
+//
+// Ingest builds exactly the host structures the reference builds
+// (storm.cpp:396-916): per row a STORM_bitmap_cont_t whose chunks are u16
+// lists below STORM_DEFAULT_SCALAR_THRESHOLD values and 1024-word bitmaps
+// otherwise, so callers that read the public structs see the same data.
+// Differences, all outside the reference's input contract and documented in
+// DESIGN.md:
+//   * the reference's one-past-the-end read in STORM_bitmap_cont_add
+//     (storm.cpp:768) and its scalar-buffer overflow when a second add brings
+//     more values than the remaining capacity (storm.cpp:513-523) are not
+//     reproduced;
+//   * values outside a chunk (the reference only asserts) are skipped.
+// All counting (every *_intersect_* call) runs on the GPU: the rows are
+// packed into HBM on first use and re-packed after STORM_add / STORM_clear.
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <unordered_map>
+
+#include "chunk_engine.cuh"
+
+namespace sb200 {
+
+static void* aligned_alloc64(size_t bytes) {
+    void* p = nullptr;
+    if (posix_memalign(&p, 64, bytes ? bytes : 64) != 0) return nullptr;
+    return p;
+}
+
+// Device-side state of a STORM_t, kept beside it (the public struct has no
+// room for it).  Invalidated by every mutating call through this library.
+struct StormDev {
+    ChunkDev dev;
+    ChunkEngine engine;
+    cudaStream_t stream = nullptr;
+    DevBuf<uint32_t> d_out;
+    bool valid = false;
+    ~StormDev() {
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+static std::mutex g_mu;
+static std::unordered_map<const STORM_t*, StormDev*>& table() {
+    static std::unordered_map<const STORM_t*, StormDev*> t;
+    return t;
+}
+
+static StormDev* state_of(const STORM_t* s) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    auto& t = table();
+    auto it = t.find(s);
+    if (it != t.end()) return it->second;
+    StormDev* d = new StormDev();
+    t[s] = d;
+    return d;
+}
+
+static void invalidate(const STORM_t* s) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    auto& t = table();
+    auto it = t.find(s);
+    if (it != t.end()) it->second->valid = false;
+}
+
+static void forget(const STORM_t* s) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    auto& t = table();
+    auto it = t.find(s);
+    if (it != t.end()) {
+        delete it->second;
+        t.erase(it);
+    }
+}
+
+static cudaStream_t stream_of(StormDev* d) {
+    require_device();
+    if (!d->stream) SB_CUDA(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
+    return d->stream;
+}
+
+static void ensure_packed(const STORM_t* s, StormDev* d) {
+    if (d->valid) return;
+    ChunkPack p;
+    for (uint32_t r = 0; r < s->n_conts; ++r) p.add_row(&s->conts[r]);
+    d->dev.upload(p, stream_of(d));
+    d->valid = true;
+}
+
+// One-shot engine for calls that compare a few chunks or rows.
+struct AdHoc {
+    ChunkPack pack;
+    ChunkDev dev;
+    ChunkEngine engine;
+    cudaStream_t st = nullptr;
+    AdHoc() {
+        require_device();
+        SB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    }
+    ~AdHoc() {
+        if (st) cudaStreamDestroy(st);
+    }
+    uint64_t rect(uint64_t n1, uint64_t n2) {
+        dev.upload(pack, st);
+        return engine.run(dev, PAIRS_RECT, n1, n2, nullptr, st);
+    }
+};
+
+}  // namespace sb200
+
+using namespace sb200;
+
+extern "C" {
+
+/* ---------------------------------------------------------------- chunks */
+
+STORM_bitmap_t* STORM_bitmap_new(void) {
+    STORM_bitmap_t* b = (STORM_bitmap_t*)malloc(sizeof(STORM_bitmap_t));
+    if (!b) return NULL;
+    STORM_bitmap_init(b);
+    return b;
+}
+
+void STORM_bitmap_init(STORM_bitmap_t* b) {
+    if (!b) return;
+    b->data = NULL;
+    b->scalar = NULL;
+    b->n_bitmap = 0;
+    b->own_data = 1;
+    b->own_scalar = 1;
+    b->n_bits_set = 0;
+    b->n_scalar = 0;
+    b->n_scalar_set = 0;
+    b->n_missing = 0;
+    b->m_scalar = 0;
+    b->id = 0;
+}
+
+static void bitmap_free_members(STORM_bitmap_t* b) {
+    if (!b) return;
+    if (b->own_data) free(b->data);
+    if (b->own_scalar) free(b->scalar);
+    b->data = NULL;
+    b->scalar = NULL;
+}
+
+void STORM_bitmap_free(STORM_bitmap_t* b) {
+    if (!b) return;
+    bitmap_free_members(b);
+    free(b);
+}
+
+static bool ensure_data(STORM_bitmap_t* b) {
+    if (b->data == NULL) {
+        b->data = (uint64_t*)aligned_alloc64(CHUNK_WORDS * sizeof(uint64_t));
+        if (!b->data) return false;
+        memset(b->data, 0, CHUNK_WORDS * sizeof(uint64_t));
+        b->own_data = 1;
+    }
+    b->n_bitmap = CHUNK_WORDS;
+    return true;
+}
+
+static bool ensure_scalar(STORM_bitmap_t* b, uint32_t extra) {
+    const uint64_t need = (uint64_t)b->n_scalar + extra;
+    if (b->scalar != NULL && need <= b->m_scalar) return true;
+    uint64_t m = b->scalar ? need + 1024 : (extra > 256 ? (uint64_t)extra + 256 : 256);
+    if (m < need) m = need;
+    uint16_t* p = (uint16_t*)aligned_alloc64(m * sizeof(uint16_t));
+    if (!p) return false;
+    if (b->scalar) {
+        memcpy(p, b->scalar, b->n_scalar * sizeof(uint16_t));
+        if (b->own_scalar) free(b->scalar);
+    }
+    b->scalar = p;
+    b->m_scalar = (uint32_t)m;
+    b->own_scalar = 1;
+    return true;
+}
+
+// storm.cpp:476-499: -1 / -2 / -3, sets bits of values in this chunk.
+int STORM_bitmap_add(STORM_bitmap_t* b, const uint32_t* values, const uint32_t n_values) {
+    if (b == NULL) return -1;
+    if (values == NULL) return -2;
+    if (n_values == 0) return -3;
+    if (!ensure_data(b)) return STORM_B200_ENOMEM;
+    const uint64_t base = (uint64_t)b->id * STORM_DEFAULT_BLOCK_SIZE;
+    for (uint32_t i = 0; i < n_values; ++i) {
+        if (values[i] < base || values[i] - base >= STORM_DEFAULT_BLOCK_SIZE) continue;
+        const uint32_t v = (uint32_t)(values[i] - base);
+        const uint64_t bit = 1ull << (v & 63);
+        b->n_bits_set += (b->data[v >> 6] & bit) == 0;
+        b->data[v >> 6] |= bit;
+    }
+    return (int)n_values;
+}
+
+// storm.cpp:502-553: -1 / -3 / -4; bitmap plus the list of newly set values.
+int STORM_bitmap_add_with_scalar(STORM_bitmap_t* b, const uint32_t* values, const uint32_t n_values) {
+    if (b == NULL) return -1;
+    if (values == NULL) return -3;
+    if (n_values == 0) return -4;
+    if (!ensure_data(b) || !ensure_scalar(b, n_values)) return STORM_B200_ENOMEM;
+    const uint64_t base = (uint64_t)b->id * STORM_DEFAULT_BLOCK_SIZE;
+    b->n_scalar_set = 1;
+    for (uint32_t i = 0; i < n_values; ++i) {
+        if (values[i] < base || values[i] - base >= STORM_DEFAULT_BLOCK_SIZE) continue;
+        const uint32_t v = (uint32_t)(values[i] - base);
+        const uint64_t bit = 1ull << (v & 63);
+        if ((b->data[v >> 6] & bit) == 0) {
+            b->data[v >> 6] |= bit;
+            b->scalar[b->n_scalar] = (uint16_t)v;
+            ++b->n_scalar;
+            ++b->n_bits_set;
+        }
+    }
+    return (int)n_values;
+}
+
+// storm.cpp:555-592: -1 / -3 / -4; appends values as chunk offsets.
+int STORM_bitmap_add_scalar_only(STORM_bitmap_t* b, const uint32_t* values, const uint32_t n_values) {
+    if (b == NULL) return -1;
+    if (values == NULL) return -3;
+    if (n_values == 0) return -4;
+    if (!ensure_scalar(b, n_values)) return STORM_B200_ENOMEM;
+    const uint64_t base = (uint64_t)b->id * STORM_DEFAULT_BLOCK_SIZE;
+    b->n_scalar_set = 1;
+    for (uint32_t i = 0; i < n_values; ++i) {
+        if (values[i] < base || values[i] - base >= STORM_DEFAULT_BLOCK_SIZE) continue;
+        b->scalar[b->n_scalar] = (uint16_t)(values[i] - base);
+        ++b->n_scalar;
+        ++b->n_bits_set;
+    }
+    return (int)n_values;
+}
+
+int STORM_bitmap_clear(STORM_bitmap_t* b) {
+    if (b == NULL) return -1;
+    if (b->data != NULL) memset(b->data, 0, sizeof(uint64_t) * b->n_bitmap);
+    b->n_scalar = 0;
+    b->n_bits_set = 0;
+    b->n_bitmap = 0;
+    return 1;
+}
+
+uint32_t STORM_bitmap_serialized_size(STORM_bitmap_t* b) {
+    uint32_t total = (uint32_t)sizeof(uint64_t) * b->n_bitmap;
+    if (b->n_scalar_set) total += (uint32_t)sizeof(uint16_t) * b->n_scalar;
+    return total + 4 * (uint32_t)sizeof(uint32_t);
+}
+
+// storm.cpp:595-650: one chunk pair, 0 for NULL or different chunk ids.
+uint64_t STORM_bitmap_intersect_cardinality(STORM_bitmap_t* STORM_RESTRICT b1, STORM_bitmap_t* STORM_RESTRICT b2) {
+    if (b1 == NULL || b2 == NULL) return 0;
+    if (b1->id != b2->id) return 0;
+    uint64_t r = 0;
+    guard([&]() -> int {
+        AdHoc h;
+        h.pack.add_chunk(b1->id, *b1);
+        h.pack.end_row();
+        h.pack.add_chunk(b2->id, *b2);
+        h.pack.end_row();
+        r = h.rect(1, 1);
+        return 0;
+    });
+    return r;
+}
+
+uint64_t STORM_bitmap_intersect_cardinality_func(STORM_bitmap_t* STORM_RESTRICT b1, STORM_bitmap_t* STORM_RESTRICT b2,
+                                                 const STORM_compute_func func) {
+    (void)func;
+    return STORM_bitmap_intersect_cardinality(b1, b2);
+}
+
+/* ------------------------------------------------------------ containers */
+
+STORM_bitmap_cont_t* STORM_bitmap_cont_new(void) {
+    STORM_bitmap_cont_t* c = (STORM_bitmap_cont_t*)malloc(sizeof(STORM_bitmap_cont_t));
+    if (!c) return NULL;
+    STORM_bitmap_cont_init(c);
+    return c;
+}
+
+void STORM_bitmap_cont_init(STORM_bitmap_cont_t* c) {
+    if (!c) return;
+    c->bitmaps = NULL;
+    c->block_ids = NULL;
+    c->n_bitmaps = 0;
+    c->m_bitmaps = 0;
+    c->prev_inserted_value = 0;
+}
+
+static void cont_free_members(STORM_bitmap_cont_t* c) {
+    if (!c) return;
+    if (c->bitmaps) {
+        // Entries past n_bitmaps only ever hold buffers that clear() kept.
+        for (uint32_t i = 0; i < c->m_bitmaps; ++i) bitmap_free_members(&c->bitmaps[i]);
+        free(c->bitmaps);
+    }
+    free(c->block_ids);
+    c->bitmaps = NULL;
+    c->block_ids = NULL;
+    c->n_bitmaps = 0;
+    c->m_bitmaps = 0;
+}
+
+void STORM_bitmap_cont_free(STORM_bitmap_cont_t* c) {
+    if (!c) return;
+    cont_free_members(c);
+    free(c);
+}
+
+static bool cont_reserve(STORM_bitmap_cont_t* c, uint32_t n) {
+    if (n <= c->m_bitmaps && c->bitmaps && c->block_ids) return true;
+    uint32_t m = c->m_bitmaps ? c->m_bitmaps : 2;
+    while (m < n) m += 8;
+    STORM_bitmap_t* nb = (STORM_bitmap_t*)realloc(c->bitmaps, sizeof(STORM_bitmap_t) * m);
+    if (!nb) return false;
+    for (uint32_t i = c->m_bitmaps; i < m; ++i) STORM_bitmap_init(&nb[i]);
+    c->bitmaps = nb;
+    uint32_t* ni = (uint32_t*)realloc(c->block_ids, sizeof(uint32_t) * m);
+    if (!ni) return false;
+    c->block_ids = ni;
+    c->m_bitmaps = m;
+    return true;
+}
+
+// storm.cpp:737-803: split sorted values by chunk; a run of fewer than
+// STORM_DEFAULT_SCALAR_THRESHOLD values becomes a u16 list, otherwise a
+// bitmap.  -1 NULL container, -2 NULL values, 0 for n == 0, 1 on success.
+int STORM_bitmap_cont_add(STORM_bitmap_cont_t* c, const uint32_t* values, const uint32_t n_values) {
+    if (c == NULL) return -1;
+    if (values == NULL) return -2;
+    if (n_values == 0) return 0;
+    uint32_t start = 0;
+    while (start < n_values) {
+        const uint32_t id = values[start] / STORM_DEFAULT_BLOCK_SIZE;
+        uint32_t stop = start;
+        while (stop < n_values && values[stop] / STORM_DEFAULT_BLOCK_SIZE == id) ++stop;
+        if (!cont_reserve(c, c->n_bitmaps + 1)) return STORM_B200_ENOMEM;
+        STORM_bitmap_t* x = &c->bitmaps[c->n_bitmaps];
+        x->id = id;
+        c->block_ids[c->n_bitmaps] = id;
+        int rc = (stop - start < STORM_DEFAULT_SCALAR_THRESHOLD)
+                     ? STORM_bitmap_add_scalar_only(x, values + start, stop - start)
+                     : STORM_bitmap_add(x, values + start, stop - start);
+        if (rc < 0) return rc;
+        ++c->n_bitmaps;
+        c->prev_inserted_value = values[stop - 1];
+        start = stop;
+    }
+    return 1;
+}
+
+int STORM_bitmap_cont_clear(STORM_bitmap_cont_t* c) {
+    if (c == NULL) return -1;
+    for (uint32_t i = 0; i < c->n_bitmaps; ++i) STORM_bitmap_clear(&c->bitmaps[i]);
+    c->n_bitmaps = 0;
+    c->prev_inserted_value = 0;
+    return 1;
+}
+
+// storm.cpp:804-833: one row pair.
+uint64_t STORM_bitmap_cont_intersect_cardinality(const STORM_bitmap_cont_t* STORM_RESTRICT c1,
+                                                 const STORM_bitmap_cont_t* STORM_RESTRICT c2) {
+    if (c1 == NULL || c2 == NULL) return 0;
+    if (c1->n_bitmaps == 0 || c2->n_bitmaps == 0) return 0;
+    uint64_t r = 0;
+    guard([&]() -> int {
+        AdHoc h;
+        h.pack.add_row(c1);
+        h.pack.add_row(c2);
+        r = h.rect(1, 1);
+        return 0;
+    });
+    return r;
+}
+
+uint64_t STORM_bitmap_cont_intersect_cardinality_premade(const STORM_bitmap_cont_t* STORM_RESTRICT c1,
+                                                         const STORM_bitmap_cont_t* STORM_RESTRICT c2,
+                                                         const STORM_compute_func func, uint32_t* out) {
+    (void)func;
+    if (out == NULL) return 0;
+    return STORM_bitmap_cont_intersect_cardinality(c1, c2);
+}
+
+uint32_t STORM_bitmap_cont_serialized_size(STORM_bitmap_cont_t* c) {
+    uint32_t total = 0;
+    if (c->bitmaps != NULL)
+        for (uint32_t i = 0; i < c->n_bitmaps; ++i) total += STORM_bitmap_serialized_size(&c->bitmaps[i]);
+    return total + (uint32_t)sizeof(uint32_t) * c->n_bitmaps + 3 * (uint32_t)sizeof(uint32_t);
+}
+
+/* ----------------------------------------------------------------- STORM_t */
+
+STORM_t* STORM_new(void) {
+    STORM_t* s = (STORM_t*)malloc(sizeof(STORM_t));
+    if (!s) return NULL;
+    s->conts = NULL;
+    s->n_conts = 0;
+    s->m_conts = 0;
+    return s;
+}
+
+void STORM_free(STORM_t* s) {
+    if (s == NULL) return;
+    forget(s);
+    if (s->conts)
+        for (uint32_t i = 0; i < s->m_conts; ++i) cont_free_members(&s->conts[i]);
+    free(s->conts);
+    free(s);
+}
+
+// storm.cpp:894-916: always appends a row (even for n == 0), returns 1.
+int STORM_add(STORM_t* s, const uint32_t* values, const uint32_t n_values) {
+    if (s == NULL) return -1;
+    invalidate(s);
+    if (s->n_conts == s->m_conts) {
+        const uint32_t m = s->m_conts + 1024;
+        STORM_bitmap_cont_t* nc = (STORM_bitmap_cont_t*)realloc(s->conts, m * sizeof(STORM_bitmap_cont_t));
+        if (!nc) return STORM_B200_ENOMEM;
+        for (uint32_t i = s->m_conts; i < m; ++i) STORM_bitmap_cont_init(&nc[i]);
+        s->conts = nc;
+        s->m_conts = m;
+    }
+    STORM_bitmap_cont_add(&s->conts[s->n_conts++], values, n_values);
+    return 1;
+}
+
+int STORM_clear(STORM_t* s) {
+    if (s == NULL) return -1;
+    invalidate(s);
+    for (uint32_t i = 0; i < s->n_conts; ++i) STORM_bitmap_cont_clear(&s->conts[i]);
+    s->n_conts = 0;
+    return 1;
+}
+
+int STORM_upload(STORM_t* s) {
+    if (s == NULL) return STORM_B200_ENULL;
+    return guard([&]() -> int {
+        ensure_packed(s, state_of(s));
+        return 0;
+    });
+}
+
+// storm.cpp:927-945: sum over i < j; (uint64_t)-1 for NULL.
+uint64_t STORM_pairw_intersect_cardinality(STORM_t* s) {
+    if (s == NULL) return (uint64_t)-1;
+    uint64_t r = 0;
+    guard([&]() -> int {
+        StormDev* d = state_of(s);
+        ensure_packed(s, d);
+        r = d->engine.run(d->dev, PAIRS_TRIANGLE, s->n_conts, 0, nullptr, stream_of(d));
+        return 0;
+    });
+    return r;
+}
+
+// storm.cpp:947-1011: the same sum, traversed in CPU cache blocks; the GPU
+// path does its own tiling, so bsize does not change the work.
+uint64_t STORM_pairw_intersect_cardinality_blocked(STORM_t* s, uint32_t bsize) {
+    (void)bsize;
+    return STORM_pairw_intersect_cardinality(s);
+}
+
+// storm.cpp:1027-1046: sum over all (i in s1, j in s2).
+uint64_t STORM_intersect_cardinality_square(const STORM_t* STORM_RESTRICT s1, const STORM_t* STORM_RESTRICT s2) {
+    if (s1 == NULL || s2 == NULL) return 0;
+    uint64_t r = 0;
+    guard([&]() -> int {
+        AdHoc h;
+        for (uint32_t i = 0; i < s1->n_conts; ++i) h.pack.add_row(&s1->conts[i]);
+        for (uint32_t i = 0; i < s2->n_conts; ++i) h.pack.add_row(&s2->conts[i]);
+        r = h.rect(s1->n_conts, s2->n_conts);
+        return 0;
+    });
+    return r;
+}
+
+uint64_t STORM_serialized_size(const STORM_t* s) {
+    if (s == NULL) return 0;
+    uint64_t tot = 0;
+    for (uint32_t i = 0; i < s->n_conts; ++i) tot += STORM_bitmap_cont_serialized_size(&s->conts[i]);
+    return tot + 2 * sizeof(uint32_t);
+}
+
+int STORM_pairw_intersect_matrix(STORM_t* s, uint32_t* out, uint64_t out_len, uint64_t* sum) {
+    if (s == NULL) return STORM_B200_ENULL;
+    const uint64_t need = tri_size(s->n_conts);
+    if (out == NULL && need) return STORM_B200_EVALUES;
+    if (out_len < need) return STORM_B200_ESIZE;
+    return guard([&]() -> int {
+        StormDev* d = state_of(s);
+        ensure_packed(s, d);
+        cudaStream_t st = stream_of(d);
+        d->d_out.reserve(need ? need : 1);
+        const uint64_t r = d->engine.run(d->dev, PAIRS_TRIANGLE, s->n_conts, 0, d->d_out.p, st);
+        if (need) {
+            SB_CUDA(cudaMemcpyAsync(out, d->d_out.p, need * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+            SB_CUDA(cudaStreamSynchronize(st));
+        }
+        if (sum) *sum = r;
+        return 0;
+    });
+}
+
+int STORM_pairw_intersect_tiles(STORM_t* s, uint32_t tile, STORM_tile_callback cb, void* ctx) {
+    if (s == NULL) return STORM_B200_ENULL;
+    if (cb == NULL || tile == 0) return STORM_B200_EARG;
+    const uint64_t n = s->n_conts;
+    std::vector<uint32_t> tri(tri_size(n) ? tri_size(n) : 1);
+    int rc = STORM_pairw_intersect_matrix(s, tri.data(), tri.size(), NULL);
+    if (rc < 0) return rc;
+    return guard([&]() -> int {
+        std::vector<uint32_t> buf((size_t)tile * tile);
+        for (uint64_t i0 = 0; i0 < n; i0 += tile) {
+            const uint64_t i1 = std::min<uint64_t>(i0 + tile, n);
+            for (uint64_t j0 = i0; j0 < n; j0 += tile) {
+                const uint64_t j1 = std::min<uint64_t>(j0 + tile, n);
+                std::fill(buf.begin(), buf.end(), 0u);
+                for (uint64_t i = i0; i < i1; ++i) {
+                    const uint64_t base = i * n - (i * (i - 1)) / 2 - i;
+                    for (uint64_t j = (j0 == i0 ? i + 1 : j0); j < j1; ++j)
+                        buf[(i - i0) * tile + (j - j0)] = tri[base + j];
+                }
+                cb((uint32_t)i0, (uint32_t)j0, (uint32_t)(i1 - i0), (uint32_t)(j1 - j0), buf.data(), ctx);
+            }
+        }
+        return 0;
+    });
+}
+
+float STORM_last_kernel_ms(const STORM_t* s) {
+    if (s == NULL) return 0.f;
+    return state_of(s)->engine.log.last_ms;
+}
+
+}  // extern "C"

@@ -1,0 +1,197 @@
+"""STORM_contiguous_t on the GPU against the oracle and the reference's
+golden vectors: both bitmap x bitmap kernels (CUDA-core POPC and tcgen05),
+bit-exact, on the reference's own cases, edge shapes and the full-size
+dense configurations (sampled pairs + size-independent identities)."""
+import numpy as np
+import pytest
+
+import gen
+import oracle_lib as ol
+
+pytestmark = pytest.mark.gpu
+
+KERNELS = ("popc", "mma")
+
+
+def _kernel(sb, name):
+    return {"popc": sb.KERNEL_POPC, "mma": sb.KERNEL_MMA}[name]
+
+
+def contig_from_words(sb, words, m, kernel):
+    c = sb.StormContig(m)
+    c.set_kernel(_kernel(sb, kernel))
+    c.add_bitmaps(words)
+    return c
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_golden_contig_cases(sb, golden, kernel):
+    names = sorted({k.split("/")[1] for k in golden.files if k.startswith("contig/")})
+    for name in names:
+        words = golden[f"contig/{name}/words"]
+        m = int(golden[f"contig/{name}/m"][0])
+        c = contig_from_words(sb, words, m, kernel)
+        mat, s = c.matrix()
+        assert s == int(golden[f"contig/{name}/sum"][0]), name
+        np.testing.assert_array_equal(mat, golden[f"contig/{name}/matrix"], err_msg=f"{name}/{kernel}")
+        assert c.pairw_intersect_cardinality() == s
+        assert c.last_kernel() == _kernel(sb, kernel)
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+@pytest.mark.parametrize("n,m,p", [
+    (1, 64, 0.5), (2, 65, 0.5), (3, 640, 0.9), (127, 1000, 0.3), (128, 4096, 0.5), (129, 4097, 0.2),
+    (255, 512, 0.5), (256, 128, 0.7), (257, 8192, 0.01), (300, 2048 + 64, 0.5), (513, 256, (0.0, 1.0)),
+])
+def test_edge_shapes_match_oracle(sb, kernel, n, m, p):
+    words = gen.bernoulli_rows(n, m, p, seed=1000 + n + m)
+    c = contig_from_words(sb, words, m, kernel)
+    mat, s = c.matrix()
+    want, ws = ol.contig_matrix(words)
+    assert s == ws
+    np.testing.assert_array_equal(mat, want)
+
+
+def test_all_ones_and_empty_rows(sb):
+    m = 4096
+    words = np.zeros((260, m // 64), dtype=np.uint64)
+    words[::3] = np.uint64(0xFFFFFFFFFFFFFFFF)
+    words[1::7, 5] = np.uint64(1)
+    for kernel in KERNELS:
+        c = contig_from_words(sb, words, m, kernel)
+        mat, s = c.matrix()
+        want, ws = ol.contig_matrix(words)
+        assert s == ws
+        np.testing.assert_array_equal(mat, want)
+
+
+def test_add_positions_with_duplicates_matches_set_semantics(sb):
+    g = gen.rng(7)
+    m = 8192
+    c = sb.StormContig(m)
+    sets = []
+    for r in range(70):
+        v = np.sort(g.integers(0, m, size=int(g.integers(1, 300)))).astype(np.uint32)  # duplicates kept
+        assert c.add(v) == v.size
+        sets.append(np.unique(v))
+    assert c.add(np.zeros(0, np.uint32)) == 0       # reference: n == 0 adds no row
+    assert len(c) == 70
+    mat, s = c.matrix()
+    want, ws = ol.contig_matrix(gen.sets_to_rows(sets, m))
+    assert s == ws
+    np.testing.assert_array_equal(mat, want)
+
+
+def test_mixed_ingest_order_clear_and_reuse(sb):
+    m = 1000
+    a = gen.bernoulli_rows(40, m, 0.2, 3)
+    b = gen.bernoulli_rows(50, m, 0.4, 4)
+    c = sb.StormContig(m)
+    for row in gen.rows_to_sets(a, m):
+        c.add(row) if row.size else None
+    c.add_bitmaps(b)
+    rows = np.concatenate([np.stack([r for r, s in zip(a, gen.rows_to_sets(a, m)) if s.size]), b])
+    mat, s = c.matrix()
+    want, ws = ol.contig_matrix(rows)
+    np.testing.assert_array_equal(mat, want)
+    assert c.clear() == 1 and len(c) == 0
+    c.add_bitmaps(b)
+    mat, s = c.matrix()
+    want, ws = ol.contig_matrix(b)
+    np.testing.assert_array_equal(mat, want)
+
+
+def test_device_input_tail_bits_are_masked(sb):
+    torch = pytest.importorskip("torch")
+    m = 100   # 2 words, 36 tail bits
+    words = gen.bernoulli_rows(33, 128, 0.5, 9)   # random bits beyond m
+    d = torch.from_numpy(words.view(np.int64)).cuda()
+    c = sb.StormContig(m)
+    rc = sb.lib().STORM_contig_add_bitmaps(c.h, sb.C.cast(d.data_ptr(), sb.u64p), 33, 2)
+    assert rc == 33
+    mat, _ = c.matrix()
+    masked = words.copy()
+    masked[:, 1] &= np.uint64((1 << 36) - 1)
+    want, _ = ol.contig_matrix(masked)
+    np.testing.assert_array_equal(mat, want)
+
+
+@pytest.mark.parametrize("tile", [8, 64, 100])
+def test_tiles_callback_matches_matrix(sb, tile):
+    words = gen.bernoulli_rows(150, 2048, 0.3, 77)
+    c = contig_from_words(sb, words, 2048, "mma")
+    mat, s = c.matrix()
+    col = c.tiles(tile)
+    n = 150
+    iu = np.triu_indices(n)
+    strict = iu[0] != iu[1]
+    np.testing.assert_array_equal(col.out[strict], mat[strict])
+    assert sum(x[4] for x in col.calls) == s
+    # every tile of the triangle visited once, diagonal tiles included
+    nt = (n + tile - 1) // tile
+    assert len(col.calls) == nt * (nt + 1) // 2
+
+
+def test_wrappers_and_lowlevel_match_reference(sb, golden):
+    w = golden["wrapper_diag/words"]
+    assert sb.wrapper_diag(w) == golden["wrapper_diag/sum"][0]
+    assert sb.wrapper_diag(w, blocked=4) == golden["wrapper_diag/sum"][1]
+    v1, v2 = w[:10], w[10:]
+    want = sum(ol.and_popcount(x, y) for x in v1 for y in v2)
+    assert sb.wrapper_square(v1, v2) == want
+
+
+def _cfg_rows_gpu(n, m, p, seed):
+    torch = pytest.importorskip("torch")
+    import bench
+    return bench.bernoulli_rows_gpu(n, m, p, seed, torch.device("cuda"))
+
+
+def _check_full_size(sb, n, m, p, seed, kernels):
+    """Full-size dense configuration: device-resident output, checked by
+    (a) oracle on every pair of a row sample, (b) diagonal = row popcounts,
+    (c) kernel-vs-kernel identity, (d) sum identity."""
+    import torch
+    rows = _cfg_rows_gpu(n, m, p, seed)           # int64 [n, w] on device
+    host = rows.cpu().numpy().view(np.uint64)
+    tri = n * (n + 1) // 2
+    results = {}
+    for k in kernels:
+        c = sb.StormContig(m)
+        c.set_kernel(_kernel(sb, k))
+        c.add_bitmaps(host)
+        out = torch.empty(tri, dtype=torch.int32, device="cuda")
+        s = c.matrix_device(out.data_ptr(), tri)
+        results[k] = (out, s)
+    out, s = results[kernels[0]]
+    # (a) sampled rows, every pair of each: oracle on the host.
+    g = gen.rng(seed)
+    sample = np.unique(np.concatenate([[0, n - 1], g.integers(0, n, size=6)]))
+    for i in sample:
+        want = ol.contig_row(host, int(i))
+        base = int(sb.tri_index(n, i, i))
+        got = out[base: base + (n - i)].cpu().numpy().view(np.uint32)
+        np.testing.assert_array_equal(got, want, err_msg=f"row {i}")
+    # (b) diagonal
+    ii = np.arange(n, dtype=np.uint64)
+    diag_idx = torch.from_numpy(sb.tri_index(n, ii, ii).astype(np.int64)).cuda()
+    diag = out[diag_idx].cpu().numpy().view(np.uint32)
+    pc = ol.row_popcounts(host).astype(np.int64)
+    np.testing.assert_array_equal(diag, pc)
+    # (c) kernels agree bit for bit
+    for k in kernels[1:]:
+        assert torch.equal(results[k][0], out), k
+        assert results[k][1] == s
+    # (d) sum over i < j = total - trace
+    total = int(out.view(torch.int32).to(torch.int64).bitwise_and(0xFFFFFFFF).sum().item())
+    assert s == total - int(pc.sum())
+
+
+def test_config1_full_size_both_kernels(sb):
+    """4096 rows x 65536 bits, Bernoulli(0.5): every pair, both kernels."""
+    _check_full_size(sb, 4096, 65536, 0.5, 101, ["mma", "popc"])
+
+
+def test_config2_full_size_tensor_kernel(sb):
+    """65536 rows x 262144 bits, p ~ U[0.05, 0.5] (2 GiB in, 8.6 GB out)."""
+    _check_full_size(sb, 65536, 262144, (0.05, 0.5), 202, ["mma"])

@@ -1,0 +1,151 @@
+"""The CPU oracle (oracle/storm_oracle.c) pinned against the golden vectors
+the reference itself produced (tests/golden/make_golden.py).  No GPU."""
+import numpy as np
+import pytest
+
+import gen
+import oracle_lib as ol
+from conftest import golden_sets
+
+P = ol._p
+
+
+def contig_cases(z):
+    return sorted({k.split("/")[1] for k in z.files if k.startswith("contig/")})
+
+
+def storm_cases(z):
+    return sorted({k.split("/")[1] for k in z.files if k.startswith("storm/")})
+
+
+def test_oracle_contig_matches_reference(golden):
+    for name in contig_cases(golden):
+        words = golden[f"contig/{name}/words"]
+        mat, s = ol.contig_matrix(words)
+        assert s == int(golden[f"contig/{name}/sum"][0]), name
+        np.testing.assert_array_equal(mat, golden[f"contig/{name}/matrix"], err_msg=name)
+
+
+def test_oracle_sets_match_reference(golden):
+    for name in storm_cases(golden):
+        vals, offs = golden[f"storm/{name}/vals"], golden[f"storm/{name}/offs"]
+        mat, s = ol.sets_matrix(vals, offs)
+        assert s == int(golden[f"storm/{name}/sum"][0]), name
+        # The reference's diagonal is not part of its output; compare i < j.
+        n = len(offs) - 1
+        iu = np.triu_indices(n)
+        strict = iu[0] != iu[1]
+        np.testing.assert_array_equal(mat[strict], golden[f"storm/{name}/matrix"][strict], err_msg=name)
+
+
+def test_oracle_chunk_split_matches_reference_layout(golden):
+    O = ol.oracle()
+    for name in storm_cases(golden):
+        if f"storm/{name}/layout" not in golden.files:
+            continue
+        r = int(golden[f"storm/{name}/layout_row"][0])
+        sets = golden_sets(golden, f"storm/{name}/")
+        v = np.ascontiguousarray(sets[r], dtype=np.uint32)
+        ids = np.zeros(v.size, np.uint32); kinds = np.zeros(v.size, np.uint8); cnt = np.zeros(v.size, np.uint32)
+        k = O.oracle_chunk_split(P(v, ol.u32p), v.size, P(ids, ol.u32p), P(kinds, ol.u8p), P(cnt, ol.u32p))
+        want = golden[f"storm/{name}/layout"]
+        np.testing.assert_array_equal(ids[:k], want[0], err_msg=name)
+        np.testing.assert_array_equal(kinds[:k], want[1], err_msg=name)
+        np.testing.assert_array_equal(cnt[:k], want[2], err_msg=name)
+
+
+def test_oracle_square_matches_reference(golden):
+    O = ol.oracle()
+    av, ao, bv, bo = (np.ascontiguousarray(golden[f"square/{k}"]) for k in ("a_vals", "a_offs", "b_vals", "b_offs"))
+    s = O.oracle_sets_square(P(av, ol.u32p), P(ao, ol.u64p), len(ao) - 1, P(bv, ol.u32p), P(bo, ol.u64p), len(bo) - 1)
+    assert s == int(golden["square/sum"][0])
+
+
+def test_oracle_lowlevel_matches_reference(golden):
+    O = ol.oracle()
+    A = golden_sets(golden, "vec16/a_")
+    B = golden_sets(golden, "vec16/b_")
+    for a, b, want in zip(A, B, golden["vec16/result"]):
+        a = np.ascontiguousarray(a, np.uint32); b = np.ascontiguousarray(b, np.uint32)
+        assert O.oracle_list_intersect(P(a, ol.u32p), a.size, P(b, ol.u32p), b.size) == want
+    A = golden_sets(golden, "bsl/a_")
+    B = golden_sets(golden, "bsl/b_")
+    for a, b, want in zip(A, B, golden["bsl/result"]):
+        a = np.ascontiguousarray(a, np.uint32); b = np.ascontiguousarray(b, np.uint32)
+        assert O.oracle_list_intersect(P(a, ol.u32p), a.size, P(b, ol.u32p), b.size) == want
+    w = golden["wrapper_diag/words"]
+    _, s = ol.contig_matrix(w)
+    assert s == golden["wrapper_diag/sum"][0] == golden["wrapper_diag/sum"][1]
+
+
+def test_oracle_kernel_layer_matches_reference(golden):
+    names = sorted({k.split("/")[1] for k in golden.files if k.startswith("rows/")})
+    assert names
+    for name in names:
+        vals, offs = golden[f"rows/{name}/vals"], golden[f"rows/{name}/offs"]
+        mat, s = ol.sets_matrix(vals, offs)
+        for pol, tile, ssum, pairs, skipped, dec in golden[f"rows/{name}/allpairs_sum"]:
+            assert ssum == s, (name, pol, tile)
+            n = len(offs) - 1
+            assert pairs == n * (n - 1) // 2
+        n = len(offs) - 1
+        iu = np.triu_indices(n)
+        strict = iu[0] != iu[1]
+        np.testing.assert_array_equal(mat[strict], golden[f"rows/{name}/tiles_strict"][strict], err_msg=name)
+    A = golden_sets(golden, "cells/a_")
+    B = golden_sets(golden, "cells/b_")
+    O = ol.oracle()
+    for a, b, want in zip(A, B, golden["cells/result"]):
+        a = np.ascontiguousarray(a, np.uint32); b = np.ascontiguousarray(b, np.uint32)
+        assert O.oracle_list_intersect(P(a, ol.u32p), a.size, P(b, ol.u32p), b.size) == want
+
+
+def _csr_item(z, key, i):
+    offs = z[key + "_offs"]
+    return z[key + "_vals"][int(offs[i]):int(offs[i + 1])]
+
+
+def test_oracle_representations_match_reference(golden):
+    O = ol.oracle()
+    rows = golden_sets(golden, "repr/")
+    for i, (v, u) in enumerate(zip(rows, golden["repr/universe"])):
+        v = np.ascontiguousarray(v, np.uint32)
+        u = int(u)
+        nw = (u + 63) // 64
+        rs = np.zeros(v.size + 1, np.uint32); re = np.zeros(v.size + 1, np.uint32)
+        k = O.oracle_runs(P(v, ol.u32p), v.size, P(rs, ol.u32p), P(re, ol.u32p))
+        np.testing.assert_array_equal(rs[:k], _csr_item(golden, "repr/runs", i))
+        np.testing.assert_array_equal(re[:k], _csr_item(golden, "repr/run_end", i))
+        bm = gen.sets_to_rows([v], u)[0]
+        ew = np.zeros(2 * nw + 2, np.uint64)
+        k = O.oracle_ewah(P(bm, ol.u64p), nw, P(ew, ol.u64p))
+        np.testing.assert_array_equal(ew[:k], _csr_item(golden, "repr/ewah", i))
+        dec = np.zeros(nw, np.uint64)
+        O.oracle_ewah_decode(P(ew, ol.u64p), k, P(dec, ol.u64p))
+        np.testing.assert_array_equal(dec, bm)
+        meta = np.zeros(8, np.uint32)
+        O.oracle_row_meta(P(v, ol.u32p), v.size, u, P(meta, ol.u32p))
+        np.testing.assert_array_equal(meta, golden["repr/meta"][i])
+        want_rank = _csr_item(golden, "repr/rank", i)
+        if want_rank.size:   # built only where the reference gates it on (mean run >= 512)
+            rk = np.zeros(2 * ((nw + 7) // 8 + 1), np.uint64)
+            O.oracle_rank9(P(bm, ol.u64p), nw, P(rk, ol.u64p))
+            np.testing.assert_array_equal(rk, want_rank)
+        want_occ = _csr_item(golden, "repr/occ", i)
+        if want_occ.size:
+            oc = np.zeros(want_occ.size, np.uint64)
+            O.oracle_occ(P(bm, ol.u64p), nw, 8, P(oc, ol.u64p))
+            np.testing.assert_array_equal(oc, want_occ)
+        want_comp = _csr_item(golden, "repr/comp", i)
+        if want_comp.size:
+            cp = np.zeros(u, np.uint32)
+            k = O.oracle_complement(P(v, ol.u32p), v.size, u, P(cp, ol.u32p))
+            np.testing.assert_array_equal(cp[:k], want_comp)
+
+
+def test_oracle_catches_a_planted_mistake(golden):
+    """A checker that cannot fail is worthless: flip one bit, expect a mismatch."""
+    words = golden["contig/dense_1024/words"].copy()
+    words[3, 5] ^= np.uint64(1 << 17)
+    mat, _ = ol.contig_matrix(words)
+    assert not np.array_equal(mat, golden["contig/dense_1024/matrix"])

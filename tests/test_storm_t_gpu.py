@@ -1,0 +1,120 @@
+"""STORM_t (65536-bit chunks) and the reference's single-pair kernels on the
+GPU, against the reference's golden vectors and the oracle."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import gen
+import oracle_lib as ol
+from conftest import golden_sets, ROOT
+
+pytestmark = pytest.mark.gpu
+
+
+def build_storm(sb, sets):
+    s = sb.Storm()
+    for v in sets:
+        s.add(np.asarray(v, dtype=np.uint32))
+    return s
+
+
+def storm_cases(z):
+    return sorted({k.split("/")[1] for k in z.files if k.startswith("storm/")})
+
+
+def test_golden_storm_sums_and_matrices(sb, golden):
+    for name in storm_cases(golden):
+        sets = golden_sets(golden, f"storm/{name}/")
+        s = build_storm(sb, sets)
+        want = int(golden[f"storm/{name}/sum"][0])
+        assert s.pairw_intersect_cardinality() == want, name
+        assert s.pairw_intersect_cardinality(blocked=5) == want, name
+        mat, ssum = s.matrix()
+        assert ssum == want
+        n = len(sets)
+        iu = np.triu_indices(n)
+        strict = iu[0] != iu[1]
+        np.testing.assert_array_equal(mat[strict], golden[f"storm/{name}/matrix"][strict], err_msg=name)
+        diag = mat[~strict]
+        np.testing.assert_array_equal(diag, [len(x) for x in sets], err_msg=name)
+
+
+def test_golden_square(sb, golden):
+    a = build_storm(sb, golden_sets(golden, "square/a_"))
+    b = build_storm(sb, golden_sets(golden, "square/b_"))
+    assert a.square(b) == int(golden["square/sum"][0])
+
+
+@pytest.mark.parametrize("case", ["zipf", "runs", "haplo", "dense", "sweep"])
+def test_config_shaped_sets_match_oracle(sb, case):
+    if case == "zipf":
+        sets = gen.zipf_sets(90, 1 << 24, 1.1, 16, 1 << 17, 5)
+    elif case == "runs":
+        sets = gen.run_sets(70, 1 << 26, 40, 256, 6)
+    elif case == "haplo":
+        sets = gen.haplotype_sets(200, 20000, 32, 7)
+    elif case == "dense":
+        sets = [gen.uniform_set(gen.rng(8 + i), 20000 + 3000 * i, 1 << 17) for i in range(20)]
+    else:
+        sets = []
+        for d in (1e-5, 1e-4, 1e-3, 1e-2):
+            sets += gen.bernoulli_sets(12, 1 << 22, d, int(d * 1e6))
+    s = build_storm(sb, sets)
+    vals, offs = gen.to_csr(sets)
+    want, ws = ol.sets_matrix(vals, offs)
+    mat, ssum = s.matrix()
+    assert ssum == ws
+    np.testing.assert_array_equal(mat, want)
+
+
+def test_empty_rows_clear_and_tiles(sb):
+    sets = [np.zeros(0, np.uint32), np.arange(0, 70000, 3, dtype=np.uint32), np.zeros(0, np.uint32),
+            np.arange(5, 200000, 11, dtype=np.uint32)]
+    s = build_storm(sb, sets)
+    vals, offs = gen.to_csr(sets)
+    want, ws = ol.sets_matrix(vals, offs)
+    assert s.pairw_intersect_cardinality() == ws
+    col = s.tiles(3)
+    iu = np.triu_indices(4)
+    strict = iu[0] != iu[1]
+    np.testing.assert_array_equal(col.out[strict], want[strict])
+    s.clear()
+    assert s.pairw_intersect_cardinality() == 0
+    s.add(np.array([1, 2, 3], np.uint32))
+    s.add(np.array([2, 3, 4], np.uint32))
+    assert s.pairw_intersect_cardinality() == 2
+
+
+def test_lowlevel_kernels_match_reference(sb, golden):
+    for a, b, want in zip(golden_sets(golden, "vec16/a_"), golden_sets(golden, "vec16/b_"), golden["vec16/result"]):
+        assert sb.intersect_vector16(a.astype(np.uint16), b.astype(np.uint16)) == want
+    for a, b, o in zip(golden_sets(golden, "vec32/a_"), golden_sets(golden, "vec32/b_"),
+                       golden_sets(golden, "vec32/out_")):
+        got = sb.intersect_vector32(a, b)
+        np.testing.assert_array_equal(got.ravel(), o)
+    for a, b, want in zip(golden_sets(golden, "bsl/a_"), golden_sets(golden, "bsl/b_"), golden["bsl/result"]):
+        ba = gen.sets_to_rows([a], 4096)[0]
+        bb = gen.sets_to_rows([b], 4096)[0]
+        assert sb.intersect_bitmaps_scalar_list(ba, bb, a, b) == want
+        assert sb.intersect_bitmaps_scalar_list(bb, ba, b, a) == want
+
+
+def test_single_bit_probe_cases(sb):
+    # tests/test_storm.c:125-132 shape: one shared bit in word 1, every bit position.
+    for bit in range(64):
+        bm = np.array([0, 1 << bit], dtype=np.uint64)
+        assert sb.intersect_bitmaps_scalar_list(bm, bm, [64 + bit], [64 + bit]) == 1
+
+
+def test_reference_test_program_against_this_library():
+    """The reference's own tests/test_storm.c, compiled unmodified against the
+    reference header and linked against libstorm_b200.so (oracle/Makefile,
+    target `dropin`), must report 0 failures."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "test_storm_b200")
+    if not os.path.exists(exe):
+        pytest.skip("oracle/_ref/test_storm_b200 not built (needs the reference sources)")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert " 0 failures" in r.stdout, r.stdout[-2000:]
