@@ -209,15 +209,10 @@ def run_reference_arm(args):
         return 0
     import torch
     threads = cpu_threads()
-    device = torch.device("cuda", 0) if torch.cuda.is_available() else None
-    if device is not None:
-        rows = bernoulli_rows_gpu(N_ROWS, M_BITS, P_RANGE, SEED, device).cpu().numpy().view(np.uint64)
-    else:
-        import gen  # noqa  (CPU-only fallback for the input generator only)
-        rows = None
-    if rows is None:
-        print(json.dumps({"impl": "reference", "unavailable": "no CUDA device to generate the workload"}))
+    if not torch.cuda.is_available():
+        print(json.dumps({"impl": "reference", "unavailable": "no CUDA device to generate the seeded workload"}))
         return 0
+    rows = bernoulli_rows_gpu(args.rows, args.bits, P_RANGE, SEED, torch.device("cuda", 0)).cpu().numpy().view(np.uint64)
     per_step_s = max(2.0, 60.0 / max(1, args.steps + args.warmup))
     for _ in range(args.warmup):
         if reference_sample(rows, min(per_step_s, 3.0), threads) is None:
@@ -262,7 +257,8 @@ def run_b200_arm(args):
     rows_d = bernoulli_rows_gpu(n, m, P_RANGE, SEED + rank, device)
     w = rows_d.shape[1]
     c = sb.StormContig(m)
-    c.set_kernel({"auto": sb.KERNEL_AUTO, "popc": sb.KERNEL_POPC, "mma": sb.KERNEL_MMA}[args.kernel])
+    c.set_kernel({"auto": sb.KERNEL_AUTO, "popc": sb.KERNEL_POPC, "mma": sb.KERNEL_MMA,
+                  "mma_ss": sb.KERNEL_MMA_SS}[args.kernel])
     rc = sb.lib().STORM_contig_add_bitmaps(c.h, C.cast(rows_d.data_ptr(), sb.u64p), n, w)
     if rc < 0:
         raise sb.StormError(rc, "STORM_contig_add_bitmaps")
@@ -291,7 +287,8 @@ def run_b200_arm(args):
     elapsed_ms = ev0.elapsed_time(ev1)
     elapsed_ms = max_over_ranks(elapsed_ms, dist, device)
     launches = args.steps * c.last_launches()
-    kernel_used = {sb.KERNEL_POPC: "bb_popc_kernel", sb.KERNEL_MMA: "bb_mma_kernel"}.get(c.last_kernel(), "?")
+    kernel_used = {sb.KERNEL_POPC: "bb_popc_kernel", sb.KERNEL_MMA: "bb_mma_ts_kernel",
+                   sb.KERNEL_MMA_SS: "bb_mma_kernel"}.get(c.last_kernel(), "?")
     ms_per_step = elapsed_ms / args.steps
     value = world * tri / (ms_per_step / 1e3)
 
@@ -302,7 +299,7 @@ def run_b200_arm(args):
     host_out = torch.empty(tri, dtype=torch.int32, pin_memory=True)
     e2e_ms = []
     L = sb.lib()
-    for it in range(1 + args.e2e_steps):
+    for it in range(1 + max(1, args.e2e_steps)):
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
@@ -319,14 +316,24 @@ def run_b200_arm(args):
         dt = (time.perf_counter() - t0) * 1e3
         if it > 0:   # first iteration re-allocates the handle's buffers
             e2e_ms.append(dt)
-    e2e_step_ms = max_over_ranks(statistics.median(e2e_ms), dist, device)
+    e2e_step_ms = max_over_ranks(statistics.median(e2e_ms), dist, device) if e2e_ms else float("nan")
     e2e_value = world * tri / (e2e_step_ms / 1e3)
-    assert int(ssum.value) == s, "device and host runs disagree"
+    if int(ssum.value) != s:
+        raise RuntimeError(f"device-resident sum {s} != host-buffer sum {int(ssum.value)}")
+    # Self-check of the timed output: two whole rows of the triangle against the oracle.
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as ol
+    host_rows = host_in.numpy().view(np.uint64)
+    host_tri = host_out.numpy().view(np.uint32)
+    for i in (0, n // 3):
+        base = int(sb.tri_index(n, i, i))
+        if not np.array_equal(host_tri[base: base + n - i], ol.contig_row(host_rows, i)):
+            raise RuntimeError(f"row {i} of the triangle differs from the oracle")
 
     # ---- roofline of the dominant kernel ----
     peaks, peak_src = measured_peaks()
     k_ms = statistics.median(kernel_ms)
-    if kernel_used == "bb_mma_kernel":
+    if kernel_used in ("bb_mma_kernel", "bb_mma_ts_kernel"):
         ops = 2.0 * tri * m                      # u8 MACs = pairs x row bits, 2 ops each
         achieved = ops / (k_ms / 1e3) / 1e12
         peak = 2.0 * peaks["bf16_tflops"]        # dense int8 rate = 2 x dense bf16 on sm_100
@@ -344,7 +351,7 @@ def run_b200_arm(args):
         "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "ns_per_pair": 1e9 / (value / world),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8 (tcgen05 kind::i8, s32 acc)"
-        if kernel_used == "bb_mma_kernel" else "u64 (AND + POPC)",
+        if kernel_used in ("bb_mma_kernel", "bb_mma_ts_kernel") else "u64 (AND + POPC)",
         "data": "synthetic (seeded Bernoulli rows generated on the GPU)",
         "config": {"workload": "dense all-bitmap XX^T: 65536 rows x 262144 bits, p~U[0.05,0.5], u32 i<=j out",
                    "rows": n, "bits": m, "pairs_per_gpu": tri, "kernel": kernel_used,
@@ -381,7 +388,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma", "mma_ss"])
     ap.add_argument("--rows", type=int, default=N_ROWS)
     ap.add_argument("--bits", type=int, default=M_BITS)
     ap.add_argument("--e2e-steps", type=int, default=2)

@@ -69,11 +69,13 @@ typedef void (*STORM_tile_callback)(uint32_t i0, uint32_t j0, uint32_t nr, uint3
 /* Bitmap x bitmap kernel used by the contiguous all-pairs calls. */
 #define STORM_B200_KERNEL_AUTO  0   /* tensor-core kernel where exact, else POPC   */
 #define STORM_B200_KERNEL_POPC  1   /* CUDA-core AND + POPC tiles                  */
-#define STORM_B200_KERNEL_MMA   2   /* tcgen05 kind::i8 tensor-core tiles          */
+#define STORM_B200_KERNEL_MMA   2   /* tcgen05 kind::i8, A operand in TMEM         */
+#define STORM_B200_KERNEL_MMA_SS 3  /* tcgen05 kind::i8, both operands in smem     */
 
 /* Append n_rows rows given as packed little-endian bitmaps of
  * words_per_row 64-bit words each, in host memory or (unified addressing)
- * device memory (bit b of row r = word b/64, bit b%64).
+ * device memory (bit b of row r = word b/64, bit b%64).  Device input is
+ * read after all work queued on the device so far has finished.
  * words_per_row must equal ceil(vector_length/64).  Bits at or above
  * vector_length must be zero (STORM_B200_EARG otherwise).  Equivalent to one
  * STORM_contig_add per row with that row's set positions, except that empty
@@ -90,7 +92,8 @@ int STORM_contig_upload(STORM_contiguous_t* c);
 int STORM_contig_pairw_intersect_matrix(STORM_contiguous_t* c, uint32_t* out,
                                         uint64_t out_len, uint64_t* sum);
 /* Same, into a DEVICE buffer on the current device (d_out may be NULL to
- * compute only the sum).  Rows must already be resident (upload). */
+ * compute only the sum).  Work already queued on other streams is waited for
+ * before d_out is written. */
 int STORM_contig_pairw_intersect_matrix_device(STORM_contiguous_t* c, uint32_t* d_out,
                                                uint64_t out_len, uint64_t* sum);
 int STORM_contig_pairw_intersect_tiles(STORM_contiguous_t* c, uint32_t tile,
@@ -101,7 +104,7 @@ void* STORM_contig_stream(STORM_contiguous_t* c);
  * handle's stream) and how many kernels it launched. */
 float STORM_contig_last_kernel_ms(const STORM_contiguous_t* c);
 uint32_t STORM_contig_last_launches(const STORM_contiguous_t* c);
-/* Which kernel the last call ran (STORM_B200_KERNEL_POPC or _MMA). */
+/* Which kernel the last call ran (STORM_B200_KERNEL_POPC, _MMA or _MMA_SS). */
 int STORM_contig_last_kernel(const STORM_contiguous_t* c);
 
 /* ---- STORM_t extensions ----------------------------------------------- */

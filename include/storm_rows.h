@@ -1,0 +1,146 @@
+/*
+ * storm_rows.h -- the reference's kernel layer (kernels/storm_allpairs.h,
+ * storm_cost.h, storm_repr.h) behind a C ABI, on the GPU.
+ *
+ * A STORM_rows_t holds rows of one universe, each given as sorted distinct
+ * positions (storm::build_row's contract, storm_repr.h:280-291).  Every row is
+ * kept in HBM in the reference's representations -- sorted list (S), maximal
+ * runs (R), EWAH-64 (W), and where memory allows bitmap (B, with the rank9
+ * index and the zone map under the reference's own gates, storm_repr.cpp:186-
+ * 189) and complement (C, density > 1/2).  The all-pairs calls traverse the
+ * upper triangle in tiles exactly like storm::allpairs_sum / allpairs_tiles
+ * (storm_allpairs.cpp:486-732): optional density order, a cell chosen per
+ * pair or per tile by a policy, the O(1) span test per pair, and a cell
+ * kernel per pair.  Counts do not depend on the policy; only the time does.
+ *
+ * Extra policies beyond the reference's:
+ *   STORM_POLICY_LEARNED   a small MLP over tile features picks the cell; it
+ *                          is trained on this GPU's own cell timings
+ *                          (STORM_rows_train_selector) and falls back to the
+ *                          cost model when untrained.
+ * Execution forms:
+ *   STORM_EXEC_PER_TILE    one kernel launch per tile (the plain GPU form)
+ *   STORM_EXEC_BATCHED     every tile in one persistent work-queue launch,
+ *                          captured in a CUDA graph and replayed
+ */
+#ifndef STORM_B200_ROWS_H_
+#define STORM_B200_ROWS_H_
+
+#include <stdint.h>
+#include <stddef.h>
+#include "storm_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct STORM_rows_s STORM_rows_t;
+
+/* storm::Policy (storm_allpairs.h:42-123), plus LEARNED. */
+#define STORM_POLICY_ALLBITMAP 0
+#define STORM_POLICY_PERPAIR   1
+#define STORM_POLICY_PERTILE   2
+#define STORM_POLICY_ORACLE    3
+#define STORM_POLICY_FIXED     4
+#define STORM_POLICY_PROBE     5
+#define STORM_POLICY_REFINE    6
+#define STORM_POLICY_LEARNED   7
+
+/* storm::Pairing (storm_cost.h:47-49). */
+#define STORM_PAIRING_BB 0
+#define STORM_PAIRING_BS 1
+#define STORM_PAIRING_BR 2
+#define STORM_PAIRING_BW 3
+#define STORM_PAIRING_SS 4
+#define STORM_PAIRING_SR 5
+#define STORM_PAIRING_SW 6
+#define STORM_PAIRING_RR 7
+#define STORM_PAIRING_RW 8
+#define STORM_PAIRING_WW 9
+#define STORM_PAIRING_EMPTY 10
+#define STORM_PAIRING_COUNT 11
+/* Complemented pairing (kernels/cell_comp.cpp): |A & B| = |B| - |A' & B|. */
+#define STORM_PAIRING_CB 11
+
+#define STORM_EXEC_PER_TILE 0
+#define STORM_EXEC_BATCHED  1
+
+/* storm::AllPairsStats (storm_allpairs.h:127-144). ns_* are device times. */
+typedef struct {
+    uint64_t sum;
+    uint64_t pairs;
+    uint64_t decisions;
+    uint64_t skipped;
+    double   ns_total;
+    double   ns_selection;
+    uint64_t cell_pairs[STORM_PAIRING_COUNT + 1];
+    uint32_t launches;
+} STORM_allpairs_stats;
+
+STORM_rows_t* STORM_rows_new(uint32_t universe);
+void STORM_rows_free(STORM_rows_t* r);
+/* Append one row: sorted, distinct positions < universe (-3 otherwise). */
+int STORM_rows_add(STORM_rows_t* r, const uint32_t* positions, uint32_t n);
+int STORM_rows_clear(STORM_rows_t* r);
+uint64_t STORM_rows_size(const STORM_rows_t* r);
+/* HBM budget for the bitmap form (bytes, 0 = automatic: a quarter of free
+ * memory).  Rows that do not get a bitmap behave like the reference's
+ * sparse_only rows (storm_repr.h:280-291): no B, no rank, no zone map. */
+int STORM_rows_set_bitmap_budget(STORM_rows_t* r, uint64_t bytes);
+int STORM_rows_upload(STORM_rows_t* r);
+/* RowMeta of one row (storm_repr.h:213-231) as 8 words: cardinality,
+ * n_runs, n_words, n_nonzero_w, first_set, last_set, has_rank, has_occ;
+ * plus a 9th word of representation flags (bit 0 bitmap, 1 complement). */
+int STORM_rows_meta(STORM_rows_t* r, uint64_t row, uint32_t* meta9);
+
+/* storm::allpairs_sum: sum over i < j (plus stats). fixed_cell is used by
+ * STORM_POLICY_FIXED.  tile 0 means 64 (storm_allpairs.h:152-201). */
+int STORM_rows_allpairs_sum(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell, int exec,
+                            STORM_allpairs_stats* st);
+/* Per-pair counts, packed upper triangle in ORIGINAL row order. */
+int STORM_rows_allpairs_matrix(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell, int exec,
+                               uint32_t* out, uint64_t out_len, STORM_allpairs_stats* st);
+/* storm::allpairs_tiles: tile visitor over ORIGINAL row indices (the
+ * reference hands out density-sorted positions and drops the permutation,
+ * storm_allpairs.cpp:689,725; this call keeps original order). */
+int STORM_rows_allpairs_tiles(STORM_rows_t* r, int policy, uint32_t tile, int exec,
+                              STORM_tile_callback cb, void* ctx, STORM_allpairs_stats* st);
+
+/* storm::select_pairing / storm::predict with the reference's default model
+ * (storm_cost.cpp:372-496), on two 8-word RowMeta records. */
+int STORM_select_pairing(const uint32_t* meta_a, const uint32_t* meta_b, double* predicted);
+double STORM_predict(int pairing, const uint32_t* meta_a, const uint32_t* meta_b);
+
+/* One cell on one pair of rows (both orders are valid); for tests and the
+ * per-cell timing the selector is trained on.  Returns the count, or a
+ * negative status when a representation the cell needs is absent. */
+int64_t STORM_rows_cell(STORM_rows_t* r, int pairing, uint64_t row_a, uint64_t row_b);
+
+/* ---- learned selector ---------------------------------------------------
+ * Features per tile pair (row tiles of the density-sorted order) -> scores
+ * per cell; argmax is the cell.  STORM_rows_train_selector times every
+ * applicable cell on sampled tiles of `r` on the GPU (the labels), trains the
+ * MLP with the device forward/backward kernels, and installs it in `r`.
+ * Returns 0; stats[0..5] = samples, epochs, final loss, train accuracy,
+ * regret of the MLP on held-out tiles, regret of the cost model there. */
+int STORM_rows_train_selector(STORM_rows_t* r, uint32_t tile, uint32_t samples, uint32_t epochs,
+                              uint64_t seed, double* stats);
+/* Reset to the untrained (cost-model fallback) selector. */
+int STORM_rows_reset_selector(STORM_rows_t* r);
+/* Parameters out/in (so a trained selector can be saved and loaded):
+ * n_params floats.  Returns the parameter count when params is NULL. */
+int64_t STORM_rows_selector_params(STORM_rows_t* r, float* params, uint64_t n_params, int load);
+
+/* MLP kernels exposed for gradient checks against the CPU oracle:
+ * a 2-layer MLP  logits = W2 relu(W1 x + b1) + b2 over a batch, softmax
+ * cross-entropy against integer labels; grads in the same layout as params
+ * (W1 [H x F], b1 [H], W2 [C x H], b2 [C]).  Device run, host buffers. */
+int STORM_mlp_forward_backward(const float* params, uint32_t F, uint32_t H, uint32_t Cn,
+                               const float* x, const int32_t* labels, uint32_t batch,
+                               float* logits, float* loss, float* grads);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* STORM_B200_ROWS_H_ */

@@ -36,7 +36,7 @@ u32p = C.POINTER(C.c_uint32)
 u64p = C.POINTER(C.c_uint64)
 TILE_CB = C.CFUNCTYPE(None, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, u32p, C.c_void_p)
 
-KERNEL_AUTO, KERNEL_POPC, KERNEL_MMA = 0, 1, 2
+KERNEL_AUTO, KERNEL_POPC, KERNEL_MMA, KERNEL_MMA_SS = 0, 1, 2, 3
 OK, ENULL, EVALUES, EARG, ENOMEM, ECUDA, ETIMEOUT, ESIZE, ELIMIT = 0, -1, -2, -3, -4, -5, -6, -7, -8
 
 
@@ -350,3 +350,161 @@ class Storm:
 
     def last_kernel_ms(self) -> float:
         return float(_lib.STORM_last_kernel_ms(self.h))
+
+
+# --- kernel layer (include/storm_rows.h) ---------------------------------
+POLICY_ALLBITMAP, POLICY_PERPAIR, POLICY_PERTILE, POLICY_ORACLE, POLICY_FIXED, POLICY_PROBE, POLICY_REFINE, \
+    POLICY_LEARNED = range(8)
+POLICY_NAMES = ["all-bitmap", "per-pair", "per-tile", "oracle", "fixed-cell", "probe", "refine", "learned"]
+PAIRINGS = ["BB", "BS", "BR", "BW", "SS", "SR", "SW", "RR", "RW", "WW", "EMPTY", "CB"]
+(P_BB, P_BS, P_BR, P_BW, P_SS, P_SR, P_SW, P_RR, P_RW, P_WW, P_EMPTY, P_CB) = range(12)
+EXEC_PER_TILE, EXEC_BATCHED = 0, 1
+
+
+class AllPairsStats(C.Structure):
+    _fields_ = [("sum", C.c_uint64), ("pairs", C.c_uint64), ("decisions", C.c_uint64), ("skipped", C.c_uint64),
+                ("ns_total", C.c_double), ("ns_selection", C.c_double), ("cell_pairs", C.c_uint64 * 12),
+                ("launches", C.c_uint32)]
+
+    def as_dict(self):
+        return {"sum": self.sum, "pairs": self.pairs, "decisions": self.decisions, "skipped": self.skipped,
+                "ns_total": self.ns_total, "ns_selection": self.ns_selection,
+                "cell_pairs": {PAIRINGS[k]: int(self.cell_pairs[k]) for k in range(12) if self.cell_pairs[k]},
+                "launches": self.launches}
+
+
+_sig("STORM_rows_new", C.c_void_p, [C.c_uint32])
+_sig("STORM_rows_free", None, [C.c_void_p])
+_sig("STORM_rows_add", C.c_int, [C.c_void_p, u32p, C.c_uint32])
+_sig("STORM_rows_clear", C.c_int, [C.c_void_p])
+_sig("STORM_rows_size", C.c_uint64, [C.c_void_p])
+_sig("STORM_rows_set_bitmap_budget", C.c_int, [C.c_void_p, C.c_uint64])
+_sig("STORM_rows_upload", C.c_int, [C.c_void_p])
+_sig("STORM_rows_meta", C.c_int, [C.c_void_p, C.c_uint64, u32p])
+_sig("STORM_rows_allpairs_sum", C.c_int, [C.c_void_p, C.c_int, C.c_uint32, C.c_int, C.c_int, C.POINTER(AllPairsStats)])
+_sig("STORM_rows_allpairs_matrix", C.c_int, [C.c_void_p, C.c_int, C.c_uint32, C.c_int, C.c_int, u32p, C.c_uint64,
+                                             C.POINTER(AllPairsStats)])
+_sig("STORM_rows_allpairs_tiles", C.c_int, [C.c_void_p, C.c_int, C.c_uint32, C.c_int, TILE_CB, C.c_void_p,
+                                            C.POINTER(AllPairsStats)])
+_sig("STORM_select_pairing", C.c_int, [u32p, u32p, C.POINTER(C.c_double)])
+_sig("STORM_predict", C.c_double, [C.c_int, u32p, u32p])
+_sig("STORM_rows_cell", C.c_int64, [C.c_void_p, C.c_int, C.c_uint64, C.c_uint64])
+_sig("STORM_rows_train_selector", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
+                                            C.POINTER(C.c_double)])
+_sig("STORM_rows_reset_selector", C.c_int, [C.c_void_p])
+_sig("STORM_rows_selector_params", C.c_int64, [C.c_void_p, C.POINTER(C.c_float), C.c_uint64, C.c_int])
+_sig("STORM_mlp_forward_backward", C.c_int, [C.POINTER(C.c_float), C.c_uint32, C.c_uint32, C.c_uint32,
+                                             C.POINTER(C.c_float), C.POINTER(C.c_int32), C.c_uint32,
+                                             C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)])
+
+
+def select_pairing(meta_a, meta_b):
+    a = np.ascontiguousarray(meta_a[:8], dtype=np.uint32)
+    b = np.ascontiguousarray(meta_b[:8], dtype=np.uint32)
+    pred = C.c_double(0)
+    return int(_lib.STORM_select_pairing(_p(a, u32p), _p(b, u32p), C.byref(pred))), float(pred.value)
+
+
+def predict(pairing, meta_a, meta_b):
+    a = np.ascontiguousarray(meta_a[:8], dtype=np.uint32)
+    b = np.ascontiguousarray(meta_b[:8], dtype=np.uint32)
+    return float(_lib.STORM_predict(pairing, _p(a, u32p), _p(b, u32p)))
+
+
+def mlp_forward_backward(params, F, H, Cn, x, labels):
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    labels = np.ascontiguousarray(labels, dtype=np.int32)
+    B = labels.size
+    logits = np.zeros((B, Cn), np.float32)
+    loss = C.c_float(0)
+    grads = np.zeros_like(params)
+    fp = C.POINTER(C.c_float)
+    _check(_lib.STORM_mlp_forward_backward(params.ctypes.data_as(fp), F, H, Cn, x.ctypes.data_as(fp),
+                                           labels.ctypes.data_as(C.POINTER(C.c_int32)), B,
+                                           logits.ctypes.data_as(fp), C.byref(loss), grads.ctypes.data_as(fp)),
+           "STORM_mlp_forward_backward")
+    return logits, float(loss.value), grads
+
+
+class StormRows:
+    """STORM_rows_t: the reference's kernel layer (kernels/storm_allpairs.h) on the GPU."""
+
+    def __init__(self, universe: int):
+        self.h = _lib.STORM_rows_new(universe)
+        if not self.h:
+            raise StormError(ENOMEM, "STORM_rows_new")
+        self.universe = universe
+
+    def close(self):
+        if self.h:
+            _lib.STORM_rows_free(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def add(self, positions) -> int:
+        v = _u32(positions)
+        return _check(_lib.STORM_rows_add(self.h, _p(v, u32p), len(v)), "STORM_rows_add")
+
+    def clear(self):
+        return _lib.STORM_rows_clear(self.h)
+
+    def __len__(self):
+        return int(_lib.STORM_rows_size(self.h))
+
+    def set_bitmap_budget(self, nbytes: int):
+        _check(_lib.STORM_rows_set_bitmap_budget(self.h, nbytes), "STORM_rows_set_bitmap_budget")
+
+    def upload(self):
+        _check(_lib.STORM_rows_upload(self.h), "STORM_rows_upload")
+
+    def meta(self, row: int) -> np.ndarray:
+        m = np.zeros(9, dtype=np.uint32)
+        _check(_lib.STORM_rows_meta(self.h, row, _p(m, u32p)), "STORM_rows_meta")
+        return m
+
+    def allpairs_sum(self, policy, tile=64, fixed_cell=P_BS, exec_=EXEC_BATCHED):
+        st = AllPairsStats()
+        _check(_lib.STORM_rows_allpairs_sum(self.h, policy, tile, fixed_cell, exec_, C.byref(st)),
+               "STORM_rows_allpairs_sum")
+        return int(st.sum), st.as_dict()
+
+    def allpairs_matrix(self, policy, tile=64, fixed_cell=P_BS, exec_=EXEC_BATCHED):
+        n = len(self)
+        out = np.zeros(max(1, tri_size(n)), dtype=np.uint32)
+        st = AllPairsStats()
+        _check(_lib.STORM_rows_allpairs_matrix(self.h, policy, tile, fixed_cell, exec_, _p(out, u32p), out.size,
+                                               C.byref(st)), "STORM_rows_allpairs_matrix")
+        return out[: tri_size(n)], st.as_dict()
+
+    def allpairs_tiles(self, policy, tile=64, exec_=EXEC_BATCHED):
+        col = _TileCollector(len(self), tile)
+        cb = TILE_CB(col)
+        st = AllPairsStats()
+        _check(_lib.STORM_rows_allpairs_tiles(self.h, policy, tile, exec_, cb, None, C.byref(st)),
+               "STORM_rows_allpairs_tiles")
+        return col, st.as_dict()
+
+    def cell(self, pairing, a, b) -> int:
+        return int(_lib.STORM_rows_cell(self.h, pairing, a, b))
+
+    def train_selector(self, tile=64, samples=0, epochs=400, seed=1):
+        stats = (C.c_double * 6)()
+        _check(_lib.STORM_rows_train_selector(self.h, tile, samples, epochs, seed, stats), "STORM_rows_train_selector")
+        keys = ["samples", "epochs", "loss", "train_accuracy", "regret_mlp", "regret_cost_model"]
+        return dict(zip(keys, list(stats)))
+
+    def reset_selector(self):
+        _check(_lib.STORM_rows_reset_selector(self.h), "STORM_rows_reset_selector")
+
+    def selector_params(self, load: np.ndarray | None = None):
+        n = int(_lib.STORM_rows_selector_params(self.h, None, 0, 0))
+        fp = C.POINTER(C.c_float)
+        if load is not None:
+            p = np.ascontiguousarray(load, dtype=np.float32)
+            _check(_lib.STORM_rows_selector_params(self.h, p.ctypes.data_as(fp), p.size, 1), "selector_params")
+            return p
+        p = np.zeros(n, dtype=np.float32)
+        _check(_lib.STORM_rows_selector_params(self.h, p.ctypes.data_as(fp), n, 0), "selector_params")
+        return p

@@ -1,0 +1,233 @@
+// bb_mma_ts.cuh -- B x B on tcgen05 with the A operand in tensor memory.
+//
+// Same arithmetic as bb_mma.cuh (u8 x u8 -> s32, A bytes weighted 2^(k mod 8),
+// B bytes 2^(7 - k mod 8), D = 128 |Xi & Xj|), different data movement: the
+// 128 rows of the A panel are expanded by their own threads straight into
+// TMEM with tcgen05.st (lane = row, four K bytes per 32-bit column), so only
+// the 256 B rows pass through shared memory.  Measured on the SS form, the
+// shared-memory pipe (expansion stores + the tensor core's operand reads)
+// was the bottleneck; this removes a third of that traffic.
+//
+// Warp roles (416 threads): warps 0-3 expand A rows into TMEM, warps 4-11
+// expand B rows into the swizzled smem ring, warp 12 owns TMEM and issues
+// the MMAs; warps 0-7 drain the accumulator in the epilogue.  Stages are 256
+// row bits: 64 TMEM columns of A + 64 KB of B, three in flight.  TMEM: 512
+// columns = accumulator [0, 256) + A stages [256, 448).
+#pragma once
+#include "bb_mma.cuh"
+
+namespace sb200 {
+
+constexpr int TS_BM = 128;
+constexpr int TS_BN = 256;
+constexpr int TS_KBITS = 256;                              // row bits per stage
+constexpr int TS_STAGES = 3;
+constexpr int TS_A_THREADS = 128;
+constexpr int TS_B_THREADS = 256;
+constexpr int TS_PRODUCERS = TS_A_THREADS + TS_B_THREADS;
+constexpr int TS_THREADS = TS_PRODUCERS + 32;
+constexpr int TS_MMA_WARP = TS_PRODUCERS / 32;             // 12
+constexpr uint32_t TS_B_ATOM_BYTES = TS_BN * 128;          // one 128-byte K atom of B
+constexpr uint32_t TS_B_STAGE_BYTES = TS_B_ATOM_BYTES * (TS_KBITS / 128);
+constexpr uint32_t TS_TMEM_COLS = 512;
+constexpr uint32_t TS_A_COL0 = 256;
+constexpr uint32_t TS_SMEM_BYTES = TS_STAGES * TS_B_STAGE_BYTES + 1024 + 256;
+
+struct TsCtl {
+    uint64_t full[TS_STAGES];
+    uint64_t empty[TS_STAGES];
+    uint64_t acc_full, acc_empty, drain;
+    uint32_t tmem_base;
+    volatile uint32_t abort;
+};
+
+__device__ __forceinline__ bool ts_wait(uint32_t bar, uint32_t parity, TsCtl* ctl, DeviceFlags* flags,
+                                        uint32_t site, bool drain = false) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer_ns();
+    for (;;) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (!drain && ctl->abort) return false;
+        if (globaltimer_ns() - t0 > WAIT_LIMIT_NS) {
+            atomicCAS(&flags->error, 0u, site);
+            ctl->abort = 1;
+            return false;
+        }
+    }
+}
+
+// 64 packed bits -> 16 u32 of A-weighted bytes (byte k carries bit k at 2^(k mod 8)).
+__device__ __forceinline__ void expand_a64(uint64_t v, uint32_t* o) {
+    const uint32_t lo = (uint32_t)v, hi = (uint32_t)(v >> 32);
+#pragma unroll
+    for (uint32_t b = 0; b < 8; ++b) {
+        const uint32_t r = __byte_perm(b < 4 ? lo : hi, 0, (b & 3) * 0x1111u);
+        o[2 * b] = r & 0x08040201u;
+        o[2 * b + 1] = r & 0x80402010u;
+    }
+}
+
+__global__ void __launch_bounds__(TS_THREADS, 1)
+bb_mma_ts_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, const uint2* __restrict__ tiles,
+                 uint32_t n_tiles, uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags) {
+    extern __shared__ __align__(1024) unsigned char ts_smem[];
+    const uint32_t raw_addr = smem_u32(ts_smem);
+    const uint32_t pad = ((raw_addr + 1023u) & ~1023u) - raw_addr;
+    uint8_t* ring = ts_smem + pad;
+    const uint32_t ring_addr = raw_addr + pad;
+    TsCtl* ctl = reinterpret_cast<TsCtl*>(ring + TS_STAGES * TS_B_STAGE_BYTES);
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const uint32_t nk = w_pad / (TS_KBITS / 64);               // stages per tile (w_pad % 8 == 0)
+
+    if (tid == 0) {
+        for (int s = 0; s < TS_STAGES; ++s) {
+            mbar_init(smem_u32(&ctl->full[s]), TS_PRODUCERS);
+            mbar_init(smem_u32(&ctl->empty[s]), 1);
+        }
+        mbar_init(smem_u32(&ctl->acc_full), 1);
+        mbar_init(smem_u32(&ctl->acc_empty), 256);
+        mbar_init(smem_u32(&ctl->drain), 1);
+        ctl->abort = 0;
+        fence_barrier_init();
+    }
+    if (warp == TS_MMA_WARP) {
+        tmem_alloc(smem_u32(&ctl->tmem_base), TS_TMEM_COLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = ctl->tmem_base;
+
+    if (warp < TS_MMA_WARP) {
+        const bool is_a = tid < TS_A_THREADS;
+        const uint32_t prow = is_a ? (uint32_t)tid : (uint32_t)(tid - TS_A_THREADS);   // operand row
+        uint32_t g = 0, tcount = 0;
+        bool ok = true;
+        for (uint32_t t = blockIdx.x; t < n_tiles && ok; t += gridDim.x, ++tcount) {
+            const uint64_t i0 = (uint64_t)tiles[t].x * TS_BM;
+            const uint64_t j0 = (uint64_t)tiles[t].y * TS_BN;
+            const uint64_t* src = X + (is_a ? i0 + prow : j0 + prow) * (uint64_t)w_pad;
+            uint4 v0 = __ldg(reinterpret_cast<const uint4*>(src));
+            uint4 v1 = __ldg(reinterpret_cast<const uint4*>(src) + 1);
+            for (uint32_t kb = 0; kb < nk; ++kb, ++g) {
+                const uint32_t s = g % TS_STAGES;
+                const uint32_t round = g / TS_STAGES;
+                uint4 n0 = make_uint4(0, 0, 0, 0), n1 = n0;
+                if (kb + 1 < nk) {
+                    n0 = __ldg(reinterpret_cast<const uint4*>(src + 4 * (kb + 1)));
+                    n1 = __ldg(reinterpret_cast<const uint4*>(src + 4 * (kb + 1)) + 1);
+                }
+                if (!ts_wait(smem_u32(&ctl->empty[s]), (round & 1) ^ 1, ctl, flags, ERR_PROD_EMPTY)) {
+                    ok = false;
+                    break;
+                }
+                const uint64_t w[4] = {((uint64_t)v0.y << 32) | v0.x, ((uint64_t)v0.w << 32) | v0.z,
+                                       ((uint64_t)v1.y << 32) | v1.x, ((uint64_t)v1.w << 32) | v1.z};
+                if (is_a) {
+                    // lanes 32*(warp%4).. ; columns A_COL0 + 64 s + [0, 64)
+                    const uint32_t taddr = tmem_base + ((uint32_t)(warp & 3) * 32u << 16) + TS_A_COL0 + 64u * s;
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        uint32_t r[32];
+                        expand_a64(w[2 * h], r);
+                        expand_a64(w[2 * h + 1], r + 16);
+                        tmem_st_32x32b_x32(taddr + 32u * h, r);
+                    }
+                    tmem_st_wait();
+                    tc_fence_before();
+                } else {
+                    uint8_t* b_stage = ring + s * TS_B_STAGE_BYTES;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        // word q covers K bytes [64q, 64q + 64): atom q/2, chunks 4(q%2)..
+                        expand_store<true>(b_stage + (q >> 1) * TS_B_ATOM_BYTES, prow, (uint32_t)(q & 1), w[q]);
+                    }
+                    fence_proxy_async_smem();
+                }
+                mbar_arrive(smem_u32(&ctl->full[s]));
+                v0 = n0;
+                v1 = n1;
+            }
+            if (!ok) break;
+            if (warp >= 8) continue;   // warps 8-11 do not take part in the epilogue
+            if (!ts_wait(smem_u32(&ctl->acc_full), tcount & 1, ctl, flags, ERR_PROD_ACCFULL)) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t lane_grp = (uint32_t)(warp & 3) * 32u;
+            const uint32_t col0 = (uint32_t)(warp >> 2) * 128u;
+            const uint64_t i = i0 + lane_grp + lane;
+            const bool row_ok = i < n;
+            const uint64_t base = row_ok ? tri_index(n, i, i) - i : 0;
+            unsigned long long local = 0;
+#pragma unroll 1
+            for (uint32_t c = 0; c < 4; ++c) {
+                uint32_t r[32];
+                tmem_ld_32x32b_x32(tmem_base + (lane_grp << 16) + col0 + 32u * c, r);
+                tmem_ld_wait();
+                if (row_ok) {
+                    const uint64_t jb = j0 + col0 + 32u * c;
+#pragma unroll
+                    for (int e = 0; e < 32; ++e) {
+                        const uint64_t j = jb + e;
+                        const uint32_t cnt = r[e] >> 7;
+                        if (j >= i && j < n) {
+                            if (out) out[base + j] = cnt;
+                            if (j > i) local += cnt;
+                        }
+                    }
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(smem_u32(&ctl->acc_empty));
+            local = warp_sum_u64(local);
+            if (lane == 0 && local) atomicAdd(&flags->sum, local);
+        }
+    } else if (lane == 0) {
+        const uint32_t idesc = umma_idesc_u8_s32(TS_BM, TS_BN);
+        uint32_t g = 0, tcount = 0;
+        bool issued = false;
+        for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x, ++tcount) {
+            if (!ts_wait(smem_u32(&ctl->acc_empty), (tcount & 1) ^ 1, ctl, flags, ERR_MMA_ACCEMPTY)) break;
+            tc_fence_after();
+            bool ok = true;
+            for (uint32_t kb = 0; kb < nk; ++kb, ++g) {
+                const uint32_t s = g % TS_STAGES;
+                if (!ts_wait(smem_u32(&ctl->full[s]), (g / TS_STAGES) & 1, ctl, flags, ERR_MMA_FULL)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t b_addr = ring_addr + s * TS_B_STAGE_BYTES;
+                const uint32_t a_col = tmem_base + TS_A_COL0 + 64u * s;
+#pragma unroll
+                for (uint32_t kk = 0; kk < TS_KBITS / 32; ++kk) {
+                    const uint32_t boff = (kk >> 2) * TS_B_ATOM_BYTES + (kk & 3) * 32u;
+                    mma_u8_ts(tmem_base, a_col + 8u * kk, umma_desc_sw128(b_addr + boff, 1024), idesc,
+                              (kb | kk) != 0);
+                }
+                issued = true;
+                tc_commit(smem_u32(&ctl->empty[s]));
+            }
+            if (!ok) break;
+            tc_commit(smem_u32(&ctl->acc_full));
+        }
+        if (issued) {
+            tc_commit(smem_u32(&ctl->drain));
+            ts_wait(smem_u32(&ctl->drain), 0, ctl, flags, ERR_MMA_DRAIN, true);
+        }
+    }
+    if (warp == TS_MMA_WARP) __syncwarp();
+    tc_fence_before();
+    __syncthreads();
+    if (warp == TS_MMA_WARP) {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, TS_TMEM_COLS);
+    }
+}
+
+}  // namespace sb200

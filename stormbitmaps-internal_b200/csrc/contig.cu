@@ -177,6 +177,9 @@ int STORM_contig_add_bitmaps(STORM_contiguous_t* c, const uint64_t* words, uint3
         const bool on_device = cudaPointerGetAttributes(&pa, words) == cudaSuccess &&
                                (pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged);
         cudaGetLastError();
+        // Device input may still be in flight on another stream (the handle's
+        // stream does not order against the legacy default stream): wait.
+        if (on_device) SB_CUDA(cudaDeviceSynchronize());
         if (c->vector_length % 64 && n_rows && !on_device) {
             const uint64_t tail_mask = ~0ull << (c->vector_length % 64);
             for (uint64_t r = 0; r < n_rows; ++r)
@@ -217,7 +220,7 @@ int STORM_contig_clear(STORM_contiguous_t* bitmap) {
 
 int STORM_contig_set_kernel(STORM_contiguous_t* c, int kernel) {
     if (c == NULL) return STORM_B200_ENULL;
-    if (kernel < STORM_B200_KERNEL_AUTO || kernel > STORM_B200_KERNEL_MMA) return STORM_B200_EARG;
+    if (kernel < STORM_B200_KERNEL_AUTO || kernel > STORM_B200_KERNEL_MMA_SS) return STORM_B200_EARG;
     c->kernel_pref = kernel;
     return 0;
 }
@@ -273,6 +276,8 @@ int STORM_contig_pairw_intersect_matrix_device(STORM_contiguous_t* c, uint32_t* 
     if (c == NULL) return STORM_B200_ENULL;
     return guard([&]() -> int {
         if (d_out && out_len < tri_size(c->n_rows)) return STORM_B200_ESIZE;
+        // The caller's buffer may still be in use by work on other streams.
+        if (d_out) SB_CUDA(cudaDeviceSynchronize());
         const uint64_t s = contig_run(c, d_out);
         if (sum) *sum = s;
         return 0;

@@ -2,12 +2,13 @@
 #include "dense.cuh"
 #include "bb_popc.cuh"
 #include "bb_mma.cuh"
+#include "bb_mma_ts.cuh"
 
 namespace sb200 {
 
 static void build_tiles(std::vector<uint2>& t, uint64_t n, int kind) {
     t.clear();
-    if (kind == STORM_B200_KERNEL_MMA) {
+    if (kind == STORM_B200_KERNEL_MMA || kind == STORM_B200_KERNEL_MMA_SS) {
         const uint64_t nbi = (n + MMA_BM - 1) / MMA_BM, nbj = (n + MMA_BN - 1) / MMA_BN;
         // Tile (bi, bj) holds a pair with i <= j iff 128 bi <= 256 bj + 255,
         // i.e. bj >= floor(bi / 2).
@@ -31,7 +32,7 @@ uint64_t DenseEngine::run(const uint64_t* dX, uint64_t n, uint32_t w_pad, uint64
     if (n > 0xFFFFFFFFull) fail(STORM_B200_ELIMIT, "more than 2^32 rows");
     int kind = kernel_pref;
     if (kind == STORM_B200_KERNEL_AUTO) kind = row_bits <= MMA_MAX_BITS ? STORM_B200_KERNEL_MMA : STORM_B200_KERNEL_POPC;
-    if (kind == STORM_B200_KERNEL_MMA && row_bits > MMA_MAX_BITS)
+    if ((kind == STORM_B200_KERNEL_MMA || kind == STORM_B200_KERNEL_MMA_SS) && row_bits > MMA_MAX_BITS)
         fail(STORM_B200_ELIMIT, "tensor-core kernel is exact only for rows of at most 2^23 bits");
 
     if (tiles_n != n || tiles_kind != kind) {
@@ -49,6 +50,16 @@ uint64_t DenseEngine::run(const uint64_t* dX, uint64_t n, uint32_t w_pad, uint64
 
     SB_CUDA(cudaEventRecord(log.ev0, st));
     if (kind == STORM_B200_KERNEL_MMA) {
+        static bool attr_set = false;
+        if (!attr_set) {
+            SB_CUDA(cudaFuncSetAttribute(bb_mma_ts_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)TS_SMEM_BYTES));
+            attr_set = true;
+        }
+        const uint32_t grid = n_tiles < (uint32_t)sms ? n_tiles : (uint32_t)sms;
+        bb_mma_ts_kernel<<<grid, TS_THREADS, TS_SMEM_BYTES, st>>>(dX, (uint32_t)n, w_pad, d_tiles.p, n_tiles,
+                                                                   d_out, d_flags.p);
+    } else if (kind == STORM_B200_KERNEL_MMA_SS) {
         static bool attr_set = false;
         if (!attr_set) {
             SB_CUDA(cudaFuncSetAttribute(bb_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

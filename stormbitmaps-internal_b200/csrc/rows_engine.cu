@@ -1,0 +1,933 @@
+// rows_engine.cu -- STORM_rows_t: the reference's batched all-pairs driver
+// (kernels/storm_allpairs.cpp) on the GPU.
+//
+// One all-pairs call = three device phases on the handle's stream:
+//   1. block_meta_kernel   per row block of the traversal order: the tile
+//                          aggregate RowMeta (tile_meta, storm_allpairs.cpp:281-312)
+//   2. select_tiles_kernel per tile pair: the policy's cell (cost model, MLP,
+//                          or top-2 for Probe/Refine), and for Probe a timed
+//                          race of the top two on up to 3 pairs of the tile
+//                          (probe_tile, storm_allpairs.cpp:445-482)
+//   3. tiles_kernel        the pairs: span test, per-pair choice where the
+//                          policy asks for it, the cell, the count written to
+//                          the packed triangle in ORIGINAL row order.
+// Execution forms: BATCHED = phase 3 as one persistent launch pulling
+// (tile, slice) items from a device work queue, the whole call captured once
+// in a CUDA graph and replayed; PER_TILE = phase 3 launched once per tile.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "../../include/storm_rows.h"
+#include "mlp.cuh"
+#include "rows_cells.cuh"
+
+namespace sb200 {
+
+constexpr int TK_WARPS = 4;
+constexpr int TK_THREADS = TK_WARPS * 32;
+
+struct TileDecision {
+    int cell, cell2;      // chosen cell; runner-up (Refine) or same
+};
+
+struct RowsStatsDev {
+    unsigned long long sum, skipped, pairs;
+    unsigned long long cell_pairs[STORM_PAIRING_COUNT + 1];
+    unsigned int queue_head;
+    unsigned int error;
+};
+
+// ---------------------------------------------------------------- phase 1
+__global__ void block_meta_kernel(RowsView v, const uint32_t* __restrict__ order, uint32_t n, uint32_t T,
+                                  RowMetaD* __restrict__ out, uint32_t* __restrict__ het_x1000) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t nb = (n + T - 1) / T;
+    if (b >= nb) return;
+    const uint32_t lo = b * T, hi = min(n, lo + T);
+    RowMetaD m{};
+    m.first = 0xFFFFFFFFu;
+    m.last = 0;
+    uint64_t card = 0, runs = 0, nnz = 0;
+    uint32_t mx = 0;
+    m.has_rank = m.has_occ = m.has_bm = 1;
+    for (uint32_t k = lo; k < hi; ++k) {
+        const RowMetaD& r = v.meta[order[k]];
+        m.has_rank &= r.has_rank;
+        m.has_occ &= r.has_occ;
+        m.has_bm &= r.has_bm;
+        card += r.card;
+        runs += r.runs;
+        nnz += r.nnz;
+        mx = max(mx, r.card);
+        m.nw = max(m.nw, r.nw);
+        if (r.card) {
+            m.first = min(m.first, r.first);
+            m.last = max(m.last, r.last);
+        }
+    }
+    const uint32_t cnt = hi - lo;
+    m.card = (uint32_t)(card / cnt);
+    m.runs = (uint32_t)(runs / cnt);
+    m.nnz = (uint32_t)(nnz / cnt);
+    if (m.first == 0xFFFFFFFFu) m.first = 0;
+    out[b] = m;
+    const double mean = (double)card / cnt;
+    het_x1000[b] = mean > 0 ? (uint32_t)fmin(4e9, 1000.0 * (double)mx / mean) : 1000u;
+}
+
+// Tile (ti, tj), ti <= tj, from a linear index over the block triangle.
+__device__ __forceinline__ void tile_decode(uint32_t nb, uint32_t t, uint32_t& ti, uint32_t& tj) {
+    // rows of the block triangle: row i holds nb - i tiles
+    const double b = 2.0 * nb + 1.0;
+    int64_t i = (int64_t)((b - sqrt(b * b - 8.0 * (double)t)) * 0.5);
+    if (i < 0) i = 0;
+    if (i >= (int64_t)nb) i = nb - 1;
+    auto S = [nb](int64_t r) { return (uint64_t)r * nb - (uint64_t)r * (r - 1) / 2; };
+    while (i > 0 && S(i) > t) --i;
+    while (i + 1 < (int64_t)nb && S(i + 1) <= t) ++i;
+    ti = (uint32_t)i;
+    tj = (uint32_t)(t - S(i) + i);
+}
+
+// ---------------------------------------------------------------- phase 2
+__global__ void select_tiles_kernel(const RowMetaD* __restrict__ bmeta, const uint32_t* __restrict__ het,
+                                    uint32_t nb, int policy, int fixed_cell, CostModelD model,
+                                    const float* __restrict__ mlp, MlpShape shape, TileDecision* __restrict__ dec) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t ntiles = nb * (nb + 1) / 2;
+    if (t >= ntiles) return;
+    uint32_t ti, tj;
+    tile_decode(nb, t, ti, tj);
+    const RowMetaD& a = bmeta[ti];
+    const RowMetaD& b = bmeta[tj];
+    TileDecision d{P_BB, P_BB};
+    if (policy == STORM_POLICY_ALLBITMAP) {
+        d.cell = d.cell2 = P_BB;
+    } else if (policy == STORM_POLICY_FIXED) {
+        d.cell = d.cell2 = fixed_cell;
+    } else if (policy == STORM_POLICY_LEARNED && mlp != nullptr) {
+        float x[MLP_MAX_F];
+        tile_features(a, b, het[ti], het[tj], x);
+        d.cell = d.cell2 = mlp_argmax_available(mlp, shape, x, a, b);
+    } else {
+        double best1 = 0.0;
+        d.cell = select_pairing_d(model, a, b, &best1);
+        if (d.cell == P_EMPTY) d.cell = (a.has_bm && b.has_bm) ? P_BB : P_SS;   // never skip a whole tile
+        d.cell2 = d.cell;
+        if (policy == STORM_POLICY_REFINE || policy == STORM_POLICY_PROBE) {
+            // runner-up (tile_top2, storm_allpairs.cpp:332-347)
+            const bool a_dense = a.card >= b.card;
+            const RowMetaD& dd = a_dense ? a : b;
+            const RowMetaD& ss = a_dense ? b : a;
+            double best2 = 1e300;
+            for (int p = 0; p < P_EMPTY; ++p) {
+                if (p == d.cell || model.ns_per_unit[p] <= 0.0 || !cell_available(p, dd, ss)) continue;
+                const double c = predict_cost(model, p, a, b);
+                if (c < best2) {
+                    best2 = c;
+                    d.cell2 = p;
+                }
+            }
+            if (policy == STORM_POLICY_REFINE) {
+                // heterogeneity gate 8 and top-2 ratio gate 3 (storm_allpairs.cpp:126-138, 402-411)
+                const double h = fmax(het[ti], het[tj]) / 1000.0;
+                const double ratio = best1 > 0.0 ? best2 / best1 : 1e300;
+                if (!(h >= 8.0 && ratio <= 3.0)) d.cell2 = d.cell;
+            }
+        }
+    }
+    dec[t] = d;
+}
+
+struct PairCtx {
+    RowsView v;
+    const uint32_t* order;
+    uint32_t n, T, nb;
+    int policy;
+    CostModelD model;
+};
+
+// One pair in the traversal order -> (count, cell used).  Warp-cooperative.
+__device__ __forceinline__ uint32_t pair_count(const PairCtx& c, uint32_t oi, uint32_t oj, const TileDecision& td,
+                                               int lane, int& used) {
+    const uint32_t ri = c.order[oi], rj = c.order[oj];
+    const RowMetaD& mi = c.v.meta[ri];
+    const RowMetaD& mj = c.v.meta[rj];
+    if (ri == rj) {
+        used = -1;
+        return lane == 0 ? mi.card : 0u;
+    }
+    const bool i_dense = mi.card >= mj.card;
+    const uint32_t d = i_dense ? ri : rj, s = i_dense ? rj : ri;
+    const RowMetaD& md = i_dense ? mi : mj;
+    const RowMetaD& ms = i_dense ? mj : mi;
+    if (c.policy != STORM_POLICY_ALLBITMAP && span_disjoint(md, ms)) {
+        used = P_EMPTY;
+        return 0;
+    }
+    int p = td.cell;
+    if (c.policy == STORM_POLICY_PERPAIR || c.policy == STORM_POLICY_ORACLE) {
+        p = select_pairing_d(c.model, md, ms, nullptr);
+    } else if (c.policy == STORM_POLICY_REFINE && td.cell2 != td.cell) {
+        p = predict_cost(c.model, td.cell2, md, ms) < predict_cost(c.model, td.cell, md, ms) ? td.cell2 : td.cell;
+    }
+    if (p == P_EMPTY) {
+        used = P_EMPTY;
+        return 0;
+    }
+    if (!cell_available(p, md, ms)) p = select_pairing_d(c.model, md, ms, nullptr);   // a row lacks the form
+    if (p == P_EMPTY) {
+        used = P_EMPTY;
+        return 0;
+    }
+    used = p;
+    return run_cell(c.v, p, d, s, lane, c.policy != STORM_POLICY_ALLBITMAP);
+}
+
+// ---------------------------------------------------------------- probe
+// One warp per tile: time the top two cells on up to three pairs of the tile
+// (clock64 on the SM) and keep the faster (probe_tile).
+__global__ void probe_tiles_kernel(PairCtx c, TileDecision* __restrict__ dec, uint32_t ntiles) {
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= ntiles) return;
+    TileDecision td = dec[warp];
+    if (td.cell2 == td.cell) return;
+    uint32_t ti, tj;
+    tile_decode(c.nb, warp, ti, tj);
+    const uint32_t i0 = ti * c.T, i1 = min(c.n, i0 + c.T), j0 = tj * c.T, j1 = min(c.n, j0 + c.T);
+    const int cand[2] = {td.cell, td.cell2};
+    long long best_t = 0x7FFFFFFFFFFFFFFFll;
+    int best = td.cell;
+    for (int q = 0; q < 2; ++q) {
+        const long long t0 = clock64();
+        uint32_t sink = 0;
+        for (uint32_t k = 0; k < 3; ++k) {
+            const uint32_t i = i0 + (uint32_t)((uint64_t)(i1 - i0) * k / 3);
+            const uint32_t j = (j0 == i0) ? i + 1 + k : j0 + (uint32_t)((uint64_t)(j1 - j0) * k / 3);
+            if (!(i < i1 && j < j1 && i != j)) continue;
+            const uint32_t ri = c.order[i], rj = c.order[j];
+            const RowMetaD& mi = c.v.meta[ri];
+            const RowMetaD& mj = c.v.meta[rj];
+            const bool idn = mi.card >= mj.card;
+            const RowMetaD& md = idn ? mi : mj;
+            const RowMetaD& ms = idn ? mj : mi;
+            if (!cell_available(cand[q], md, ms)) continue;
+            sink += run_cell(c.v, cand[q], idn ? ri : rj, idn ? rj : ri, lane, true);
+        }
+        sink = warp_sum_u32(sink);
+        const long long dt = clock64() - t0 + (sink == 0xFFFFFFFFu ? 1 : 0);
+        if (dt < best_t) {
+            best_t = dt;
+            best = cand[q];
+        }
+    }
+    if (lane == 0) dec[warp] = TileDecision{best, best};
+}
+
+// ---------------------------------------------------------------- phase 3
+__global__ void __launch_bounds__(TK_THREADS)
+tiles_kernel(PairCtx c, const TileDecision* __restrict__ dec, uint32_t first_tile, uint32_t tile_count,
+             uint32_t slices, int use_queue, const uint32_t* __restrict__ tile_list, uint32_t* __restrict__ out,
+             RowsStatsDev* __restrict__ st) {
+    __shared__ unsigned long long s_cells[STORM_PAIRING_COUNT + 1];
+    __shared__ unsigned long long s_sum, s_skip, s_pairs;
+    __shared__ uint32_t s_item;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x < STORM_PAIRING_COUNT + 1) s_cells[threadIdx.x] = 0;
+    if (threadIdx.x == 0) s_sum = s_skip = s_pairs = 0;
+    __syncthreads();
+    const uint32_t n_items = tile_count * slices;
+    uint32_t item = blockIdx.x;
+    unsigned long long my_sum = 0, my_skip = 0, my_pairs = 0;
+    uint32_t my_cells[STORM_PAIRING_COUNT + 1];
+    for (int k = 0; k <= STORM_PAIRING_COUNT; ++k) my_cells[k] = 0;
+    for (;;) {
+        if (use_queue) {
+            if (threadIdx.x == 0) s_item = atomicAdd(&st->queue_head, 1u);
+            __syncthreads();
+            item = s_item;
+            __syncthreads();
+        }
+        if (item >= n_items) break;
+        const uint32_t t_local = item / slices, slice = item % slices;
+        const uint32_t t = tile_list ? tile_list[first_tile + t_local] : first_tile + t_local;
+        uint32_t ti, tj;
+        tile_decode(c.nb, t, ti, tj);
+        const TileDecision td = dec[t];
+        const uint32_t i0 = ti * c.T, i1 = min(c.n, i0 + c.T), j0 = tj * c.T, j1 = min(c.n, j0 + c.T);
+        const uint32_t nr = i1 - i0, nc = j1 - j0, np = nr * nc;
+        for (uint32_t q = slice * TK_WARPS + warp; q < np; q += slices * TK_WARPS) {
+            const uint32_t oi = i0 + q / nc, oj = j0 + q % nc;
+            if (ti == tj && oj < oi) continue;
+            int used;
+            uint32_t cnt = pair_count(c, oi, oj, td, lane, used);
+            cnt = warp_sum_u32(cnt);
+            if (lane == 0) {
+                const uint32_t ri = c.order[oi], rj = c.order[oj];
+                const uint32_t lo = min(ri, rj), hi = max(ri, rj);
+                if (out) out[tri_index(c.n, lo, hi)] = cnt;
+                if (used >= 0) {
+                    my_sum += cnt;
+                    ++my_pairs;
+                    ++my_cells[used];
+                    if (used == P_EMPTY) ++my_skip;
+                }
+            }
+        }
+        if (!use_queue) item += gridDim.x;
+    }
+    if (lane == 0) {
+        atomicAdd(&s_sum, my_sum);
+        atomicAdd(&s_skip, my_skip);
+        atomicAdd(&s_pairs, my_pairs);
+        for (int k = 0; k <= STORM_PAIRING_COUNT; ++k)
+            if (my_cells[k]) atomicAdd(&s_cells[k], (unsigned long long)my_cells[k]);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        atomicAdd(&st->sum, s_sum);
+        atomicAdd(&st->skipped, s_skip);
+        atomicAdd(&st->pairs, s_pairs);
+    }
+    if (threadIdx.x < STORM_PAIRING_COUNT + 1 && s_cells[threadIdx.x])
+        atomicAdd(&st->cell_pairs[threadIdx.x], s_cells[threadIdx.x]);
+}
+
+// One cell on one ordered pair (tests / selector labels).
+__global__ void one_cell_kernel(RowsView v, int p, uint32_t a, uint32_t b, unsigned long long* out) {
+    const int lane = threadIdx.x & 31;
+    uint32_t c = 0;
+    switch (p) {
+        case P_BB: c = cell_bb(v, a, b, lane, true); break;
+        case P_BS: c = cell_bs(v, a, b, lane); break;
+        case P_BR: c = cell_br(v, a, b, lane); break;
+        case P_BW: c = cell_bw(v, a, b, lane); break;
+        case P_SS: c = cell_ss(v, a, b, lane); break;
+        case P_SR: c = cell_sr(v, a, b, lane); break;
+        case P_SW: c = cell_sw(v, a, b, lane); break;
+        case P_RR: c = cell_rr(v, a, b, lane); break;
+        case P_RW: c = cell_rw(v, a, b, lane); break;
+        case P_WW: c = cell_ww(v, a, b, lane); break;
+        case P_CB: c = cell_cb(v, a, b, lane); break;
+        default: break;
+    }
+    c = warp_sum_u32(c);
+    if (lane == 0) *out = c;
+}
+
+}  // namespace sb200
+
+// ============================================================== handle
+using namespace sb200;
+
+struct STORM_rows_s {
+    uint32_t universe = 0;
+    std::vector<uint32_t> vals;
+    std::vector<uint64_t> offs{0};
+    uint64_t bitmap_budget = 0;
+    bool dirty = true;
+    RowsPack pack;
+    RowsDev dev;
+    cudaStream_t stream = nullptr;
+    DevBuf<uint32_t> d_order, d_het, d_out, d_tile_list;
+    DevBuf<RowMetaD> d_bmeta;
+    DevBuf<TileDecision> d_dec;
+    DevBuf<RowsStatsDev> d_stats;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // learned selector
+    Mlp mlp;
+    // CUDA graph of the batched form, keyed by the call's shape
+    cudaGraphExec_t graph = nullptr;
+    uint64_t graph_key[6] = {0, 0, 0, 0, 0, 0};
+    ~STORM_rows_s() {
+        if (graph) cudaGraphExecDestroy(graph);
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace sb200 {
+
+static cudaStream_t rows_stream(STORM_rows_t* r) {
+    require_device();
+    if (!r->stream) SB_CUDA(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking));
+    for (auto& e : r->ev)
+        if (!e) SB_CUDA(cudaEventCreate(&e));
+    return r->stream;
+}
+
+void rows_ensure_uploaded(STORM_rows_t* r) {
+    cudaStream_t st = rows_stream(r);
+    if (!r->dirty) return;
+    const uint64_t n = r->offs.size() - 1;
+    const uint32_t nw = (uint32_t)(((uint64_t)r->universe + 63) / 64);
+    const uint64_t row_bytes = (uint64_t)((nw + 1) & ~1u) * 8;
+    uint64_t budget = r->bitmap_budget;
+    if (budget == 0) {
+        size_t fr = 0, tot = 0;
+        SB_CUDA(cudaMemGetInfo(&fr, &tot));
+        budget = fr / 4;
+    }
+    std::vector<uint8_t> bm_rows(n, 1);
+    if (row_bytes * n > budget) {
+        // densest rows first get a bitmap (they are the ones B x * serves)
+        std::vector<uint64_t> ord(n);
+        std::iota(ord.begin(), ord.end(), 0);
+        std::stable_sort(ord.begin(), ord.end(), [&](uint64_t a, uint64_t b) {
+            return (r->offs[a + 1] - r->offs[a]) > (r->offs[b + 1] - r->offs[b]);
+        });
+        std::fill(bm_rows.begin(), bm_rows.end(), 0);
+        const uint64_t fit = budget / row_bytes;
+        for (uint64_t k = 0; k < n && k < fit; ++k) bm_rows[ord[k]] = 1;
+    }
+    pack_rows(r->vals, r->offs, r->universe, bm_rows, r->pack);
+    upload_rows(r->pack, r->universe, r->dev, st);
+    r->dirty = false;
+    if (r->graph) {
+        cudaGraphExecDestroy(r->graph);
+        r->graph = nullptr;
+    }
+}
+
+static bool sorted_order_policy(int policy) {
+    return policy == STORM_POLICY_PERTILE || policy == STORM_POLICY_PROBE || policy == STORM_POLICY_ORACLE ||
+           policy == STORM_POLICY_REFINE || policy == STORM_POLICY_LEARNED;
+}
+
+// density_order (storm_allpairs.cpp:316-323): stable sort by cardinality.
+std::vector<uint32_t> rows_order(const STORM_rows_t* r, int policy) {
+    const uint32_t n = (uint32_t)(r->offs.size() - 1);
+    std::vector<uint32_t> o(n);
+    std::iota(o.begin(), o.end(), 0u);
+    if (sorted_order_policy(policy))
+        std::stable_sort(o.begin(), o.end(), [&](uint32_t a, uint32_t b) {
+            return r->pack.meta[a].card < r->pack.meta[b].card;
+        });
+    return o;
+}
+
+// Full all-pairs call.  out may be null (sum only).
+static void rows_run(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell, int exec, uint32_t* d_out,
+                     STORM_allpairs_stats* st_out) {
+    if (policy < 0 || policy > STORM_POLICY_LEARNED) fail(STORM_B200_EARG, "unknown policy");
+    if (policy == STORM_POLICY_FIXED && (fixed_cell < 0 || fixed_cell >= P_EMPTY))
+        fail(STORM_B200_EARG, "fixed cell must be a pairing below STORM_PAIRING_EMPTY");
+    rows_ensure_uploaded(r);
+    cudaStream_t st = rows_stream(r);
+    const uint32_t n = (uint32_t)(r->offs.size() - 1);
+    const uint32_t T = tile ? tile : 64;
+    STORM_allpairs_stats S{};
+    if (policy == STORM_POLICY_ALLBITMAP)
+        for (uint32_t i = 0; i < n; ++i)
+            if (!r->pack.meta[i].has_bm) fail(STORM_B200_ELIMIT, "all-bitmap policy needs a bitmap for every row");
+    if (n == 0) {
+        if (st_out) *st_out = S;
+        return;
+    }
+    const std::vector<uint32_t> order = rows_order(r, policy);
+    const uint32_t nb = (n + T - 1) / T;
+    const uint32_t ntiles = nb * (nb + 1) / 2;
+    r->d_order.reserve(n);
+    r->d_bmeta.reserve(nb);
+    r->d_het.reserve(nb);
+    r->d_dec.reserve(ntiles);
+    r->d_stats.reserve(1);
+    SB_CUDA(cudaMemcpyAsync(r->d_order.p, order.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+
+    PairCtx c;
+    c.v = r->dev.view;
+    c.order = r->d_order.p;
+    c.n = n;
+    c.T = T;
+    c.nb = nb;
+    c.policy = policy;
+    c.model = default_cost_model();
+    const bool learned = policy == STORM_POLICY_LEARNED && r->mlp.trained;
+    if (learned) r->mlp.ensure_device(st);
+
+    // slices per tile so the launch has enough CTAs
+    const int sms = require_device();
+    uint32_t slices = 1;
+    while ((uint64_t)ntiles * slices < (uint64_t)sms * 8 && slices < 64) slices *= 2;
+
+    auto phases_1_2 = [&]() {
+        SB_CUDA(cudaMemsetAsync(r->d_stats.p, 0, sizeof(RowsStatsDev), st));
+        block_meta_kernel<<<(nb + 127) / 128, 128, 0, st>>>(c.v, c.order, n, T, r->d_bmeta.p, r->d_het.p);
+        select_tiles_kernel<<<(ntiles + 127) / 128, 128, 0, st>>>(
+            r->d_bmeta.p, r->d_het.p, nb, learned ? policy : (policy == STORM_POLICY_LEARNED ? STORM_POLICY_PERTILE : policy),
+            fixed_cell, c.model, learned ? r->mlp.d_params.p : nullptr, r->mlp.shape, r->d_dec.p);
+        if (policy == STORM_POLICY_PROBE)
+            probe_tiles_kernel<<<(ntiles * 32 + 127) / 128, 128, 0, st>>>(c, r->d_dec.p, ntiles);
+    };
+
+    uint32_t launches = 0;
+    SB_CUDA(cudaEventRecord(r->ev[0], st));
+    if (exec == STORM_EXEC_BATCHED) {
+        const uint64_t key[6] = {(uint64_t)policy, T, (uint64_t)fixed_cell, (uint64_t)(uintptr_t)d_out, n,
+                                 learned ? 1ull : 0ull};
+        const bool reuse = r->graph && std::equal(key, key + 6, r->graph_key);
+        if (!reuse) {
+            if (r->graph) {
+                cudaGraphExecDestroy(r->graph);
+                r->graph = nullptr;
+            }
+            cudaGraph_t g;
+            SB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            phases_1_2();
+            const uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)ntiles * slices, (uint64_t)sms * 8);
+            tiles_kernel<<<grid, TK_THREADS, 0, st>>>(c, r->d_dec.p, 0, ntiles, slices, 1, nullptr, d_out,
+                                                      r->d_stats.p);
+            SB_CUDA(cudaStreamEndCapture(st, &g));
+            SB_CUDA(cudaGraphInstantiate(&r->graph, g, 0));
+            cudaGraphDestroy(g);
+            std::copy(key, key + 6, r->graph_key);
+        }
+        SB_CUDA(cudaGraphLaunch(r->graph, st));
+        launches = 3 + (policy == STORM_POLICY_PROBE ? 1 : 0);
+    } else {
+        phases_1_2();
+        SB_CUDA(cudaEventRecord(r->ev[1], st));
+        for (uint32_t t = 0; t < ntiles; ++t) {
+            tiles_kernel<<<slices, TK_THREADS, 0, st>>>(c, r->d_dec.p, t, 1, slices, 0, nullptr, d_out, r->d_stats.p);
+        }
+        launches = 2 + (policy == STORM_POLICY_PROBE ? 1 : 0) + ntiles;
+    }
+    SB_CUDA(cudaGetLastError());
+    SB_CUDA(cudaEventRecord(r->ev[2], st));
+    RowsStatsDev hs;
+    SB_CUDA(cudaMemcpyAsync(&hs, r->d_stats.p, sizeof(hs), cudaMemcpyDeviceToHost, st));
+    SB_CUDA(cudaStreamSynchronize(st));
+    float total_ms = 0.f, sel_ms = 0.f;
+    SB_CUDA(cudaEventElapsedTime(&total_ms, r->ev[0], r->ev[2]));
+    if (exec != STORM_EXEC_BATCHED) SB_CUDA(cudaEventElapsedTime(&sel_ms, r->ev[0], r->ev[1]));
+    S.sum = hs.sum;
+    S.pairs = hs.pairs;
+    S.skipped = hs.skipped;
+    for (int k = 0; k <= STORM_PAIRING_COUNT; ++k) S.cell_pairs[k] = hs.cell_pairs[k];
+    S.decisions = (policy == STORM_POLICY_PERPAIR || policy == STORM_POLICY_ORACLE) ? hs.pairs
+                  : (policy == STORM_POLICY_ALLBITMAP || policy == STORM_POLICY_FIXED) ? 0 : ntiles;
+    S.ns_total = total_ms * 1e6;
+    S.ns_selection = sel_ms * 1e6;
+    S.launches = launches;
+    if (st_out) *st_out = S;
+}
+
+}  // namespace sb200
+
+extern "C" {
+
+STORM_rows_t* STORM_rows_new(uint32_t universe) {
+    try {
+        STORM_rows_t* r = new STORM_rows_t();
+        r->universe = universe;
+        return r;
+    } catch (...) {
+        return NULL;
+    }
+}
+
+void STORM_rows_free(STORM_rows_t* r) { delete r; }
+
+int STORM_rows_add(STORM_rows_t* r, const uint32_t* positions, uint32_t n) {
+    if (r == NULL) return STORM_B200_ENULL;
+    if (positions == NULL && n) return STORM_B200_EVALUES;
+    return guard([&]() -> int {
+        for (uint32_t i = 0; i < n; ++i) {
+            if (positions[i] >= r->universe) return STORM_B200_EARG;
+            if (i && positions[i] <= positions[i - 1]) return STORM_B200_EARG;
+        }
+        r->vals.insert(r->vals.end(), positions, positions + n);
+        r->offs.push_back(r->vals.size());
+        r->dirty = true;
+        return (int)n;
+    });
+}
+
+int STORM_rows_clear(STORM_rows_t* r) {
+    if (r == NULL) return STORM_B200_ENULL;
+    r->vals.clear();
+    r->offs.assign(1, 0);
+    r->dirty = true;
+    return 1;
+}
+
+uint64_t STORM_rows_size(const STORM_rows_t* r) { return r ? r->offs.size() - 1 : 0; }
+
+int STORM_rows_set_bitmap_budget(STORM_rows_t* r, uint64_t bytes) {
+    if (r == NULL) return STORM_B200_ENULL;
+    r->bitmap_budget = bytes;
+    r->dirty = true;
+    return 0;
+}
+
+int STORM_rows_upload(STORM_rows_t* r) {
+    if (r == NULL) return STORM_B200_ENULL;
+    return guard([&]() -> int {
+        rows_ensure_uploaded(r);
+        return 0;
+    });
+}
+
+int STORM_rows_meta(STORM_rows_t* r, uint64_t row, uint32_t* meta9) {
+    if (r == NULL) return STORM_B200_ENULL;
+    if (meta9 == NULL) return STORM_B200_EVALUES;
+    return guard([&]() -> int {
+        rows_ensure_uploaded(r);
+        if (row >= r->pack.meta.size()) return STORM_B200_EARG;
+        const RowMetaD& m = r->pack.meta[row];
+        const uint32_t w[9] = {m.card, m.runs, m.nw, m.nnz, m.first, m.last, m.has_rank, m.has_occ,
+                               (uint32_t)(m.has_bm ? 1 : 0) | (uint32_t)(m.has_comp ? 2 : 0)};
+        std::copy(w, w + 9, meta9);
+        return 0;
+    });
+}
+
+int STORM_rows_allpairs_sum(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell, int exec,
+                            STORM_allpairs_stats* st) {
+    if (r == NULL) return STORM_B200_ENULL;
+    return guard([&]() -> int {
+        rows_run(r, policy, tile, fixed_cell, exec, nullptr, st);
+        return 0;
+    });
+}
+
+int STORM_rows_allpairs_matrix(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell, int exec, uint32_t* out,
+                               uint64_t out_len, STORM_allpairs_stats* st) {
+    if (r == NULL) return STORM_B200_ENULL;
+    return guard([&]() -> int {
+        const uint64_t n = r->offs.size() - 1, need = tri_size(n);
+        if (out_len < need) return STORM_B200_ESIZE;
+        if (out == NULL && need) return STORM_B200_EVALUES;
+        r->d_out.reserve(need ? need : 1);
+        rows_run(r, policy, tile, fixed_cell, exec, r->d_out.p, st);
+        if (need) {
+            SB_CUDA(cudaMemcpyAsync(out, r->d_out.p, need * sizeof(uint32_t), cudaMemcpyDeviceToHost, r->stream));
+            SB_CUDA(cudaStreamSynchronize(r->stream));
+        }
+        return 0;
+    });
+}
+
+int STORM_rows_allpairs_tiles(STORM_rows_t* r, int policy, uint32_t tile, int exec, STORM_tile_callback cb,
+                              void* ctx, STORM_allpairs_stats* st) {
+    if (r == NULL) return STORM_B200_ENULL;
+    if (cb == NULL) return STORM_B200_EARG;
+    const uint64_t n = r->offs.size() - 1;
+    const uint32_t T = tile ? tile : 64;
+    std::vector<uint32_t> tri(tri_size(n) ? tri_size(n) : 1);
+    int rc = STORM_rows_allpairs_matrix(r, policy, T, STORM_PAIRING_BS, exec, tri.data(), tri.size(), st);
+    if (rc < 0) return rc;
+    return guard([&]() -> int {
+        std::vector<uint32_t> buf((size_t)T * T);
+        for (uint64_t i0 = 0; i0 < n; i0 += T) {
+            const uint64_t i1 = std::min<uint64_t>(i0 + T, n);
+            for (uint64_t j0 = i0; j0 < n; j0 += T) {
+                const uint64_t j1 = std::min<uint64_t>(j0 + T, n);
+                std::fill(buf.begin(), buf.end(), 0u);
+                for (uint64_t i = i0; i < i1; ++i) {
+                    const uint64_t base = i * n - (i * (i - 1)) / 2 - i;
+                    for (uint64_t j = (j0 == i0 ? i + 1 : j0); j < j1; ++j) buf[(i - i0) * T + (j - j0)] = tri[base + j];
+                }
+                cb((uint32_t)i0, (uint32_t)j0, (uint32_t)(i1 - i0), (uint32_t)(j1 - j0), buf.data(), ctx);
+            }
+        }
+        return 0;
+    });
+}
+
+static RowMetaD meta_from8(const uint32_t* m) {
+    RowMetaD r{};
+    r.card = m[0]; r.runs = m[1]; r.nw = m[2]; r.nnz = m[3]; r.first = m[4]; r.last = m[5];
+    r.has_rank = m[6] != 0; r.has_occ = m[7] != 0; r.has_bm = 1; r.has_comp = 0;
+    return r;
+}
+
+int STORM_select_pairing(const uint32_t* ma, const uint32_t* mb, double* predicted) {
+    if (ma == NULL || mb == NULL) return STORM_B200_EVALUES;
+    const CostModelD m = default_cost_model();
+    return select_pairing_d(m, meta_from8(ma), meta_from8(mb), predicted);
+}
+
+double STORM_predict(int pairing, const uint32_t* ma, const uint32_t* mb) {
+    if (ma == NULL || mb == NULL || pairing < 0 || pairing > P_EMPTY) return -1.0;
+    const CostModelD m = default_cost_model();
+    return predict_cost(m, pairing, meta_from8(ma), meta_from8(mb));
+}
+
+int64_t STORM_rows_cell(STORM_rows_t* r, int pairing, uint64_t a, uint64_t b) {
+    if (r == NULL) return STORM_B200_ENULL;
+    int64_t res = 0;
+    int rc = guard([&]() -> int {
+        rows_ensure_uploaded(r);
+        const uint64_t n = r->offs.size() - 1;
+        if (a >= n || b >= n || pairing < 0 || pairing > P_CB || pairing == P_EMPTY) return STORM_B200_EARG;
+        const RowMetaD& ma = r->pack.meta[a];
+        const RowMetaD& mb = r->pack.meta[b];
+        const bool need_a_bm = pairing == P_BB || pairing == P_BS || pairing == P_BR || pairing == P_BW;
+        if ((need_a_bm && !ma.has_bm) || (pairing == P_BB && !mb.has_bm)) return STORM_B200_ELIMIT;
+        if (pairing == P_CB && (!ma.has_comp || !mb.has_bm)) return STORM_B200_ELIMIT;
+        cudaStream_t st = rows_stream(r);
+        DevBuf<unsigned long long> d;
+        d.reserve(1);
+        one_cell_kernel<<<1, 32, 0, st>>>(r->dev.view, pairing, (uint32_t)a, (uint32_t)b, d.p);
+        SB_CUDA(cudaGetLastError());
+        unsigned long long h = 0;
+        SB_CUDA(cudaMemcpyAsync(&h, d.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+        SB_CUDA(cudaStreamSynchronize(st));
+        res = (int64_t)h;
+        return 0;
+    });
+    return rc < 0 ? rc : res;
+}
+
+}  // extern "C"
+
+// ======================================================= selector training
+namespace sb200 {
+
+// Labels for the learned selector: every cell on (a sample of the pairs of)
+// each sampled tile, timed with the SM clock.  One CTA per (tile, cell);
+// cycles = ~0 when some pair of the tile lacks a form the cell needs.
+__global__ void __launch_bounds__(TK_THREADS)
+time_cells_kernel(PairCtx c, const uint32_t* __restrict__ tiles, uint32_t n_samples, uint32_t max_pairs,
+                  unsigned long long* __restrict__ cycles) {
+    const uint32_t sample = blockIdx.x / P_EMPTY, cell = blockIdx.x % P_EMPTY;
+    if (sample >= n_samples) return;
+    __shared__ int s_missing;
+    __shared__ long long s_t0;
+    __shared__ unsigned int s_sink;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t ti, tj;
+    tile_decode(c.nb, tiles[sample], ti, tj);
+    const uint32_t i0 = ti * c.T, i1 = min(c.n, i0 + c.T), j0 = tj * c.T, j1 = min(c.n, j0 + c.T);
+    const uint32_t nr = i1 - i0, nc = j1 - j0, np = nr * nc;
+    const uint32_t step = np > max_pairs ? np / max_pairs : 1;
+    if (threadIdx.x == 0) {
+        s_missing = 0;
+        s_sink = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) s_t0 = clock64();
+    __syncthreads();
+    uint32_t sink = 0;
+    for (uint32_t q = warp * step; q < np; q += TK_WARPS * step) {
+        const uint32_t oi = i0 + q / nc, oj = j0 + q % nc;
+        if (ti == tj && oj <= oi) continue;
+        const uint32_t ri = c.order[oi], rj = c.order[oj];
+        const RowMetaD& mi = c.v.meta[ri];
+        const RowMetaD& mj = c.v.meta[rj];
+        const bool idn = mi.card >= mj.card;
+        const RowMetaD& md = idn ? mi : mj;
+        const RowMetaD& ms = idn ? mj : mi;
+        if (span_disjoint(md, ms)) continue;
+        if (!cell_available((int)cell, md, ms)) {
+            s_missing = 1;
+            continue;
+        }
+        sink += run_cell(c.v, (int)cell, idn ? ri : rj, idn ? rj : ri, lane, true);
+    }
+    sink = warp_sum_u32(sink);
+    if (lane == 0) atomicAdd(&s_sink, sink);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const long long dt = clock64() - s_t0;
+        cycles[(uint64_t)sample * P_EMPTY + cell] =
+            s_missing ? ~0ull : (unsigned long long)dt + (s_sink == 0xFFFFFFFFu ? 1ull : 0ull);
+    }
+}
+
+}  // namespace sb200
+
+extern "C" {
+
+int STORM_rows_train_selector(STORM_rows_t* r, uint32_t tile, uint32_t samples, uint32_t epochs, uint64_t seed,
+                              double* stats) {
+    if (r == NULL) return STORM_B200_ENULL;
+    return guard([&]() -> int {
+        rows_ensure_uploaded(r);
+        cudaStream_t st = rows_stream(r);
+        const uint32_t n = (uint32_t)(r->offs.size() - 1);
+        if (n < 2) return STORM_B200_EARG;
+        const uint32_t T = tile ? tile : 64;
+        const std::vector<uint32_t> order = rows_order(r, STORM_POLICY_PERTILE);
+        const uint32_t nb = (n + T - 1) / T, ntiles = nb * (nb + 1) / 2;
+        r->d_order.reserve(n);
+        r->d_bmeta.reserve(nb);
+        r->d_het.reserve(nb);
+        SB_CUDA(cudaMemcpyAsync(r->d_order.p, order.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        PairCtx c;
+        c.v = r->dev.view;
+        c.order = r->d_order.p;
+        c.n = n;
+        c.T = T;
+        c.nb = nb;
+        c.policy = STORM_POLICY_PERTILE;
+        c.model = default_cost_model();
+        block_meta_kernel<<<(nb + 127) / 128, 128, 0, st>>>(c.v, c.order, n, T, r->d_bmeta.p, r->d_het.p);
+        std::vector<RowMetaD> bmeta(nb);
+        std::vector<uint32_t> het(nb);
+        SB_CUDA(cudaMemcpyAsync(bmeta.data(), r->d_bmeta.p, nb * sizeof(RowMetaD), cudaMemcpyDeviceToHost, st));
+        SB_CUDA(cudaMemcpyAsync(het.data(), r->d_het.p, nb * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        // sample tiles (all of them when there are few)
+        uint64_t s = seed ? seed : 0x5E1EC7;
+        auto rnd = [&s]() {
+            uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+            z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+            z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+            return z ^ (z >> 31);
+        };
+        std::vector<uint32_t> pick;
+        if (samples == 0 || samples >= ntiles) {
+            pick.resize(ntiles);
+            std::iota(pick.begin(), pick.end(), 0u);
+        } else {
+            std::vector<uint32_t> all(ntiles);
+            std::iota(all.begin(), all.end(), 0u);
+            for (uint32_t k = 0; k < samples; ++k) std::swap(all[k], all[k + rnd() % (ntiles - k)]);
+            pick.assign(all.begin(), all.begin() + samples);
+        }
+        const uint32_t ns = (uint32_t)pick.size();
+        DevBuf<uint32_t> dpick;
+        DevBuf<unsigned long long> dcyc;
+        dpick.reserve(ns);
+        dcyc.reserve((size_t)ns * P_EMPTY);
+        SB_CUDA(cudaMemcpyAsync(dpick.p, pick.data(), ns * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        std::vector<unsigned long long> cyc((size_t)ns * P_EMPTY, ~0ull), tmp((size_t)ns * P_EMPTY);
+        for (int rep = 0; rep < 3; ++rep) {   // min of three timings per (tile, cell)
+            time_cells_kernel<<<ns * P_EMPTY, TK_THREADS, 0, st>>>(c, dpick.p, ns, 256, dcyc.p);
+            SB_CUDA(cudaGetLastError());
+            SB_CUDA(cudaMemcpyAsync(tmp.data(), dcyc.p, tmp.size() * sizeof(unsigned long long),
+                                    cudaMemcpyDeviceToHost, st));
+            SB_CUDA(cudaStreamSynchronize(st));
+            for (size_t k = 0; k < cyc.size(); ++k) cyc[k] = std::min(cyc[k], tmp[k]);
+        }
+        // features, labels, the cost model's choice
+        const MlpShape sh = r->mlp.shape;
+        std::vector<float> X;
+        std::vector<int32_t> Y;
+        std::vector<uint32_t> idx;
+        for (uint32_t k = 0; k < ns; ++k) {
+            uint32_t best = P_EMPTY;
+            unsigned long long bc = ~0ull;
+            for (uint32_t cl = 0; cl < P_EMPTY; ++cl)
+                if (cyc[(size_t)k * P_EMPTY + cl] < bc) {
+                    bc = cyc[(size_t)k * P_EMPTY + cl];
+                    best = cl;
+                }
+            if (best == P_EMPTY) continue;
+            uint32_t ti, tj;
+            {   // host copy of tile_decode
+                uint64_t t = pick[k], i = 0;
+                auto S = [nb](uint64_t q) { return q * nb - q * (q - 1) / 2; };
+                while (i + 1 < nb && S(i + 1) <= t) ++i;
+                ti = (uint32_t)i;
+                tj = (uint32_t)(t - S(i) + i);
+            }
+            float x[MLP_MAX_F];
+            tile_features(bmeta[ti], bmeta[tj], het[ti], het[tj], x);
+            X.insert(X.end(), x, x + sh.F);
+            Y.push_back((int32_t)best);
+            idx.push_back(k);
+        }
+        const uint32_t nl = (uint32_t)Y.size();
+        if (nl < 4) return STORM_B200_EARG;
+        // 80 / 20 split, deterministic by sample position
+        std::vector<float> Xtr, Xte;
+        std::vector<int32_t> Ytr, Yte;
+        std::vector<uint32_t> te_idx;
+        for (uint32_t k = 0; k < nl; ++k) {
+            const bool test = (k % 5) == 4;
+            (test ? Xte : Xtr).insert((test ? Xte : Xtr).end(), X.begin() + (size_t)k * sh.F,
+                                      X.begin() + (size_t)(k + 1) * sh.F);
+            (test ? Yte : Ytr).push_back(Y[k]);
+            if (test) te_idx.push_back(idx[k]);
+        }
+        mlp_init(r->mlp, seed ^ 0xA5A5A5A5ull);
+        r->mlp.dirty = true;
+        const float loss = mlp_train(r->mlp, Xtr, Ytr, epochs ? epochs : 400, st);
+        r->mlp.trained = true;
+        // accuracy on the training split
+        uint32_t correct = 0;
+        for (size_t k = 0; k < Ytr.size(); ++k) {
+            float h[MLP_MAX_H], lg[MLP_MAX_C];
+            mlp_forward(r->mlp.params.data(), sh, Xtr.data() + k * sh.F, h, lg);
+            uint32_t am = 0;
+            for (uint32_t cl = 1; cl < sh.C; ++cl)
+                if (lg[cl] > lg[am]) am = cl;
+            correct += (am == (uint32_t)Ytr[k]);
+        }
+        // regret on the held-out tiles: sum of chosen cycles / sum of best - 1
+        const CostModelD model = default_cost_model();
+        double best_sum = 0, mlp_sum = 0, cost_sum = 0;
+        for (size_t q = 0; q < te_idx.size(); ++q) {
+            const uint32_t k = te_idx[q];
+            uint32_t ti, tj;
+            {
+                uint64_t t = pick[k], i = 0;
+                auto S = [nb](uint64_t z) { return z * nb - z * (z - 1) / 2; };
+                while (i + 1 < nb && S(i + 1) <= t) ++i;
+                ti = (uint32_t)i;
+                tj = (uint32_t)(t - S(i) + i);
+            }
+            const unsigned long long* cy = cyc.data() + (size_t)k * P_EMPTY;
+            const int y = Yte[q];
+            const int m_cell = mlp_argmax_available(r->mlp.params.data(), sh, Xte.data() + q * sh.F, bmeta[ti], bmeta[tj]);
+            int c_cell = select_pairing_d(model, bmeta[ti], bmeta[tj], nullptr);
+            if (c_cell == P_EMPTY) c_cell = (bmeta[ti].has_bm && bmeta[tj].has_bm) ? P_BB : P_SS;
+            auto cost = [&](int cl) { return cy[cl] == ~0ull ? (double)cy[y] * 4.0 : (double)cy[cl]; };
+            best_sum += (double)cy[y];
+            mlp_sum += cost(m_cell);
+            cost_sum += cost(c_cell);
+        }
+        if (stats) {
+            stats[0] = ns;
+            stats[1] = epochs ? epochs : 400;
+            stats[2] = loss;
+            stats[3] = Ytr.empty() ? 0.0 : (double)correct / Ytr.size();
+            stats[4] = best_sum > 0 ? mlp_sum / best_sum - 1.0 : 0.0;
+            stats[5] = best_sum > 0 ? cost_sum / best_sum - 1.0 : 0.0;
+        }
+        if (r->graph) {
+            cudaGraphExecDestroy(r->graph);
+            r->graph = nullptr;
+        }
+        return 0;
+    });
+}
+
+int STORM_rows_reset_selector(STORM_rows_t* r) {
+    if (r == NULL) return STORM_B200_ENULL;
+    r->mlp.trained = false;
+    if (r->graph) {
+        cudaGraphExecDestroy(r->graph);
+        r->graph = nullptr;
+    }
+    return 0;
+}
+
+int64_t STORM_rows_selector_params(STORM_rows_t* r, float* params, uint64_t n_params, int load) {
+    if (r == NULL) return STORM_B200_ENULL;
+    const uint64_t np = r->mlp.shape.n_params();
+    if (params == NULL) return (int64_t)np;
+    if (n_params < np) return STORM_B200_ESIZE;
+    if (load) {
+        r->mlp.params.assign(params, params + np);
+        r->mlp.trained = true;
+        r->mlp.dirty = true;
+        if (r->graph) {
+            cudaGraphExecDestroy(r->graph);
+            r->graph = nullptr;
+        }
+    } else {
+        if (r->mlp.params.size() != np) return STORM_B200_EARG;
+        std::copy(r->mlp.params.begin(), r->mlp.params.end(), params);
+    }
+    return (int64_t)np;
+}
+
+}  // extern "C"

@@ -10,11 +10,11 @@ import oracle_lib as ol
 
 pytestmark = pytest.mark.gpu
 
-KERNELS = ("popc", "mma")
+KERNELS = ("popc", "mma", "mma_ss")
 
 
 def _kernel(sb, name):
-    return {"popc": sb.KERNEL_POPC, "mma": sb.KERNEL_MMA}[name]
+    return {"popc": sb.KERNEL_POPC, "mma": sb.KERNEL_MMA, "mma_ss": sb.KERNEL_MMA_SS}[name]
 
 
 def contig_from_words(sb, words, m, kernel):
@@ -189,9 +189,28 @@ def _check_full_size(sb, n, m, p, seed, kernels):
 
 def test_config1_full_size_both_kernels(sb):
     """4096 rows x 65536 bits, Bernoulli(0.5): every pair, both kernels."""
-    _check_full_size(sb, 4096, 65536, 0.5, 101, ["mma", "popc"])
+    _check_full_size(sb, 4096, 65536, 0.5, 101, ["mma", "mma_ss", "popc"])
 
 
 def test_config2_full_size_tensor_kernel(sb):
     """65536 rows x 262144 bits, p ~ U[0.05, 0.5] (2 GiB in, 8.6 GB out)."""
     _check_full_size(sb, 65536, 262144, (0.05, 0.5), 202, ["mma"])
+
+
+def test_device_pointer_ingest_orders_after_producer(sb):
+    """Rows generated on torch's stream and handed over as a device pointer
+    right away must be read only after the generator finished."""
+    import torch
+    import bench
+    n, m = 4096, 65536
+    rows = bench.bernoulli_rows_gpu(n, m, (0.05, 0.5), 31, torch.device("cuda"))
+    c = sb.StormContig(m)
+    assert sb.lib().STORM_contig_add_bitmaps(c.h, sb.C.cast(rows.data_ptr(), sb.u64p), n, m // 64) == n
+    host = rows.cpu().numpy().view(np.uint64)
+    ref = sb.StormContig(m)
+    ref.add_bitmaps(host)
+    assert c.pairw_intersect_cardinality() == ref.pairw_intersect_cardinality()
+    want = ol.contig_row(host, 5)
+    mat, _ = c.matrix()
+    base = int(sb.tri_index(n, 5, 5))
+    np.testing.assert_array_equal(mat[base: base + n - 5], want)

@@ -1,0 +1,144 @@
+"""The kernel layer on the GPU (STORM_rows_t): every cell on every ordered
+pair of the reference's edge rows, every policy and both execution forms
+against the reference's golden all-pairs outputs and the oracle."""
+import numpy as np
+import pytest
+
+import gen
+import oracle_lib as ol
+from conftest import golden_sets
+
+pytestmark = pytest.mark.gpu
+
+
+def rows_of(sb, sets, universe, budget=None):
+    r = sb.StormRows(universe)
+    if budget is not None:
+        r.set_bitmap_budget(budget)
+    for s in sets:
+        r.add(np.asarray(s, dtype=np.uint32))
+    return r
+
+
+def edge_rows(u):
+    cand = [[], [0], [u - 1], [63, 64], [511, 512], list(range(u)), list(range(0, u, 64)), list(range(0, u, 2)),
+            list(range(u // 2, min(u // 2 + 300, u))), list(range(1, min(200, u)))]
+    return [np.array(sorted(set(p for p in c if p < u)), dtype=np.uint32) for c in cand]
+
+
+CELLS = ["BB", "BS", "BR", "BW", "SS", "SR", "SW", "RR", "RW", "WW", "CB"]
+
+
+@pytest.mark.parametrize("u", [64, 128, 1024, 1025, 4033, 5000, 8192, 65536, 70001])
+def test_every_cell_on_edge_rows_both_orders(sb, u):
+    """tests/test_cells.cpp:195-230 shapes at the same universes, every cell,
+    both argument orders, against the oracle."""
+    rows = edge_rows(u) + gen.run_sets(3, u, 6, 40, u) + [gen.uniform_set(gen.rng(u), u // 3, u)]
+    r = rows_of(sb, rows, u)
+    n = len(rows)
+    for i in range(n):
+        for j in range(n):
+            want = ol.oracle().oracle_list_intersect(ol._p(rows[i], ol.u32p), rows[i].size,
+                                                     ol._p(rows[j], ol.u32p), rows[j].size)
+            meta_i = r.meta(i)
+            for name in CELLS:
+                p = CELLS.index(name) if name != "CB" else sb.P_CB
+                if name == "CB" and not (meta_i[8] & 2):
+                    continue   # complement exists only above density 1/2
+                got = r.cell(p, i, j)
+                assert got == want, (u, name, i, j, got, want)
+
+
+def test_representation_metadata_matches_reference(sb, golden):
+    rows = golden_sets(golden, "repr/")
+    for k, (v, u) in enumerate(zip(rows, golden["repr/universe"])):
+        r = rows_of(sb, [v], int(u))
+        m = r.meta(0)
+        np.testing.assert_array_equal(m[:8], golden["repr/meta"][k], err_msg=f"row {k}")
+        assert bool(m[8] & 2) == (golden["repr/sizes"][k][4] > 0)   # complement built iff reference builds it
+
+
+POLICIES = ["ALLBITMAP", "PERPAIR", "PERTILE", "ORACLE", "PROBE", "REFINE", "LEARNED"]
+
+
+@pytest.mark.parametrize("exec_", ["batched", "per_tile"])
+def test_golden_allpairs_every_policy(sb, golden, exec_):
+    ex = sb.EXEC_BATCHED if exec_ == "batched" else sb.EXEC_PER_TILE
+    names = sorted({k.split("/")[1] for k in golden.files if k.startswith("rows/")})
+    for name in names:
+        sets = golden_sets(golden, f"rows/{name}/")
+        u = int(golden[f"rows/{name}/universe"][0])
+        r = rows_of(sb, sets, u)
+        want = int(golden[f"rows/{name}/allpairs_sum"][0][2])
+        n = len(sets)
+        strict_want = golden[f"rows/{name}/tiles_strict"]
+        iu = np.triu_indices(n)
+        strict = iu[0] != iu[1]
+        for pol in POLICIES:
+            for tile in (8, 16, 64):
+                s, st = r.allpairs_sum(getattr(sb, "POLICY_" + pol), tile, exec_=ex)
+                assert s == want, (name, pol, tile)
+                assert st["pairs"] == n * (n - 1) // 2, (name, pol, tile, st)
+            mat, st = r.allpairs_matrix(getattr(sb, "POLICY_" + pol), 16, exec_=ex)
+            np.testing.assert_array_equal(mat[strict], strict_want[strict], err_msg=f"{name}/{pol}")
+            np.testing.assert_array_equal(mat[~strict], [len(x) for x in sets])
+
+
+def test_fixed_cell_policy_every_cell(sb, golden):
+    sets = golden_sets(golden, "rows/runs_u4033/")
+    r = rows_of(sb, sets, 4033)
+    want = int(golden["rows/runs_u4033/allpairs_sum"][0][2])
+    for p in range(10):
+        s, st = r.allpairs_sum(sb.POLICY_FIXED, 16, fixed_cell=p)
+        assert s == want, sb.PAIRINGS[p]
+        live = {k: v for k, v in st["cell_pairs"].items() if k != "EMPTY"}
+        assert set(live) <= {sb.PAIRINGS[p]}, st
+
+
+def test_tiles_visitor_original_order(sb, golden):
+    sets = golden_sets(golden, "rows/inverse_u16384/")
+    r = rows_of(sb, sets, 16384)
+    col, st = r.allpairs_tiles(sb.POLICY_PERTILE, 64)
+    n = len(sets)
+    iu = np.triu_indices(n)
+    strict = iu[0] != iu[1]
+    np.testing.assert_array_equal(col.out[strict], golden["rows/inverse_u16384/tiles_strict"][strict])
+
+
+@pytest.mark.parametrize("case", ["zipf", "runs", "haplo", "sweep"])
+def test_config_shaped_corpora_all_policies(sb, case):
+    if case == "zipf":
+        sets, u = gen.zipf_sets(120, 1 << 24, 1.1, 16, 1 << 16, 41), 1 << 24
+    elif case == "runs":
+        sets, u = gen.run_sets(100, 1 << 26, 30, 256, 42), 1 << 26
+    elif case == "haplo":
+        sets, u = gen.haplotype_sets(240, 20000, 32, 43), 20000
+    else:
+        sets, u = [], 1 << 22
+        for d in (1e-5, 1e-4, 1e-3, 1e-2, 0.17):
+            sets += gen.bernoulli_sets(20, u, d, int(d * 1e6) + 44)
+    r = rows_of(sb, sets, u)
+    vals, offs = gen.to_csr(sets)
+    want, ws = ol.sets_matrix(vals, offs)
+    for pol in ("PERPAIR", "PERTILE", "PROBE", "REFINE", "LEARNED"):
+        for ex in (sb.EXEC_BATCHED, sb.EXEC_PER_TILE):
+            mat, st = r.allpairs_matrix(getattr(sb, "POLICY_" + pol), 32, exec_=ex)
+            assert st["sum"] == ws, (case, pol)
+            np.testing.assert_array_equal(mat, want, err_msg=f"{case}/{pol}/{ex}")
+
+
+def test_rows_without_bitmaps_stay_exact(sb):
+    """A bitmap budget too small for every row leaves the sparse rows without
+    B (the reference's sparse_only rows): B cells are skipped for them and
+    all-bitmap is refused, every other policy stays exact."""
+    sets = gen.zipf_sets(80, 1 << 20, 1.1, 16, 1 << 15, 51)
+    r = rows_of(sb, sets, 1 << 20, budget=10 * (1 << 20) // 8)   # room for ~10 bitmaps
+    metas = [r.meta(i) for i in range(len(sets))]
+    assert 0 < sum(int(m[8] & 1) for m in metas) < len(sets)
+    vals, offs = gen.to_csr(sets)
+    want, ws = ol.sets_matrix(vals, offs)
+    with pytest.raises(sb.StormError):
+        r.allpairs_sum(sb.POLICY_ALLBITMAP)
+    for pol in ("PERPAIR", "PERTILE", "PROBE", "REFINE"):
+        mat, st = r.allpairs_matrix(getattr(sb, "POLICY_" + pol), 16)
+        np.testing.assert_array_equal(mat, want, err_msg=pol)
