@@ -107,6 +107,32 @@ uint32_t STORM_contig_last_launches(const STORM_contiguous_t* c);
 /* Which kernel the last call ran (STORM_B200_KERNEL_POPC, _MMA or _MMA_SS). */
 int STORM_contig_last_kernel(const STORM_contiguous_t* c);
 
+/* All pairs of rows that are already in device memory, into a device buffer,
+ * without allocating anything.  No counterpart in the reference: it is for
+ * callers that cannot allocate device memory when they need the counts -- a
+ * service that reserves all of HBM for its own pool at start-up and forbids
+ * cudaMalloc afterwards, or a framework whose allocator owns every device
+ * buffer.  The caller owns both buffers:
+ *   d_rows  row r at d_rows + r * row_pitch_words (pitch a multiple of 8
+ *           words); ceil(n_rows / 256) * 256 rows must be readable, the
+ *           rows from n_rows on must be zero, and so must every bit of a row
+ *           at or past row_bits (up to the pitch);
+ *   d_out   n_rows*(n_rows+1)/2 u32, packed upper triangle (may be NULL for
+ *           the sum only).
+ * Runs the tensor-core kernel (row_bits <= 2^23) on `stream` (a
+ * cudaStream_t; NULL = the default stream) and waits for it.  Its scratch
+ * (status/sum words and a tile list of at most 32768 tiles of 128 x 256
+ * pairs, about 23,000 rows) is a 256 KiB array in the library that every GPU
+ * holding the library keeps until exit; larger problems return
+ * STORM_B200_ELIMIT.  The first call on a device looks that array up (and
+ * opts the kernel into its shared memory), so make the first call before any
+ * stream capture.  All calls share the one array: calls that overlap on the
+ * GPU race and must not be issued. */
+int STORM_contig_pairw_intersect_matrix_noalloc(const uint64_t* d_rows, uint64_t n_rows,
+                                                uint32_t row_pitch_words, uint64_t row_bits,
+                                                uint32_t* d_out, uint64_t out_len, uint64_t* sum,
+                                                void* stream);
+
 /* ---- STORM_t extensions ----------------------------------------------- */
 int STORM_upload(STORM_t* s);
 int STORM_pairw_intersect_matrix(STORM_t* s, uint32_t* out, uint64_t out_len, uint64_t* sum);

@@ -4,6 +4,8 @@
 #include "bb_mma.cuh"
 #include "bb_mma_ts.cuh"
 
+#include <mutex>
+
 namespace sb200 {
 
 static void build_tiles(std::vector<uint2>& t, uint64_t n, int kind) {
@@ -94,3 +96,99 @@ uint64_t DenseEngine::run(const uint64_t* dX, uint64_t n, uint32_t w_pad, uint64
 }
 
 }  // namespace sb200
+
+// ===================================================================
+// Allocation-free entry point.
+//
+// Some callers cannot allocate device memory at the time they need the
+// counts: a service that reserves all of HBM for its own pool at start-up
+// and forbids cudaMalloc afterwards (a cudaMalloc on a busy device can
+// stall other work and can fail mid-request), or a host framework that owns
+// every device buffer through its own allocator.  They hand in the rows and
+// the output buffer; this path adds nothing to them.  The tensor-core
+// kernel's scratch -- the status / sum words and the tile list -- lives in
+// the file-scope array below, sized for at most NOALLOC_MAX_TILES tiles,
+// which every GPU that loads the library keeps until the process exits.
+// ===================================================================
+namespace sb200 {
+
+constexpr uint32_t NOALLOC_MAX_TILES = 32768;   // 256 KiB of (bi, bj) pairs
+
+struct NoAllocScratch {
+    DeviceFlags flags;
+    uint2 tiles[NOALLOC_MAX_TILES];
+};
+
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+// One thread per A block row bi writes its tiles (bi, bj), bj >= bi / 2,
+// at offset bi * nbj - sum_{k < bi} floor(k / 2).
+__global__ void noalloc_tiles_kernel(NoAllocScratch* s, uint32_t nbi, uint32_t nbj) {
+    const uint32_t bi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (bi >= nbi) return;
+    const uint64_t m = bi / 2;
+    const uint64_t below = (bi % 2 == 0) ? m * (m - (m > 0 ? 1 : 0)) : m * m;
+    uint64_t t = (uint64_t)bi * nbj - below;
+    for (uint32_t bj = bi / 2; bj < nbj; ++bj, ++t) s->tiles[t] = make_uint2(bi, bj);
+}
+
+}  // namespace sb200
+
+extern "C" int STORM_contig_pairw_intersect_matrix_noalloc(const uint64_t* d_rows, uint64_t n_rows,
+                                                           uint32_t row_pitch_words, uint64_t row_bits,
+                                                           uint32_t* d_out, uint64_t out_len, uint64_t* sum,
+                                                           void* stream) {
+    using namespace sb200;
+    if (d_rows == NULL) return STORM_B200_EVALUES;
+    if (n_rows == 0 || n_rows > 0xFFFFFFFFull) return STORM_B200_EARG;
+    if (row_pitch_words == 0 || row_pitch_words % 8 != 0 || (uint64_t)row_pitch_words * 64 < row_bits)
+        return STORM_B200_EARG;
+    if (row_bits > MMA_MAX_BITS) return STORM_B200_ELIMIT;
+    const uint64_t need = n_rows * (n_rows + 1) / 2;
+    if (d_out != NULL && out_len < need) return STORM_B200_ESIZE;
+    const uint32_t nbi = (uint32_t)((n_rows + TS_BM - 1) / TS_BM), nbj = (uint32_t)((n_rows + TS_BN - 1) / TS_BN);
+    uint64_t n_tiles = 0;
+    for (uint32_t bi = 0; bi < nbi; ++bi) n_tiles += nbj - bi / 2;
+    if (n_tiles > NOALLOC_MAX_TILES) return STORM_B200_ELIMIT;
+
+    // Once per device, with that device current: the device address of the
+    // scratch array, and the kernel's shared-memory opt-in.
+    static std::mutex mu;
+    static void* scratch_of[64] = {nullptr};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return STORM_B200_ECUDA;
+    NoAllocScratch* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (scratch_of[dev] == nullptr) {
+            int major = 0, sms = 0;
+            if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess || major != 10)
+                return STORM_B200_ECUDA;
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr) return STORM_B200_ECUDA;
+            if (cudaFuncSetAttribute(bb_mma_ts_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)TS_SMEM_BYTES) != cudaSuccess)
+                return STORM_B200_ECUDA;
+            (void)sms;
+            scratch_of[dev] = p;
+        }
+        scratch = static_cast<NoAllocScratch*>(scratch_of[dev]);
+    }
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return STORM_B200_ECUDA;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cudaMemsetAsync(&scratch->flags, 0, sizeof(DeviceFlags), st) != cudaSuccess) return STORM_B200_ECUDA;
+    noalloc_tiles_kernel<<<(nbi + 127) / 128, 128, 0, st>>>(scratch, nbi, nbj);
+    const uint32_t grid = n_tiles < (uint64_t)sms ? (uint32_t)n_tiles : (uint32_t)sms;
+    bb_mma_ts_kernel<<<grid, TS_THREADS, TS_SMEM_BYTES, st>>>(d_rows, (uint32_t)n_rows, row_pitch_words,
+                                                               scratch->tiles, (uint32_t)n_tiles, d_out,
+                                                               &scratch->flags);
+    if (cudaGetLastError() != cudaSuccess) return STORM_B200_ECUDA;
+    DeviceFlags f;
+    if (cudaMemcpyAsync(&f, &scratch->flags, sizeof(f), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return STORM_B200_ECUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return STORM_B200_ECUDA;
+    if (f.error) return STORM_B200_ETIMEOUT;
+    if (sum) *sum = f.sum;
+    return 0;
+}
