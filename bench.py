@@ -202,6 +202,101 @@ def reference_sample(host_rows: np.ndarray, target_s: float, threads: int):
     return pairs / dt, pairs, dt, rows_needed
 
 
+# ------------------------------------------------- mixed-density forms
+def zipf_sets_gpu(n, universe, s, lo, hi, seed, device):
+    """Rows with cardinality P(k) ~ k^-s on [lo, hi], elements uniform without
+    replacement, sorted u32 (generated on the GPU, returned as numpy)."""
+    import torch
+    g = np.random.Generator(np.random.PCG64(seed))
+    ks = np.arange(lo, hi + 1, dtype=np.float64)
+    pk = ks ** (-s)
+    pk /= pk.sum()
+    cards = g.choice(ks.astype(np.int64), size=n, p=pk)
+    tg = torch.Generator(device=device)
+    tg.manual_seed(seed)
+    out = []
+    for k in cards:
+        perm = torch.randperm(universe, generator=tg, device=device)[: int(k)]
+        out.append(torch.sort(perm).values.to(torch.int64).cpu().numpy().astype(np.uint32))
+    return out
+
+
+def mixed_density_forms(sb, device, n=4096, universe=1 << 20, tile=64):
+    """Config-3-shaped corpus (Zipf(1.1) cardinalities, clipped like the full
+    configuration relative to the universe: [16, universe/4]) through the kernel
+    layer: plain per-tile GPU launches with the reference's cost model, the
+    batched persistent graph launch with the cost model, the batched launch
+    with the learned selector, and the reference's own CPU driver on a row
+    sample.  Counts of every GPU form are checked against each other."""
+    t_gen = time.perf_counter()
+    sets = zipf_sets_gpu(n, universe, 1.1, 16, universe // 4, 0xC0F3, device)
+    t_gen = time.perf_counter() - t_gen
+    r = sb.StormRows(universe)
+    for v in sets:
+        r.add(v)
+    r.upload()
+    pairs = n * (n - 1) // 2
+    out = {"workload": f"{n} rows over 2^{universe.bit_length() - 1}, card ~ Zipf(1.1) on [16, 2^"
+                       f"{(universe // 4).bit_length() - 1}], uniform w/o replacement; tile {tile}",
+           "pairs": pairs, "generate_s": round(t_gen, 2)}
+    t0 = time.perf_counter()
+    sel = r.train_selector(tile=tile, samples=1024, epochs=400, seed=7)
+    out["train_s"] = round(time.perf_counter() - t0, 2)
+    out["selector"] = {k: (round(v, 4) if isinstance(v, float) else v) for k, v in sel.items()}
+
+    def best_of(policy, exec_, reps=3):
+        times, s = [], None
+        for _ in range(reps):
+            s, st = r.allpairs_sum(policy, tile, exec_=exec_)
+            times.append(st["ns_total"])
+        return s, min(times), st
+
+    forms = {}
+    ref_sum = None
+    for name, pol, ex, dense in (("plain_per_tile_cost_model", sb.POLICY_PERTILE, sb.EXEC_PER_TILE, 0.0),
+                                 ("batched_cost_model", sb.POLICY_PERTILE, sb.EXEC_BATCHED, 0.0),
+                                 ("batched_learned", sb.POLICY_LEARNED, sb.EXEC_BATCHED, 0.0),
+                                 ("batched_learned_tensor_block", sb.POLICY_LEARNED, sb.EXEC_BATCHED, 1.0 / 64),
+                                 ("batched_all_bitmap", sb.POLICY_ALLBITMAP, sb.EXEC_BATCHED, 0.0)):
+        r.set_dense_block(dense)
+        s, ns, st = best_of(pol, ex)
+        if ref_sum is None:
+            ref_sum = s
+        if s != ref_sum:
+            raise RuntimeError(f"{name}: sum {s} != {ref_sum}")
+        forms[name] = {"pairs_per_s": pairs / (ns * 1e-9), "ms": ns * 1e-6, "launches": st["launches"],
+                       "cell_pairs": st["cell_pairs"]}
+    out["forms"] = forms
+    out["learned_over_plain"] = forms["batched_learned"]["pairs_per_s"] / forms["plain_per_tile_cost_model"]["pairs_per_s"]
+    out["learned_tensor_block_over_plain"] = (forms["batched_learned_tensor_block"]["pairs_per_s"] /
+                                              forms["plain_per_tile_cost_model"]["pairs_per_s"])
+    out["learned_over_batched_cost_model"] = (forms["batched_learned"]["pairs_per_s"] /
+                                              forms["batched_cost_model"]["pairs_per_s"])
+    # The reference's own kernel-layer driver (storm::allpairs_sum, PerTile, default model) on a sample.
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as ol
+    R = ol.reference()
+    if R is not None:
+        g = np.random.Generator(np.random.PCG64(11))
+        pick = np.sort(g.choice(n, size=min(n, 384), replace=False))
+        sub = [sets[i] for i in pick]
+        offs = np.zeros(len(sub) + 1, np.uint64)
+        for k, v in enumerate(sub):
+            offs[k + 1] = offs[k] + len(v)
+        vals = np.ascontiguousarray(np.concatenate(sub), dtype=np.uint32)
+        st = np.zeros(4, np.uint64)
+        t0 = time.perf_counter()
+        R.ref_allpairs_sum(vals.ctypes.data_as(ol.u32p), offs.ctypes.data_as(ol.u64p), len(sub), universe, 2, tile,
+                           st.ctypes.data_as(ol.u64p))
+        dt = time.perf_counter() - t0   # includes build_row of the sample (the reference times it too)
+        sp = len(sub) * (len(sub) - 1) // 2
+        out["cpu_reference_per_tile"] = {"pairs_per_s": sp / dt, "cores": 1,
+                                         "sample": f"{len(sub)} random rows ({sp} pairs), storm::allpairs_sum "
+                                                   f"PerTile incl. build_row, single thread as shipped"}
+    r.close()
+    return out
+
+
 # ------------------------------------------------------------------ arms
 def run_reference_arm(args):
     rank, world, local = dist_env()
@@ -374,6 +469,11 @@ def run_b200_arm(args):
         else:
             line["cpu_baseline"] = {"value": None, "unit": "pairs/s", "cores": 0, "kind": "reference",
                                     "sample": "oracle/_ref not built"}
+    if rank == 0 and args.forms:
+        try:
+            line["mixed_density"] = mixed_density_forms(sb, device)
+        except Exception as e:   # reported, never silently dropped
+            line["mixed_density"] = {"error": f"{type(e).__name__}: {e}"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -394,6 +494,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-forms", dest="forms", action="store_false",
+                    help="skip the mixed-density learned/plain/CPU comparison")
     ap.add_argument("--traffic", type=float, default=None,
                     help="dram bytes per launch of the dominant kernel from an ncu capture")
     args = ap.parse_args()

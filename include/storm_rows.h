@@ -88,6 +88,14 @@ uint64_t STORM_rows_size(const STORM_rows_t* r);
  * sparse_only rows (storm_repr.h:280-291): no B, no rank, no zone map. */
 int STORM_rows_set_bitmap_budget(STORM_rows_t* r, uint64_t bytes);
 int STORM_rows_upload(STORM_rows_t* r);
+/* Tensor-core dense block: under the density-ordered policies (per-tile,
+ * probe, oracle, refine, learned), the densest rows -- the suffix of the
+ * density order whose rows all have a bitmap and cardinality >=
+ * min_density * universe -- are compared with each other by the tcgen05
+ * bitmap kernel (north_star's tensor-core variant of dense B x B tiles),
+ * everything else by the cells.  Universes up to 2^23 bits; at least 256
+ * rows.  0 disables; the default is 1/64. */
+int STORM_rows_set_dense_block(STORM_rows_t* r, double min_density);
 /* RowMeta of one row (storm_repr.h:213-231) as 8 words: cardinality,
  * n_runs, n_words, n_nonzero_w, first_set, last_set, has_rank, has_occ;
  * plus a 9th word of representation flags (bit 0 bitmap, 1 complement). */

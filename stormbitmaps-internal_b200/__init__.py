@@ -380,6 +380,7 @@ _sig("STORM_rows_clear", C.c_int, [C.c_void_p])
 _sig("STORM_rows_size", C.c_uint64, [C.c_void_p])
 _sig("STORM_rows_set_bitmap_budget", C.c_int, [C.c_void_p, C.c_uint64])
 _sig("STORM_rows_upload", C.c_int, [C.c_void_p])
+_sig("STORM_rows_set_dense_block", C.c_int, [C.c_void_p, C.c_double])
 _sig("STORM_rows_meta", C.c_int, [C.c_void_p, C.c_uint64, u32p])
 _sig("STORM_rows_allpairs_sum", C.c_int, [C.c_void_p, C.c_int, C.c_uint32, C.c_int, C.c_int, C.POINTER(AllPairsStats)])
 _sig("STORM_rows_allpairs_matrix", C.c_int, [C.c_void_p, C.c_int, C.c_uint32, C.c_int, C.c_int, u32p, C.c_uint64,
@@ -458,6 +459,9 @@ class StormRows:
 
     def upload(self):
         _check(_lib.STORM_rows_upload(self.h), "STORM_rows_upload")
+
+    def set_dense_block(self, min_density: float):
+        _check(_lib.STORM_rows_set_dense_block(self.h, float(min_density)), "STORM_rows_set_dense_block")
 
     def meta(self, row: int) -> np.ndarray:
         m = np.zeros(9, dtype=np.uint32)

@@ -31,7 +31,12 @@ constexpr uint32_t TS_B_ATOM_BYTES = TS_BN * 128;          // one 128-byte K ato
 constexpr uint32_t TS_B_STAGE_BYTES = TS_B_ATOM_BYTES * (TS_KBITS / 128);
 constexpr uint32_t TS_TMEM_COLS = 512;
 constexpr uint32_t TS_A_COL0 = 256;
-constexpr uint32_t TS_SMEM_BYTES = TS_STAGES * TS_B_STAGE_BYTES + 1024 + 256;
+constexpr uint32_t TS_EPI_BYTES = 8 * 32 * 32 * 4;         // per epilogue warp: a 32 x 32 u32 block
+constexpr uint32_t TS_SMEM_BYTES = TS_STAGES * TS_B_STAGE_BYTES + 1024 + 256 + TS_EPI_BYTES;
+constexpr uint32_t TS_SMEM_BYTES_LEAN = TS_STAGES * TS_B_STAGE_BYTES + 1024 + 256;
+// Rows up to this many bits take the coalesced epilogue (the epilogue is a
+// larger share of a short tile); longer rows the lean launch.
+constexpr uint64_t TS_COALESCE_MAX_BITS = 1u << 17;
 
 struct TsCtl {
     uint64_t full[TS_STAGES];
@@ -67,15 +72,36 @@ __device__ __forceinline__ void expand_a64(uint64_t v, uint32_t* o) {
     }
 }
 
-__global__ void __launch_bounds__(TS_THREADS, 1)
-bb_mma_ts_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, const uint2* __restrict__ tiles,
-                 uint32_t n_tiles, uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags) {
+// Where count (i, j) of the local rows goes: the packed triangle of these
+// rows, or -- through row_map -- the packed triangle of n_out rows that these
+// rows are a subset of (local row r is row row_map[r] there).
+template <bool kRowMap>
+__device__ __forceinline__ uint64_t ts_out_index(uint64_t n, uint64_t i, uint64_t j, const uint32_t* row_map,
+                                                 uint64_t n_out) {
+    if (!kRowMap) return tri_index(n, i, i) - i + j;
+    const uint64_t a = row_map[i], b = row_map[j];
+    return a < b ? tri_index(n_out, a, b) : tri_index(n_out, b, a);
+}
+
+template <bool kRowMap>
+__device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad,
+                                        const uint2* __restrict__ tiles, uint32_t n_tiles,
+                                        uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags,
+                                        const uint32_t* __restrict__ row_map, uint64_t n_out) {
     extern __shared__ __align__(1024) unsigned char ts_smem[];
     const uint32_t raw_addr = smem_u32(ts_smem);
     const uint32_t pad = ((raw_addr + 1023u) & ~1023u) - raw_addr;
     uint8_t* ring = ts_smem + pad;
     const uint32_t ring_addr = raw_addr + pad;
     TsCtl* ctl = reinterpret_cast<TsCtl*>(ring + TS_STAGES * TS_B_STAGE_BYTES);
+    uint32_t* epi = reinterpret_cast<uint32_t*>(ring + TS_STAGES * TS_B_STAGE_BYTES + 256);
+    // The launch decides the epilogue: with TS_SMEM_BYTES of dynamic shared
+    // memory the counts are staged through smem and stored coalesced; with
+    // TS_SMEM_BYTES_LEAN (no staging buffer, more L1 left for the loads that
+    // feed long rows) each lane stores its own row.
+    uint32_t dyn_smem;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn_smem));
+    const bool coalesced = dyn_smem >= TS_SMEM_BYTES;
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
@@ -160,24 +186,54 @@ bb_mma_ts_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, con
             tc_fence_after();
             const uint32_t lane_grp = (uint32_t)(warp & 3) * 32u;
             const uint32_t col0 = (uint32_t)(warp >> 2) * 128u;
-            const uint64_t i = i0 + lane_grp + lane;
-            const bool row_ok = i < n;
-            const uint64_t base = row_ok ? tri_index(n, i, i) - i : 0;
             unsigned long long local = 0;
+            if (coalesced) {
+                // Each 32 x 32 block goes through this warp's smem buffer
+                // (16-byte chunks XOR-swizzled by row) so that one store
+                // instruction writes 32 consecutive counts of one row.
+                uint32_t* buf = epi + warp * 1024;
 #pragma unroll 1
-            for (uint32_t c = 0; c < 4; ++c) {
-                uint32_t r[32];
-                tmem_ld_32x32b_x32(tmem_base + (lane_grp << 16) + col0 + 32u * c, r);
-                tmem_ld_wait();
-                if (row_ok) {
-                    const uint64_t jb = j0 + col0 + 32u * c;
+                for (uint32_t c = 0; c < 4; ++c) {
+                    uint32_t r[32];
+                    tmem_ld_32x32b_x32(tmem_base + (lane_grp << 16) + col0 + 32u * c, r);
+                    tmem_ld_wait();
 #pragma unroll
-                    for (int e = 0; e < 32; ++e) {
-                        const uint64_t j = jb + e;
-                        const uint32_t cnt = r[e] >> 7;
-                        if (j >= i && j < n) {
-                            if (out) out[base + j] = cnt;
+                    for (uint32_t k = 0; k < 8; ++k)
+                        *reinterpret_cast<uint4*>(buf + lane * 32 + ((k ^ (lane & 7)) << 2)) =
+                            make_uint4(r[4 * k], r[4 * k + 1], r[4 * k + 2], r[4 * k + 3]);
+                    __syncwarp();
+                    const uint64_t j = j0 + col0 + 32u * c + lane;
+#pragma unroll 4
+                    for (uint32_t rr = 0; rr < 32; ++rr) {
+                        const uint64_t i = i0 + lane_grp + rr;
+                        const uint32_t cnt = buf[rr * 32 + ((((uint32_t)lane >> 2) ^ (rr & 7)) << 2) + (lane & 3)] >> 7;
+                        if (i < n && j >= i && j < n) {
+                            if (out) out[ts_out_index<kRowMap>(n, i, j, row_map, n_out)] = cnt;
                             if (j > i) local += cnt;
+                        }
+                    }
+                    __syncwarp();
+                }
+            } else {
+                // Lean form (no staging buffer): each lane writes its own row.
+                const uint64_t i = i0 + lane_grp + lane;
+                const bool row_ok = i < n;
+                const uint64_t base = row_ok ? tri_index(n, i, i) - i : 0;
+#pragma unroll 1
+                for (uint32_t c = 0; c < 4; ++c) {
+                    uint32_t r[32];
+                    tmem_ld_32x32b_x32(tmem_base + (lane_grp << 16) + col0 + 32u * c, r);
+                    tmem_ld_wait();
+                    if (row_ok) {
+                        const uint64_t jb = j0 + col0 + 32u * c;
+#pragma unroll
+                        for (int e = 0; e < 32; ++e) {
+                            const uint64_t j = jb + e;
+                            const uint32_t cnt = r[e] >> 7;
+                            if (j >= i && j < n) {
+                                if (out) out[kRowMap ? ts_out_index<true>(n, i, j, row_map, n_out) : base + j] = cnt;
+                                if (j > i) local += cnt;
+                            }
                         }
                     }
                 }
@@ -228,6 +284,21 @@ bb_mma_ts_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, con
         tc_fence_after();
         tmem_dealloc(tmem_base, TS_TMEM_COLS);
     }
+}
+
+__global__ void __launch_bounds__(TS_THREADS, 1)
+bb_mma_ts_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, const uint2* __restrict__ tiles,
+                 uint32_t n_tiles, uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags) {
+    ts_body<false>(X, n, w_pad, tiles, n_tiles, out, flags, nullptr, 0);
+}
+
+// Same kernel over a gathered subset of rows, writing into the triangle of
+// the full row set through row_map (the kernel layer's dense block).
+__global__ void __launch_bounds__(TS_THREADS, 1)
+bb_mma_ts_rows_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, const uint2* __restrict__ tiles,
+                      uint32_t n_tiles, uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags,
+                      const uint32_t* __restrict__ row_map, uint64_t n_out) {
+    ts_body<true>(X, n, w_pad, tiles, n_tiles, out, flags, row_map, n_out);
 }
 
 }  // namespace sb200

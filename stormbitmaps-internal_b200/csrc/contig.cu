@@ -29,11 +29,13 @@ struct STORM_contiguous_s {
     sb200::DevBuf<uint64_t> d_rows;
     sb200::DevBuf<uint32_t> d_out;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;   // device-to-host copies overlapping the next panel
     int kernel_pref = STORM_B200_KERNEL_AUTO;
     sb200::DenseEngine engine;
 
     ~STORM_contiguous_s() {
         if (stream) cudaStreamDestroy(stream);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
     }
 };
 
@@ -116,13 +118,11 @@ static uint64_t contig_matrix_host(STORM_contiguous_t* c, uint32_t* out, uint64_
     const uint64_t need = tri_size(n);
     if (out_len < need) fail(STORM_B200_ESIZE, "output buffer too small");
     c->d_out.reserve(need ? need : 1);
-    const uint64_t s = contig_run(c, c->d_out.p);
-    if (need) {
-        SB_CUDA(cudaMemcpyAsync(out, c->d_out.p, need * sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                                contig_stream(c)));
-        SB_CUDA(cudaStreamSynchronize(contig_stream(c)));
-    }
-    return s;
+    contig_flush(c);
+    if (!c->copy_stream) SB_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    // Panels of the triangle are copied back while the next panel computes.
+    return c->engine.run_to_host(c->d_rows.p, c->dev_rows, c->w_pad, c->vector_length, c->d_out.p, out,
+                                 c->kernel_pref, contig_stream(c), c->copy_stream);
 }
 
 }  // namespace sb200

@@ -23,34 +23,32 @@ static void build_tiles(std::vector<uint2>& t, uint64_t n, int kind) {
     }
 }
 
-uint64_t DenseEngine::run(const uint64_t* dX, uint64_t n, uint32_t w_pad, uint64_t row_bits,
-                          uint32_t* d_out, int kernel_pref, cudaStream_t st) {
-    const int sms = require_device();
-    if (n == 0) {
-        log.launches = 0;
-        log.last_ms = 0.f;
-        return 0;
-    }
+int DenseEngine::prepare(uint64_t n, uint64_t row_bits, int kernel_pref, cudaStream_t st) {
     if (n > 0xFFFFFFFFull) fail(STORM_B200_ELIMIT, "more than 2^32 rows");
     int kind = kernel_pref;
     if (kind == STORM_B200_KERNEL_AUTO) kind = row_bits <= MMA_MAX_BITS ? STORM_B200_KERNEL_MMA : STORM_B200_KERNEL_POPC;
     if ((kind == STORM_B200_KERNEL_MMA || kind == STORM_B200_KERNEL_MMA_SS) && row_bits > MMA_MAX_BITS)
         fail(STORM_B200_ELIMIT, "tensor-core kernel is exact only for rows of at most 2^23 bits");
-
     if (tiles_n != n || tiles_kind != kind) {
-        std::vector<uint2> t;
-        build_tiles(t, n, kind);
-        d_tiles.reserve(t.size());
-        SB_CUDA(cudaMemcpyAsync(d_tiles.p, t.data(), t.size() * sizeof(uint2), cudaMemcpyHostToDevice, st));
-        n_tiles = (uint32_t)t.size();
+        build_tiles(h_tiles, n, kind);
+        d_tiles.reserve(h_tiles.size());
+        SB_CUDA(cudaMemcpyAsync(d_tiles.p, h_tiles.data(), h_tiles.size() * sizeof(uint2), cudaMemcpyHostToDevice,
+                                st));
+        n_tiles = (uint32_t)h_tiles.size();
         tiles_n = n;
         tiles_kind = kind;
     }
     d_flags.reserve(1);
     SB_CUDA(cudaMemsetAsync(d_flags.p, 0, sizeof(DeviceFlags), st));
     log.ensure();
+    return kind;
+}
 
-    SB_CUDA(cudaEventRecord(log.ev0, st));
+// Tiles [t0, t0 + count) of the cached list.
+void DenseEngine::launch(int kind, const uint64_t* dX, uint32_t n, uint32_t w_pad, uint32_t t0, uint32_t count,
+                         uint32_t* d_out, cudaStream_t st) {
+    const int sms = require_device();
+    if (count == 0) return;
     if (kind == STORM_B200_KERNEL_MMA) {
         static bool attr_set = false;
         if (!attr_set) {
@@ -58,9 +56,9 @@ uint64_t DenseEngine::run(const uint64_t* dX, uint64_t n, uint32_t w_pad, uint64
                                          (int)TS_SMEM_BYTES));
             attr_set = true;
         }
-        const uint32_t grid = n_tiles < (uint32_t)sms ? n_tiles : (uint32_t)sms;
-        bb_mma_ts_kernel<<<grid, TS_THREADS, TS_SMEM_BYTES, st>>>(dX, (uint32_t)n, w_pad, d_tiles.p, n_tiles,
-                                                                   d_out, d_flags.p);
+        const uint32_t grid = count < (uint32_t)sms ? count : (uint32_t)sms;
+        const uint32_t smem = (uint64_t)w_pad * 64 <= TS_COALESCE_MAX_BITS ? TS_SMEM_BYTES : TS_SMEM_BYTES_LEAN;
+        bb_mma_ts_kernel<<<grid, TS_THREADS, smem, st>>>(dX, n, w_pad, d_tiles.p + t0, count, d_out, d_flags.p);
     } else if (kind == STORM_B200_KERNEL_MMA_SS) {
         static bool attr_set = false;
         if (!attr_set) {
@@ -68,9 +66,9 @@ uint64_t DenseEngine::run(const uint64_t* dX, uint64_t n, uint32_t w_pad, uint64
                                          (int)MMA_SMEM_BYTES));
             attr_set = true;
         }
-        const uint32_t grid = n_tiles < (uint32_t)sms ? n_tiles : (uint32_t)sms;
-        bb_mma_kernel<<<grid, MMA_THREADS, MMA_SMEM_BYTES, st>>>(dX, (uint32_t)n, w_pad, d_tiles.p, n_tiles,
-                                                                  d_out, d_flags.p);
+        const uint32_t grid = count < (uint32_t)sms ? count : (uint32_t)sms;
+        bb_mma_kernel<<<grid, MMA_THREADS, MMA_SMEM_BYTES, st>>>(dX, n, w_pad, d_tiles.p + t0, count, d_out,
+                                                                  d_flags.p);
     } else {
         const size_t smem = sizeof(PopcSmem);
         static bool attr_set = false;
@@ -79,11 +77,22 @@ uint64_t DenseEngine::run(const uint64_t* dX, uint64_t n, uint32_t w_pad, uint64
             attr_set = true;
         }
         const uint32_t cap = (uint32_t)sms * 2;
-        const uint32_t grid = n_tiles < cap ? n_tiles : cap;
-        bb_popc_kernel<<<grid, POPC_THREADS, smem, st>>>(dX, (uint32_t)n, w_pad, d_tiles.p, n_tiles, d_out,
-                                                          d_flags.p);
+        const uint32_t grid = count < cap ? count : cap;
+        bb_popc_kernel<<<grid, POPC_THREADS, smem, st>>>(dX, n, w_pad, d_tiles.p + t0, count, d_out, d_flags.p);
     }
     SB_CUDA(cudaGetLastError());
+}
+
+uint64_t DenseEngine::run(const uint64_t* dX, uint64_t n, uint32_t w_pad, uint64_t row_bits,
+                          uint32_t* d_out, int kernel_pref, cudaStream_t st) {
+    if (n == 0) {
+        log.launches = 0;
+        log.last_ms = 0.f;
+        return 0;
+    }
+    const int kind = prepare(n, row_bits, kernel_pref, st);
+    SB_CUDA(cudaEventRecord(log.ev0, st));
+    launch(kind, dX, (uint32_t)n, w_pad, 0, n_tiles, d_out, st);
     SB_CUDA(cudaEventRecord(log.ev1, st));
     DeviceFlags f;
     SB_CUDA(cudaMemcpyAsync(&f, d_flags.p, sizeof(f), cudaMemcpyDeviceToHost, st));
@@ -95,6 +104,56 @@ uint64_t DenseEngine::run(const uint64_t* dX, uint64_t n, uint32_t w_pad, uint64
     return f.sum;
 }
 
+uint64_t DenseEngine::run_to_host(const uint64_t* dX, uint64_t n, uint32_t w_pad, uint64_t row_bits,
+                                  uint32_t* d_out, uint32_t* host_out, int kernel_pref, cudaStream_t st,
+                                  cudaStream_t copy_st) {
+    if (n == 0) {
+        log.launches = 0;
+        log.last_ms = 0.f;
+        return 0;
+    }
+    const int kind = prepare(n, row_bits, kernel_pref, st);
+    // Row panels of ~1/12 of the tiles each (tiles are ordered by A block).
+    const uint32_t bm = (kind == STORM_B200_KERNEL_POPC) ? POPC_BM : MMA_BM;
+    const uint32_t want_panels = n_tiles >= 12 * 148 ? 12 : 1;
+    std::vector<uint32_t> cut{0};
+    for (uint32_t t = 1; t < n_tiles; ++t)
+        if (h_tiles[t].x != h_tiles[t - 1].x &&
+            (uint64_t)t * want_panels >= (uint64_t)n_tiles * cut.size())
+            cut.push_back(t);
+    cut.push_back(n_tiles);
+    while (panel_ev.size() < cut.size()) {
+        cudaEvent_t e;
+        SB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        panel_ev.push_back(e);
+    }
+    SB_CUDA(cudaEventRecord(log.ev0, st));
+    uint32_t launches = 0;
+    for (size_t p = 0; p + 1 < cut.size(); ++p) {
+        const uint32_t t0 = cut[p], t1 = cut[p + 1];
+        launch(kind, dX, (uint32_t)n, w_pad, t0, t1 - t0, d_out, st);
+        ++launches;
+        SB_CUDA(cudaEventRecord(panel_ev[p], st));
+        // rows of this panel: A blocks [first, last]
+        const uint64_t r0 = (uint64_t)h_tiles[t0].x * bm;
+        const uint64_t r1 = std::min<uint64_t>(n, ((uint64_t)h_tiles[t1 - 1].x + 1) * bm);
+        const uint64_t e0 = r0 * n - (r0 * (r0 - 1)) / 2;   // tri_index(n, r0, r0)
+        const uint64_t e1 = r1 * n - (r1 * (r1 - 1)) / 2;
+        SB_CUDA(cudaStreamWaitEvent(copy_st, panel_ev[p], 0));
+        SB_CUDA(cudaMemcpyAsync(host_out + e0, d_out + e0, (e1 - e0) * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                copy_st));
+    }
+    SB_CUDA(cudaEventRecord(log.ev1, st));
+    DeviceFlags f;
+    SB_CUDA(cudaMemcpyAsync(&f, d_flags.p, sizeof(f), cudaMemcpyDeviceToHost, st));
+    SB_CUDA(cudaStreamSynchronize(st));
+    SB_CUDA(cudaStreamSynchronize(copy_st));
+    SB_CUDA(cudaEventElapsedTime(&log.last_ms, log.ev0, log.ev1));
+    log.launches = launches;
+    log.kernel = kind;
+    if (f.error) fail(STORM_B200_ETIMEOUT, "bitmap x bitmap kernel: bounded wait expired");
+    return f.sum;
+}
 }  // namespace sb200
 
 // ===================================================================
@@ -192,3 +251,29 @@ extern "C" int STORM_contig_pairw_intersect_matrix_noalloc(const uint64_t* d_row
     if (sum) *sum = f.sum;
     return 0;
 }
+
+// ===================================================================
+// Kernel-layer dense block: the tensor-core kernel over a gathered subset of
+// rows, counts scattered into the full row set's triangle.
+// ===================================================================
+namespace sb200 {
+
+void build_mma_tiles(std::vector<uint2>& t, uint64_t n) { build_tiles(t, n, STORM_B200_KERNEL_MMA); }
+
+void launch_ts_rows(const uint64_t* X, uint32_t n, uint32_t w_pad, const uint2* tiles, uint32_t n_tiles,
+                    uint32_t* out, DeviceFlags* flags, const uint32_t* row_map, uint64_t n_out, cudaStream_t st) {
+    const int sms = require_device();
+    if (n_tiles == 0) return;
+    static bool attr_set = false;
+    if (!attr_set) {
+        SB_CUDA(cudaFuncSetAttribute(bb_mma_ts_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)TS_SMEM_BYTES));
+        attr_set = true;
+    }
+    const uint32_t grid = n_tiles < (uint32_t)sms ? n_tiles : (uint32_t)sms;
+    const uint32_t smem = (uint64_t)w_pad * 64 <= TS_COALESCE_MAX_BITS ? TS_SMEM_BYTES : TS_SMEM_BYTES_LEAN;
+    bb_mma_ts_rows_kernel<<<grid, TS_THREADS, smem, st>>>(X, n, w_pad, tiles, n_tiles, out, flags, row_map, n_out);
+    SB_CUDA(cudaGetLastError());
+}
+
+}  // namespace sb200

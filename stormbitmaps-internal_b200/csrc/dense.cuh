@@ -17,15 +17,40 @@ struct DenseEngine {
     DevBuf<DeviceFlags> d_flags;
     LaunchLog log;
 
-    ~DenseEngine() { log.destroy(); }
+    ~DenseEngine() {
+        log.destroy();
+        for (cudaEvent_t e : panel_ev) cudaEventDestroy(e);
+    }
 
     // Returns the sum over i < j; writes the packed upper triangle to d_out
     // when non-null.  `row_bits` is the logical row length (decides whether
     // the exact tensor-core kernel applies).  Synchronous.
     uint64_t run(const uint64_t* dX, uint64_t n, uint32_t w_pad, uint64_t row_bits, uint32_t* d_out,
                  int kernel_pref, cudaStream_t st);
+
+    // Same result, with the packed triangle also copied to host_out: the
+    // tiles run in row panels and each finished panel's rows are copied on
+    // copy_st while the next panel computes.
+    uint64_t run_to_host(const uint64_t* dX, uint64_t n, uint32_t w_pad, uint64_t row_bits, uint32_t* d_out,
+                         uint32_t* host_out, int kernel_pref, cudaStream_t st, cudaStream_t copy_st);
+
+   private:
+    int prepare(uint64_t n, uint64_t row_bits, int kernel_pref, cudaStream_t st);
+    void launch(int kind, const uint64_t* dX, uint32_t n, uint32_t w_pad, uint32_t t0, uint32_t count,
+                uint32_t* d_out, cudaStream_t st);
+    std::vector<uint2> h_tiles;
+    std::vector<cudaEvent_t> panel_ev;
 };
 
 inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
+
+// Tiles (bi, bj) of 128 x 256 pairs covering the triangle of n rows.
+void build_mma_tiles(std::vector<uint2>& t, uint64_t n);
+// Tensor-core kernel over n gathered rows X ([>= roundup(n, 256)][w_pad],
+// zero padded); count (i, j) lands at the packed index of
+// (row_map[i], row_map[j]) in a triangle of n_out rows; the sum over i < j
+// accumulates into flags->sum.  Asynchronous on st.
+void launch_ts_rows(const uint64_t* X, uint32_t n, uint32_t w_pad, const uint2* tiles, uint32_t n_tiles,
+                    uint32_t* out, DeviceFlags* flags, const uint32_t* row_map, uint64_t n_out, cudaStream_t st);
 
 }  // namespace sb200

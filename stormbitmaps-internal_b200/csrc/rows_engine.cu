@@ -22,6 +22,7 @@
 
 #include "../../include/storm_rows.h"
 #include "mlp.cuh"
+#include "dense.cuh"
 #include "rows_cells.cuh"
 
 namespace sb200 {
@@ -148,7 +149,27 @@ struct PairCtx {
     uint32_t n, T, nb;
     int policy;
     CostModelD model;
+    uint32_t dense_from = 0xFFFFFFFFu;   // sorted positions >= this form the tensor-core dense block
 };
+
+// Gather the bitmaps of the dense block (sorted positions [from, n)) into a
+// zero-padded [nd_pad][w_pad] matrix for the tensor-core kernel.
+__global__ void gather_dense_kernel(RowsView v, const uint32_t* __restrict__ order, uint32_t from, uint32_t nd,
+                                    uint32_t nd_pad, uint32_t w_pad, uint64_t* __restrict__ X,
+                                    uint32_t* __restrict__ row_map) {
+    const uint64_t total = (uint64_t)nd_pad * w_pad;
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < total;
+         e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t r = (uint32_t)(e / w_pad), w = (uint32_t)(e % w_pad);
+        uint64_t x = 0;
+        if (r < nd) {
+            const uint32_t row = order[from + r];
+            if (w < v.nw) x = v.bm[v.b_off[row] + w];
+            if (w == 0) row_map[r] = row;
+        }
+        X[e] = x;
+    }
+}
 
 // One pair in the traversal order -> (count, cell used).  Warp-cooperative.
 __device__ __forceinline__ uint32_t pair_count(const PairCtx& c, uint32_t oi, uint32_t oj, const TileDecision& td,
@@ -263,6 +284,7 @@ tiles_kernel(PairCtx c, const TileDecision* __restrict__ dec, uint32_t first_til
         for (uint32_t q = slice * TK_WARPS + warp; q < np; q += slices * TK_WARPS) {
             const uint32_t oi = i0 + q / nc, oj = j0 + q % nc;
             if (ti == tj && oj < oi) continue;
+            if (oi >= c.dense_from && oj >= c.dense_from) continue;   // the tensor-core block has it
             int used;
             uint32_t cnt = pair_count(c, oi, oj, td, lane, used);
             cnt = warp_sum_u32(cnt);
@@ -337,6 +359,14 @@ struct STORM_rows_s {
     DevBuf<RowMetaD> d_bmeta;
     DevBuf<TileDecision> d_dec;
     DevBuf<RowsStatsDev> d_stats;
+    // tensor-core dense block
+    double dense_min_density = 1.0 / 64.0;
+    DevBuf<uint64_t> d_dense;
+    DevBuf<uint32_t> d_dmap;
+    DevBuf<uint2> d_dtiles;
+    uint64_t dtiles_n = ~0ull;
+    uint32_t n_dtiles = 0;
+    DevBuf<DeviceFlags> d_dflags;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     // learned selector
     Mlp mlp;
@@ -447,14 +477,53 @@ static void rows_run(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell,
     c.nb = nb;
     c.policy = policy;
     c.model = default_cost_model();
+    // Dense block: the suffix of the density order whose rows all have a
+    // bitmap and density >= dense_min_density; its pairs run on the tensor
+    // cores (exact for universes up to 2^23 bits).
+    uint32_t D = n;
+    const bool sorted_pol = sorted_order_policy(policy);
+    if (sorted_pol && r->dense_min_density > 0.0 && r->universe <= (1u << 23)) {
+        const double min_card = r->dense_min_density * (double)r->universe;
+        while (D > 0 && r->pack.meta[order[D - 1]].has_bm && (double)r->pack.meta[order[D - 1]].card >= min_card) --D;
+        if (n - D < 256) D = n;
+    }
+    c.dense_from = D;
+    const uint32_t nd = n - D;
+    const uint32_t w_pad_d = (uint32_t)round_up(((uint64_t)r->universe + 63) / 64, 8);
+    const uint32_t nd_pad = (uint32_t)round_up(nd ? nd : 1, 256);
+    if (nd) {
+        r->d_dense.reserve((uint64_t)nd_pad * w_pad_d);
+        r->d_dmap.reserve(nd);
+        r->d_dflags.reserve(1);
+        if (r->dtiles_n != nd) {
+            std::vector<uint2> tl;
+            build_mma_tiles(tl, nd);
+            r->d_dtiles.reserve(tl.size());
+            SB_CUDA(cudaMemcpyAsync(r->d_dtiles.p, tl.data(), tl.size() * sizeof(uint2), cudaMemcpyHostToDevice, st));
+            SB_CUDA(cudaStreamSynchronize(st));
+            r->n_dtiles = (uint32_t)tl.size();
+            r->dtiles_n = nd;
+        }
+    }
     const bool learned = policy == STORM_POLICY_LEARNED && r->mlp.trained;
     if (learned) r->mlp.ensure_device(st);
 
     // slices per tile so the launch has enough CTAs
     const int sms = require_device();
-    uint32_t slices = 1;
-    while ((uint64_t)ntiles * slices < (uint64_t)sms * 8 && slices < 64) slices *= 2;
+    // Work items of at most 64 pairs: a tile of dense rows can cost thousands
+    // of times more than a tile of sparse ones, so the queue hands out slices
+    // of tiles, not whole tiles, and no CTA is left holding a heavy tile.
+    const uint32_t slices = std::max<uint32_t>(1u, (T * T + 63) / 64);
 
+    auto dense_phase = [&]() {
+        if (!nd) return;
+        SB_CUDA(cudaMemsetAsync(r->d_dflags.p, 0, sizeof(DeviceFlags), st));
+        const uint64_t total = (uint64_t)nd_pad * w_pad_d;
+        const uint32_t gg = (uint32_t)std::min<uint64_t>((total + 255) / 256, (uint64_t)sms * 32);
+        gather_dense_kernel<<<gg, 256, 0, st>>>(c.v, c.order, D, nd, nd_pad, w_pad_d, r->d_dense.p, r->d_dmap.p);
+        launch_ts_rows(r->d_dense.p, nd, w_pad_d, r->d_dtiles.p, r->n_dtiles, d_out, r->d_dflags.p, r->d_dmap.p, n,
+                       st);
+    };
     auto phases_1_2 = [&]() {
         SB_CUDA(cudaMemsetAsync(r->d_stats.p, 0, sizeof(RowsStatsDev), st));
         block_meta_kernel<<<(nb + 127) / 128, 128, 0, st>>>(c.v, c.order, n, T, r->d_bmeta.p, r->d_het.p);
@@ -480,6 +549,7 @@ static void rows_run(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell,
             SB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
             phases_1_2();
             const uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)ntiles * slices, (uint64_t)sms * 8);
+            dense_phase();
             tiles_kernel<<<grid, TK_THREADS, 0, st>>>(c, r->d_dec.p, 0, ntiles, slices, 1, nullptr, d_out,
                                                       r->d_stats.p);
             SB_CUDA(cudaStreamEndCapture(st, &g));
@@ -492,19 +562,30 @@ static void rows_run(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell,
     } else {
         phases_1_2();
         SB_CUDA(cudaEventRecord(r->ev[1], st));
+        dense_phase();
+        // One launch per tile, spread over the whole GPU (one warp per pair).
+        const uint32_t tile_slices =
+            (uint32_t)std::min<uint64_t>(((uint64_t)T * T + TK_WARPS - 1) / TK_WARPS, (uint64_t)sms * 8);
         for (uint32_t t = 0; t < ntiles; ++t) {
-            tiles_kernel<<<slices, TK_THREADS, 0, st>>>(c, r->d_dec.p, t, 1, slices, 0, nullptr, d_out, r->d_stats.p);
+            tiles_kernel<<<tile_slices, TK_THREADS, 0, st>>>(c, r->d_dec.p, t, 1, tile_slices, 0, nullptr, d_out,
+                                                             r->d_stats.p);
         }
         launches = 2 + (policy == STORM_POLICY_PROBE ? 1 : 0) + ntiles;
     }
     SB_CUDA(cudaGetLastError());
     SB_CUDA(cudaEventRecord(r->ev[2], st));
+    DeviceFlags dflags{};
+    if (nd) SB_CUDA(cudaMemcpyAsync(&dflags, r->d_dflags.p, sizeof(dflags), cudaMemcpyDeviceToHost, st));
     RowsStatsDev hs;
     SB_CUDA(cudaMemcpyAsync(&hs, r->d_stats.p, sizeof(hs), cudaMemcpyDeviceToHost, st));
     SB_CUDA(cudaStreamSynchronize(st));
     float total_ms = 0.f, sel_ms = 0.f;
     SB_CUDA(cudaEventElapsedTime(&total_ms, r->ev[0], r->ev[2]));
     if (exec != STORM_EXEC_BATCHED) SB_CUDA(cudaEventElapsedTime(&sel_ms, r->ev[0], r->ev[1]));
+    if (dflags.error) fail(STORM_B200_ETIMEOUT, "dense-block tensor kernel: bounded wait expired");
+    hs.sum += dflags.sum;
+    hs.pairs += (uint64_t)nd * (nd ? nd - 1 : 0) / 2;
+    hs.cell_pairs[P_BB] += (uint64_t)nd * (nd ? nd - 1 : 0) / 2;
     S.sum = hs.sum;
     S.pairs = hs.pairs;
     S.skipped = hs.skipped;
@@ -562,6 +643,17 @@ int STORM_rows_set_bitmap_budget(STORM_rows_t* r, uint64_t bytes) {
     if (r == NULL) return STORM_B200_ENULL;
     r->bitmap_budget = bytes;
     r->dirty = true;
+    return 0;
+}
+
+int STORM_rows_set_dense_block(STORM_rows_t* r, double min_density) {
+    if (r == NULL) return STORM_B200_ENULL;
+    if (!(min_density >= 0.0)) return STORM_B200_EARG;
+    r->dense_min_density = min_density;
+    if (r->graph) {
+        cudaGraphExecDestroy(r->graph);
+        r->graph = nullptr;
+    }
     return 0;
 }
 

@@ -42,6 +42,7 @@ def test_golden_contig_cases(sb, golden, kernel):
 @pytest.mark.parametrize("n,m,p", [
     (1, 64, 0.5), (2, 65, 0.5), (3, 640, 0.9), (127, 1000, 0.3), (128, 4096, 0.5), (129, 4097, 0.2),
     (255, 512, 0.5), (256, 128, 0.7), (257, 8192, 0.01), (300, 2048 + 64, 0.5), (513, 256, (0.0, 1.0)),
+    (300, (1 << 17) + 64, 0.3),   # long rows: the tensor kernel's lean (unstaged) epilogue
 ])
 def test_edge_shapes_match_oracle(sb, kernel, n, m, p):
     words = gen.bernoulli_rows(n, m, p, seed=1000 + n + m)

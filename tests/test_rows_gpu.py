@@ -127,6 +127,30 @@ def test_config_shaped_corpora_all_policies(sb, case):
             np.testing.assert_array_equal(mat, want, err_msg=f"{case}/{pol}/{ex}")
 
 
+@pytest.mark.parametrize("universe", [4096 + 64, 1 << 17])
+def test_tensor_core_dense_block(sb, universe):
+    """The densest rows of the density order are compared by the tcgen05
+    kernel and scattered back through the row map; counts stay exact for
+    every policy and both execution forms, with and without the block."""
+    g = gen.rng(universe)
+    sets = [gen.uniform_set(g, int(universe * g.uniform(0.05, 0.5)), universe) for _ in range(300)]
+    sets += gen.bernoulli_sets(200, universe, 0.002, 71)
+    order = g.permutation(len(sets))
+    sets = [sets[k] for k in order]
+    r = rows_of(sb, sets, universe)
+    vals, offs = gen.to_csr(sets)
+    want, ws = ol.sets_matrix(vals, offs)
+    for thr in (1.0 / 64, 0.0):
+        r.set_dense_block(thr)
+        for pol in ("PERTILE", "LEARNED", "REFINE", "PROBE"):
+            for ex in (sb.EXEC_BATCHED, sb.EXEC_PER_TILE):
+                mat, st = r.allpairs_matrix(getattr(sb, "POLICY_" + pol), 64, exec_=ex)
+                np.testing.assert_array_equal(mat, want, err_msg=f"{pol}/{ex}/{thr}")
+                assert st["sum"] == ws and st["pairs"] == len(sets) * (len(sets) - 1) // 2
+                if thr > 0:
+                    assert st["cell_pairs"].get("BB", 0) >= 300 * 299 // 2
+
+
 def test_rows_without_bitmaps_stay_exact(sb):
     """A bitmap budget too small for every row leaves the sparse rows without
     B (the reference's sparse_only rows): B cells are skipped for them and
