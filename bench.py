@@ -71,6 +71,42 @@ def pairs_of(n):
     return n * (n + 1) // 2
 
 
+def haplotype_rows_gpu(n_sites, n_hap, block, seed, device, chunk=4096):
+    """Haplotype-like matrix: per site an allele count k with P(k) ~ 1/k on
+    [1, n_hap - 1]; carriers are whole contiguous blocks of `block`
+    haplotypes, ceil(k / block) distinct blocks at random, the last selected
+    block (in haplotype order) filled only up to k carriers.  Returns
+    [n_sites, ceil(n_hap/64)] int64 on the device."""
+    import torch
+    g = np.random.Generator(np.random.PCG64(seed))
+    ks = np.arange(1, n_hap, dtype=np.float64)
+    pk = 1.0 / ks
+    pk /= pk.sum()
+    kk = g.choice(ks.astype(np.int64), size=n_sites, p=pk)
+    n_blocks = (n_hap + block - 1) // block
+    w = (n_hap + 63) // 64
+    tg = torch.Generator(device=device)
+    tg.manual_seed(seed)
+    out = torch.empty((n_sites, w), dtype=torch.int64, device=device)
+    shifts = torch.arange(64, device=device, dtype=torch.int64)
+    hap = torch.arange(w * 64, device=device)
+    blk_of = (hap // block).clamp(max=n_blocks - 1)
+    off_in = hap % block
+    for r0 in range(0, n_sites, chunk):
+        r1 = min(n_sites, r0 + chunk)
+        k = torch.from_numpy(kk[r0:r1]).to(device)
+        nb = torch.clamp((k + block - 1) // block, max=n_blocks)
+        keys = torch.rand((r1 - r0, n_blocks), generator=tg, device=device)
+        rank = keys.argsort(dim=1).argsort(dim=1)               # random rank of each block
+        sel = rank < nb[:, None]
+        ordinal = torch.cumsum(sel.to(torch.int32), dim=1)      # 1-based order among selected blocks
+        last_fill = (k - block * (nb - 1))[:, None]              # carriers in the last selected block
+        bits = sel[:, blk_of] & ((ordinal[:, blk_of] < nb[:, None]) | (off_in[None, :] < last_fill))
+        bits &= hap[None, :] < n_hap
+        out[r0:r1] = (bits.view(r1 - r0, w, 64).to(torch.int64) << shifts).sum(dim=-1)
+    return out
+
+
 # ----------------------------------------------------------------- clocks
 class ClockSampler:
     """nvidia-smi samples during the timed region (200 ms period)."""
@@ -256,7 +292,8 @@ def mixed_density_forms(sb, device, n=4096, universe=1 << 20, tile=64):
     for name, pol, ex, dense in (("plain_per_tile_cost_model", sb.POLICY_PERTILE, sb.EXEC_PER_TILE, 0.0),
                                  ("batched_cost_model", sb.POLICY_PERTILE, sb.EXEC_BATCHED, 0.0),
                                  ("batched_learned", sb.POLICY_LEARNED, sb.EXEC_BATCHED, 0.0),
-                                 ("batched_learned_tensor_block", sb.POLICY_LEARNED, sb.EXEC_BATCHED, 1.0 / 64),
+                                 ("batched_learned_tensor_block", sb.POLICY_LEARNED, sb.EXEC_BATCHED,
+                                  DENSE_BLOCK_DEFAULT),
                                  ("batched_all_bitmap", sb.POLICY_ALLBITMAP, sb.EXEC_BATCHED, 0.0)):
         r.set_dense_block(dense)
         s, ns, st = best_of(pol, ex)
@@ -294,6 +331,95 @@ def mixed_density_forms(sb, device, n=4096, universe=1 << 20, tile=64):
                                          "sample": f"{len(sub)} random rows ({sp} pairs), storm::allpairs_sum "
                                                    f"PerTile incl. build_row, single thread as shipped"}
     r.close()
+    return out
+
+
+def run_sets_gpu(n, universe, mean_runs, mean_len, seed, device):
+    """Run-clustered rows: Poisson(mean_runs) runs per row, start uniform,
+    length Geometric(mean mean_len); the row is the union (sorted u32)."""
+    import torch
+    g = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for _ in range(n):
+        k = int(g.poisson(mean_runs))
+        if k == 0:
+            out.append(np.zeros(0, np.uint32))
+            continue
+        starts = torch.from_numpy(g.integers(0, universe, size=k)).to(device)
+        lens = torch.from_numpy(g.geometric(1.0 / mean_len, size=k)).to(device)
+        pos = torch.repeat_interleave(starts, lens) + (torch.arange(int(lens.sum().item()), device=device) -
+                                                       torch.repeat_interleave(torch.cumsum(lens, 0) - lens, lens))
+        pos = torch.unique(pos[pos < universe])
+        out.append(pos.to(torch.int64).cpu().numpy().astype(np.uint32))
+    return out
+
+
+def bernoulli_sets_gpu(n, universe, density, seed, device):
+    import torch
+    g = np.random.Generator(np.random.PCG64(seed))
+    tg = torch.Generator(device=device)
+    tg.manual_seed(seed)
+    out = []
+    for k in g.binomial(universe, density, size=n):
+        perm = torch.randperm(universe, generator=tg, device=device)[: int(k)]
+        out.append(torch.sort(perm).values.to(torch.int64).cpu().numpy().astype(np.uint32))
+    return out
+
+
+# The library's default tensor-core dense-block threshold (rows whose sparse
+# form is at least 2^-14 of the universe).
+DENSE_BLOCK_DEFAULT = 1.0 / 16384
+
+
+def forms_on(sb, sets, universe, tile=64, samples=1024, with_plain=True):
+    """Learned selector trained on this corpus (held-out regret), then the
+    batched learned form against the batched and per-tile cost-model forms."""
+    r = sb.StormRows(universe)
+    for v in sets:
+        r.add(v)
+    r.upload()
+    n = len(sets)
+    pairs = n * (n - 1) // 2
+    sel = r.train_selector(tile=tile, samples=samples, epochs=400, seed=7)
+    res = {"rows": n, "pairs": pairs,
+           "regret_learned": round(sel["regret_mlp"], 4), "regret_cost_model": round(sel["regret_cost_model"], 4),
+           "train_accuracy": round(sel["train_accuracy"], 3)}
+    sums = set()
+    dflt = DENSE_BLOCK_DEFAULT
+    for name, pol, ex, dense in (("batched_learned", sb.POLICY_LEARNED, sb.EXEC_BATCHED, dflt),
+                                 ("batched_learned_no_tensor_block", sb.POLICY_LEARNED, sb.EXEC_BATCHED, 0.0),
+                                 ("batched_cost_model", sb.POLICY_PERTILE, sb.EXEC_BATCHED, dflt)) + (
+            (("plain_per_tile_cost_model", sb.POLICY_PERTILE, sb.EXEC_PER_TILE, 0.0),) if with_plain else ()):
+        r.set_dense_block(dense)
+        best = None
+        for _ in range(2):
+            s, st = r.allpairs_sum(pol, tile, exec_=ex)
+            best = st["ns_total"] if best is None else min(best, st["ns_total"])
+            sums.add(s)
+        res[name + "_pairs_per_s"] = pairs / (best * 1e-9)
+    if len(sums) != 1:
+        raise RuntimeError(f"forms disagree: {sums}")
+    r.close()
+    return res
+
+
+def config45_forms(device):
+    """Config-4-shaped run-clustered rows and the config-5b density sweep
+    (reduced N), each with the learned selector's held-out regret against
+    the measured-best cell, beside the cost model's."""
+    import importlib
+    sb = importlib.import_module("stormbitmaps-internal_b200")
+    out = {}
+    t0 = time.perf_counter()
+    sets = run_sets_gpu(2048, 1 << 26, 200, 256, 0xC0F4, device)
+    out["runs_2^26"] = forms_on(sb, sets, 1 << 26)
+    out["runs_2^26"]["workload"] = "2048 rows over 2^26, Poisson(200) runs of Geometric(mean 256) length"
+    sweep = {}
+    for d, n in ((1e-6, 4096), (1e-5, 4096), (1e-4, 2048), (1e-3, 1024), (1e-2, 512), (0.17, 256)):
+        sets = bernoulli_sets_gpu(n, 1 << 24, d, int(1e7 * d) + 5, device)
+        sweep[f"{d:g}"] = forms_on(sb, sets, 1 << 24, samples=512, with_plain=False)
+    out["density_sweep_2^24"] = sweep
+    out["seconds"] = round(time.perf_counter() - t0, 1)
     return out
 
 
@@ -474,6 +600,10 @@ def run_b200_arm(args):
             line["mixed_density"] = mixed_density_forms(sb, device)
         except Exception as e:   # reported, never silently dropped
             line["mixed_density"] = {"error": f"{type(e).__name__}: {e}"}
+        try:
+            line["configs_4_5"] = config45_forms(device)
+        except Exception as e:
+            line["configs_4_5"] = {"error": f"{type(e).__name__}: {e}"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

@@ -90,11 +90,15 @@ int STORM_rows_set_bitmap_budget(STORM_rows_t* r, uint64_t bytes);
 int STORM_rows_upload(STORM_rows_t* r);
 /* Tensor-core dense block: under the density-ordered policies (per-tile,
  * probe, oracle, refine, learned), the densest rows -- the suffix of the
- * density order whose rows all have a bitmap and cardinality >=
- * min_density * universe -- are compared with each other by the tcgen05
- * bitmap kernel (north_star's tensor-core variant of dense B x B tiles),
- * everything else by the cells.  Universes up to 2^23 bits; at least 256
- * rows.  0 disables; the default is 1/64. */
+ * density order whose rows all have a bitmap and whose smallest sparse form
+ * min(cardinality, 2 x runs) is >= min_density * universe --
+ * are compared with each other by the tcgen05 bitmap kernel (the
+ * tensor-core form of dense B x B tiles), everything else by the cells.
+ * The tensor cores pay per pair in proportion to the universe, the cells in
+ * proportion to the sparse sizes, so a row joins only when its sparse form
+ * is a large enough share of the universe: run-clustered rows with few runs
+ * stay on the run cells.  Universes up to 2^27 bits; at least 256 rows.
+ * 0 disables; the default is 2^-14. */
 int STORM_rows_set_dense_block(STORM_rows_t* r, double min_density);
 /* RowMeta of one row (storm_repr.h:213-231) as 8 words: cardinality,
  * n_runs, n_words, n_nonzero_w, first_set, last_set, has_rank, has_occ;

@@ -43,7 +43,8 @@ constexpr uint32_t MMA_STAGE_BYTES = MMA_A_BYTES + MMA_B_BYTES;
 constexpr uint32_t MMA_TMEM_COLS = 256;
 constexpr uint32_t MMA_SMEM_BYTES = MMA_STAGES * MMA_STAGE_BYTES + 1024 /*align slack*/ + 256;
 constexpr uint64_t WAIT_LIMIT_NS = 2000000000ull;        // 2 s per wait
-constexpr uint32_t MMA_MAX_BITS = 1u << 23;
+constexpr uint32_t MMA_MAX_BITS = 1u << 23;        // 8-byte weight cycle (D = 128 x count)
+constexpr uint32_t MMA_MAX_BITS_W4 = 1u << 27;     // 4-byte weight cycle (D = 8 x count)
 
 // Error sites (flags->error = site).
 enum : uint32_t {
@@ -77,7 +78,9 @@ __device__ __forceinline__ bool mma_wait(uint32_t bar, uint32_t parity, MmaCtl* 
 }
 
 // Expand 64 packed bits (one task) into 4 swizzled 16-byte chunks.
-template <bool kIsB>
+// kW4: weights cycle over 4 bytes instead of 8 (A 2^(k mod 4), B 2^(3 - k mod 4),
+// every product 0 or 8), exact for rows up to 2^27 bits instead of 2^23.
+template <bool kIsB, bool kW4 = false>
 __device__ __forceinline__ void expand_store(uint8_t* op_base, uint32_t r, uint32_t half, uint64_t v) {
     uint8_t* row = op_base + (r >> 3) * 1024u + (r & 7u) * 128u;
     const uint32_t lo = (uint32_t)v, hi = (uint32_t)(v >> 32);
@@ -91,17 +94,17 @@ __device__ __forceinline__ void expand_store(uint8_t* op_base, uint32_t r, uint3
             const uint32_t r0 = __byte_perm(src0, 0, (b0 & 3) * 0x1111u);
             const uint32_t r1 = __byte_perm(src1, 0, (b1 & 3) * 0x1111u);
             o.x = r0 & 0x08040201u;
-            o.y = r0 & 0x80402010u;
+            o.y = kW4 ? (r0 >> 4) & 0x08040201u : r0 & 0x80402010u;
             o.z = r1 & 0x08040201u;
-            o.w = r1 & 0x80402010u;
+            o.w = kW4 ? (r1 >> 4) & 0x08040201u : r1 & 0x80402010u;
         } else {
             // Byte b of a 32-bit word, bit-reversed, is byte (3 - b) of __brev(word).
             const uint32_t src0 = b0 < 4 ? rl : rh, src1 = b1 < 4 ? rl : rh;
             const uint32_t r0 = __byte_perm(src0, 0, (3u - (b0 & 3)) * 0x1111u);
             const uint32_t r1 = __byte_perm(src1, 0, (3u - (b1 & 3)) * 0x1111u);
-            o.x = r0 & 0x10204080u;
+            o.x = kW4 ? (r0 >> 4) & 0x01020408u : r0 & 0x10204080u;
             o.y = r0 & 0x01020408u;
-            o.z = r1 & 0x10204080u;
+            o.z = kW4 ? (r1 >> 4) & 0x01020408u : r1 & 0x10204080u;
             o.w = r1 & 0x01020408u;
         }
         const uint32_t chunk = half * 4 + q;

@@ -61,14 +61,16 @@ __device__ __forceinline__ bool ts_wait(uint32_t bar, uint32_t parity, TsCtl* ct
     }
 }
 
-// 64 packed bits -> 16 u32 of A-weighted bytes (byte k carries bit k at 2^(k mod 8)).
+// 64 packed bits -> 16 u32 of A-weighted bytes (byte k carries bit k at
+// 2^(k mod 8), or 2^(k mod 4) with kW4).
+template <bool kW4>
 __device__ __forceinline__ void expand_a64(uint64_t v, uint32_t* o) {
     const uint32_t lo = (uint32_t)v, hi = (uint32_t)(v >> 32);
 #pragma unroll
     for (uint32_t b = 0; b < 8; ++b) {
         const uint32_t r = __byte_perm(b < 4 ? lo : hi, 0, (b & 3) * 0x1111u);
         o[2 * b] = r & 0x08040201u;
-        o[2 * b + 1] = r & 0x80402010u;
+        o[2 * b + 1] = kW4 ? (r >> 4) & 0x08040201u : r & 0x80402010u;
     }
 }
 
@@ -83,11 +85,11 @@ __device__ __forceinline__ uint64_t ts_out_index(uint64_t n, uint64_t i, uint64_
     return a < b ? tri_index(n_out, a, b) : tri_index(n_out, b, a);
 }
 
-template <bool kRowMap>
+template <bool kRowMap, bool kW4>
 __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad,
                                         const uint2* __restrict__ tiles, uint32_t n_tiles,
                                         uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags,
-                                        const uint32_t* __restrict__ row_map, uint64_t n_out) {
+                                        const uint32_t* __restrict__ row_map, uint64_t n_out, uint32_t k_splits) {
     extern __shared__ __align__(1024) unsigned char ts_smem[];
     const uint32_t raw_addr = smem_u32(ts_smem);
     const uint32_t pad = ((raw_addr + 1023u) & ~1023u) - raw_addr;
@@ -132,17 +134,21 @@ __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t
         const uint32_t prow = is_a ? (uint32_t)tid : (uint32_t)(tid - TS_A_THREADS);   // operand row
         uint32_t g = 0, tcount = 0;
         bool ok = true;
-        for (uint32_t t = blockIdx.x; t < n_tiles && ok; t += gridDim.x, ++tcount) {
+        for (uint32_t it = blockIdx.x; it < n_tiles * k_splits && ok; it += gridDim.x, ++tcount) {
+            // work item = (tile, K slice); the host keeps k_splits <= nk
+            const uint32_t t = it / k_splits, ks = it % k_splits;
+            const uint32_t kb0 = (uint32_t)((uint64_t)nk * ks / k_splits);
+            const uint32_t kb1 = (uint32_t)((uint64_t)nk * (ks + 1) / k_splits);
             const uint64_t i0 = (uint64_t)tiles[t].x * TS_BM;
             const uint64_t j0 = (uint64_t)tiles[t].y * TS_BN;
             const uint64_t* src = X + (is_a ? i0 + prow : j0 + prow) * (uint64_t)w_pad;
-            uint4 v0 = __ldg(reinterpret_cast<const uint4*>(src));
-            uint4 v1 = __ldg(reinterpret_cast<const uint4*>(src) + 1);
-            for (uint32_t kb = 0; kb < nk; ++kb, ++g) {
+            uint4 v0 = __ldg(reinterpret_cast<const uint4*>(src + 4 * kb0));
+            uint4 v1 = __ldg(reinterpret_cast<const uint4*>(src + 4 * kb0) + 1);
+            for (uint32_t kb = kb0; kb < kb1; ++kb, ++g) {
                 const uint32_t s = g % TS_STAGES;
                 const uint32_t round = g / TS_STAGES;
                 uint4 n0 = make_uint4(0, 0, 0, 0), n1 = n0;
-                if (kb + 1 < nk) {
+                if (kb + 1 < kb1) {
                     n0 = __ldg(reinterpret_cast<const uint4*>(src + 4 * (kb + 1)));
                     n1 = __ldg(reinterpret_cast<const uint4*>(src + 4 * (kb + 1)) + 1);
                 }
@@ -158,8 +164,8 @@ __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
                         uint32_t r[32];
-                        expand_a64(w[2 * h], r);
-                        expand_a64(w[2 * h + 1], r + 16);
+                        expand_a64<kW4>(w[2 * h], r);
+                        expand_a64<kW4>(w[2 * h + 1], r + 16);
                         tmem_st_32x32b_x32(taddr + 32u * h, r);
                     }
                     tmem_st_wait();
@@ -169,7 +175,8 @@ __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         // word q covers K bytes [64q, 64q + 64): atom q/2, chunks 4(q%2)..
-                        expand_store<true>(b_stage + (q >> 1) * TS_B_ATOM_BYTES, prow, (uint32_t)(q & 1), w[q]);
+                        expand_store<true, kW4>(b_stage + (q >> 1) * TS_B_ATOM_BYTES, prow, (uint32_t)(q & 1),
+                                                w[q]);
                     }
                     fence_proxy_async_smem();
                 }
@@ -206,9 +213,14 @@ __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t
 #pragma unroll 4
                     for (uint32_t rr = 0; rr < 32; ++rr) {
                         const uint64_t i = i0 + lane_grp + rr;
-                        const uint32_t cnt = buf[rr * 32 + ((((uint32_t)lane >> 2) ^ (rr & 7)) << 2) + (lane & 3)] >> 7;
+                        const uint32_t cnt =
+                            buf[rr * 32 + ((((uint32_t)lane >> 2) ^ (rr & 7)) << 2) + (lane & 3)] >> (kW4 ? 3 : 7);
                         if (i < n && j >= i && j < n) {
-                            if (out) out[ts_out_index<kRowMap>(n, i, j, row_map, n_out)] = cnt;
+                            if (out) {
+                                uint32_t* dst = out + ts_out_index<kRowMap>(n, i, j, row_map, n_out);
+                                if (k_splits > 1) atomicAdd(dst, cnt);   // partial count of one K slice
+                                else *dst = cnt;
+                            }
                             if (j > i) local += cnt;
                         }
                     }
@@ -229,9 +241,14 @@ __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t
 #pragma unroll
                         for (int e = 0; e < 32; ++e) {
                             const uint64_t j = jb + e;
-                            const uint32_t cnt = r[e] >> 7;
+                            const uint32_t cnt = r[e] >> (kW4 ? 3 : 7);
                             if (j >= i && j < n) {
-                                if (out) out[kRowMap ? ts_out_index<true>(n, i, j, row_map, n_out) : base + j] = cnt;
+                                if (out) {
+                                    uint32_t* dst = out + (kRowMap ? ts_out_index<true>(n, i, j, row_map, n_out)
+                                                                   : base + j);
+                                    if (k_splits > 1) atomicAdd(dst, cnt);
+                                    else *dst = cnt;
+                                }
                                 if (j > i) local += cnt;
                             }
                         }
@@ -247,11 +264,14 @@ __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t
         const uint32_t idesc = umma_idesc_u8_s32(TS_BM, TS_BN);
         uint32_t g = 0, tcount = 0;
         bool issued = false;
-        for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x, ++tcount) {
+        for (uint32_t it = blockIdx.x; it < n_tiles * k_splits; it += gridDim.x, ++tcount) {
+            const uint32_t ks = it % k_splits;
+            const uint32_t kb0 = (uint32_t)((uint64_t)nk * ks / k_splits);
+            const uint32_t kb1 = (uint32_t)((uint64_t)nk * (ks + 1) / k_splits);
             if (!ts_wait(smem_u32(&ctl->acc_empty), (tcount & 1) ^ 1, ctl, flags, ERR_MMA_ACCEMPTY)) break;
             tc_fence_after();
             bool ok = true;
-            for (uint32_t kb = 0; kb < nk; ++kb, ++g) {
+            for (uint32_t kb = kb0; kb < kb1; ++kb, ++g) {
                 const uint32_t s = g % TS_STAGES;
                 if (!ts_wait(smem_u32(&ctl->full[s]), (g / TS_STAGES) & 1, ctl, flags, ERR_MMA_FULL)) {
                     ok = false;
@@ -264,7 +284,7 @@ __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t
                 for (uint32_t kk = 0; kk < TS_KBITS / 32; ++kk) {
                     const uint32_t boff = (kk >> 2) * TS_B_ATOM_BYTES + (kk & 3) * 32u;
                     mma_u8_ts(tmem_base, a_col + 8u * kk, umma_desc_sw128(b_addr + boff, 1024), idesc,
-                              (kb | kk) != 0);
+                              (kb != kb0 || kk != 0) ? 1u : 0u);
                 }
                 issued = true;
                 tc_commit(smem_u32(&ctl->empty[s]));
@@ -286,10 +306,21 @@ __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t
     }
 }
 
+// k_splits > 1 divides each tile's K range into that many work items whose
+// partial counts are added into out with atomics (out zeroed beforehand):
+// used when there are fewer tiles than SMs.
 __global__ void __launch_bounds__(TS_THREADS, 1)
 bb_mma_ts_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, const uint2* __restrict__ tiles,
-                 uint32_t n_tiles, uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags) {
-    ts_body<false>(X, n, w_pad, tiles, n_tiles, out, flags, nullptr, 0);
+                 uint32_t n_tiles, uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags, uint32_t k_splits) {
+    ts_body<false, false>(X, n, w_pad, tiles, n_tiles, out, flags, nullptr, 0, k_splits);
+}
+
+// Rows of 2^23 .. 2^27 bits: the 4-byte weight cycle keeps D = 8 x count < 2^31.
+__global__ void __launch_bounds__(TS_THREADS, 1)
+bb_mma_ts_long_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, const uint2* __restrict__ tiles,
+                      uint32_t n_tiles, uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags,
+                      uint32_t k_splits) {
+    ts_body<false, true>(X, n, w_pad, tiles, n_tiles, out, flags, nullptr, 0, k_splits);
 }
 
 // Same kernel over a gathered subset of rows, writing into the triangle of
@@ -297,8 +328,16 @@ bb_mma_ts_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, con
 __global__ void __launch_bounds__(TS_THREADS, 1)
 bb_mma_ts_rows_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, const uint2* __restrict__ tiles,
                       uint32_t n_tiles, uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags,
-                      const uint32_t* __restrict__ row_map, uint64_t n_out) {
-    ts_body<true>(X, n, w_pad, tiles, n_tiles, out, flags, row_map, n_out);
+                      const uint32_t* __restrict__ row_map, uint64_t n_out, uint32_t k_splits) {
+    ts_body<true, false>(X, n, w_pad, tiles, n_tiles, out, flags, row_map, n_out, k_splits);
+}
+
+__global__ void __launch_bounds__(TS_THREADS, 1)
+bb_mma_ts_rows_long_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad,
+                           const uint2* __restrict__ tiles, uint32_t n_tiles, uint32_t* __restrict__ out,
+                           DeviceFlags* __restrict__ flags, const uint32_t* __restrict__ row_map, uint64_t n_out,
+                           uint32_t k_splits) {
+    ts_body<true, true>(X, n, w_pad, tiles, n_tiles, out, flags, row_map, n_out, k_splits);
 }
 
 }  // namespace sb200

@@ -8,6 +8,17 @@
 
 namespace sb200 {
 
+// K slices per tile for the tensor-core kernel: with fewer tiles than half
+// the SMs, each tile's K range is cut so the launch fills the GPU; a slice
+// keeps at least 32 stages (8192 bits) so the per-item epilogue stays small
+// against the MMA work.
+static uint32_t ts_k_splits(uint32_t n_tiles, int sms, uint32_t w_pad) {
+    const uint32_t nk = w_pad / (TS_KBITS / 64);
+    if (n_tiles == 0 || (uint64_t)n_tiles * 2 > (uint64_t)sms) return 1;
+    const uint32_t k = std::min<uint32_t>((uint32_t)sms / n_tiles, nk / 32);
+    return k < 2 ? 1 : k;
+}
+
 static void build_tiles(std::vector<uint2>& t, uint64_t n, int kind) {
     t.clear();
     if (kind == STORM_B200_KERNEL_MMA || kind == STORM_B200_KERNEL_MMA_SS) {
@@ -26,9 +37,12 @@ static void build_tiles(std::vector<uint2>& t, uint64_t n, int kind) {
 int DenseEngine::prepare(uint64_t n, uint64_t row_bits, int kernel_pref, cudaStream_t st) {
     if (n > 0xFFFFFFFFull) fail(STORM_B200_ELIMIT, "more than 2^32 rows");
     int kind = kernel_pref;
-    if (kind == STORM_B200_KERNEL_AUTO) kind = row_bits <= MMA_MAX_BITS ? STORM_B200_KERNEL_MMA : STORM_B200_KERNEL_POPC;
-    if ((kind == STORM_B200_KERNEL_MMA || kind == STORM_B200_KERNEL_MMA_SS) && row_bits > MMA_MAX_BITS)
-        fail(STORM_B200_ELIMIT, "tensor-core kernel is exact only for rows of at most 2^23 bits");
+    if (kind == STORM_B200_KERNEL_AUTO)
+        kind = row_bits <= MMA_MAX_BITS_W4 ? STORM_B200_KERNEL_MMA : STORM_B200_KERNEL_POPC;
+    if (kind == STORM_B200_KERNEL_MMA && row_bits > MMA_MAX_BITS_W4)
+        fail(STORM_B200_ELIMIT, "tensor-core kernel is exact only for rows of at most 2^27 bits");
+    if (kind == STORM_B200_KERNEL_MMA_SS && row_bits > MMA_MAX_BITS)
+        fail(STORM_B200_ELIMIT, "shared-memory tensor-core kernel is exact only for rows of at most 2^23 bits");
     if (tiles_n != n || tiles_kind != kind) {
         build_tiles(h_tiles, n, kind);
         d_tiles.reserve(h_tiles.size());
@@ -54,11 +68,23 @@ void DenseEngine::launch(int kind, const uint64_t* dX, uint32_t n, uint32_t w_pa
         if (!attr_set) {
             SB_CUDA(cudaFuncSetAttribute(bb_mma_ts_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)TS_SMEM_BYTES));
+            SB_CUDA(cudaFuncSetAttribute(bb_mma_ts_long_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)TS_SMEM_BYTES));
             attr_set = true;
         }
-        const uint32_t grid = count < (uint32_t)sms ? count : (uint32_t)sms;
+        // split K only for a launch over the whole tile list, whose output
+        // triangle can be zeroed first for the partial-count atomics
+        const uint32_t ks = (t0 == 0 && count == n_tiles) ? ts_k_splits(count, sms, w_pad) : 1;
+        if (ks > 1 && d_out) SB_CUDA(cudaMemsetAsync(d_out, 0, tri_size(n) * sizeof(uint32_t), st));
+        const uint32_t items = count * ks;
+        const uint32_t grid = items < (uint32_t)sms ? items : (uint32_t)sms;
         const uint32_t smem = (uint64_t)w_pad * 64 <= TS_COALESCE_MAX_BITS ? TS_SMEM_BYTES : TS_SMEM_BYTES_LEAN;
-        bb_mma_ts_kernel<<<grid, TS_THREADS, smem, st>>>(dX, n, w_pad, d_tiles.p + t0, count, d_out, d_flags.p);
+        if ((uint64_t)w_pad * 64 <= MMA_MAX_BITS)
+            bb_mma_ts_kernel<<<grid, TS_THREADS, smem, st>>>(dX, n, w_pad, d_tiles.p + t0, count, d_out, d_flags.p,
+                                                             ks);
+        else
+            bb_mma_ts_long_kernel<<<grid, TS_THREADS, smem, st>>>(dX, n, w_pad, d_tiles.p + t0, count, d_out,
+                                                                  d_flags.p, ks);
     } else if (kind == STORM_B200_KERNEL_MMA_SS) {
         static bool attr_set = false;
         if (!attr_set) {
@@ -241,7 +267,7 @@ extern "C" int STORM_contig_pairw_intersect_matrix_noalloc(const uint64_t* d_row
     const uint32_t grid = n_tiles < (uint64_t)sms ? (uint32_t)n_tiles : (uint32_t)sms;
     bb_mma_ts_kernel<<<grid, TS_THREADS, TS_SMEM_BYTES, st>>>(d_rows, (uint32_t)n_rows, row_pitch_words,
                                                                scratch->tiles, (uint32_t)n_tiles, d_out,
-                                                               &scratch->flags);
+                                                               &scratch->flags, 1u);
     if (cudaGetLastError() != cudaSuccess) return STORM_B200_ECUDA;
     DeviceFlags f;
     if (cudaMemcpyAsync(&f, &scratch->flags, sizeof(f), cudaMemcpyDeviceToHost, st) != cudaSuccess)
@@ -268,11 +294,24 @@ void launch_ts_rows(const uint64_t* X, uint32_t n, uint32_t w_pad, const uint2* 
     if (!attr_set) {
         SB_CUDA(cudaFuncSetAttribute(bb_mma_ts_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)TS_SMEM_BYTES));
+        SB_CUDA(cudaFuncSetAttribute(bb_mma_ts_rows_long_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)TS_SMEM_BYTES));
         attr_set = true;
     }
-    const uint32_t grid = n_tiles < (uint32_t)sms ? n_tiles : (uint32_t)sms;
+    if ((uint64_t)w_pad * 64 > MMA_MAX_BITS_W4) fail(STORM_B200_ELIMIT, "dense block rows longer than 2^27 bits");
+    // With split K the partial counts are added into out, so the whole
+    // triangle is zeroed first; the other phases write their own pairs after.
+    const uint32_t ks = ts_k_splits(n_tiles, sms, w_pad);
+    if (ks > 1 && out) SB_CUDA(cudaMemsetAsync(out, 0, tri_size(n_out) * sizeof(uint32_t), st));
+    const uint32_t items = n_tiles * ks;
+    const uint32_t grid = items < (uint32_t)sms ? items : (uint32_t)sms;
     const uint32_t smem = (uint64_t)w_pad * 64 <= TS_COALESCE_MAX_BITS ? TS_SMEM_BYTES : TS_SMEM_BYTES_LEAN;
-    bb_mma_ts_rows_kernel<<<grid, TS_THREADS, smem, st>>>(X, n, w_pad, tiles, n_tiles, out, flags, row_map, n_out);
+    if ((uint64_t)w_pad * 64 <= MMA_MAX_BITS)
+        bb_mma_ts_rows_kernel<<<grid, TS_THREADS, smem, st>>>(X, n, w_pad, tiles, n_tiles, out, flags, row_map, n_out,
+                                                              ks);
+    else
+        bb_mma_ts_rows_long_kernel<<<grid, TS_THREADS, smem, st>>>(X, n, w_pad, tiles, n_tiles, out, flags, row_map,
+                                                                   n_out, ks);
     SB_CUDA(cudaGetLastError());
 }
 

@@ -360,7 +360,7 @@ struct STORM_rows_s {
     DevBuf<TileDecision> d_dec;
     DevBuf<RowsStatsDev> d_stats;
     // tensor-core dense block
-    double dense_min_density = 1.0 / 64.0;
+    double dense_min_density = 1.0 / 16384.0;
     DevBuf<uint64_t> d_dense;
     DevBuf<uint32_t> d_dmap;
     DevBuf<uint2> d_dtiles;
@@ -478,13 +478,20 @@ static void rows_run(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell,
     c.policy = policy;
     c.model = default_cost_model();
     // Dense block: the suffix of the density order whose rows all have a
-    // bitmap and density >= dense_min_density; its pairs run on the tensor
-    // cores (exact for universes up to 2^23 bits).
+    // bitmap and whose smallest sparse form (elements or run bounds) is
+    // >= dense_min_density x universe; its pairs run on the tensor
+    // cores (exact for universes up to 2^27 bits). A tensor-core pair costs
+    // in proportion to the universe, a cell pair to the sparse sizes.
     uint32_t D = n;
     const bool sorted_pol = sorted_order_policy(policy);
-    if (sorted_pol && r->dense_min_density > 0.0 && r->universe <= (1u << 23)) {
-        const double min_card = r->dense_min_density * (double)r->universe;
-        while (D > 0 && r->pack.meta[order[D - 1]].has_bm && (double)r->pack.meta[order[D - 1]].card >= min_card) --D;
+    if (sorted_pol && r->dense_min_density > 0.0 && r->universe <= (1u << 27)) {
+        const double min_size = r->dense_min_density * (double)r->universe;
+        auto joins = [&](uint32_t row) {
+            const RowMetaD& m = r->pack.meta[row];
+            const double sparse = std::min<double>((double)m.card, 2.0 * m.runs);
+            return m.has_bm && sparse >= min_size;
+        };
+        while (D > 0 && joins(order[D - 1])) --D;
         if (n - D < 256) D = n;
     }
     c.dense_from = D;

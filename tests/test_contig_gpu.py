@@ -53,6 +53,26 @@ def test_edge_shapes_match_oracle(sb, kernel, n, m, p):
     np.testing.assert_array_equal(mat, want)
 
 
+def test_long_rows_tensor_kernel(sb):
+    """Rows past 2^23 bits take the 4-byte weight cycle (D = 8 x count):
+    random rows, and all-ones rows of 2^26 bits (count 2^26, D = 2^29)."""
+    m = (1 << 23) + 4096
+    words = gen.bernoulli_rows(40, m, 0.3, 4242)
+    c = contig_from_words(sb, words, m, "mma")
+    mat, s = c.matrix()
+    want, ws = ol.contig_matrix(words)
+    assert s == ws
+    np.testing.assert_array_equal(mat, want)
+    m = 1 << 26
+    ones = np.full((3, m // 64), np.uint64(0xFFFFFFFFFFFFFFFF), dtype=np.uint64)
+    ones[1, ::2] = 0
+    c = contig_from_words(sb, ones, m, "mma")
+    mat, s = c.matrix()
+    want, ws = ol.contig_matrix(ones)
+    assert s == ws and mat[0] == m
+    np.testing.assert_array_equal(mat, want)
+
+
 def test_all_ones_and_empty_rows(sb):
     m = 4096
     words = np.zeros((260, m // 64), dtype=np.uint64)
@@ -193,6 +213,38 @@ def test_config1_full_size_both_kernels(sb):
     _check_full_size(sb, 4096, 65536, 0.5, 101, ["mma", "mma_ss", "popc"])
 
 
+def test_config5a_haplotypes_full_size(sb):
+    """200,000 sites x 20,000 haplotypes, 1/k allele counts in 32-haplotype
+    blocks: 2.0e10 pairs, 80 GB of counts kept in HBM.  Checked on sampled
+    whole rows against the oracle, the diagonal and the sum identity."""
+    import torch
+    import bench
+    n, m = 200000, 20000
+    rows = bench.haplotype_rows_gpu(n, m, 32, 55, torch.device("cuda"))
+    host = rows.cpu().numpy().view(np.uint64)
+    pc = ol.row_popcounts(host).astype(np.int64)
+    assert pc.min() >= 1 and pc.max() <= m - 1
+    c = sb.StormContig(m)
+    c.add_bitmaps(host)
+    tri = n * (n + 1) // 2
+    out = torch.empty(tri, dtype=torch.int32, device="cuda")
+    s = c.matrix_device(out.data_ptr(), tri)
+    assert c.last_kernel() == sb.KERNEL_MMA
+    g = gen.rng(5)
+    for i in np.unique(np.concatenate([[0, n - 1], g.integers(0, n, size=5)])):
+        base = int(sb.tri_index(n, i, i))
+        got = out[base: base + (n - i)].cpu().numpy().view(np.uint32)
+        np.testing.assert_array_equal(got, ol.contig_row(host, int(i)), err_msg=f"row {i}")
+    ii = np.arange(n, dtype=np.uint64)
+    diag = out[torch.from_numpy(sb.tri_index(n, ii, ii).astype(np.int64)).cuda()].cpu().numpy().view(np.uint32)
+    np.testing.assert_array_equal(diag, pc)
+    total = 0
+    step = 1 << 30
+    for a in range(0, tri, step):
+        total += int(out[a: a + step].to(torch.int64).bitwise_and(0xFFFFFFFF).sum().item())
+    assert s == total - int(pc.sum())
+
+
 def test_config2_full_size_tensor_kernel(sb):
     """65536 rows x 262144 bits, p ~ U[0.05, 0.5] (2 GiB in, 8.6 GB out)."""
     _check_full_size(sb, 65536, 262144, (0.05, 0.5), 202, ["mma"])
@@ -215,3 +267,25 @@ def test_device_pointer_ingest_orders_after_producer(sb):
     mat, _ = c.matrix()
     base = int(sb.tri_index(n, 5, 5))
     np.testing.assert_array_equal(mat[base: base + n - 5], want)
+
+
+@pytest.mark.parametrize("n,m", [(200, (1 << 20) + 64), (130, (1 << 23) + 256), (5, 1 << 22), (300, 1 << 16)])
+def test_split_k_few_tiles(sb, n, m):
+    """Fewer tiles than SMs: each tile's K range is cut into slices whose
+    partial counts are added into the zeroed triangle. Exact through the host
+    matrix, the sum-only call, and a device buffer that held garbage."""
+    import torch
+    g = gen.rng(77 + n)
+    words = g.integers(0, 1 << 63, size=(n, (m + 63) // 64), dtype=np.uint64) & g.integers(
+        0, 1 << 63, size=(n, (m + 63) // 64), dtype=np.uint64)        # p = 1/4, top bit clear
+    if m % 64:
+        words[:, -1] &= np.uint64((1 << (m % 64)) - 1)
+    c = contig_from_words(sb, words, m, "mma")
+    mat, s = c.matrix()
+    want, ws = ol.contig_matrix(words)
+    assert s == ws
+    np.testing.assert_array_equal(mat, want)
+    assert c.pairw_intersect_cardinality() == ws
+    d = torch.full((want.size,), -1, dtype=torch.int32, device="cuda")
+    assert c.matrix_device(d.data_ptr(), want.size) == ws
+    np.testing.assert_array_equal(d.cpu().numpy().view(np.uint32), want)
