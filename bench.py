@@ -423,6 +423,105 @@ def config45_forms(device):
     return out
 
 
+def chunk_alg_bytes(sets):
+    """Algorithmic bytes of the chunked all-pairs sum: over pairs i < j and the
+    65536-bit chunks both rows hold, the bytes of both chunks (bitmap 8192 B
+    when it holds >= 4096 values, else a u16 list of 2 B per value) --
+    sum over chunks c of (rows holding c - 1) x (bytes of c over those rows)."""
+    n_c, s_c = {}, {}
+    ids_all, sz_all = [], []
+    for v in sets:
+        if len(v) == 0:
+            continue
+        ids, cnt = np.unique(np.asarray(v, np.uint32) >> 16, return_counts=True)
+        ids_all.append(ids)
+        sz_all.append(np.where(cnt >= 4096, 8192, 2 * cnt).astype(np.float64))
+    if not ids_all:
+        return 0.0
+    ids = np.concatenate(ids_all)
+    sz = np.concatenate(sz_all)
+    m = int(ids.max()) + 1
+    n_c = np.bincount(ids, minlength=m).astype(np.float64)
+    s_c = np.bincount(ids, weights=sz, minlength=m)
+    return float(np.sum(np.maximum(n_c - 1, 0) * s_c))
+
+
+def storm_t_forms(device, cpu_seconds=2.0):
+    """STORM_t (the reference's chunked rows, storm.h:158-178) all-pairs sum
+    on config-3/4/5-shaped corpora at reduced N: the chunk kernel alone (the
+    plain per-pair GPU form), the default form (tensor-core dense block chosen
+    by the chunk cost model), and the reference's STORM_pairw_intersect_
+    cardinality on 1 core over a prefix of the rows (all-pairs call only)."""
+    import ctypes as C
+    import importlib
+    sb = importlib.import_module("stormbitmaps-internal_b200")
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as ol
+    R = ol.reference()
+    corpora = [
+        ("zipf_2^24", lambda: zipf_sets_gpu(4096, 1 << 24, 1.1, 16, 1 << 22, 0xC0F3, device),
+         "4096 rows over 2^24, card ~ Zipf(1.1) on [16, 2^22]"),
+        ("runs_2^26", lambda: run_sets_gpu(2048, 1 << 26, 200, 256, 0xC0F4, device),
+         "2048 rows over 2^26, Poisson(200) runs of Geometric(mean 256)"),
+        ("haplotypes_20000", lambda: [np.flatnonzero(np.unpackbits(r.view(np.uint8), bitorder="little"))
+                                      .astype(np.uint32) for r in
+                                      haplotype_rows_gpu(8192, 20000, 32, 0xC0F5, device).cpu().numpy()],
+         "8192 sites x 20000 haplotypes, P(k) ~ 1/k, 32-haplotype carrier blocks"),
+    ]
+    for d, nn in ((1e-6, 4096), (1e-5, 4096), (1e-4, 4096), (1e-3, 2048), (1e-2, 2048), (0.17, 1024)):
+        corpora.append((f"bernoulli_{d:g}_2^24",
+                        (lambda d=d, nn=nn: bernoulli_sets_gpu(nn, 1 << 24, d, int(1e7 * d) + 5, device)),
+                        f"{nn} rows over 2^24, Bernoulli({d:g})"))
+    out = {}
+    for name, make, desc in corpora:
+        sets = make()
+        n = len(sets)
+        pairs = n * (n - 1) // 2
+        s = sb.Storm()
+        for v in sets:
+            s.add(v)
+        s.upload()
+        res = {"workload": desc, "pairs_i_lt_j": pairs}
+        sums = set()
+        for form, thr in (("gpu_chunk_kernel", 0.0), ("gpu_default", -1.0)):
+            s.set_dense_block(thr)
+            best = None
+            for _ in range(2):
+                sums.add(s.pairw_intersect_cardinality())
+                ms = s.last_kernel_ms()
+                best = ms if best is None else min(best, ms)
+            res[form] = {"pairs_per_s": pairs / (best * 1e-3), "ms": round(best, 3),
+                         "dense_rows": s.last_dense()[0]}
+        s.close()
+        if len(sums) != 1:
+            raise RuntimeError(f"{name}: forms disagree {sums}")
+        alg = chunk_alg_bytes(sets)
+        res["alg_bytes"] = alg
+        for form in ("gpu_chunk_kernel", "gpu_default"):
+            res[form]["alg_GBps"] = alg / (res[form]["ms"] * 1e-3) / 1e9
+        if R is not None:
+            k, rate, secs = 64, None, 0.0
+            while True:
+                k = min(k, n)
+                vals = np.ascontiguousarray(np.concatenate(sets[:k]), dtype=np.uint32)
+                offs = np.zeros(k + 1, np.uint64)
+                offs[1:] = np.cumsum([len(x) for x in sets[:k]])
+                sec = C.c_double(0.0)
+                R.ref_storm_sum_timed(vals.ctypes.data_as(ol.u32p), offs.ctypes.data_as(ol.u64p), k, C.byref(sec))
+                secs = sec.value
+                rate = (k * (k - 1) // 2) / max(secs, 1e-9)
+                if secs >= cpu_seconds or k == n:
+                    break
+                k *= 2
+            res["cpu_reference"] = {"pairs_per_s": rate, "cores": 1,
+                                    "sample": f"first {k} rows ({k * (k - 1) // 2} pairs, {secs:.2f} s), "
+                                              f"STORM_pairw_intersect_cardinality as shipped (all-pairs call only)"}
+            res["gpu_default_over_cpu"] = res["gpu_default"]["pairs_per_s"] / rate
+        res["gpu_default_over_chunk_kernel"] = res["gpu_default"]["pairs_per_s"] / res["gpu_chunk_kernel"]["pairs_per_s"]
+        out[name] = res
+    return out
+
+
 # ------------------------------------------------------------------ arms
 def run_reference_arm(args):
     rank, world, local = dist_env()
@@ -604,6 +703,10 @@ def run_b200_arm(args):
             line["configs_4_5"] = config45_forms(device)
         except Exception as e:
             line["configs_4_5"] = {"error": f"{type(e).__name__}: {e}"}
+        try:
+            line["storm_t"] = storm_t_forms(device)
+        except Exception as e:
+            line["storm_t"] = {"error": f"{type(e).__name__}: {e}"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

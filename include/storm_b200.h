@@ -138,6 +138,23 @@ int STORM_upload(STORM_t* s);
 int STORM_pairw_intersect_matrix(STORM_t* s, uint32_t* out, uint64_t out_len, uint64_t* sum);
 int STORM_pairw_intersect_tiles(STORM_t* s, uint32_t tile, STORM_tile_callback cb, void* ctx);
 float STORM_last_kernel_ms(const STORM_t* s);
+/* Tensor-core dense block of the STORM_t all-pairs calls (no counterpart in
+ * the reference, which compares chunk by chunk): rows with strictly
+ * ascending chunk ids, no repeated list value and full 1024-word bitmap
+ * chunks are candidates (universe = 65536 x (largest chunk id + 1), at most
+ * 2^27 bits).  The chosen ones are expanded into contiguous bitmaps and
+ * compared with each other by the tcgen05 kernel; pairs with any other row
+ * stay on the chunk kernel.  Counts are identical either way.
+ * min_density < 0 (the default): a candidate joins when its predicted chunk-
+ * kernel cost against a row like itself exceeds the tensor-core cost of a
+ * pair (which grows with the universe); min_density > 0: when its value
+ * count is >= min_density x universe; 0 disables the block.
+ * budget_bytes bounds the expanded rows held at once (0: 60 % of free device
+ * memory); larger sets run in panels.  Applies to later all-pairs calls. */
+int STORM_set_dense_block(STORM_t* s, double min_density, uint64_t budget_bytes);
+/* Rows / panels the last all-pairs call on s gave to the dense block. */
+uint64_t STORM_last_dense_rows(const STORM_t* s);
+uint64_t STORM_last_dense_panels(const STORM_t* s);
 
 #ifdef __cplusplus
 } /* extern "C" */

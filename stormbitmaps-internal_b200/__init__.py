@@ -87,6 +87,9 @@ _sig("STORM_upload", C.c_int, [C.c_void_p])
 _sig("STORM_pairw_intersect_matrix", C.c_int, [C.c_void_p, u32p, C.c_uint64, u64p])
 _sig("STORM_pairw_intersect_tiles", C.c_int, [C.c_void_p, C.c_uint32, TILE_CB, C.c_void_p])
 _sig("STORM_last_kernel_ms", C.c_float, [C.c_void_p])
+_sig("STORM_set_dense_block", C.c_int, [C.c_void_p, C.c_double, C.c_uint64])
+_sig("STORM_last_dense_rows", C.c_uint64, [C.c_void_p])
+_sig("STORM_last_dense_panels", C.c_uint64, [C.c_void_p])
 
 
 class StormError(RuntimeError):
@@ -350,6 +353,13 @@ class Storm:
 
     def last_kernel_ms(self) -> float:
         return float(_lib.STORM_last_kernel_ms(self.h))
+
+    def set_dense_block(self, min_density: float, budget_bytes: int = 0):
+        _check(_lib.STORM_set_dense_block(self.h, float(min_density), int(budget_bytes)), "STORM_set_dense_block")
+
+    def last_dense(self):
+        """(rows, panels) the last all-pairs call gave to the tensor-core block."""
+        return int(_lib.STORM_last_dense_rows(self.h)), int(_lib.STORM_last_dense_panels(self.h))
 
 
 # --- kernel layer (include/storm_rows.h) ---------------------------------

@@ -42,16 +42,31 @@ struct ChunkView {
     const uint16_t* lst;
 };
 
-// Host staging of the packed layout.
+// What the dense block needs to know of a row: its value count, chunk
+// counts by kind, list entries, and whether it is "plain" (strictly
+// ascending chunk ids, no repeated list value, full 1024-word bitmaps -- so
+// that its chunks expand to one contiguous bitmap with the same counts).
+struct ChunkRowFacts {
+    uint64_t card = 0, list_entries = 0;
+    uint32_t chunks = 0, bitmap_chunks = 0;
+    bool plain = true;
+};
+
+// Host staging of the packed layout, with the per-row facts and the largest
+// chunk id.
 struct ChunkPack {
     std::vector<uint64_t> row_off{0};
     std::vector<uint32_t> cid, ckl;
     std::vector<uint64_t> coff;
     std::vector<uint64_t> bm;
     std::vector<uint16_t> lst;
+    std::vector<ChunkRowFacts> facts;
+    uint32_t max_cid = 0;
     void clear() {
         row_off.assign(1, 0);
         cid.clear(); ckl.clear(); coff.clear(); bm.clear(); lst.clear();
+        facts.clear();
+        max_cid = 0;
     }
     uint64_t rows() const { return row_off.size() - 1; }
     void add_chunk(uint32_t id, const STORM_bitmap_t& b);
@@ -64,6 +79,8 @@ struct ChunkDev {
     DevBuf<uint32_t> cid, ckl;
     DevBuf<uint16_t> lst;
     uint64_t n_rows = 0;
+    std::vector<ChunkRowFacts> facts;   // host copy of the per-row facts
+    uint32_t max_cid = 0;
     void upload(const ChunkPack& p, cudaStream_t st);
     ChunkView view() const {
         return ChunkView{row_off.p, cid.p, ckl.p, coff.p, bm.p, lst.p};
@@ -76,9 +93,42 @@ enum PairMode : uint32_t {
     PAIRS_RECT = 1,       // i < n1, n1 <= j < n1 + n2 (sum only)
 };
 
+// Tensor-core dense block of the chunked engine (triangle mode): chosen plain
+// rows (universe = 65536 x (largest chunk id + 1), at most 2^27 bits) are
+// expanded, panel by panel, into contiguous bitmaps in HBM and compared with
+// each other by the tcgen05 kernel; the chunk kernel then walks only the
+// pairs with another row.
+//
+// Which rows: with dense_min_density > 0, those whose value count is at least
+// that share of the universe; with dense_min_density < 0 (the default), those
+// whose predicted chunk-kernel cost against a copy of themselves exceeds the
+// predicted tensor-core cost of one pair. A tensor-core pair costs in
+// proportion to the universe; a chunk pair costs per shared chunk (a fixed
+// part plus lane iterations: 32 for a bitmap chunk, ceil(e / 32) x
+// (log2 e + 1) for lists of e entries -- the binary-search probe), and two
+// rows of c chunks each share about c^2 / slots of them. The constants are
+// B200 throughput figures (ns per pair with the whole GPU busy) fitted on
+// Bernoulli rows at 1e-5 .. 0.17 over 2^24 and run-clustered rows over 2^26.
+struct ChunkCostModel {
+    double ns_per_shared_chunk = 0.086;
+    double ns_per_lane_iteration = 0.0228;
+    double ns_per_tensor_bit = 1.3e-6;
+};
+double chunk_self_pair_ns(const ChunkCostModel& m, const ChunkRowFacts& f, uint64_t slots);
+double tensor_pair_ns(const ChunkCostModel& m, uint64_t slots);
+
+constexpr double CHUNK_DENSE_AUTO = -1.0;
+
 struct ChunkEngine {
     DevBuf<DeviceFlags> d_flags;
     LaunchLog log;
+    double dense_min_density = CHUNK_DENSE_AUTO;
+    ChunkCostModel cost;
+    uint64_t dense_budget_bytes = 0;   // 0: 60 % of free device memory
+    uint64_t last_dense_rows = 0, last_dense_panels = 0;
+    DevBuf<uint32_t> d_perm, d_map;
+    DevBuf<uint64_t> d_panel;
+    DevBuf<uint2> d_tiles;
     ~ChunkEngine() { log.destroy(); }
     // Returns the sum over i < j (triangle) or over all (i, j) (rect).
     uint64_t run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_t n2, uint32_t* d_out,

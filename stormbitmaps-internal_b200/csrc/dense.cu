@@ -287,7 +287,8 @@ namespace sb200 {
 void build_mma_tiles(std::vector<uint2>& t, uint64_t n) { build_tiles(t, n, STORM_B200_KERNEL_MMA); }
 
 void launch_ts_rows(const uint64_t* X, uint32_t n, uint32_t w_pad, const uint2* tiles, uint32_t n_tiles,
-                    uint32_t* out, DeviceFlags* flags, const uint32_t* row_map, uint64_t n_out, cudaStream_t st) {
+                    uint32_t* out, DeviceFlags* flags, const uint32_t* row_map, uint64_t n_out, cudaStream_t st,
+                    bool out_zeroed) {
     const int sms = require_device();
     if (n_tiles == 0) return;
     static bool attr_set = false;
@@ -302,7 +303,7 @@ void launch_ts_rows(const uint64_t* X, uint32_t n, uint32_t w_pad, const uint2* 
     // With split K the partial counts are added into out, so the whole
     // triangle is zeroed first; the other phases write their own pairs after.
     const uint32_t ks = ts_k_splits(n_tiles, sms, w_pad);
-    if (ks > 1 && out) SB_CUDA(cudaMemsetAsync(out, 0, tri_size(n_out) * sizeof(uint32_t), st));
+    if (ks > 1 && out && !out_zeroed) SB_CUDA(cudaMemsetAsync(out, 0, tri_size(n_out) * sizeof(uint32_t), st));
     const uint32_t items = n_tiles * ks;
     const uint32_t grid = items < (uint32_t)sms ? items : (uint32_t)sms;
     const uint32_t smem = (uint64_t)w_pad * 64 <= TS_COALESCE_MAX_BITS ? TS_SMEM_BYTES : TS_SMEM_BYTES_LEAN;

@@ -46,11 +46,17 @@ inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
 
 // Tiles (bi, bj) of 128 x 256 pairs covering the triangle of n rows.
 void build_mma_tiles(std::vector<uint2>& t, uint64_t n);
-// Tensor-core kernel over n gathered rows X ([>= roundup(n, 256)][w_pad],
-// zero padded); count (i, j) lands at the packed index of
-// (row_map[i], row_map[j]) in a triangle of n_out rows; the sum over i < j
-// accumulates into flags->sum.  Asynchronous on st.
+// Longest row the tensor-core kernels count exactly (4-byte weight cycle).
+constexpr uint64_t TC_MAX_ROW_BITS = 1ull << 27;
+
+// Tensor-core kernel over n gathered rows X ([>= roundup(n, 256)][w_pad]);
+// count (i, j) lands at the packed index of (row_map[i], row_map[j]) in a
+// triangle of n_out rows; the sum over i < j accumulates into flags->sum.
+// With few tiles the K range is split and partial counts are added into
+// out: out_zeroed says the caller has zeroed the triangle already, else it
+// is zeroed here when a split is taken.  Asynchronous on st.
 void launch_ts_rows(const uint64_t* X, uint32_t n, uint32_t w_pad, const uint2* tiles, uint32_t n_tiles,
-                    uint32_t* out, DeviceFlags* flags, const uint32_t* row_map, uint64_t n_out, cudaStream_t st);
+                    uint32_t* out, DeviceFlags* flags, const uint32_t* row_map, uint64_t n_out, cudaStream_t st,
+                    bool out_zeroed = false);
 
 }  // namespace sb200

@@ -20,6 +20,7 @@
 #include <mutex>
 #include <unordered_map>
 
+#include <cmath>
 #include "chunk_engine.cuh"
 
 namespace sb200 {
@@ -537,5 +538,17 @@ float STORM_last_kernel_ms(const STORM_t* s) {
     if (s == NULL) return 0.f;
     return state_of(s)->engine.log.last_ms;
 }
+
+int STORM_set_dense_block(STORM_t* s, double min_density, uint64_t budget_bytes) {
+    if (s == NULL) return STORM_B200_ENULL;
+    if (std::isnan(min_density)) return STORM_B200_EARG;
+    StormDev* d = state_of(s);
+    d->engine.dense_min_density = min_density;
+    d->engine.dense_budget_bytes = budget_bytes;
+    return 0;
+}
+
+uint64_t STORM_last_dense_rows(const STORM_t* s) { return s ? state_of(s)->engine.last_dense_rows : 0; }
+uint64_t STORM_last_dense_panels(const STORM_t* s) { return s ? state_of(s)->engine.last_dense_panels : 0; }
 
 }  // extern "C"

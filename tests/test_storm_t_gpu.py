@@ -118,3 +118,86 @@ def test_reference_test_program_against_this_library():
     r = subprocess.run([exe], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     assert " 0 failures" in r.stdout, r.stdout[-2000:]
+
+
+def _dense_corpus(n_dense, n_sparse, universe, lo, hi, seed):
+    g = gen.rng(seed)
+    sets = [gen.uniform_set(g, int(g.integers(lo, hi)), universe) for _ in range(n_dense)]
+    sets += [gen.uniform_set(g, int(g.integers(1, 40)), universe) for _ in range(n_sparse)]
+    return [sets[k] for k in g.permutation(len(sets))]
+
+
+def test_tensor_dense_block_matches_chunk_kernel_and_oracle(sb):
+    """Plain dense rows are expanded into contiguous bitmaps and compared on
+    the tensor cores; sparse rows stay on the chunk kernel. Counts are the
+    oracle's, and identical with the block switched off."""
+    sets = _dense_corpus(300, 150, 1 << 20, 1000, 8000, 91)
+    s = build_storm(sb, sets)
+    vals, offs = gen.to_csr(sets)
+    want, ws = ol.sets_matrix(vals, offs)
+    s.set_dense_block(1.0 / 16384)          # by value count: the 300 dense rows
+    mat, ssum = s.matrix()
+    rows, panels = s.last_dense()
+    assert rows == 300 and panels == 1
+    assert ssum == ws
+    np.testing.assert_array_equal(mat, want)
+    assert s.pairw_intersect_cardinality() == ws
+    s.set_dense_block(-1.0)                 # by predicted cost (the default)
+    mat, ssum = s.matrix()
+    assert s.last_dense()[0] >= 300 and ssum == ws
+    np.testing.assert_array_equal(mat, want)
+    s.set_dense_block(0.0)
+    mat0, s0 = s.matrix()
+    assert s.last_dense() == (0, 0) and s0 == ws
+    np.testing.assert_array_equal(mat0, want)
+
+
+def test_tensor_dense_block_in_panels(sb):
+    """A budget of two 256-row panels forces three panels (full, full, ragged):
+    triangle launches per panel, rectangle launches per panel pair, and the
+    split-K path on the ragged panel's few tiles."""
+    universe = 1 << 20
+    sets = _dense_corpus(700, 60, universe, 500, 4000, 92)
+    s = build_storm(sb, sets)
+    row_bytes = universe // 8
+    s.set_dense_block(1.0 / 16384, 2 * 256 * row_bytes + 4096)
+    vals, offs = gen.to_csr(sets)
+    want, ws = ol.sets_matrix(vals, offs)
+    mat, ssum = s.matrix()
+    assert s.last_dense() == (700, 3)
+    assert ssum == ws
+    np.testing.assert_array_equal(mat, want)
+    assert s.pairw_intersect_cardinality() == ws
+
+
+def test_tensor_dense_block_rows_with_repeats_stay_on_chunks(sb):
+    """Rows whose list chunks hold a repeated value (STORM_add does not
+    deduplicate lists) keep the chunk kernel's k-th-copy count; the block
+    takes only the plain rows and the totals match the block-off run."""
+    sets = _dense_corpus(280, 20, 1 << 18, 300, 3000, 93)
+    dup_rows = [3, 50, 120]
+    s = sb.Storm()
+    for k, v in enumerate(sets):
+        if k in dup_rows:
+            v = np.sort(np.concatenate([v, v[:7]]))
+        s.add(np.asarray(v, dtype=np.uint32))
+    mat, ssum = s.matrix()
+    rows, _ = s.last_dense()
+    assert 256 <= rows <= len(sets) - len(dup_rows)
+    s.set_dense_block(0.0)
+    mat0, s0 = s.matrix()
+    assert s0 == ssum
+    np.testing.assert_array_equal(mat, mat0)
+
+
+def test_tensor_dense_block_long_universe(sb):
+    """A 2^24-value universe (256 chunks per row, rows past 2^23 bits take the
+    4-byte weight cycle) with Bernoulli(1e-3) rows."""
+    sets = gen.bernoulli_sets(260, 1 << 24, 1e-3, 94)
+    s = build_storm(sb, sets)
+    vals, offs = gen.to_csr(sets)
+    want, ws = ol.sets_matrix(vals, offs)
+    mat, ssum = s.matrix()
+    assert s.last_dense()[0] == 260
+    assert ssum == ws
+    np.testing.assert_array_equal(mat, want)
