@@ -40,6 +40,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N_ROWS, M_BITS, P_RANGE, SEED = 65536, 262144, (0.05, 0.5), 0x5EED2
+L2_BYTES = 126 * 1000 * 1000
 METRIC = "exact pairs/sec & ns/pair on 1 B200: learned-batched vs plain GPU vs CPU"
 
 
@@ -552,7 +553,7 @@ def run_reference_arm(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * pairs_of(N_ROWS) / value,
         "ns_per_pair": 1e9 / value, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u64 (AND + popcount)", "data": "synthetic (seeded, generated on the GPU, copied to host)",
-        "config": {"workload": "dense all-bitmap XX^T: 65536 rows x 262144 bits, p~U[0.05,0.5], u32 i<=j out",
+        "config": {"workload": f"dense all-bitmap XX^T: {N_ROWS} rows x {M_BITS} bits, p~U[0.05,0.5], u32 i<=j out",
                    "rows": N_ROWS, "bits": M_BITS, "pairs": pairs_of(N_ROWS),
                    "sampled": f"rows 0..{last_rows} of the triangle per step (every j >= i)"},
         "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": "reference",
@@ -579,6 +580,7 @@ def run_b200_arm(args):
     c = sb.StormContig(m)
     c.set_kernel({"auto": sb.KERNEL_AUTO, "popc": sb.KERNEL_POPC, "mma": sb.KERNEL_MMA,
                   "mma_ss": sb.KERNEL_MMA_SS}[args.kernel])
+    c.set_schedule({"auto": sb.SCHED_AUTO, "tiles": sb.SCHED_TILES, "stream_k": sb.SCHED_STREAM_K}[args.schedule])
     rc = sb.lib().STORM_contig_add_bitmaps(c.h, C.cast(rows_d.data_ptr(), sb.u64p), n, w)
     if rc < 0:
         raise sb.StormError(rc, "STORM_contig_add_bitmaps")
@@ -595,16 +597,32 @@ def run_b200_arm(args):
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    # Working sets smaller than twice L2 (126 MB) get an L2 flush between
+    # steps (a 256 MiB write on the library's stream), timed outside the
+    # per-step events; larger ones stream from HBM anyway.
+    fits_l2 = n * w * 8 + tri * 4 < 2 * L2_BYTES
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device) if fits_l2 else None
+    step_ms = []
     with ClockSampler(local) as clocks:
-        ev0.record(stream)
+        if flush is None:
+            ev0.record(stream)
         for _ in range(args.steps):
+            if flush is not None:
+                with torch.cuda.stream(stream):
+                    flush.zero_()
+                ev0.record(stream)
             s = c.matrix_device(out_d.data_ptr(), tri)
             kernel_ms.append(c.last_kernel_ms())
-        ev1.record(stream)
+            if flush is not None:
+                ev1.record(stream)
+                ev1.synchronize()
+                step_ms.append(ev0.elapsed_time(ev1))
+        if flush is None:
+            ev1.record(stream)
         torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    elapsed_ms = ev0.elapsed_time(ev1)
+    elapsed_ms = sum(step_ms) if flush is not None else ev0.elapsed_time(ev1)
     elapsed_ms = max_over_ranks(elapsed_ms, dist, device)
     launches = args.steps * c.last_launches()
     kernel_used = {sb.KERNEL_POPC: "bb_popc_kernel", sb.KERNEL_MMA: "bb_mma_ts_kernel",
@@ -673,9 +691,12 @@ def run_b200_arm(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8 (tcgen05 kind::i8, s32 acc)"
         if kernel_used in ("bb_mma_kernel", "bb_mma_ts_kernel") else "u64 (AND + POPC)",
         "data": "synthetic (seeded Bernoulli rows generated on the GPU)",
-        "config": {"workload": "dense all-bitmap XX^T: 65536 rows x 262144 bits, p~U[0.05,0.5], u32 i<=j out",
-                   "rows": n, "bits": m, "pairs_per_gpu": tri, "kernel": kernel_used,
-                   "l2": "inputs (2 GiB) and outputs (8.6 GB) exceed L2 (126 MB); no flush needed",
+        "config": {"workload": f"dense all-bitmap XX^T: {n} rows x {m} bits, p~U[0.05,0.5], u32 i<=j out",
+                   "rows": n, "bits": m, "pairs_per_gpu": tri, "kernel": kernel_used, "schedule": args.schedule,
+                   "l2": (f"inputs ({n * w * 8 / 1e6:.1f} MB) and outputs ({tri * 4 / 1e6:.1f} MB) fit in twice "
+                          f"L2 (126 MB): 256 MiB L2 flush between steps, outside the step events") if fits_l2 else
+                         (f"inputs ({n * w * 8 / 2**30:.2f} GiB) and outputs ({tri * 4 / 1e9:.2f} GB) exceed "
+                          f"L2 (126 MB); no flush needed"),
                    "parallelism": f"{world} independent instances (weak)"},
         "kernel_ms_median": k_ms,
         "gpu_launches": launches,
@@ -722,6 +743,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma", "mma_ss"])
+    ap.add_argument("--schedule", default="auto", choices=["auto", "tiles", "stream_k"],
+                    help="tensor-core work schedule (whole tiles or stream-K; auto picks per launch)")
     ap.add_argument("--rows", type=int, default=N_ROWS)
     ap.add_argument("--bits", type=int, default=M_BITS)
     ap.add_argument("--e2e-steps", type=int, default=2)

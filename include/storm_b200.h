@@ -86,6 +86,15 @@ int STORM_contig_add_bitmaps(STORM_contiguous_t* c, const uint64_t* words,
 /* Number of rows held. */
 uint64_t STORM_contig_size(const STORM_contiguous_t* c);
 int STORM_contig_set_kernel(STORM_contiguous_t* c, int kernel);
+/* Work schedule of the tensor-core kernel: STORM_B200_SCHED_AUTO picks per
+ * launch (stream-K when the last wave of whole tiles would be less than 95 %
+ * full), _TILES deals whole tiles round robin, _STREAM_K always
+ * splits the (tile, K stage) space evenly over the SMs. Counts are the same
+ * under every schedule. */
+#define STORM_B200_SCHED_AUTO     0
+#define STORM_B200_SCHED_TILES    1
+#define STORM_B200_SCHED_STREAM_K 2
+int STORM_contig_set_schedule(STORM_contiguous_t* c, int schedule);
 /* Pack the rows into HBM now (otherwise done by the first all-pairs call). */
 int STORM_contig_upload(STORM_contiguous_t* c);
 /* Per-pair counts into a HOST buffer of out_len >= n*(n+1)/2 entries. */

@@ -37,6 +37,7 @@ u64p = C.POINTER(C.c_uint64)
 TILE_CB = C.CFUNCTYPE(None, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, u32p, C.c_void_p)
 
 KERNEL_AUTO, KERNEL_POPC, KERNEL_MMA, KERNEL_MMA_SS = 0, 1, 2, 3
+SCHED_AUTO, SCHED_TILES, SCHED_STREAM_K = 0, 1, 2
 OK, ENULL, EVALUES, EARG, ENOMEM, ECUDA, ETIMEOUT, ESIZE, ELIMIT = 0, -1, -2, -3, -4, -5, -6, -7, -8
 
 
@@ -67,6 +68,7 @@ _sig("STORM_contig_pairw_intersect_cardinality_blocked_list", C.c_uint64, [C.c_v
 _sig("STORM_contig_add_bitmaps", C.c_int, [C.c_void_p, u64p, C.c_uint32, C.c_uint32])
 _sig("STORM_contig_size", C.c_uint64, [C.c_void_p])
 _sig("STORM_contig_set_kernel", C.c_int, [C.c_void_p, C.c_int])
+_sig("STORM_contig_set_schedule", C.c_int, [C.c_void_p, C.c_int])
 _sig("STORM_contig_upload", C.c_int, [C.c_void_p])
 _sig("STORM_contig_pairw_intersect_matrix", C.c_int, [C.c_void_p, u32p, C.c_uint64, u64p])
 _sig("STORM_contig_pairw_intersect_matrix_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, u64p])
@@ -243,6 +245,9 @@ class StormContig:
 
     def set_kernel(self, kernel: int):
         _check(_lib.STORM_contig_set_kernel(self.h, kernel), "STORM_contig_set_kernel")
+
+    def set_schedule(self, schedule: int):
+        _check(_lib.STORM_contig_set_schedule(self.h, schedule), "STORM_contig_set_schedule")
 
     def upload(self):
         _check(_lib.STORM_contig_upload(self.h), "STORM_contig_upload")

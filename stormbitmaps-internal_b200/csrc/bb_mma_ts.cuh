@@ -85,6 +85,43 @@ __device__ __forceinline__ uint64_t ts_out_index(uint64_t n, uint64_t i, uint64_
     return a < b ? tri_index(n_out, a, b) : tri_index(n_out, b, a);
 }
 
+// Work schedule, identical in the three roles of a CTA. k_splits >= 1:
+// whole tiles (or k_splits even K slices of each) dealt round robin over the
+// grid. k_splits == 0 (stream-K): CTA c takes the contiguous range
+// [S c / G, S (c + 1) / G) of the flattened (tile, K stage) space, S = tiles
+// x stages, G = grid, cut at tile boundaries into segments. A segment that
+// is not a whole tile adds its partial counts into the (zeroed) output.
+struct TsSched {
+    uint32_t nk, n_tiles, k_splits, it;
+    uint64_t pos, end;
+    __device__ __forceinline__ TsSched(uint32_t nk_, uint32_t n_tiles_, uint32_t k_splits_)
+        : nk(nk_), n_tiles(n_tiles_), k_splits(k_splits_), it(blockIdx.x) {
+        const uint64_t S = (uint64_t)n_tiles * nk;
+        pos = S * blockIdx.x / gridDim.x;
+        end = S * (blockIdx.x + 1) / gridDim.x;
+    }
+    __device__ __forceinline__ bool next(uint32_t& t, uint32_t& kb0, uint32_t& kb1, bool& partial) {
+        if (k_splits == 0) {
+            if (pos >= end) return false;
+            t = (uint32_t)(pos / nk);
+            kb0 = (uint32_t)(pos % nk);
+            const uint64_t stop = (uint64_t)kb0 + (end - pos);
+            kb1 = stop < nk ? (uint32_t)stop : nk;
+            pos += kb1 - kb0;
+            partial = kb0 != 0 || kb1 != nk;
+            return true;
+        }
+        if (it >= n_tiles * k_splits) return false;
+        t = it / k_splits;
+        const uint32_t ks = it % k_splits;
+        kb0 = (uint32_t)((uint64_t)nk * ks / k_splits);
+        kb1 = (uint32_t)((uint64_t)nk * (ks + 1) / k_splits);
+        partial = k_splits > 1;
+        it += gridDim.x;
+        return true;
+    }
+};
+
 template <bool kRowMap, bool kW4>
 __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad,
                                         const uint2* __restrict__ tiles, uint32_t n_tiles,
@@ -134,11 +171,10 @@ __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t
         const uint32_t prow = is_a ? (uint32_t)tid : (uint32_t)(tid - TS_A_THREADS);   // operand row
         uint32_t g = 0, tcount = 0;
         bool ok = true;
-        for (uint32_t it = blockIdx.x; it < n_tiles * k_splits && ok; it += gridDim.x, ++tcount) {
-            // work item = (tile, K slice); the host keeps k_splits <= nk
-            const uint32_t t = it / k_splits, ks = it % k_splits;
-            const uint32_t kb0 = (uint32_t)((uint64_t)nk * ks / k_splits);
-            const uint32_t kb1 = (uint32_t)((uint64_t)nk * (ks + 1) / k_splits);
+        TsSched sched(nk, n_tiles, k_splits);
+        uint32_t t, kb0, kb1;
+        bool partial;
+        for (; ok && sched.next(t, kb0, kb1, partial); ++tcount) {
             const uint64_t i0 = (uint64_t)tiles[t].x * TS_BM;
             const uint64_t j0 = (uint64_t)tiles[t].y * TS_BN;
             const uint64_t* src = X + (is_a ? i0 + prow : j0 + prow) * (uint64_t)w_pad;
@@ -218,7 +254,7 @@ __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t
                         if (i < n && j >= i && j < n) {
                             if (out) {
                                 uint32_t* dst = out + ts_out_index<kRowMap>(n, i, j, row_map, n_out);
-                                if (k_splits > 1) atomicAdd(dst, cnt);   // partial count of one K slice
+                                if (partial) atomicAdd(dst, cnt);   // one K segment's share
                                 else *dst = cnt;
                             }
                             if (j > i) local += cnt;
@@ -246,7 +282,7 @@ __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t
                                 if (out) {
                                     uint32_t* dst = out + (kRowMap ? ts_out_index<true>(n, i, j, row_map, n_out)
                                                                    : base + j);
-                                    if (k_splits > 1) atomicAdd(dst, cnt);
+                                    if (partial) atomicAdd(dst, cnt);
                                     else *dst = cnt;
                                 }
                                 if (j > i) local += cnt;
@@ -264,10 +300,10 @@ __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t
         const uint32_t idesc = umma_idesc_u8_s32(TS_BM, TS_BN);
         uint32_t g = 0, tcount = 0;
         bool issued = false;
-        for (uint32_t it = blockIdx.x; it < n_tiles * k_splits; it += gridDim.x, ++tcount) {
-            const uint32_t ks = it % k_splits;
-            const uint32_t kb0 = (uint32_t)((uint64_t)nk * ks / k_splits);
-            const uint32_t kb1 = (uint32_t)((uint64_t)nk * (ks + 1) / k_splits);
+        TsSched sched(nk, n_tiles, k_splits);
+        uint32_t t, kb0, kb1;
+        bool partial;
+        for (; sched.next(t, kb0, kb1, partial); ++tcount) {
             if (!ts_wait(smem_u32(&ctl->acc_empty), (tcount & 1) ^ 1, ctl, flags, ERR_MMA_ACCEMPTY)) break;
             tc_fence_after();
             bool ok = true;
@@ -306,9 +342,9 @@ __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t
     }
 }
 
-// k_splits > 1 divides each tile's K range into that many work items whose
-// partial counts are added into out with atomics (out zeroed beforehand):
-// used when there are fewer tiles than SMs.
+// k_splits: the work schedule (TsSched). 1 = whole tiles round robin;
+// > 1 = that many K slices per tile; 0 = stream-K. For any value but 1 the
+// partial counts are added into out with atomics (out zeroed beforehand).
 __global__ void __launch_bounds__(TS_THREADS, 1)
 bb_mma_ts_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, const uint2* __restrict__ tiles,
                  uint32_t n_tiles, uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags, uint32_t k_splits) {

@@ -225,6 +225,13 @@ int STORM_contig_set_kernel(STORM_contiguous_t* c, int kernel) {
     return 0;
 }
 
+int STORM_contig_set_schedule(STORM_contiguous_t* c, int schedule) {
+    if (c == NULL) return STORM_B200_ENULL;
+    if (schedule < STORM_B200_SCHED_AUTO || schedule > STORM_B200_SCHED_STREAM_K) return STORM_B200_EARG;
+    c->engine.schedule = schedule;
+    return 0;
+}
+
 int STORM_contig_upload(STORM_contiguous_t* c) {
     if (c == NULL) return STORM_B200_ENULL;
     return guard([&]() -> int {

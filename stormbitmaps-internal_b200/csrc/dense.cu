@@ -8,15 +8,27 @@
 
 namespace sb200 {
 
-// K slices per tile for the tensor-core kernel: with fewer tiles than half
-// the SMs, each tile's K range is cut so the launch fills the GPU; a slice
-// keeps at least 32 stages (8192 bits) so the per-item epilogue stays small
-// against the MMA work.
-static uint32_t ts_k_splits(uint32_t n_tiles, int sms, uint32_t w_pad) {
-    const uint32_t nk = w_pad / (TS_KBITS / 64);
-    if (n_tiles == 0 || (uint64_t)n_tiles * 2 > (uint64_t)sms) return 1;
-    const uint32_t k = std::min<uint32_t>((uint32_t)sms / n_tiles, nk / 32);
-    return k < 2 ? 1 : k;
+// Work schedule of the tensor-core kernel (TsSched in bb_mma_ts.cuh): whole
+// tiles round robin when the last wave is nearly full (>= 95 %) or a tile
+// has fewer than 32 K stages; otherwise stream-K over the (tile, K stage)
+// space, at least 32 stages (8192 bits) per CTA so the per-segment epilogue
+// stays small against the MMAs. Measured on B200: 272 tiles (1.8 waves) of
+// 2^18-bit rows run 8 % faster under stream-K, 136 tiles 1.9x, 1088 tiles
+// (7.4 waves, 92 % fill) 7 %; 2176 tiles (98 % fill) 3 % slower. Returns the
+// kernel's k_splits argument (1 or 0) and sets the grid.
+static uint32_t ts_schedule(uint32_t n_tiles, int sms, uint32_t w_pad, uint32_t& grid,
+                            int pref = STORM_B200_SCHED_AUTO) {
+    const uint64_t nk = w_pad / (TS_KBITS / 64);
+    const uint64_t waves = ((uint64_t)n_tiles + sms - 1) / sms;
+    const double fill = waves ? (double)n_tiles / (double)(waves * (uint64_t)sms) : 1.0;
+    const bool tiles = pref == STORM_B200_SCHED_TILES ||
+                       (pref == STORM_B200_SCHED_AUTO && (fill >= 0.95 || nk < 32));
+    if (tiles) {
+        grid = n_tiles < (uint32_t)sms ? n_tiles : (uint32_t)sms;
+        return 1;
+    }
+    grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sms, (uint64_t)n_tiles * nk / 32));
+    return 0;
 }
 
 static void build_tiles(std::vector<uint2>& t, uint64_t n, int kind) {
@@ -72,12 +84,11 @@ void DenseEngine::launch(int kind, const uint64_t* dX, uint32_t n, uint32_t w_pa
                                          (int)TS_SMEM_BYTES));
             attr_set = true;
         }
-        // split K only for a launch over the whole tile list, whose output
+        // stream-K only for a launch over the whole tile list, whose output
         // triangle can be zeroed first for the partial-count atomics
-        const uint32_t ks = (t0 == 0 && count == n_tiles) ? ts_k_splits(count, sms, w_pad) : 1;
-        if (ks > 1 && d_out) SB_CUDA(cudaMemsetAsync(d_out, 0, tri_size(n) * sizeof(uint32_t), st));
-        const uint32_t items = count * ks;
-        const uint32_t grid = items < (uint32_t)sms ? items : (uint32_t)sms;
+        uint32_t grid = count < (uint32_t)sms ? count : (uint32_t)sms;
+        const uint32_t ks = (t0 == 0 && count == n_tiles) ? ts_schedule(count, sms, w_pad, grid, schedule) : 1;
+        if (ks != 1 && d_out) SB_CUDA(cudaMemsetAsync(d_out, 0, tri_size(n) * sizeof(uint32_t), st));
         const uint32_t smem = (uint64_t)w_pad * 64 <= TS_COALESCE_MAX_BITS ? TS_SMEM_BYTES : TS_SMEM_BYTES_LEAN;
         if ((uint64_t)w_pad * 64 <= MMA_MAX_BITS)
             bb_mma_ts_kernel<<<grid, TS_THREADS, smem, st>>>(dX, n, w_pad, d_tiles.p + t0, count, d_out, d_flags.p,
@@ -300,12 +311,11 @@ void launch_ts_rows(const uint64_t* X, uint32_t n, uint32_t w_pad, const uint2* 
         attr_set = true;
     }
     if ((uint64_t)w_pad * 64 > MMA_MAX_BITS_W4) fail(STORM_B200_ELIMIT, "dense block rows longer than 2^27 bits");
-    // With split K the partial counts are added into out, so the whole
+    // With stream-K the partial counts are added into out, so the whole
     // triangle is zeroed first; the other phases write their own pairs after.
-    const uint32_t ks = ts_k_splits(n_tiles, sms, w_pad);
-    if (ks > 1 && out && !out_zeroed) SB_CUDA(cudaMemsetAsync(out, 0, tri_size(n_out) * sizeof(uint32_t), st));
-    const uint32_t items = n_tiles * ks;
-    const uint32_t grid = items < (uint32_t)sms ? items : (uint32_t)sms;
+    uint32_t grid = 0;
+    const uint32_t ks = ts_schedule(n_tiles, sms, w_pad, grid);
+    if (ks != 1 && out && !out_zeroed) SB_CUDA(cudaMemsetAsync(out, 0, tri_size(n_out) * sizeof(uint32_t), st));
     const uint32_t smem = (uint64_t)w_pad * 64 <= TS_COALESCE_MAX_BITS ? TS_SMEM_BYTES : TS_SMEM_BYTES_LEAN;
     if ((uint64_t)w_pad * 64 <= MMA_MAX_BITS)
         bb_mma_ts_rows_kernel<<<grid, TS_THREADS, smem, st>>>(X, n, w_pad, tiles, n_tiles, out, flags, row_map, n_out,

@@ -10,6 +10,7 @@ namespace sb200 {
 // Device rows: X is [n_pad][w_pad] u64, zero padded, n_pad % 256 == 0 and
 // w_pad % 8 == 0.
 struct DenseEngine {
+    int schedule = STORM_B200_SCHED_AUTO;   // tensor-core work schedule
     DevBuf<uint2> d_tiles;
     uint64_t tiles_n = ~0ull;
     int tiles_kind = -1;

@@ -289,3 +289,18 @@ def test_split_k_few_tiles(sb, n, m):
     d = torch.full((want.size,), -1, dtype=torch.int32, device="cuda")
     assert c.matrix_device(d.data_ptr(), want.size) == ws
     np.testing.assert_array_equal(d.cpu().numpy().view(np.uint32), want)
+
+
+@pytest.mark.parametrize("n,m", [(300, (1 << 17) + 64), (700, 16384), (129, 4097), (1000, 1 << 15)])
+def test_every_schedule_is_exact(sb, n, m):
+    """Whole tiles round robin and stream-K (partial tiles added with atomics
+    into the zeroed triangle) give the oracle's counts; the automatic choice
+    too."""
+    words = gen.bernoulli_rows(n, m, (0.05, 0.6), seed=500 + n)
+    want, ws = ol.contig_matrix(words)
+    c = contig_from_words(sb, words, m, "mma")
+    for sched in (sb.SCHED_TILES, sb.SCHED_STREAM_K, sb.SCHED_AUTO):
+        c.set_schedule(sched)
+        mat, s = c.matrix()
+        assert s == ws, sched
+        np.testing.assert_array_equal(mat, want, err_msg=str(sched))
