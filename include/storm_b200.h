@@ -164,6 +164,15 @@ int STORM_set_dense_block(STORM_t* s, double min_density, uint64_t budget_bytes)
 /* Rows / panels the last all-pairs call on s gave to the dense block. */
 uint64_t STORM_last_dense_rows(const STORM_t* s);
 uint64_t STORM_last_dense_panels(const STORM_t* s);
+/* Postings for the sparse rows of the STORM_t all-pairs calls (no
+ * counterpart in the reference): plain rows without bitmap chunks outside
+ * the dense block are indexed by value (a histogram over the universe, at
+ * most 2^27 values), and each pair of them gets one increment per shared
+ * value -- pairs with nothing in common cost nothing.  mode -1 (default):
+ * used when the exact increment count predicts less time than the chunk
+ * kernel; 1: whenever rows qualify; 0: never.  Counts are identical. */
+int STORM_set_sparse_postings(STORM_t* s, int mode);
+uint64_t STORM_last_postings_rows(const STORM_t* s);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -92,6 +92,8 @@ _sig("STORM_last_kernel_ms", C.c_float, [C.c_void_p])
 _sig("STORM_set_dense_block", C.c_int, [C.c_void_p, C.c_double, C.c_uint64])
 _sig("STORM_last_dense_rows", C.c_uint64, [C.c_void_p])
 _sig("STORM_last_dense_panels", C.c_uint64, [C.c_void_p])
+_sig("STORM_set_sparse_postings", C.c_int, [C.c_void_p, C.c_int])
+_sig("STORM_last_postings_rows", C.c_uint64, [C.c_void_p])
 
 
 class StormError(RuntimeError):
@@ -361,6 +363,12 @@ class Storm:
 
     def set_dense_block(self, min_density: float, budget_bytes: int = 0):
         _check(_lib.STORM_set_dense_block(self.h, float(min_density), int(budget_bytes)), "STORM_set_dense_block")
+
+    def set_sparse_postings(self, mode: int):
+        _check(_lib.STORM_set_sparse_postings(self.h, int(mode)), "STORM_set_sparse_postings")
+
+    def last_postings_rows(self) -> int:
+        return int(_lib.STORM_last_postings_rows(self.h))
 
     def last_dense(self):
         """(rows, panels) the last all-pairs call gave to the tensor-core block."""

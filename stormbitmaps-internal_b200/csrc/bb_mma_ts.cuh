@@ -77,6 +77,13 @@ __device__ __forceinline__ void expand_a64(uint64_t v, uint32_t* o) {
 // Where count (i, j) of the local rows goes: the packed triangle of these
 // rows, or -- through row_map -- the packed triangle of n_out rows that these
 // rows are a subset of (local row r is row row_map[r] there).
+// Row-mapped launches may hold padding rows, mapped to ~0: nothing of
+// theirs is written.
+template <bool kRowMap>
+__device__ __forceinline__ bool ts_mapped(const uint32_t* row_map, uint64_t i, uint64_t j) {
+    return !kRowMap || (row_map[i] != ~0u && row_map[j] != ~0u);
+}
+
 template <bool kRowMap>
 __device__ __forceinline__ uint64_t ts_out_index(uint64_t n, uint64_t i, uint64_t j, const uint32_t* row_map,
                                                  uint64_t n_out) {
@@ -251,7 +258,7 @@ __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t
                         const uint64_t i = i0 + lane_grp + rr;
                         const uint32_t cnt =
                             buf[rr * 32 + ((((uint32_t)lane >> 2) ^ (rr & 7)) << 2) + (lane & 3)] >> (kW4 ? 3 : 7);
-                        if (i < n && j >= i && j < n) {
+                        if (i < n && j >= i && j < n && ts_mapped<kRowMap>(row_map, i, j)) {
                             if (out) {
                                 uint32_t* dst = out + ts_out_index<kRowMap>(n, i, j, row_map, n_out);
                                 if (partial) atomicAdd(dst, cnt);   // one K segment's share
@@ -278,7 +285,7 @@ __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t
                         for (int e = 0; e < 32; ++e) {
                             const uint64_t j = jb + e;
                             const uint32_t cnt = r[e] >> (kW4 ? 3 : 7);
-                            if (j >= i && j < n) {
+                            if (j >= i && j < n && ts_mapped<kRowMap>(row_map, i, j)) {
                                 if (out) {
                                     uint32_t* dst = out + (kRowMap ? ts_out_index<true>(n, i, j, row_map, n_out)
                                                                    : base + j);

@@ -164,8 +164,12 @@ expand_rows_kernel(ChunkView v, const uint32_t* __restrict__ rows, uint32_t m, u
     const uint32_t slots = W / CHUNK_WORDS;
     for (uint32_t r = blockIdx.x; r < m; r += gridDim.x) {
         const uint32_t row = rows[r];
-        const uint64_t c0 = v.row_off[row], c1 = v.row_off[row + 1];
         uint4* dst_row = reinterpret_cast<uint4*>(X + (uint64_t)r * W);
+        if (row == ~0u) {   // padding row: zeros
+            for (uint64_t q = threadIdx.x; q < (uint64_t)W / 2; q += blockDim.x) dst_row[q] = make_uint4(0, 0, 0, 0);
+            continue;
+        }
+        const uint64_t c0 = v.row_off[row], c1 = v.row_off[row + 1];
         uint64_t pos = c0;
         for (uint32_t s = warp; s < slots; s += EXPAND_WARPS) {
             while (pos < c1 && v.cid[pos] < s) ++pos;   // ids ascend: a forward walk
@@ -197,12 +201,17 @@ expand_rows_kernel(ChunkView v, const uint32_t* __restrict__ rows, uint32_t m, u
     }
 }
 
-// perm (optional) maps the walk's row index to the stored row: with the
-// dense block on, the sparse rows come first and the walk stops after the
-// pairs whose first row is sparse.
+// Pair p of the walk -> rows (i, j), i < j or i == j, as stored:
+//   PAIRS_TRIANGLE  p-th entry of the packed triangle of n1 walk rows (a
+//                   prefix of it when n_pairs < n1 (n1 + 1) / 2);
+//   PAIRS_RECT      walk rows ib + p / n2 and jb + p % n2.
+// perm (optional) maps walk rows to stored rows. Counts land at the packed
+// index of (i, j) in the triangle of n_out rows when out is given; the sum
+// over i != j accumulates into flags->sum.
 __global__ void __launch_bounds__(256)
 chunk_pairs_kernel(ChunkView v, uint32_t mode, uint64_t n1, uint64_t n2, uint64_t n_pairs,
-                   const uint32_t* __restrict__ perm, uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags) {
+                   const uint32_t* __restrict__ perm, uint64_t ib, uint64_t jb, uint64_t n_out,
+                   uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags) {
     const int lane = threadIdx.x & 31;
     const uint64_t wid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -211,14 +220,14 @@ chunk_pairs_kernel(ChunkView v, uint32_t mode, uint64_t n1, uint64_t n2, uint64_
         uint64_t i, j;
         if (mode == PAIRS_TRIANGLE) {
             tri_decode(n1, p, i, j);
-            if (perm) {
-                const uint64_t a = perm[i], b = perm[j];
-                i = a < b ? a : b;
-                j = a < b ? b : a;
-            }
         } else {
-            i = p / n2;
-            j = n1 + p % n2;
+            i = ib + p / n2;
+            j = jb + p % n2;
+        }
+        if (perm) {
+            const uint64_t a = perm[i], b = perm[j];
+            i = a < b ? a : b;
+            j = a < b ? b : a;
         }
         const uint64_t a0 = v.row_off[i], b0 = v.row_off[j];
         const uint32_t na = (uint32_t)(v.row_off[i + 1] - a0), nb = (uint32_t)(v.row_off[j + 1] - b0);
@@ -248,15 +257,161 @@ chunk_pairs_kernel(ChunkView v, uint32_t mode, uint64_t n1, uint64_t n2, uint64_
         }
         cnt = warp_sum_u32(cnt);
         if (lane == 0) {
-            if (mode == PAIRS_TRIANGLE) {
-                if (out) out[tri_index(n1, i, j)] = cnt;
-                if (j > i) local += cnt;
-            } else {
-                local += cnt;
-            }
+            if (out) out[tri_index(n_out, i, j)] = cnt;
+            if (j != i) local += cnt;
         }
     }
     if (lane == 0 && local) atomicAdd(&flags->sum, local);
+}
+
+// ---- postings: pairs of plain rows without bitmap chunks ----------------
+// value of entry e of list chunk c: cid << 16 | entry (universe <= 2^27)
+
+__global__ void postings_hist_kernel(ChunkView v, const uint32_t* __restrict__ rows, uint32_t nq,
+                                     uint32_t* __restrict__ counts) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nq; r += nw) {
+        const uint32_t row = rows[r];
+        for (uint64_t c = v.row_off[row]; c < v.row_off[row + 1]; ++c) {
+            const uint32_t base = v.cid[c] << 16;
+            const uint16_t* l = v.lst + v.coff[c];
+            const uint32_t nl = v.ckl[c] & CK_LEN;
+            for (uint32_t e = lane; e < nl; e += 32) atomicAdd(&counts[base | l[e]], 1u);
+        }
+    }
+}
+
+struct PostingsStats {
+    unsigned long long pairs;     // sum over values of C(rows holding it, 2)
+    unsigned long long lists;     // values held by >= 2 rows
+    unsigned long long entries;   // their rows, summed
+    unsigned long long cursor[2]; // allocation cursors (entries, lists)
+};
+
+__global__ void postings_stats_kernel(const uint32_t* __restrict__ counts, uint64_t U, PostingsStats* st) {
+    unsigned long long p = 0, l = 0, e = 0;
+    for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < U; x += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t c = counts[x];
+        if (c >= 2) {
+            p += (unsigned long long)c * (c - 1) / 2;
+            l += 1;
+            e += c;
+        }
+    }
+    p = warp_sum_u64(p);
+    l = warp_sum_u64(l);
+    e = warp_sum_u64(e);
+    if ((threadIdx.x & 31) == 0 && l) {
+        atomicAdd(&st->pairs, p);
+        atomicAdd(&st->lists, l);
+        atomicAdd(&st->entries, e);
+    }
+}
+
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x, int lane) {
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= d) x += y;
+    }
+    return x;
+}
+
+// Gives every value held by >= 2 rows a slot range in the postings array
+// (start) and a list record; other values get start = ~0. One atomic per
+// warp per 32 values.
+__global__ void postings_alloc_kernel(const uint32_t* __restrict__ counts, uint64_t U, uint32_t* __restrict__ start,
+                                      uint2* __restrict__ lists, PostingsStats* st) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t x0 = (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; x0 < U; x0 += nw * 32) {
+        const uint64_t x = x0 + lane;
+        const uint32_t c = x < U ? counts[x] : 0u;
+        const bool want = c >= 2;
+        const uint32_t n_incl = warp_incl_scan(want ? c : 0u, lane);
+        const uint32_t b = __ballot_sync(0xffffffffu, want);
+        unsigned long long e0 = 0, l0 = 0;
+        if (lane == 31 && b) {
+            e0 = atomicAdd(&st->cursor[0], (unsigned long long)n_incl);
+            l0 = atomicAdd(&st->cursor[1], (unsigned long long)__popc(b));
+        }
+        e0 = __shfl_sync(0xffffffffu, e0, 31);
+        l0 = __shfl_sync(0xffffffffu, l0, 31);
+        if (x < U) {
+            if (want) {
+                const uint32_t s = (uint32_t)(e0 + n_incl - c);
+                start[x] = s;
+                lists[l0 + __popc(b & ((1u << lane) - 1u))] = make_uint2(s, c);
+            } else {
+                start[x] = ~0u;
+            }
+        }
+    }
+}
+
+__global__ void postings_scatter_kernel(ChunkView v, const uint32_t* __restrict__ rows, uint32_t nq,
+                                        uint32_t* __restrict__ counts, const uint32_t* __restrict__ start,
+                                        uint32_t* __restrict__ post) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nq; r += nw) {
+        const uint32_t row = rows[r];
+        for (uint64_t c = v.row_off[row]; c < v.row_off[row + 1]; ++c) {
+            const uint32_t base = v.cid[c] << 16;
+            const uint16_t* l = v.lst + v.coff[c];
+            const uint32_t nl = v.ckl[c] & CK_LEN;
+            for (uint32_t e = lane; e < nl; e += 32) {
+                const uint32_t x = base | l[e];
+                const uint32_t s0 = start[x];
+                if (s0 != ~0u) post[s0 + atomicSub(&counts[x], 1u) - 1u] = row;
+            }
+        }
+    }
+}
+
+// One increment per (pair of rows, shared value): thread per list for lists
+// of up to POST_THREAD_MAX rows, warp per list beyond.
+constexpr uint32_t POST_THREAD_MAX = 64;
+
+__global__ void postings_pairs_kernel(const uint2* __restrict__ lists, uint64_t n_lists,
+                                      const uint32_t* __restrict__ post, uint64_t n, uint32_t* __restrict__ out) {
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t nt = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t li = tid; li < n_lists; li += nt) {
+        const uint2 L = lists[li];
+        if (L.y > POST_THREAD_MAX) continue;
+        for (uint32_t a = 0; a + 1 < L.y; ++a) {
+            const uint32_t ra = post[L.x + a];
+            for (uint32_t b = a + 1; b < L.y; ++b) {
+                const uint32_t rb = post[L.x + b];
+                atomicAdd(&out[ra < rb ? tri_index(n, ra, rb) : tri_index(n, rb, ra)], 1u);
+            }
+        }
+    }
+    const int lane = threadIdx.x & 31;
+    for (uint64_t li = tid >> 5; li < n_lists; li += nt >> 5) {
+        const uint2 L = lists[li];
+        if (L.y <= POST_THREAD_MAX) continue;
+        for (uint32_t a = 0; a + 1 < L.y; ++a) {
+            const uint32_t ra = post[L.x + a];
+            for (uint32_t b = a + 1 + lane; b < L.y; b += 32) {
+                const uint32_t rb = post[L.x + b];
+                atomicAdd(&out[ra < rb ? tri_index(n, ra, rb) : tri_index(n, rb, ra)], 1u);
+            }
+        }
+    }
+}
+
+// Diagonal of the postings rows: their value count.
+__global__ void postings_diag_kernel(ChunkView v, const uint32_t* __restrict__ rows, uint32_t nq, uint64_t n,
+                                     uint32_t* __restrict__ out) {
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < nq; r += gridDim.x * blockDim.x) {
+        const uint32_t row = rows[r];
+        uint32_t card = 0;
+        for (uint64_t c = v.row_off[row]; c < v.row_off[row + 1]; ++c) card += v.ckl[c] & CK_LEN;
+        out[tri_index(n, row, row)] = card;
+    }
 }
 
 uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_t n2, uint32_t* d_out,
@@ -265,79 +420,225 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
     const uint64_t n_pairs_all = mode == PAIRS_TRIANGLE ? tri_size(n1) : n1 * n2;
     log.launches = 0;
     log.last_ms = 0.f;
-    last_dense_rows = last_dense_panels = 0;
+    last_dense_rows = last_dense_panels = last_postings_rows = 0;
     if (n_pairs_all == 0) return 0;
     d_flags.reserve(1);
     SB_CUDA(cudaMemsetAsync(d_flags.p, 0, sizeof(DeviceFlags), st));
     log.ensure();
-
-    // ---- dense block plan (triangle walks only)
-    std::vector<uint32_t> dense;
-    const uint64_t slots = (uint64_t)d.max_cid + 1;
-    const uint64_t W = slots * CHUNK_WORDS;               // words per expanded row
-    uint64_t P = 0;                                        // rows per panel
-    bool single = false;
-    if (mode == PAIRS_TRIANGLE && dense_min_density != 0.0 && slots * 65536 <= TC_MAX_ROW_BITS &&
-        n1 >= 256 && d.facts.size() == n1) {
-        const double min_card = dense_min_density * (double)(slots * 65536);
-        const double tc_ns = tensor_pair_ns(cost, slots);
-        for (uint32_t r = 0; r < n1; ++r) {
-            const ChunkRowFacts& f = d.facts[r];
-            if (!f.plain) continue;
-            const bool joins = dense_min_density > 0.0 ? (double)f.card >= min_card
-                                                       : chunk_self_pair_ns(cost, f, slots) >= tc_ns;
-            if (joins) dense.push_back(r);
-        }
-        if (dense.size() >= 256) {
-            uint64_t budget = dense_budget_bytes;
-            if (!budget) {
-                size_t fr = 0, tot = 0;
-                SB_CUDA(cudaMemGetInfo(&fr, &tot));
-                budget = (uint64_t)(0.6 * (double)(fr + d_panel.n * sizeof(uint64_t)));
-            }
-            const uint64_t cap_rows = budget / (W * sizeof(uint64_t));
-            if (round_up(dense.size(), 256) <= cap_rows) {
-                single = true;
-                P = round_up(dense.size(), 256);
-            } else {
-                P = cap_rows / 2 / 256 * 256;
-            }
-        }
-        if (P == 0) dense.clear();
+    uint32_t launches = 0;
+    auto chunk_launch = [&](uint32_t m, uint64_t np, const uint32_t* perm, uint64_t ib, uint64_t jb, uint64_t nn1,
+                            uint64_t nn2) {
+        if (np == 0) return;
+        const uint64_t want_blocks = (np + 7) / 8;
+        const uint32_t grid = (uint32_t)(want_blocks < (uint64_t)sms * 16 ? want_blocks : (uint64_t)sms * 16);
+        chunk_pairs_kernel<<<grid, 256, 0, st>>>(d.view(), m, nn1, nn2, np, perm, ib, jb, n1, d_out, d_flags.p);
+        SB_CUDA(cudaGetLastError());
+        ++launches;
+    };
+    if (mode == PAIRS_RECT) {   // the rectangle of rows [0, n1) x [n1, n1 + n2): sums only
+        SB_CUDA(cudaEventRecord(log.ev0, st));
+        uint32_t* keep = d_out;
+        d_out = nullptr;
+        chunk_launch(PAIRS_RECT, n_pairs_all, nullptr, 0, n1, n1, n2);
+        d_out = keep;
+        SB_CUDA(cudaEventRecord(log.ev1, st));
+        DeviceFlags f;
+        SB_CUDA(cudaMemcpyAsync(&f, d_flags.p, sizeof(f), cudaMemcpyDeviceToHost, st));
+        SB_CUDA(cudaStreamSynchronize(st));
+        SB_CUDA(cudaEventElapsedTime(&log.last_ms, log.ev0, log.ev1));
+        log.launches = launches;
+        return f.sum;
     }
-    const uint64_t nd = dense.size();
+
+    // ---- row classes: D (tensor cores: every pair with a D row), Q (postings:
+    // pairs of two Q rows), C (chunk kernel: every pair with a C row).
+    const uint64_t n = n1;
+    const uint64_t slots = (uint64_t)d.max_cid + 1;
+    const uint64_t U = slots * 65536;                      // universe of the rows' values
+    const uint64_t W = slots * CHUNK_WORDS;                // words per expanded row
+    const bool facts_ok = d.facts.size() == n;
+    const bool tc_ok = dense_min_density != 0.0 && U <= TC_MAX_ROW_BITS && facts_ok;
+    const bool post_ok = postings_mode != 0 && U <= POSTINGS_MAX_UNIVERSE && facts_ok;
+    const double tc_ns = tensor_pair_ns(cost, slots);
+    std::vector<uint8_t> cls(n, 0);                        // 0 C, 1 Q, 2 D
 
     SB_CUDA(cudaEventRecord(log.ev0, st));
-    uint32_t launches = 0;
-    const uint32_t* perm = nullptr;
-    uint64_t n_pairs = n_pairs_all;
-    if (nd) {
-        // Walk order: sparse rows first, then the dense rows; the chunk
-        // kernel stops after the pairs whose first row is sparse.
-        std::vector<uint32_t> h_perm;
-        h_perm.reserve(n1);
-        std::vector<uint8_t> is_dense(n1, 0);
-        for (uint32_t r : dense) is_dense[r] = 1;
-        for (uint32_t r = 0; r < n1; ++r)
-            if (!is_dense[r]) h_perm.push_back(r);
-        const uint64_t ns = h_perm.size();
-        h_perm.insert(h_perm.end(), dense.begin(), dense.end());
-        d_perm.reserve(n1);
-        SB_CUDA(cudaMemcpyAsync(d_perm.p, h_perm.data(), n1 * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-        perm = d_perm.p;
-        n_pairs = ns * n1 - (ns * (ns - 1)) / 2 * (ns ? 1 : 0);
+    PostingsStats ps{};
+    auto histogram = [&](const std::vector<uint32_t>& rows) {
+        d_qrows.reserve(rows.size());
+        SB_CUDA(cudaMemcpyAsync(d_qrows.p, rows.data(), rows.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        d_counts.reserve(U);
+        d_pstats.reserve(1);
+        SB_CUDA(cudaMemsetAsync(d_counts.p, 0, U * sizeof(uint32_t), st));
+        SB_CUDA(cudaMemsetAsync(d_pstats.p, 0, sizeof(PostingsStats), st));
+        const uint32_t gq = (uint32_t)std::min<uint64_t>((rows.size() + 7) / 8, (uint64_t)sms * 16);
+        postings_hist_kernel<<<gq, 256, 0, st>>>(d.view(), d_qrows.p, (uint32_t)rows.size(), d_counts.p);
+        postings_stats_kernel<<<sms * 8, 256, 0, st>>>(d_counts.p, U, d_pstats.p);
+        SB_CUDA(cudaGetLastError());
+        launches += 2;
+        PostingsStats h{};
+        SB_CUDA(cudaMemcpyAsync(&h, d_pstats.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+        SB_CUDA(cudaStreamSynchronize(st));
+        return h;
+    };
+    // ns of the postings for a set with h increments (the per-pair form;
+    // sums need only the histogram)
+    auto post_ns = [&](double incr) {
+        return (d_out ? incr * cost.ns_per_posting_pair : 0.0) + (double)U * cost.ns_per_universe_value;
+    };
+    std::vector<uint32_t> qrows, dense;
 
+    if (tc_ok && dense_min_density > 0.0) {
+        // Explicit threshold: plain rows with value count >= min_density x U.
+        const double min_card = dense_min_density * (double)U;
+        std::vector<uint32_t> rest;
+        double chunk_rest = 0.0;
+        for (uint32_t r = 0; r < n; ++r) {
+            const ChunkRowFacts& f = d.facts[r];
+            if (!f.plain) continue;
+            if ((double)f.card >= min_card) {
+                dense.push_back(r);
+            } else if (post_ok && f.bitmap_chunks == 0) {
+                rest.push_back(r);
+                chunk_rest += chunk_self_pair_ns(cost, f, slots);
+            }
+        }
+        if (rest.size() >= 2) {
+            ps = histogram(rest);
+            const double alt = 0.5 * ((double)rest.size() - 1.0) * chunk_rest;
+            if (ps.entries < (1ull << 32) && (postings_mode > 0 || post_ns((double)ps.pairs) < alt)) qrows = rest;
+        }
+    } else if (tc_ok && post_ok) {
+        // Cost-chosen cut: plain rows with bitmap chunks go to D; the list
+        // rows, heaviest first, join D while that lowers tensor time (every
+        // pair of a D row) + postings time (pairs of the rest; increments
+        // estimated as for independent uniform rows, sum_{i<j} c_i c_j / U).
+        std::vector<uint32_t> lists;
+        for (uint32_t r = 0; r < n; ++r) {
+            const ChunkRowFacts& f = d.facts[r];
+            if (!f.plain) continue;
+            if (f.bitmap_chunks) dense.push_back(r);
+            else lists.push_back(r);
+        }
+        std::stable_sort(lists.begin(), lists.end(),
+                         [&](uint32_t x, uint32_t y) { return d.facts[x].card > d.facts[y].card; });
+        const double np = (double)(dense.size() + lists.size());
+        double s1 = 0.0, s2 = 0.0;
+        for (uint32_t r : lists) {
+            const double c = (double)d.facts[r].card;
+            s1 += c;
+            s2 += c * c;
+        }
+        auto cost_at = [&](double k, double r1, double r2) {
+            const double tens = k > 0 ? tc_ns * (k * (k - 1.0) / 2.0 + k * (np - k)) : 0.0;
+            return tens + post_ns((r1 * r1 - r2) / (2.0 * (double)U));
+        };
+        size_t best_k = 0;
+        double best = cost_at((double)dense.size(), s1, s2);
+        double r1 = s1, r2 = s2;
+        for (size_t k = 1; k <= lists.size(); ++k) {
+            const double c = (double)d.facts[lists[k - 1]].card;
+            r1 -= c;
+            r2 -= c * c;
+            const double v = cost_at((double)(dense.size() + k), r1, r2);
+            if (v < best) {
+                best = v;
+                best_k = k;
+            }
+        }
+        if (postings_mode > 0) best_k = 0;                 // forced: every list row to the postings
+        std::vector<uint32_t> rest(lists.begin() + best_k, lists.end());
+        dense.insert(dense.end(), lists.begin(), lists.begin() + best_k);
+        if (rest.size() >= 2) {
+            ps = histogram(rest);
+            // The estimate assumes independent rows; correlated rows share
+            // more. With the exact count, keep the postings only if they beat
+            // the tensor cores on these pairs.
+            const double q = (double)rest.size();
+            const double tens_rest = tc_ns * (q * (q - 1.0) / 2.0);
+            if (ps.entries < (1ull << 32) && (postings_mode > 0 || post_ns((double)ps.pairs) < tens_rest)) qrows = rest;
+            else dense.insert(dense.end(), rest.begin(), rest.end());
+        } else {
+            dense.insert(dense.end(), rest.begin(), rest.end());
+        }
+    } else if (tc_ok) {
+        // Per-row rule: plain rows whose chunk-kernel cost against a row
+        // like themselves exceeds a tensor-core pair.
+        for (uint32_t r = 0; r < n; ++r) {
+            const ChunkRowFacts& f = d.facts[r];
+            if (f.plain && chunk_self_pair_ns(cost, f, slots) >= tc_ns) dense.push_back(r);
+        }
+    } else if (post_ok) {
+        std::vector<uint32_t> rest;
+        double chunk_rest = 0.0;
+        for (uint32_t r = 0; r < n; ++r) {
+            const ChunkRowFacts& f = d.facts[r];
+            if (f.plain && f.bitmap_chunks == 0) {
+                rest.push_back(r);
+                chunk_rest += chunk_self_pair_ns(cost, f, slots);
+            }
+        }
+        if (rest.size() >= 2) {
+            ps = histogram(rest);
+            const double alt = 0.5 * ((double)rest.size() - 1.0) * chunk_rest;
+            if (ps.entries < (1ull << 32) && (postings_mode > 0 || post_ns((double)ps.pairs) < alt)) qrows = rest;
+        }
+    }
+    // The tensor cores take D x D and D x Q: expanded rows in the order
+    // [D | padding to a multiple of 256 | Q], so that every 128-row and
+    // 256-row block is all D or all Q and the Q x Q blocks can be left out.
+    // Panels of P rows when they do not all fit the budget.
+    const uint64_t nd0 = dense.size();
+    const uint64_t nd_pad = round_up(nd0, 256);
+    const uint64_t ne = nd0 ? nd_pad + qrows.size() : 0;
+    uint64_t P = 0;
+    if (ne) {
+        uint64_t budget = dense_budget_bytes;
+        if (!budget) {
+            size_t fr = 0, tot = 0;
+            SB_CUDA(cudaMemGetInfo(&fr, &tot));
+            budget = (uint64_t)(0.6 * (double)(fr + d_panel.n * sizeof(uint64_t)));
+        }
+        const uint64_t cap_rows = budget / (W * sizeof(uint64_t));
+        P = round_up(ne, 256) <= cap_rows ? round_up(ne, 256) : cap_rows / 2 / 256 * 256;
+        if (P == 0) {   // not even two panels fit: the D rows go to the chunk kernel
+            dense.clear();
+        }
+    }
+    for (uint32_t r : qrows) cls[r] = 1;
+    for (uint32_t r : dense) cls[r] = 2;
+    // Walk order: C rows, then Q rows, then D rows.
+    std::vector<uint32_t> h_perm;
+    h_perm.reserve(n);
+    for (int k = 0; k < 3; ++k)
+        for (uint32_t r = 0; r < n; ++r)
+            if (cls[r] == k) h_perm.push_back(r);
+    const uint64_t nd = dense.size(), nq = qrows.size(), nc = n - nd - nq;
+    const uint32_t* perm = nullptr;
+    if (nd || nq) {
+        d_perm.reserve(n);
+        SB_CUDA(cudaMemcpyAsync(d_perm.p, h_perm.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        perm = d_perm.p;
+        // The tensor cores (stream-K) and the postings add into the triangle.
+        if (d_out) SB_CUDA(cudaMemsetAsync(d_out, 0, tri_size(n) * sizeof(uint32_t), st));
+    }
+
+    // ---- tensor cores: D x D and D x Q, panel by panel
+    if (nd) {
+        std::vector<uint32_t> emap(nd_pad + nq, ~0u);    // expanded row -> stored row (~0: padding)
+        std::copy(dense.begin(), dense.end(), emap.begin());
+        std::copy(qrows.begin(), qrows.end(), emap.begin() + nd_pad);
+        const uint64_t ne2 = emap.size();
+        const bool single = P >= round_up(ne2, 256);
         const uint64_t rows_alloc = single ? P : 2 * P;
         d_panel.reserve(rows_alloc * W);
         d_map.reserve(rows_alloc);
-        // every tile list below fits: (P / 128) row blocks x (2P / 256) column blocks
         d_tiles.reserve((P / 128) * (2 * P / 256 + 1));
-        // Split-K tensor launches add partial counts: zero the triangle once.
-        if (d_out) SB_CUDA(cudaMemsetAsync(d_out, 0, tri_size(n1) * sizeof(uint32_t), st));
-        const uint64_t npan = single ? 1 : (nd + P - 1) / P;
+        const uint64_t npan = single ? 1 : (ne2 + P - 1) / P;
+        auto is_q = [&](uint64_t global_row) { return global_row >= nd_pad; };
         std::vector<uint2> tl;
         auto expand = [&](uint64_t first, uint64_t m, uint64_t slot) {
-            SB_CUDA(cudaMemcpyAsync(d_map.p + slot, dense.data() + first, m * sizeof(uint32_t),
+            SB_CUDA(cudaMemcpyAsync(d_map.p + slot, emap.data() + first, m * sizeof(uint32_t),
                                     cudaMemcpyHostToDevice, st));
             const uint32_t grid = (uint32_t)std::min<uint64_t>(m, (uint64_t)sms * 16);
             expand_rows_kernel<<<grid, EXPAND_WARPS * 32, 0, st>>>(d.view(), d_map.p + slot, (uint32_t)m,
@@ -346,36 +647,61 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
             ++launches;
         };
         auto tensor = [&](uint64_t n_local) {
+            if (tl.empty()) return;
             SB_CUDA(cudaMemcpyAsync(d_tiles.p, tl.data(), tl.size() * sizeof(uint2), cudaMemcpyHostToDevice, st));
             launch_ts_rows(d_panel.p, (uint32_t)n_local, (uint32_t)W, d_tiles.p, (uint32_t)tl.size(), d_out,
-                           d_flags.p, d_map.p, n1, st, /*out_zeroed=*/true);
+                           d_flags.p, d_map.p, n, st, /*out_zeroed=*/true);
             ++launches;
         };
         for (uint64_t I = 0; I < npan; ++I) {
-            const uint64_t mI = std::min<uint64_t>(P, nd - I * P);
-            expand(I * P, mI, 0);
-            build_mma_tiles(tl, mI);                       // I x I triangle
+            const uint64_t gI = I * P, mI = std::min<uint64_t>(P, ne2 - gI);
+            if (is_q(gI)) break;                          // this and later panels are all Q
+            expand(gI, mI, 0);
+            std::vector<uint2> tri;
+            build_mma_tiles(tri, mI);                      // I x I triangle, Q x Q blocks left out
+            tl.clear();
+            for (const uint2& t : tri)
+                if (!(is_q(gI + (uint64_t)t.x * 128) && is_q(gI + (uint64_t)t.y * 256))) tl.push_back(t);
             tensor(mI);
-            for (uint64_t J = I + 1; J < npan; ++J) {        // I x J rectangle (I is a full panel)
-                const uint64_t mJ = std::min<uint64_t>(P, nd - J * P);
-                expand(J * P, mJ, P);
+            for (uint64_t J = I + 1; J < npan; ++J) {      // I x J rectangle (I is a full panel)
+                const uint64_t gJ = J * P, mJ = std::min<uint64_t>(P, ne2 - gJ);
+                expand(gJ, mJ, P);
                 tl.clear();
-                for (uint32_t bi = 0; bi < P / 128; ++bi)
+                for (uint32_t bi = 0; bi < P / 128; ++bi) {
+                    if (is_q(gI + (uint64_t)bi * 128) && is_q(gJ)) continue;
                     for (uint32_t bj = (uint32_t)(P / 256); bj < (uint32_t)((P + mJ + 255) / 256); ++bj)
-                        tl.push_back(make_uint2(bi, bj));
+                        if (!(is_q(gI + (uint64_t)bi * 128) && is_q(gJ + (uint64_t)bj * 256 - P)))
+                            tl.push_back(make_uint2(bi, bj));
+                }
                 tensor(P + mJ);
             }
         }
         last_dense_rows = nd;
         last_dense_panels = npan;
     }
-    if (n_pairs) {
-        const uint64_t want_blocks = (n_pairs + 7) / 8;
-        const uint32_t grid = (uint32_t)(want_blocks < (uint64_t)sms * 16 ? want_blocks : (uint64_t)sms * 16);
-        chunk_pairs_kernel<<<grid, 256, 0, st>>>(d.view(), (uint32_t)mode, n1, n2, n_pairs, perm, d_out,
-                                                  d_flags.p);
-        SB_CUDA(cudaGetLastError());
-        ++launches;
+    // ---- chunk kernel: every pair with a C row (the walk's triangle prefix)
+    chunk_launch(PAIRS_TRIANGLE, nc * n - (nc * (nc - 1)) / 2 * (nc ? 1 : 0), perm, 0, 0, n, 0);
+    // ---- Q x Q by postings
+    uint64_t q_sum = 0;
+    if (nq) {
+        q_sum = ps.pairs;
+        if (d_out) {
+            d_start.reserve(U);
+            d_lists.reserve(ps.lists ? ps.lists : 1);
+            d_post.reserve(ps.entries ? ps.entries : 1);
+            postings_alloc_kernel<<<sms * 8, 256, 0, st>>>(d_counts.p, U, d_start.p, d_lists.p, d_pstats.p);
+            const uint32_t gq = (uint32_t)std::min<uint64_t>((nq + 7) / 8, (uint64_t)sms * 16);
+            postings_scatter_kernel<<<gq, 256, 0, st>>>(d.view(), d_qrows.p, (uint32_t)nq, d_counts.p, d_start.p,
+                                                        d_post.p);
+            const uint32_t gp = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((ps.lists + 255) / 256,
+                                                                                   (uint64_t)sms * 16));
+            postings_pairs_kernel<<<gp, 256, 0, st>>>(d_lists.p, ps.lists, d_post.p, n, d_out);
+            postings_diag_kernel<<<(uint32_t)std::min<uint64_t>((nq + 255) / 256, (uint64_t)sms * 4), 256, 0, st>>>(
+                d.view(), d_qrows.p, (uint32_t)nq, n, d_out);
+            SB_CUDA(cudaGetLastError());
+            launches += 4;
+        }
+        last_postings_rows = nq;
     }
     SB_CUDA(cudaEventRecord(log.ev1, st));
     DeviceFlags f;
@@ -384,7 +710,7 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
     if (f.error) fail(STORM_B200_ETIMEOUT, "tensor-core dense block: a pipeline wait timed out");
     SB_CUDA(cudaEventElapsedTime(&log.last_ms, log.ev0, log.ev1));
     log.launches = launches;
-    return f.sum;
+    return f.sum + q_sum;
 }
 
 }  // namespace sb200

@@ -87,6 +87,8 @@ struct ChunkDev {
     }
 };
 
+struct PostingsStats;   // chunk_engine.cu
+
 // Pair spaces the chunk kernel walks.
 enum PairMode : uint32_t {
     PAIRS_TRIANGLE = 0,   // i <= j < n, packed output
@@ -113,11 +115,22 @@ struct ChunkCostModel {
     double ns_per_shared_chunk = 0.086;
     double ns_per_lane_iteration = 0.0228;
     double ns_per_tensor_bit = 1.3e-6;
+    double ns_per_posting_pair = 0.05;       // one increment of a (pair, shared value)
+    double ns_per_universe_value = 2e-4;     // histogram clear + scan per universe value
 };
 double chunk_self_pair_ns(const ChunkCostModel& m, const ChunkRowFacts& f, uint64_t slots);
 double tensor_pair_ns(const ChunkCostModel& m, uint64_t slots);
 
 constexpr double CHUNK_DENSE_AUTO = -1.0;
+
+// Postings for the sparse rows (plain rows without bitmap chunks, outside the
+// dense block): a histogram of their values over the universe gives, per
+// value, the rows holding it; each pair of those rows gets one increment
+// per shared value, so pairs with nothing in common cost nothing. Used for
+// the pairs among these rows when the exact increment count (from the
+// histogram) predicts less time than the chunk kernel; sums need only the
+// histogram: the sum over those pairs is sum_v C(rows holding v, 2).
+constexpr uint64_t POSTINGS_MAX_UNIVERSE = 1ull << 27;
 
 struct ChunkEngine {
     DevBuf<DeviceFlags> d_flags;
@@ -125,8 +138,12 @@ struct ChunkEngine {
     double dense_min_density = CHUNK_DENSE_AUTO;
     ChunkCostModel cost;
     uint64_t dense_budget_bytes = 0;   // 0: 60 % of free device memory
-    uint64_t last_dense_rows = 0, last_dense_panels = 0;
+    int postings_mode = -1;            // -1 by cost, 0 never, 1 always (when the rows qualify)
+    uint64_t last_dense_rows = 0, last_dense_panels = 0, last_postings_rows = 0;
     DevBuf<uint32_t> d_perm, d_map;
+    DevBuf<uint32_t> d_qrows, d_counts, d_start, d_post;
+    DevBuf<uint2> d_lists;
+    DevBuf<PostingsStats> d_pstats;
     DevBuf<uint64_t> d_panel;
     DevBuf<uint2> d_tiles;
     ~ChunkEngine() { log.destroy(); }

@@ -551,4 +551,13 @@ int STORM_set_dense_block(STORM_t* s, double min_density, uint64_t budget_bytes)
 uint64_t STORM_last_dense_rows(const STORM_t* s) { return s ? state_of(s)->engine.last_dense_rows : 0; }
 uint64_t STORM_last_dense_panels(const STORM_t* s) { return s ? state_of(s)->engine.last_dense_panels : 0; }
 
+int STORM_set_sparse_postings(STORM_t* s, int mode) {
+    if (s == NULL) return STORM_B200_ENULL;
+    if (mode < -1 || mode > 1) return STORM_B200_EARG;
+    state_of(s)->engine.postings_mode = mode;
+    return 0;
+}
+
+uint64_t STORM_last_postings_rows(const STORM_t* s) { return s ? state_of(s)->engine.last_postings_rows : 0; }
+
 }  // extern "C"

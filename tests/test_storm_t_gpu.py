@@ -133,6 +133,7 @@ def test_tensor_dense_block_matches_chunk_kernel_and_oracle(sb):
     oracle's, and identical with the block switched off."""
     sets = _dense_corpus(300, 150, 1 << 20, 1000, 8000, 91)
     s = build_storm(sb, sets)
+    s.set_sparse_postings(0)                # the dense block alone (postings tested below)
     vals, offs = gen.to_csr(sets)
     want, ws = ol.sets_matrix(vals, offs)
     s.set_dense_block(1.0 / 16384)          # by value count: the 300 dense rows
@@ -159,6 +160,7 @@ def test_tensor_dense_block_in_panels(sb):
     universe = 1 << 20
     sets = _dense_corpus(700, 60, universe, 500, 4000, 92)
     s = build_storm(sb, sets)
+    s.set_sparse_postings(0)                # the dense block alone (postings tested below)
     row_bytes = universe // 8
     s.set_dense_block(1.0 / 16384, 2 * 256 * row_bytes + 4096)
     vals, offs = gen.to_csr(sets)
@@ -177,6 +179,7 @@ def test_tensor_dense_block_rows_with_repeats_stay_on_chunks(sb):
     sets = _dense_corpus(280, 20, 1 << 18, 300, 3000, 93)
     dup_rows = [3, 50, 120]
     s = sb.Storm()
+    s.set_sparse_postings(0)
     for k, v in enumerate(sets):
         if k in dup_rows:
             v = np.sort(np.concatenate([v, v[:7]]))
@@ -195,9 +198,95 @@ def test_tensor_dense_block_long_universe(sb):
     4-byte weight cycle) with Bernoulli(1e-3) rows."""
     sets = gen.bernoulli_sets(260, 1 << 24, 1e-3, 94)
     s = build_storm(sb, sets)
+    s.set_sparse_postings(0)                # the dense block alone (postings tested below)
     vals, offs = gen.to_csr(sets)
     want, ws = ol.sets_matrix(vals, offs)
     mat, ssum = s.matrix()
     assert s.last_dense()[0] == 260
     assert ssum == ws
     np.testing.assert_array_equal(mat, want)
+
+
+def test_postings_sparse_rows_match_oracle(sb):
+    """Sparse plain rows through the postings (value histogram, one increment
+    per pair and shared value): forced, automatic and off agree with the
+    oracle, for the per-pair matrix and the sum."""
+    sets = gen.bernoulli_sets(400, 1 << 20, 2e-4, 95) + gen.bernoulli_sets(100, 1 << 20, 3e-5, 96)
+    s = build_storm(sb, sets)
+    s.set_dense_block(0.0)
+    vals, offs = gen.to_csr(sets)
+    want, ws = ol.sets_matrix(vals, offs)
+    for mode in (1, -1, 0):
+        s.set_sparse_postings(mode)
+        mat, ssum = s.matrix()
+        if mode == 1:
+            assert s.last_postings_rows() == len(sets)
+        if mode == 0:
+            assert s.last_postings_rows() == 0
+        assert ssum == ws, mode
+        np.testing.assert_array_equal(mat, want, err_msg=str(mode))
+        assert s.pairw_intersect_cardinality() == ws
+
+
+def test_postings_with_dense_block_and_chunk_rows(sb):
+    """All three row classes at once -- tensor-core dense block, postings
+    rows, and rows that must stay on the chunk kernel (repeated list values)
+    -- give the same counts as the chunk kernel alone."""
+    g = gen.rng(97)
+    # dense rows with bitmap chunks (>= 4096 values per 65536-bit chunk)
+    sets = [gen.uniform_set(g, int(g.integers(70000, 200000)), 1 << 20) for _ in range(280)]
+    sets += [gen.uniform_set(g, int(g.integers(1, 40)), 1 << 20) for _ in range(150)]
+    dup = [np.sort(np.concatenate([v, v[:3]])) for v in
+           (gen.uniform_set(g, int(g.integers(20, 60)), 1 << 20) for _ in range(4))]
+    sets += dup
+    sets = [sets[k] for k in g.permutation(len(sets))]
+    s = build_storm(sb, sets)
+    s.set_dense_block(1.0 / 16384)
+    s.set_sparse_postings(1)
+    mat, ssum = s.matrix()
+    assert s.last_dense()[0] == 280 and s.last_postings_rows() == 150
+    s.set_dense_block(0.0)
+    s.set_sparse_postings(0)
+    mat0, s0 = s.matrix()
+    assert s.last_dense()[0] == 0 and s.last_postings_rows() == 0
+    assert ssum == s0
+    np.testing.assert_array_equal(mat, mat0)
+    s.set_dense_block(1.0 / 16384)
+    s.set_sparse_postings(1)
+    assert s.pairw_intersect_cardinality() == s0
+
+
+def test_tensor_rows_with_postings_in_panels(sb):
+    """Heavy rows on the tensor cores for all their pairs (heavy x heavy and
+    heavy x light, the light rows expanded too), light x light pairs by the
+    postings; a budget of two 256-row panels makes the expanded order
+    [heavy | padding | light] span four panels."""
+    universe = 1 << 20
+    g = gen.rng(98)
+    sets = [gen.uniform_set(g, int(g.integers(2000, 6000)), universe) for _ in range(300)]
+    sets += [gen.uniform_set(g, int(g.integers(5, 50)), universe) for _ in range(300)]
+    sets = [sets[k] for k in g.permutation(len(sets))]
+    s = build_storm(sb, sets)
+    s.set_dense_block(1.0 / 1024, 2 * 256 * (universe // 8) + 4096)
+    s.set_sparse_postings(1)
+    vals, offs = gen.to_csr(sets)
+    want, ws = ol.sets_matrix(vals, offs)
+    mat, ssum = s.matrix()
+    assert s.last_dense() == (300, 4) and s.last_postings_rows() == 300
+    assert ssum == ws
+    np.testing.assert_array_equal(mat, want)
+    assert s.pairw_intersect_cardinality() == ws
+
+
+def test_default_plan_on_mixed_rows_matches_oracle(sb):
+    """The default plan (cost-chosen cut between tensor rows and postings
+    rows) on Zipf-distributed rows."""
+    sets = gen.zipf_sets(600, 1 << 20, 1.1, 16, 1 << 15, 99)
+    s = build_storm(sb, sets)
+    vals, offs = gen.to_csr(sets)
+    want, ws = ol.sets_matrix(vals, offs)
+    mat, ssum = s.matrix()
+    assert s.last_dense()[0] + s.last_postings_rows() > 0
+    assert ssum == ws
+    np.testing.assert_array_equal(mat, want)
+    assert s.pairw_intersect_cardinality() == ws
