@@ -447,11 +447,41 @@ def chunk_alg_bytes(sets):
     return float(np.sum(np.maximum(n_c - 1, 0) * s_c))
 
 
-def storm_t_forms(device, cpu_seconds=2.0):
-    """STORM_t (the reference's chunked rows, storm.h:158-178) all-pairs sum
-    on config-3/4/5-shaped corpora at reduced N: the chunk kernel alone (the
-    plain per-pair GPU form), the default form (tensor-core dense block chosen
-    by the chunk cost model), and the reference's STORM_pairw_intersect_
+def sparse_bernoulli_sets_gpu(n, universe, density, seed, device, chunk_rows=2048):
+    """Rows of about Bernoulli(density) over [0, universe) for small densities,
+    generated in bulk on the GPU: Binomial(universe, density) draws per row,
+    uniform positions, sorted, repeats within a row removed (about k^2 / 2U
+    per row of k values). Sorted u32 numpy arrays."""
+    import torch
+    g = np.random.Generator(np.random.PCG64(seed))
+    tg = torch.Generator(device=device)
+    tg.manual_seed(seed)
+    cards = g.binomial(universe, density, size=n)
+    out = []
+    for r0 in range(0, n, chunk_rows):
+        k = torch.from_numpy(cards[r0:r0 + chunk_rows].astype(np.int64)).to(device)
+        row = torch.repeat_interleave(torch.arange(len(k), device=device), k)
+        pos = torch.randint(0, universe, (int(k.sum().item()),), generator=tg, device=device)
+        key = torch.unique(row * universe + pos)                  # sorted, repeats removed
+        rr = (key // universe).cpu().numpy()
+        vv = (key % universe).to(torch.int64).cpu().numpy().astype(np.uint32)
+        cuts = np.searchsorted(rr, np.arange(len(k) + 1))
+        out.extend(vv[cuts[i]:cuts[i + 1]] for i in range(len(k)))
+    return out
+
+
+STORM_T_CASES = ("zipf_2^24", "runs_2^26", "haplotypes_20000", "bernoulli_1e-06_2^24_N20000",
+                 "bernoulli_1e-05_2^24_N20000", "bernoulli_0.0001_2^24_N20000", "bernoulli_0.001_2^24_N20000",
+                 "bernoulli_0.01_2^24", "bernoulli_0.17_2^24")
+
+
+def storm_t_forms(device, cpu_seconds=2.0, only=None):
+    """STORM_t (the reference's chunked rows, storm.h:158-178) all-pairs on
+    config-3/4/5-shaped corpora: per-pair counts (the packed triangle, i <= j)
+    by the chunk kernel alone (the plain per-pair GPU form, at N <= 4096) and
+    by the default plan (tensor cores for the heavy rows' pairs, value
+    postings for pairs of light rows, chunk kernel for the rest), the default
+    plan's sum-only call, and the reference's STORM_pairw_intersect_
     cardinality on 1 core over a prefix of the rows (all-pairs call only)."""
     import ctypes as C
     import importlib
@@ -461,44 +491,64 @@ def storm_t_forms(device, cpu_seconds=2.0):
     R = ol.reference()
     corpora = [
         ("zipf_2^24", lambda: zipf_sets_gpu(4096, 1 << 24, 1.1, 16, 1 << 22, 0xC0F3, device),
-         "4096 rows over 2^24, card ~ Zipf(1.1) on [16, 2^22]"),
-        ("runs_2^26", lambda: run_sets_gpu(2048, 1 << 26, 200, 256, 0xC0F4, device),
-         "2048 rows over 2^26, Poisson(200) runs of Geometric(mean 256)"),
+         "config 3 shape, N reduced: 4096 rows over 2^24, card ~ Zipf(1.1) on [16, 2^22]"),
+        ("runs_2^26", lambda: run_sets_gpu(8192, 1 << 26, 200, 256, 0xC0F4, device),
+         "config 4 shape, N reduced: 8192 rows over 2^26, Poisson(200) runs of Geometric(mean 256)"),
         ("haplotypes_20000", lambda: [np.flatnonzero(np.unpackbits(r.view(np.uint8), bitorder="little"))
                                       .astype(np.uint32) for r in
                                       haplotype_rows_gpu(8192, 20000, 32, 0xC0F5, device).cpu().numpy()],
-         "8192 sites x 20000 haplotypes, P(k) ~ 1/k, 32-haplotype carrier blocks"),
+         "config 5a shape, N reduced: 8192 sites x 20000 haplotypes, P(k) ~ 1/k, 32-haplotype carrier blocks"),
     ]
-    for d, nn in ((1e-6, 4096), (1e-5, 4096), (1e-4, 4096), (1e-3, 2048), (1e-2, 2048), (0.17, 1024)):
+    for d in (1e-6, 1e-5, 1e-4, 1e-3):
+        corpora.append((f"bernoulli_{d:g}_2^24_N20000",
+                        (lambda d=d: sparse_bernoulli_sets_gpu(20000, 1 << 24, d, int(1e7 * d) + 5, device)),
+                        f"config 5b at full N: 20000 rows over 2^24, Bernoulli({d:g})"))
+    for d, nn in ((1e-2, 2048), (0.17, 1024)):
         corpora.append((f"bernoulli_{d:g}_2^24",
                         (lambda d=d, nn=nn: bernoulli_sets_gpu(nn, 1 << 24, d, int(1e7 * d) + 5, device)),
-                        f"{nn} rows over 2^24, Bernoulli({d:g})"))
+                        f"config 5b, N reduced: {nn} rows over 2^24, Bernoulli({d:g})"))
+    assert [c[0] for c in corpora] == list(STORM_T_CASES)
     out = {}
     for name, make, desc in corpora:
+        if only is not None and name != only:
+            continue
+        t0 = time.perf_counter()
         sets = make()
         n = len(sets)
-        pairs = n * (n - 1) // 2
+        pairs = n * (n + 1) // 2
         s = sb.Storm()
         for v in sets:
             s.add(v)
         s.upload()
-        res = {"workload": desc, "pairs_i_lt_j": pairs}
+        res = {"workload": desc, "pairs_i_le_j": pairs, "setup_s": round(time.perf_counter() - t0, 1)}
         sums = set()
-        for form, thr in (("gpu_chunk_kernel", 0.0), ("gpu_default", -1.0)):
+        forms = [("gpu_default", -1.0, -1)]
+        if n <= 4096:
+            forms.insert(0, ("gpu_chunk_kernel", 0.0, 0))
+        buf = np.zeros(pairs, np.uint32)
+        for form, thr, post in forms:
             s.set_dense_block(thr)
+            s.set_sparse_postings(post)
             best = None
             for _ in range(2):
-                sums.add(s.pairw_intersect_cardinality())
+                _, v = s.matrix(buf)
+                sums.add(v)
                 ms = s.last_kernel_ms()
                 best = ms if best is None else min(best, ms)
             res[form] = {"pairs_per_s": pairs / (best * 1e-3), "ms": round(best, 3),
-                         "dense_rows": s.last_dense()[0]}
+                         "tensor_rows": s.last_dense()[0], "postings_rows": s.last_postings_rows()}
+        best = None
+        for _ in range(2):
+            sums.add(s.pairw_intersect_cardinality())
+            ms = s.last_kernel_ms()
+            best = ms if best is None else min(best, ms)
+        res["gpu_default_sum_only_ms"] = round(best, 3)
         s.close()
         if len(sums) != 1:
             raise RuntimeError(f"{name}: forms disagree {sums}")
         alg = chunk_alg_bytes(sets)
         res["alg_bytes"] = alg
-        for form in ("gpu_chunk_kernel", "gpu_default"):
+        for form, _, _ in forms:
             res[form]["alg_GBps"] = alg / (res[form]["ms"] * 1e-3) / 1e9
         if R is not None:
             k, rate, secs = 64, None, 0.0
@@ -515,11 +565,14 @@ def storm_t_forms(device, cpu_seconds=2.0):
                     break
                 k *= 2
             res["cpu_reference"] = {"pairs_per_s": rate, "cores": 1,
-                                    "sample": f"first {k} rows ({k * (k - 1) // 2} pairs, {secs:.2f} s), "
+                                    "sample": f"first {k} rows ({k * (k - 1) // 2} pairs i < j, {secs:.2f} s), "
                                               f"STORM_pairw_intersect_cardinality as shipped (all-pairs call only)"}
             res["gpu_default_over_cpu"] = res["gpu_default"]["pairs_per_s"] / rate
-        res["gpu_default_over_chunk_kernel"] = res["gpu_default"]["pairs_per_s"] / res["gpu_chunk_kernel"]["pairs_per_s"]
+        if "gpu_chunk_kernel" in res:
+            res["gpu_default_over_chunk_kernel"] = (res["gpu_default"]["pairs_per_s"] /
+                                                    res["gpu_chunk_kernel"]["pairs_per_s"])
         out[name] = res
+        del sets
     return out
 
 
@@ -754,7 +807,13 @@ def main():
                     help="skip the mixed-density learned/plain/CPU comparison")
     ap.add_argument("--traffic", type=float, default=None,
                     help="dram bytes per launch of the dominant kernel from an ncu capture")
+    ap.add_argument("--storm-t-case", default=None, choices=STORM_T_CASES,
+                    help="run only this STORM_t corpus of the forms (one JSON line) and exit")
     args = ap.parse_args()
+    if args.storm_t_case:
+        import torch
+        print(json.dumps({"storm_t": storm_t_forms(torch.device("cuda", 0), only=args.storm_t_case)}), flush=True)
+        return 0
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_b200_arm(args)

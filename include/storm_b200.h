@@ -170,7 +170,13 @@ uint64_t STORM_last_dense_panels(const STORM_t* s);
  * most 2^27 values), and each pair of them gets one increment per shared
  * value -- pairs with nothing in common cost nothing.  mode -1 (default):
  * used when the exact increment count predicts less time than the chunk
- * kernel; 1: whenever rows qualify; 0: never.  Counts are identical. */
+ * kernel; 1: whenever rows qualify; 0: never.  Per-pair counts take one of
+ * two forms: the increments go list by list into the output, or -- for
+ * outputs larger than L2, at most 53248 postings rows, and when predicted
+ * faster from the exact increment count -- a row sweep counts each row's
+ * partners in shared memory and writes its slice once.  Modes 2
+ * and 3 force the rows in and pick the list-by-list or the row-sweep form.
+ * Counts are identical. */
 int STORM_set_sparse_postings(STORM_t* s, int mode);
 uint64_t STORM_last_postings_rows(const STORM_t* s);
 

@@ -345,8 +345,9 @@ class Storm:
     def serialized_size(self) -> int:
         return int(_lib.STORM_serialized_size(self.h))
 
-    def matrix(self):
-        out = np.zeros(max(1, tri_size(self.n)), dtype=np.uint32)
+    def matrix(self, out: np.ndarray | None = None):
+        if out is None:
+            out = np.zeros(max(1, tri_size(self.n)), dtype=np.uint32)
         s = C.c_uint64(0)
         _check(_lib.STORM_pairw_intersect_matrix(self.h, _p(out, u32p), out.size, C.byref(s)),
                "STORM_pairw_intersect_matrix")

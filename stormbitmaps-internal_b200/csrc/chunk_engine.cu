@@ -350,9 +350,10 @@ __global__ void postings_alloc_kernel(const uint32_t* __restrict__ counts, uint6
     }
 }
 
+// Writes each Q row's position in the Q list (its local index) into the
+// lists of its values; start[x] advances to the end of x's list.
 __global__ void postings_scatter_kernel(ChunkView v, const uint32_t* __restrict__ rows, uint32_t nq,
-                                        uint32_t* __restrict__ counts, const uint32_t* __restrict__ start,
-                                        uint32_t* __restrict__ post) {
+                                        uint32_t* __restrict__ start, uint32_t* __restrict__ post) {
     const int lane = threadIdx.x & 31;
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nq; r += nw) {
@@ -363,8 +364,7 @@ __global__ void postings_scatter_kernel(ChunkView v, const uint32_t* __restrict_
             const uint32_t nl = v.ckl[c] & CK_LEN;
             for (uint32_t e = lane; e < nl; e += 32) {
                 const uint32_t x = base | l[e];
-                const uint32_t s0 = start[x];
-                if (s0 != ~0u) post[s0 + atomicSub(&counts[x], 1u) - 1u] = row;
+                if (start[x] != ~0u) post[atomicAdd(&start[x], 1u)] = r;
             }
         }
     }
@@ -375,16 +375,17 @@ __global__ void postings_scatter_kernel(ChunkView v, const uint32_t* __restrict_
 constexpr uint32_t POST_THREAD_MAX = 64;
 
 __global__ void postings_pairs_kernel(const uint2* __restrict__ lists, uint64_t n_lists,
-                                      const uint32_t* __restrict__ post, uint64_t n, uint32_t* __restrict__ out) {
+                                      const uint32_t* __restrict__ post, const uint32_t* __restrict__ qrows,
+                                      uint64_t n, uint32_t* __restrict__ out) {
     const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     const uint64_t nt = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t li = tid; li < n_lists; li += nt) {
         const uint2 L = lists[li];
         if (L.y > POST_THREAD_MAX) continue;
         for (uint32_t a = 0; a + 1 < L.y; ++a) {
-            const uint32_t ra = post[L.x + a];
+            const uint32_t ra = qrows[post[L.x + a]];
             for (uint32_t b = a + 1; b < L.y; ++b) {
-                const uint32_t rb = post[L.x + b];
+                const uint32_t rb = qrows[post[L.x + b]];
                 atomicAdd(&out[ra < rb ? tri_index(n, ra, rb) : tri_index(n, rb, ra)], 1u);
             }
         }
@@ -394,12 +395,62 @@ __global__ void postings_pairs_kernel(const uint2* __restrict__ lists, uint64_t 
         const uint2 L = lists[li];
         if (L.y <= POST_THREAD_MAX) continue;
         for (uint32_t a = 0; a + 1 < L.y; ++a) {
-            const uint32_t ra = post[L.x + a];
+            const uint32_t ra = qrows[post[L.x + a]];
             for (uint32_t b = a + 1 + lane; b < L.y; b += 32) {
-                const uint32_t rb = post[L.x + b];
+                const uint32_t rb = qrows[post[L.x + b]];
                 atomicAdd(&out[ra < rb ? tri_index(n, ra, rb) : tri_index(n, rb, ra)], 1u);
             }
         }
+    }
+}
+
+// Row sweep: CTA per Q row a; for every value of a, the rows b > a on that
+// value's list get one shared-memory increment; then a's slice of the
+// triangle (its Q partners b > a and its diagonal) is written once, in
+// ascending order. Needs nq counters in shared memory; lists hold local
+// indices, list x is [end[x] - counts[x], end[x]).
+constexpr uint32_t POST_SWEEP_THREADS = 256;
+constexpr uint32_t POST_SWEEP_MAX_ROWS = 53248;   // 208 KiB of counters
+
+__global__ void __launch_bounds__(POST_SWEEP_THREADS)
+postings_rows_kernel(ChunkView v, const uint32_t* __restrict__ qrows, uint32_t nq, const uint32_t* __restrict__ counts,
+                     const uint32_t* __restrict__ end, const uint32_t* __restrict__ post, uint64_t n,
+                     uint32_t* __restrict__ out) {
+    extern __shared__ uint32_t cnt[];
+    __shared__ uint32_t card;
+    for (uint32_t a = blockIdx.x; a < nq; a += gridDim.x) {
+        for (uint32_t b = threadIdx.x; b < nq; b += blockDim.x) cnt[b] = 0;
+        if (threadIdx.x == 0) card = 0;
+        __syncthreads();
+        const uint32_t row = qrows[a];
+        const uint64_t c0 = v.row_off[row], c1 = v.row_off[row + 1];
+        uint32_t mine = 0;
+        // a thread per chunk (chunks of a sparse row are many and short)
+        for (uint64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+            const uint32_t base = v.cid[c] << 16;
+            const uint16_t* l = v.lst + v.coff[c];
+            const uint32_t nl = v.ckl[c] & CK_LEN;
+            mine += nl;
+            for (uint32_t e = 0; e < nl; ++e) {
+                const uint32_t x = base | l[e];
+                const uint32_t len = counts[x];
+                if (len < 2) continue;
+                const uint32_t e1 = end[x];
+                for (uint32_t k = e1 - len; k < e1; ++k) {
+                    const uint32_t b = post[k];
+                    if (b > a) atomicAdd(&cnt[b], 1u);
+                }
+            }
+        }
+        if (mine) atomicAdd(&card, mine);
+        __syncthreads();
+        const uint64_t base = tri_index(n, row, row) - row;   // out index of (row, j) is base + j
+        for (uint32_t b = a + 1 + threadIdx.x; b < nq; b += blockDim.x) {
+            const uint32_t gb = qrows[b];   // ascending: gb > row (the other order kept exact too)
+            out[gb > row ? base + gb : tri_index(n, gb, row)] = cnt[b];
+        }
+        if (threadIdx.x == 0) out[base + row] = card;
+        __syncthreads();
     }
 }
 
@@ -481,10 +532,23 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         SB_CUDA(cudaStreamSynchronize(st));
         return h;
     };
-    // ns of the postings for a set with h increments (the per-pair form;
-    // sums need only the histogram)
-    auto post_ns = [&](double incr) {
-        return (d_out ? incr * cost.ns_per_posting_pair : 0.0) + (double)U * cost.ns_per_universe_value;
+    // Per-pair form of the postings: list by list into the output while the
+    // triangle fits in L2 (its atomics stay on chip), else the row sweep
+    // (partners counted in shared memory, each output written once).
+    const bool big_out = tri_size(n) * sizeof(uint32_t) > L2_BYTES_B200;
+    const double c_list = big_out ? cost.ns_per_posting_pair_hbm : cost.ns_per_posting_pair;
+    auto sweep_ns = [&](double incr, uint64_t q) {
+        return (double)q * (double)q * cost.ns_per_sweep_row_pair + incr * cost.ns_per_posting_sweep;
+    };
+    auto sweep_form = [&](double incr, uint64_t q) {
+        if (q > POST_SWEEP_MAX_ROWS || postings_mode == 2) return false;
+        return postings_mode == 3 || (big_out && sweep_ns(incr, q) < incr * c_list);
+    };
+    // ns of the postings for a set of q rows with incr increments (sums need
+    // only the histogram)
+    auto post_ns = [&](double incr, uint64_t q) {
+        const double per_pair = sweep_form(incr, q) ? sweep_ns(incr, q) : incr * c_list;
+        return (d_out ? per_pair : 0.0) + (double)U * cost.ns_per_universe_value;
     };
     std::vector<uint32_t> qrows, dense;
 
@@ -506,7 +570,7 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         if (rest.size() >= 2) {
             ps = histogram(rest);
             const double alt = 0.5 * ((double)rest.size() - 1.0) * chunk_rest;
-            if (ps.entries < (1ull << 32) && (postings_mode > 0 || post_ns((double)ps.pairs) < alt)) qrows = rest;
+            if (ps.entries < (1ull << 32) && (postings_mode > 0 || post_ns((double)ps.pairs, rest.size()) < alt)) qrows = rest;
         }
     } else if (tc_ok && post_ok) {
         // Cost-chosen cut: plain rows with bitmap chunks go to D; the list
@@ -531,7 +595,7 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         }
         auto cost_at = [&](double k, double r1, double r2) {
             const double tens = k > 0 ? tc_ns * (k * (k - 1.0) / 2.0 + k * (np - k)) : 0.0;
-            return tens + post_ns((r1 * r1 - r2) / (2.0 * (double)U));
+            return tens + post_ns((r1 * r1 - r2) / (2.0 * (double)U), (uint64_t)(np - k));
         };
         size_t best_k = 0;
         double best = cost_at((double)dense.size(), s1, s2);
@@ -548,6 +612,7 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         }
         if (postings_mode > 0) best_k = 0;                 // forced: every list row to the postings
         std::vector<uint32_t> rest(lists.begin() + best_k, lists.end());
+        std::sort(rest.begin(), rest.end());             // stored order: ascending output writes
         dense.insert(dense.end(), lists.begin(), lists.begin() + best_k);
         if (rest.size() >= 2) {
             ps = histogram(rest);
@@ -556,7 +621,7 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
             // the tensor cores on these pairs.
             const double q = (double)rest.size();
             const double tens_rest = tc_ns * (q * (q - 1.0) / 2.0);
-            if (ps.entries < (1ull << 32) && (postings_mode > 0 || post_ns((double)ps.pairs) < tens_rest)) qrows = rest;
+            if (ps.entries < (1ull << 32) && (postings_mode > 0 || post_ns((double)ps.pairs, rest.size()) < tens_rest)) qrows = rest;
             else dense.insert(dense.end(), rest.begin(), rest.end());
         } else {
             dense.insert(dense.end(), rest.begin(), rest.end());
@@ -581,7 +646,7 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         if (rest.size() >= 2) {
             ps = histogram(rest);
             const double alt = 0.5 * ((double)rest.size() - 1.0) * chunk_rest;
-            if (ps.entries < (1ull << 32) && (postings_mode > 0 || post_ns((double)ps.pairs) < alt)) qrows = rest;
+            if (ps.entries < (1ull << 32) && (postings_mode > 0 || post_ns((double)ps.pairs, rest.size()) < alt)) qrows = rest;
         }
     }
     // The tensor cores take D x D and D x Q: expanded rows in the order
@@ -685,21 +750,35 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
     uint64_t q_sum = 0;
     if (nq) {
         q_sum = ps.pairs;
+        const bool sweep = sweep_form((double)ps.pairs, nq);
         if (d_out) {
             d_start.reserve(U);
             d_lists.reserve(ps.lists ? ps.lists : 1);
             d_post.reserve(ps.entries ? ps.entries : 1);
             postings_alloc_kernel<<<sms * 8, 256, 0, st>>>(d_counts.p, U, d_start.p, d_lists.p, d_pstats.p);
             const uint32_t gq = (uint32_t)std::min<uint64_t>((nq + 7) / 8, (uint64_t)sms * 16);
-            postings_scatter_kernel<<<gq, 256, 0, st>>>(d.view(), d_qrows.p, (uint32_t)nq, d_counts.p, d_start.p,
-                                                        d_post.p);
-            const uint32_t gp = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((ps.lists + 255) / 256,
-                                                                                   (uint64_t)sms * 16));
-            postings_pairs_kernel<<<gp, 256, 0, st>>>(d_lists.p, ps.lists, d_post.p, n, d_out);
-            postings_diag_kernel<<<(uint32_t)std::min<uint64_t>((nq + 255) / 256, (uint64_t)sms * 4), 256, 0, st>>>(
-                d.view(), d_qrows.p, (uint32_t)nq, n, d_out);
+            postings_scatter_kernel<<<gq, 256, 0, st>>>(d.view(), d_qrows.p, (uint32_t)nq, d_start.p, d_post.p);
+            if (sweep) {
+                const uint32_t smem = (uint32_t)(nq * sizeof(uint32_t));
+                static bool attr = false;
+                if (!attr) {
+                    SB_CUDA(cudaFuncSetAttribute(postings_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)(POST_SWEEP_MAX_ROWS * sizeof(uint32_t))));
+                    attr = true;
+                }
+                const uint32_t gr = (uint32_t)std::min<uint64_t>(nq, (uint64_t)sms * 8);
+                postings_rows_kernel<<<gr, POST_SWEEP_THREADS, smem, st>>>(d.view(), d_qrows.p, (uint32_t)nq,
+                                                                           d_counts.p, d_start.p, d_post.p, n, d_out);
+                launches += 3;
+            } else {
+                const uint32_t gp = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((ps.lists + 255) / 256,
+                                                                                       (uint64_t)sms * 16));
+                postings_pairs_kernel<<<gp, 256, 0, st>>>(d_lists.p, ps.lists, d_post.p, d_qrows.p, n, d_out);
+                postings_diag_kernel<<<(uint32_t)std::min<uint64_t>((nq + 255) / 256, (uint64_t)sms * 4), 256, 0,
+                                       st>>>(d.view(), d_qrows.p, (uint32_t)nq, n, d_out);
+                launches += 4;
+            }
             SB_CUDA(cudaGetLastError());
-            launches += 4;
         }
         last_postings_rows = nq;
     }

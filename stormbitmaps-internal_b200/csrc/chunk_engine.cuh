@@ -115,7 +115,10 @@ struct ChunkCostModel {
     double ns_per_shared_chunk = 0.086;
     double ns_per_lane_iteration = 0.0228;
     double ns_per_tensor_bit = 1.3e-6;
-    double ns_per_posting_pair = 0.05;       // one increment of a (pair, shared value)
+    double ns_per_posting_pair = 0.05;       // one (pair, shared value) increment, output in L2
+    double ns_per_posting_pair_hbm = 0.042;  // the same, output larger than L2
+    double ns_per_posting_sweep = 0.016;     // the same in the row sweep (shared memory)
+    double ns_per_sweep_row_pair = 0.0047;   // row sweep: clearing and writing, per (row, row)
     double ns_per_universe_value = 2e-4;     // histogram clear + scan per universe value
 };
 double chunk_self_pair_ns(const ChunkCostModel& m, const ChunkRowFacts& f, uint64_t slots);
@@ -131,6 +134,7 @@ constexpr double CHUNK_DENSE_AUTO = -1.0;
 // histogram) predicts less time than the chunk kernel; sums need only the
 // histogram: the sum over those pairs is sum_v C(rows holding v, 2).
 constexpr uint64_t POSTINGS_MAX_UNIVERSE = 1ull << 27;
+constexpr uint64_t L2_BYTES_B200 = 126ull << 20;
 
 struct ChunkEngine {
     DevBuf<DeviceFlags> d_flags;
@@ -138,7 +142,8 @@ struct ChunkEngine {
     double dense_min_density = CHUNK_DENSE_AUTO;
     ChunkCostModel cost;
     uint64_t dense_budget_bytes = 0;   // 0: 60 % of free device memory
-    int postings_mode = -1;            // -1 by cost, 0 never, 1 always (when the rows qualify)
+    int postings_mode = -1;            // -1 by cost, 0 never, 1 always (when the rows qualify);
+                                       // 2 / 3 always, per-pair form list by list / row sweep
     uint64_t last_dense_rows = 0, last_dense_panels = 0, last_postings_rows = 0;
     DevBuf<uint32_t> d_perm, d_map;
     DevBuf<uint32_t> d_qrows, d_counts, d_start, d_post;

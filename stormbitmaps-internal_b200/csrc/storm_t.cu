@@ -553,7 +553,7 @@ uint64_t STORM_last_dense_panels(const STORM_t* s) { return s ? state_of(s)->eng
 
 int STORM_set_sparse_postings(STORM_t* s, int mode) {
     if (s == NULL) return STORM_B200_ENULL;
-    if (mode < -1 || mode > 1) return STORM_B200_EARG;
+    if (mode < -1 || mode > 3) return STORM_B200_EARG;
     state_of(s)->engine.postings_mode = mode;
     return 0;
 }

@@ -209,17 +209,18 @@ def test_tensor_dense_block_long_universe(sb):
 
 def test_postings_sparse_rows_match_oracle(sb):
     """Sparse plain rows through the postings (value histogram, one increment
-    per pair and shared value): forced, automatic and off agree with the
-    oracle, for the per-pair matrix and the sum."""
+    per pair and shared value): forced (row sweep in shared memory, and list
+    by list into the output), automatic and off agree with the oracle, for
+    the per-pair matrix and the sum."""
     sets = gen.bernoulli_sets(400, 1 << 20, 2e-4, 95) + gen.bernoulli_sets(100, 1 << 20, 3e-5, 96)
     s = build_storm(sb, sets)
     s.set_dense_block(0.0)
     vals, offs = gen.to_csr(sets)
     want, ws = ol.sets_matrix(vals, offs)
-    for mode in (1, -1, 0):
+    for mode in (1, 2, 3, -1, 0):           # 2 / 3: list-by-list / row-sweep form
         s.set_sparse_postings(mode)
         mat, ssum = s.matrix()
-        if mode == 1:
+        if mode in (1, 2, 3):
             assert s.last_postings_rows() == len(sets)
         if mode == 0:
             assert s.last_postings_rows() == 0
@@ -268,13 +269,14 @@ def test_tensor_rows_with_postings_in_panels(sb):
     sets = [sets[k] for k in g.permutation(len(sets))]
     s = build_storm(sb, sets)
     s.set_dense_block(1.0 / 1024, 2 * 256 * (universe // 8) + 4096)
-    s.set_sparse_postings(1)
     vals, offs = gen.to_csr(sets)
     want, ws = ol.sets_matrix(vals, offs)
-    mat, ssum = s.matrix()
-    assert s.last_dense() == (300, 4) and s.last_postings_rows() == 300
-    assert ssum == ws
-    np.testing.assert_array_equal(mat, want)
+    for mode in (2, 3):
+        s.set_sparse_postings(mode)
+        mat, ssum = s.matrix()
+        assert s.last_dense() == (300, 4) and s.last_postings_rows() == 300
+        assert ssum == ws
+        np.testing.assert_array_equal(mat, want)
     assert s.pairw_intersect_cardinality() == ws
 
 
