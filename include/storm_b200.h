@@ -142,7 +142,25 @@ int STORM_contig_pairw_intersect_matrix_noalloc(const uint64_t* d_rows, uint64_t
                                                 uint32_t* d_out, uint64_t out_len, uint64_t* sum,
                                                 void* stream);
 
+/* Thresholded all-pairs: the opt-in contract of the reference's thresholded
+ * mode (bench/bench_threshold.cpp:129-132, README.md "Thresholded mode"): only
+ * the pairs i < j whose exact count v = |Xi & Xj| is > 0 and whose Jaccard
+ * v / (|Xi| + |Xj| - v) >= jaccard_min (compared in double precision) are
+ * reported, with v; the counts are exact, only the set of reported pairs is
+ * restricted.  No per-pair triangle reaches the host: on the tensor-core
+ * kernel the filter runs in the epilogue and nothing else is written.
+ * out_i / out_j / out_count receive min(found, cap) pairs sorted by (i, j);
+ * *n_found = how many passed.  Returns 0, or STORM_B200_ESIZE when more than
+ * cap passed (the arrays then hold cap of them, not necessarily the first).
+ * No counterpart in storm.h (the reference's thresholded mode is a bench). */
+int STORM_contig_pairw_threshold(STORM_contiguous_t* c, double jaccard_min, uint32_t* out_i, uint32_t* out_j,
+                                 uint32_t* out_count, uint64_t cap, uint64_t* n_found);
+
 /* ---- STORM_t extensions ----------------------------------------------- */
+/* Thresholded all-pairs over STORM_t rows: as STORM_contig_pairw_threshold;
+ * |Xi| is row i's count against itself. */
+int STORM_pairw_threshold(STORM_t* s, double jaccard_min, uint32_t* out_i, uint32_t* out_j, uint32_t* out_count,
+                          uint64_t cap, uint64_t* n_found);
 int STORM_upload(STORM_t* s);
 int STORM_pairw_intersect_matrix(STORM_t* s, uint32_t* out, uint64_t out_len, uint64_t* sum);
 int STORM_pairw_intersect_tiles(STORM_t* s, uint32_t tile, STORM_tile_callback cb, void* ctx);

@@ -69,6 +69,10 @@ _sig("STORM_contig_add_bitmaps", C.c_int, [C.c_void_p, u64p, C.c_uint32, C.c_uin
 _sig("STORM_contig_size", C.c_uint64, [C.c_void_p])
 _sig("STORM_contig_set_kernel", C.c_int, [C.c_void_p, C.c_int])
 _sig("STORM_contig_set_schedule", C.c_int, [C.c_void_p, C.c_int])
+_sig("STORM_contig_pairw_threshold", C.c_int, [C.c_void_p, C.c_double, u32p, u32p, u32p, C.c_uint64,
+                                               C.POINTER(C.c_uint64)])
+_sig("STORM_pairw_threshold", C.c_int, [C.c_void_p, C.c_double, u32p, u32p, u32p, C.c_uint64,
+                                        C.POINTER(C.c_uint64)])
 _sig("STORM_contig_upload", C.c_int, [C.c_void_p])
 _sig("STORM_contig_pairw_intersect_matrix", C.c_int, [C.c_void_p, u32p, C.c_uint64, u64p])
 _sig("STORM_contig_pairw_intersect_matrix_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, u64p])
@@ -122,6 +126,20 @@ def _check_status(where: str):
 
 def _p(a: np.ndarray, t):
     return a.ctypes.data_as(t)
+
+
+def _threshold(fn, h, jaccard_min, cap):
+    """(i, j, counts, found) of a thresholded call; raises on errors other
+    than a full output (STORM_B200_ESIZE, when found > cap)."""
+    oi = np.zeros(max(1, cap), np.uint32)
+    oj = np.zeros(max(1, cap), np.uint32)
+    oc = np.zeros(max(1, cap), np.uint32)
+    found = C.c_uint64(0)
+    rc = fn(h, float(jaccard_min), _p(oi, u32p), _p(oj, u32p), _p(oc, u32p), cap, C.byref(found))
+    if rc < 0 and rc != ESIZE:
+        raise StormError(rc, "thresholded all-pairs")
+    m = min(int(found.value), cap)
+    return oi[:m], oj[:m], oc[:m], int(found.value)
 
 
 def tri_size(n: int) -> int:
@@ -248,6 +266,9 @@ class StormContig:
     def set_kernel(self, kernel: int):
         _check(_lib.STORM_contig_set_kernel(self.h, kernel), "STORM_contig_set_kernel")
 
+    def threshold(self, jaccard_min: float, cap: int = 1 << 20):
+        return _threshold(_lib.STORM_contig_pairw_threshold, self.h, jaccard_min, cap)
+
     def set_schedule(self, schedule: int):
         _check(_lib.STORM_contig_set_schedule(self.h, schedule), "STORM_contig_set_schedule")
 
@@ -364,6 +385,9 @@ class Storm:
 
     def set_dense_block(self, min_density: float, budget_bytes: int = 0):
         _check(_lib.STORM_set_dense_block(self.h, float(min_density), int(budget_bytes)), "STORM_set_dense_block")
+
+    def threshold(self, jaccard_min: float, cap: int = 1 << 20):
+        return _threshold(_lib.STORM_pairw_threshold, self.h, jaccard_min, cap)
 
     def set_sparse_postings(self, mode: int):
         _check(_lib.STORM_set_sparse_postings(self.h, int(mode)), "STORM_set_sparse_postings")

@@ -129,11 +129,26 @@ struct TsSched {
     }
 };
 
-template <bool kRowMap, bool kW4>
+// Thresholded output (the opt-in contract of the reference's thresholded
+// mode, bench/bench_threshold.cpp:129-132): pair i < j is reported when its
+// count v > 0 and v / (|Xi| + |Xj| - v) >= t in double precision; reported
+// pairs are appended (unordered) to pairs/cnts, found counts all of them
+// (entries past cap are counted, not written).
+struct TsThresh {
+    const uint32_t* card;            // |Xi| per row
+    double t;
+    uint2* pairs;
+    uint32_t* cnts;
+    unsigned long long cap;
+    unsigned long long* found;
+};
+
+template <bool kRowMap, bool kW4, bool kThresh = false>
 __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad,
                                         const uint2* __restrict__ tiles, uint32_t n_tiles,
                                         uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags,
-                                        const uint32_t* __restrict__ row_map, uint64_t n_out, uint32_t k_splits) {
+                                        const uint32_t* __restrict__ row_map, uint64_t n_out, uint32_t k_splits,
+                                        TsThresh th = TsThresh{}) {
     extern __shared__ __align__(1024) unsigned char ts_smem[];
     const uint32_t raw_addr = smem_u32(ts_smem);
     const uint32_t pad = ((raw_addr + 1023u) & ~1023u) - raw_addr;
@@ -147,7 +162,7 @@ __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t
     // feed long rows) each lane stores its own row.
     uint32_t dyn_smem;
     asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn_smem));
-    const bool coalesced = dyn_smem >= TS_SMEM_BYTES;
+    const bool coalesced = !kThresh && dyn_smem >= TS_SMEM_BYTES;
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
@@ -279,7 +294,39 @@ __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t
                     uint32_t r[32];
                     tmem_ld_32x32b_x32(tmem_base + (lane_grp << 16) + col0 + 32u * c, r);
                     tmem_ld_wait();
-                    if (row_ok) {
+                    if constexpr (kThresh) {
+                        // whole tiles only (no partial segments); every lane
+                        // stays in the loop for the warp-aggregated appends
+                        const uint64_t jb = j0 + col0 + 32u * c;
+                        const double ci = row_ok ? (double)th.card[i] : 0.0;
+#pragma unroll
+                        for (int e = 0; e < 32; ++e) {
+                            const uint64_t j = jb + e;
+                            const uint32_t cnt = r[e] >> (kW4 ? 3 : 7);
+                            bool pass = false;
+                            if (row_ok && j > i && j < n) {
+                                local += cnt;
+                                if (cnt) {
+                                    const double u = ci + (double)th.card[j] - (double)cnt;
+                                    pass = u > 0.0 && (double)cnt / u >= th.t;
+                                }
+                            }
+                            const uint32_t m = __ballot_sync(0xffffffffu, pass);
+                            if (m) {
+                                const int leader = __ffs(m) - 1;
+                                unsigned long long b0 = 0;
+                                if (lane == leader) b0 = atomicAdd(th.found, (unsigned long long)__popc(m));
+                                b0 = __shfl_sync(0xffffffffu, b0, leader);
+                                if (pass) {
+                                    const unsigned long long k = b0 + __popc(m & ((1u << lane) - 1u));
+                                    if (k < th.cap) {
+                                        th.pairs[k] = make_uint2((uint32_t)i, (uint32_t)j);
+                                        th.cnts[k] = cnt;
+                                    }
+                                }
+                            }
+                        }
+                    } else if (row_ok) {
                         const uint64_t jb = j0 + col0 + 32u * c;
 #pragma unroll
                         for (int e = 0; e < 32; ++e) {
@@ -381,6 +428,20 @@ bb_mma_ts_rows_long_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t 
                            DeviceFlags* __restrict__ flags, const uint32_t* __restrict__ row_map, uint64_t n_out,
                            uint32_t k_splits) {
     ts_body<true, true>(X, n, w_pad, tiles, n_tiles, out, flags, row_map, n_out, k_splits);
+}
+
+// Thresholded form over contiguous rows (whole tiles round robin).
+__global__ void __launch_bounds__(TS_THREADS, 1)
+bb_mma_ts_thresh_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, const uint2* __restrict__ tiles,
+                        uint32_t n_tiles, DeviceFlags* __restrict__ flags, TsThresh th) {
+    ts_body<false, false, true>(X, n, w_pad, tiles, n_tiles, nullptr, flags, nullptr, 0, 1u, th);
+}
+
+__global__ void __launch_bounds__(TS_THREADS, 1)
+bb_mma_ts_thresh_long_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad,
+                             const uint2* __restrict__ tiles, uint32_t n_tiles, DeviceFlags* __restrict__ flags,
+                             TsThresh th) {
+    ts_body<false, true, true>(X, n, w_pad, tiles, n_tiles, nullptr, flags, nullptr, 0, 1u, th);
 }
 
 }  // namespace sb200

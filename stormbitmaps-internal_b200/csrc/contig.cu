@@ -13,6 +13,7 @@
 // staged in host memory and flushed in one copy at the next device call;
 // STORM_contig_add_bitmaps copies straight into HBM.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -32,6 +33,8 @@ struct STORM_contiguous_s {
     cudaStream_t copy_stream = nullptr;   // device-to-host copies overlapping the next panel
     int kernel_pref = STORM_B200_KERNEL_AUTO;
     sb200::DenseEngine engine;
+    sb200::DevBuf<uint2> d_hits;               // thresholded form: reported pairs and counts
+    sb200::DevBuf<uint32_t> d_hit_cnt;
 
     ~STORM_contiguous_s() {
         if (stream) cudaStreamDestroy(stream);
@@ -288,6 +291,24 @@ int STORM_contig_pairw_intersect_matrix_device(STORM_contiguous_t* c, uint32_t* 
         const uint64_t s = contig_run(c, d_out);
         if (sum) *sum = s;
         return 0;
+    });
+}
+
+int STORM_contig_pairw_threshold(STORM_contiguous_t* c, double jaccard_min, uint32_t* out_i, uint32_t* out_j,
+                                 uint32_t* out_count, uint64_t cap, uint64_t* n_found) {
+    if (c == NULL) return STORM_B200_ENULL;
+    if (std::isnan(jaccard_min)) return STORM_B200_EARG;
+    if (cap && (out_i == NULL || out_j == NULL || out_count == NULL)) return STORM_B200_EVALUES;
+    return guard([&]() -> int {
+        contig_flush(c);
+        cudaStream_t st = contig_stream(c);
+        c->d_hits.reserve(cap ? cap : 1);
+        c->d_hit_cnt.reserve(cap ? cap : 1);
+        const uint64_t found = c->engine.run_threshold(c->d_rows.p, c->dev_rows, c->w_pad, c->vector_length,
+                                                       c->kernel_pref, jaccard_min, c->d_hits.p, c->d_hit_cnt.p, cap,
+                                                       nullptr, st);
+        if (n_found) *n_found = found;
+        return threshold_to_host(c->d_hits.p, c->d_hit_cnt.p, found, cap, out_i, out_j, out_count, st);
     });
 }
 

@@ -4,6 +4,7 @@
 #include "bb_mma.cuh"
 #include "bb_mma_ts.cuh"
 
+#include <algorithm>
 #include <mutex>
 
 namespace sb200 {
@@ -288,6 +289,167 @@ extern "C" int STORM_contig_pairw_intersect_matrix_noalloc(const uint64_t* d_row
     if (sum) *sum = f.sum;
     return 0;
 }
+
+// ===================================================================
+// Thresholded output
+// ===================================================================
+namespace sb200 {
+
+// |Xi| of each row: warp per row.
+__global__ void row_popcount_kernel(const uint64_t* __restrict__ X, uint64_t n, uint32_t w_pad,
+                                    uint32_t* __restrict__ card) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += nw) {
+        uint32_t c = 0;
+        for (uint32_t w = lane; w < w_pad; w += 32) c += __popcll(X[r * w_pad + w]);
+        c = warp_sum_u32(c);
+        if (lane == 0) card[r] = c;
+    }
+}
+
+__global__ void diag_card_kernel(const uint32_t* __restrict__ tri, uint64_t n, uint32_t* __restrict__ card) {
+    for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < n; r += (uint64_t)gridDim.x * blockDim.x)
+        card[r] = tri[tri_index(n, r, r)];
+}
+
+// Warp per row i, lanes over j > i; warp-aggregated appends.
+__global__ void tri_threshold_kernel(const uint32_t* __restrict__ tri, uint64_t n, const uint32_t* __restrict__ card,
+                                     double t, uint2* __restrict__ pairs, uint32_t* __restrict__ cnts,
+                                     unsigned long long cap, unsigned long long* __restrict__ found) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+        const uint64_t base = tri_index(n, i, i) - i;
+        const double ci = (double)card[i];
+        for (uint64_t j0 = i + 1; j0 < n; j0 += 32) {
+            const uint64_t j = j0 + lane;
+            bool pass = false;
+            uint32_t cnt = 0;
+            if (j < n) {
+                cnt = tri[base + j];
+                if (cnt) {
+                    const double u = ci + (double)card[j] - (double)cnt;
+                    pass = u > 0.0 && (double)cnt / u >= t;
+                }
+            }
+            const uint32_t m = __ballot_sync(0xffffffffu, pass);
+            if (!m) continue;
+            const int leader = __ffs(m) - 1;
+            unsigned long long b0 = 0;
+            if (lane == leader) b0 = atomicAdd(found, (unsigned long long)__popc(m));
+            b0 = __shfl_sync(0xffffffffu, b0, leader);
+            if (pass) {
+                const unsigned long long k = b0 + __popc(m & ((1u << lane) - 1u));
+                if (k < cap) {
+                    pairs[k] = make_uint2((uint32_t)i, (uint32_t)j);
+                    cnts[k] = cnt;
+                }
+            }
+        }
+    }
+}
+
+uint64_t threshold_from_triangle(const uint32_t* d_tri, uint64_t n, double t, uint32_t* card,
+                                 unsigned long long* found, uint2* d_pairs, uint32_t* d_cnts, uint64_t cap,
+                                 cudaStream_t st) {
+    const int sms = require_device();
+    SB_CUDA(cudaMemsetAsync(found, 0, sizeof(unsigned long long), st));
+    if (n) {
+        diag_card_kernel<<<(uint32_t)std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 8), 256, 0, st>>>(d_tri, n,
+                                                                                                          card);
+        tri_threshold_kernel<<<(uint32_t)std::min<uint64_t>((n + 7) / 8, (uint64_t)sms * 16), 256, 0, st>>>(
+            d_tri, n, card, t, d_pairs, d_cnts, cap, found);
+        SB_CUDA(cudaGetLastError());
+    }
+    unsigned long long h = 0;
+    SB_CUDA(cudaMemcpyAsync(&h, found, sizeof(h), cudaMemcpyDeviceToHost, st));
+    SB_CUDA(cudaStreamSynchronize(st));
+    return h;
+}
+
+int threshold_to_host(const uint2* d_pairs, const uint32_t* d_cnts, uint64_t found, uint64_t cap, uint32_t* out_i,
+                      uint32_t* out_j, uint32_t* out_count, cudaStream_t st) {
+    const uint64_t m = std::min<uint64_t>(found, cap);
+    std::vector<uint2> pr(m);
+    std::vector<uint32_t> ct(m);
+    if (m) {
+        SB_CUDA(cudaMemcpyAsync(pr.data(), d_pairs, m * sizeof(uint2), cudaMemcpyDeviceToHost, st));
+        SB_CUDA(cudaMemcpyAsync(ct.data(), d_cnts, m * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        SB_CUDA(cudaStreamSynchronize(st));
+    }
+    std::vector<uint64_t> idx(m);
+    for (uint64_t k = 0; k < m; ++k) idx[k] = k;
+    std::sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) {
+        return pr[a].x != pr[b].x ? pr[a].x < pr[b].x : pr[a].y < pr[b].y;
+    });
+    for (uint64_t k = 0; k < m; ++k) {
+        if (out_i) out_i[k] = pr[idx[k]].x;
+        if (out_j) out_j[k] = pr[idx[k]].y;
+        if (out_count) out_count[k] = ct[idx[k]];
+    }
+    return found > cap ? STORM_B200_ESIZE : 0;
+}
+
+uint64_t DenseEngine::run_threshold(const uint64_t* dX, uint64_t n, uint32_t w_pad, uint64_t row_bits,
+                                    int kernel_pref, double t, uint2* d_pairs, uint32_t* d_cnts, uint64_t cap,
+                                    uint64_t* sum, cudaStream_t st) {
+    const int sms = require_device();
+    d_found.reserve(1);
+    d_card.reserve(n ? n : 1);
+    if (n == 0) {
+        log.launches = 0;
+        log.last_ms = 0.f;
+        if (sum) *sum = 0;
+        return 0;
+    }
+    const int kind = prepare(n, row_bits, kernel_pref, st);
+    SB_CUDA(cudaEventRecord(log.ev0, st));
+    uint64_t found = 0;
+    if (kind == STORM_B200_KERNEL_MMA) {
+        static bool attr_set = false;
+        if (!attr_set) {
+            SB_CUDA(cudaFuncSetAttribute(bb_mma_ts_thresh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)TS_SMEM_BYTES));
+            SB_CUDA(cudaFuncSetAttribute(bb_mma_ts_thresh_long_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)TS_SMEM_BYTES));
+            attr_set = true;
+        }
+        SB_CUDA(cudaMemsetAsync(d_found.p, 0, sizeof(unsigned long long), st));
+        row_popcount_kernel<<<(uint32_t)std::min<uint64_t>((n + 7) / 8, (uint64_t)sms * 16), 256, 0, st>>>(
+            dX, n, w_pad, d_card.p);
+        const TsThresh th{d_card.p, t, d_pairs, d_cnts, (unsigned long long)cap, d_found.p};
+        const uint32_t grid = n_tiles < (uint32_t)sms ? n_tiles : (uint32_t)sms;
+        if ((uint64_t)w_pad * 64 <= MMA_MAX_BITS)
+            bb_mma_ts_thresh_kernel<<<grid, TS_THREADS, TS_SMEM_BYTES_LEAN, st>>>(dX, (uint32_t)n, w_pad, d_tiles.p,
+                                                                                   n_tiles, d_flags.p, th);
+        else
+            bb_mma_ts_thresh_long_kernel<<<grid, TS_THREADS, TS_SMEM_BYTES_LEAN, st>>>(
+                dX, (uint32_t)n, w_pad, d_tiles.p, n_tiles, d_flags.p, th);
+        SB_CUDA(cudaGetLastError());
+        unsigned long long h = 0;
+        SB_CUDA(cudaMemcpyAsync(&h, d_found.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+        SB_CUDA(cudaStreamSynchronize(st));
+        found = h;
+        log.launches = 2;
+    } else {
+        d_scratch_tri.reserve(tri_size(n));
+        launch(kind, dX, (uint32_t)n, w_pad, 0, n_tiles, d_scratch_tri.p, st);
+        found = threshold_from_triangle(d_scratch_tri.p, n, t, d_card.p, d_found.p, d_pairs, d_cnts, cap, st);
+        log.launches = 3;
+    }
+    SB_CUDA(cudaEventRecord(log.ev1, st));
+    DeviceFlags f;
+    SB_CUDA(cudaMemcpyAsync(&f, d_flags.p, sizeof(f), cudaMemcpyDeviceToHost, st));
+    SB_CUDA(cudaStreamSynchronize(st));
+    SB_CUDA(cudaEventElapsedTime(&log.last_ms, log.ev0, log.ev1));
+    log.kernel = kind;
+    if (f.error) fail(STORM_B200_ETIMEOUT, "bitmap x bitmap kernel: bounded wait expired");
+    if (sum) *sum = f.sum;
+    return found;
+}
+
+}  // namespace sb200
 
 // ===================================================================
 // Kernel-layer dense block: the tensor-core kernel over a gathered subset of

@@ -35,6 +35,17 @@ struct DenseEngine {
     uint64_t run_to_host(const uint64_t* dX, uint64_t n, uint32_t w_pad, uint64_t row_bits, uint32_t* d_out,
                          uint32_t* host_out, int kernel_pref, cudaStream_t st, cudaStream_t copy_st);
 
+    // Thresholded form: the pairs i < j with count v > 0 and
+    // v / (|Xi| + |Xj| - v) >= t, appended to d_pairs / d_cnts (up to cap,
+    // unordered); returns how many pairs passed. The tensor-core kernel
+    // filters in its epilogue (no triangle is written); other kernels write
+    // the triangle into scratch and compact it. Synchronous.
+    uint64_t run_threshold(const uint64_t* dX, uint64_t n, uint32_t w_pad, uint64_t row_bits, int kernel_pref,
+                           double t, uint2* d_pairs, uint32_t* d_cnts, uint64_t cap, uint64_t* sum,
+                           cudaStream_t st);
+    DevBuf<uint32_t> d_card, d_scratch_tri;
+    DevBuf<unsigned long long> d_found;
+
    private:
     int prepare(uint64_t n, uint64_t row_bits, int kernel_pref, cudaStream_t st);
     void launch(int kind, const uint64_t* dX, uint32_t n, uint32_t w_pad, uint32_t t0, uint32_t count,
@@ -59,5 +70,19 @@ constexpr uint64_t TC_MAX_ROW_BITS = 1ull << 27;
 void launch_ts_rows(const uint64_t* X, uint32_t n, uint32_t w_pad, const uint2* tiles, uint32_t n_tiles,
                     uint32_t* out, DeviceFlags* flags, const uint32_t* row_map, uint64_t n_out, cudaStream_t st,
                     bool out_zeroed = false);
+
+// Thresholded pairs from a packed triangle of n rows already on the device
+// (row cardinalities from its diagonal): appends the pairs i < j with
+// v > 0 and v / (d_i + d_j - v) >= t to d_pairs / d_cnts (up to cap) and
+// returns how many passed. card must hold n entries, found one. Synchronous.
+uint64_t threshold_from_triangle(const uint32_t* d_tri, uint64_t n, double t, uint32_t* card,
+                                 unsigned long long* found, uint2* d_pairs, uint32_t* d_cnts, uint64_t cap,
+                                 cudaStream_t st);
+
+// Host side of the thresholded C-ABI calls: copies min(found, cap) hits to
+// the caller's arrays sorted by (i, j); returns 0, or STORM_B200_ESIZE when
+// more pairs passed than cap (the arrays then hold cap of them).
+int threshold_to_host(const uint2* d_pairs, const uint32_t* d_cnts, uint64_t found, uint64_t cap, uint32_t* out_i,
+                      uint32_t* out_j, uint32_t* out_count, cudaStream_t st);
 
 }  // namespace sb200

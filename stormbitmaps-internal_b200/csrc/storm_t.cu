@@ -22,6 +22,7 @@
 
 #include <cmath>
 #include "chunk_engine.cuh"
+#include "dense.cuh"
 
 namespace sb200 {
 
@@ -38,6 +39,9 @@ struct StormDev {
     ChunkEngine engine;
     cudaStream_t stream = nullptr;
     DevBuf<uint32_t> d_out;
+    DevBuf<uint32_t> d_card, d_hit_cnt;    // thresholded form
+    DevBuf<uint2> d_hits;
+    DevBuf<unsigned long long> d_found;
     bool valid = false;
     ~StormDev() {
         if (stream) cudaStreamDestroy(stream);
@@ -505,6 +509,29 @@ int STORM_pairw_intersect_matrix(STORM_t* s, uint32_t* out, uint64_t out_len, ui
         }
         if (sum) *sum = r;
         return 0;
+    });
+}
+
+int STORM_pairw_threshold(STORM_t* s, double jaccard_min, uint32_t* out_i, uint32_t* out_j, uint32_t* out_count,
+                          uint64_t cap, uint64_t* n_found) {
+    if (s == NULL) return STORM_B200_ENULL;
+    if (std::isnan(jaccard_min)) return STORM_B200_EARG;
+    if (cap && (out_i == NULL || out_j == NULL || out_count == NULL)) return STORM_B200_EVALUES;
+    return guard([&]() -> int {
+        StormDev* d = state_of(s);
+        ensure_packed(s, d);
+        cudaStream_t st = stream_of(d);
+        const uint64_t n = s->n_conts;
+        d->d_out.reserve(tri_size(n) ? tri_size(n) : 1);
+        d->engine.run(d->dev, PAIRS_TRIANGLE, n, 0, d->d_out.p, st);
+        d->d_card.reserve(n ? n : 1);
+        d->d_found.reserve(1);
+        d->d_hits.reserve(cap ? cap : 1);
+        d->d_hit_cnt.reserve(cap ? cap : 1);
+        const uint64_t found = threshold_from_triangle(d->d_out.p, n, jaccard_min, d->d_card.p, d->d_found.p,
+                                                       d->d_hits.p, d->d_hit_cnt.p, cap, st);
+        if (n_found) *n_found = found;
+        return threshold_to_host(d->d_hits.p, d->d_hit_cnt.p, found, cap, out_i, out_j, out_count, st);
     });
 }
 

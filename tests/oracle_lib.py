@@ -129,3 +129,18 @@ def row_popcounts(words: np.ndarray) -> np.ndarray:
     out = np.zeros(n, dtype=np.uint32)
     oracle().oracle_row_popcounts(_p(words, u64p), n, w, _p(out, u32p))
     return out
+
+
+def threshold_pairs(tri: np.ndarray, n: int, t: float):
+    """The thresholded contract on a packed triangle (i <= j, diagonal = |Xi|):
+    pairs i < j with v > 0 and v / (|Xi| + |Xj| - v) >= t in double precision
+    (bench/bench_threshold.cpp:129-132). Returns (i, j, v) sorted by (i, j)."""
+    iu = np.triu_indices(n)
+    v = tri.astype(np.float64)
+    diag = v[iu[0] == iu[1]]
+    off = iu[0] != iu[1]
+    i, j, c = iu[0][off], iu[1][off], v[off]
+    u = diag[i] + diag[j] - c
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ok = (c > 0) & (u > 0) & (c / np.where(u > 0, u, 1.0) >= t)
+    return i[ok].astype(np.uint32), j[ok].astype(np.uint32), c[ok].astype(np.uint32)

@@ -304,3 +304,46 @@ def test_every_schedule_is_exact(sb, n, m):
         mat, s = c.matrix()
         assert s == ws, sched
         np.testing.assert_array_equal(mat, want, err_msg=str(sched))
+
+
+@pytest.mark.parametrize("kernel", ("mma", "popc"))
+@pytest.mark.parametrize("n,m", [(300, (1 << 17) + 64), (700, 16384), (129, 4097)])
+def test_threshold_matches_oracle(sb, kernel, n, m):
+    """Thresholded form (pairs with v > 0 and Jaccard >= t, exact v): fused in
+    the tensor-core epilogue, and by compaction of the triangle for POPC."""
+    words = gen.bernoulli_rows(n, m, (0.05, 0.6), seed=800 + n)
+    tri, _ = ol.contig_matrix(words)
+    c = contig_from_words(sb, words, m, kernel)
+    for t in (0.0, 0.2, 0.35, 1.0):
+        wi, wj, wc = ol.threshold_pairs(tri, n, t)
+        gi, gj, gc, found = c.threshold(t, cap=n * n)
+        assert found == len(wi), t
+        np.testing.assert_array_equal(gi, wi)
+        np.testing.assert_array_equal(gj, wj)
+        np.testing.assert_array_equal(gc, wc)
+
+
+def test_threshold_long_rows_and_small_cap(sb):
+    """Rows past 2^23 bits (4-byte weight cycle), and an output capacity
+    smaller than the hit count: STORM_B200_ESIZE, the true count, and cap
+    hits that all belong to the answer."""
+    m = (1 << 23) + 4096
+    g = gen.rng(4343)
+    words = g.integers(0, 1 << 63, size=(40, (m + 63) // 64), dtype=np.uint64)
+    words[:, -1] &= np.uint64((1 << (m % 64)) - 1)
+    tri, _ = ol.contig_matrix(words)
+    c = contig_from_words(sb, words, m, "mma")
+    wi, wj, wc = ol.threshold_pairs(tri, 40, 0.3)
+    gi, gj, gc, found = c.threshold(0.3, cap=2000)
+    assert found == len(wi) and len(wi) > 10
+    np.testing.assert_array_equal(gi, wi)
+    np.testing.assert_array_equal(gc, wc)
+    oi = np.zeros(5, np.uint32)
+    oj = np.zeros(5, np.uint32)
+    oc = np.zeros(5, np.uint32)
+    f = sb.C.c_uint64(0)
+    rc = sb.lib().STORM_contig_pairw_threshold(c.h, 0.3, sb._p(oi, sb.u32p), sb._p(oj, sb.u32p),
+                                               sb._p(oc, sb.u32p), 5, sb.C.byref(f))
+    assert rc == sb.ESIZE and f.value == len(wi)
+    want = {(a, b, v) for a, b, v in zip(wi.tolist(), wj.tolist(), wc.tolist())}
+    assert all((a, b, v) in want for a, b, v in zip(oi.tolist(), oj.tolist(), oc.tolist()))

@@ -292,3 +292,21 @@ def test_default_plan_on_mixed_rows_matches_oracle(sb):
     assert ssum == ws
     np.testing.assert_array_equal(mat, want)
     assert s.pairw_intersect_cardinality() == ws
+
+
+def test_threshold_storm_t_matches_oracle(sb):
+    """Thresholded form over STORM_t rows (triangle compaction on the device),
+    on a mix of heavy, light and very sparse rows."""
+    g = gen.rng(101)
+    sets = [gen.uniform_set(g, int(g.integers(2000, 6000)), 1 << 18) for _ in range(150)]
+    sets += [gen.uniform_set(g, int(g.integers(1, 80)), 1 << 18) for _ in range(250)]
+    s = build_storm(sb, sets)
+    vals, offs = gen.to_csr(sets)
+    want, _ = ol.sets_matrix(vals, offs)
+    for t in (0.0, 0.01, 0.05, 0.5):
+        wi, wj, wc = ol.threshold_pairs(want, len(sets), t)
+        gi, gj, gc, found = s.threshold(t, cap=len(sets) ** 2)
+        assert found == len(wi), t
+        np.testing.assert_array_equal(gi, wi)
+        np.testing.assert_array_equal(gj, wj)
+        np.testing.assert_array_equal(gc, wc)
