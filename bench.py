@@ -568,6 +568,27 @@ def storm_t_forms(device, cpu_seconds=2.0, only=None):
                                     "sample": f"first {k} rows ({k * (k - 1) // 2} pairs i < j, {secs:.2f} s), "
                                               f"STORM_pairw_intersect_cardinality as shipped (all-pairs call only)"}
             res["gpu_default_over_cpu"] = res["gpu_default"]["pairs_per_s"] / rate
+            threads = cpu_threads()
+            k, rate_mt, secs = 64, None, 0.0
+            while True:
+                k = min(k, n)
+                vals = np.ascontiguousarray(np.concatenate(sets[:k]), dtype=np.uint32)
+                offs = np.zeros(k + 1, np.uint64)
+                offs[1:] = np.cumsum([len(x) for x in sets[:k]])
+                sec = C.c_double(0.0)
+                R.ref_storm_sum_mt(vals.ctypes.data_as(ol.u32p), offs.ctypes.data_as(ol.u64p), k, threads,
+                                   C.byref(sec))
+                secs = sec.value
+                rate_mt = (k * (k - 1) // 2) / max(secs, 1e-9)
+                if secs >= cpu_seconds or k == n:
+                    break
+                k *= 2
+            res["cpu_reference_all_threads"] = {
+                "pairs_per_s": rate_mt, "cores": threads,
+                "sample": f"first {k} rows ({k * (k - 1) // 2} pairs i < j, {secs:.2f} s), project harness: "
+                          f"the reference's per-pair STORM_bitmap_cont_intersect_cardinality_premade over "
+                          f"{threads} threads"}
+            res["gpu_default_over_cpu_all_threads"] = res["gpu_default"]["pairs_per_s"] / rate_mt
         if "gpu_chunk_kernel" in res:
             res["gpu_default_over_chunk_kernel"] = (res["gpu_default"]["pairs_per_s"] /
                                                     res["gpu_chunk_kernel"]["pairs_per_s"])
@@ -721,6 +742,19 @@ def run_b200_arm(args):
         if not np.array_equal(host_tri[base: base + n - i], ol.contig_row(host_rows, i)):
             raise RuntimeError(f"row {i} of the triangle differs from the oracle")
 
+    # ---- thresholded form (pairs with Jaccard >= t): filter fused into the
+    # tensor-core epilogue, no triangle written
+    thresh = None
+    if args.forms and rank == 0:
+        t_j = 0.3
+        tms, hits = [], 0
+        for _ in range(3):
+            _, _, _, hits = c.threshold(t_j, cap=1 << 25)
+            tms.append(c.last_kernel_ms())
+        thresh = {"jaccard_min": t_j, "ms": round(min(tms), 3), "pairs_per_s": tri / (min(tms) * 1e-3),
+                  "hits": hits, "hit_fraction": hits / tri, "triangle_bytes_not_written": tri * 4,
+                  "vs_full_triangle_kernel_ms": round(statistics.median(kernel_ms), 3)}
+
     # ---- roofline of the dominant kernel ----
     peaks, peak_src = measured_peaks()
     k_ms = statistics.median(kernel_ms)
@@ -768,6 +802,8 @@ def run_b200_arm(args):
         else:
             line["cpu_baseline"] = {"value": None, "unit": "pairs/s", "cores": 0, "kind": "reference",
                                     "sample": "oracle/_ref not built"}
+    if thresh is not None:
+        line["threshold_form"] = thresh
     if rank == 0 and args.forms:
         try:
             line["mixed_density"] = mixed_density_forms(sb, device)

@@ -157,6 +157,21 @@ int STORM_contig_pairw_threshold(STORM_contiguous_t* c, double jaccard_min, uint
                                  uint32_t* out_count, uint64_t cap, uint64_t* n_found);
 
 /* ---- STORM_t extensions ----------------------------------------------- */
+/* Append the rows of a STORMBIN corpus file (the reference's on-disk format:
+ * "STORMBIN", u32 version 1, n_rows, n_bits, pad, then per row a u32 count
+ * and that many strictly ascending u32 positions < n_bits;
+ * bench/bench_allpairs.cpp:44-72) to s with STORM_add.  As the reference's
+ * loaders do, empty rows are skipped and every stride-th row (0 or 1: all)
+ * is kept, up to max_rows (0: all).  Returns the rows added and sets
+ * *n_bits (may be NULL); STORM_B200_EARG if the file cannot be opened,
+ * STORM_B200_EVALUES for a bad header, a truncated row or positions out of
+ * order or range. */
+int64_t STORM_load_stormbin(STORM_t* s, const char* path, uint32_t max_rows, uint32_t stride, uint32_t* n_bits);
+/* Append the rows of a STORMPACK file (the reference's packed format with one
+ * stored representation per row -- bitmap, u16 array, u16 runs, full, empty;
+ * tools/pack.cpp:100-145) to s, every row including empty ones.  Returns the
+ * rows added and sets *n_bits; errors as STORM_load_stormbin. */
+int64_t STORM_load_stormpack(STORM_t* s, const char* path, uint32_t* n_bits);
 /* Thresholded all-pairs over STORM_t rows: as STORM_contig_pairw_threshold;
  * |Xi| is row i's count against itself. */
 int STORM_pairw_threshold(STORM_t* s, double jaccard_min, uint32_t* out_i, uint32_t* out_j, uint32_t* out_count,
@@ -190,7 +205,7 @@ uint64_t STORM_last_dense_panels(const STORM_t* s);
  * used when the exact increment count predicts less time than the chunk
  * kernel; 1: whenever rows qualify; 0: never.  Per-pair counts take one of
  * two forms: the increments go list by list into the output, or -- for
- * outputs larger than L2, at most 53248 postings rows, and when predicted
+ * outputs larger than L2, at most 51200 postings rows, and when predicted
  * faster from the exact increment count -- a row sweep counts each row's
  * partners in shared memory and writes its slice once.  Modes 2
  * and 3 force the rows in and pick the list-by-list or the row-sweep form.

@@ -83,11 +83,18 @@ void STORM_rows_free(STORM_rows_t* r);
 int STORM_rows_add(STORM_rows_t* r, const uint32_t* positions, uint32_t n);
 int STORM_rows_clear(STORM_rows_t* r);
 uint64_t STORM_rows_size(const STORM_rows_t* r);
+uint32_t STORM_rows_universe(const STORM_rows_t* r);
 /* HBM budget for the bitmap form (bytes, 0 = automatic: a quarter of free
  * memory).  Rows that do not get a bitmap behave like the reference's
  * sparse_only rows (storm_repr.h:280-291): no B, no rank, no zone map. */
 int STORM_rows_set_bitmap_budget(STORM_rows_t* r, uint64_t bytes);
 int STORM_rows_upload(STORM_rows_t* r);
+/* A new STORM_rows_t (universe = the file's n_bits) holding the rows of a
+ * STORMBIN corpus file; same format, stride and max_rows rules and errors
+ * as STORM_load_stormbin.  Returns the rows loaded; *out is NULL on error. */
+int64_t STORM_rows_load_stormbin(const char* path, uint32_t max_rows, uint32_t stride, STORM_rows_t** out);
+/* The same for a STORMPACK file (every row, empty ones included). */
+int64_t STORM_rows_load_stormpack(const char* path, STORM_rows_t** out);
 /* Tensor-core dense block: under the density-ordered policies (per-tile,
  * probe, oracle, refine, learned), the densest rows -- the suffix of the
  * density order whose rows all have a bitmap and whose smallest sparse form

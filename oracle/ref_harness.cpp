@@ -110,6 +110,41 @@ uint64_t ref_storm_sum_timed(const uint32_t* values, const uint64_t* offsets, ui
     return v;
 }
 
+/* A harness over the reference's own per-pair STORM_t call: the pair loop of
+ * STORM_pairw_intersect_cardinality (storm.cpp:927-945) split over threads
+ * (rows handed out one at a time from a shared counter), each thread with
+ * its own scratch buffer, calling STORM_bitmap_cont_intersect_cardinality_
+ * premade with the kernel STORM_get_intersect_count_func selects. Returns
+ * the same sum; *seconds = wall time of the pair loop alone. */
+uint64_t ref_storm_sum_mt(const uint32_t* values, const uint64_t* offsets, uint64_t n, uint32_t threads,
+                          double* seconds) {
+    STORM_t* s = STORM_new();
+    for (uint64_t r = 0; r < n; ++r)
+        STORM_add(s, values + offsets[r], (uint32_t)(offsets[r + 1] - offsets[r]));
+    if (threads == 0) threads = 1;
+    const STORM_compute_func f = STORM_get_intersect_count_func((uint32_t)(STORM_DEFAULT_BLOCK_SIZE / 64));
+    std::atomic<uint64_t> next(0), total(0);
+    const auto t0 = std::chrono::steady_clock::now();
+    auto work = [&]() {
+        std::vector<uint32_t> out(2 * STORM_DEFAULT_SCALAR_THRESHOLD);
+        uint64_t local = 0;
+        for (;;) {
+            const uint64_t i = next.fetch_add(1);
+            if (i >= s->n_conts) break;
+            for (uint64_t j = i + 1; j < s->n_conts; ++j)
+                local += STORM_bitmap_cont_intersect_cardinality_premade(&s->conts[i], &s->conts[j], f, out.data());
+        }
+        total += local;
+    };
+    std::vector<std::thread> pool;
+    for (uint32_t t = 0; t < threads; ++t) pool.emplace_back(work);
+    for (auto& th : pool) th.join();
+    const auto t1 = std::chrono::steady_clock::now();
+    if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+    STORM_free(s);
+    return total.load();
+}
+
 /* Reference rectangular form (storm.cpp:1027). */
 uint64_t ref_storm_square(const uint32_t* xv, const uint64_t* xo, uint64_t nx,
                           const uint32_t* yv, const uint64_t* yo, uint64_t ny) {

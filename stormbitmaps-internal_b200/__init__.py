@@ -71,6 +71,11 @@ _sig("STORM_contig_set_kernel", C.c_int, [C.c_void_p, C.c_int])
 _sig("STORM_contig_set_schedule", C.c_int, [C.c_void_p, C.c_int])
 _sig("STORM_contig_pairw_threshold", C.c_int, [C.c_void_p, C.c_double, u32p, u32p, u32p, C.c_uint64,
                                                C.POINTER(C.c_uint64)])
+_sig("STORM_load_stormbin", C.c_int64, [C.c_void_p, C.c_char_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32)])
+_sig("STORM_rows_universe", C.c_uint32, [C.c_void_p])
+_sig("STORM_load_stormpack", C.c_int64, [C.c_void_p, C.c_char_p, C.POINTER(C.c_uint32)])
+_sig("STORM_rows_load_stormpack", C.c_int64, [C.c_char_p, C.POINTER(C.c_void_p)])
+_sig("STORM_rows_load_stormbin", C.c_int64, [C.c_char_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_void_p)])
 _sig("STORM_pairw_threshold", C.c_int, [C.c_void_p, C.c_double, u32p, u32p, u32p, C.c_uint64,
                                         C.POINTER(C.c_uint64)])
 _sig("STORM_contig_upload", C.c_int, [C.c_void_p])
@@ -389,6 +394,22 @@ class Storm:
     def threshold(self, jaccard_min: float, cap: int = 1 << 20):
         return _threshold(_lib.STORM_pairw_threshold, self.h, jaccard_min, cap)
 
+    def load_stormbin(self, path: str, max_rows: int = 0, stride: int = 1):
+        """Append a STORMBIN corpus file's rows; returns (rows added, n_bits)."""
+        nb = C.c_uint32(0)
+        r = _lib.STORM_load_stormbin(self.h, os.fsencode(path), max_rows, stride, C.byref(nb))
+        _check(int(r), "STORM_load_stormbin")
+        self.n += int(r)
+        return int(r), int(nb.value)
+
+    def load_stormpack(self, path: str):
+        """Append a STORMPACK file's rows; returns (rows added, n_bits)."""
+        nb = C.c_uint32(0)
+        r = _lib.STORM_load_stormpack(self.h, os.fsencode(path), C.byref(nb))
+        _check(int(r), "STORM_load_stormpack")
+        self.n += int(r)
+        return int(r), int(nb.value)
+
     def set_sparse_postings(self, mode: int):
         _check(_lib.STORM_set_sparse_postings(self.h, int(mode)), "STORM_set_sparse_postings")
 
@@ -478,6 +499,26 @@ def mlp_forward_backward(params, F, H, Cn, x, labels):
 
 class StormRows:
     """STORM_rows_t: the reference's kernel layer (kernels/storm_allpairs.h) on the GPU."""
+
+    @classmethod
+    def from_stormpack(cls, path: str) -> "StormRows":
+        h = C.c_void_p(None)
+        r = _lib.STORM_rows_load_stormpack(os.fsencode(path), C.byref(h))
+        _check(int(r), "STORM_rows_load_stormpack")
+        obj = cls.__new__(cls)
+        obj.h = h.value
+        obj.universe = int(_lib.STORM_rows_universe(obj.h))
+        return obj
+
+    @classmethod
+    def from_stormbin(cls, path: str, max_rows: int = 0, stride: int = 1) -> "StormRows":
+        h = C.c_void_p(None)
+        r = _lib.STORM_rows_load_stormbin(os.fsencode(path), max_rows, stride, C.byref(h))
+        _check(int(r), "STORM_rows_load_stormbin")
+        obj = cls.__new__(cls)
+        obj.h = h.value
+        obj.universe = int(_lib.STORM_rows_universe(obj.h))
+        return obj
 
     def __init__(self, universe: int):
         self.h = _lib.STORM_rows_new(universe)

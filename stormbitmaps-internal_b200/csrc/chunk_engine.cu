@@ -267,19 +267,40 @@ chunk_pairs_kernel(ChunkView v, uint32_t mode, uint64_t n1, uint64_t n2, uint64_
 // ---- postings: pairs of plain rows without bitmap chunks ----------------
 // value of entry e of list chunk c: cid << 16 | entry (universe <= 2^27)
 
+// rows == nullptr: rows [0, nq). Bitmap chunks count every set bit (only the
+// rectangle sums send rows that have them).
 __global__ void postings_hist_kernel(ChunkView v, const uint32_t* __restrict__ rows, uint32_t nq,
                                      uint32_t* __restrict__ counts) {
     const int lane = threadIdx.x & 31;
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nq; r += nw) {
-        const uint32_t row = rows[r];
+        const uint32_t row = rows ? rows[r] : r;
         for (uint64_t c = v.row_off[row]; c < v.row_off[row + 1]; ++c) {
             const uint32_t base = v.cid[c] << 16;
-            const uint16_t* l = v.lst + v.coff[c];
-            const uint32_t nl = v.ckl[c] & CK_LEN;
-            for (uint32_t e = lane; e < nl; e += 32) atomicAdd(&counts[base | l[e]], 1u);
+            const uint32_t k = v.ckl[c];
+            if (k & CK_BITMAP) {
+                const uint64_t* wd = v.bm + v.coff[c];
+                for (uint32_t w = lane; w < CHUNK_WORDS; w += 32)
+                    for (uint64_t x = wd[w]; x; x &= x - 1)
+                        atomicAdd(&counts[base | (w << 6) | (uint32_t)__ffsll((long long)x) - 1u], 1u);
+            } else {
+                const uint16_t* l = v.lst + v.coff[c];
+                const uint32_t nl = k & CK_LEN;
+                for (uint32_t e = lane; e < nl; e += 32) atomicAdd(&counts[base | l[e]], 1u);
+            }
         }
     }
+}
+
+// sum over values of a[x] * b[x] into flags->sum: the rectangle sum of two
+// sets of plain rows.
+__global__ void counts_dot_kernel(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b, uint64_t U,
+                                  DeviceFlags* __restrict__ flags) {
+    unsigned long long acc = 0;
+    for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < U; x += (uint64_t)gridDim.x * blockDim.x)
+        acc += (unsigned long long)a[x] * b[x];
+    acc = warp_sum_u64(acc);
+    if ((threadIdx.x & 31) == 0 && acc) atomicAdd(&flags->sum, acc);
 }
 
 struct PostingsStats {
@@ -407,49 +428,60 @@ __global__ void postings_pairs_kernel(const uint2* __restrict__ lists, uint64_t 
 // Row sweep: CTA per Q row a; for every value of a, the rows b > a on that
 // value's list get one shared-memory increment; then a's slice of the
 // triangle (its Q partners b > a and its diagonal) is written once, in
-// ascending order. Needs nq counters in shared memory; lists hold local
-// indices, list x is [end[x] - counts[x], end[x]).
+// ascending order. The row's entries are split evenly over the threads (a
+// shared-memory prefix of its chunk lengths maps entry -> chunk), so rows of
+// one long chunk and rows of many short ones both keep every thread busy.
+// Shared memory: nq counters, then up to POST_SWEEP_MAX_CHUNKS + 1 prefix
+// words. Lists hold local indices, list x is [end[x] - counts[x], end[x]).
 constexpr uint32_t POST_SWEEP_THREADS = 256;
-constexpr uint32_t POST_SWEEP_MAX_ROWS = 53248;   // 208 KiB of counters
+constexpr uint32_t POST_SWEEP_MAX_CHUNKS = 2048;  // universe <= 2^27
+constexpr uint32_t POST_SWEEP_MAX_ROWS = 51200;   // 200 KiB of counters + 8 KiB of prefix
 
 __global__ void __launch_bounds__(POST_SWEEP_THREADS)
 postings_rows_kernel(ChunkView v, const uint32_t* __restrict__ qrows, uint32_t nq, const uint32_t* __restrict__ counts,
                      const uint32_t* __restrict__ end, const uint32_t* __restrict__ post, uint64_t n,
                      uint32_t* __restrict__ out) {
     extern __shared__ uint32_t cnt[];
-    __shared__ uint32_t card;
+    uint32_t* pref = cnt + nq;                 // pref[k] = entries of the row's chunks before chunk k
     for (uint32_t a = blockIdx.x; a < nq; a += gridDim.x) {
-        for (uint32_t b = threadIdx.x; b < nq; b += blockDim.x) cnt[b] = 0;
-        if (threadIdx.x == 0) card = 0;
-        __syncthreads();
         const uint32_t row = qrows[a];
-        const uint64_t c0 = v.row_off[row], c1 = v.row_off[row + 1];
-        uint32_t mine = 0;
-        // a thread per chunk (chunks of a sparse row are many and short)
-        for (uint64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
-            const uint32_t base = v.cid[c] << 16;
-            const uint16_t* l = v.lst + v.coff[c];
-            const uint32_t nl = v.ckl[c] & CK_LEN;
-            mine += nl;
-            for (uint32_t e = 0; e < nl; ++e) {
-                const uint32_t x = base | l[e];
-                const uint32_t len = counts[x];
-                if (len < 2) continue;
-                const uint32_t e1 = end[x];
-                for (uint32_t k = e1 - len; k < e1; ++k) {
-                    const uint32_t b = post[k];
-                    if (b > a) atomicAdd(&cnt[b], 1u);
-                }
+        const uint64_t c0 = v.row_off[row];
+        const uint32_t nc = (uint32_t)(v.row_off[row + 1] - c0);   // <= POST_SWEEP_MAX_CHUNKS (plain rows)
+        for (uint32_t b = threadIdx.x; b < nq; b += blockDim.x) cnt[b] = 0;
+        if (threadIdx.x == 0) {
+            uint32_t acc = 0;
+            for (uint32_t k = 0; k < nc; ++k) {
+                pref[k] = acc;
+                acc += v.ckl[c0 + k] & CK_LEN;
+            }
+            pref[nc] = acc;
+        }
+        __syncthreads();
+        const uint32_t total = pref[nc];
+        for (uint32_t e = threadIdx.x; e < total; e += blockDim.x) {
+            uint32_t lo = 0, hi = nc;              // last chunk k with pref[k] <= e
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (pref[mid] <= e) lo = mid;
+                else hi = mid;
+            }
+            const uint64_t c = c0 + lo;
+            const uint32_t x = (v.cid[c] << 16) | v.lst[v.coff[c] + (e - pref[lo])];
+            const uint32_t len = counts[x];
+            if (len < 2) continue;
+            const uint32_t e1 = end[x];
+            for (uint32_t k = e1 - len; k < e1; ++k) {
+                const uint32_t b = post[k];
+                if (b > a) atomicAdd(&cnt[b], 1u);
             }
         }
-        if (mine) atomicAdd(&card, mine);
         __syncthreads();
         const uint64_t base = tri_index(n, row, row) - row;   // out index of (row, j) is base + j
         for (uint32_t b = a + 1 + threadIdx.x; b < nq; b += blockDim.x) {
             const uint32_t gb = qrows[b];   // ascending: gb > row (the other order kept exact too)
             out[gb > row ? base + gb : tri_index(n, gb, row)] = cnt[b];
         }
-        if (threadIdx.x == 0) out[base + row] = card;
+        if (threadIdx.x == 0) out[base + row] = total;
         __syncthreads();
     }
 }
@@ -488,10 +520,35 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
     };
     if (mode == PAIRS_RECT) {   // the rectangle of rows [0, n1) x [n1, n1 + n2): sums only
         SB_CUDA(cudaEventRecord(log.ev0, st));
-        uint32_t* keep = d_out;
-        d_out = nullptr;
-        chunk_launch(PAIRS_RECT, n_pairs_all, nullptr, 0, n1, n1, n2);
-        d_out = keep;
+        // All rows plain: sum over values of (rows of the first set holding
+        // it) x (rows of the second set holding it), from two histograms.
+        const uint64_t U = ((uint64_t)d.max_cid + 1) * 65536;
+        bool plain = postings_mode != 0 && U <= POSTINGS_MAX_UNIVERSE && d.facts.size() == n1 + n2 &&
+                     n_pairs_all >= 1024;
+        for (uint64_t r = 0; plain && r < n1 + n2; ++r) plain = d.facts[r].plain;
+        if (plain) {
+            d_counts.reserve(U);
+            d_start.reserve(U);
+            SB_CUDA(cudaMemsetAsync(d_counts.p, 0, U * sizeof(uint32_t), st));
+            SB_CUDA(cudaMemsetAsync(d_start.p, 0, U * sizeof(uint32_t), st));
+            d_qrows.reserve(n2);
+            std::vector<uint32_t> second(n2);
+            for (uint64_t r = 0; r < n2; ++r) second[r] = (uint32_t)(n1 + r);
+            SB_CUDA(cudaMemcpyAsync(d_qrows.p, second.data(), n2 * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+            postings_hist_kernel<<<(uint32_t)std::min<uint64_t>((n1 + 7) / 8, (uint64_t)sms * 16), 256, 0, st>>>(
+                d.view(), nullptr, (uint32_t)n1, d_counts.p);
+            postings_hist_kernel<<<(uint32_t)std::min<uint64_t>((n2 + 7) / 8, (uint64_t)sms * 16), 256, 0, st>>>(
+                d.view(), d_qrows.p, (uint32_t)n2, d_start.p);
+            counts_dot_kernel<<<sms * 8, 256, 0, st>>>(d_counts.p, d_start.p, U, d_flags.p);
+            SB_CUDA(cudaGetLastError());
+            launches += 3;
+            last_postings_rows = n1 + n2;
+        } else {
+            uint32_t* keep = d_out;
+            d_out = nullptr;
+            chunk_launch(PAIRS_RECT, n_pairs_all, nullptr, 0, n1, n1, n2);
+            d_out = keep;
+        }
         SB_CUDA(cudaEventRecord(log.ev1, st));
         DeviceFlags f;
         SB_CUDA(cudaMemcpyAsync(&f, d_flags.p, sizeof(f), cudaMemcpyDeviceToHost, st));
@@ -759,11 +816,12 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
             const uint32_t gq = (uint32_t)std::min<uint64_t>((nq + 7) / 8, (uint64_t)sms * 16);
             postings_scatter_kernel<<<gq, 256, 0, st>>>(d.view(), d_qrows.p, (uint32_t)nq, d_start.p, d_post.p);
             if (sweep) {
-                const uint32_t smem = (uint32_t)(nq * sizeof(uint32_t));
+                const uint32_t smem = (uint32_t)((nq + POST_SWEEP_MAX_CHUNKS + 1) * sizeof(uint32_t));
                 static bool attr = false;
                 if (!attr) {
                     SB_CUDA(cudaFuncSetAttribute(postings_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)(POST_SWEEP_MAX_ROWS * sizeof(uint32_t))));
+                                                 (int)((POST_SWEEP_MAX_ROWS + POST_SWEEP_MAX_CHUNKS + 1) *
+                                                       sizeof(uint32_t))));
                     attr = true;
                 }
                 const uint32_t gr = (uint32_t)std::min<uint64_t>(nq, (uint64_t)sms * 8);

@@ -644,6 +644,8 @@ int STORM_rows_clear(STORM_rows_t* r) {
     return 1;
 }
 
+uint32_t STORM_rows_universe(const STORM_rows_t* r) { return r ? r->universe : 0; }
+
 uint64_t STORM_rows_size(const STORM_rows_t* r) { return r ? r->offs.size() - 1 : 0; }
 
 int STORM_rows_set_bitmap_budget(STORM_rows_t* r, uint64_t bytes) {

@@ -5,8 +5,7 @@
 // (storm.cpp:396-916): per row a STORM_bitmap_cont_t whose chunks are u16
 // lists below STORM_DEFAULT_SCALAR_THRESHOLD values and 1024-word bitmaps
 // otherwise, so callers that read the public structs see the same data.
-// Differences, all outside the reference's input contract and documented in
-// DESIGN.md:
+// Differences, all outside the reference's input contract:
 //   * the reference's one-past-the-end read in STORM_bitmap_cont_add
 //     (storm.cpp:768) and its scalar-buffer overflow when a second add brings
 //     more values than the remaining capacity (storm.cpp:513-523) are not

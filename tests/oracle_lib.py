@@ -68,6 +68,7 @@ def reference():
         "ref_contig_matrix_mt": (C.c_uint64, [u64p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, u32p, C.c_uint32]),
         "ref_storm_sum": (C.c_uint64, [u32p, u64p, C.c_uint64, C.c_uint32]),
         "ref_storm_sum_timed": (C.c_uint64, [u32p, u64p, C.c_uint64, C.POINTER(C.c_double)]),
+        "ref_storm_sum_mt": (C.c_uint64, [u32p, u64p, C.c_uint64, C.c_uint32, C.POINTER(C.c_double)]),
         "ref_storm_square": (C.c_uint64, [u32p, u64p, C.c_uint64, u32p, u64p, C.c_uint64]),
         "ref_storm_matrix": (C.c_uint64, [u32p, u64p, C.c_uint64, u32p]),
         "ref_storm_layout": (C.c_uint32, [u32p, C.c_uint32, u32p, u8p, u32p]),

@@ -310,3 +310,19 @@ def test_threshold_storm_t_matches_oracle(sb):
         np.testing.assert_array_equal(gi, wi)
         np.testing.assert_array_equal(gj, wj)
         np.testing.assert_array_equal(gc, wc)
+
+
+def test_square_of_plain_rows_by_histograms(sb):
+    """STORM_intersect_cardinality_square on plain rows (list and bitmap
+    chunks): the rectangle sum from two value histograms equals the oracle's."""
+    g = gen.rng(102)
+    xa = [gen.uniform_set(g, int(g.integers(1, 9000)), 1 << 19) for _ in range(60)]
+    xa += [gen.uniform_set(g, int(g.integers(70000, 120000)), 1 << 19) for _ in range(10)]   # bitmap chunks
+    yb = [gen.uniform_set(g, int(g.integers(1, 3000)), 1 << 19) for _ in range(50)]
+    a, b = build_storm(sb, xa), build_storm(sb, yb)
+    xv, xo = gen.to_csr(xa)
+    yv, yo = gen.to_csr(yb)
+    want = ol.oracle().oracle_sets_square(xv.ctypes.data_as(ol.u32p), xo.ctypes.data_as(ol.u64p), len(xa),
+                                          yv.ctypes.data_as(ol.u32p), yo.ctypes.data_as(ol.u64p), len(yb))
+    assert a.square(b) == want
+    assert b.square(a) == want
