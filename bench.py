@@ -41,6 +41,10 @@ sys.path.insert(0, ROOT)
 
 N_ROWS, M_BITS, P_RANGE, SEED = 65536, 262144, (0.05, 0.5), 0x5EED2
 L2_BYTES = 126 * 1000 * 1000
+# DRAM bytes per launch of the tensor-core kernel on the 65536 x 262144 workload:
+# one ncu capture at 16384 x 262144 (10.710 GB read + 0.525 GB written), scaled
+# by the pairs ratio 16 (tiles, and the rows they re-read, grow with the pairs).
+TS_TRAFFIC_BENCH_WORKLOAD = 11.2358e9 * 16
 METRIC = "exact pairs/sec & ns/pair on 1 B200: learned-batched vs plain GPU vs CPU"
 
 
@@ -766,6 +770,10 @@ def run_b200_arm(args):
                 "frac": achieved / peak,
                 "peak_source": f"2 x bf16_tflops {peak_src} ({peaks['bf16_tflops']}); int8 dense = 2 x bf16",
                 "algorithmic": f"pairs(i<=j) x {m} bit-MACs x 2 ops", "traffic": args.traffic}
+        if args.traffic is None and (n, m) == (N_ROWS, M_BITS) and kernel_used == "bb_mma_ts_kernel":
+            roof["traffic"] = TS_TRAFFIC_BENCH_WORKLOAD
+            roof["traffic_source"] = ("dram__bytes_read.sum + dram__bytes_write.sum of one launch at 16384 x 262144 "
+                                      "(11.24 GB, profiles/bb_mma_ts_dram_16384x262144.md) x 16 (pairs ratio)")
     else:
         ops = 2.0 * tri * m
         achieved = ops / (k_ms / 1e3) / 1e12
