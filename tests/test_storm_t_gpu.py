@@ -326,3 +326,30 @@ def test_square_of_plain_rows_by_histograms(sb):
                                           yv.ctypes.data_as(ol.u32p), yo.ctypes.data_as(ol.u64p), len(yb))
     assert a.square(b) == want
     assert b.square(a) == want
+
+
+def test_planner_at_the_largest_universe(sb):
+    """Values up to 2^27 - 1 (2048 chunks, the largest universe of the tensor
+    rows and the postings): forced tensor rows, forced postings and the
+    chunk kernel agree with the oracle."""
+    g = gen.rng(103)
+    top = (1 << 27) - 1
+    sets = []
+    for k in range(300):
+        v = gen.uniform_set(g, int(g.integers(1, 300)), 1 << 27)
+        if k % 7 == 0:
+            v = np.unique(np.concatenate([v, [top]])).astype(np.uint32)
+        sets.append(v)
+    s = build_storm(sb, sets)
+    vals, offs = gen.to_csr(sets)
+    want, ws = ol.sets_matrix(vals, offs)
+    for dense, post in ((1e-9, 0), (0.0, 1), (0.0, 3), (0.0, 0), (-1.0, -1)):
+        s.set_dense_block(dense)
+        s.set_sparse_postings(post)
+        mat, ssum = s.matrix()
+        if dense > 0:
+            assert s.last_dense()[0] == len(sets)
+        if post > 0:
+            assert s.last_postings_rows() == len(sets)
+        assert ssum == ws, (dense, post)
+        np.testing.assert_array_equal(mat, want, err_msg=f"{dense}/{post}")
