@@ -817,13 +817,9 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
             postings_scatter_kernel<<<gq, 256, 0, st>>>(d.view(), d_qrows.p, (uint32_t)nq, d_start.p, d_post.p);
             if (sweep) {
                 const uint32_t smem = (uint32_t)((nq + POST_SWEEP_MAX_CHUNKS + 1) * sizeof(uint32_t));
-                static bool attr = false;
-                if (!attr) {
-                    SB_CUDA(cudaFuncSetAttribute(postings_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)((POST_SWEEP_MAX_ROWS + POST_SWEEP_MAX_CHUNKS + 1) *
-                                                       sizeof(uint32_t))));
-                    attr = true;
-                }
+                static std::atomic<uint64_t> done{0};
+                smem_attr_once(postings_rows_kernel,
+                               (int)((POST_SWEEP_MAX_ROWS + POST_SWEEP_MAX_CHUNKS + 1) * sizeof(uint32_t)), done);
                 const uint32_t gr = (uint32_t)std::min<uint64_t>(nq, (uint64_t)sms * 8);
                 postings_rows_kernel<<<gr, POST_SWEEP_THREADS, smem, st>>>(d.view(), d_qrows.p, (uint32_t)nq,
                                                                            d_counts.p, d_start.p, d_post.p, n, d_out);

@@ -13,6 +13,7 @@
 #include <stdio.h>
 #include <new>
 #include <stdexcept>
+#include <atomic>
 #include <string>
 
 #include "../../include/storm.h"
@@ -113,6 +114,18 @@ struct DeviceFlags {
 };
 
 inline uint64_t tri_size(uint64_t n) { return n * (n + 1) / 2; }
+
+// Raises a kernel's dynamic shared-memory limit once per device (the
+// attribute is per device; `done` holds one bit per device ordinal).
+template <class K>
+inline void smem_attr_once(K* kernel, int bytes, std::atomic<uint64_t>& done) {
+    int dev = 0;
+    SB_CUDA(cudaGetDevice(&dev));
+    const uint64_t bit = 1ull << (dev & 63);
+    if (done.load() & bit) return;
+    SB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    done.fetch_or(bit);
+}
 
 }  // namespace sb200
 

@@ -77,14 +77,9 @@ void DenseEngine::launch(int kind, const uint64_t* dX, uint32_t n, uint32_t w_pa
     const int sms = require_device();
     if (count == 0) return;
     if (kind == STORM_B200_KERNEL_MMA) {
-        static bool attr_set = false;
-        if (!attr_set) {
-            SB_CUDA(cudaFuncSetAttribute(bb_mma_ts_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)TS_SMEM_BYTES));
-            SB_CUDA(cudaFuncSetAttribute(bb_mma_ts_long_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)TS_SMEM_BYTES));
-            attr_set = true;
-        }
+        static std::atomic<uint64_t> done_a{0}, done_b{0};
+        smem_attr_once(bb_mma_ts_kernel, (int)TS_SMEM_BYTES, done_a);
+        smem_attr_once(bb_mma_ts_long_kernel, (int)TS_SMEM_BYTES, done_b);
         // stream-K only for a launch over the whole tile list, whose output
         // triangle can be zeroed first for the partial-count atomics
         uint32_t grid = count < (uint32_t)sms ? count : (uint32_t)sms;
@@ -98,22 +93,15 @@ void DenseEngine::launch(int kind, const uint64_t* dX, uint32_t n, uint32_t w_pa
             bb_mma_ts_long_kernel<<<grid, TS_THREADS, smem, st>>>(dX, n, w_pad, d_tiles.p + t0, count, d_out,
                                                                   d_flags.p, ks);
     } else if (kind == STORM_B200_KERNEL_MMA_SS) {
-        static bool attr_set = false;
-        if (!attr_set) {
-            SB_CUDA(cudaFuncSetAttribute(bb_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)MMA_SMEM_BYTES));
-            attr_set = true;
-        }
+        static std::atomic<uint64_t> done{0};
+        smem_attr_once(bb_mma_kernel, (int)MMA_SMEM_BYTES, done);
         const uint32_t grid = count < (uint32_t)sms ? count : (uint32_t)sms;
         bb_mma_kernel<<<grid, MMA_THREADS, MMA_SMEM_BYTES, st>>>(dX, n, w_pad, d_tiles.p + t0, count, d_out,
                                                                   d_flags.p);
     } else {
         const size_t smem = sizeof(PopcSmem);
-        static bool attr_set = false;
-        if (!attr_set) {
-            SB_CUDA(cudaFuncSetAttribute(bb_popc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            attr_set = true;
-        }
+        static std::atomic<uint64_t> done{0};
+        smem_attr_once(bb_popc_kernel, (int)smem, done);
         const uint32_t cap = (uint32_t)sms * 2;
         const uint32_t grid = count < cap ? count : cap;
         bb_popc_kernel<<<grid, POPC_THREADS, smem, st>>>(dX, n, w_pad, d_tiles.p + t0, count, d_out, d_flags.p);
@@ -407,14 +395,9 @@ uint64_t DenseEngine::run_threshold(const uint64_t* dX, uint64_t n, uint32_t w_p
     SB_CUDA(cudaEventRecord(log.ev0, st));
     uint64_t found = 0;
     if (kind == STORM_B200_KERNEL_MMA) {
-        static bool attr_set = false;
-        if (!attr_set) {
-            SB_CUDA(cudaFuncSetAttribute(bb_mma_ts_thresh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)TS_SMEM_BYTES));
-            SB_CUDA(cudaFuncSetAttribute(bb_mma_ts_thresh_long_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)TS_SMEM_BYTES));
-            attr_set = true;
-        }
+        static std::atomic<uint64_t> done_a{0}, done_b{0};
+        smem_attr_once(bb_mma_ts_thresh_kernel, (int)TS_SMEM_BYTES, done_a);
+        smem_attr_once(bb_mma_ts_thresh_long_kernel, (int)TS_SMEM_BYTES, done_b);
         SB_CUDA(cudaMemsetAsync(d_found.p, 0, sizeof(unsigned long long), st));
         row_popcount_kernel<<<(uint32_t)std::min<uint64_t>((n + 7) / 8, (uint64_t)sms * 16), 256, 0, st>>>(
             dX, n, w_pad, d_card.p);
@@ -464,14 +447,9 @@ void launch_ts_rows(const uint64_t* X, uint32_t n, uint32_t w_pad, const uint2* 
                     bool out_zeroed) {
     const int sms = require_device();
     if (n_tiles == 0) return;
-    static bool attr_set = false;
-    if (!attr_set) {
-        SB_CUDA(cudaFuncSetAttribute(bb_mma_ts_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)TS_SMEM_BYTES));
-        SB_CUDA(cudaFuncSetAttribute(bb_mma_ts_rows_long_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)TS_SMEM_BYTES));
-        attr_set = true;
-    }
+    static std::atomic<uint64_t> done_a{0}, done_b{0};
+    smem_attr_once(bb_mma_ts_rows_kernel, (int)TS_SMEM_BYTES, done_a);
+    smem_attr_once(bb_mma_ts_rows_long_kernel, (int)TS_SMEM_BYTES, done_b);
     if ((uint64_t)w_pad * 64 > MMA_MAX_BITS_W4) fail(STORM_B200_ELIMIT, "dense block rows longer than 2^27 bits");
     // With stream-K the partial counts are added into out, so the whole
     // triangle is zeroed first; the other phases write their own pairs after.
