@@ -87,8 +87,9 @@ int STORM_contig_add_bitmaps(STORM_contiguous_t* c, const uint64_t* words,
 uint64_t STORM_contig_size(const STORM_contiguous_t* c);
 int STORM_contig_set_kernel(STORM_contiguous_t* c, int kernel);
 /* Work schedule of the tensor-core kernel: STORM_B200_SCHED_AUTO picks per
- * launch (stream-K when the last wave of whole tiles would be less than 95 %
- * full), _TILES deals whole tiles round robin, _STREAM_K always
+ * launch (stream-K when the last wave of whole tiles would be less than
+ * 98.5 % full and rows have at least 32768 bits), _TILES deals whole tiles
+ * round robin, _STREAM_K always
  * splits the (tile, K stage) space evenly over the SMs. Counts are the same
  * under every schedule. */
 #define STORM_B200_SCHED_AUTO     0

@@ -10,20 +10,22 @@
 namespace sb200 {
 
 // Work schedule of the tensor-core kernel (TsSched in bb_mma_ts.cuh): whole
-// tiles round robin when the last wave is nearly full (>= 95 %) or a tile
-// has fewer than 32 K stages; otherwise stream-K over the (tile, K stage)
-// space, at least 32 stages (8192 bits) per CTA so the per-segment epilogue
-// stays small against the MMAs. Measured on B200: 272 tiles (1.8 waves) of
-// 2^18-bit rows run 8 % faster under stream-K, 136 tiles 1.9x, 1088 tiles
-// (7.4 waves, 92 % fill) 7 %; 2176 tiles (98 % fill) 3 % slower. Returns the
-// kernel's k_splits argument (1 or 0) and sets the grid.
+// tiles round robin when the last wave is nearly full (>= 98.5 %) or a tile
+// has fewer than 128 K stages (32768 bits: shorter tiles lose more to the
+// extra segment boundaries and partial-tile atomics than they gain); else
+// stream-K over the (tile, K stage) space, at least 32 stages per CTA.
+// Measured on B200: 272 tiles (1.8 waves) of 2^18-bit rows run 8 % faster
+// under stream-K, 136 tiles 1.9x, 1088 tiles (92 % fill) 7 %, 4160 tiles
+// (97 % fill) 3 %; 2176 tiles (98 % fill) of 2^16-bit rows 3 % slower, and
+// 80-stage tiles (20000-bit rows) 7 % slower. Returns the kernel's k_splits
+// argument (1 or 0) and sets the grid.
 static uint32_t ts_schedule(uint32_t n_tiles, int sms, uint32_t w_pad, uint32_t& grid,
                             int pref = STORM_B200_SCHED_AUTO) {
     const uint64_t nk = w_pad / (TS_KBITS / 64);
     const uint64_t waves = ((uint64_t)n_tiles + sms - 1) / sms;
     const double fill = waves ? (double)n_tiles / (double)(waves * (uint64_t)sms) : 1.0;
     const bool tiles = pref == STORM_B200_SCHED_TILES ||
-                       (pref == STORM_B200_SCHED_AUTO && (fill >= 0.95 || nk < 32));
+                       (pref == STORM_B200_SCHED_AUTO && (fill >= 0.985 || nk < 128));
     if (tiles) {
         grid = n_tiles < (uint32_t)sms ? n_tiles : (uint32_t)sms;
         return 1;
