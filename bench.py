@@ -557,15 +557,26 @@ def storm_t_forms(device, cpu_seconds=2.0, only=None):
         n = len(sets)
         pairs = n * (n + 1) // 2
         s = sb.Storm()
+        t_add = time.perf_counter()
         for v in sets:
             s.add(v)
-        s.upload()
-        res = {"workload": desc, "pairs_i_le_j": pairs, "setup_s": round(time.perf_counter() - t0, 1)}
+        t_add = time.perf_counter() - t_add
+        res = {"workload": desc, "pairs_i_le_j": pairs}
         sums = set()
         forms = [("gpu_default", -1.0, -1)]
         if n <= 4096:
             forms.insert(0, ("gpu_chunk_kernel", 0.0, 0))
         buf = np.zeros(pairs, np.uint32)
+        # End to end through the C ABI: the first per-pair call packs the rows,
+        # uploads them and copies the triangle back to host memory.
+        t_e2e = time.perf_counter()
+        _, v = s.matrix(buf)
+        t_e2e = time.perf_counter() - t_e2e
+        sums.add(v)
+        res["e2e"] = {"STORM_add_s": round(t_add, 3), "first_matrix_call_s": round(t_e2e, 3),
+                      "pairs_per_s_incl_pack_upload_download": pairs / t_e2e,
+                      "d2h_bytes": pairs * 4}
+        res["setup_s"] = round(time.perf_counter() - t0, 1)
         for form, thr, post in forms:
             s.set_dense_block(thr)
             s.set_sparse_postings(post)
