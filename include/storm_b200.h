@@ -96,6 +96,14 @@ int STORM_contig_set_kernel(STORM_contiguous_t* c, int kernel);
 #define STORM_B200_SCHED_TILES    1
 #define STORM_B200_SCHED_STREAM_K 2
 int STORM_contig_set_schedule(STORM_contiguous_t* c, int schedule);
+/* Autotuner (no counterpart in the reference): times this container's own
+ * all-pairs call on the GPU with each bitmap x bitmap kernel that is exact
+ * for its row length -- tcgen05 with A in tensor memory under whole-tile and
+ * stream-K schedules, tcgen05 with both operands in shared memory, CUDA-core
+ * POPC -- best of two calls each, and keeps the fastest kernel and schedule
+ * for later calls.  times_ms (4 entries in that order, -1 when skipped) and
+ * the choice are reported when non-NULL.  Counts do not depend on it. */
+int STORM_contig_autotune(STORM_contiguous_t* c, int* best_kernel, int* best_schedule, double* times_ms);
 /* Pack the rows into HBM now (otherwise done by the first all-pairs call). */
 int STORM_contig_upload(STORM_contiguous_t* c);
 /* Per-pair counts into a HOST buffer of out_len >= n*(n+1)/2 entries. */
@@ -212,6 +220,14 @@ uint64_t STORM_last_dense_panels(const STORM_t* s);
  * and 3 force the rows in and pick the list-by-list or the row-sweep form.
  * Counts are identical. */
 int STORM_set_sparse_postings(STORM_t* s, int mode);
+/* Autotuner (no counterpart in the reference): times the per-pair all-pairs
+ * call on the GPU with the tensor-core rows on (cost rule) or off, crossed
+ * with the postings on (cost rule) or off, best of two calls each, and keeps
+ * the fastest settings for later calls (as STORM_set_dense_block(s, -1 or 0,
+ * budget unchanged) and STORM_set_sparse_postings(s, -1 or 0)).  times_ms (4
+ * entries: both on, postings off, tensor rows off, both off) and the choice
+ * are reported when non-NULL.  Counts do not depend on the choice. */
+int STORM_autotune(STORM_t* s, double* best_min_density, int* best_postings, double* times_ms);
 uint64_t STORM_last_postings_rows(const STORM_t* s);
 
 #ifdef __cplusplus

@@ -112,8 +112,21 @@ int STORM_rows_set_dense_block(STORM_rows_t* r, double min_density);
  * plus a 9th word of representation flags (bit 0 bitmap, 1 complement). */
 int STORM_rows_meta(STORM_rows_t* r, uint64_t row, uint32_t* meta9);
 
+/* Autotuner (no counterpart in the reference, which fixes its tile at 64):
+ * times this container's own all-pairs sum on the GPU for every tile in
+ * {32, 64, 128, 256} x tensor dense-block threshold in {0, 2^-16, 2^-14,
+ * 2^-12} under the given policy and execution form (best of two calls each;
+ * a trained learned selector keeps its training tile), then keeps the
+ * fastest: the threshold becomes the container's dense block and the tile
+ * is used by later calls that pass tile 0.  times_ms (16 entries, tile-major,
+ * -1 for a skipped candidate) and the choice are reported when non-NULL.
+ * Counts do not depend on the choice. */
+int STORM_rows_autotune(STORM_rows_t* r, int policy, int exec, uint32_t* best_tile, double* best_min_density,
+                        double* times_ms);
+
 /* storm::allpairs_sum: sum over i < j (plus stats). fixed_cell is used by
- * STORM_POLICY_FIXED.  tile 0 means 64 (storm_allpairs.h:152-201). */
+ * STORM_POLICY_FIXED.  tile 0 means 64 (storm_allpairs.h:152-201), or the
+ * tile STORM_rows_autotune chose. */
 int STORM_rows_allpairs_sum(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell, int exec,
                             STORM_allpairs_stats* st);
 /* Per-pair counts, packed upper triangle in ORIGINAL row order. */

@@ -69,6 +69,10 @@ _sig("STORM_contig_add_bitmaps", C.c_int, [C.c_void_p, u64p, C.c_uint32, C.c_uin
 _sig("STORM_contig_size", C.c_uint64, [C.c_void_p])
 _sig("STORM_contig_set_kernel", C.c_int, [C.c_void_p, C.c_int])
 _sig("STORM_contig_set_schedule", C.c_int, [C.c_void_p, C.c_int])
+_sig("STORM_contig_autotune", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)])
+_sig("STORM_autotune", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_double)])
+_sig("STORM_rows_autotune", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_double),
+                                      C.POINTER(C.c_double)])
 _sig("STORM_contig_pairw_threshold", C.c_int, [C.c_void_p, C.c_double, u32p, u32p, u32p, C.c_uint64,
                                                C.POINTER(C.c_uint64)])
 _sig("STORM_load_stormbin", C.c_int64, [C.c_void_p, C.c_char_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32)])
@@ -274,6 +278,13 @@ class StormContig:
     def threshold(self, jaccard_min: float, cap: int = 1 << 20):
         return _threshold(_lib.STORM_contig_pairw_threshold, self.h, jaccard_min, cap)
 
+    def autotune(self):
+        """Time every exact kernel/schedule on these rows and keep the fastest:
+        (kernel, schedule, times_ms[4])."""
+        k, sc, t = C.c_int(0), C.c_int(0), (C.c_double * 4)()
+        _check(_lib.STORM_contig_autotune(self.h, C.byref(k), C.byref(sc), t), "STORM_contig_autotune")
+        return k.value, sc.value, list(t)
+
     def set_schedule(self, schedule: int):
         _check(_lib.STORM_contig_set_schedule(self.h, schedule), "STORM_contig_set_schedule")
 
@@ -409,6 +420,12 @@ class Storm:
         _check(int(r), "STORM_load_stormpack")
         self.n += int(r)
         return int(r), int(nb.value)
+
+    def autotune(self):
+        """(min_density, postings_mode, times_ms[4]) kept for later calls."""
+        dm, pm, t = C.c_double(0), C.c_int(0), (C.c_double * 4)()
+        _check(_lib.STORM_autotune(self.h, C.byref(dm), C.byref(pm), t), "STORM_autotune")
+        return dm.value, pm.value, list(t)
 
     def set_sparse_postings(self, mode: int):
         _check(_lib.STORM_set_sparse_postings(self.h, int(mode)), "STORM_set_sparse_postings")
@@ -551,6 +568,12 @@ class StormRows:
 
     def set_dense_block(self, min_density: float):
         _check(_lib.STORM_rows_set_dense_block(self.h, float(min_density)), "STORM_rows_set_dense_block")
+
+    def autotune(self, policy, exec_=EXEC_BATCHED):
+        """(tile, min_density, times_ms[16]) kept for later calls with tile 0."""
+        bt, bd, t = C.c_uint32(0), C.c_double(0), (C.c_double * 16)()
+        _check(_lib.STORM_rows_autotune(self.h, policy, exec_, C.byref(bt), C.byref(bd), t), "STORM_rows_autotune")
+        return bt.value, bd.value, list(t)
 
     def meta(self, row: int) -> np.ndarray:
         m = np.zeros(9, dtype=np.uint32)

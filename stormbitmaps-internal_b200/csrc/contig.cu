@@ -235,6 +235,48 @@ int STORM_contig_set_schedule(STORM_contiguous_t* c, int schedule) {
     return 0;
 }
 
+int STORM_contig_autotune(STORM_contiguous_t* c, int* best_kernel, int* best_schedule, double* times_ms) {
+    if (c == NULL) return STORM_B200_ENULL;
+    return guard([&]() -> int {
+        const uint64_t n = c->n_rows;
+        contig_flush(c);
+        c->d_out.reserve(tri_size(n) ? tri_size(n) : 1);
+        const uint64_t bits = c->vector_length;
+        // tcgen05 (A in TMEM) under both schedules, tcgen05 with both operands
+        // in shared memory, CUDA-core POPC -- each where it is exact.
+        const int kern[4] = {STORM_B200_KERNEL_MMA, STORM_B200_KERNEL_MMA, STORM_B200_KERNEL_MMA_SS,
+                             STORM_B200_KERNEL_POPC};
+        const int sched[4] = {STORM_B200_SCHED_TILES, STORM_B200_SCHED_STREAM_K, STORM_B200_SCHED_AUTO,
+                              STORM_B200_SCHED_AUTO};
+        const bool ok[4] = {bits <= TC_MAX_ROW_BITS, bits <= TC_MAX_ROW_BITS, bits <= TC_SS_MAX_ROW_BITS, true};
+        const int keep_sched = c->engine.schedule;
+        double best = -1.0;
+        int bk = c->kernel_pref, bs = keep_sched;
+        for (int k = 0; k < 4; ++k) {
+            if (times_ms) times_ms[k] = -1.0;
+            if (!ok[k] || n == 0) continue;
+            c->engine.schedule = sched[k];
+            double ms = -1.0;
+            for (int rep = 0; rep < 2; ++rep) {
+                c->engine.run(c->d_rows.p, c->dev_rows, c->w_pad, bits, c->d_out.p, kern[k], contig_stream(c));
+                const double m = c->engine.log.last_ms;
+                ms = ms < 0 ? m : std::min(ms, m);
+            }
+            if (times_ms) times_ms[k] = ms;
+            if (best < 0 || ms < best) {
+                best = ms;
+                bk = kern[k];
+                bs = sched[k];
+            }
+        }
+        c->kernel_pref = bk;
+        c->engine.schedule = bs;
+        if (best_kernel) *best_kernel = bk;
+        if (best_schedule) *best_schedule = bs;
+        return 0;
+    });
+}
+
 int STORM_contig_upload(STORM_contiguous_t* c) {
     if (c == NULL) return STORM_B200_ENULL;
     return guard([&]() -> int {

@@ -60,6 +60,8 @@ inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
 void build_mma_tiles(std::vector<uint2>& t, uint64_t n);
 // Longest row the tensor-core kernels count exactly (4-byte weight cycle).
 constexpr uint64_t TC_MAX_ROW_BITS = 1ull << 27;
+// ... and the shared-memory form (8-byte weight cycle only).
+constexpr uint64_t TC_SS_MAX_ROW_BITS = 1ull << 23;
 
 // Tensor-core kernel over n gathered rows X ([>= roundup(n, 256)][w_pad]);
 // count (i, j) lands at the packed index of (row_map[i], row_map[j]) in a

@@ -361,6 +361,8 @@ struct STORM_rows_s {
     DevBuf<RowsStatsDev> d_stats;
     // tensor-core dense block
     double dense_min_density = 1.0 / 16384.0;
+    uint32_t tuned_tile = 0;      // STORM_rows_autotune's tile (used for calls with tile 0)
+    uint32_t trained_tile = 0;    // the tile the learned selector was trained on
     DevBuf<uint64_t> d_dense;
     DevBuf<uint32_t> d_dmap;
     DevBuf<uint2> d_dtiles;
@@ -450,7 +452,7 @@ static void rows_run(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell,
     rows_ensure_uploaded(r);
     cudaStream_t st = rows_stream(r);
     const uint32_t n = (uint32_t)(r->offs.size() - 1);
-    const uint32_t T = tile ? tile : 64;
+    const uint32_t T = tile ? tile : (r->tuned_tile ? r->tuned_tile : 64);
     STORM_allpairs_stats S{};
     if (policy == STORM_POLICY_ALLBITMAP)
         for (uint32_t i = 0; i < n; ++i)
@@ -688,6 +690,51 @@ int STORM_rows_meta(STORM_rows_t* r, uint64_t row, uint32_t* meta9) {
     });
 }
 
+int STORM_rows_autotune(STORM_rows_t* r, int policy, int exec, uint32_t* best_tile, double* best_min_density,
+                        double* times_ms) {
+    if (r == NULL) return STORM_B200_ENULL;
+    return guard([&]() -> int {
+        // Candidates: tile x dense-block threshold. A trained learned selector
+        // keeps the tile it was trained on (its features are per tile).
+        const uint32_t tiles[4] = {32, 64, 128, 256};
+        const double dens[4] = {0.0, 1.0 / 65536, 1.0 / 16384, 1.0 / 4096};
+        const bool fixed_tile = policy == STORM_POLICY_LEARNED && r->mlp.trained && r->trained_tile;
+        const double keep_density = r->dense_min_density;
+        double best = -1.0;
+        uint32_t bt = 64;
+        double bd = keep_density;
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b < 4; ++b) {
+                const int k = a * 4 + b;
+                if (times_ms) times_ms[k] = -1.0;
+                if (fixed_tile && tiles[a] != r->trained_tile) continue;
+                r->dense_min_density = dens[b];
+                STORM_allpairs_stats st{};
+                double ms = -1.0;
+                for (int rep = 0; rep < 2; ++rep) {   // first call builds the launch; keep the faster
+                    rows_run(r, policy, tiles[a], STORM_PAIRING_BS, exec, nullptr, &st);
+                    const double m = st.ns_total * 1e-6;
+                    ms = ms < 0 ? m : std::min(ms, m);
+                }
+                if (times_ms) times_ms[k] = ms;
+                if (best < 0 || ms < best) {
+                    best = ms;
+                    bt = tiles[a];
+                    bd = dens[b];
+                }
+            }
+        r->dense_min_density = bd;
+        r->tuned_tile = bt;
+        if (r->graph) {
+            cudaGraphExecDestroy(r->graph);
+            r->graph = nullptr;
+        }
+        if (best_tile) *best_tile = bt;
+        if (best_min_density) *best_min_density = bd;
+        return 0;
+    });
+}
+
 int STORM_rows_allpairs_sum(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell, int exec,
                             STORM_allpairs_stats* st) {
     if (r == NULL) return STORM_B200_ENULL;
@@ -719,9 +766,9 @@ int STORM_rows_allpairs_tiles(STORM_rows_t* r, int policy, uint32_t tile, int ex
     if (r == NULL) return STORM_B200_ENULL;
     if (cb == NULL) return STORM_B200_EARG;
     const uint64_t n = r->offs.size() - 1;
-    const uint32_t T = tile ? tile : 64;
+    const uint32_t T = tile ? tile : 64;   // the callback's tile; the computation may use a tuned one
     std::vector<uint32_t> tri(tri_size(n) ? tri_size(n) : 1);
-    int rc = STORM_rows_allpairs_matrix(r, policy, T, STORM_PAIRING_BS, exec, tri.data(), tri.size(), st);
+    int rc = STORM_rows_allpairs_matrix(r, policy, tile, STORM_PAIRING_BS, exec, tri.data(), tri.size(), st);
     if (rc < 0) return rc;
     return guard([&]() -> int {
         std::vector<uint32_t> buf((size_t)T * T);
@@ -855,6 +902,7 @@ int STORM_rows_train_selector(STORM_rows_t* r, uint32_t tile, uint32_t samples, 
         const uint32_t n = (uint32_t)(r->offs.size() - 1);
         if (n < 2) return STORM_B200_EARG;
         const uint32_t T = tile ? tile : 64;
+        r->trained_tile = T;
         const std::vector<uint32_t> order = rows_order(r, STORM_POLICY_PERTILE);
         const uint32_t nb = (n + T - 1) / T, ntiles = nb * (nb + 1) / 2;
         r->d_order.reserve(n);

@@ -577,6 +577,45 @@ int STORM_set_dense_block(STORM_t* s, double min_density, uint64_t budget_bytes)
 uint64_t STORM_last_dense_rows(const STORM_t* s) { return s ? state_of(s)->engine.last_dense_rows : 0; }
 uint64_t STORM_last_dense_panels(const STORM_t* s) { return s ? state_of(s)->engine.last_dense_panels : 0; }
 
+int STORM_autotune(STORM_t* s, double* best_min_density, int* best_postings, double* times_ms) {
+    if (s == NULL) return STORM_B200_ENULL;
+    return guard([&]() -> int {
+        StormDev* d = state_of(s);
+        ensure_packed(s, d);
+        cudaStream_t st = stream_of(d);
+        const uint64_t n = s->n_conts;
+        d->d_out.reserve(tri_size(n) ? tri_size(n) : 1);
+        // Which engines may take rows: tensor rows by the cost rule or none,
+        // postings by cost or none; timed with the per-pair call.
+        const double dens[4] = {CHUNK_DENSE_AUTO, CHUNK_DENSE_AUTO, 0.0, 0.0};
+        const int post[4] = {-1, 0, -1, 0};
+        double best = -1.0;
+        double bd = d->engine.dense_min_density;
+        int bp = d->engine.postings_mode;
+        for (int k = 0; k < 4; ++k) {
+            d->engine.dense_min_density = dens[k];
+            d->engine.postings_mode = post[k];
+            double ms = -1.0;
+            for (int rep = 0; rep < 2; ++rep) {
+                d->engine.run(d->dev, PAIRS_TRIANGLE, n, 0, d->d_out.p, st);
+                const double m = d->engine.log.last_ms;
+                ms = ms < 0 ? m : std::min(ms, m);
+            }
+            if (times_ms) times_ms[k] = ms;
+            if (best < 0 || ms < best) {
+                best = ms;
+                bd = dens[k];
+                bp = post[k];
+            }
+        }
+        d->engine.dense_min_density = bd;
+        d->engine.postings_mode = bp;
+        if (best_min_density) *best_min_density = bd;
+        if (best_postings) *best_postings = bp;
+        return 0;
+    });
+}
+
 int STORM_set_sparse_postings(STORM_t* s, int mode) {
     if (s == NULL) return STORM_B200_ENULL;
     if (mode < -1 || mode > 3) return STORM_B200_EARG;

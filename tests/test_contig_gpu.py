@@ -347,3 +347,29 @@ def test_threshold_long_rows_and_small_cap(sb):
     assert rc == sb.ESIZE and f.value == len(wi)
     want = {(a, b, v) for a, b, v in zip(wi.tolist(), wj.tolist(), wc.tolist())}
     assert all((a, b, v) in want for a, b, v in zip(oi.tolist(), oj.tolist(), oc.tolist()))
+
+
+def test_autotune_keeps_the_fastest_exact_kernel(sb):
+    """The autotuner times every kernel/schedule exact for the row length on
+    these rows, keeps the fastest, and later calls stay exact."""
+    n, m = 700, 16384
+    words = gen.bernoulli_rows(n, m, (0.05, 0.6), seed=901)
+    want, ws = ol.contig_matrix(words)
+    c = contig_from_words(sb, words, m, "mma")
+    k, sched, times = c.autotune()
+    assert all(t > 0 for t in times)
+    cands = [(sb.KERNEL_MMA, sb.SCHED_TILES), (sb.KERNEL_MMA, sb.SCHED_STREAM_K), (sb.KERNEL_MMA_SS, sb.SCHED_AUTO),
+             (sb.KERNEL_POPC, sb.SCHED_AUTO)]
+    assert (k, sched) == cands[int(np.argmin(times))]
+    mat, s = c.matrix()
+    assert s == ws and c.last_kernel() == k
+    np.testing.assert_array_equal(mat, want)
+    # rows past 2^23 bits: only the tensor-core kernel in the 4-byte cycle and POPC qualify
+    m = (1 << 23) + 64
+    g = gen.rng(902)
+    words = g.integers(0, 1 << 63, size=(20, (m + 63) // 64), dtype=np.uint64)
+    words[:, -1] &= np.uint64((1 << (m % 64)) - 1)
+    c = contig_from_words(sb, words, m, "mma")
+    k, sched, times = c.autotune()
+    assert times[2] == -1.0 and times[0] > 0 and times[3] > 0
+    assert c.matrix()[1] == ol.contig_matrix(words)[1]

@@ -166,3 +166,26 @@ def test_rows_without_bitmaps_stay_exact(sb):
     for pol in ("PERPAIR", "PERTILE", "PROBE", "REFINE"):
         mat, st = r.allpairs_matrix(getattr(sb, "POLICY_" + pol), 16)
         np.testing.assert_array_equal(mat, want, err_msg=pol)
+
+
+def test_autotune_tile_and_dense_block(sb):
+    """The kernel-layer autotuner times tile x dense-block candidates on the
+    corpus, keeps the fastest (tile used when calls pass tile 0), and a
+    trained learned selector keeps its training tile."""
+    g = gen.rng(903)
+    sets = gen.zipf_sets(400, 1 << 18, 1.1, 16, 1 << 15, 904)
+    r = rows_of(sb, sets, 1 << 18)
+    vals, offs = gen.to_csr(sets)
+    want, ws = ol.sets_matrix(vals, offs)
+    tile, dens, times = r.autotune(sb.POLICY_PERTILE)
+    assert all(t > 0 for t in times)
+    k = int(np.argmin(times))
+    assert tile == (32, 64, 128, 256)[k // 4] and dens == (0.0, 1 / 65536, 1 / 16384, 1 / 4096)[k % 4]
+    mat, st = r.allpairs_matrix(sb.POLICY_PERTILE, 0)
+    assert st["sum"] == ws
+    np.testing.assert_array_equal(mat, want)
+    r.train_selector(tile=64, samples=256, epochs=50, seed=3)
+    tile, dens, times = r.autotune(sb.POLICY_LEARNED)
+    assert tile == 64 and all(t < 0 for k, t in enumerate(times) if k // 4 != 1)
+    mat, st = r.allpairs_matrix(sb.POLICY_LEARNED, 0)
+    np.testing.assert_array_equal(mat, want)

@@ -353,3 +353,21 @@ def test_planner_at_the_largest_universe(sb):
             assert s.last_postings_rows() == len(sets)
         assert ssum == ws, (dense, post)
         np.testing.assert_array_equal(mat, want, err_msg=f"{dense}/{post}")
+
+
+def test_autotune_storm_t(sb):
+    """The STORM_t autotuner times the planner with tensor rows and postings on
+    or off, keeps the fastest, and later calls stay exact."""
+    g = gen.rng(905)
+    sets = [gen.uniform_set(g, int(g.integers(1000, 6000)), 1 << 20) for _ in range(260)]
+    sets += gen.bernoulli_sets(300, 1 << 20, 2e-5, 906)
+    s = build_storm(sb, sets)
+    vals, offs = gen.to_csr(sets)
+    want, ws = ol.sets_matrix(vals, offs)
+    dens, post, times = s.autotune()
+    assert all(t > 0 for t in times)
+    k = int(np.argmin(times))
+    assert (dens, post) == ((-1.0, -1), (-1.0, 0), (0.0, -1), (0.0, 0))[k]
+    mat, ssum = s.matrix()
+    assert ssum == ws
+    np.testing.assert_array_equal(mat, want)
