@@ -285,7 +285,7 @@ def mixed_density_forms(sb, device, n=4096, universe=1 << 20, tile=64):
     out["train_s"] = round(time.perf_counter() - t0, 2)
     out["selector"] = {k: (round(v, 4) if isinstance(v, float) else v) for k, v in sel.items()}
 
-    def best_of(policy, exec_, reps=3):
+    def best_of(policy, exec_, reps=3, tile=tile):
         times, s = [], None
         for _ in range(reps):
             s, st = r.allpairs_sum(policy, tile, exec_=exec_)
@@ -308,7 +308,19 @@ def mixed_density_forms(sb, device, n=4096, universe=1 << 20, tile=64):
             raise RuntimeError(f"{name}: sum {s} != {ref_sum}")
         forms[name] = {"pairs_per_s": pairs / (ns * 1e-9), "ms": ns * 1e-6, "launches": st["launches"],
                        "cell_pairs": st["cell_pairs"]}
+    # Autotuned: tile x dense-block threshold timed on this corpus (the
+    # learned selector keeps its training tile), best kept for tile-0 calls.
+    for name, pol in (("batched_cost_model_autotuned", sb.POLICY_PERTILE),
+                      ("batched_learned_autotuned", sb.POLICY_LEARNED)):
+        t_tile, t_dens, _ = r.autotune(pol, sb.EXEC_BATCHED)
+        s, ns, st = best_of(pol, sb.EXEC_BATCHED, tile=0)
+        if s != ref_sum:
+            raise RuntimeError(f"{name}: sum {s} != {ref_sum}")
+        forms[name] = {"pairs_per_s": pairs / (ns * 1e-9), "ms": ns * 1e-6, "launches": st["launches"],
+                       "tile": t_tile, "dense_block_min_density": t_dens, "cell_pairs": st["cell_pairs"]}
     out["forms"] = forms
+    out["learned_autotuned_over_plain"] = (forms["batched_learned_autotuned"]["pairs_per_s"] /
+                                           forms["plain_per_tile_cost_model"]["pairs_per_s"])
     out["learned_over_plain"] = forms["batched_learned"]["pairs_per_s"] / forms["plain_per_tile_cost_model"]["pairs_per_s"]
     out["learned_tensor_block_over_plain"] = (forms["batched_learned_tensor_block"]["pairs_per_s"] /
                                               forms["plain_per_tile_cost_model"]["pairs_per_s"])
@@ -442,6 +454,25 @@ def config5a_full(sb, device, steps=3):
     c.close()
     torch.cuda.empty_cache()
     return res
+
+
+def autotune_config1(sb, device):
+    """The contiguous autotuner on the config 1 geometry (4096 rows x 65536
+    bits, Bernoulli(0.5)): per-candidate device times and the kept choice."""
+    import torch
+    rows = bernoulli_rows_gpu(4096, 65536, 0.5, 0xC001, device)
+    torch.cuda.synchronize()
+    c = sb.StormContig(65536)
+    rc = sb.lib().STORM_contig_add_bitmaps(c.h, C.cast(rows.data_ptr(), sb.u64p), 4096, 1024)
+    if rc < 0:
+        raise sb.StormError(rc, "STORM_contig_add_bitmaps")
+    k, sched, times = c.autotune()
+    names = ("tcgen05_ts_tiles", "tcgen05_ts_stream_k", "tcgen05_ss", "popc")
+    c.close()
+    return {"workload": "4096 rows x 65536 bits, Bernoulli(0.5)",
+            "candidates_ms": {nm: round(t, 4) for nm, t in zip(names, times)},
+            "kept": names[[(sb.KERNEL_MMA, sb.SCHED_TILES), (sb.KERNEL_MMA, sb.SCHED_STREAM_K),
+                           (sb.KERNEL_MMA_SS, sb.SCHED_AUTO), (sb.KERNEL_POPC, sb.SCHED_AUTO)].index((k, sched))]}
 
 
 def config45_forms(device):
@@ -872,6 +903,10 @@ def run_b200_arm(args):
             line["storm_t"] = storm_t_forms(device)
         except Exception as e:
             line["storm_t"] = {"error": f"{type(e).__name__}: {e}"}
+        try:
+            line["autotune_config1"] = autotune_config1(sb, device)
+        except Exception as e:
+            line["autotune_config1"] = {"error": f"{type(e).__name__}: {e}"}
         try:
             line["config5a_full"] = config5a_full(sb, device)
         except Exception as e:
