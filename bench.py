@@ -939,7 +939,31 @@ def main():
                     help="dram bytes per launch of the dominant kernel from an ncu capture")
     ap.add_argument("--storm-t-case", default=None, choices=STORM_T_CASES,
                     help="run only this STORM_t corpus of the forms (one JSON line) and exit")
+    ap.add_argument("--mixed-density-only", action="store_true",
+                    help="run only the kernel layer's mixed-density forms (one JSON line) and exit")
+    ap.add_argument("--mixed-density-batched", action="store_true",
+                    help="only the batched cost-model form of that corpus, no selector training (for profiling)")
     args = ap.parse_args()
+    if args.mixed_density_batched:
+        import torch
+        sb = importlib.import_module("stormbitmaps-internal_b200")
+        # generated on the host so that a profiler sees only this library's launches
+        sets = zipf_sets_gpu(4096, 1 << 20, 1.1, 16, 1 << 18, 0xC0F3, torch.device("cpu"))
+        r = sb.StormRows(1 << 20)
+        for v in sets:
+            r.add(v)
+        r.upload()
+        res = []
+        for _ in range(3):
+            s_, st = r.allpairs_sum(sb.POLICY_PERTILE, 64, exec_=sb.EXEC_BATCHED)
+            res.append(st["ns_total"] * 1e-6)
+        print(json.dumps({"mixed_density_batched_cost_model_ms": res, "sum": s_}), flush=True)
+        return 0
+    if args.mixed_density_only:
+        import torch
+        sb = importlib.import_module("stormbitmaps-internal_b200")
+        print(json.dumps({"mixed_density": mixed_density_forms(sb, torch.device("cuda", 0))}), flush=True)
+        return 0
     if args.storm_t_case:
         import torch
         print(json.dumps({"storm_t": storm_t_forms(torch.device("cuda", 0), only=args.storm_t_case)}), flush=True)
