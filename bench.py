@@ -827,7 +827,7 @@ def run_b200_arm(args):
     # ---- thresholded form (pairs with Jaccard >= t): filter fused into the
     # tensor-core epilogue, no triangle written
     thresh = None
-    if args.forms and rank == 0:
+    if args.forms and rank == 0 and world == 1:   # single-GPU characterisation forms
         t_j = 0.3
         tms, hits = [], 0
         for _ in range(3):
@@ -878,7 +878,7 @@ def run_b200_arm(args):
         "e2e": {"value": e2e_value, "unit": "pairs/s", "ms_per_step": e2e_step_ms,
                 "h2d_bytes_per_step": int(n * w * 8), "d2h_bytes_per_step": int(tri * 4)},
     }
-    if rank == 0 and args.cpu_baseline:
+    if rank == 0 and world == 1 and args.cpu_baseline:   # the CPU baseline is an N=1 figure
         r = reference_sample(host_in.numpy().view(np.uint64), args.cpu_seconds, cpu_threads())
         if r is not None:
             rate, pairs, dt, nrows = r
@@ -890,7 +890,7 @@ def run_b200_arm(args):
                                     "sample": "oracle/_ref not built"}
     if thresh is not None:
         line["threshold_form"] = thresh
-    if rank == 0 and args.forms:
+    if rank == 0 and world == 1 and args.forms:
         try:
             line["mixed_density"] = mixed_density_forms(sb, device)
         except Exception as e:   # reported, never silently dropped
