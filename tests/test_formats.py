@@ -159,3 +159,50 @@ def test_loaded_stormpack_all_pairs_match_oracle(sb, tmp_path):
     r = sb.StormRows.from_stormpack(p)
     mat, st = r.allpairs_matrix(sb.POLICY_PERTILE, 64)
     np.testing.assert_array_equal(mat, want)
+
+
+def _fixture_sets():
+    import importlib.util
+    import os
+    path = os.path.join(os.path.dirname(__file__), "golden", "make_corpus_fixtures.py")
+    spec = importlib.util.spec_from_file_location("make_corpus_fixtures", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.corpus_sets()
+
+
+def _fixture(name):
+    import os
+    return os.path.join(os.path.dirname(__file__), "golden", name)
+
+
+def test_reference_written_fixtures_load(sb):
+    """Files written by the reference's own tools (tools/sets2bin.py and
+    tools/pack.cpp, tests/golden/make_corpus_fixtures.py) load with their row
+    counts and universe."""
+    rows = _fixture_sets()
+    s = sb.Storm()
+    assert s.load_stormbin(_fixture("corpus.stormbin")) == (len(rows), 5008)
+    s = sb.Storm()
+    assert s.load_stormpack(_fixture("corpus.stormpack")) == (len(rows), 5008)
+    r = sb.StormRows.from_stormpack(_fixture("corpus.stormpack"))
+    assert (len(r), r.universe) == (len(rows), 5008)
+
+
+@pytest.mark.gpu
+def test_reference_written_fixtures_match_oracle(sb):
+    """All-pairs counts of the reference-written STORMBIN and STORMPACK files
+    equal the oracle's on the sets they were written from."""
+    rows = _fixture_sets()
+    vals, offs = gen.to_csr(rows)
+    want, ws = ol.sets_matrix(vals, offs)
+    for loader in ("stormbin", "stormpack"):
+        s = sb.Storm()
+        getattr(s, "load_" + loader)(_fixture("corpus." + loader))
+        mat, ssum = s.matrix()
+        assert ssum == ws, loader
+        np.testing.assert_array_equal(mat, want, err_msg=loader)
+        r = (sb.StormRows.from_stormbin if loader == "stormbin" else sb.StormRows.from_stormpack)(
+            _fixture("corpus." + loader))
+        mat, st = r.allpairs_matrix(sb.POLICY_PERTILE, 64)
+        np.testing.assert_array_equal(mat, want, err_msg=loader)
