@@ -5,12 +5,18 @@ writes rather than to a restatement of its layout:
   * STORMBIN: tools/sets2bin.py (adjacency input: one set per line),
   * STORMPACK: tools/pack.cpp compiled from the reference sources, run on
     that STORMBIN file (stride 1, card_max_array 32: every stored
-    representation appears -- bitmap, u16 array, u16 runs, full, empty).
+    representation appears -- bitmap, u16 array, u16 runs, full, empty);
+  * tests/golden/threshold_hits.json: the reference's thresholded mode,
+    bench/bench_threshold.cpp compiled with kernels/*.cpp, run on the
+    STORMBIN file at several Jaccard thresholds; its CSV line's hit count
+    (pairs i < j with |Xi & Xj| > 0 and Jaccard >= t) per threshold.
 
 The sets are regenerated from the same seed by corpus_sets() in the tests.
 Run in a container that has the reference tree (REF below); the outputs are
 committed. Test infrastructure only.
 """
+import glob
+import json
 import os
 import subprocess
 import sys
@@ -21,6 +27,7 @@ import numpy as np
 REF = os.environ.get("STORM_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
 UNIVERSE = 5008
+THRESHOLDS = (0.0, 0.001, 0.01, 0.05, 0.1, 0.3, 0.6)
 
 
 def corpus_sets():
@@ -60,6 +67,19 @@ def main():
         subprocess.run(["g++", "-O2", "-std=c++17", "-I", REF, os.path.join(REF, "tools", "pack.cpp"),
                         os.path.join(REF, "kernels", "storm_repr.cpp"), "-o", exe], check=True)
         subprocess.run([exe, binf, os.path.join(HERE, "corpus.stormpack"), "1", "32"], check=True)
+        thr = os.path.join(tmp, "bench_threshold")
+        srcs = sorted(glob.glob(os.path.join(REF, "kernels", "*.cpp")))
+        subprocess.run(["g++", "-O2", "-std=c++17", "-march=native", "-I", REF,
+                        os.path.join(REF, "bench", "bench_threshold.cpp")] + srcs + ["-o", thr], check=True)
+        hits = {}
+        for t in THRESHOLDS:
+            out = subprocess.run([thr, "--file", binf, "--rows", "1000", "--t", repr(t), "--repeats", "1", "--csv"],
+                                 check=True, capture_output=True, text=True).stdout.strip().splitlines()[-1]
+            fields = out.split(",")    # corpus,t,N,pairs,hits,candidates,...,correct
+            assert fields[-1] == "1", out
+            hits[repr(t)] = int(fields[4])
+        with open(os.path.join(HERE, "threshold_hits.json"), "w") as f:
+            json.dump(hits, f, indent=1)
 
 
 if __name__ == "__main__":

@@ -206,3 +206,42 @@ def test_reference_written_fixtures_match_oracle(sb):
             _fixture("corpus." + loader))
         mat, st = r.allpairs_matrix(sb.POLICY_PERTILE, 64)
         np.testing.assert_array_equal(mat, want, err_msg=loader)
+
+
+def _threshold_golden():
+    import json
+    with open(_fixture("threshold_hits.json")) as f:
+        return {float(k): v for k, v in json.load(f).items()}
+
+
+def test_oracle_threshold_pinned_to_reference():
+    """The oracle's thresholded set on the fixture corpus has exactly the hit
+    counts the reference's bench/bench_threshold.cpp reports for it."""
+    rows = _fixture_sets()
+    vals, offs = gen.to_csr(rows)
+    tri, _ = ol.sets_matrix(vals, offs)
+    for t, hits in _threshold_golden().items():
+        assert len(ol.threshold_pairs(tri, len(rows), t)[0]) == hits, t
+
+
+@pytest.mark.gpu
+def test_threshold_forms_match_reference_counts(sb):
+    """STORM_t (loaded from the reference-written STORMBIN file) and
+    STORM_contiguous_t thresholded forms: the reference's hit counts, and the
+    oracle's pairs and counts."""
+    rows = _fixture_sets()
+    vals, offs = gen.to_csr(rows)
+    tri, _ = ol.sets_matrix(vals, offs)
+    s = sb.Storm()
+    s.load_stormbin(_fixture("corpus.stormbin"))
+    words = gen.sets_to_rows(rows, 5008)
+    c = sb.StormContig(5008)
+    c.add_bitmaps(words)
+    for t, hits in _threshold_golden().items():
+        wi, wj, wc = ol.threshold_pairs(tri, len(rows), t)
+        for h in (s, c):
+            gi, gj, gc, found = h.threshold(t, cap=4096)
+            assert found == hits, (type(h).__name__, t)
+            np.testing.assert_array_equal(gi, wi)
+            np.testing.assert_array_equal(gj, wj)
+            np.testing.assert_array_equal(gc, wc)
