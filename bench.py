@@ -447,7 +447,8 @@ def config5a_full(sb, device, steps=3):
     res = {"workload": "200000 sites x 20000 haplotypes, P(k) ~ 1/k, 32-haplotype carrier blocks; "
                        "80 GB u32 triangle in HBM", "pairs_i_le_j": tri, "ms": round(k, 2),
            "pairs_per_s": tri / (k * 1e-3), "checksum_sum_i_lt_j": sums.pop() if len(sums) == 1 else None,
-           "kernel": {sb.KERNEL_POPC: "bb_popc_kernel", sb.KERNEL_MMA: "bb_mma_ts_kernel"}.get(c.last_kernel(), "?"),
+           "kernel": {sb.KERNEL_POPC: "bb_popc_kernel", sb.KERNEL_MMA: "bb_mma_ts_kernel",
+                      sb.KERNEL_MMA_DB: "bb_mma_ts2_kernel"}.get(c.last_kernel(), "?"),
            "roofline": {"achieved_tops_int8": tops, "peak": 2.0 * peaks["bf16_tflops"],
                         "frac": tops / (2.0 * peaks["bf16_tflops"])}}
     del out
@@ -467,11 +468,13 @@ def autotune_config1(sb, device):
     if rc < 0:
         raise sb.StormError(rc, "STORM_contig_add_bitmaps")
     k, sched, times = c.autotune()
-    names = ("tcgen05_ts_tiles", "tcgen05_ts_stream_k", "tcgen05_ss", "popc")
+    names = ("tcgen05_ts_tiles", "tcgen05_ts_stream_k", "tcgen05_db_tiles", "tcgen05_db_stream_k", "tcgen05_ss",
+             "popc")
     c.close()
     return {"workload": "4096 rows x 65536 bits, Bernoulli(0.5)",
             "candidates_ms": {nm: round(t, 4) for nm, t in zip(names, times)},
             "kept": names[[(sb.KERNEL_MMA, sb.SCHED_TILES), (sb.KERNEL_MMA, sb.SCHED_STREAM_K),
+                           (sb.KERNEL_MMA_DB, sb.SCHED_TILES), (sb.KERNEL_MMA_DB, sb.SCHED_STREAM_K),
                            (sb.KERNEL_MMA_SS, sb.SCHED_AUTO), (sb.KERNEL_POPC, sb.SCHED_AUTO)].index((k, sched))]}
 
 
@@ -735,7 +738,7 @@ def run_b200_arm(args):
     w = rows_d.shape[1]
     c = sb.StormContig(m)
     c.set_kernel({"auto": sb.KERNEL_AUTO, "popc": sb.KERNEL_POPC, "mma": sb.KERNEL_MMA,
-                  "mma_ss": sb.KERNEL_MMA_SS}[args.kernel])
+                  "mma_ss": sb.KERNEL_MMA_SS, "mma_db": sb.KERNEL_MMA_DB}[args.kernel])
     c.set_schedule({"auto": sb.SCHED_AUTO, "tiles": sb.SCHED_TILES, "stream_k": sb.SCHED_STREAM_K}[args.schedule])
     rc = sb.lib().STORM_contig_add_bitmaps(c.h, C.cast(rows_d.data_ptr(), sb.u64p), n, w)
     if rc < 0:
@@ -782,7 +785,7 @@ def run_b200_arm(args):
     elapsed_ms = max_over_ranks(elapsed_ms, dist, device)
     launches = args.steps * c.last_launches()
     kernel_used = {sb.KERNEL_POPC: "bb_popc_kernel", sb.KERNEL_MMA: "bb_mma_ts_kernel",
-                   sb.KERNEL_MMA_SS: "bb_mma_kernel"}.get(c.last_kernel(), "?")
+                   sb.KERNEL_MMA_SS: "bb_mma_kernel", sb.KERNEL_MMA_DB: "bb_mma_ts2_kernel"}.get(c.last_kernel(), "?")
     ms_per_step = elapsed_ms / args.steps
     value = world * tri / (ms_per_step / 1e3)
 
@@ -840,7 +843,7 @@ def run_b200_arm(args):
     # ---- roofline of the dominant kernel ----
     peaks, peak_src = measured_peaks()
     k_ms = statistics.median(kernel_ms)
-    if kernel_used in ("bb_mma_kernel", "bb_mma_ts_kernel"):
+    if kernel_used in ("bb_mma_kernel", "bb_mma_ts_kernel", "bb_mma_ts2_kernel"):
         ops = 2.0 * tri * m                      # u8 MACs = pairs x row bits, 2 ops each
         achieved = ops / (k_ms / 1e3) / 1e12
         peak = 2.0 * peaks["bf16_tflops"]        # dense int8 rate = 2 x dense bf16 on sm_100
@@ -862,7 +865,7 @@ def run_b200_arm(args):
         "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "ns_per_pair": 1e9 / (value / world),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8 (tcgen05 kind::i8, s32 acc)"
-        if kernel_used in ("bb_mma_kernel", "bb_mma_ts_kernel") else "u64 (AND + POPC)",
+        if kernel_used in ("bb_mma_kernel", "bb_mma_ts_kernel", "bb_mma_ts2_kernel") else "u64 (AND + POPC)",
         "data": "synthetic (seeded Bernoulli rows generated on the GPU)",
         "config": {"workload": f"dense all-bitmap XX^T: {n} rows x {m} bits, p~U[0.05,0.5], u32 i<=j out",
                    "rows": n, "bits": m, "pairs_per_gpu": tri, "kernel": kernel_used, "schedule": args.schedule,
@@ -925,7 +928,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma", "mma_ss"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma", "mma_ss", "mma_db"])
     ap.add_argument("--schedule", default="auto", choices=["auto", "tiles", "stream_k"],
                     help="tensor-core work schedule (whole tiles or stream-K; auto picks per launch)")
     ap.add_argument("--rows", type=int, default=N_ROWS)

@@ -71,6 +71,9 @@ typedef void (*STORM_tile_callback)(uint32_t i0, uint32_t j0, uint32_t nr, uint3
 #define STORM_B200_KERNEL_POPC  1   /* CUDA-core AND + POPC tiles                  */
 #define STORM_B200_KERNEL_MMA   2   /* tcgen05 kind::i8, A operand in TMEM         */
 #define STORM_B200_KERNEL_MMA_SS 3  /* tcgen05 kind::i8, both operands in smem     */
+#define STORM_B200_KERNEL_MMA_DB 4  /* tcgen05 kind::i8, A in TMEM, 128 x 192 tiles
+                                       with two accumulators drained by their own
+                                       warps while the next tile computes        */
 
 /* Append n_rows rows given as packed little-endian bitmaps of
  * words_per_row 64-bit words each, in host memory or (unified addressing)
@@ -98,11 +101,12 @@ int STORM_contig_set_kernel(STORM_contiguous_t* c, int kernel);
 int STORM_contig_set_schedule(STORM_contiguous_t* c, int schedule);
 /* Autotuner (no counterpart in the reference): times this container's own
  * all-pairs call on the GPU with each bitmap x bitmap kernel that is exact
- * for its row length -- tcgen05 with A in tensor memory under whole-tile and
- * stream-K schedules, tcgen05 with both operands in shared memory, CUDA-core
- * POPC -- best of two calls each, and keeps the fastest kernel and schedule
- * for later calls.  times_ms (4 entries in that order, -1 when skipped) and
- * the choice are reported when non-NULL.  Counts do not depend on it. */
+ * for its row length -- tcgen05 with A in tensor memory (128 x 256 tiles,
+ * then 128 x 192 double-buffered tiles), each under whole-tile and stream-K
+ * schedules; tcgen05 with both operands in shared memory; CUDA-core POPC --
+ * best of two calls each, and keeps the fastest kernel and schedule for
+ * later calls.  times_ms (6 entries in that order, -1 when skipped) and the
+ * choice are reported when non-NULL.  Counts do not depend on it. */
 int STORM_contig_autotune(STORM_contiguous_t* c, int* best_kernel, int* best_schedule, double* times_ms);
 /* Pack the rows into HBM now (otherwise done by the first all-pairs call). */
 int STORM_contig_upload(STORM_contiguous_t* c);

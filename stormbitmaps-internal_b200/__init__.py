@@ -36,7 +36,7 @@ u32p = C.POINTER(C.c_uint32)
 u64p = C.POINTER(C.c_uint64)
 TILE_CB = C.CFUNCTYPE(None, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, u32p, C.c_void_p)
 
-KERNEL_AUTO, KERNEL_POPC, KERNEL_MMA, KERNEL_MMA_SS = 0, 1, 2, 3
+KERNEL_AUTO, KERNEL_POPC, KERNEL_MMA, KERNEL_MMA_SS, KERNEL_MMA_DB = 0, 1, 2, 3, 4
 SCHED_AUTO, SCHED_TILES, SCHED_STREAM_K = 0, 1, 2
 OK, ENULL, EVALUES, EARG, ENOMEM, ECUDA, ETIMEOUT, ESIZE, ELIMIT = 0, -1, -2, -3, -4, -5, -6, -7, -8
 
@@ -280,8 +280,8 @@ class StormContig:
 
     def autotune(self):
         """Time every exact kernel/schedule on these rows and keep the fastest:
-        (kernel, schedule, times_ms[4])."""
-        k, sc, t = C.c_int(0), C.c_int(0), (C.c_double * 4)()
+        (kernel, schedule, times_ms[6])."""
+        k, sc, t = C.c_int(0), C.c_int(0), (C.c_double * 6)()
         _check(_lib.STORM_contig_autotune(self.h, C.byref(k), C.byref(sc), t), "STORM_contig_autotune")
         return k.value, sc.value, list(t)
 

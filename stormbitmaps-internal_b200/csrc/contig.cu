@@ -223,7 +223,7 @@ int STORM_contig_clear(STORM_contiguous_t* bitmap) {
 
 int STORM_contig_set_kernel(STORM_contiguous_t* c, int kernel) {
     if (c == NULL) return STORM_B200_ENULL;
-    if (kernel < STORM_B200_KERNEL_AUTO || kernel > STORM_B200_KERNEL_MMA_SS) return STORM_B200_EARG;
+    if (kernel < STORM_B200_KERNEL_AUTO || kernel > STORM_B200_KERNEL_MMA_DB) return STORM_B200_EARG;
     c->kernel_pref = kernel;
     return 0;
 }
@@ -242,17 +242,19 @@ int STORM_contig_autotune(STORM_contiguous_t* c, int* best_kernel, int* best_sch
         contig_flush(c);
         c->d_out.reserve(tri_size(n) ? tri_size(n) : 1);
         const uint64_t bits = c->vector_length;
-        // tcgen05 (A in TMEM) under both schedules, tcgen05 with both operands
-        // in shared memory, CUDA-core POPC -- each where it is exact.
-        const int kern[4] = {STORM_B200_KERNEL_MMA, STORM_B200_KERNEL_MMA, STORM_B200_KERNEL_MMA_SS,
-                             STORM_B200_KERNEL_POPC};
-        const int sched[4] = {STORM_B200_SCHED_TILES, STORM_B200_SCHED_STREAM_K, STORM_B200_SCHED_AUTO,
-                              STORM_B200_SCHED_AUTO};
-        const bool ok[4] = {bits <= TC_MAX_ROW_BITS, bits <= TC_MAX_ROW_BITS, bits <= TC_SS_MAX_ROW_BITS, true};
+        // tcgen05 (A in TMEM) with 128 x 256 tiles and with 128 x 192 double-
+        // buffered tiles, each under both schedules; tcgen05 with both
+        // operands in shared memory; CUDA-core POPC -- each where it is exact.
+        const int kern[6] = {STORM_B200_KERNEL_MMA,    STORM_B200_KERNEL_MMA,    STORM_B200_KERNEL_MMA_DB,
+                             STORM_B200_KERNEL_MMA_DB, STORM_B200_KERNEL_MMA_SS, STORM_B200_KERNEL_POPC};
+        const int sched[6] = {STORM_B200_SCHED_TILES, STORM_B200_SCHED_STREAM_K, STORM_B200_SCHED_TILES,
+                              STORM_B200_SCHED_STREAM_K, STORM_B200_SCHED_AUTO, STORM_B200_SCHED_AUTO};
+        const bool ok[6] = {bits <= TC_MAX_ROW_BITS, bits <= TC_MAX_ROW_BITS, bits <= TC_MAX_ROW_BITS,
+                            bits <= TC_MAX_ROW_BITS, bits <= TC_SS_MAX_ROW_BITS, true};
         const int keep_sched = c->engine.schedule;
         double best = -1.0;
         int bk = c->kernel_pref, bs = keep_sched;
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < 6; ++k) {
             if (times_ms) times_ms[k] = -1.0;
             if (!ok[k] || n == 0) continue;
             c->engine.schedule = sched[k];

@@ -3,6 +3,7 @@
 #include "bb_popc.cuh"
 #include "bb_mma.cuh"
 #include "bb_mma_ts.cuh"
+#include "bb_mma_ts2.cuh"
 
 #include <algorithm>
 #include <mutex>
@@ -34,6 +35,8 @@ static uint32_t ts_schedule(uint32_t n_tiles, int sms, uint32_t w_pad, uint32_t&
     return 0;
 }
 
+constexpr uint64_t DB_AUTO_MAX_BITS = 1ull << 17;
+
 static void build_tiles(std::vector<uint2>& t, uint64_t n, int kind) {
     t.clear();
     if (kind == STORM_B200_KERNEL_MMA || kind == STORM_B200_KERNEL_MMA_SS) {
@@ -42,6 +45,11 @@ static void build_tiles(std::vector<uint2>& t, uint64_t n, int kind) {
         // i.e. bj >= floor(bi / 2).
         for (uint64_t bi = 0; bi < nbi; ++bi)
             for (uint64_t bj = bi / 2; bj < nbj; ++bj) t.push_back(make_uint2((uint32_t)bi, (uint32_t)bj));
+    } else if (kind == STORM_B200_KERNEL_MMA_DB) {
+        const uint64_t nbi = (n + T2_BM - 1) / T2_BM, nbj = (n + T2_BN - 1) / T2_BN;
+        // 128 bi <= 192 bj + 191  <=>  bj >= floor(128 bi / 192)
+        for (uint64_t bi = 0; bi < nbi; ++bi)
+            for (uint64_t bj = (128 * bi) / 192; bj < nbj; ++bj) t.push_back(make_uint2((uint32_t)bi, (uint32_t)bj));
     } else {
         const uint64_t nb = (n + POPC_BM - 1) / POPC_BM;
         for (uint64_t bi = 0; bi < nb; ++bi)
@@ -52,9 +60,16 @@ static void build_tiles(std::vector<uint2>& t, uint64_t n, int kind) {
 int DenseEngine::prepare(uint64_t n, uint64_t row_bits, int kernel_pref, cudaStream_t st) {
     if (n > 0xFFFFFFFFull) fail(STORM_B200_ELIMIT, "more than 2^32 rows");
     int kind = kernel_pref;
+    // Automatic choice: rows of at most 2^17 bits (tiles of at most 512 K
+    // stages) take the double-buffered tensor-core kernel, whose drain of one
+    // tile overlaps the next tile's MMAs (measured on B200: 19 % faster at
+    // 20000-bit rows, 3 % at 65536, even at 2^18); longer rows up to 2^27
+    // bits the 128 x 256 kernel; past that the CUDA-core POPC kernel.
     if (kind == STORM_B200_KERNEL_AUTO)
-        kind = row_bits <= MMA_MAX_BITS_W4 ? STORM_B200_KERNEL_MMA : STORM_B200_KERNEL_POPC;
-    if (kind == STORM_B200_KERNEL_MMA && row_bits > MMA_MAX_BITS_W4)
+        kind = row_bits <= DB_AUTO_MAX_BITS    ? STORM_B200_KERNEL_MMA_DB
+               : row_bits <= MMA_MAX_BITS_W4 ? STORM_B200_KERNEL_MMA
+                                             : STORM_B200_KERNEL_POPC;
+    if ((kind == STORM_B200_KERNEL_MMA || kind == STORM_B200_KERNEL_MMA_DB) && row_bits > MMA_MAX_BITS_W4)
         fail(STORM_B200_ELIMIT, "tensor-core kernel is exact only for rows of at most 2^27 bits");
     if (kind == STORM_B200_KERNEL_MMA_SS && row_bits > MMA_MAX_BITS)
         fail(STORM_B200_ELIMIT, "shared-memory tensor-core kernel is exact only for rows of at most 2^23 bits");
@@ -94,6 +109,19 @@ void DenseEngine::launch(int kind, const uint64_t* dX, uint32_t n, uint32_t w_pa
         else
             bb_mma_ts_long_kernel<<<grid, TS_THREADS, smem, st>>>(dX, n, w_pad, d_tiles.p + t0, count, d_out,
                                                                   d_flags.p, ks);
+    } else if (kind == STORM_B200_KERNEL_MMA_DB) {
+        static std::atomic<uint64_t> done_a{0}, done_b{0};
+        smem_attr_once(bb_mma_ts2_kernel, (int)T2_SMEM_BYTES, done_a);
+        smem_attr_once(bb_mma_ts2_long_kernel, (int)T2_SMEM_BYTES, done_b);
+        uint32_t grid = count < (uint32_t)sms ? count : (uint32_t)sms;
+        const uint32_t ks = (t0 == 0 && count == n_tiles) ? ts_schedule(count, sms, w_pad, grid, schedule) : 1;
+        if (ks != 1 && d_out) SB_CUDA(cudaMemsetAsync(d_out, 0, tri_size(n) * sizeof(uint32_t), st));
+        if ((uint64_t)w_pad * 64 <= MMA_MAX_BITS)
+            bb_mma_ts2_kernel<<<grid, T2_THREADS, T2_SMEM_BYTES, st>>>(dX, n, w_pad, d_tiles.p + t0, count, d_out,
+                                                                      d_flags.p, ks);
+        else
+            bb_mma_ts2_long_kernel<<<grid, T2_THREADS, T2_SMEM_BYTES, st>>>(dX, n, w_pad, d_tiles.p + t0, count,
+                                                                           d_out, d_flags.p, ks);
     } else if (kind == STORM_B200_KERNEL_MMA_SS) {
         static std::atomic<uint64_t> done{0};
         smem_attr_once(bb_mma_kernel, (int)MMA_SMEM_BYTES, done);
@@ -393,6 +421,12 @@ uint64_t DenseEngine::run_threshold(const uint64_t* dX, uint64_t n, uint32_t w_p
         if (sum) *sum = 0;
         return 0;
     }
+    // The thresholded form has its filter fused into the 128 x 256 tensor-core
+    // kernel's drain; the double-buffered kernel has none, so rows it would
+    // take go to the fused one.
+    if ((kernel_pref == STORM_B200_KERNEL_AUTO || kernel_pref == STORM_B200_KERNEL_MMA_DB) &&
+        row_bits <= MMA_MAX_BITS_W4)
+        kernel_pref = STORM_B200_KERNEL_MMA;
     const int kind = prepare(n, row_bits, kernel_pref, st);
     SB_CUDA(cudaEventRecord(log.ev0, st));
     uint64_t found = 0;

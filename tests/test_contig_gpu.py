@@ -10,11 +10,11 @@ import oracle_lib as ol
 
 pytestmark = pytest.mark.gpu
 
-KERNELS = ("popc", "mma", "mma_ss")
+KERNELS = ("popc", "mma", "mma_ss", "mma_db")
 
 
 def _kernel(sb, name):
-    return {"popc": sb.KERNEL_POPC, "mma": sb.KERNEL_MMA, "mma_ss": sb.KERNEL_MMA_SS}[name]
+    return {"popc": sb.KERNEL_POPC, "mma": sb.KERNEL_MMA, "mma_ss": sb.KERNEL_MMA_SS, "mma_db": sb.KERNEL_MMA_DB}[name]
 
 
 def contig_from_words(sb, words, m, kernel):
@@ -53,12 +53,13 @@ def test_edge_shapes_match_oracle(sb, kernel, n, m, p):
     np.testing.assert_array_equal(mat, want)
 
 
-def test_long_rows_tensor_kernel(sb):
+@pytest.mark.parametrize("kernel", ("mma", "mma_db"))
+def test_long_rows_tensor_kernel(sb, kernel):
     """Rows past 2^23 bits take the 4-byte weight cycle (D = 8 x count):
     random rows, and all-ones rows of 2^26 bits (count 2^26, D = 2^29)."""
     m = (1 << 23) + 4096
     words = gen.bernoulli_rows(40, m, 0.3, 4242)
-    c = contig_from_words(sb, words, m, "mma")
+    c = contig_from_words(sb, words, m, kernel)
     mat, s = c.matrix()
     want, ws = ol.contig_matrix(words)
     assert s == ws
@@ -66,7 +67,7 @@ def test_long_rows_tensor_kernel(sb):
     m = 1 << 26
     ones = np.full((3, m // 64), np.uint64(0xFFFFFFFFFFFFFFFF), dtype=np.uint64)
     ones[1, ::2] = 0
-    c = contig_from_words(sb, ones, m, "mma")
+    c = contig_from_words(sb, ones, m, kernel)
     mat, s = c.matrix()
     want, ws = ol.contig_matrix(ones)
     assert s == ws and mat[0] == m
@@ -210,7 +211,7 @@ def _check_full_size(sb, n, m, p, seed, kernels):
 
 def test_config1_full_size_both_kernels(sb):
     """4096 rows x 65536 bits, Bernoulli(0.5): every pair, both kernels."""
-    _check_full_size(sb, 4096, 65536, 0.5, 101, ["mma", "mma_ss", "popc"])
+    _check_full_size(sb, 4096, 65536, 0.5, 101, ["mma", "mma_db", "mma_ss", "popc"])
 
 
 def test_config5a_haplotypes_full_size(sb):
@@ -229,7 +230,7 @@ def test_config5a_haplotypes_full_size(sb):
     tri = n * (n + 1) // 2
     out = torch.empty(tri, dtype=torch.int32, device="cuda")
     s = c.matrix_device(out.data_ptr(), tri)
-    assert c.last_kernel() == sb.KERNEL_MMA
+    assert c.last_kernel() == sb.KERNEL_MMA_DB   # the automatic choice for 20000-bit rows
     g = gen.rng(5)
     for i in np.unique(np.concatenate([[0, n - 1], g.integers(0, n, size=5)])):
         base = int(sb.tri_index(n, i, i))
@@ -291,14 +292,15 @@ def test_split_k_few_tiles(sb, n, m):
     np.testing.assert_array_equal(d.cpu().numpy().view(np.uint32), want)
 
 
+@pytest.mark.parametrize("kernel", ("mma", "mma_db"))
 @pytest.mark.parametrize("n,m", [(300, (1 << 17) + 64), (700, 16384), (129, 4097), (1000, 1 << 15)])
-def test_every_schedule_is_exact(sb, n, m):
+def test_every_schedule_is_exact(sb, kernel, n, m):
     """Whole tiles round robin and stream-K (partial tiles added with atomics
     into the zeroed triangle) give the oracle's counts; the automatic choice
-    too."""
+    too -- for both tensor-core tile shapes."""
     words = gen.bernoulli_rows(n, m, (0.05, 0.6), seed=500 + n)
     want, ws = ol.contig_matrix(words)
-    c = contig_from_words(sb, words, m, "mma")
+    c = contig_from_words(sb, words, m, kernel)
     for sched in (sb.SCHED_TILES, sb.SCHED_STREAM_K, sb.SCHED_AUTO):
         c.set_schedule(sched)
         mat, s = c.matrix()
@@ -358,8 +360,8 @@ def test_autotune_keeps_the_fastest_exact_kernel(sb):
     c = contig_from_words(sb, words, m, "mma")
     k, sched, times = c.autotune()
     assert all(t > 0 for t in times)
-    cands = [(sb.KERNEL_MMA, sb.SCHED_TILES), (sb.KERNEL_MMA, sb.SCHED_STREAM_K), (sb.KERNEL_MMA_SS, sb.SCHED_AUTO),
-             (sb.KERNEL_POPC, sb.SCHED_AUTO)]
+    cands = [(sb.KERNEL_MMA, sb.SCHED_TILES), (sb.KERNEL_MMA, sb.SCHED_STREAM_K), (sb.KERNEL_MMA_DB, sb.SCHED_TILES),
+             (sb.KERNEL_MMA_DB, sb.SCHED_STREAM_K), (sb.KERNEL_MMA_SS, sb.SCHED_AUTO), (sb.KERNEL_POPC, sb.SCHED_AUTO)]
     assert (k, sched) == cands[int(np.argmin(times))]
     mat, s = c.matrix()
     assert s == ws and c.last_kernel() == k
@@ -371,5 +373,5 @@ def test_autotune_keeps_the_fastest_exact_kernel(sb):
     words[:, -1] &= np.uint64((1 << (m % 64)) - 1)
     c = contig_from_words(sb, words, m, "mma")
     k, sched, times = c.autotune()
-    assert times[2] == -1.0 and times[0] > 0 and times[3] > 0
+    assert times[4] == -1.0 and times[0] > 0 and times[2] > 0 and times[5] > 0
     assert c.matrix()[1] == ol.contig_matrix(words)[1]
