@@ -67,7 +67,8 @@ typedef void (*STORM_tile_callback)(uint32_t i0, uint32_t j0, uint32_t nr, uint3
 
 /* ---- STORM_contiguous_t extensions ------------------------------------ */
 /* Bitmap x bitmap kernel used by the contiguous all-pairs calls. */
-#define STORM_B200_KERNEL_AUTO  0   /* tensor-core kernel where exact, else POPC   */
+#define STORM_B200_KERNEL_AUTO  0   /* MMA_DB for rows <= 2^17 bits, MMA up to
+                                       2^27, POPC beyond                         */
 #define STORM_B200_KERNEL_POPC  1   /* CUDA-core AND + POPC tiles                  */
 #define STORM_B200_KERNEL_MMA   2   /* tcgen05 kind::i8, A operand in TMEM         */
 #define STORM_B200_KERNEL_MMA_SS 3  /* tcgen05 kind::i8, both operands in smem     */
@@ -126,7 +127,8 @@ void* STORM_contig_stream(STORM_contiguous_t* c);
  * handle's stream) and how many kernels it launched. */
 float STORM_contig_last_kernel_ms(const STORM_contiguous_t* c);
 uint32_t STORM_contig_last_launches(const STORM_contiguous_t* c);
-/* Which kernel the last call ran (STORM_B200_KERNEL_POPC, _MMA or _MMA_SS). */
+/* Which kernel the last call ran (STORM_B200_KERNEL_POPC, _MMA, _MMA_SS or
+ * _MMA_DB). */
 int STORM_contig_last_kernel(const STORM_contiguous_t* c);
 
 /* All pairs of rows that are already in device memory, into a device buffer,
