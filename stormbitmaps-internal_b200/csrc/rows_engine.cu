@@ -374,7 +374,7 @@ struct STORM_rows_s {
     Mlp mlp;
     // CUDA graph of the batched form, keyed by the call's shape
     cudaGraphExec_t graph = nullptr;
-    uint64_t graph_key[6] = {0, 0, 0, 0, 0, 0};
+    std::vector<uint64_t> graph_key;
     ~STORM_rows_s() {
         if (graph) cudaGraphExecDestroy(graph);
         for (auto& e : ev)
@@ -546,9 +546,31 @@ static void rows_run(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell,
     uint32_t launches = 0;
     SB_CUDA(cudaEventRecord(r->ev[0], st));
     if (exec == STORM_EXEC_BATCHED) {
-        const uint64_t key[6] = {(uint64_t)policy, T, (uint64_t)fixed_cell, (uint64_t)(uintptr_t)d_out, n,
-                                 learned ? 1ull : 0ull};
-        const bool reuse = r->graph && std::equal(key, key + 6, r->graph_key);
+        // Everything the captured launches bake in: the call's shape, the
+        // dense block's split, every device buffer they address (a buffer
+        // that grew since the capture has moved), and the selector's shape.
+        auto ptr = [](const void* p) { return (uint64_t)(uintptr_t)p; };
+        const std::vector<uint64_t> key = {(uint64_t)policy,
+                                           T,
+                                           (uint64_t)fixed_cell,
+                                           ptr(d_out),
+                                           n,
+                                           learned ? 1ull : 0ull,
+                                           D,
+                                           ptr(r->d_order.p),
+                                           ptr(r->d_bmeta.p),
+                                           ptr(r->d_het.p),
+                                           ptr(r->d_dec.p),
+                                           ptr(r->d_stats.p),
+                                           nd ? ptr(r->d_dense.p) : 0ull,
+                                           nd ? ptr(r->d_dmap.p) : 0ull,
+                                           nd ? ptr(r->d_dtiles.p) : 0ull,
+                                           nd ? ptr(r->d_dflags.p) : 0ull,
+                                           learned ? ptr(r->mlp.d_params.p) : 0ull,
+                                           learned ? ((uint64_t)r->mlp.shape.H << 40 | (uint64_t)r->mlp.shape.F << 20 |
+                                                      r->mlp.shape.C)
+                                                   : 0ull};
+        const bool reuse = r->graph && key == r->graph_key;
         if (!reuse) {
             if (r->graph) {
                 cudaGraphExecDestroy(r->graph);
@@ -564,7 +586,7 @@ static void rows_run(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell,
             SB_CUDA(cudaStreamEndCapture(st, &g));
             SB_CUDA(cudaGraphInstantiate(&r->graph, g, 0));
             cudaGraphDestroy(g);
-            std::copy(key, key + 6, r->graph_key);
+            r->graph_key = key;
         }
         SB_CUDA(cudaGraphLaunch(r->graph, st));
         launches = 3 + (policy == STORM_POLICY_PROBE ? 1 : 0);

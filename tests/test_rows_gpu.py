@@ -189,3 +189,42 @@ def test_autotune_tile_and_dense_block(sb):
     assert tile == 64 and all(t < 0 for k, t in enumerate(times) if k // 4 != 1)
     mat, st = r.allpairs_matrix(sb.POLICY_LEARNED, 0)
     np.testing.assert_array_equal(mat, want)
+
+
+def test_autotune_times_each_dense_block_candidate(sb):
+    """The batched form's CUDA graph is re-captured when the dense block
+    changes: on rows where the tensor block is many times faster than the
+    B x B cells, the autotuner's density-0 candidate (no block) must time
+    slower than the candidates that put every row in the block, and counts
+    stay equal to the oracle's."""
+    u, n = 1 << 18, 1024
+    words = gen.bernoulli_rows(n, u, 0.3, 913)
+    sets = gen.rows_to_sets(words, u)
+    r = rows_of(sb, sets, u)
+    _, want = ol.contig_matrix(words, want_matrix=False)
+    tile, dens, times = r.autotune(sb.POLICY_PERTILE)
+    for a in range(4):
+        t = times[4 * a: 4 * a + 4]
+        assert t[0] > 1.5 * min(t[1:]), (a, t)
+    assert dens > 0.0
+    for d in (0.0, 1 / 16384, 0.0):
+        r.set_dense_block(d)
+        s, st = r.allpairs_sum(sb.POLICY_PERTILE, 64, exec_=sb.EXEC_BATCHED)
+        assert s == want
+        if d > 0.0:   # every row is in the block: all pairs on the tensor cores
+            assert st["cell_pairs"] == {"BB": n * (n - 1) // 2}
+
+
+def test_batched_graph_after_buffers_grow(sb):
+    """A batched call, a per-tile call at a smaller tile (which grows the
+    per-call device buffers), then the first call again: the replayed graph
+    must not address the buffers freed in between."""
+    sets = gen.zipf_sets(700, 1 << 16, 1.1, 8, 1 << 12, 918)
+    r = rows_of(sb, sets, 1 << 16)
+    vals, offs = gen.to_csr(sets)
+    want, ws = ol.sets_matrix(vals, offs)
+    for tile, ex in ((64, sb.EXEC_BATCHED), (32, sb.EXEC_PER_TILE), (64, sb.EXEC_BATCHED), (16, sb.EXEC_PER_TILE),
+                     (64, sb.EXEC_BATCHED)):
+        mat, st = r.allpairs_matrix(sb.POLICY_PERTILE, tile, exec_=ex)
+        assert st["sum"] == ws
+        np.testing.assert_array_equal(mat, want)
