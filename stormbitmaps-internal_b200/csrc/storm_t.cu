@@ -42,6 +42,7 @@ struct StormDev {
     DevBuf<uint2> d_hits;
     DevBuf<unsigned long long> d_found;
     bool valid = false;
+    uint64_t shape = 0;    // row_shape() of the rows last packed
     ~StormDev() {
         if (stream) cudaStreamDestroy(stream);
     }
@@ -86,12 +87,31 @@ static cudaStream_t stream_of(StormDev* d) {
     return d->stream;
 }
 
+// The public struct can also be changed without this library's STORM_add /
+// STORM_clear (STORM_bitmap_cont_add on one of s->conts, as the layout
+// allows): a hash of each row's chunk count, last inserted value and chunk
+// array catches that too, at O(rows) host cost per call.
+static uint64_t row_shape(const STORM_t* s) {
+    uint64_t h = 0x9E3779B97F4A7C15ull ^ (uint64_t)(uintptr_t)s->conts ^ ((uint64_t)s->n_conts << 1);
+    auto mix = [&](uint64_t v) {
+        h ^= v + 0x9E3779B97F4A7C15ull + (h << 6) + (h >> 2);
+    };
+    for (uint32_t r = 0; r < s->n_conts; ++r) {
+        const STORM_bitmap_cont_t& c = s->conts[r];
+        mix((uint64_t)c.n_bitmaps << 32 | c.prev_inserted_value);
+        mix((uint64_t)(uintptr_t)c.bitmaps);
+    }
+    return h;
+}
+
 static void ensure_packed(const STORM_t* s, StormDev* d) {
-    if (d->valid) return;
+    const uint64_t shape = row_shape(s);
+    if (d->valid && d->shape == shape) return;
     ChunkPack p;
     for (uint32_t r = 0; r < s->n_conts; ++r) p.add_row(&s->conts[r]);
     d->dev.upload(p, stream_of(d));
     d->valid = true;
+    d->shape = shape;
 }
 
 // One-shot engine for calls that compare a few chunks or rows.

@@ -371,3 +371,42 @@ def test_autotune_storm_t(sb):
     mat, ssum = s.matrix()
     assert ssum == ws
     np.testing.assert_array_equal(mat, want)
+
+
+def test_row_changed_through_public_struct_is_repacked(sb):
+    """The STORM_t layout is public, so a caller may append to one of its rows
+    with STORM_bitmap_cont_add on s->conts[r] instead of STORM_add; the next
+    all-pairs call must see the new values (the device copy is re-packed)."""
+    import ctypes as C
+
+    class Cont(C.Structure):
+        _fields_ = [("bitmaps", C.c_void_p), ("block_ids", C.c_void_p), ("n_bitmaps", C.c_uint32),
+                    ("m_bitmaps", C.c_uint32), ("prev", C.c_uint32)]
+
+    class StormT(C.Structure):
+        _fields_ = [("conts", C.POINTER(Cont)), ("n_conts", C.c_uint32), ("m_conts", C.c_uint32)]
+
+    g = gen.rng(931)
+    u = 1 << 20
+    sets = [gen.uniform_set(g, int(g.integers(50, 5000)), u // 2) for _ in range(40)]
+    s = build_storm(sb, sets)
+    vals, offs = gen.to_csr(sets)
+    assert s.pairw_intersect_cardinality() == ol.sets_matrix(vals, offs)[1]
+    # rows 3 and 17 get values past their maximum, in chunks they already have and in new ones
+    L = sb.lib()
+    st = C.cast(s.h, C.POINTER(StormT)).contents
+    for r in (3, 17):
+        extra = np.unique(np.concatenate([g.integers(int(sets[r][-1]) + 1, int(sets[r][-1]) + 3000, 200),
+                                          g.integers(u // 2, u, 500)])).astype(np.uint32)
+        cont = C.addressof(st.conts[r])
+        assert L.STORM_bitmap_cont_add(C.c_void_p(cont), extra.ctypes.data_as(sb.u32p), extra.size) >= 0
+        sets[r] = np.concatenate([sets[r], extra])
+    vals, offs = gen.to_csr(sets)
+    want_mat, want_sum = ol.sets_matrix(vals, offs)
+    assert s.pairw_intersect_cardinality() == want_sum
+    mat, ssum = s.matrix()
+    assert ssum == want_sum
+    n = len(sets)
+    iu = np.triu_indices(n)
+    strict = iu[0] != iu[1]
+    np.testing.assert_array_equal(mat[strict], want_mat[strict])
