@@ -376,7 +376,12 @@ def test_autotune_storm_t(sb):
 def test_row_changed_through_public_struct_is_repacked(sb):
     """The STORM_t layout is public, so a caller may append to one of its rows
     with STORM_bitmap_cont_add on s->conts[r] instead of STORM_add; the next
-    all-pairs call must see the new values (the device copy is re-packed)."""
+    all-pairs call must see the new values (the device copy is re-packed).
+
+    Values appended into a chunk the row already holds become a second chunk
+    with the same id (storm.cpp:737-803), which the reference's chunk-id merge
+    matches once: that case is checked against the reference library itself
+    when it is built, the new-chunk case against the set oracle."""
     import ctypes as C
 
     class Cont(C.Structure):
@@ -386,20 +391,23 @@ def test_row_changed_through_public_struct_is_repacked(sb):
     class StormT(C.Structure):
         _fields_ = [("conts", C.POINTER(Cont)), ("n_conts", C.c_uint32), ("m_conts", C.c_uint32)]
 
+    def append(lib, h, r, extra):
+        st = C.cast(h, C.POINTER(StormT)).contents
+        cont = C.addressof(st.conts[r])
+        return lib.STORM_bitmap_cont_add(C.c_void_p(cont), extra.ctypes.data_as(sb.u32p), C.c_uint32(extra.size))
+
     g = gen.rng(931)
     u = 1 << 20
     sets = [gen.uniform_set(g, int(g.integers(50, 5000)), u // 2) for _ in range(40)]
     s = build_storm(sb, sets)
     vals, offs = gen.to_csr(sets)
     assert s.pairw_intersect_cardinality() == ol.sets_matrix(vals, offs)[1]
-    # rows 3 and 17 get values past their maximum, in chunks they already have and in new ones
+    # new chunks only (every row lies below u / 2): the set oracle applies;
+    # rows 3 and 17 share the appended values, so their count must move
     L = sb.lib()
-    st = C.cast(s.h, C.POINTER(StormT)).contents
+    extra = np.unique(g.integers(u // 2, u, 500)).astype(np.uint32)
     for r in (3, 17):
-        extra = np.unique(np.concatenate([g.integers(int(sets[r][-1]) + 1, int(sets[r][-1]) + 3000, 200),
-                                          g.integers(u // 2, u, 500)])).astype(np.uint32)
-        cont = C.addressof(st.conts[r])
-        assert L.STORM_bitmap_cont_add(C.c_void_p(cont), extra.ctypes.data_as(sb.u32p), extra.size) >= 0
+        assert append(L, s.h, r, extra) == 1
         sets[r] = np.concatenate([sets[r], extra])
     vals, offs = gen.to_csr(sets)
     want_mat, want_sum = ol.sets_matrix(vals, offs)
@@ -410,3 +418,24 @@ def test_row_changed_through_public_struct_is_repacked(sb):
     iu = np.triu_indices(n)
     strict = iu[0] != iu[1]
     np.testing.assert_array_equal(mat[strict], want_mat[strict])
+    # into the row's last chunk: against the reference's own containers
+    if ol.reference() is None:
+        return
+    R = ol.reference()
+    R.STORM_new.restype = C.c_void_p
+    R.STORM_add.argtypes = [C.c_void_p, sb.u32p, C.c_uint32]
+    R.STORM_pairw_intersect_cardinality.restype = C.c_uint64
+    R.STORM_pairw_intersect_cardinality.argtypes = [C.c_void_p]
+    R.STORM_free.argtypes = [C.c_void_p]
+    hr = R.STORM_new()
+    try:
+        for v in sets:
+            v = np.ascontiguousarray(v, dtype=np.uint32)
+            R.STORM_add(hr, v.ctypes.data_as(sb.u32p), v.size)
+        for r in (5, 29):
+            top = int(sets[r][-1])
+            extra = np.unique(g.integers(top + 1, top + 3000, 200)).astype(np.uint32)
+            assert append(L, s.h, r, extra) == 1 and append(R, hr, r, extra) == 1
+        assert s.pairw_intersect_cardinality() == R.STORM_pairw_intersect_cardinality(hr)
+    finally:
+        R.STORM_free(hr)
