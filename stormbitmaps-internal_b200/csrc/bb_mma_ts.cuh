@@ -94,21 +94,35 @@ __device__ __forceinline__ uint64_t ts_out_index(uint64_t n, uint64_t i, uint64_
 
 // Work schedule, identical in the three roles of a CTA. k_splits >= 1:
 // whole tiles (or k_splits even K slices of each) dealt round robin over the
-// grid. k_splits == 0 (stream-K): CTA c takes the contiguous range
-// [S c / G, S (c + 1) / G) of the flattened (tile, K stage) space, S = tiles
-// x stages, G = grid, cut at tile boundaries into segments. A segment that
-// is not a whole tile adds its partial counts into the (zeroed) output.
+// grid. k_splits == 0 (stream-K, data-parallel head): the first
+// W = floor(tiles / G) x G tiles go whole, round robin (G = grid); CTA c then
+// takes the contiguous range [W nk + S c / G, W nk + S (c + 1) / G) of the
+// remaining tiles' flattened (tile, K stage) space, S = (tiles - W) x nk,
+// cut at tile boundaries into segments. A segment that is not a whole tile
+// adds its partial counts into the output, which must be zeroed for the
+// tiles from W on; whole tiles store theirs.
 struct TsSched {
-    uint32_t nk, n_tiles, k_splits, it;
-    uint64_t pos, end;
+    uint32_t nk, n_tiles, k_splits, it, whole = 0;
+    uint64_t pos = 0, end = 0;
     __device__ __forceinline__ TsSched(uint32_t nk_, uint32_t n_tiles_, uint32_t k_splits_)
         : nk(nk_), n_tiles(n_tiles_), k_splits(k_splits_), it(blockIdx.x) {
-        const uint64_t S = (uint64_t)n_tiles * nk;
-        pos = S * blockIdx.x / gridDim.x;
-        end = S * (blockIdx.x + 1) / gridDim.x;
+        if (k_splits == 0) {
+            whole = (n_tiles / gridDim.x) * gridDim.x;
+            const uint64_t S = (uint64_t)(n_tiles - whole) * nk;
+            pos = (uint64_t)whole * nk + S * blockIdx.x / gridDim.x;
+            end = (uint64_t)whole * nk + S * (blockIdx.x + 1) / gridDim.x;
+        }
     }
     __device__ __forceinline__ bool next(uint32_t& t, uint32_t& kb0, uint32_t& kb1, bool& partial) {
         if (k_splits == 0) {
+            if (it < whole) {
+                t = it;
+                kb0 = 0;
+                kb1 = nk;
+                partial = false;
+                it += gridDim.x;
+                return true;
+            }
             if (pos >= end) return false;
             t = (uint32_t)(pos / nk);
             kb0 = (uint32_t)(pos % nk);

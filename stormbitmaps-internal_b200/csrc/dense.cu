@@ -18,8 +18,12 @@ namespace sb200 {
 // Measured on B200: 272 tiles (1.8 waves) of 2^18-bit rows run 8 % faster
 // under stream-K, 136 tiles 1.9x, 1088 tiles (92 % fill) 7 %, 4160 tiles
 // (97 % fill) 3 %; 2176 tiles (98 % fill) of 2^16-bit rows 3 % slower, and
-// 80-stage tiles (20000-bit rows) 7 % slower. Returns the kernel's k_splits
-// argument (1 or 0) and sets the grid.
+// 80-stage tiles (20000-bit rows) 7 % slower. Those figures are for stream-K
+// over every tile; the kernels now run the first floor(tiles / grid) waves
+// as whole tiles and stream-K only the rest (TsSched), which measured faster
+// still on B200 (double-buffered kernel: 50000 x 20000 bits 7 %, 16384 x
+// 262144 5 %, 4096 x 65536 1 %) with counts unchanged. Returns the kernel's
+// k_splits argument (1 or 0) and sets the grid.
 static uint32_t ts_schedule(uint32_t n_tiles, int sms, uint32_t w_pad, uint32_t& grid,
                             int pref = STORM_B200_SCHED_AUTO) {
     const uint64_t nk = w_pad / (TS_KBITS / 64);
@@ -88,6 +92,20 @@ int DenseEngine::prepare(uint64_t n, uint64_t row_bits, int kernel_pref, cudaStr
     return kind;
 }
 
+// Stream-K over the whole cached list (TsSched, k_splits 0): tiles from
+// W = floor(tiles / grid) x grid on add into the output, and every one of them
+// has its A block at or past tile W's (the list is ordered by A block), so
+// zeroing the triangle from that block's first row on covers them.
+static_assert(T2_BM == MMA_BM, "both tensor-core tilings use 128-row A blocks");
+
+void DenseEngine::zero_stream_k_rows(uint32_t* d_out, uint32_t n, uint32_t grid, cudaStream_t st) {
+    const uint32_t whole = (n_tiles / grid) * grid;
+    if (whole >= n_tiles) return;
+    const uint64_t r0 = (uint64_t)h_tiles[whole].x * MMA_BM;   // 128-row A blocks in both tensor-core tilings
+    const uint64_t e0 = r0 * n - (r0 * (r0 - 1)) / 2;          // tri_index(n, r0, r0)
+    SB_CUDA(cudaMemsetAsync(d_out + e0, 0, (tri_size(n) - e0) * sizeof(uint32_t), st));
+}
+
 // Tiles [t0, t0 + count) of the cached list.
 void DenseEngine::launch(int kind, const uint64_t* dX, uint32_t n, uint32_t w_pad, uint32_t t0, uint32_t count,
                          uint32_t* d_out, cudaStream_t st) {
@@ -101,7 +119,7 @@ void DenseEngine::launch(int kind, const uint64_t* dX, uint32_t n, uint32_t w_pa
         // triangle can be zeroed first for the partial-count atomics
         uint32_t grid = count < (uint32_t)sms ? count : (uint32_t)sms;
         const uint32_t ks = (t0 == 0 && count == n_tiles) ? ts_schedule(count, sms, w_pad, grid, schedule) : 1;
-        if (ks != 1 && d_out) SB_CUDA(cudaMemsetAsync(d_out, 0, tri_size(n) * sizeof(uint32_t), st));
+        if (ks != 1 && d_out) zero_stream_k_rows(d_out, n, grid, st);
         const uint32_t smem = (uint64_t)w_pad * 64 <= TS_COALESCE_MAX_BITS ? TS_SMEM_BYTES : TS_SMEM_BYTES_LEAN;
         if ((uint64_t)w_pad * 64 <= MMA_MAX_BITS)
             bb_mma_ts_kernel<<<grid, TS_THREADS, smem, st>>>(dX, n, w_pad, d_tiles.p + t0, count, d_out, d_flags.p,
@@ -115,7 +133,7 @@ void DenseEngine::launch(int kind, const uint64_t* dX, uint32_t n, uint32_t w_pa
         smem_attr_once(bb_mma_ts2_long_kernel, (int)T2_SMEM_BYTES, done_b);
         uint32_t grid = count < (uint32_t)sms ? count : (uint32_t)sms;
         const uint32_t ks = (t0 == 0 && count == n_tiles) ? ts_schedule(count, sms, w_pad, grid, schedule) : 1;
-        if (ks != 1 && d_out) SB_CUDA(cudaMemsetAsync(d_out, 0, tri_size(n) * sizeof(uint32_t), st));
+        if (ks != 1 && d_out) zero_stream_k_rows(d_out, n, grid, st);
         if ((uint64_t)w_pad * 64 <= MMA_MAX_BITS)
             bb_mma_ts2_kernel<<<grid, T2_THREADS, T2_SMEM_BYTES, st>>>(dX, n, w_pad, d_tiles.p + t0, count, d_out,
                                                                       d_flags.p, ks);

@@ -50,6 +50,7 @@ struct DenseEngine {
     int prepare(uint64_t n, uint64_t row_bits, int kernel_pref, cudaStream_t st);
     void launch(int kind, const uint64_t* dX, uint32_t n, uint32_t w_pad, uint32_t t0, uint32_t count,
                 uint32_t* d_out, cudaStream_t st);
+    void zero_stream_k_rows(uint32_t* d_out, uint32_t n, uint32_t grid, cudaStream_t st);
     std::vector<uint2> h_tiles;
     std::vector<cudaEvent_t> panel_ev;
 };
