@@ -180,11 +180,14 @@ def dist_env():
     return rank, world, local
 
 
-def init_dist(world, backend):
+def init_dist(world, backend, timeout_s=180.0):
+    """Process group for N > 1 (None at N = 1). The timeout bounds every
+    collective: a rank that never arrives (it failed between steps) ends the
+    others' next collective with an error instead of a hang."""
     import torch.distributed as dist
     if world > 1 and not dist.is_initialized():
         import datetime
-        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=timeout_s))
     return dist if world > 1 else None
 
 
