@@ -114,6 +114,19 @@ int STORM_contig_upload(STORM_contiguous_t* c);
 /* Per-pair counts into a HOST buffer of out_len >= n*(n+1)/2 entries. */
 int STORM_contig_pairw_intersect_matrix(STORM_contiguous_t* c, uint32_t* out,
                                         uint64_t out_len, uint64_t* sum);
+/* STORM_contig_clear + STORM_contig_add_bitmaps + STORM_contig_pairw_intersect_matrix
+ * in one call, so that the three overlap: n_rows rows of words_per_row (=
+ * ceil(vector_length / 64)) words in HOST memory -- pinned memory lets the
+ * copies run asynchronously -- replace the container's rows and are copied
+ * to the device last rows first, while the tiles that read only those rows
+ * already run (from the bottom of the triangle up) and the finished rows of
+ * the triangle are copied back into out (out_len >= n*(n+1)/2).  Same checks
+ * and codes as the three calls; device-memory rows get STORM_B200_EARG (use
+ * STORM_contig_add_bitmaps).  Afterwards the container holds the rows; on an
+ * error it is left empty.  Counts are those of the three calls. */
+int STORM_contig_pairw_intersect_matrix_from_host(STORM_contiguous_t* c, const uint64_t* rows, uint32_t n_rows,
+                                                  uint32_t words_per_row, uint32_t* out, uint64_t out_len,
+                                                  uint64_t* sum);
 /* Same, into a DEVICE buffer on the current device (d_out may be NULL to
  * compute only the sum).  Work already queued on other streams is waited for
  * before d_out is written. */

@@ -84,6 +84,8 @@ _sig("STORM_pairw_threshold", C.c_int, [C.c_void_p, C.c_double, u32p, u32p, u32p
                                         C.POINTER(C.c_uint64)])
 _sig("STORM_contig_upload", C.c_int, [C.c_void_p])
 _sig("STORM_contig_pairw_intersect_matrix", C.c_int, [C.c_void_p, u32p, C.c_uint64, u64p])
+_sig("STORM_contig_pairw_intersect_matrix_from_host", C.c_int,
+     [C.c_void_p, u64p, C.c_uint32, C.c_uint32, u32p, C.c_uint64, u64p])
 _sig("STORM_contig_pairw_intersect_matrix_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, u64p])
 _sig("STORM_contig_pairw_intersect_tiles", C.c_int, [C.c_void_p, C.c_uint32, TILE_CB, C.c_void_p])
 _sig("STORM_contig_stream", C.c_void_p, [C.c_void_p])
@@ -306,6 +308,19 @@ class StormContig:
         s = C.c_uint64(0)
         _check(_lib.STORM_contig_pairw_intersect_matrix(self.h, _p(out, u32p), out.size, C.byref(s)),
                "STORM_contig_pairw_intersect_matrix")
+        return out[: tri_size(n)], int(s.value)
+
+    def matrix_from_host(self, words: np.ndarray, out: np.ndarray | None = None):
+        """Replace the rows with `words` (n x ceil(len/64) u64, host) and return
+        (packed triangle, sum) in one overlapped call."""
+        words = np.ascontiguousarray(words, dtype=np.uint64)
+        n = words.shape[0]
+        if out is None:
+            out = np.zeros(max(1, tri_size(n)), dtype=np.uint32)
+        s = C.c_uint64(0)
+        _check(_lib.STORM_contig_pairw_intersect_matrix_from_host(self.h, _p(words, u64p), n, words.shape[1],
+                                                                  _p(out, u32p), out.size, C.byref(s)),
+               "STORM_contig_pairw_intersect_matrix_from_host")
         return out[: tri_size(n)], int(s.value)
 
     def matrix_device(self, d_out_ptr: int, out_len: int) -> int:

@@ -31,6 +31,7 @@ struct STORM_contiguous_s {
     sb200::DevBuf<uint32_t> d_out;
     cudaStream_t stream = nullptr;
     cudaStream_t copy_stream = nullptr;   // device-to-host copies overlapping the next panel
+    cudaStream_t h2d_stream = nullptr;    // host-to-device row copies of the one-call host form
     int kernel_pref = STORM_B200_KERNEL_AUTO;
     sb200::DenseEngine engine;
     sb200::DevBuf<uint2> d_hits;               // thresholded form: reported pairs and counts
@@ -39,6 +40,7 @@ struct STORM_contiguous_s {
     ~STORM_contiguous_s() {
         if (stream) cudaStreamDestroy(stream);
         if (copy_stream) cudaStreamDestroy(copy_stream);
+        if (h2d_stream) cudaStreamDestroy(h2d_stream);
     }
 };
 
@@ -320,6 +322,44 @@ int STORM_contig_pairw_intersect_matrix(STORM_contiguous_t* c, uint32_t* out, ui
     if (out == NULL && c->n_rows) return STORM_B200_EVALUES;
     return guard([&]() -> int {
         const uint64_t s = contig_matrix_host(c, out, out_len);
+        if (sum) *sum = s;
+        return 0;
+    });
+}
+
+int STORM_contig_pairw_intersect_matrix_from_host(STORM_contiguous_t* c, const uint64_t* rows, uint32_t n_rows,
+                                                  uint32_t words_per_row, uint32_t* out, uint64_t out_len,
+                                                  uint64_t* sum) {
+    if (c == NULL) return STORM_B200_ENULL;
+    if ((rows == NULL || out == NULL) && n_rows) return STORM_B200_EVALUES;
+    return guard([&]() -> int {
+        if (words_per_row != c->n_words) return STORM_B200_EARG;
+        if (out_len < tri_size(n_rows)) return STORM_B200_ESIZE;
+        if (n_rows) {
+            cudaPointerAttributes pa;
+            const bool on_device = cudaPointerGetAttributes(&pa, rows) == cudaSuccess &&
+                                   (pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged);
+            cudaGetLastError();
+            if (on_device) return STORM_B200_EARG;
+        }
+        if (c->vector_length % 64 && n_rows) {
+            const uint64_t tail_mask = ~0ull << (c->vector_length % 64);
+            for (uint64_t r = 0; r < n_rows; ++r)
+                if (rows[r * words_per_row + words_per_row - 1] & tail_mask) return STORM_B200_EARG;
+        }
+        c->stage.clear();
+        c->n_rows = 0;
+        c->dev_rows = 0;
+        if (sum) *sum = 0;
+        if (n_rows == 0) return 0;
+        contig_grow(c, n_rows);
+        c->d_out.reserve(tri_size(n_rows));
+        if (!c->copy_stream) SB_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        if (!c->h2d_stream) SB_CUDA(cudaStreamCreateWithFlags(&c->h2d_stream, cudaStreamNonBlocking));
+        const uint64_t s = c->engine.run_host_to_host(c->d_rows.p, n_rows, c->w_pad, c->vector_length, rows,
+                                                      words_per_row, c->d_out.p, out, c->kernel_pref,
+                                                      contig_stream(c), c->copy_stream, c->h2d_stream);
+        c->n_rows = c->dev_rows = n_rows;
         if (sum) *sum = s;
         return 0;
     });

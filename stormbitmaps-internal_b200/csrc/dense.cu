@@ -178,6 +178,42 @@ uint64_t DenseEngine::run(const uint64_t* dX, uint64_t n, uint32_t w_pad, uint64
     return f.sum;
 }
 
+// Panels of the host-output forms, in processing order (the bottom of the
+// triangle first): [t0, t1) ranges of the tile list. Sizes are whole waves of
+// the launch's grid (no SM idles at a launch's end), growing from one wave at
+// both ends -- the first panel reads only the last rows, the last panel's
+// rows are the only copy still running when the tiles end -- to about 1/24
+// of the tiles. Small lists run as one launch.
+static std::vector<std::pair<uint32_t, uint32_t>> host_panels(uint32_t n_tiles, uint32_t wave) {
+    std::vector<std::pair<uint32_t, uint32_t>> p;
+    if (n_tiles <= 4ull * wave) {
+        p.emplace_back(0u, n_tiles);
+        return p;
+    }
+    const uint64_t total_w = n_tiles / wave;   // the remainder (< 1 wave) joins the last panel
+    const uint64_t cap = std::max<uint64_t>(1, total_w / 24);
+    std::vector<uint64_t> head;
+    uint64_t used = 0;
+    for (uint64_t s = 1; s < cap && used + 2 * s <= total_w / 2; s *= 2) {
+        head.push_back(s);
+        used += s;
+    }
+    std::vector<uint64_t> sizes(head);
+    for (uint64_t mid = total_w - 2 * used; mid > 0;) {
+        const uint64_t s = std::min(cap, mid);
+        sizes.push_back(s);
+        mid -= s;
+    }
+    sizes.insert(sizes.end(), head.rbegin(), head.rend());
+    uint64_t hi = n_tiles;
+    for (size_t k = 0; k < sizes.size(); ++k) {
+        const uint64_t lo = (k + 1 == sizes.size()) ? 0 : hi - sizes[k] * wave;
+        p.emplace_back((uint32_t)lo, (uint32_t)hi);
+        hi = lo;
+    }
+    return p;
+}
+
 uint64_t DenseEngine::run_to_host(const uint64_t* dX, uint64_t n, uint32_t w_pad, uint64_t row_bits,
                                   uint32_t* d_out, uint32_t* host_out, int kernel_pref, cudaStream_t st,
                                   cudaStream_t copy_st) {
@@ -187,35 +223,106 @@ uint64_t DenseEngine::run_to_host(const uint64_t* dX, uint64_t n, uint32_t w_pad
         return 0;
     }
     const int kind = prepare(n, row_bits, kernel_pref, st);
-    // Row panels of ~1/12 of the tiles each (tiles are ordered by A block).
-    const uint32_t bm = (kind == STORM_B200_KERNEL_POPC) ? POPC_BM : MMA_BM;
-    const uint32_t want_panels = n_tiles >= 12 * 148 ? 12 : 1;
-    std::vector<uint32_t> cut{0};
-    for (uint32_t t = 1; t < n_tiles; ++t)
-        if (h_tiles[t].x != h_tiles[t - 1].x &&
-            (uint64_t)t * want_panels >= (uint64_t)n_tiles * cut.size())
-            cut.push_back(t);
-    cut.push_back(n_tiles);
-    while (panel_ev.size() < cut.size()) {
+    return panels_to_host(dX, n, w_pad, kind, d_out, host_out, st, copy_st, 0);
+}
+
+uint64_t DenseEngine::run_host_to_host(uint64_t* dX, uint64_t n, uint32_t w_pad, uint64_t row_bits,
+                                       const uint64_t* host_rows, uint32_t host_wpr, uint32_t* d_out,
+                                       uint32_t* host_out, int kernel_pref, cudaStream_t st, cudaStream_t copy_st,
+                                       cudaStream_t h2d_st) {
+    if (n == 0) {
+        log.launches = 0;
+        log.last_ms = 0.f;
+        return 0;
+    }
+    const int kind = prepare(n, row_bits, kernel_pref, st);
+    // What the copies do not cover reads as zero: the row pitch's padding
+    // words and the rows [n, n_pad) that whole 128 x 256 tiles read.
+    const uint64_t n_pad = round_up(n, 256);
+    if (host_wpr != w_pad)
+        SB_CUDA(cudaMemsetAsync(dX, 0, n_pad * w_pad * sizeof(uint64_t), h2d_st));
+    else if (n_pad > n)
+        SB_CUDA(cudaMemsetAsync(dX + n * w_pad, 0, (n_pad - n) * w_pad * sizeof(uint64_t), h2d_st));
+    const uint64_t chunk_rows = round_up(std::max<uint64_t>(1, (n + 31) / 32), 128);
+    const uint64_t chunks = (n + chunk_rows - 1) / chunk_rows;
+    while (h2d_ev.size() < chunks) {
+        cudaEvent_t e;
+        SB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        h2d_ev.push_back(e);
+    }
+    // Last rows first: the bottom panels read only them. Event c marks rows
+    // [c x chunk_rows, n) (and the zeroing) as resident.
+    for (uint64_t c = chunks; c-- > 0;) {
+        const uint64_t r0 = c * chunk_rows, r1 = std::min(n, r0 + chunk_rows);
+        SB_CUDA(cudaMemcpy2DAsync(dX + r0 * w_pad, (size_t)w_pad * sizeof(uint64_t), host_rows + r0 * host_wpr,
+                                  (size_t)host_wpr * sizeof(uint64_t), (size_t)host_wpr * sizeof(uint64_t),
+                                  r1 - r0, cudaMemcpyHostToDevice, h2d_st));
+        SB_CUDA(cudaEventRecord(h2d_ev[c], h2d_st));
+    }
+    uint64_t s = 0;
+    try {
+        s = panels_to_host(dX, n, w_pad, kind, d_out, host_out, st, copy_st, chunk_rows);
+    } catch (...) {
+        cudaStreamSynchronize(h2d_st);   // no copy may still read the caller's rows after the return
+        throw;
+    }
+    SB_CUDA(cudaStreamSynchronize(h2d_st));
+    return s;
+}
+
+// chunk_rows != 0: rows arrive in chunks of chunk_rows on h2d_ev; each panel
+// waits for the chunk holding the lowest row its tiles read.
+uint64_t DenseEngine::panels_to_host(const uint64_t* dX, uint64_t n, uint32_t w_pad, int kind, uint32_t* d_out,
+                                     uint32_t* host_out, cudaStream_t st, cudaStream_t copy_st,
+                                     uint64_t chunk_rows) {
+    const int sms = require_device();
+    const uint64_t bm = (kind == STORM_B200_KERNEL_POPC) ? POPC_BM : MMA_BM;
+    const uint64_t bn = (kind == STORM_B200_KERNEL_POPC)     ? POPC_BM
+                        : (kind == STORM_B200_KERNEL_MMA_DB) ? T2_BN
+                                                             : MMA_BN;
+    const uint32_t wave = (kind == STORM_B200_KERNEL_POPC) ? 2u * (uint32_t)sms : (uint32_t)sms;
+    const auto panels = host_panels(n_tiles, wave);
+    // first tile of each A block (the list is ordered by A block)
+    std::vector<uint32_t> first_tile((size_t)h_tiles.back().x + 1, 0);
+    for (uint32_t t = n_tiles; t-- > 0;) first_tile[h_tiles[t].x] = t;
+    while (panel_ev.size() < panels.size()) {
         cudaEvent_t e;
         SB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         panel_ev.push_back(e);
     }
     SB_CUDA(cudaEventRecord(log.ev0, st));
-    uint32_t launches = 0;
-    for (size_t p = 0; p + 1 < cut.size(); ++p) {
-        const uint32_t t0 = cut[p], t1 = cut[p + 1];
-        launch(kind, dX, (uint32_t)n, w_pad, t0, t1 - t0, d_out, st);
-        ++launches;
-        SB_CUDA(cudaEventRecord(panel_ev[p], st));
-        // rows of this panel: A blocks [first, last]
-        const uint64_t r0 = (uint64_t)h_tiles[t0].x * bm;
-        const uint64_t r1 = std::min<uint64_t>(n, ((uint64_t)h_tiles[t1 - 1].x + 1) * bm);
-        const uint64_t e0 = r0 * n - (r0 * (r0 - 1)) / 2;   // tri_index(n, r0, r0)
-        const uint64_t e1 = r1 * n - (r1 * (r1 - 1)) / 2;
-        SB_CUDA(cudaStreamWaitEvent(copy_st, panel_ev[p], 0));
-        SB_CUDA(cudaMemcpyAsync(host_out + e0, d_out + e0, (e1 - e0) * sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                                copy_st));
+    uint64_t copied_from = n;   // rows [copied_from, n) are on their way to the host
+    try {
+        for (size_t p = 0; p < panels.size(); ++p) {
+            const uint32_t t0 = panels[p].first, t1 = panels[p].second;
+            if (chunk_rows) {
+                uint64_t need = n;
+                for (uint32_t t = t0; t < t1; ++t)
+                    need = std::min(need, std::min<uint64_t>(h_tiles[t].x * bm, h_tiles[t].y * bn));
+                SB_CUDA(cudaStreamWaitEvent(st, h2d_ev[need / chunk_rows], 0));
+            }
+            launch(kind, dX, (uint32_t)n, w_pad, t0, t1 - t0, d_out, st);
+            SB_CUDA(cudaEventRecord(panel_ev[p], st));
+            // Every tile from t0 on is done: the A blocks whose first tile is at
+            // or past t0 are complete, and their rows are contiguous in the
+            // packed triangle.
+            uint64_t b = h_tiles[t0].x;
+            if (first_tile[b] != t0) ++b;
+            const uint64_t r = std::min<uint64_t>(n, b * bm);
+            if (r < copied_from) {
+                const uint64_t e0 = r * n - (r * (r - 1)) / 2;   // tri_index(n, r, r)
+                const uint64_t e1 = copied_from * n - (copied_from * (copied_from - 1)) / 2;
+                SB_CUDA(cudaStreamWaitEvent(copy_st, panel_ev[p], 0));
+                SB_CUDA(cudaMemcpyAsync(host_out + e0, d_out + e0, (e1 - e0) * sizeof(uint32_t),
+                                        cudaMemcpyDeviceToHost, copy_st));
+                copied_from = r;
+            }
+        }
+    } catch (...) {
+        // no copy may still write the caller's buffer after the return
+        cudaStreamSynchronize(st);
+        cudaStreamSynchronize(copy_st);
+        throw;
     }
     SB_CUDA(cudaEventRecord(log.ev1, st));
     DeviceFlags f;
@@ -223,9 +330,10 @@ uint64_t DenseEngine::run_to_host(const uint64_t* dX, uint64_t n, uint32_t w_pad
     SB_CUDA(cudaStreamSynchronize(st));
     SB_CUDA(cudaStreamSynchronize(copy_st));
     SB_CUDA(cudaEventElapsedTime(&log.last_ms, log.ev0, log.ev1));
-    log.launches = launches;
+    log.launches = (uint32_t)panels.size();
     log.kernel = kind;
     if (f.error) fail(STORM_B200_ETIMEOUT, "bitmap x bitmap kernel: bounded wait expired");
+    if (copied_from != 0) fail(STORM_B200_ECUDA, "panel schedule left rows uncopied");
     return f.sum;
 }
 }  // namespace sb200

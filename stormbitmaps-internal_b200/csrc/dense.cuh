@@ -21,6 +21,7 @@ struct DenseEngine {
     ~DenseEngine() {
         log.destroy();
         for (cudaEvent_t e : panel_ev) cudaEventDestroy(e);
+        for (cudaEvent_t e : h2d_ev) cudaEventDestroy(e);
     }
 
     // Returns the sum over i < j; writes the packed upper triangle to d_out
@@ -30,10 +31,19 @@ struct DenseEngine {
                  int kernel_pref, cudaStream_t st);
 
     // Same result, with the packed triangle also copied to host_out: the
-    // tiles run in row panels and each finished panel's rows are copied on
-    // copy_st while the next panel computes.
+    // tiles run in panels from the bottom of the triangle up, and the rows
+    // each panel completes are copied on copy_st while the next computes.
     uint64_t run_to_host(const uint64_t* dX, uint64_t n, uint32_t w_pad, uint64_t row_bits, uint32_t* d_out,
                          uint32_t* host_out, int kernel_pref, cudaStream_t st, cudaStream_t copy_st);
+
+    // run_to_host with the rows also coming from the host: host_rows (n x
+    // host_wpr words, host memory) are copied into dX ([n_pad][w_pad],
+    // zero padded here) on h2d_st, last rows first, and each panel waits
+    // only for the rows its tiles read, so the upload, the tiles and the
+    // copy back overlap.
+    uint64_t run_host_to_host(uint64_t* dX, uint64_t n, uint32_t w_pad, uint64_t row_bits,
+                              const uint64_t* host_rows, uint32_t host_wpr, uint32_t* d_out, uint32_t* host_out,
+                              int kernel_pref, cudaStream_t st, cudaStream_t copy_st, cudaStream_t h2d_st);
 
     // Thresholded form: the pairs i < j with count v > 0 and
     // v / (|Xi| + |Xj| - v) >= t, appended to d_pairs / d_cnts (up to cap,
@@ -51,8 +61,10 @@ struct DenseEngine {
     void launch(int kind, const uint64_t* dX, uint32_t n, uint32_t w_pad, uint32_t t0, uint32_t count,
                 uint32_t* d_out, cudaStream_t st);
     void zero_stream_k_rows(uint32_t* d_out, uint32_t n, uint32_t grid, cudaStream_t st);
+    uint64_t panels_to_host(const uint64_t* dX, uint64_t n, uint32_t w_pad, int kind, uint32_t* d_out,
+                            uint32_t* host_out, cudaStream_t st, cudaStream_t copy_st, uint64_t chunk_rows);
     std::vector<uint2> h_tiles;
-    std::vector<cudaEvent_t> panel_ev;
+    std::vector<cudaEvent_t> panel_ev, h2d_ev;
 };
 
 inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }

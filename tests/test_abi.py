@@ -96,6 +96,19 @@ def test_host_argument_checks_follow_reference_codes(sb):
         assert L.STORM_contig_add(c, bad.ctypes.data_as(sb.u32p), 2) == sb.EARG
         assert L.STORM_contig_add(c, v.ctypes.data_as(sb.u32p), 3) == 3
         assert L.STORM_contig_size(c) == 1
+        # the one-call host form checks its arguments before any device work
+        F = L.STORM_contig_pairw_intersect_matrix_from_host
+        rows = np.zeros((4, 16), dtype=np.uint64)                           # ceil(1000 / 64) = 16 words
+        out = np.zeros(10, dtype=np.uint32)
+        u64 = rows.ctypes.data_as(sb.u64p)
+        assert F(None, u64, 4, 16, out.ctypes.data_as(sb.u32p), 10, None) == sb.ENULL
+        assert F(c, None, 4, 16, out.ctypes.data_as(sb.u32p), 10, None) == sb.EVALUES
+        assert F(c, u64, 4, 16, None, 10, None) == sb.EVALUES
+        assert F(c, u64, 4, 15, out.ctypes.data_as(sb.u32p), 10, None) == sb.EARG    # words per row
+        assert F(c, u64, 4, 16, out.ctypes.data_as(sb.u32p), 9, None) == sb.ESIZE    # 4 rows: 10 counts
+        rows[2, 15] = 1 << 40                                                         # bit 1000 >= length
+        assert F(c, u64, 4, 16, out.ctypes.data_as(sb.u32p), 10, None) == sb.EARG
+        assert L.STORM_contig_size(c) == 1                                            # untouched on a refusal
     finally:
         L.STORM_contig_free(c)
 

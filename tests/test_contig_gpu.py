@@ -375,3 +375,44 @@ def test_autotune_keeps_the_fastest_exact_kernel(sb):
     k, sched, times = c.autotune()
     assert times[4] == -1.0 and times[0] > 0 and times[2] > 0 and times[5] > 0
     assert c.matrix()[1] == ol.contig_matrix(words)[1]
+
+
+@pytest.mark.parametrize("kernel", ("auto",) + KERNELS)
+def test_matrix_from_host_overlapped(sb, kernel):
+    """The one-call host form (rows in from host memory, triangle out to host
+    memory, upload / tiles / copy-back overlapped in panels from the bottom of
+    the triangle up) equals the oracle; the container then holds the rows and
+    the two-call host form (bottom-up panels too) gives the same counts.
+    9000 rows: 8 to 11 panels, whichever kernel."""
+    n, m = 9000, 512
+    words = gen.bernoulli_rows(n, m, (0.05, 0.5), 71)
+    want, ws = ol.contig_matrix(words)
+    c = sb.StormContig(m)
+    if kernel != "auto":
+        c.set_kernel(_kernel(sb, kernel))
+    got, s = c.matrix_from_host(words)
+    assert s == ws
+    np.testing.assert_array_equal(got, want)
+    assert len(c) == n
+    got2, s2 = c.matrix()
+    assert s2 == ws
+    np.testing.assert_array_equal(got2, want)
+    c.close()
+
+
+def test_matrix_from_host_ragged_rows(sb):
+    """Row length not a multiple of 64 or of the 512-bit pitch (zeroed pitch
+    padding), a repeated call replacing the rows, and 0 / 1 rows."""
+    m = 4100
+    c = sb.StormContig(m)
+    for n, seed in ((7000, 72), (300, 73), (1, 74), (0, 75), (5000, 76)):
+        words = gen.bernoulli_rows(n, m, (0.05, 0.5), seed) if n else np.zeros((0, 65), dtype=np.uint64)
+        got, s = c.matrix_from_host(words)
+        assert len(c) == n
+        if n == 0:
+            assert s == 0
+            continue
+        want, ws = ol.contig_matrix(words)
+        assert s == ws, n
+        np.testing.assert_array_equal(got, want, err_msg=str(n))
+    c.close()
