@@ -859,13 +859,16 @@ def run_b200_arm(args):
     thresh = None
     if args.forms and rank == 0 and world == 1:   # single-GPU characterisation forms
         t_j = 0.3
-        tms, hits = [], 0
-        for _ in range(3):
-            _, _, _, hits = c.threshold(t_j, cap=1 << 25)
-            tms.append(c.last_kernel_ms())
-        thresh = {"jaccard_min": t_j, "ms": round(min(tms), 3), "pairs_per_s": tri / (min(tms) * 1e-3),
-                  "hits": hits, "hit_fraction": hits / tri, "triangle_bytes_not_written": tri * 4,
-                  "vs_full_triangle_kernel_ms": round(statistics.median(kernel_ms), 3)}
+        try:
+            tms, hits = [], 0
+            for _ in range(3):
+                _, _, _, hits = c.threshold(t_j, cap=1 << 25)
+                tms.append(c.last_kernel_ms())
+            thresh = {"jaccard_min": t_j, "ms": round(min(tms), 3), "pairs_per_s": tri / (min(tms) * 1e-3),
+                      "hits": hits, "hit_fraction": hits / tri, "triangle_bytes_not_written": tri * 4,
+                      "vs_full_triangle_kernel_ms": round(statistics.median(kernel_ms), 3)}
+        except Exception as e:   # reported, never silently dropped
+            thresh = {"error": f"{type(e).__name__}: {e}"}
 
     # ---- roofline of the dominant kernel ----
     peaks, peak_src = measured_peaks()
