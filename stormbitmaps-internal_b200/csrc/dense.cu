@@ -43,6 +43,14 @@ constexpr uint64_t DB_AUTO_MAX_BITS = 1ull << 17;
 
 static void build_tiles(std::vector<uint2>& t, uint64_t n, int kind) {
     t.clear();
+    // tile indices and counts are 32-bit (the kernels' work lists); bound the
+    // count by the full block grid before building anything
+    const uint64_t bm = (kind == STORM_B200_KERNEL_POPC) ? POPC_BM : MMA_BM;
+    const uint64_t bn = (kind == STORM_B200_KERNEL_POPC)     ? POPC_BM
+                        : (kind == STORM_B200_KERNEL_MMA_DB) ? T2_BN
+                                                             : MMA_BN;
+    if (((n + bm - 1) / bm) * ((n + bn - 1) / bn) > 0xFFFFFFFFull)
+        fail(STORM_B200_ELIMIT, "more than 2^32 tiles: split the rows into several containers");
     if (kind == STORM_B200_KERNEL_MMA || kind == STORM_B200_KERNEL_MMA_SS) {
         const uint64_t nbi = (n + MMA_BM - 1) / MMA_BM, nbj = (n + MMA_BN - 1) / MMA_BN;
         // Tile (bi, bj) holds a pair with i <= j iff 128 bi <= 256 bj + 255,
