@@ -461,9 +461,11 @@ static void rows_run(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell,
         if (st_out) *st_out = S;
         return;
     }
-    const std::vector<uint32_t> order = rows_order(r, policy);
     const uint32_t nb = (n + T - 1) / T;
+    if ((uint64_t)nb * (nb + 1) / 2 > 0xFFFFFFFFull)
+        fail(STORM_B200_ELIMIT, "more than 2^32 tiles: use a larger tile or split the rows");
     const uint32_t ntiles = nb * (nb + 1) / 2;
+    const std::vector<uint32_t> order = rows_order(r, policy);
     r->d_order.reserve(n);
     r->d_bmeta.reserve(nb);
     r->d_het.reserve(nb);
@@ -925,8 +927,10 @@ int STORM_rows_train_selector(STORM_rows_t* r, uint32_t tile, uint32_t samples, 
         if (n < 2) return STORM_B200_EARG;
         const uint32_t T = tile ? tile : 64;
         r->trained_tile = T;
+        const uint32_t nb = (n + T - 1) / T;
+        if ((uint64_t)nb * (nb + 1) / 2 > 0xFFFFFFFFull) return STORM_B200_ELIMIT;
+        const uint32_t ntiles = nb * (nb + 1) / 2;
         const std::vector<uint32_t> order = rows_order(r, STORM_POLICY_PERTILE);
-        const uint32_t nb = (n + T - 1) / T, ntiles = nb * (nb + 1) / 2;
         r->d_order.reserve(n);
         r->d_bmeta.reserve(nb);
         r->d_het.reserve(nb);
