@@ -1,7 +1,9 @@
 // chunk_engine.cu -- packing and the warp-per-pair kernel over 65536-bit
 // chunks (layout and cell rules: chunk_engine.cuh).
 #include <cmath>
+#include <cstring>
 #include <algorithm>
+#include <thread>
 #include "chunk_engine.cuh"
 #include "dense.cuh"
 
@@ -55,6 +57,126 @@ void ChunkPack::add_row(const STORM_bitmap_cont_t* c) {
     end_row();
 }
 
+void ChunkPack::add_rows(const STORM_bitmap_cont_t* rows, uint64_t n) {
+    if (n == 0) return;
+    auto live = [&](uint64_t r) { return rows[r].bitmaps && rows[r].block_ids ? rows[r].n_bitmaps : 0u; };
+    // Pass 1: every row's chunk count, bitmap chunks and list slots (each
+    // list starts on a multiple of 8 entries, as add_chunk places them).
+    std::vector<uint64_t> c_base(n + 1), b_base(n + 1), l_base(n + 1);
+    std::vector<uint64_t> l_used(n);
+    std::vector<uint8_t> has_list(n);
+    for (uint64_t r = 0; r < n; ++r) {
+        const uint32_t k_n = live(r);
+        uint64_t nb = 0, pos = 0;
+        bool lists = false;
+        for (uint32_t k = 0; k < k_n; ++k) {
+            const STORM_bitmap_t& b = rows[r].bitmaps[k];
+            if (b.n_bitmap) {
+                ++nb;
+            } else {
+                pos = (pos + 7) / 8 * 8 + (b.scalar ? b.n_scalar : 0);
+                lists = true;
+            }
+        }
+        c_base[r + 1] = c_base[r] + k_n;
+        b_base[r + 1] = b_base[r] + nb * CHUNK_WORDS;
+        l_used[r] = pos;
+        has_list[r] = lists;
+        l_base[r + 1] = l_base[r] + (pos + 7) / 8 * 8;
+    }
+    // Global placement: appended after what the pack already holds.
+    const uint64_t c0 = cid.size(), b0 = bm.size();
+    uint64_t last_list_row = n;
+    for (uint64_t r = n; r-- > 0;)
+        if (has_list[r]) {
+            last_list_row = r;
+            break;
+        }
+    const uint64_t l0 = last_list_row < n ? (lst.size() + 7) / 8 * 8 : lst.size();
+    const uint64_t l_end = last_list_row < n ? l0 + l_base[last_list_row] + l_used[last_list_row] : lst.size();
+    cid.resize(c0 + c_base[n]);
+    ckl.resize(c0 + c_base[n]);
+    coff.resize(c0 + c_base[n]);
+    bm.resize(b0 + b_base[n]);
+    lst.resize(l_end, 0);   // padding between lists stays zero
+    std::vector<ChunkRowFacts> fr(n);
+    std::vector<uint32_t> row_max(n, 0);
+    // Pass 2: fill, rows split over threads by the bytes they copy.
+    auto fill = [&](uint64_t r0, uint64_t r1) {
+        for (uint64_t r = r0; r < r1; ++r) {
+            ChunkRowFacts f;
+            uint32_t mx = 0;
+            uint64_t c = c0 + c_base[r], w = b0 + b_base[r], pos = 0;
+            const uint64_t lb = l0 + l_base[r];
+            const uint32_t k_n = live(r);
+            for (uint32_t k = 0; k < k_n; ++k, ++c) {
+                const STORM_bitmap_t& b = rows[r].bitmaps[k];
+                const uint32_t id = rows[r].block_ids[k];
+                cid[c] = id;
+                ++f.chunks;
+                if (k > 0 && id <= rows[r].block_ids[k - 1]) f.plain = false;
+                if (b.n_bitmap) {
+                    const uint32_t nw = b.n_bitmap < CHUNK_WORDS ? b.n_bitmap : CHUNK_WORDS;
+                    coff[c] = w;
+                    ckl[c] = CK_BITMAP | nw;
+                    uint64_t* dst = bm.data() + w;
+                    const uint32_t copied = b.data ? nw : 0;
+                    if (copied) std::memcpy(dst, b.data, copied * sizeof(uint64_t));
+                    std::memset(dst + copied, 0, (CHUNK_WORDS - copied) * sizeof(uint64_t));
+                    w += CHUNK_WORDS;
+                    if (b.n_bitmap != CHUNK_WORDS || b.data == NULL) f.plain = false;
+                    f.card += b.n_bits_set;
+                    ++f.bitmap_chunks;
+                } else {
+                    const uint32_t ns = b.scalar ? b.n_scalar : 0;
+                    pos = (pos + 7) / 8 * 8;
+                    coff[c] = lb + pos;
+                    uint32_t flags = ns & CK_LEN;
+                    for (uint32_t e = 1; e < ns; ++e)
+                        if (b.scalar[e] == b.scalar[e - 1]) {
+                            flags |= CK_DUP;
+                            break;
+                        }
+                    ckl[c] = flags;
+                    if (ns) std::memcpy(lst.data() + lb + pos, b.scalar, ns * sizeof(uint16_t));
+                    pos += ns;
+                    if (flags & CK_DUP) f.plain = false;
+                    f.card += ns;
+                    f.list_entries += ns;
+                }
+                if (id > mx) mx = id;
+            }
+            fr[r] = f;
+            row_max[r] = mx;
+        }
+    };
+    const uint64_t work = b_base[n] * 8 + l_base[n] * 2 + c_base[n] * 16;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const uint64_t n_thr = std::min<uint64_t>({(uint64_t)std::min(hw, 32u), n, 1 + work / (8u << 20)});
+    if (n_thr <= 1) {
+        fill(0, n);
+    } else {
+        // contiguous row ranges of about equal bytes
+        std::vector<uint64_t> cut{0};
+        uint64_t acc = 0;
+        for (uint64_t r = 0; r < n && cut.size() < n_thr; ++r) {
+            acc += (b_base[r + 1] - b_base[r]) * 8 + (l_base[r + 1] - l_base[r]) * 2 +
+                   (c_base[r + 1] - c_base[r]) * 16;
+            if (acc * n_thr >= work * cut.size()) cut.push_back(r + 1);
+        }
+        if (cut.back() != n) cut.push_back(n);
+        std::vector<std::thread> th;
+        for (size_t t = 0; t + 1 < cut.size(); ++t)
+            if (cut[t] < cut[t + 1]) th.emplace_back(fill, cut[t], cut[t + 1]);
+        for (auto& t : th) t.join();
+    }
+    for (uint64_t r = 0; r < n; ++r) {
+        facts.push_back(fr[r]);
+        row_off.push_back(c0 + c_base[r + 1]);
+        if (row_max[r] > max_cid) max_cid = row_max[r];
+    }
+}
+
 double chunk_self_pair_ns(const ChunkCostModel& m, const ChunkRowFacts& f, uint64_t slots) {
     if (f.chunks == 0 || slots == 0) return 0.0;
     const uint32_t lists = f.chunks - f.bitmap_chunks;
@@ -69,8 +191,8 @@ double chunk_self_pair_ns(const ChunkCostModel& m, const ChunkRowFacts& f, uint6
 
 double tensor_pair_ns(const ChunkCostModel& m, uint64_t slots) { return m.ns_per_tensor_bit * 65536.0 * slots; }
 
-template <class T>
-static void put(DevBuf<T>& d, const std::vector<T>& h, cudaStream_t st) {
+template <class T, class A>
+static void put(DevBuf<T>& d, const std::vector<T, A>& h, cudaStream_t st) {
     d.reserve(h.size() ? h.size() : 1);
     if (!h.empty()) SB_CUDA(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
 }

@@ -23,6 +23,8 @@
 //          matching the k-th copy of a value with the k-th copy (the scalar
 //          merge's count, storm.cpp:72-86).
 #pragma once
+#include <memory>
+#include <utility>
 #include <vector>
 #include "common.cuh"
 
@@ -46,6 +48,27 @@ struct ChunkView {
 // counts by kind, list entries, and whether it is "plain" (strictly
 // ascending chunk ids, no repeated list value, full 1024-word bitmaps -- so
 // that its chunks expand to one contiguous bitmap with the same counts).
+// Allocator whose resize() leaves new elements unwritten (the bitmap pool is
+// filled entirely by the packer, so zeroing it first only costs time).
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template <class U>
+    NoInitAlloc(const NoInitAlloc<U>&) {}
+    template <class U>
+    void construct(U* p) {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <class U, class... Args>
+    void construct(U* p, Args&&... args) {
+        ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
+    }
+};
+
 struct ChunkRowFacts {
     uint64_t card = 0, list_entries = 0;
     uint32_t chunks = 0, bitmap_chunks = 0;
@@ -58,7 +81,7 @@ struct ChunkPack {
     std::vector<uint64_t> row_off{0};
     std::vector<uint32_t> cid, ckl;
     std::vector<uint64_t> coff;
-    std::vector<uint64_t> bm;
+    std::vector<uint64_t, NoInitAlloc<uint64_t>> bm;   // every word is written by the packer
     std::vector<uint16_t> lst;
     std::vector<ChunkRowFacts> facts;
     uint32_t max_cid = 0;
@@ -71,6 +94,9 @@ struct ChunkPack {
     uint64_t rows() const { return row_off.size() - 1; }
     void add_chunk(uint32_t id, const STORM_bitmap_t& b);
     void add_row(const STORM_bitmap_cont_t* c);   // c may be NULL (empty row)
+    // n rows at once, filled by several host threads; the result is the
+    // same as n calls of add_row.
+    void add_rows(const STORM_bitmap_cont_t* rows, uint64_t n);
     void end_row() { row_off.push_back(cid.size()); }
 };
 

@@ -108,7 +108,7 @@ static void ensure_packed(const STORM_t* s, StormDev* d) {
     const uint64_t shape = row_shape(s);
     if (d->valid && d->shape == shape) return;
     ChunkPack p;
-    for (uint32_t r = 0; r < s->n_conts; ++r) p.add_row(&s->conts[r]);
+    p.add_rows(s->conts, s->n_conts);
     d->dev.upload(p, stream_of(d));
     d->valid = true;
     d->shape = shape;
@@ -496,8 +496,8 @@ uint64_t STORM_intersect_cardinality_square(const STORM_t* STORM_RESTRICT s1, co
     uint64_t r = 0;
     guard([&]() -> int {
         AdHoc h;
-        for (uint32_t i = 0; i < s1->n_conts; ++i) h.pack.add_row(&s1->conts[i]);
-        for (uint32_t i = 0; i < s2->n_conts; ++i) h.pack.add_row(&s2->conts[i]);
+        h.pack.add_rows(s1->conts, s1->n_conts);
+        h.pack.add_rows(s2->conts, s2->n_conts);
         r = h.rect(s1->n_conts, s2->n_conts);
         return 0;
     });
