@@ -212,12 +212,28 @@ int STORM_bitmap_add(STORM_bitmap_t* b, const uint32_t* values, const uint32_t n
     if (n_values == 0) return -3;
     if (!ensure_data(b)) return STORM_B200_ENOMEM;
     const uint64_t base = (uint64_t)b->id * STORM_DEFAULT_BLOCK_SIZE;
+    // Bits of one word are gathered in a register while consecutive values
+    // stay in that word (sorted input: up to 64 per store), and the word's
+    // newly set bits are counted when it is written back -- the same bits
+    // and the same n_bits_set as setting them one value at a time.
+    uint32_t cur = ~0u;
+    uint64_t acc = 0;
     for (uint32_t i = 0; i < n_values; ++i) {
         if (values[i] < base || values[i] - base >= STORM_DEFAULT_BLOCK_SIZE) continue;
         const uint32_t v = (uint32_t)(values[i] - base);
-        const uint64_t bit = 1ull << (v & 63);
-        b->n_bits_set += (b->data[v >> 6] & bit) == 0;
-        b->data[v >> 6] |= bit;
+        if ((v >> 6) != cur) {
+            if (cur != ~0u) {
+                b->n_bits_set += (uint32_t)__builtin_popcountll(acc & ~b->data[cur]);
+                b->data[cur] |= acc;
+            }
+            cur = v >> 6;
+            acc = 0;
+        }
+        acc |= 1ull << (v & 63);
+    }
+    if (cur != ~0u) {
+        b->n_bits_set += (uint32_t)__builtin_popcountll(acc & ~b->data[cur]);
+        b->data[cur] |= acc;
     }
     return (int)n_values;
 }
