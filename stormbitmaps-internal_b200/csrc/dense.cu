@@ -41,7 +41,7 @@ static uint32_t ts_schedule(uint32_t n_tiles, int sms, uint32_t w_pad, uint32_t&
 
 constexpr uint64_t DB_AUTO_MAX_BITS = 1ull << 17;
 
-static void build_tiles(std::vector<uint2>& t, uint64_t n, int kind) {
+void build_tiles(std::vector<uint2>& t, uint64_t n, int kind) {
     t.clear();
     // tile indices and counts are 32-bit (the kernels' work lists); bound the
     // count by the full block grid before building anything
@@ -192,7 +192,7 @@ uint64_t DenseEngine::run(const uint64_t* dX, uint64_t n, uint32_t w_pad, uint64
 // both ends -- the first panel reads only the last rows, the last panel's
 // rows are the only copy still running when the tiles end -- to about 1/24
 // of the tiles. Small lists run as one launch.
-static std::vector<std::pair<uint32_t, uint32_t>> host_panels(uint32_t n_tiles, uint32_t wave) {
+std::vector<std::pair<uint32_t, uint32_t>> host_panels(uint32_t n_tiles, uint32_t wave) {
     std::vector<std::pair<uint32_t, uint32_t>> p;
     if (n_tiles <= 4ull * wave) {
         p.emplace_back(0u, n_tiles);

@@ -2,6 +2,7 @@
 // STORM_contiguous_t, the STORM_wrapper_* calls and the dense tiles of the
 // chunked engine.
 #pragma once
+#include <utility>
 #include <vector>
 #include "common.cuh"
 
@@ -71,6 +72,14 @@ inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
 
 // Tiles (bi, bj) of 128 x 256 pairs covering the triangle of n rows.
 void build_mma_tiles(std::vector<uint2>& t, uint64_t n);
+// The tile list of a bitmap x bitmap kernel (STORM_B200_KERNEL_*): 128 x 256
+// (tcgen05), 128 x 192 (double-buffered tcgen05) or 128 x 128 (POPC) tiles
+// covering every pair i <= j < n once, ordered by A block.
+void build_tiles(std::vector<uint2>& t, uint64_t n, int kind);
+// Panels of the host-output forms over a tile list of n_tiles, in processing
+// order (the end of the list first), each a whole number of waves but the
+// last.
+std::vector<std::pair<uint32_t, uint32_t>> host_panels(uint32_t n_tiles, uint32_t wave);
 // Longest row the tensor-core kernels count exactly (4-byte weight cycle).
 constexpr uint64_t TC_MAX_ROW_BITS = 1ull << 27;
 // ... and the shared-memory form (8-byte weight cycle only).
