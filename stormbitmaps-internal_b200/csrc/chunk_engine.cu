@@ -6,6 +6,7 @@
 #include <thread>
 #include "chunk_engine.cuh"
 #include "dense.cuh"
+#include "list16_ref.cuh"
 
 namespace sb200 {
 
@@ -25,7 +26,7 @@ void ChunkPack::add_chunk(uint32_t id, const STORM_bitmap_t& b) {
         coff.push_back(lst.size());
         uint32_t flags = ns & CK_LEN;
         for (uint32_t e = 1; e < ns; ++e)
-            if (b.scalar[e] == b.scalar[e - 1]) { flags |= CK_DUP; break; }
+            if (b.scalar[e] <= b.scalar[e - 1]) { flags |= CK_DUP; break; }
         ckl.push_back(flags);
         lst.insert(lst.end(), b.scalar, b.scalar + ns);
     }
@@ -133,7 +134,7 @@ void ChunkPack::add_rows(const STORM_bitmap_cont_t* rows, uint64_t n) {
                     coff[c] = lb + pos;
                     uint32_t flags = ns & CK_LEN;
                     for (uint32_t e = 1; e < ns; ++e)
-                        if (b.scalar[e] == b.scalar[e - 1]) {
+                        if (b.scalar[e] <= b.scalar[e - 1]) {
                             flags |= CK_DUP;
                             break;
                         }
@@ -241,17 +242,23 @@ __device__ __forceinline__ uint32_t chunk_cell_lane(const ChunkView& v, uint64_t
             const uint32_t x = l[e];
             cnt += (uint32_t)(w[x >> 6] >> (x & 63)) & 1u;
         }
+    } else if ((ka | kb) & CK_DUP) {
+        // A list with a repeated or out-of-order entry: the reference's
+        // blocked SSE4.2 count, which then differs from the set size, on
+        // one lane (ca is row i's chunk: the reference's first list).
+        if (lane == 0)
+            cnt = (uint32_t)list16_blocked_count(v.lst + v.coff[ca], v.lst + v.coff[cb], ka & CK_LEN, kb & CK_LEN);
     } else {
+        // Strictly increasing lists: each entry of the shorter one is
+        // searched in the longer one.
         const uint32_t la = ka & CK_LEN, lb = kb & CK_LEN;
         const bool a_short = la <= lb;
         const uint16_t* s = v.lst + v.coff[a_short ? ca : cb];
         const uint16_t* g = v.lst + v.coff[a_short ? cb : ca];
         const uint32_t ns = a_short ? la : lb, ng = a_short ? lb : la;
-        const bool sdup = ((a_short ? ka : kb) & CK_DUP) != 0;
         for (uint32_t e = lane; e < ns; e += 32) {
             const uint16_t x = s[e];
-            const uint32_t r = sdup ? e - lower_bound_dev<uint16_t>(s, e, x) : 0;
-            const uint32_t p = lower_bound_dev<uint16_t>(g, ng, x) + r;
+            const uint32_t p = lower_bound_dev<uint16_t>(g, ng, x);
             cnt += (p < ng && g[p] == x) ? 1u : 0u;
         }
     }

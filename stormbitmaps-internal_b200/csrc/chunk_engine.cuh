@@ -5,8 +5,10 @@
 // HBM layout (CSR over rows, structure of arrays over chunks):
 //   row_off[r] .. row_off[r+1]   the row's chunks, ascending chunk id
 //   cid[c]                       chunk id (value >> 16)
-//   ckl[c]                       bit 31: bitmap chunk; bit 30: list holds a
-//                                repeated value; bits 0..29: words or entries
+//   ckl[c]                       bit 31: bitmap chunk; bit 30: list is not
+//                                strictly increasing (a repeated or
+//                                out-of-order entry); bits 0..29: words or
+//                                entries
 //   coff[c]                      offset into bm (words) or lst (entries)
 //   bm                           1024-word bitmaps, 16-byte aligned
 //   lst                          u16 offsets within the chunk, ascending
@@ -19,9 +21,10 @@
 // exactly as STORM_bitmap_intersect_cardinality_func does (storm.cpp:652-690):
 //   B x B  1024-word AND + POPC, 32 words per lane;
 //   B x S  probe: lanes stride over the list, one bit test each;
-//   S x S  lanes stride over the shorter list and binary-search the longer,
-//          matching the k-th copy of a value with the k-th copy (the scalar
-//          merge's count, storm.cpp:72-86).
+//   S x S  strictly increasing lists: lanes stride over the shorter list
+//          and binary-search the longer; otherwise one lane restates the
+//          reference's blocked SSE4.2 count (list16_ref.cuh), which a repeat
+//          or an out-of-order entry makes differ from the set size.
 #pragma once
 #include <memory>
 #include <utility>
