@@ -16,7 +16,10 @@
  *     (rebuild both sides from positions, count common bits) -- restated as a
  *     two-pointer merge over the sorted distinct lists.
  *   - the STORM_t chunk split (storm.cpp:737-803): chunk = value / 65536,
- *     list chunk when fewer than 4096 values, bitmap chunk otherwise.
+ *     list chunk when fewer than 4096 values, bitmap chunk otherwise; and
+ *     STORM_t counted chunk by chunk as the reference counts it, which
+ *     differs from the set intersection for rows with repeated or
+ *     out-of-order list entries (oracle_storm_matrix).
  *   - representation builders of kernels/storm_repr.cpp: maximal runs
  *     (:118-128), EWAH-64 (:78-100, marker layout storm_repr.h:28-31),
  *     rank9 (:25-45), zone map (:47-59), complement (:139-154) and RowMeta
@@ -108,6 +111,192 @@ uint64_t oracle_sets_square(const uint32_t* xv, const uint64_t* xo, uint64_t nx,
     for (uint64_t i = 0; i < nx; ++i)
         for (uint64_t j = 0; j < ny; ++j)
             sum += oracle_list_intersect(xv + xo[i], xo[i + 1] - xo[i], yv + yo[j], yo[j + 1] - yo[j]);
+    return sum;
+}
+
+/* ---- STORM_t counted chunk by chunk, as the reference counts it ----------
+ * For rows handed to STORM_add as given (sorted, repeats allowed; values out
+ * of order only inside one chunk), the count STORM_pairw_intersect_cardinality
+ * and STORM_bitmap_cont_intersect_cardinality produce, which for rows with
+ * repeated or out-of-order list entries is not the set intersection:
+ *   - each row is cut into chunks as STORM_bitmap_cont_add does
+ *     (storm.cpp:737-803): a run of consecutive values with one chunk id
+ *     (value / 65536) is a u16 list (entries as given) when it has fewer
+ *     than 4096 values, else a 1024-word bitmap;
+ *   - the chunk ids of two rows are matched by the two-pointer loop of
+ *     STORM_intersect_vector32_unsafe (storm.cpp:90-121);
+ *   - each matched pair is counted by STORM_bitmap_intersect_cardinality_func
+ *     (storm.cpp:652-690): list x list by the SSE4.2 build of
+ *     STORM_intersect_vector16_cardinality (storm.cpp:15-88, restated in
+ *     oracle_list16_blocked), bitmap x list one bit test per list entry,
+ *     bitmap x bitmap AND + popcount over 1024 words. */
+
+/* Entries of an 8-entry block before its first 0 (8 if none): the implicit
+ * string length of the reference's _mm_cmpistrm compare. */
+static uint32_t o_block_len(const uint16_t* b) {
+    uint32_t n = 0;
+    while (n < 8 && b[n] != 0) ++n;
+    return n;
+}
+
+/* Entries i < la of a equal to some entry k < lb of b (the "equal any" mask
+ * of the reference's _mm_cmpestrm / _mm_cmpistrm, popcounted). */
+static uint32_t o_block_any(const uint16_t* a, uint32_t la, const uint16_t* b, uint32_t lb) {
+    uint32_t c = 0;
+    for (uint32_t i = 0; i < la; ++i) {
+        uint32_t hit = 0;
+        for (uint32_t k = 0; k < lb; ++k) hit |= a[i] == b[k];
+        c += hit;
+    }
+    return c;
+}
+
+/* storm.cpp:15-88 (SSE4.2 build): blocks of 8 while both lists have a whole
+ * block left -- full-length compares while either block starts with 0, then
+ * compares ending each block at its first 0; the block with the smaller last
+ * entry advances (both on a tie) -- then the scalar merge of the rest. */
+uint64_t oracle_list16_blocked(const uint16_t* v1, const uint16_t* v2, uint32_t len1, uint32_t len2) {
+    uint64_t count = 0;
+    uint32_t ia = 0, ib = 0;
+    const uint32_t sta = len1 / 8 * 8, stb = len2 / 8 * 8;
+    if (ia < sta && ib < stb) {
+        int done = 0;
+        while (v1[ia] == 0 || v2[ib] == 0) {
+            count += o_block_any(v1 + ia, 8, v2 + ib, 8);
+            const uint16_t am = v1[ia + 7], bm = v2[ib + 7];
+            if (am <= bm) { ia += 8; if (ia == sta) { done = 1; break; } }
+            if (bm <= am) { ib += 8; if (ib == stb) { done = 1; break; } }
+        }
+        if (!done && ia < sta && ib < stb)
+            for (;;) {
+                count += o_block_any(v1 + ia, o_block_len(v1 + ia), v2 + ib, o_block_len(v2 + ib));
+                const uint16_t am = v1[ia + 7], bm = v2[ib + 7];
+                if (am <= bm) { ia += 8; if (ia == sta) break; }
+                if (bm <= am) { ib += 8; if (ib == stb) break; }
+            }
+    }
+    while (ia < len1 && ib < len2) {
+        if (v1[ia] < v2[ib]) ++ia;
+        else if (v2[ib] < v1[ia]) ++ib;
+        else { ++count; ++ia; ++ib; }
+    }
+    return count;
+}
+
+typedef struct {
+    uint32_t id, bitmap, len;   /* len: list entries (bitmap chunks: 0) */
+    uint64_t off;               /* into the list pool (u16) or the bitmap pool (words) */
+} o_chunk;
+
+typedef struct {
+    o_chunk* ch;
+    uint64_t* row;              /* row r: chunks [row[r], row[r+1]) */
+    uint16_t* lst;
+    uint64_t* bm;
+} o_rows;
+
+static void o_rows_build(const uint32_t* values, const uint64_t* offsets, uint64_t n, o_rows* R) {
+    uint64_t nch = 0, nl = 0, nb = 0;
+    for (uint64_t r = 0; r < n; ++r)
+        for (uint64_t s = offsets[r]; s < offsets[r + 1];) {
+            const uint32_t id = values[s] / 65536u;
+            uint64_t e = s;
+            while (e < offsets[r + 1] && values[e] / 65536u == id) ++e;
+            ++nch;
+            if (e - s < 4096) nl += e - s; else ++nb;
+            s = e;
+        }
+    R->ch = (o_chunk*)malloc(sizeof(o_chunk) * (nch ? nch : 1));
+    R->row = (uint64_t*)malloc(sizeof(uint64_t) * (n + 1));
+    R->lst = (uint16_t*)malloc(sizeof(uint16_t) * (nl ? nl : 1));
+    R->bm = (uint64_t*)calloc((nb ? nb : 1) * 1024, sizeof(uint64_t));
+    uint64_t c = 0, l = 0, b = 0;
+    for (uint64_t r = 0; r < n; ++r) {
+        R->row[r] = c;
+        for (uint64_t s = offsets[r]; s < offsets[r + 1];) {
+            const uint32_t id = values[s] / 65536u;
+            uint64_t e = s;
+            while (e < offsets[r + 1] && values[e] / 65536u == id) ++e;
+            o_chunk* k = &R->ch[c++];
+            k->id = id;
+            if (e - s < 4096) {
+                k->bitmap = 0;
+                k->len = (uint32_t)(e - s);
+                k->off = l;
+                for (uint64_t q = s; q < e; ++q) R->lst[l++] = (uint16_t)(values[q] - id * 65536u);
+            } else {
+                k->bitmap = 1;
+                k->len = 0;
+                k->off = b * 1024;
+                for (uint64_t q = s; q < e; ++q) {
+                    const uint32_t x = values[q] - id * 65536u;
+                    R->bm[b * 1024 + (x >> 6)] |= 1ull << (x & 63);
+                }
+                ++b;
+            }
+            s = e;
+        }
+    }
+    R->row[n] = c;
+}
+
+static void o_rows_free(o_rows* R) {
+    free(R->ch);
+    free(R->row);
+    free(R->lst);
+    free(R->bm);
+}
+
+static uint64_t o_chunk_pair(const o_rows* R, const o_chunk* a, const o_chunk* b) {
+    if (!a->bitmap && !b->bitmap) return oracle_list16_blocked(R->lst + a->off, R->lst + b->off, a->len, b->len);
+    if (a->bitmap && b->bitmap) return oracle_and_popcount(R->bm + a->off, R->bm + b->off, 1024);
+    const o_chunk* bmc = a->bitmap ? a : b;
+    const o_chunk* lc = a->bitmap ? b : a;
+    uint64_t c = 0;
+    for (uint32_t e = 0; e < lc->len; ++e) {
+        const uint32_t x = R->lst[lc->off + e];
+        c += (R->bm[bmc->off + (x >> 6)] >> (x & 63)) & 1u;
+    }
+    return c;
+}
+
+/* Two rows: STORM_intersect_vector32_unsafe's chunk-id loop (storm.cpp:90-121),
+ * then the matched chunk pairs (storm.cpp:835-860). */
+static uint64_t o_row_pair(const o_rows* R, uint64_t i, uint64_t j) {
+    const o_chunk* a = R->ch + R->row[i];
+    const o_chunk* b = R->ch + R->row[j];
+    const uint64_t la = R->row[i + 1] - R->row[i], lb = R->row[j + 1] - R->row[j];
+    if (la == 0 || lb == 0) return 0;
+    uint64_t A = 0, B = 0, c = 0;
+    for (;;) {
+        while (a[A].id < b[B].id)
+            if (++A == la) return c;
+        while (a[A].id > b[B].id)
+            if (++B == lb) return c;
+        if (a[A].id == b[B].id) {
+            c += o_chunk_pair(R, &a[A], &b[B]);
+            if (++A == la || ++B == lb) return c;
+        } else if (++A == la) {
+            return c;
+        }
+    }
+}
+
+/* Per-pair counts (packed upper triangle incl. the diagonal, the same
+ * convention as oracle_contig_matrix) and the sum over i < j. */
+uint64_t oracle_storm_matrix(const uint32_t* values, const uint64_t* offsets, uint64_t n, uint32_t* out) {
+    o_rows R;
+    o_rows_build(values, offsets, n, &R);
+    uint64_t sum = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        const uint64_t base = i * n - (i * (i - 1)) / 2 - i;
+        for (uint64_t j = i; j < n; ++j) {
+            const uint64_t c = o_row_pair(&R, i, j);
+            if (out) out[base + j] = (uint32_t)c;
+            if (j > i) sum += c;
+        }
+    }
+    o_rows_free(&R);
     return sum;
 }
 

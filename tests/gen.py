@@ -130,3 +130,25 @@ def bernoulli_sets(n: int, universe: int, density: float, seed: int):
     g = rng(seed)
     cards = g.binomial(universe, density, size=n)
     return [uniform_set(g, int(c), universe) for c in cards]
+
+
+def repeat_corpus(seed: int):
+    """Rows whose list chunks repeat values (STORM_add keeps repeats), rows
+    whose single chunk is given out of order, plain rows and bitmap-chunk
+    rows beside them."""
+    g = rng(seed)
+    sets = []
+    for k in range(50):
+        kind = k % 4 if k < 46 else 4
+        if kind == 0:      # sorted with many repeats, spread over three chunks
+            v = np.sort(g.integers(0, 3 << 16, int(g.integers(100, 3000))))
+        elif kind == 1:    # plain: sorted distinct
+            v = uniform_set(g, int(g.integers(50, 3000)), 3 << 16)
+        elif kind == 2:    # one chunk, distinct values out of order
+            v = g.permutation(uniform_set(g, int(g.integers(20, 900)), 1 << 16))
+        elif kind == 3:    # every value twice, sorted
+            v = np.sort(np.repeat(uniform_set(g, int(g.integers(20, 900)), 3 << 16), 2))
+        else:              # bitmap chunks (>= 4096 values) that the lists above probe
+            v = uniform_set(g, int(g.integers(13000, 30000)), 3 << 16)
+        sets.append(np.asarray(v, dtype=np.uint32))
+    return sets

@@ -39,6 +39,8 @@ def oracle():
         "oracle_sets_matrix": (C.c_uint64, [u32p, u64p, C.c_uint64, C.c_uint64, C.c_uint64, u32p]),
         "oracle_sets_square": (C.c_uint64, [u32p, u64p, C.c_uint64, u32p, u64p, C.c_uint64]),
         "oracle_chunk_split": (C.c_uint64, [u32p, C.c_uint64, u32p, u8p, u32p]),
+        "oracle_storm_matrix": (C.c_uint64, [u32p, u64p, C.c_uint64, u32p]),
+        "oracle_list16_blocked": (C.c_uint64, [u16p, u16p, C.c_uint32, C.c_uint32]),
         "oracle_runs": (C.c_uint64, [u32p, C.c_uint64, u32p, u32p]),
         "oracle_ewah": (C.c_uint64, [u64p, C.c_uint64, u64p]),
         "oracle_ewah_decode": (None, [u64p, C.c_uint64, u64p]),
@@ -106,6 +108,17 @@ def sets_matrix(vals: np.ndarray, offs: np.ndarray):
     n = len(offs) - 1
     out = np.zeros(max(1, n * (n + 1) // 2), dtype=np.uint32)
     s = oracle().oracle_sets_matrix(_p(vals, u32p), _p(offs, u64p), n, 0, n, _p(out, u32p))
+    return out[: n * (n + 1) // 2], int(s)
+
+
+def storm_matrix(vals: np.ndarray, offs: np.ndarray):
+    """STORM_t counts chunk by chunk as the reference counts them (rows as
+    handed to STORM_add): packed triangle incl. the diagonal, sum over i < j."""
+    vals = np.ascontiguousarray(vals, dtype=np.uint32)
+    offs = np.ascontiguousarray(offs, dtype=np.uint64)
+    n = len(offs) - 1
+    out = np.zeros(max(1, n * (n + 1) // 2), dtype=np.uint32)
+    s = oracle().oracle_storm_matrix(_p(vals, u32p), _p(offs, u64p), n, _p(out, u32p))
     return out[: n * (n + 1) // 2], int(s)
 
 

@@ -38,6 +38,47 @@ def test_oracle_sets_match_reference(golden):
         np.testing.assert_array_equal(mat[strict], golden[f"storm/{name}/matrix"][strict], err_msg=name)
 
 
+def test_oracle_chunk_by_chunk_matches_reference(golden):
+    """oracle_storm_matrix (STORM_t counted chunk by chunk, as the reference
+    counts it) equals the golden matrices and sums, and -- on rows with
+    repeated and out-of-order list entries, where that count is not the set
+    size -- the reference's own STORM_t (oracle/_ref) when it is built; its
+    list x list count equals the reference's STORM_intersect_vector16_
+    cardinality on seeded lists."""
+    import ctypes as C
+    for name in storm_cases(golden):
+        vals, offs = golden[f"storm/{name}/vals"], golden[f"storm/{name}/offs"]
+        mat, s = ol.storm_matrix(vals, offs)
+        assert s == int(golden[f"storm/{name}/sum"][0]), name
+        n = len(offs) - 1
+        iu = np.triu_indices(n)
+        strict = iu[0] != iu[1]
+        np.testing.assert_array_equal(mat[strict], golden[f"storm/{name}/matrix"][strict], err_msg=name)
+    R = ol.reference()
+    if R is None:
+        pytest.skip("reference library not built (oracle/_ref)")
+    u16p, u32p, u64p = C.POINTER(C.c_uint16), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)
+    for seed in range(941, 947):
+        sets = gen.repeat_corpus(seed)
+        vals, offs = gen.to_csr(sets)
+        n = len(sets)
+        mat, s = ol.storm_matrix(vals, offs)
+        ref = np.zeros(n * (n + 1) // 2, dtype=np.uint32)
+        assert R.ref_storm_matrix(vals.ctypes.data_as(u32p), offs.ctypes.data_as(u64p), n,
+                                  ref.ctypes.data_as(u32p)) == s, seed
+        np.testing.assert_array_equal(mat, ref, err_msg=str(seed))
+        assert ol.sets_matrix(vals, offs)[1] != s     # the corpus reaches the non-set counts
+    g = gen.rng(948)
+    for _ in range(3000):
+        a = np.sort(g.integers(0, int(g.integers(2, 400)), int(g.integers(1, 80)))).astype(np.uint16)
+        b = g.integers(0, 400, int(g.integers(1, 80))).astype(np.uint16)
+        if g.random() < 0.5:
+            b = np.sort(b)
+        want = R.ref_vector16(a.ctypes.data_as(u16p), b.ctypes.data_as(u16p), a.size, b.size)
+        got = ol.oracle().oracle_list16_blocked(a.ctypes.data_as(u16p), b.ctypes.data_as(u16p), a.size, b.size)
+        assert got == want, (a, b)
+
+
 def test_oracle_chunk_split_matches_reference_layout(golden):
     O = ol.oracle()
     for name in storm_cases(golden):

@@ -441,60 +441,41 @@ def test_row_changed_through_public_struct_is_repacked(sb):
         R.STORM_free(hr)
 
 
-def _repeat_corpus(seed):
-    """Rows whose list chunks repeat values (STORM_add keeps repeats), rows
-    whose single chunk is given out of order, plain rows and bitmap-chunk
-    rows beside them."""
-    g = gen.rng(seed)
-    sets = []
-    for k in range(50):
-        kind = k % 4 if k < 46 else 4
-        if kind == 0:      # sorted with many repeats, spread over three chunks
-            v = np.sort(g.integers(0, 3 << 16, int(g.integers(100, 3000))))
-        elif kind == 1:    # plain: sorted distinct
-            v = gen.uniform_set(g, int(g.integers(50, 3000)), 3 << 16)
-        elif kind == 2:    # one chunk, distinct values out of order
-            v = g.permutation(gen.uniform_set(g, int(g.integers(20, 900)), 1 << 16))
-        elif kind == 3:    # every value twice, sorted
-            v = np.sort(np.repeat(gen.uniform_set(g, int(g.integers(20, 900)), 3 << 16), 2))
-        else:              # bitmap chunks (>= 4096 values) that the lists above probe
-            v = gen.uniform_set(g, int(g.integers(13000, 30000)), 3 << 16)
-        sets.append(np.asarray(v, dtype=np.uint32))
-    return sets
-
-
 def test_repeated_and_unordered_list_values_match_reference(sb):
     """List chunks that are not strictly increasing are counted as the
     reference counts them (its SSE4.2 list x list kernel, storm.cpp:15-88,
     whose answer then differs from the set size): per-pair counts and the sum
-    against the reference's own STORM_t built from the same rows
-    (oracle/_ref); skipped when it is not built. The single-pair
-    STORM_intersect_vector16_cardinality is checked on the same lists."""
+    against the oracle's chunk-by-chunk restatement (itself checked against
+    the reference's own STORM_t, oracle/_ref, when that is built). The
+    single-pair STORM_intersect_vector16_cardinality is checked on the same
+    lists."""
     import ctypes as C
-    R = ol.reference()
-    if R is None:
-        pytest.skip("reference library not built (oracle/_ref)")
-    sets = _repeat_corpus(941)
-    n = len(sets)
-    vals, offs = gen.to_csr(sets)
-    want = np.zeros(n * (n + 1) // 2, dtype=np.uint32)
-    u32p, u64p = C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)
-    ws = R.ref_storm_matrix(vals.ctypes.data_as(u32p), offs.ctypes.data_as(u64p), n, want.ctypes.data_as(u32p))
-    # the corpus does reach the cases where the reference's count is not the set size
-    _, set_sum = ol.sets_matrix(vals, offs)
-    assert set_sum != ws
-    s = build_storm(sb, sets)
-    assert s.pairw_intersect_cardinality() == ws
-    mat, ssum = s.matrix()
-    assert ssum == ws
-    iu = np.triu_indices(n)
-    strict = iu[0] != iu[1]
-    np.testing.assert_array_equal(mat[strict], want[strict])
-    # single pair, lists as given (the reference's first argument is v1)
-    for a, b in ((0, 2), (2, 0), (3, 7), (4, 8), (6, 10), (11, 3)):
-        la = (sets[a][sets[a] < 65536]).astype(np.uint16)
-        lb = (sets[b][sets[b] < 65536]).astype(np.uint16)
-        if la.size and lb.size:
-            assert sb.intersect_vector16(la, lb) == R.ref_vector16(la.ctypes.data_as(C.POINTER(C.c_uint16)),
-                                                                   lb.ctypes.data_as(C.POINTER(C.c_uint16)),
-                                                                   la.size, lb.size), (a, b)
+    for seed in (941, 942):
+        sets = gen.repeat_corpus(seed)
+        n = len(sets)
+        vals, offs = gen.to_csr(sets)
+        want, ws = ol.storm_matrix(vals, offs)
+        # the corpus does reach the cases where the reference's count is not the set size
+        assert ol.sets_matrix(vals, offs)[1] != ws
+        R = ol.reference()
+        if R is not None:   # the oracle is pinned to the reference here too
+            ref = np.zeros(n * (n + 1) // 2, dtype=np.uint32)
+            u32p, u64p = C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)
+            assert R.ref_storm_matrix(vals.ctypes.data_as(u32p), offs.ctypes.data_as(u64p), n,
+                                      ref.ctypes.data_as(u32p)) == ws
+            np.testing.assert_array_equal(ref, want)
+        s = build_storm(sb, sets)
+        assert s.pairw_intersect_cardinality() == ws
+        mat, ssum = s.matrix()
+        assert ssum == ws
+        iu = np.triu_indices(n)
+        strict = iu[0] != iu[1]
+        np.testing.assert_array_equal(mat[strict], want[strict], err_msg=str(seed))
+        # single pair, lists as given (the reference's first argument is v1)
+        for a, b in ((0, 2), (2, 0), (3, 7), (4, 8), (6, 10), (11, 3)):
+            la = np.ascontiguousarray(sets[a][sets[a] < 65536], dtype=np.uint16)
+            lb = np.ascontiguousarray(sets[b][sets[b] < 65536], dtype=np.uint16)
+            if la.size and lb.size:
+                want1 = ol.oracle().oracle_list16_blocked(la.ctypes.data_as(C.POINTER(C.c_uint16)),
+                                                          lb.ctypes.data_as(C.POINTER(C.c_uint16)), la.size, lb.size)
+                assert sb.intersect_vector16(la, lb) == want1, (seed, a, b)
