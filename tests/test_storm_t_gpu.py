@@ -191,6 +191,14 @@ def test_tensor_dense_block_rows_with_repeats_stay_on_chunks(sb):
     mat0, s0 = s.matrix()
     assert s0 == ssum
     np.testing.assert_array_equal(mat, mat0)
+    # and both are the reference's chunk-by-chunk counts (repeats included)
+    added = [np.sort(np.concatenate([v, v[:7]])) if k in dup_rows else v for k, v in enumerate(sets)]
+    vals, offs = gen.to_csr(added)
+    want, ws = ol.storm_matrix(vals, offs)
+    assert ssum == ws
+    iu = np.triu_indices(len(added))
+    strict = iu[0] != iu[1]
+    np.testing.assert_array_equal(mat[strict], want[strict])
 
 
 def test_tensor_dense_block_long_universe(sb):
@@ -255,6 +263,13 @@ def test_postings_with_dense_block_and_chunk_rows(sb):
     s.set_dense_block(1.0 / 16384)
     s.set_sparse_postings(1)
     assert s.pairw_intersect_cardinality() == s0
+    # the reference's chunk-by-chunk counts (the repeated-value rows included)
+    vals, offs = gen.to_csr(sets)
+    want, ws = ol.storm_matrix(vals, offs)
+    assert s0 == ws
+    iu = np.triu_indices(len(sets))
+    strict = iu[0] != iu[1]
+    np.testing.assert_array_equal(mat[strict], want[strict])
 
 
 def test_tensor_rows_with_postings_in_panels(sb):
