@@ -157,14 +157,17 @@ int STORM_contig_last_kernel(const STORM_contiguous_t* c);
  *   d_out   n_rows*(n_rows+1)/2 u32, packed upper triangle (may be NULL for
  *           the sum only).
  * Runs the tensor-core kernel (row_bits <= 2^23) on `stream` (a
- * cudaStream_t; NULL = the default stream) and waits for it.  Its scratch
+ * cudaStream_t; NULL = the default stream) and waits for that stream before
+ * returning, so the counts and the sum are complete on return.  Its scratch
  * (status/sum words and a tile list of at most 32768 tiles of 128 x 256
- * pairs, about 23,000 rows) is a 256 KiB array in the library that every GPU
- * holding the library keeps until exit; larger problems return
+ * pairs: n_rows up to 46080) is a 256 KiB array in the library that every
+ * GPU holding the library keeps until exit; larger problems return
  * STORM_B200_ELIMIT.  The first call on a device looks that array up (and
  * opts the kernel into its shared memory), so make the first call before any
- * stream capture.  All calls share the one array: calls that overlap on the
- * GPU race and must not be issued. */
+ * stream capture.  A CUDA error still pending from earlier work on the
+ * thread is returned as STORM_B200_ECUDA before anything is launched.  All
+ * calls share the one array: calls that overlap on the GPU race and must not
+ * be issued. */
 int STORM_contig_pairw_intersect_matrix_noalloc(const uint64_t* d_rows, uint64_t n_rows,
                                                 uint32_t row_pitch_words, uint64_t row_bits,
                                                 uint32_t* d_out, uint64_t out_len, uint64_t* sum,

@@ -56,22 +56,34 @@ uint64_t ref_contig_sum(const uint64_t* words, uint64_t n, uint64_t nw, uint64_t
 
 /* Per-pair counts with the reference's bitmap kernel, rows [r0, r1) of the
  * packed upper triangle, split over `threads` host threads.  Returns the sum
- * over i < j of the processed rows. */
+ * over i < j of the processed rows.  The traversal is the reference's cache
+ * blocking (STORM_contig_pairw_intersect_cardinality_blocked,
+ * storm.cpp:1248-1281): a thread takes a block of REF_BLOCK rows i and walks
+ * every row j >= the block's first row once, pairing it with each row of the
+ * block, so the block's rows stay in cache and each j row is read once per
+ * block instead of once per row. */
+static const uint64_t REF_BLOCK = 16;
+
 uint64_t ref_contig_matrix_mt(const uint64_t* words, uint64_t n, uint64_t nw, uint64_t r0,
                               uint64_t r1, uint32_t* out, uint32_t threads) {
     const STORM_compute_func f = STORM_get_intersect_count_func(nw);
     if (threads == 0) threads = 1;
+    if (r1 > n) r1 = n;
     std::atomic<uint64_t> next(r0), total(0);
     auto work = [&]() {
         uint64_t local = 0;
         for (;;) {
-            const uint64_t i = next.fetch_add(1);
-            if (i >= r1 || i >= n) break;
-            const uint64_t base = i * n - (i * (i - 1)) / 2 - i;
-            for (uint64_t j = i; j < n; ++j) {
-                const uint64_t c = (*f)(words + i * nw, words + j * nw, nw);
-                if (out) out[base + j] = (uint32_t)c;
-                if (j > i) local += c;
+            const uint64_t i0 = next.fetch_add(REF_BLOCK);
+            if (i0 >= r1) break;
+            const uint64_t i1 = std::min(r1, i0 + REF_BLOCK);
+            for (uint64_t j = i0; j < n; ++j) {
+                const uint64_t* wj = words + j * nw;
+                const uint64_t ie = std::min(i1, j + 1);   // rows i <= j of the block
+                for (uint64_t i = i0; i < ie; ++i) {
+                    const uint64_t c = (*f)(words + i * nw, wj, nw);
+                    if (out) out[i * n - (i * (i - 1)) / 2 - i + j] = (uint32_t)c;
+                    if (j > i) local += c;
+                }
             }
         }
         total.fetch_add(local);

@@ -361,7 +361,7 @@ uint64_t DenseEngine::panels_to_host(const uint64_t* dX, uint64_t n, uint32_t w_
 // ===================================================================
 namespace sb200 {
 
-constexpr uint32_t NOALLOC_MAX_TILES = 32768;   // 256 KiB of (bi, bj) pairs
+constexpr uint32_t NOALLOC_MAX_TILES = 32768;   // 256 KiB of (bi, bj) pairs: up to 46080 rows
 
 struct NoAllocScratch {
     DeviceFlags flags;
@@ -425,14 +425,23 @@ extern "C" int STORM_contig_pairw_intersect_matrix_noalloc(const uint64_t* d_row
     }
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return STORM_B200_ECUDA;
+    // A CUDA error still pending from earlier work is reported before
+    // anything is queued, so that it cannot be taken for a failed launch here.
+    if (cudaPeekAtLastError() != cudaSuccess) return STORM_B200_ECUDA;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (cudaMemsetAsync(&scratch->flags, 0, sizeof(DeviceFlags), st) != cudaSuccess) return STORM_B200_ECUDA;
     noalloc_tiles_kernel<<<(nbi + 127) / 128, 128, 0, st>>>(scratch, nbi, nbj);
     const uint32_t grid = n_tiles < (uint64_t)sms ? (uint32_t)n_tiles : (uint32_t)sms;
-    bb_mma_ts_kernel<<<grid, TS_THREADS, TS_SMEM_BYTES, st>>>(d_rows, (uint32_t)n_rows, row_pitch_words,
-                                                               scratch->tiles, (uint32_t)n_tiles, d_out,
-                                                               &scratch->flags, 1u);
-    if (cudaGetLastError() != cudaSuccess) return STORM_B200_ECUDA;
+    // The same epilogue rule as the allocating path: rows up to
+    // TS_COALESCE_MAX_BITS stage their counts through shared memory.
+    const uint32_t smem =
+        (uint64_t)row_pitch_words * 64 <= TS_COALESCE_MAX_BITS ? TS_SMEM_BYTES : TS_SMEM_BYTES_LEAN;
+    bb_mma_ts_kernel<<<grid, TS_THREADS, smem, st>>>(d_rows, (uint32_t)n_rows, row_pitch_words, scratch->tiles,
+                                                      (uint32_t)n_tiles, d_out, &scratch->flags, 1u);
+    if (cudaGetLastError() != cudaSuccess) {
+        cudaStreamSynchronize(st);   // nothing already queued may still write d_out after the return
+        return STORM_B200_ECUDA;
+    }
     DeviceFlags f;
     if (cudaMemcpyAsync(&f, &scratch->flags, sizeof(f), cudaMemcpyDeviceToHost, st) != cudaSuccess)
         return STORM_B200_ECUDA;

@@ -9,7 +9,8 @@
 //   instruction descriptor (32 bit) for kind::i8: D format in [4,6)
 //     (2 = s32), A / B format in [7,10) / [10,13) (0 = u8), A / B major in
 //     bits 15 / 16 (0 = K-major), N >> 3 in [17,23), M >> 4 in [24,29).
-// tests/test_descriptors.py checks these packings on the host.
+// tests/descriptors_check.cu (run by tests/test_descriptors_cpu.py) decodes
+// these packings field by field on the host.
 #pragma once
 #include <stdint.h>
 

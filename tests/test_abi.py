@@ -72,7 +72,7 @@ int main(void) {
 def test_public_struct_layout_matches_reference():
     ours = _layout_probe(INCLUDE)
     assert ours[:2] == ["128", "64"]   # 64-byte aligned members: scalar at 64, struct 128 bytes
-    ref = "/root/reference"
+    ref = os.environ.get("STORM_REFERENCE", "/root/reference")
     if os.path.exists(os.path.join(ref, "storm.h")):
         assert _layout_probe(ref, "_ref") == ours
 

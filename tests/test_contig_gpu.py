@@ -2,6 +2,8 @@
 golden vectors: both bitmap x bitmap kernels (CUDA-core POPC and tcgen05),
 bit-exact, on the reference's own cases, edge shapes and the full-size
 dense configurations (sampled pairs + size-independent identities)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -169,10 +171,12 @@ def _cfg_rows_gpu(n, m, p, seed):
     return bench.bernoulli_rows_gpu(n, m, p, seed, torch.device("cuda"))
 
 
-def _check_full_size(sb, n, m, p, seed, kernels):
+def _check_full_size(sb, n, m, p, seed, kernels, every_pair=False):
     """Full-size dense configuration: device-resident output, checked by
-    (a) oracle on every pair of a row sample, (b) diagonal = row popcounts,
-    (c) kernel-vs-kernel identity, (d) sum identity."""
+    (a) oracle on every pair of a row sample -- or, with every_pair, the whole
+    triangle against the reference's own AND+popcount kernel on all host
+    threads (the oracle where the reference was not built), (b) diagonal = row
+    popcounts, (c) kernel-vs-kernel identity, (d) sum identity."""
     import torch
     rows = _cfg_rows_gpu(n, m, p, seed)           # int64 [n, w] on device
     host = rows.cpu().numpy().view(np.uint64)
@@ -194,6 +198,16 @@ def _check_full_size(sb, n, m, p, seed, kernels):
         base = int(sb.tri_index(n, i, i))
         got = out[base: base + (n - i)].cpu().numpy().view(np.uint32)
         np.testing.assert_array_equal(got, want, err_msg=f"row {i}")
+    if every_pair:
+        want = np.zeros(tri, np.uint32)
+        R = ol.reference()
+        if R is not None:
+            ws = R.ref_contig_matrix_mt(host.ctypes.data_as(ol.u64p), n, host.shape[1], 0, n,
+                                        want.ctypes.data_as(ol.u32p), os.cpu_count() or 1)
+        else:
+            want, ws = ol.contig_matrix(host)
+        assert ws == s
+        np.testing.assert_array_equal(out.cpu().numpy().view(np.uint32), want)
     # (b) diagonal
     ii = np.arange(n, dtype=np.uint64)
     diag_idx = torch.from_numpy(sb.tri_index(n, ii, ii).astype(np.int64)).cuda()
@@ -209,9 +223,10 @@ def _check_full_size(sb, n, m, p, seed, kernels):
     assert s == total - int(pc.sum())
 
 
-def test_config1_full_size_both_kernels(sb):
-    """4096 rows x 65536 bits, Bernoulli(0.5): every pair, both kernels."""
-    _check_full_size(sb, 4096, 65536, 0.5, 101, ["mma", "mma_db", "mma_ss", "popc"])
+def test_config1_full_size_every_pair(sb):
+    """4096 rows x 65536 bits, Bernoulli(0.5): all 8,390,656 pairs against the
+    reference's own kernel, and the four bitmap x bitmap kernels bit for bit."""
+    _check_full_size(sb, 4096, 65536, 0.5, 101, ["mma", "mma_db", "mma_ss", "popc"], every_pair=True)
 
 
 def test_config5a_haplotypes_full_size(sb):
@@ -246,9 +261,12 @@ def test_config5a_haplotypes_full_size(sb):
     assert s == total - int(pc.sum())
 
 
-def test_config2_full_size_tensor_kernel(sb):
-    """65536 rows x 262144 bits, p ~ U[0.05, 0.5] (2 GiB in, 8.6 GB out)."""
-    _check_full_size(sb, 65536, 262144, (0.05, 0.5), 202, ["mma"])
+def test_config2_full_size_tensor_and_popc_kernels(sb):
+    """65536 rows x 262144 bits, p ~ U[0.05, 0.5] (2 GiB in, 8.6 GB out): the
+    tensor-core kernel against the CUDA-core AND + POPC kernel -- an
+    independent code path -- on all 2,147,516,416 pairs, plus sampled rows
+    against the oracle, the diagonal and the sum identity."""
+    _check_full_size(sb, 65536, 262144, (0.05, 0.5), 202, ["mma", "popc"])
 
 
 def test_device_pointer_ingest_orders_after_producer(sb):

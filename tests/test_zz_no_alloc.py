@@ -21,8 +21,12 @@ def _entry(sb):
     return f
 
 
-@pytest.mark.parametrize("n,m", [(300, 4096 + 64), (1000, 65536)])
-def test_noalloc_matches_allocating_entry_point_twice(sb, n, m):
+# (rows, bits, calls): short and long rows (rows over 2^17 bits take the
+# epilogue without the shared-memory staging), and the largest row count the
+# 32768-tile list holds (46080 rows, tiles at large block-row offsets).
+@pytest.mark.parametrize("n,m,calls", [(300, 4096 + 64, 3), (1000, 65536, 3), (300, (1 << 17) + 512, 2),
+                                       (46080, 512, 2)])
+def test_noalloc_matches_allocating_entry_point_twice(sb, n, m, calls):
     import torch
     import bench
     dev = torch.device("cuda")
@@ -42,7 +46,7 @@ def test_noalloc_matches_allocating_entry_point_twice(sb, n, m):
     want_sum = c.matrix_device(want.data_ptr(), tri)
 
     f = _entry(sb)
-    outs = [torch.full((tri,), -1, dtype=torch.int32, device=dev) for _ in range(3)]
+    outs = [torch.full((tri,), -1, dtype=torch.int32, device=dev) for _ in range(calls)]
     torch.cuda.synchronize()
     sums, free = [], []
     for out in outs:
@@ -54,7 +58,7 @@ def test_noalloc_matches_allocating_entry_point_twice(sb, n, m):
         free.append(torch.cuda.mem_get_info()[0])
     # The first call on a device may load kernel code (lazy module loading);
     # the calls after it must not change free device memory at all.
-    assert free[1] == free[0] and free[2] == free[0], free
+    assert all(fr == free[0] for fr in free[1:]), free
     for out, s in zip(outs, sums):   # every call, the last two in a row included
         assert torch.equal(out, want)
         assert s == want_sum
@@ -69,5 +73,5 @@ def test_noalloc_rejects_what_it_cannot_do(sb):
     assert f(d.data_ptr(), 10, 7, 448, None, 0, C.byref(s), None) == sb.EARG       # pitch not a multiple of 8
     big = (1 << 23) + 64                                                           # rows too long to stay exact
     assert f(d.data_ptr(), 10, (big // 64 + 7) // 8 * 8, big, None, 0, C.byref(s), None) == sb.ELIMIT
-    assert f(d.data_ptr(), 60000, 8, 512, None, 0, C.byref(s), None) == sb.ELIMIT  # tile list over its maximum
+    assert f(d.data_ptr(), 46081, 8, 512, None, 0, C.byref(s), None) == sb.ELIMIT  # tile list over its maximum
     assert f(d.data_ptr(), 10, 8, 512, d.data_ptr(), 3, C.byref(s), None) == sb.ESIZE
