@@ -473,6 +473,411 @@ def bernoulli_sets_gpu(n, universe, density, seed, device):
     return out
 
 
+# ------------------------------------------- full-size STORM_t corpora
+def zipf_cards(n, s, lo, hi, seed):
+    """Row cardinalities with P(k) ~ k^-s on [lo, hi] (the same draw as
+    zipf_sets_gpu for the same seed)."""
+    g = np.random.Generator(np.random.PCG64(seed))
+    ks = np.arange(lo, hi + 1, dtype=np.float64)
+    pk = ks ** (-s)
+    pk /= pk.sum()
+    return g.choice(ks.astype(np.int64), size=n, p=pk)
+
+
+def batch_plan(sizes, max_values):
+    """Consecutive row ranges [r0, r1) holding at most max_values values
+    (a single larger row gets a range of its own)."""
+    out, r0, acc = [], 0, 0
+    for r, k in enumerate(sizes):
+        if r > r0 and acc + int(k) > max_values:
+            out.append((r0, r))
+            r0, acc = r, 0
+        acc += int(k)
+    if r0 < len(sizes):
+        out.append((r0, len(sizes)))
+    return out
+
+
+def uniform_rows_batch(cards, universe, seed, device):
+    """Rows r of one batch: cards[r] distinct positions uniform without
+    replacement over [0, universe), sorted.  Positions are drawn with
+    repeats (enough draws that the expected distinct count exceeds the
+    cardinality by several standard deviations; rows left short draw again),
+    repeats are removed, and a uniformly random subset of the wanted size is
+    kept (random priorities, the lowest per row).  Returns (values int32 on
+    the device, offsets numpy u64 from 0)."""
+    import torch
+    U = int(universe)
+    nb = len(cards)
+    k = torch.as_tensor(np.asarray(cards, np.int64), device=device)
+    if nb == 0:
+        return torch.zeros(0, dtype=torch.int32, device=device), np.zeros(1, np.uint64)
+    if float(k.max().item()) > 0.5 * U:
+        raise ValueError("uniform_rows_batch: density above 1/2")
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    kd = k.to(torch.float64)
+    dens = kd / U
+    m = torch.where(k > 0, torch.ceil(-U * torch.log1p(-dens) + 6.0 * torch.sqrt(kd) + 32.0),
+                    torch.zeros_like(kd)).to(torch.int64)
+    rid = torch.arange(nb, device=device, dtype=torch.int64)
+    key = torch.unique(torch.repeat_interleave(rid, m) * U +
+                       torch.randint(0, U, (int(m.sum().item()),), generator=g, device=device))
+    for _ in range(64):
+        cnt = torch.bincount(key // U, minlength=nb)
+        short = cnt < k
+        if not bool(short.any()):
+            break
+        extra = torch.where(short, 2 * (k - cnt) + 64, torch.zeros_like(k))
+        more = torch.repeat_interleave(rid, extra) * U + torch.randint(0, U, (int(extra.sum().item()),),
+                                                                       generator=g, device=device)
+        key = torch.unique(torch.cat([key, more]))
+    else:
+        raise RuntimeError("uniform_rows_batch: rows stayed short")
+    krow = key // U
+    pr = torch.rand(key.numel(), generator=g, device=device, dtype=torch.float64)
+    order = torch.argsort(krow.to(torch.float64) * 2.0 + pr)
+    start = torch.cumsum(cnt, 0) - cnt
+    rank = torch.arange(key.numel(), device=device) - start[krow[order]]
+    keep = order[rank < k[krow[order]]]
+    key = torch.sort(key[keep]).values
+    vals = (key % U).to(torch.int32)
+    offs = np.zeros(nb + 1, np.uint64)
+    offs[1:] = np.cumsum(np.asarray(cards, np.uint64))
+    return vals, offs
+
+
+def run_rows_batch(starts, lens, nrun, universe, device):
+    """Rows of one batch as unions of runs [start, start + len) clipped to
+    the universe: nrun[r] runs for row r, starts/lens their concatenation.
+    Returns (values int32 on the device, offsets numpy u64 from 0)."""
+    import torch
+    U = int(universe)
+    nb = len(nrun)
+    st = torch.as_tensor(np.asarray(starts, np.int64), device=device)
+    ln = torch.as_tensor(np.asarray(lens, np.int64), device=device)
+    rr = torch.repeat_interleave(torch.arange(nb, device=device), torch.as_tensor(np.asarray(nrun, np.int64),
+                                                                                     device=device))
+    tot = int(ln.sum().item())
+    run_of = torch.repeat_interleave(torch.arange(st.numel(), device=device), ln)
+    first = torch.cumsum(ln, 0) - ln
+    pos = st[run_of] + (torch.arange(tot, device=device) - first[run_of])
+    ok = pos < U
+    key = torch.unique(rr[run_of][ok] * U + pos[ok])
+    cnt = torch.bincount(key // U, minlength=nb).cpu().numpy()
+    offs = np.zeros(nb + 1, np.uint64)
+    offs[1:] = np.cumsum(cnt.astype(np.uint64))
+    return (key % U).to(torch.int32), offs
+
+
+class FullCorpus:
+    """One of the full-size STORM_t configurations, generated on the GPU
+    batch by batch, each batch from its own seed, so that any batch can be
+    made again on its own.  kind:
+      "zipf"      N rows over `universe`, card ~ Zipf(s) on [lo, hi] (P(k) ~
+                  k^-s restricted to the range), uniform without replacement;
+      "runs"      N rows over `universe`, Poisson(mean_runs) runs per row,
+                  start uniform, length Geometric(mean mean_len);
+      "bernoulli" N rows over `universe`, every bit iid Bernoulli(density):
+                  card ~ Binomial, positions uniform without replacement;
+      "bits"      the same distribution made as packed bitmaps (every bit
+                  drawn), for densities whose value lists would be larger.
+    batch(b) -> (r0, r1, values int32 on the device, offsets numpy u64), or
+    for "bits" (r0, r1, words int64 [rows, universe / 64] on the device,
+    None)."""
+
+    def __init__(self, kind, n, universe, seed, device, max_values=1 << 28, **kw):
+        self.kind, self.n, self.universe, self.seed, self.device = kind, n, int(universe), seed, device
+        g = np.random.Generator(np.random.PCG64(seed))
+        self.density = kw.get("density")
+        if kind == "zipf":
+            self.cards = zipf_cards(n, kw.get("s", 1.1), kw["lo"], kw["hi"], seed)
+            sizes = self.cards
+        elif kind == "bernoulli":
+            self.cards = g.binomial(self.universe, self.density, size=n).astype(np.int64)
+            sizes = self.cards
+        elif kind == "bits":
+            self.cards = None
+            sizes = np.full(n, self.universe // 32, np.int64)      # u64 words, in 32-bit units
+        elif kind == "runs":
+            self.nrun = g.poisson(kw["mean_runs"], size=n).astype(np.int64)
+            tot = int(self.nrun.sum())
+            self.starts = g.integers(0, self.universe, size=tot)
+            self.lens = g.geometric(1.0 / kw["mean_len"], size=tot).astype(np.int64)
+            self.run0 = np.zeros(n + 1, np.int64)
+            self.run0[1:] = np.cumsum(self.nrun)
+            sizes = np.zeros(n, np.int64)
+            nz = self.nrun > 0
+            sizes[nz] = np.add.reduceat(self.lens, self.run0[:-1][nz]) if tot else 0
+            self.cards = None
+        else:
+            raise ValueError(kind)
+        self.plan = batch_plan(sizes, max_values)
+
+    def batch(self, b):
+        import torch
+        r0, r1 = self.plan[b]
+        if self.kind == "runs":
+            a, z = int(self.run0[r0]), int(self.run0[r1])
+            vals, offs = run_rows_batch(self.starts[a:z], self.lens[a:z], self.nrun[r0:r1], self.universe,
+                                        self.device)
+            return r0, r1, vals, offs
+        if self.kind == "bits":
+            g = torch.Generator(device=self.device)
+            g.manual_seed(self.seed * 1000003 + b)
+            w = self.universe // 64
+            out = torch.empty((r1 - r0, w), dtype=torch.int64, device=self.device)
+            shifts = torch.arange(64, device=self.device, dtype=torch.int64)
+            for q0 in range(0, r1 - r0, 16):
+                q1 = min(r1 - r0, q0 + 16)
+                bits = torch.rand((q1 - q0, self.universe), generator=g, device=self.device) < self.density
+                out[q0:q1] = (bits.view(q1 - q0, w, 64).to(torch.int64) << shifts).sum(dim=-1)
+                del bits
+            return r0, r1, out, None
+        vals, offs = uniform_rows_batch(self.cards[r0:r1], self.universe, self.seed * 1000003 + b, self.device)
+        return r0, r1, vals, offs
+
+
+def full_corpus(name, device):
+    """The full-size configurations run through STORM_t."""
+    if name == "config3":
+        return FullCorpus("zipf", 100000, 1 << 24, 0xC0F3, device, s=1.1, lo=16, hi=1 << 22)
+    if name == "config4":
+        return FullCorpus("runs", 50000, 1 << 26, 0xC0F4, device, mean_runs=200, mean_len=256)
+    if name == "config5b_0.01":
+        return FullCorpus("bernoulli", 20000, 1 << 24, 0xC05B, device, density=0.01)
+    if name == "config5b_0.17":
+        return FullCorpus("bits", 20000, 1 << 24, 0xC05C, device, density=0.17, max_values=1 << 27)
+    raise ValueError(name)
+
+
+FULL_CORPORA = {
+    "config3": "100000 rows over 2^24, card ~ Zipf(1.1) on [16, 2^22], uniform w/o replacement (5.0e9 pairs)",
+    "config4": "50000 rows over 2^26, Poisson(200) runs of Geometric(mean 256) length (1.25e9 pairs)",
+    "config5b_0.01": "20000 rows over 2^24, Bernoulli(0.01) (2.0e8 pairs)",
+    "config5b_0.17": "20000 rows over 2^24, Bernoulli(0.17) (2.0e8 pairs)",
+}
+
+
+def _batch_hist_and_cards(corpus, vals_or_words, offs):
+    """(value histogram of the batch over the universe, per-row counts)."""
+    import torch
+    if offs is not None:
+        return torch.bincount(vals_or_words, minlength=corpus.universe), np.diff(offs.astype(np.int64))
+    w = vals_or_words
+    shifts = torch.arange(64, device=w.device, dtype=torch.int64)
+    h = torch.zeros(corpus.universe, dtype=torch.int64, device=w.device)
+    cards = torch.zeros(w.shape[0], dtype=torch.int64, device=w.device)
+    for q0 in range(0, w.shape[0], 16):
+        bits = ((w[q0:q0 + 16, :, None] >> shifts) & 1).view(-1, corpus.universe)
+        h += bits.sum(dim=0)
+        cards[q0:q0 + 16] = bits.sum(dim=1)
+        del bits
+    return h, cards.cpu().numpy()
+
+
+def _batch_row_sums(corpus, vals_or_words, offs, hist):
+    """Per row of the batch: sum over its values v of hist[v]."""
+    import torch
+    if offs is not None:
+        nb = len(offs) - 1
+        seg = torch.repeat_interleave(torch.arange(nb, device=hist.device),
+                                      torch.as_tensor(np.diff(offs.astype(np.int64)), device=hist.device))
+        out = torch.zeros(nb, dtype=torch.int64, device=hist.device)
+        out.index_add_(0, seg, hist[vals_or_words.to(torch.int64)])
+        return out
+    w = vals_or_words
+    shifts = torch.arange(64, device=w.device, dtype=torch.int64)
+    hf = hist.to(torch.float64)
+    out = torch.zeros(w.shape[0], dtype=torch.int64, device=w.device)
+    for q0 in range(0, w.shape[0], 8):
+        bits = ((w[q0:q0 + 8, :, None] >> shifts) & 1).view(-1, corpus.universe).to(torch.float64)
+        out[q0:q0 + 8] = torch.round(bits @ hf).to(torch.int64)   # exact: every partial sum < 2^53
+        del bits
+    return out
+
+
+def load_full_corpus(sb, corpus, on_batch=None, row_sums=True, keep_limit=100 << 30):
+    """Generates every batch in row order and appends it to a new STORM_t
+    (STORM_add_rows for value lists, STORM_add_bitmap_rows for bitmaps, from
+    host memory), accumulating the value histogram on the device; calls
+    on_batch(r0, r1, host values or words, offsets or None) per batch.  With
+    row_sums, also returns every row's sum over its values v of (rows
+    holding v) -- from batches kept on the device when they fit keep_limit,
+    else from a second pass that makes each batch again.  Returns a dict:
+    storm, hist, cards, want_row (or None), gen_s, add_s."""
+    import torch
+    st = sb.Storm()
+    hist = torch.zeros(corpus.universe, dtype=torch.int64, device=corpus.device)
+    cards = np.zeros(corpus.n, np.int64)
+    t_gen = t_add = 0.0
+    kept, kept_bytes, keep = [], 0, row_sums
+    for b in range(len(corpus.plan)):
+        t0 = time.perf_counter()
+        r0, r1, x, offs = corpus.batch(b)
+        h, c = _batch_hist_and_cards(corpus, x, offs)
+        hist += h
+        cards[r0:r1] = c
+        host = x.cpu().numpy()
+        t1 = time.perf_counter()
+        if offs is not None:
+            st.add_rows(host.view(np.uint32), offs)
+        else:
+            st.add_bitmap_rows(host.view(np.uint64))
+        t2 = time.perf_counter()
+        t_gen += t1 - t0
+        t_add += t2 - t1
+        if on_batch is not None:
+            on_batch(r0, r1, host.view(np.uint32) if offs is not None else host.view(np.uint64), offs)
+        if keep:
+            kept_bytes += x.numel() * x.element_size()
+            if kept_bytes <= keep_limit:
+                kept.append((r0, r1, x, offs))
+            else:
+                keep, kept = False, []
+        del x, host
+    want_row = None
+    if row_sums:
+        want_row = torch.zeros(corpus.n, dtype=torch.int64, device=corpus.device)
+        if keep:
+            for r0, r1, x, offs in kept:
+                want_row[r0:r1] = _batch_row_sums(corpus, x, offs, hist)
+            kept = []
+        else:
+            for b in range(len(corpus.plan)):
+                r0, r1, x, offs = corpus.batch(b)
+                want_row[r0:r1] = _batch_row_sums(corpus, x, offs, hist)
+                del x
+    torch.cuda.empty_cache()
+    return {"storm": st, "hist": hist, "cards": cards, "want_row": want_row, "gen_s": t_gen, "add_s": t_add}
+
+
+def triangle_row_sums(d_tri, n):
+    """Per row i of the full symmetric matrix held as a packed device
+    triangle (i <= j): the upper part of row i plus column i above the
+    diagonal; and the diagonal.  Returns (row sums int64, diagonal int64),
+    both on the device."""
+    import torch
+    dev = d_tri.device
+    ii = np.arange(n + 1, dtype=np.int64)
+    S = ii * n - (ii * (ii - 1)) // 2                  # start of row i; S[n] = n(n+1)/2
+    got = torch.zeros(n, dtype=torch.int64, device=dev)
+    diag = torch.zeros(n, dtype=torch.int64, device=dev)
+    i = 0
+    while i < n:
+        i1 = int(np.searchsorted(S, S[i] + (1 << 27), side="right")) - 1   # rows whose entries fit the step
+        i1 = min(n, max(i + 1, i1))
+        a, b = int(S[i]), int(S[i1])
+        seg = d_tri[a:b].to(torch.int64) & 0xFFFFFFFF
+        lens = torch.as_tensor(n - ii[i:i1], device=dev)
+        rows = torch.repeat_interleave(torch.arange(i, i1, device=dev), lens)
+        first = torch.as_tensor(S[i:i1] - a, device=dev)
+        cols = rows + (torch.arange(b - a, device=dev) - torch.repeat_interleave(first, lens))
+        got.index_add_(0, rows, seg)
+        off = cols != rows
+        got.index_add_(0, cols[off], seg[off])
+        diag[i:i1] = seg[first]
+        del seg, rows, cols, off
+        i = i1
+    return got, diag
+
+
+def storm_t_full(device, names=tuple(FULL_CORPORA), cpu_seconds=2.0):
+    """The sparse and mixed-density configurations at full size through
+    STORM_t: rows generated on the GPU and appended from host memory
+    (STORM_add_rows / STORM_add_bitmap_rows), then
+      e2e       the first per-pair call into a host buffer (packs the rows,
+                uploads them, computes, copies the triangle back);
+      device    per-pair counts into HBM, device time of the call (best of 2);
+      sum_only  the reference's STORM_pairw_intersect_cardinality;
+    every triangle checked against the value-histogram identities (every
+    row's sum, the diagonal, the total) before it is reported; and the
+    reference's own STORM_pairw_intersect_cardinality on 1 core plus a
+    harness over all host threads, on a prefix of the rows."""
+    import torch
+    import importlib
+    sb = importlib.import_module("stormbitmaps-internal_b200")
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as ol
+    R = ol.reference()
+    out = {}
+    for name in names:
+        torch.cuda.empty_cache()
+        t0 = time.perf_counter()
+        corpus = full_corpus(name, device)
+        prefix = {}
+
+        def keep_prefix(r0, r1, host, offs):
+            if r0 == 0:
+                prefix["host"], prefix["offs"] = host.copy(), None if offs is None else offs.copy()
+
+        res = load_full_corpus(sb, corpus, on_batch=keep_prefix)
+        st, hist, cards = res["storm"], res["hist"], res["cards"]
+        n = corpus.n
+        tri = n * (n + 1) // 2
+        r = {"workload": FULL_CORPORA[name], "rows": n, "pairs_i_le_j": tri, "values": int(cards.sum()),
+             "generate_s": round(res["gen_s"], 1), "STORM_add_rows_s": round(res["add_s"], 1)}
+        want_sum = int((hist * (hist - 1) // 2).sum().item())
+        # end to end: the first per-pair call into host memory
+        host_out = torch.empty(tri, dtype=torch.int32, pin_memory=True)
+        t1 = time.perf_counter()
+        _, s_e2e = st.matrix(host_out.numpy().view(np.uint32))
+        r["e2e"] = {"first_matrix_call_s": round(time.perf_counter() - t1, 3),
+                    "pairs_per_s": tri / (time.perf_counter() - t1), "d2h_bytes": tri * 4,
+                    "call": "STORM_pairw_intersect_matrix (pack + upload + all pairs + copy back)"}
+        del host_out
+        d_tri = torch.empty(tri, dtype=torch.int32, device=device)
+        best, sums = None, {s_e2e}
+        for _ in range(2):
+            sums.add(st.matrix_device(d_tri.data_ptr(), tri))
+            ms = st.last_kernel_ms()
+            best = ms if best is None else min(best, ms)
+        r["device"] = {"ms": round(best, 2), "pairs_per_s": tri / (best * 1e-3), "ns_per_pair": best * 1e6 / tri,
+                       "tensor_rows": st.last_dense()[0], "postings_rows": st.last_postings_rows()}
+        got_row, diag = triangle_row_sums(d_tri, n)
+        ok = (bool(torch.equal(diag.cpu(), torch.as_tensor(cards))) and
+              int((got_row != res["want_row"]).sum().item()) == 0 and sums == {want_sum})
+        r["checked"] = {"identities_hold": ok, "sum_i_lt_j": want_sum}
+        del d_tri, got_row, diag
+        torch.cuda.empty_cache()
+        best = None
+        for _ in range(2):
+            v = st.pairw_intersect_cardinality()
+            ms = st.last_kernel_ms()
+            best = ms if best is None else min(best, ms)
+            r["checked"]["identities_hold"] &= v == want_sum
+        r["sum_only_ms"] = round(best, 2)
+        st.close()
+        if R is not None and prefix.get("offs") is not None:
+            vals_p, offs_p = prefix["host"], prefix["offs"]
+            for label, mt in (("cpu_reference", False), ("cpu_reference_all_threads", True)):
+                k = 64
+                while True:
+                    k = min(k, len(offs_p) - 1)
+                    v = np.ascontiguousarray(vals_p[:int(offs_p[k])], dtype=np.uint32)
+                    o = np.ascontiguousarray(offs_p[:k + 1], dtype=np.uint64)
+                    sec = C.c_double(0.0)
+                    if mt:
+                        R.ref_storm_sum_mt(v.ctypes.data_as(ol.u32p), o.ctypes.data_as(ol.u64p), k, cpu_threads(),
+                                           C.byref(sec))
+                    else:
+                        R.ref_storm_sum_timed(v.ctypes.data_as(ol.u32p), o.ctypes.data_as(ol.u64p), k, C.byref(sec))
+                    if sec.value >= cpu_seconds or k == len(offs_p) - 1:
+                        break
+                    k *= 2
+                rate = (k * (k - 1) // 2) / max(sec.value, 1e-9)
+                r[label] = {"pairs_per_s": rate, "cores": cpu_threads() if mt else 1,
+                            "sample": f"first {k} rows ({k * (k - 1) // 2} pairs i < j, {sec.value:.2f} s), " +
+                                      ("project harness over the reference's per-pair "
+                                       "STORM_bitmap_cont_intersect_cardinality_premade" if mt else
+                                       "STORM_pairw_intersect_cardinality as shipped")}
+                r["device_over_" + label] = r["device"]["pairs_per_s"] / rate
+        r["seconds"] = round(time.perf_counter() - t0, 1)
+        out[name] = r
+        del res, prefix
+    return out
+
+
 # The library's default tensor-core dense-block threshold (rows whose sparse
 # form is at least 2^-14 of the universe).
 DENSE_BLOCK_DEFAULT = 1.0 / 16384
@@ -1027,6 +1432,10 @@ def run_b200_arm(args):
         except Exception as e:
             line["storm_t"] = {"error": f"{type(e).__name__}: {e}"}
         try:
+            line["storm_t_full"] = storm_t_full(device)
+        except Exception as e:
+            line["storm_t_full"] = {"error": f"{type(e).__name__}: {e}"}
+        try:
             line["autotune_config1"] = autotune_config1(sb, device)
         except Exception as e:
             line["autotune_config1"] = {"error": f"{type(e).__name__}: {e}"}
@@ -1062,6 +1471,8 @@ def main():
                     help="dram bytes per launch of the dominant kernel from an ncu capture")
     ap.add_argument("--storm-t-case", default=None, choices=STORM_T_CASES,
                     help="run only this STORM_t corpus of the forms (one JSON line) and exit")
+    ap.add_argument("--storm-t-full", default=None, choices=tuple(FULL_CORPORA),
+                    help="run only this full-size STORM_t configuration (one JSON line) and exit")
     ap.add_argument("--mixed-density-only", action="store_true",
                     help="run only the kernel layer's mixed-density forms (one JSON line) and exit")
     ap.add_argument("--mixed-density-batched", action="store_true",
@@ -1086,6 +1497,11 @@ def main():
         import torch
         sb = importlib.import_module("stormbitmaps-internal_b200")
         print(json.dumps({"mixed_density": mixed_density_forms(sb, torch.device("cuda", 0))}), flush=True)
+        return 0
+    if args.storm_t_full:
+        import torch
+        print(json.dumps({"storm_t_full": storm_t_full(torch.device("cuda", 0), names=(args.storm_t_full,))}),
+              flush=True)
         return 0
     if args.storm_t_case:
         import torch

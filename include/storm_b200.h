@@ -188,6 +188,21 @@ int STORM_contig_pairw_threshold(STORM_contiguous_t* c, double jaccard_min, uint
                                  uint32_t* out_count, uint64_t cap, uint64_t* n_found);
 
 /* ---- STORM_t extensions ----------------------------------------------- */
+/* n_rows STORM_add calls in one (no counterpart in the reference, whose
+ * callers loop over STORM_add, storm.cpp:894-916): row r is values
+ * [offsets[r], offsets[r+1]) (offsets has n_rows + 1 entries, ascending),
+ * appended with exactly the chunks STORM_add builds -- empty rows included --
+ * while the rows are split into chunks on several host threads.  Returns
+ * n_rows; STORM_B200_EARG for offsets that decrease or a row of 2^32 values
+ * or more, STORM_B200_ENOMEM when a chunk could not be allocated (the rows
+ * are then appended with what fit). */
+int64_t STORM_add_rows(STORM_t* s, const uint32_t* values, const uint64_t* offsets, uint64_t n_rows);
+/* The same for rows given as little-endian bitmaps in host memory: row r is
+ * words [r * words_per_row, (r + 1) * words_per_row), bit b = word b / 64,
+ * bit b % 64 (words_per_row <= 2^26), appended as STORM_add appends the
+ * row's set positions in ascending order.  Returns n_rows; errors as
+ * STORM_add_rows. */
+int64_t STORM_add_bitmap_rows(STORM_t* s, const uint64_t* words, uint64_t n_rows, uint64_t words_per_row);
 /* Append the rows of a STORMBIN corpus file (the reference's on-disk format:
  * "STORMBIN", u32 version 1, n_rows, n_bits, pad, then per row a u32 count
  * and that many strictly ascending u32 positions < n_bits;
@@ -209,6 +224,10 @@ int STORM_pairw_threshold(STORM_t* s, double jaccard_min, uint32_t* out_i, uint3
                           uint64_t cap, uint64_t* n_found);
 int STORM_upload(STORM_t* s);
 int STORM_pairw_intersect_matrix(STORM_t* s, uint32_t* out, uint64_t out_len, uint64_t* sum);
+/* Same, into a DEVICE buffer on the current device (d_out may be NULL to
+ * compute only the sum).  Work already queued on other streams is waited for
+ * before d_out is written. */
+int STORM_pairw_intersect_matrix_device(STORM_t* s, uint32_t* d_out, uint64_t out_len, uint64_t* sum);
 int STORM_pairw_intersect_tiles(STORM_t* s, uint32_t tile, STORM_tile_callback cb, void* ctx);
 float STORM_last_kernel_ms(const STORM_t* s);
 /* Tensor-core dense block of the STORM_t all-pairs calls (no counterpart in
@@ -251,6 +270,22 @@ int STORM_set_sparse_postings(STORM_t* s, int mode);
  * are reported when non-NULL.  Counts do not depend on the choice. */
 int STORM_autotune(STORM_t* s, double* best_min_density, int* best_postings, double* times_ms);
 uint64_t STORM_last_postings_rows(const STORM_t* s);
+/* Transposed panel of the STORM_t per-pair calls (no counterpart in the
+ * reference): plain rows below the tensor-core rows in value count are
+ * queried, value by value, against blocks of up to 2048 denser rows stored
+ * transposed in HBM (per value, one bit per panel row), so that a pair of a
+ * sparse row x and a dense row costs |x| bits of traffic instead of the
+ * universe's.  The planner then splits plain rows three ways -- postings
+ * rows (pairs among themselves by value postings), panel rows, tensor rows
+ * (pairs among themselves on the tensor cores) -- by predicted time.
+ * mode -1 (default): when predicted faster than the plan without it; 1:
+ * whenever the rows and device memory allow (universe up to 2^26 values);
+ * 2: every plain row in the panel (all their pairs by it); 0: never.  Applies with the automatic dense block and postings
+ * (STORM_set_dense_block(s, -1, ...), STORM_set_sparse_postings(s, -1)).
+ * Counts are identical. */
+int STORM_set_panel(STORM_t* s, int mode);
+/* Rows the last per-pair call stored in the transposed panel. */
+uint64_t STORM_last_panel_rows(const STORM_t* s);
 
 #ifdef __cplusplus
 } /* extern "C" */

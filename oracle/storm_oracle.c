@@ -457,3 +457,63 @@ void oracle_row_popcounts(const uint64_t* words, uint64_t n, uint64_t nw, uint32
         out[r] = (uint32_t)c;
     }
 }
+
+/* Strips of the per-pair matrix for up to 8 query rows against many rows,
+ * without the n^2 buffer: |Q_k & R_j| = the number of values of R_j that Q_k
+ * holds (the set intersection oracle_sets_matrix counts, by a membership
+ * table instead of a merge).  o_strip_new builds the table: byte v has bit k
+ * set when query k holds value v (values < universe).  o_strip_count fills
+ * out[j * nq + k] for rows j of a CSR batch and may be called from several
+ * threads at once on disjoint batches. */
+typedef struct {
+    uint8_t* mask;
+    uint64_t universe;
+    uint32_t nq;
+} o_strip;
+
+void* oracle_strip_new(const uint32_t* qvals, const uint64_t* qoffs, uint32_t nq, uint64_t universe) {
+    if (nq == 0 || nq > 8) return NULL;
+    o_strip* h = (o_strip*)malloc(sizeof(o_strip));
+    if (!h) return NULL;
+    h->mask = (uint8_t*)calloc(universe ? universe : 1, 1);
+    if (!h->mask) {
+        free(h);
+        return NULL;
+    }
+    h->universe = universe;
+    h->nq = nq;
+    for (uint32_t k = 0; k < nq; ++k)
+        for (uint64_t e = qoffs[k]; e < qoffs[k + 1]; ++e)
+            if (qvals[e] < universe) h->mask[qvals[e]] |= (uint8_t)(1u << k);
+    return h;
+}
+
+void oracle_strip_count(const void* hp, const uint32_t* vals, const uint64_t* offs, uint64_t n, uint32_t* out) {
+    const o_strip* h = (const o_strip*)hp;
+    for (uint64_t j = 0; j < n; ++j) {
+        uint32_t c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (uint64_t e = offs[j]; e < offs[j + 1]; ++e) {
+            const uint32_t v = vals[e];
+            if (v >= h->universe) continue;
+            const uint32_t m = h->mask[v];
+            for (uint32_t k = 0; k < h->nq; ++k) c[k] += (m >> k) & 1u;
+        }
+        for (uint32_t k = 0; k < h->nq; ++k) out[j * h->nq + k] = c[k];
+    }
+}
+
+void oracle_strip_free(void* hp) {
+    o_strip* h = (o_strip*)hp;
+    if (!h) return;
+    free(h->mask);
+    free(h);
+}
+
+/* The same strips for rows given as packed bitmaps (nw words each):
+ * out[j * nq + k] = |Q_k & R_j| by AND + popcount (oracle_and_popcount). */
+void oracle_contig_strip(const uint64_t* q, uint32_t nq, const uint64_t* words, uint64_t n, uint64_t nw,
+                         uint32_t* out) {
+    for (uint64_t j = 0; j < n; ++j)
+        for (uint32_t k = 0; k < nq; ++k)
+            out[j * nq + k] = (uint32_t)oracle_and_popcount(q + (uint64_t)k * nw, words + j * nw, nw);
+}

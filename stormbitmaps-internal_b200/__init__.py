@@ -96,6 +96,9 @@ _sig("STORM_new", C.c_void_p, [])
 _sig("STORM_free", None, [C.c_void_p])
 _sig("STORM_add", C.c_int, [C.c_void_p, u32p, C.c_uint32])
 _sig("STORM_clear", C.c_int, [C.c_void_p])
+_sig("STORM_add_rows", C.c_int64, [C.c_void_p, u32p, u64p, C.c_uint64])
+_sig("STORM_add_bitmap_rows", C.c_int64, [C.c_void_p, u64p, C.c_uint64, C.c_uint64])
+_sig("STORM_pairw_intersect_matrix_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, u64p])
 _sig("STORM_pairw_intersect_cardinality", C.c_uint64, [C.c_void_p])
 _sig("STORM_pairw_intersect_cardinality_blocked", C.c_uint64, [C.c_void_p, C.c_uint32])
 _sig("STORM_intersect_cardinality_square", C.c_uint64, [C.c_void_p, C.c_void_p])
@@ -109,6 +112,8 @@ _sig("STORM_last_dense_rows", C.c_uint64, [C.c_void_p])
 _sig("STORM_last_dense_panels", C.c_uint64, [C.c_void_p])
 _sig("STORM_set_sparse_postings", C.c_int, [C.c_void_p, C.c_int])
 _sig("STORM_last_postings_rows", C.c_uint64, [C.c_void_p])
+_sig("STORM_set_panel", C.c_int, [C.c_void_p, C.c_int])
+_sig("STORM_last_panel_rows", C.c_uint64, [C.c_void_p])
 
 
 class StormError(RuntimeError):
@@ -371,6 +376,32 @@ class Storm:
         self.n += 1
         return rc
 
+    def add_rows(self, vals, offs) -> int:
+        """Rows in CSR form (u32 values, u64 offsets of n + 1 entries) through
+        STORM_add_rows: the same rows as one add() per row."""
+        v = np.ascontiguousarray(vals, dtype=np.uint32)
+        o = np.ascontiguousarray(offs, dtype=np.uint64)
+        rc = int(_lib.STORM_add_rows(self.h, _p(v, u32p), _p(o, u64p), len(o) - 1))
+        _check(rc, "STORM_add_rows")
+        self.n += rc
+        return rc
+
+    def add_bitmap_rows(self, words: np.ndarray) -> int:
+        """Rows as packed bitmaps ([n, words_per_row] u64, host memory) through
+        STORM_add_bitmap_rows: the same rows as add() of each row's positions."""
+        w = np.ascontiguousarray(words, dtype=np.uint64)
+        rc = int(_lib.STORM_add_bitmap_rows(self.h, _p(w, u64p), w.shape[0], w.shape[1]))
+        _check(rc, "STORM_add_bitmap_rows")
+        self.n += rc
+        return rc
+
+    def matrix_device(self, d_out_ptr: int, out_len: int) -> int:
+        """Per-pair counts into a device buffer (0 = sum only); returns the sum."""
+        s = C.c_uint64(0)
+        _check(_lib.STORM_pairw_intersect_matrix_device(self.h, C.c_void_p(d_out_ptr or None), out_len,
+                                                        C.byref(s)), "STORM_pairw_intersect_matrix_device")
+        return int(s.value)
+
     def clear(self):
         self.n = 0
         return _lib.STORM_clear(self.h)
@@ -447,6 +478,12 @@ class Storm:
 
     def last_postings_rows(self) -> int:
         return int(_lib.STORM_last_postings_rows(self.h))
+
+    def set_panel(self, mode: int):
+        _check(_lib.STORM_set_panel(self.h, int(mode)), "STORM_set_panel")
+
+    def last_panel_rows(self) -> int:
+        return int(_lib.STORM_last_panel_rows(self.h))
 
     def last_dense(self):
         """(rows, panels) the last all-pairs call gave to the tensor-core block."""

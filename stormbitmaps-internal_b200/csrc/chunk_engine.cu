@@ -7,6 +7,7 @@
 #include "chunk_engine.cuh"
 #include "dense.cuh"
 #include "list16_ref.cuh"
+#include "panel.cuh"
 
 namespace sb200 {
 
@@ -615,6 +616,29 @@ postings_rows_kernel(ChunkView v, const uint32_t* __restrict__ qrows, uint32_t n
     }
 }
 
+// Diagonal of rows with bitmap chunks too (warp per row): each row's value
+// count, set bits of its bitmap chunks plus its list entries.
+__global__ void row_card_diag_kernel(ChunkView v, const uint32_t* __restrict__ rows, uint32_t m, uint64_t n,
+                                     uint32_t* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
+        const uint32_t row = rows[r];
+        uint32_t card = 0;
+        for (uint64_t c = v.row_off[row]; c < v.row_off[row + 1]; ++c) {
+            const uint32_t k = v.ckl[c];
+            if (k & CK_BITMAP) {
+                const uint64_t* wd = v.bm + v.coff[c];
+                for (uint32_t w = lane; w < (k & CK_LEN); w += 32) card += __popcll(wd[w]);
+            } else if (lane == 0) {
+                card += k & CK_LEN;
+            }
+        }
+        card = warp_sum_u32(card);
+        if (lane == 0) out[tri_index(n, row, row)] = card;
+    }
+}
+
 // Diagonal of the postings rows: their value count.
 __global__ void postings_diag_kernel(ChunkView v, const uint32_t* __restrict__ rows, uint32_t nq, uint64_t n,
                                      uint32_t* __restrict__ out) {
@@ -687,8 +711,14 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         return f.sum;
     }
 
-    // ---- row classes: D (tensor cores: every pair with a D row), Q (postings:
-    // pairs of two Q rows), C (chunk kernel: every pair with a C row).
+    // ---- row classes, in walk order [C | L | M | H]:
+    //   C  chunk kernel: every pair with a C row (rows with a repeated list
+    //      value, or anything the other engines cannot take);
+    //   L  postings rows (plain, no bitmap chunk): L x L by value postings;
+    //   M  panel rows queried and stored: (L u M) x (M u H) pairs by the
+    //      transposed-panel engine (panel.cuh), each pair once;
+    //   H  tensor rows: H x H on the tensor cores -- and, in the plan without
+    //      a panel, H x L too (the L rows expanded behind the H rows).
     const uint64_t n = n1;
     const uint64_t slots = (uint64_t)d.max_cid + 1;
     const uint64_t U = slots * 65536;                      // universe of the rows' values
@@ -697,7 +727,8 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
     const bool tc_ok = dense_min_density != 0.0 && U <= TC_MAX_ROW_BITS && facts_ok;
     const bool post_ok = postings_mode != 0 && U <= POSTINGS_MAX_UNIVERSE && facts_ok;
     const double tc_ns = tensor_pair_ns(cost, slots);
-    std::vector<uint8_t> cls(n, 0);                        // 0 C, 1 Q, 2 D
+    std::vector<uint8_t> cls(n, 0);                        // 0 C, 1 L, 2 M, 3 H
+    last_panel_rows = last_panel_queries = 0;
 
     SB_CUDA(cudaEventRecord(log.ev0, st));
     PostingsStats ps{};
@@ -718,6 +749,45 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         SB_CUDA(cudaStreamSynchronize(st));
         return h;
     };
+    auto finish = [&](uint64_t extra_sum) {
+        SB_CUDA(cudaEventRecord(log.ev1, st));
+        DeviceFlags f;
+        SB_CUDA(cudaMemcpyAsync(&f, d_flags.p, sizeof(f), cudaMemcpyDeviceToHost, st));
+        SB_CUDA(cudaStreamSynchronize(st));
+        if (f.error) fail(STORM_B200_ETIMEOUT, "tensor-core dense block: a pipeline wait timed out");
+        SB_CUDA(cudaEventElapsedTime(&log.last_ms, log.ev0, log.ev1));
+        log.launches = launches;
+        return f.sum + extra_sum;
+    };
+
+    // Sum-only calls: over every pair of plain rows the sum is
+    // sum_v C(rows holding v, 2) -- one value histogram, no pair touched
+    // (bitmap chunks count every set bit); pairs with another row run on the
+    // chunk kernel.
+    if (!d_out && post_ok) {
+        std::vector<uint32_t> plain;
+        for (uint32_t r = 0; r < n; ++r)
+            if (d.facts[r].plain) plain.push_back(r);
+        uint64_t q_sum = 0;
+        if (plain.size() >= 2) {
+            q_sum = histogram(plain).pairs;
+            last_postings_rows = plain.size();
+        }
+        const uint64_t nc = n - plain.size();
+        if (nc) {
+            for (uint32_t r : plain) cls[r] = 1;
+            std::vector<uint32_t> h_perm;
+            h_perm.reserve(n);
+            for (int k = 0; k < 2; ++k)
+                for (uint32_t r = 0; r < n; ++r)
+                    if (cls[r] == k) h_perm.push_back(r);
+            d_perm.reserve(n);
+            SB_CUDA(cudaMemcpyAsync(d_perm.p, h_perm.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+            chunk_launch(PAIRS_TRIANGLE, nc * n - (nc * (nc - 1)) / 2, d_perm.p, 0, 0, n, 0);
+        }
+        return finish(q_sum);
+    }
+
     // Per-pair form of the postings: list by list into the output while the
     // triangle fits in L2 (its atomics stay on chip), else the row sweep
     // (partners counted in shared memory, each output written once).
@@ -736,9 +806,24 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         const double per_pair = sweep_form(incr, q) ? sweep_ns(incr, q) : incr * c_list;
         return (d_out ? per_pair : 0.0) + (double)U * cost.ns_per_universe_value;
     };
-    std::vector<uint32_t> qrows, dense;
+    std::vector<uint32_t> qrows, dense, mrows;             // L, H, M
+    bool panel_plan = false;
+    // The panel needs a block of expanded rows and its transpose in HBM.
+    const uint64_t panel_bytes = 2ull * PANEL_ROWS * W * sizeof(uint64_t);
+    auto panel_fits = [&]() {
+        if (!facts_ok || panel_mode == 0 || U > PANEL_MAX_UNIVERSE) return false;
+        size_t fr = 0, tot = 0;
+        SB_CUDA(cudaMemGetInfo(&fr, &tot));
+        return (double)panel_bytes < 0.5 * ((double)fr + (double)(d_pX.n + d_DT.n) * sizeof(uint64_t));
+    };
 
-    if (tc_ok && dense_min_density > 0.0) {
+    if (panel_mode == 2 && facts_ok && U <= PANEL_MAX_UNIVERSE) {
+        // Every plain row in the panel: all their pairs by the transposed
+        // panel, rows queried against the blocks after them.
+        for (uint32_t r = 0; r < n; ++r)
+            if (d.facts[r].plain) mrows.push_back(r);
+        panel_plan = true;
+    } else if (tc_ok && dense_min_density > 0.0) {
         // Explicit threshold: plain rows with value count >= min_density x U.
         const double min_card = dense_min_density * (double)U;
         std::vector<uint32_t> rest;
@@ -759,56 +844,104 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
             if (ps.entries < (1ull << 32) && (postings_mode > 0 || post_ns((double)ps.pairs, rest.size()) < alt)) qrows = rest;
         }
     } else if (tc_ok && post_ok) {
-        // Cost-chosen cut: plain rows with bitmap chunks go to D; the list
-        // rows, heaviest first, join D while that lowers tensor time (every
-        // pair of a D row) + postings time (pairs of the rest; increments
-        // estimated as for independent uniform rows, sum_{i<j} c_i c_j / U).
-        std::vector<uint32_t> lists;
-        for (uint32_t r = 0; r < n; ++r) {
-            const ChunkRowFacts& f = d.facts[r];
-            if (!f.plain) continue;
-            if (f.bitmap_chunks) dense.push_back(r);
-            else lists.push_back(r);
-        }
-        std::stable_sort(lists.begin(), lists.end(),
+        // Plain rows, heaviest first.  Plan A (no panel): rows with bitmap
+        // chunks go to H, list rows join H while that lowers tensor time (H x
+        // everything) + postings time (increments estimated as for
+        // independent uniform rows, sum_{i<j} c_i c_j / U).  Plan B (panel):
+        // the top h rows H, the next m rows M, the rest L; every row with a
+        // bitmap chunk in H u M.  The cheaper predicted plan runs.
+        std::vector<uint32_t> pl;
+        for (uint32_t r = 0; r < n; ++r)
+            if (d.facts[r].plain) pl.push_back(r);
+        std::stable_sort(pl.begin(), pl.end(),
                          [&](uint32_t x, uint32_t y) { return d.facts[x].card > d.facts[y].card; });
-        const double np = (double)(dense.size() + lists.size());
-        double s1 = 0.0, s2 = 0.0;
-        for (uint32_t r : lists) {
-            const double c = (double)d.facts[r].card;
-            s1 += c;
-            s2 += c * c;
+        const uint64_t np = pl.size();
+        std::vector<double> S1(np + 1, 0.0), S2(np + 1, 0.0);
+        uint64_t lb = 0;                                   // rows [0, lb) hold every bitmap-chunk row
+        for (uint64_t t = 0; t < np; ++t) {
+            const double c = (double)d.facts[pl[t]].card;
+            S1[t + 1] = S1[t] + c;
+            S2[t + 1] = S2[t] + c * c;
+            if (d.facts[pl[t]].bitmap_chunks) lb = t + 1;
         }
-        auto cost_at = [&](double k, double r1, double r2) {
-            const double tens = k > 0 ? tc_ns * (k * (k - 1.0) / 2.0 + k * (np - k)) : 0.0;
-            return tens + post_ns((r1 * r1 - r2) / (2.0 * (double)U), (uint64_t)(np - k));
+        auto post_est = [&](uint64_t from) {   // postings ns of the rows [from, np)
+            const uint64_t q = np - from;
+            if (q < 2) return 0.0;
+            const double r1 = S1[np] - S1[from], r2 = S2[np] - S2[from];
+            return post_ns((r1 * r1 - r2) / (2.0 * (double)U), q);
         };
-        size_t best_k = 0;
-        double best = cost_at((double)dense.size(), s1, s2);
-        double r1 = s1, r2 = s2;
-        for (size_t k = 1; k <= lists.size(); ++k) {
-            const double c = (double)d.facts[lists[k - 1]].card;
-            r1 -= c;
-            r2 -= c * c;
-            const double v = cost_at((double)(dense.size() + k), r1, r2);
-            if (v < best) {
-                best = v;
+        // Plan A: H = [0, k) for k >= lb.
+        uint64_t best_k = lb;
+        double best_a = -1.0;
+        for (uint64_t k = lb; k <= np; ++k) {
+            const double kk = (double)k;
+            const double v = tc_ns * (kk * (kk - 1.0) / 2.0 + kk * (double)(np - k)) + post_est(k);
+            if (best_a < 0 || v < best_a) {
+                best_a = v;
                 best_k = k;
             }
         }
-        if (postings_mode > 0) best_k = 0;                 // forced: every list row to the postings
-        std::vector<uint32_t> rest(lists.begin() + best_k, lists.end());
-        std::sort(rest.begin(), rest.end());             // stored order: ascending output writes
-        dense.insert(dense.end(), lists.begin(), lists.begin() + best_k);
+        if (postings_mode > 0) best_k = lb;                // forced: every list row to the postings
+        // Plan B over candidate cuts (h, m).
+        uint64_t best_h = 0, best_m = 0;
+        double best_b = -1.0;
+        if (postings_mode < 0 && panel_mode != 0 && panel_fits()) {
+            std::vector<uint64_t> cand{0, lb, np};
+            for (double x = 1.0; x < (double)np; x *= 1.12) cand.push_back((uint64_t)x);
+            std::sort(cand.begin(), cand.end());
+            cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+            const double build_ns = 3.0 * (double)PANEL_ROWS * (double)W * 8.0 * cost.ns_per_panel_byte;
+            for (uint64_t h : cand) {
+                for (uint64_t e : cand) {                  // e = h + m
+                    if (e < h || e < lb || e > np || e == 0) continue;
+                    if (panel_mode > 0 && e == h) continue;    // forced: some rows in M
+                    const double m = (double)(e - h), hh = (double)h, nl = (double)(np - e);
+                    const double nb = std::ceil((double)e / PANEL_ROWS);
+                    const double nbh = hh / PANEL_ROWS, nbm = m / PANEL_ROWS;
+                    const double sl = S1[np] - S1[e], sm = S1[e] - S1[h];
+                    const double panel = cost.ns_per_panel_value * (sl * nb + sm * (nbh + 0.5 * nbm + 0.5)) +
+                                         cost.ns_per_panel_pair * (nl * (double)e + m * (m - 1.0) / 2.0 + m * hh) +
+                                         nb * build_ns;
+                    const double v = tc_ns * hh * (hh - 1.0) / 2.0 + panel + post_est(e);
+                    if (best_b < 0 || v < best_b) {
+                        best_b = v;
+                        best_h = h;
+                        best_m = e - h;
+                    }
+                }
+            }
+        }
+        panel_plan = best_b >= 0 && (panel_mode > 0 || best_b < best_a);
+        std::vector<uint32_t> rest;
+        if (panel_plan) {
+            dense.assign(pl.begin(), pl.begin() + best_h);
+            mrows.assign(pl.begin() + best_h, pl.begin() + best_h + best_m);
+            rest.assign(pl.begin() + best_h + best_m, pl.end());
+        } else {
+            dense.assign(pl.begin(), pl.begin() + best_k);
+            rest.assign(pl.begin() + best_k, pl.end());
+        }
+        std::sort(rest.begin(), rest.end());               // stored order: ascending output writes
         if (rest.size() >= 2) {
             ps = histogram(rest);
             // The estimate assumes independent rows; correlated rows share
             // more. With the exact count, keep the postings only if they beat
-            // the tensor cores on these pairs.
+            // the alternative on these pairs: the panel (the rows queried
+            // against themselves) or the tensor cores.
             const double q = (double)rest.size();
-            const double tens_rest = tc_ns * (q * (q - 1.0) / 2.0);
-            if (ps.entries < (1ull << 32) && (postings_mode > 0 || post_ns((double)ps.pairs, rest.size()) < tens_rest)) qrows = rest;
-            else dense.insert(dense.end(), rest.begin(), rest.end());
+            const double alt = panel_plan ? cost.ns_per_panel_value * (S1[np] - S1[np - rest.size()]) *
+                                                (0.5 * std::ceil(q / PANEL_ROWS) + 0.5) +
+                                                cost.ns_per_panel_pair * q * (q - 1.0) / 2.0
+                                          : tc_ns * (q * (q - 1.0) / 2.0);
+            if (ps.entries < (1ull << 32) && (postings_mode > 0 || post_ns((double)ps.pairs, rest.size()) < alt)) {
+                qrows = rest;
+            } else if (panel_plan) {
+                mrows.insert(mrows.end(), rest.begin(), rest.end());
+            } else {
+                dense.insert(dense.end(), rest.begin(), rest.end());
+            }
+        } else if (panel_plan) {
+            mrows.insert(mrows.end(), rest.begin(), rest.end());
         } else {
             dense.insert(dense.end(), rest.begin(), rest.end());
         }
@@ -835,13 +968,22 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
             if (ps.entries < (1ull << 32) && (postings_mode > 0 || post_ns((double)ps.pairs, rest.size()) < alt)) qrows = rest;
         }
     }
-    // The tensor cores take D x D and D x Q: expanded rows in the order
-    // [D | padding to a multiple of 256 | Q], so that every 128-row and
-    // 256-row block is all D or all Q and the Q x Q blocks can be left out.
+    if (panel_plan && mrows.empty() && dense.empty()) panel_plan = false;
+    // Rows the tensor cores expand behind the H rows: the L rows in the plan
+    // without a panel (H x L on the tensor cores), none with it.
+    const std::vector<uint32_t> none;
+    const std::vector<uint32_t>& tq = panel_plan ? none : qrows;
+    // The tensor cores take H x H (and H x tq): expanded rows in the order
+    // [H | padding to a multiple of 256 | tq], so that every 128-row and
+    // 256-row block is all H or all tq and the tq x tq blocks can be left out.
     // Panels of P rows when they do not all fit the budget.
+    if (panel_plan) {
+        d_pX.reserve(PANEL_ROWS * W);
+        d_DT.reserve(PANEL_ROWS * W);
+    }
     const uint64_t nd0 = dense.size();
     const uint64_t nd_pad = round_up(nd0, 256);
-    const uint64_t ne = nd0 ? nd_pad + qrows.size() : 0;
+    const uint64_t ne = nd0 ? nd_pad + tq.size() : 0;
     uint64_t P = 0;
     if (ne) {
         uint64_t budget = dense_budget_bytes;
@@ -852,21 +994,23 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         }
         const uint64_t cap_rows = budget / (W * sizeof(uint64_t));
         P = round_up(ne, 256) <= cap_rows ? round_up(ne, 256) : cap_rows / 2 / 256 * 256;
-        if (P == 0) {   // not even two panels fit: the D rows go to the chunk kernel
+        if (P == 0) {   // not even two panels fit: the H rows go to the chunk kernel (or the panel)
+            if (panel_plan) mrows.insert(mrows.end(), dense.begin(), dense.end());
             dense.clear();
         }
     }
     for (uint32_t r : qrows) cls[r] = 1;
-    for (uint32_t r : dense) cls[r] = 2;
-    // Walk order: C rows, then Q rows, then D rows.
+    for (uint32_t r : mrows) cls[r] = 2;
+    for (uint32_t r : dense) cls[r] = 3;
+    // Walk order: C, L, M, H rows.
     std::vector<uint32_t> h_perm;
     h_perm.reserve(n);
-    for (int k = 0; k < 3; ++k)
+    for (int k = 0; k < 4; ++k)
         for (uint32_t r = 0; r < n; ++r)
             if (cls[r] == k) h_perm.push_back(r);
-    const uint64_t nd = dense.size(), nq = qrows.size(), nc = n - nd - nq;
+    const uint64_t nd = dense.size(), nq = qrows.size(), nm = mrows.size(), nc = n - nd - nq - nm;
     const uint32_t* perm = nullptr;
-    if (nd || nq) {
+    if (nd || nq || nm) {
         d_perm.reserve(n);
         SB_CUDA(cudaMemcpyAsync(d_perm.p, h_perm.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
         perm = d_perm.p;
@@ -874,11 +1018,11 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         if (d_out) SB_CUDA(cudaMemsetAsync(d_out, 0, tri_size(n) * sizeof(uint32_t), st));
     }
 
-    // ---- tensor cores: D x D and D x Q, panel by panel
+    // ---- tensor cores: H x H and H x tq, panel by panel
     if (nd) {
-        std::vector<uint32_t> emap(nd_pad + nq, ~0u);    // expanded row -> stored row (~0: padding)
+        std::vector<uint32_t> emap(nd_pad + tq.size(), ~0u);   // expanded row -> stored row (~0: padding)
         std::copy(dense.begin(), dense.end(), emap.begin());
-        std::copy(qrows.begin(), qrows.end(), emap.begin() + nd_pad);
+        std::copy(tq.begin(), tq.end(), emap.begin() + nd_pad);
         const uint64_t ne2 = emap.size();
         const bool single = P >= round_up(ne2, 256);
         const uint64_t rows_alloc = single ? P : 2 * P;
@@ -906,10 +1050,10 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         };
         for (uint64_t I = 0; I < npan; ++I) {
             const uint64_t gI = I * P, mI = std::min<uint64_t>(P, ne2 - gI);
-            if (is_q(gI)) break;                          // this and later panels are all Q
+            if (is_q(gI)) break;                          // this and later panels are all tq
             expand(gI, mI, 0);
             std::vector<uint2> tri;
-            build_mma_tiles(tri, mI);                      // I x I triangle, Q x Q blocks left out
+            build_mma_tiles(tri, mI);                      // I x I triangle, tq x tq blocks left out
             tl.clear();
             for (const uint2& t : tri)
                 if (!(is_q(gI + (uint64_t)t.x * 128) && is_q(gI + (uint64_t)t.y * 256))) tl.push_back(t);
@@ -932,7 +1076,60 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
     }
     // ---- chunk kernel: every pair with a C row (the walk's triangle prefix)
     chunk_launch(PAIRS_TRIANGLE, nc * n - (nc * (nc - 1)) / 2 * (nc ? 1 : 0), perm, 0, 0, n, 0);
-    // ---- Q x Q by postings
+    // ---- transposed panel: (L u M) x (M u H), blocks of PANEL_ROWS panel rows
+    if (panel_plan && (nm || nd) && (nq + nm)) {
+        const uint64_t pw0 = nc + nq;                      // walk position of the first panel row
+        const uint64_t npw = nm + nd;
+        // query rows (walk positions of L and M), heaviest first
+        std::vector<uint32_t> xo;
+        xo.reserve(nq + nm);
+        uint64_t max_card = 0;
+        for (uint64_t w = nc; w < nc + nq + nm; ++w) {
+            xo.push_back((uint32_t)w);
+            max_card = std::max<uint64_t>(max_card, d.facts[h_perm[w]].card);
+        }
+        std::stable_sort(xo.begin(), xo.end(), [&](uint32_t x, uint32_t y) {
+            return d.facts[h_perm[x]].card > d.facts[h_perm[y]].card;
+        });
+        d_xorder.reserve(xo.size());
+        d_ctr.reserve(1);
+        d_pmap.reserve(PANEL_ROWS);
+        SB_CUDA(cudaMemcpyAsync(d_xorder.p, xo.data(), xo.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        static std::atomic<uint64_t> t_done{0};
+        smem_attr_once(panel_transpose_kernel, (int)PANEL_T_SMEM, t_done);
+        std::vector<uint32_t> bmap(PANEL_ROWS);
+        const uint32_t qgrid = (uint32_t)sms * 8;
+        for (uint64_t b0 = 0; b0 < npw; b0 += PANEL_ROWS) {
+            const uint32_t prows = (uint32_t)std::min<uint64_t>(PANEL_ROWS, npw - b0);
+            for (uint32_t t = 0; t < PANEL_ROWS; ++t) bmap[t] = t < prows ? h_perm[pw0 + b0 + t] : ~0u;
+            SB_CUDA(cudaMemcpyAsync(d_pmap.p, bmap.data(), PANEL_ROWS * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+            expand_rows_kernel<<<(uint32_t)std::min<uint64_t>(PANEL_ROWS, (uint64_t)sms * 16), EXPAND_WARPS * 32, 0,
+                                 st>>>(d.view(), d_pmap.p, PANEL_ROWS, (uint32_t)W, d_pX.p);
+            panel_transpose_kernel<<<(uint32_t)(W / PANEL_T_WORDS), 1024, PANEL_T_SMEM, st>>>(d_pX.p, W, d_DT.p);
+            SB_CUDA(cudaMemsetAsync(d_ctr.p, 0, sizeof(unsigned long long), st));
+            const uint32_t nx = (uint32_t)xo.size();
+            if (max_card < (1ull << 11))
+                panel_query_kernel<8><<<qgrid, PANEL_Q_WARPS * 32, 0, st>>>(d.view(), perm, d_xorder.p, nx, pw0 + b0,
+                                                                            prows, d_DT.p, n, d_out, d_flags.p, d_ctr.p);
+            else if (max_card < (1ull << 15))
+                panel_query_kernel<12><<<qgrid, PANEL_Q_WARPS * 32, 0, st>>>(d.view(), perm, d_xorder.p, nx, pw0 + b0,
+                                                                             prows, d_DT.p, n, d_out, d_flags.p, d_ctr.p);
+            else if (max_card < (1ull << 19))
+                panel_query_kernel<16><<<qgrid, PANEL_Q_WARPS * 32, 0, st>>>(d.view(), perm, d_xorder.p, nx, pw0 + b0,
+                                                                             prows, d_DT.p, n, d_out, d_flags.p, d_ctr.p);
+            else if (max_card < (1ull << 23))
+                panel_query_kernel<20><<<qgrid, PANEL_Q_WARPS * 32, 0, st>>>(d.view(), perm, d_xorder.p, nx, pw0 + b0,
+                                                                             prows, d_DT.p, n, d_out, d_flags.p, d_ctr.p);
+            else
+                panel_query_kernel<24><<<qgrid, PANEL_Q_WARPS * 32, 0, st>>>(d.view(), perm, d_xorder.p, nx, pw0 + b0,
+                                                                             prows, d_DT.p, n, d_out, d_flags.p, d_ctr.p);
+            SB_CUDA(cudaGetLastError());
+            launches += 3;
+        }
+        last_panel_rows = npw;
+        last_panel_queries = nq + nm;
+    }
+    // ---- L x L by postings
     uint64_t q_sum = 0;
     if (nq) {
         q_sum = ps.pairs;
@@ -965,14 +1162,16 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         }
         last_postings_rows = nq;
     }
-    SB_CUDA(cudaEventRecord(log.ev1, st));
-    DeviceFlags f;
-    SB_CUDA(cudaMemcpyAsync(&f, d_flags.p, sizeof(f), cudaMemcpyDeviceToHost, st));
-    SB_CUDA(cudaStreamSynchronize(st));
-    if (f.error) fail(STORM_B200_ETIMEOUT, "tensor-core dense block: a pipeline wait timed out");
-    SB_CUDA(cudaEventElapsedTime(&log.last_ms, log.ev0, log.ev1));
-    log.launches = launches;
-    return f.sum + q_sum;
+    // ---- diagonal of the M rows (no other engine pairs them with themselves)
+    if (nm && d_out) {
+        d_mrows.reserve(nm);
+        SB_CUDA(cudaMemcpyAsync(d_mrows.p, h_perm.data() + nc + nq, nm * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        row_card_diag_kernel<<<(uint32_t)std::min<uint64_t>((nm + 7) / 8, (uint64_t)sms * 16), 256, 0, st>>>(
+            d.view(), d_mrows.p, (uint32_t)nm, n, d_out);
+        SB_CUDA(cudaGetLastError());
+        ++launches;
+    }
+    return finish(q_sum);
 }
 
 }  // namespace sb200

@@ -149,6 +149,9 @@ struct ChunkCostModel {
     double ns_per_posting_sweep = 0.016;     // the same in the row sweep (shared memory)
     double ns_per_sweep_row_pair = 0.0047;   // row sweep: clearing and writing, per (row, row)
     double ns_per_universe_value = 2e-4;     // histogram clear + scan per universe value
+    double ns_per_panel_value = 0.05;        // transposed panel: one query value against one 2048-row block
+    double ns_per_panel_pair = 0.005;        // transposed panel: one count written
+    double ns_per_panel_byte = 1.0 / 6000.0; // transposed panel: expansion and transpose traffic
 };
 double chunk_self_pair_ns(const ChunkCostModel& m, const ChunkRowFacts& f, uint64_t slots);
 double tensor_pair_ns(const ChunkCostModel& m, uint64_t slots);
@@ -173,7 +176,13 @@ struct ChunkEngine {
     uint64_t dense_budget_bytes = 0;   // 0: 60 % of free device memory
     int postings_mode = -1;            // -1 by cost, 0 never, 1 always (when the rows qualify);
                                        // 2 / 3 always, per-pair form list by list / row sweep
+    int panel_mode = -1;               // transposed panel: -1 by cost, 0 never, 1 whenever it can run,
+                                       // 2 every plain row in it
     uint64_t last_dense_rows = 0, last_dense_panels = 0, last_postings_rows = 0;
+    uint64_t last_panel_rows = 0, last_panel_queries = 0;
+    DevBuf<uint64_t> d_pX, d_DT;       // panel block: expanded rows, transposed
+    DevBuf<uint32_t> d_xorder, d_pmap, d_mrows;
+    DevBuf<unsigned long long> d_ctr;
     DevBuf<uint32_t> d_perm, d_map;
     DevBuf<uint32_t> d_qrows, d_counts, d_start, d_post;
     DevBuf<uint2> d_lists;

@@ -16,8 +16,11 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <mutex>
+#include <thread>
 #include <unordered_map>
+#include <vector>
 
 #include <cmath>
 #include "chunk_engine.cuh"
@@ -470,6 +473,103 @@ int STORM_add(STORM_t* s, const uint32_t* values, const uint32_t n_values) {
     return 1;
 }
 
+// n_rows STORM_add calls at once: the row array grows once, then the rows
+// are split into chunks on several host threads (each row is its own
+// STORM_bitmap_cont_t, so threads never share one).
+int64_t STORM_add_rows(STORM_t* s, const uint32_t* values, const uint64_t* offsets, uint64_t n_rows) {
+    if (s == NULL) return STORM_B200_ENULL;
+    if (n_rows == 0) return 0;
+    if (offsets == NULL || (values == NULL && offsets[n_rows] > offsets[0])) return STORM_B200_EVALUES;
+    for (uint64_t r = 0; r < n_rows; ++r)
+        if (offsets[r + 1] < offsets[r] || offsets[r + 1] - offsets[r] > 0xFFFFFFFFull) return STORM_B200_EARG;
+    if ((uint64_t)s->n_conts + n_rows > 0xFFFFFFFFull) return STORM_B200_ELIMIT;
+    invalidate(s);
+    const uint64_t need = (uint64_t)s->n_conts + n_rows;
+    if (need > s->m_conts) {
+        const uint64_t m = (need + 1023) / 1024 * 1024;
+        if (m > 0xFFFFFFFFull) return STORM_B200_ELIMIT;
+        STORM_bitmap_cont_t* nc = (STORM_bitmap_cont_t*)realloc(s->conts, m * sizeof(STORM_bitmap_cont_t));
+        if (!nc) return STORM_B200_ENOMEM;
+        for (uint64_t i = s->m_conts; i < m; ++i) STORM_bitmap_cont_init(&nc[i]);
+        s->conts = nc;
+        s->m_conts = (uint32_t)m;
+    }
+    const uint32_t first = s->n_conts;
+    std::atomic<int> failed{0};
+    auto fill = [&](uint64_t r0, uint64_t r1) {
+        for (uint64_t r = r0; r < r1; ++r) {
+            const uint64_t a = offsets[r], b = offsets[r + 1];
+            if (STORM_bitmap_cont_add(&s->conts[first + r], b > a ? values + a : values, (uint32_t)(b - a)) < 0)
+                failed.store(1);
+        }
+    };
+    const uint64_t total = offsets[n_rows] - offsets[0];
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const uint64_t n_thr = std::min<uint64_t>({(uint64_t)std::min(hw, 64u), n_rows, 1 + total / (1u << 20)});
+    if (n_thr <= 1) {
+        fill(0, n_rows);
+    } else {
+        // contiguous row ranges of about equal value counts
+        std::vector<uint64_t> cut{0};
+        for (uint64_t r = 0; r < n_rows && cut.size() < n_thr; ++r)
+            if ((offsets[r + 1] - offsets[0]) * n_thr >= total * cut.size()) cut.push_back(r + 1);
+        if (cut.back() != n_rows) cut.push_back(n_rows);
+        std::vector<std::thread> th;
+        for (size_t t = 0; t + 1 < cut.size(); ++t)
+            if (cut[t] < cut[t + 1]) th.emplace_back(fill, cut[t], cut[t + 1]);
+        for (auto& t : th) t.join();
+    }
+    s->n_conts = (uint32_t)need;
+    return failed.load() ? STORM_B200_ENOMEM : (int64_t)n_rows;
+}
+
+// Rows given as bitmaps: each row's set positions, ascending, through the
+// same chunk split as STORM_add, one host thread per range of rows.
+int64_t STORM_add_bitmap_rows(STORM_t* s, const uint64_t* words, uint64_t n_rows, uint64_t words_per_row) {
+    if (s == NULL) return STORM_B200_ENULL;
+    if (n_rows == 0) return 0;
+    if (words == NULL) return STORM_B200_EVALUES;
+    if (words_per_row == 0 || words_per_row > (1ull << 26)) return STORM_B200_EARG;   // positions < 2^32
+    if ((uint64_t)s->n_conts + n_rows > 0xFFFFFFFFull) return STORM_B200_ELIMIT;
+    invalidate(s);
+    const uint64_t need = (uint64_t)s->n_conts + n_rows;
+    if (need > s->m_conts) {
+        const uint64_t m = (need + 1023) / 1024 * 1024;
+        if (m > 0xFFFFFFFFull) return STORM_B200_ELIMIT;
+        STORM_bitmap_cont_t* nc = (STORM_bitmap_cont_t*)realloc(s->conts, m * sizeof(STORM_bitmap_cont_t));
+        if (!nc) return STORM_B200_ENOMEM;
+        for (uint64_t i = s->m_conts; i < m; ++i) STORM_bitmap_cont_init(&nc[i]);
+        s->conts = nc;
+        s->m_conts = (uint32_t)m;
+    }
+    const uint32_t first = s->n_conts;
+    std::atomic<int> failed{0};
+    auto fill = [&](uint64_t r0, uint64_t r1) {
+        std::vector<uint32_t> pos;
+        for (uint64_t r = r0; r < r1; ++r) {
+            const uint64_t* w = words + r * words_per_row;
+            pos.clear();
+            for (uint64_t k = 0; k < words_per_row; ++k)
+                for (uint64_t x = w[k]; x; x &= x - 1) pos.push_back((uint32_t)(k * 64 + __builtin_ctzll(x)));
+            if (STORM_bitmap_cont_add(&s->conts[first + r], pos.empty() ? nullptr : pos.data(),
+                                      (uint32_t)pos.size()) < 0 && !pos.empty())
+                failed.store(1);
+        }
+    };
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const uint64_t n_thr = std::min<uint64_t>({(uint64_t)std::min(hw, 64u), n_rows,
+                                               1 + n_rows * words_per_row / (1u << 17)});
+    if (n_thr <= 1) {
+        fill(0, n_rows);
+    } else {
+        std::vector<std::thread> th;
+        for (uint64_t t = 0; t < n_thr; ++t) th.emplace_back(fill, n_rows * t / n_thr, n_rows * (t + 1) / n_thr);
+        for (auto& t : th) t.join();
+    }
+    s->n_conts = (uint32_t)need;
+    return failed.load() ? STORM_B200_ENOMEM : (int64_t)n_rows;
+}
+
 int STORM_clear(STORM_t* s) {
     if (s == NULL) return -1;
     invalidate(s);
@@ -542,6 +642,20 @@ int STORM_pairw_intersect_matrix(STORM_t* s, uint32_t* out, uint64_t out_len, ui
             SB_CUDA(cudaMemcpyAsync(out, d->d_out.p, need * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
             SB_CUDA(cudaStreamSynchronize(st));
         }
+        if (sum) *sum = r;
+        return 0;
+    });
+}
+
+int STORM_pairw_intersect_matrix_device(STORM_t* s, uint32_t* d_out, uint64_t out_len, uint64_t* sum) {
+    if (s == NULL) return STORM_B200_ENULL;
+    if (d_out && out_len < tri_size(s->n_conts)) return STORM_B200_ESIZE;
+    return guard([&]() -> int {
+        StormDev* d = state_of(s);
+        ensure_packed(s, d);
+        // The caller's buffer may still be in use by work on other streams.
+        if (d_out) SB_CUDA(cudaDeviceSynchronize());
+        const uint64_t r = d->engine.run(d->dev, PAIRS_TRIANGLE, s->n_conts, 0, d_out, stream_of(d));
         if (sum) *sum = r;
         return 0;
     });
@@ -660,5 +774,14 @@ int STORM_set_sparse_postings(STORM_t* s, int mode) {
 }
 
 uint64_t STORM_last_postings_rows(const STORM_t* s) { return s ? state_of(s)->engine.last_postings_rows : 0; }
+
+int STORM_set_panel(STORM_t* s, int mode) {
+    if (s == NULL) return STORM_B200_ENULL;
+    if (mode < -1 || mode > 2) return STORM_B200_EARG;
+    state_of(s)->engine.panel_mode = mode;
+    return 0;
+}
+
+uint64_t STORM_last_panel_rows(const STORM_t* s) { return s ? state_of(s)->engine.last_panel_rows : 0; }
 
 }  // extern "C"

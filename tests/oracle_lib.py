@@ -50,6 +50,10 @@ def oracle():
         "oracle_complement": (C.c_uint64, [u32p, C.c_uint64, C.c_uint32, u32p]),
         "oracle_contig_row": (C.c_uint64, [u64p, C.c_uint64, C.c_uint64, C.c_uint64, u32p]),
         "oracle_row_popcounts": (None, [u64p, C.c_uint64, C.c_uint64, u32p]),
+        "oracle_strip_new": (C.c_void_p, [u32p, u64p, C.c_uint32, C.c_uint64]),
+        "oracle_strip_count": (None, [C.c_void_p, u32p, u64p, C.c_uint64, u32p]),
+        "oracle_strip_free": (None, [C.c_void_p]),
+        "oracle_contig_strip": (None, [u64p, C.c_uint32, u64p, C.c_uint64, C.c_uint64, u32p]),
     }
     for k, (r, a) in sigs.items():
         f = getattr(L, k)
@@ -158,3 +162,72 @@ def threshold_pairs(tri: np.ndarray, n: int, t: float):
     with np.errstate(divide="ignore", invalid="ignore"):
         ok = (c > 0) & (u > 0) & (c / np.where(u > 0, u, 1.0) >= t)
     return i[ok].astype(np.uint32), j[ok].astype(np.uint32), c[ok].astype(np.uint32)
+
+
+class SetStrip:
+    """Whole rows of the per-pair matrix for up to 8 query rows, counted
+    against row batches streamed through count() (several host threads at
+    once, one batch each): oracle_strip_* of oracle/storm_oracle.c."""
+
+    def __init__(self, queries, universe: int):
+        L = oracle()
+        qv = np.ascontiguousarray(np.concatenate(queries) if len(queries) else np.zeros(0), dtype=np.uint32)
+        qo = np.zeros(len(queries) + 1, np.uint64)
+        qo[1:] = np.cumsum([len(q) for q in queries])
+        self.nq = len(queries)
+        self.h = L.oracle_strip_new(_p(qv, u32p), _p(qo, u64p), self.nq, universe)
+        if not self.h:
+            raise ValueError("oracle_strip_new: 1..8 query rows")
+
+    def count(self, vals: np.ndarray, offs: np.ndarray, threads: int = 1) -> np.ndarray:
+        """[n_rows, nq] counts for the CSR batch (vals u32, offs u64 from 0)."""
+        import concurrent.futures as cf
+        vals = np.ascontiguousarray(vals, dtype=np.uint32)
+        offs = np.ascontiguousarray(offs, dtype=np.uint64)
+        n = len(offs) - 1
+        out = np.zeros((n, self.nq), np.uint32)
+        L = oracle()
+        cuts = np.linspace(0, n, max(1, min(threads, n)) + 1).astype(np.int64)
+
+        def part(a, b):
+            if b > a:
+                L.oracle_strip_count(self.h, _p(vals, u32p), offs[a:].ctypes.data_as(u64p), b - a,
+                                     out[a:].ctypes.data_as(u32p))
+
+        with cf.ThreadPoolExecutor(max_workers=len(cuts) - 1) as ex:
+            list(ex.map(lambda k: part(int(cuts[k]), int(cuts[k + 1])), range(len(cuts) - 1)))
+        return out
+
+    def close(self):
+        if self.h:
+            oracle().oracle_strip_free(self.h)
+            self.h = None
+
+
+class BitmapStrip:
+    """Whole rows of the per-pair matrix for query rows given as packed
+    bitmaps, counted against bitmap row batches (oracle_contig_strip)."""
+
+    def __init__(self, qwords: np.ndarray):
+        self.q = np.ascontiguousarray(qwords, dtype=np.uint64)
+        self.nq = self.q.shape[0]
+
+    def count(self, words: np.ndarray, offs=None, threads: int = 1) -> np.ndarray:
+        import concurrent.futures as cf
+        words = np.ascontiguousarray(words, dtype=np.uint64)
+        n, nw = words.shape
+        out = np.zeros((n, self.nq), np.uint32)
+        L = oracle()
+        cuts = np.linspace(0, n, max(1, min(threads, n)) + 1).astype(np.int64)
+
+        def part(a, b):
+            if b > a:
+                L.oracle_contig_strip(_p(self.q, u64p), self.nq, words[a:].ctypes.data_as(u64p), b - a, nw,
+                                      out[a:].ctypes.data_as(u32p))
+
+        with cf.ThreadPoolExecutor(max_workers=len(cuts) - 1) as ex:
+            list(ex.map(lambda k: part(int(cuts[k]), int(cuts[k + 1])), range(len(cuts) - 1)))
+        return out
+
+    def close(self):
+        pass

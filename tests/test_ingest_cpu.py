@@ -72,3 +72,76 @@ def test_storm_add_matches_reference_structs(sb):
         finally:
             R.STORM_free(hr)
             L.STORM_free(hl)
+
+
+def test_add_rows_builds_what_add_builds(sb):
+    """STORM_add_rows (rows split on several host threads) leaves exactly the
+    public structs that one STORM_add per row leaves -- empty rows, sorted,
+    unsorted and repeated values included -- appended after existing rows."""
+    L = sb.lib()
+    L.STORM_new.restype = C.c_void_p
+    L.STORM_add.argtypes = [C.c_void_p, sb.u32p, C.c_uint32]
+    L.STORM_free.argtypes = [C.c_void_p]
+    g = np.random.default_rng(77)
+    rows = []
+    for r in range(3000):
+        kind, n = int(g.integers(0, 5)), int(g.integers(0, 9000))
+        if kind == 0:
+            v = np.sort(g.integers(0, 1 << 20, n))
+        elif kind == 1:
+            v = np.sort(g.choice(1 << 18, size=min(n * 8, 1 << 17), replace=False))
+        elif kind == 2:
+            v = g.integers(0, 1 << 20, n)
+        elif kind == 3:
+            v = np.sort(np.repeat(g.integers(0, 1 << 19, n // 3 + 1), 3))
+        else:
+            v = np.zeros(0)
+        rows.append(np.ascontiguousarray(v, dtype=np.uint32))
+    one, bulk = L.STORM_new(), L.STORM_new()
+    try:
+        head = rows[:7]
+        for v in rows:
+            assert L.STORM_add(one, v.ctypes.data_as(sb.u32p), v.size) == 1
+        for v in head:   # rows already present before the bulk call
+            L.STORM_add(bulk, v.ctypes.data_as(sb.u32p), v.size)
+        rest = rows[7:]
+        vals = np.ascontiguousarray(np.concatenate(rest), dtype=np.uint32)
+        offs = np.zeros(len(rest) + 1, np.uint64)
+        offs[1:] = np.cumsum([len(v) for v in rest])
+        assert L.STORM_add_rows(bulk, vals.ctypes.data_as(sb.u32p), offs.ctypes.data_as(sb.u64p), len(rest)) == len(rest)
+        assert _dump(bulk) == _dump(one)
+        bad = np.array([0, 5, 3], np.uint64)
+        assert L.STORM_add_rows(bulk, vals.ctypes.data_as(sb.u32p), bad.ctypes.data_as(sb.u64p), 2) == sb.EARG
+        assert L.STORM_add_rows(None, vals.ctypes.data_as(sb.u32p), offs.ctypes.data_as(sb.u64p), 1) == sb.ENULL
+    finally:
+        L.STORM_free(one)
+        L.STORM_free(bulk)
+
+
+def test_add_bitmap_rows_builds_what_add_builds(sb):
+    """STORM_add_bitmap_rows leaves the public structs that STORM_add of each
+    row's set positions leaves: empty rows, list chunks, bitmap chunks and a
+    partial last chunk."""
+    import gen
+    L = sb.lib()
+    L.STORM_new.restype = C.c_void_p
+    L.STORM_add.argtypes = [C.c_void_p, sb.u32p, C.c_uint32]
+    L.STORM_free.argtypes = [C.c_void_p]
+    g = np.random.default_rng(5)
+    m = 3 * 65536 + 4096 + 64 * 7        # three whole chunks and a partial one
+    nw = (m + 63) // 64
+    words = np.zeros((40, nw), np.uint64)
+    for r in range(40):
+        p = [0.0, 1e-4, 0.03, 0.3][r % 4]
+        bits = g.random(m) < p
+        words[r] = gen.pack_bool_rows(bits[None, :])[0]
+    one, bulk = L.STORM_new(), L.STORM_new()
+    try:
+        for v in gen.rows_to_sets(words, m):
+            v = np.ascontiguousarray(v, dtype=np.uint32)
+            L.STORM_add(one, v.ctypes.data_as(sb.u32p), v.size)
+        assert L.STORM_add_bitmap_rows(bulk, words.ctypes.data_as(sb.u64p), 40, nw) == 40
+        assert _dump(bulk) == _dump(one)
+    finally:
+        L.STORM_free(one)
+        L.STORM_free(bulk)

@@ -38,6 +38,31 @@ def test_oracle_sets_match_reference(golden):
         np.testing.assert_array_equal(mat[strict], golden[f"storm/{name}/matrix"][strict], err_msg=name)
 
 
+def test_oracle_strips_match_reference(golden):
+    """oracle_strip_* (whole rows of the matrix for a few query rows, rows
+    streamed in batches on several threads) equals the reference's per-pair
+    counts i < j on every golden set corpus, for query rows at the start, in
+    the middle and at the end."""
+    for name in storm_cases(golden):
+        vals, offs = golden[f"storm/{name}/vals"], golden[f"storm/{name}/offs"]
+        n = len(offs) - 1
+        full = golden[f"storm/{name}/matrix"]
+        sets = gen.from_csr(vals, offs)
+        q = sorted({0, n // 2, n - 1})
+        universe = int(vals.max()) + 1 if vals.size else 1
+        st = ol.SetStrip([sets[i] for i in q], universe)
+        got = np.concatenate([st.count(vals[int(offs[a]):], offs[a:b + 1] - offs[a], threads=3)
+                              for a, b in ((0, n // 3), (n // 3, n))])
+        st.close()
+        for k, i in enumerate(q):
+            for j in range(n):
+                if i == j:
+                    assert got[j, k] == len(sets[i])
+                    continue
+                a, b = min(i, j), max(i, j)
+                assert got[j, k] == full[a * n - (a * (a - 1)) // 2 + (b - a)], (name, i, j)
+
+
 def test_oracle_chunk_by_chunk_matches_reference(golden):
     """oracle_storm_matrix (STORM_t counted chunk by chunk, as the reference
     counts it) equals the golden matrices and sums, and -- on rows with
