@@ -50,6 +50,16 @@ const char* STORM_b200_strerror(int status);
  * for a NULL STORM_t, exactly as the reference does). */
 int STORM_b200_last_status(void);
 
+/* Failure detection, exercised without a fault (no counterpart in the
+ * reference): runs the bounded mbarrier wait of the tensor-core kernels on a
+ * barrier nothing arrives on, with a limit of limit_us microseconds (1 ..
+ * 10,000,000), in a kernel that holds tensor memory as they do.  When the
+ * wait gives up the kernel records where, frees its tensor memory and
+ * returns, and this call returns STORM_B200_ETIMEOUT -- the status every
+ * all-pairs call returns when one of its waits gives up -- with the context
+ * still usable.  Returns 0 if the wait did not give up. */
+int STORM_b200_wait_selftest(uint32_t limit_us);
+
 /* Packed upper-triangle index of pair (i, j), i <= j < n. */
 static inline uint64_t STORM_tri_index(uint64_t n, uint64_t i, uint64_t j) {
     /* rows 0..i-1 hold n, n-1, ..., n-i+1 entries; i*(i-1) is even */

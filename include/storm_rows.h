@@ -157,8 +157,35 @@ int64_t STORM_rows_cell(STORM_rows_t* r, int pairing, uint64_t row_a, uint64_t r
  * regret of the MLP on held-out tiles, regret of the cost model there. */
 int STORM_rows_train_selector(STORM_rows_t* r, uint32_t tile, uint32_t samples, uint32_t epochs,
                               uint64_t seed, double* stats);
+/* The selector's training also fits this container's cost model to the
+ * cell timings of its training tiles (as STORM_rows_calibrate does), so
+ * the cost-model policies and the untrained/fallback selector price cells
+ * with this GPU's constants from then on; stats[5] is the regret of that
+ * calibrated model.  STORM_rows_last_training reports the last training:
+ * out8 = regret of the MLP, of the calibrated model and of the reference's
+ * default model on the held-out tiles, held-out and training tile counts,
+ * the calibration's relative RMS error, its fixed term, sampled tiles. */
+int STORM_rows_last_training(const STORM_rows_t* r, double* out8);
 /* Reset to the untrained (cost-model fallback) selector. */
 int STORM_rows_reset_selector(STORM_rows_t* r);
+
+/* GPU calibration of the cost model (the reference's calibrate /
+ * calibrate_on_rows, storm_cost.cpp:556-769, 779-895, which time each cell
+ * on the host CPU): every cell is timed on this GPU (SM clock) on sampled
+ * tiles of r's own rows -- tile rows of the density order, `samples` tiles
+ * (0: all), seeded -- and the model keeps the reference's work formulas with
+ * constants fitted to those timings: cycles(tile, cell) ~ a_cell x (the
+ * reference default model's prediction above its fixed term) + f x pairs,
+ * one weighted least-squares fit (relative error).  The result replaces r's
+ * cost model (the cost-model policies and the untrained learned policy use
+ * it; counts never depend on it).  model_out (14 entries, may be NULL):
+ * ns_per_unit[11] and the fixed and zone-map-word terms in SM cycles, then
+ * the fit's relative RMS error.  No counterpart in the reference's C ABI. */
+int STORM_rows_calibrate(STORM_rows_t* r, uint32_t tile, uint32_t samples, uint64_t seed, double* model_out);
+/* r's cost model: set = 0 copies it into model[13] (ns_per_unit[11], fixed,
+ * zone-map word) and returns 1 when calibrated, 0 for the reference default;
+ * set = 1 installs model[13], or the reference default when model is NULL. */
+int STORM_rows_cost_model(STORM_rows_t* r, double* model, int set);
 /* Parameters out/in (so a trained selector can be saved and loaded):
  * n_params floats.  Returns the parameter count when params is NULL. */
 int64_t STORM_rows_selector_params(STORM_rows_t* r, float* params, uint64_t n_params, int load);

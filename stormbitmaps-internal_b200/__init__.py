@@ -51,6 +51,7 @@ def _sig(name, res, args):
 # --- declarations (include/storm.h, include/storm_b200.h) ----------------
 _sig("STORM_b200_strerror", C.c_char_p, [C.c_int])
 _sig("STORM_b200_last_status", C.c_int, [])
+_sig("STORM_b200_wait_selftest", C.c_int, [C.c_uint32])
 _sig("STORM_intersect_vector16_cardinality", C.c_uint64, [u16p, u16p, C.c_uint32, C.c_uint32])
 _sig("STORM_intersect_vector32_unsafe", C.c_uint64, [u32p, u32p, C.c_uint32, C.c_uint32, u32p])
 _sig("STORM_intersect_bitmaps_scalar_list", C.c_uint64, [u64p, u64p, u32p, u32p, C.c_uint32, C.c_uint32])
@@ -531,6 +532,9 @@ _sig("STORM_rows_cell", C.c_int64, [C.c_void_p, C.c_int, C.c_uint64, C.c_uint64]
 _sig("STORM_rows_train_selector", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
                                             C.POINTER(C.c_double)])
 _sig("STORM_rows_reset_selector", C.c_int, [C.c_void_p])
+_sig("STORM_rows_last_training", C.c_int, [C.c_void_p, C.POINTER(C.c_double)])
+_sig("STORM_rows_calibrate", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(C.c_double)])
+_sig("STORM_rows_cost_model", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int])
 _sig("STORM_rows_selector_params", C.c_int64, [C.c_void_p, C.POINTER(C.c_float), C.c_uint64, C.c_int])
 _sig("STORM_mlp_forward_backward", C.c_int, [C.POINTER(C.c_float), C.c_uint32, C.c_uint32, C.c_uint32,
                                              C.POINTER(C.c_float), C.POINTER(C.c_int32), C.c_uint32,
@@ -662,6 +666,34 @@ class StormRows:
         _check(_lib.STORM_rows_train_selector(self.h, tile, samples, epochs, seed, stats), "STORM_rows_train_selector")
         keys = ["samples", "epochs", "loss", "train_accuracy", "regret_mlp", "regret_cost_model"]
         return dict(zip(keys, list(stats)))
+
+    def last_training(self):
+        out = (C.c_double * 8)()
+        _check(_lib.STORM_rows_last_training(self.h, out), "STORM_rows_last_training")
+        keys = ["regret_mlp", "regret_calibrated_model", "regret_default_model", "test_tiles", "train_tiles",
+                "calibration_rms", "calibrated_fixed_cycles", "sampled_tiles"]
+        return dict(zip(keys, list(out)))
+
+    def calibrate(self, tile=64, samples=0, seed=1):
+        """GPU calibration of the cost model on these rows; returns the model
+        (ns_per_unit[11], fixed, zone-map word, in SM cycles) and the fit's
+        relative RMS error."""
+        out = (C.c_double * 14)()
+        _check(_lib.STORM_rows_calibrate(self.h, tile, samples, seed, out), "STORM_rows_calibrate")
+        return list(out)[:13], float(out[13])
+
+    def cost_model(self, set_to=None, reset=False):
+        """Read the cost model ((model[13], calibrated)) or install one / the default."""
+        if reset:
+            _check(_lib.STORM_rows_cost_model(self.h, None, 1), "STORM_rows_cost_model")
+            return None
+        if set_to is not None:
+            m = (C.c_double * 13)(*[float(x) for x in set_to])
+            _check(_lib.STORM_rows_cost_model(self.h, m, 1), "STORM_rows_cost_model")
+            return None
+        m = (C.c_double * 13)()
+        rc = _check(_lib.STORM_rows_cost_model(self.h, m, 0), "STORM_rows_cost_model")
+        return list(m), bool(rc)
 
     def reset_selector(self):
         _check(_lib.STORM_rows_reset_selector(self.h), "STORM_rows_reset_selector")

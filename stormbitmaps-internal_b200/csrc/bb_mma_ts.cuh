@@ -47,13 +47,13 @@ struct TsCtl {
 };
 
 __device__ __forceinline__ bool ts_wait(uint32_t bar, uint32_t parity, TsCtl* ctl, DeviceFlags* flags,
-                                        uint32_t site, bool drain = false) {
+                                        uint32_t site, bool drain = false, uint64_t limit_ns = WAIT_LIMIT_NS) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = globaltimer_ns();
     for (;;) {
         if (mbar_try_wait(bar, parity)) return true;
         if (!drain && ctl->abort) return false;
-        if (globaltimer_ns() - t0 > WAIT_LIMIT_NS) {
+        if (globaltimer_ns() - t0 > limit_ns) {
             atomicCAS(&flags->error, 0u, site);
             ctl->abort = 1;
             return false;

@@ -452,6 +452,70 @@ extern "C" int STORM_contig_pairw_intersect_matrix_noalloc(const uint64_t* d_row
 }
 
 // ===================================================================
+// Bounded-wait self-test
+//
+// The tensor-core kernels bound every mbarrier wait (ts_wait): when a wait
+// gives up, the kernel records the site in the status word, stops its other
+// roles, frees its tensor memory and returns, and the host call returns
+// STORM_B200_ETIMEOUT with the context still usable.  This kernel runs that
+// path on purpose, on a barrier nothing ever arrives on, with a short limit:
+// warp 1 holds tensor memory as the real kernels do, warp 0's lane 0 waits.
+// ===================================================================
+namespace sb200 {
+
+constexpr uint32_t ERR_SELFTEST = 0x301;
+
+__global__ void __launch_bounds__(64) wait_selftest_kernel(DeviceFlags* flags, uint64_t limit_ns) {
+    __shared__ TsCtl ctl;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        mbar_init(smem_u32(&ctl.full[0]), 1);
+        ctl.abort = 0;
+        fence_barrier_init();
+    }
+    if (warp == 1) {
+        tmem_alloc(smem_u32(&ctl.tmem_base), 32);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0 && lane == 0) ts_wait(smem_u32(&ctl.full[0]), 0, &ctl, flags, ERR_SELFTEST, false, limit_ns);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(ctl.tmem_base, 32);
+    }
+}
+
+}  // namespace sb200
+
+extern "C" int STORM_b200_wait_selftest(uint32_t limit_us) {
+    using namespace sb200;
+    if (limit_us == 0 || limit_us > 10000000u) return STORM_B200_EARG;
+    return guard([&]() -> int {
+        require_device();
+        cudaStream_t st = nullptr;
+        SB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        DevBuf<DeviceFlags> f;
+        f.reserve(1);
+        DeviceFlags h{};
+        cudaError_t e = cudaMemsetAsync(f.p, 0, sizeof(DeviceFlags), st);
+        if (e == cudaSuccess) {
+            wait_selftest_kernel<<<1, 64, 0, st>>>(f.p, (uint64_t)limit_us * 1000ull);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&h, f.p, sizeof(h), cudaMemcpyDeviceToHost, st);
+        const cudaError_t es = cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+        SB_CUDA(e);
+        SB_CUDA(es);
+        return h.error == ERR_SELFTEST ? STORM_B200_ETIMEOUT : 0;
+    });
+}
+
+// ===================================================================
 // Thresholded output
 // ===================================================================
 namespace sb200 {

@@ -6,6 +6,7 @@
 // program written against storm.h links and gets identical numbers.  The
 // STORM_compute_func / STORM_compute_lfunc arguments select CPU SIMD kernels
 // in the reference and are ignored here.
+#include "oneshot.cuh"
 #include <algorithm>
 #include <vector>
 
@@ -63,23 +64,6 @@ __global__ void rect_sum_kernel(const uint32_t* __restrict__ tri, uint64_t n, ui
     if ((threadIdx.x & 31) == 0 && s) atomicAdd(&flags->sum, s);
 }
 
-struct Scratch {
-    cudaStream_t st = nullptr;
-    Scratch() {
-        require_device();
-        SB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    }
-    ~Scratch() {
-        if (st) cudaStreamDestroy(st);
-    }
-    uint64_t read_sum(DeviceFlags* d) {
-        DeviceFlags f;
-        SB_CUDA(cudaMemcpyAsync(&f, d, sizeof(f), cudaMemcpyDeviceToHost, st));
-        SB_CUDA(cudaStreamSynchronize(st));
-        return f.sum;
-    }
-};
-
 // Upload n rows of n_ints words into a padded dense layout.
 static void upload_dense(DevBuf<uint64_t>& d, const uint64_t* rows, uint64_t n, uint32_t n_ints, uint32_t& w_pad,
                          cudaStream_t st) {
@@ -94,12 +78,10 @@ static void upload_dense(DevBuf<uint64_t>& d, const uint64_t* rows, uint64_t n, 
 
 static uint64_t dense_diag_sum(const uint64_t* vals, uint32_t n, uint32_t n_ints) {
     if (n < 2 || vals == NULL) return 0;
-    Scratch s;
-    DevBuf<uint64_t> d;
+    OneShot& s = one_shot();
     uint32_t w_pad = 0;
-    upload_dense(d, vals, n, n_ints, w_pad, s.st);
-    DenseEngine e;
-    return e.run(d.p, n, w_pad, (uint64_t)n_ints * 64, nullptr, STORM_B200_KERNEL_AUTO, s.st);
+    upload_dense(s.w64, vals, n, n_ints, w_pad, s.st);
+    return s.dense.run(s.w64.p, n, w_pad, (uint64_t)n_ints * 64, nullptr, STORM_B200_KERNEL_AUTO, s.st);
 }
 
 }  // namespace sb200
@@ -121,16 +103,12 @@ uint64_t STORM_intersect_vector16_cardinality(const uint16_t* STORM_RESTRICT v1,
         a.n_scalar = len1;
         b.scalar = const_cast<uint16_t*>(v2);
         b.n_scalar = len2;
-        ChunkPack p;
-        p.add_chunk(0, a);
-        p.end_row();
-        p.add_chunk(0, b);
-        p.end_row();
-        Scratch s;
-        ChunkDev dev;
-        dev.upload(p, s.st);
-        ChunkEngine e;
-        r = e.run(dev, PAIRS_RECT, 1, 1, nullptr, s.st);
+        OneShot& s = one_shot();
+        s.pack.add_chunk(0, a);
+        s.pack.end_row();
+        s.pack.add_chunk(0, b);
+        s.pack.end_row();
+        r = s.rect(1, 1);
         return 0;
     });
     return r;
@@ -142,19 +120,17 @@ uint64_t STORM_intersect_vector32_unsafe(const uint32_t* STORM_RESTRICT v1, cons
     if (len1 == 0 || len2 == 0) return 0;
     uint64_t r = 0;
     guard([&]() -> int {
-        Scratch s;
-        DevBuf<uint32_t> da, db;
-        DevBuf<int64_t> dm;
-        da.reserve(len1);
-        db.reserve(len2);
-        dm.reserve(len1);
-        SB_CUDA(cudaMemcpyAsync(da.p, v1, len1 * sizeof(uint32_t), cudaMemcpyHostToDevice, s.st));
-        SB_CUDA(cudaMemcpyAsync(db.p, v2, len2 * sizeof(uint32_t), cudaMemcpyHostToDevice, s.st));
+        OneShot& s = one_shot();
+        s.u32a.reserve(len1);
+        s.u32b.reserve(len2);
+        s.i64.reserve(len1);
+        SB_CUDA(cudaMemcpyAsync(s.u32a.p, v1, len1 * sizeof(uint32_t), cudaMemcpyHostToDevice, s.st));
+        SB_CUDA(cudaMemcpyAsync(s.u32b.p, v2, len2 * sizeof(uint32_t), cudaMemcpyHostToDevice, s.st));
         const uint32_t grid = std::min<uint32_t>((len1 + 255) / 256, 1024);
-        match32_kernel<<<grid, 256, 0, s.st>>>(da.p, len1, db.p, len2, dm.p);
+        match32_kernel<<<grid, 256, 0, s.st>>>(s.u32a.p, len1, s.u32b.p, len2, s.i64.p);
         SB_CUDA(cudaGetLastError());
         std::vector<int64_t> m(len1);
-        SB_CUDA(cudaMemcpyAsync(m.data(), dm.p, len1 * sizeof(int64_t), cudaMemcpyDeviceToHost, s.st));
+        SB_CUDA(cudaMemcpyAsync(m.data(), s.i64.p, len1 * sizeof(int64_t), cudaMemcpyDeviceToHost, s.st));
         SB_CUDA(cudaStreamSynchronize(s.st));
         // Emit the matched index pairs in the reference's order (ascending A).
         uint64_t k = 0;
@@ -182,19 +158,16 @@ uint64_t STORM_intersect_bitmaps_scalar_list(const uint64_t* STORM_RESTRICT b1, 
         uint32_t mx = 0;
         for (uint32_t i = 0; i < n; ++i) mx = std::max(mx, list[i]);
         const uint64_t words = (uint64_t)(mx >> 6) + 1;   // the bitmap words the probes reach
-        Scratch s;
-        DevBuf<uint64_t> db;
-        DevBuf<uint32_t> dl;
-        DevBuf<DeviceFlags> df;
-        db.reserve(words);
-        dl.reserve(n);
-        df.reserve(1);
-        SB_CUDA(cudaMemcpyAsync(db.p, bm, words * sizeof(uint64_t), cudaMemcpyHostToDevice, s.st));
-        SB_CUDA(cudaMemcpyAsync(dl.p, list, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s.st));
-        SB_CUDA(cudaMemsetAsync(df.p, 0, sizeof(DeviceFlags), s.st));
-        probe_kernel<<<std::min<uint32_t>((n + 255) / 256, 512), 256, 0, s.st>>>(db.p, dl.p, n, df.p);
+        OneShot& s = one_shot();
+        s.w64.reserve(words);
+        s.u32a.reserve(n);
+        s.flags.reserve(1);
+        SB_CUDA(cudaMemcpyAsync(s.w64.p, bm, words * sizeof(uint64_t), cudaMemcpyHostToDevice, s.st));
+        SB_CUDA(cudaMemcpyAsync(s.u32a.p, list, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s.st));
+        SB_CUDA(cudaMemsetAsync(s.flags.p, 0, sizeof(DeviceFlags), s.st));
+        probe_kernel<<<std::min<uint32_t>((n + 255) / 256, 512), 256, 0, s.st>>>(s.w64.p, s.u32a.p, n, s.flags.p);
         SB_CUDA(cudaGetLastError());
-        r = s.read_sum(df.p);
+        r = s.read_sum(s.flags.p);
         return 0;
     });
     return r;
@@ -246,26 +219,22 @@ uint64_t STORM_wrapper_square(const uint32_t n1, const uint64_t* STORM_RESTRICT 
     if (n1 == 0 || n2 == 0 || vals1 == NULL || vals2 == NULL) return 0;
     uint64_t r = 0;
     guard([&]() -> int {
-        Scratch s;
+        OneShot& s = one_shot();
         const uint64_t n = (uint64_t)n1 + n2;
         std::vector<uint64_t> both(n * n_ints);
         std::copy(vals1, vals1 + (uint64_t)n1 * n_ints, both.begin());
         std::copy(vals2, vals2 + (uint64_t)n2 * n_ints, both.begin() + (uint64_t)n1 * n_ints);
-        DevBuf<uint64_t> d;
         uint32_t w_pad = 0;
-        upload_dense(d, both.data(), n, n_ints, w_pad, s.st);
-        DevBuf<uint32_t> tri;
-        tri.reserve(tri_size(n));
-        DenseEngine e;
-        e.run(d.p, n, w_pad, (uint64_t)n_ints * 64, tri.p, STORM_B200_KERNEL_AUTO, s.st);
-        DevBuf<DeviceFlags> df;
-        df.reserve(1);
-        SB_CUDA(cudaMemsetAsync(df.p, 0, sizeof(DeviceFlags), s.st));
+        upload_dense(s.w64, both.data(), n, n_ints, w_pad, s.st);
+        s.tri.reserve(tri_size(n));
+        s.dense.run(s.w64.p, n, w_pad, (uint64_t)n_ints * 64, s.tri.p, STORM_B200_KERNEL_AUTO, s.st);
+        s.flags.reserve(1);
+        SB_CUDA(cudaMemsetAsync(s.flags.p, 0, sizeof(DeviceFlags), s.st));
         const uint64_t total = (uint64_t)n1 * n2;
         const uint32_t grid = (uint32_t)std::min<uint64_t>((total + 255) / 256, 4096);
-        rect_sum_kernel<<<grid, 256, 0, s.st>>>(tri.p, n, n1, n2, df.p);
+        rect_sum_kernel<<<grid, 256, 0, s.st>>>(s.tri.p, n, n1, n2, s.flags.p);
         SB_CUDA(cudaGetLastError());
-        r = s.read_sum(df.p);
+        r = s.read_sum(s.flags.p);
         return 0;
     });
     return r;

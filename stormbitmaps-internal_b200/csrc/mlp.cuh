@@ -5,7 +5,8 @@
 // The features are the tile aggregates the cost model reads (storm_cost.cpp:
 // work_units inputs: cardinality, runs, non-zero words, universe words, the
 // index flags) on a log scale, plus what the cost model cannot see: the span
-// overlap of the two row blocks and their cardinality spread (max / mean).
+// overlap of the two row blocks, their cardinality spread (max / mean) and
+// the overlap of their zone maps.
 // Inference runs inside the tile-selection kernel (one thread per tile) and
 // takes the best-scoring cell among those whose representations exist.
 // Training (mlp.cu) uses device forward/backward kernels and labels timed on
@@ -50,9 +51,31 @@ __host__ __device__ inline float flog2(double v) {
 #endif
 }
 
-// 16 features of a tile pair from the two row blocks' aggregate metadata.
+// Zone map of a row block: BZONE_WORDS x 64 coarse bins over the universe,
+// a bin set when some row of the block holds a value in it (the OR of the
+// rows' zone maps, storm_repr.cpp:47-59, at a coarser grain).
+constexpr uint32_t BZONE_WORDS = 64;
+
+// Overlap of two block zone maps: bins both hold / bins either holds (the
+// zone-map test the reference's B x B plans from, cell_bb.cpp:522-550).
+__host__ __device__ inline float zone_overlap(const uint64_t* za, const uint64_t* zb) {
+    uint32_t both = 0, any = 0;
+    for (uint32_t k = 0; k < BZONE_WORDS; ++k) {
+#ifdef __CUDA_ARCH__
+        both += __popcll(za[k] & zb[k]);
+        any += __popcll(za[k] | zb[k]);
+#else
+        both += (uint32_t)__builtin_popcountll(za[k] & zb[k]);
+        any += (uint32_t)__builtin_popcountll(za[k] | zb[k]);
+#endif
+    }
+    return any ? (float)both / (float)any : 0.0f;
+}
+
+// 16 features of a tile pair from the two row blocks' aggregate metadata
+// and the overlap of their zone maps.
 __host__ __device__ inline void tile_features(const RowMetaD& a, const RowMetaD& b, uint32_t het_a_x1000,
-                                              uint32_t het_b_x1000, float* x) {
+                                              uint32_t het_b_x1000, float zone, float* x) {
     const float s = 1.0f / 32.0f;
     x[0] = flog2(1.0 + a.card) * s;
     x[1] = flog2(1.0 + b.card) * s;
@@ -71,7 +94,7 @@ __host__ __device__ inline void tile_features(const RowMetaD& a, const RowMetaD&
     x[12] = (hi > lo && span > 0) ? (float)((hi - lo) / span) : 0.0f;
     x[13] = flog2(het_a_x1000 / 1000.0 + 1e-3) * 0.25f;
     x[14] = flog2(het_b_x1000 / 1000.0 + 1e-3) * 0.25f;
-    x[15] = 1.0f;
+    x[15] = zone;
 }
 
 __host__ __device__ inline void mlp_forward(const float* p, const MlpShape& sh, const float* x, float* h,

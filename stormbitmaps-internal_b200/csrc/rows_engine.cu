@@ -79,6 +79,42 @@ __global__ void block_meta_kernel(RowsView v, const uint32_t* __restrict__ order
     het_x1000[b] = mean > 0 ? (uint32_t)fmin(4e9, 1000.0 * (double)mx / mean) : 1000u;
 }
 
+// Block zone maps (one CTA per row block of the traversal order): the bins
+// of the block's values, from each row's zone map where it has one, else from
+// up to 1024 of its values (evenly strided; the overlap is a selection
+// feature, not a count).
+__global__ void __launch_bounds__(256)
+block_zone_kernel(RowsView v, const uint32_t* __restrict__ order, uint32_t n, uint32_t T,
+                  uint64_t* __restrict__ out) {
+    __shared__ unsigned long long z[BZONE_WORDS];
+    const uint32_t b = blockIdx.x;
+    const uint32_t lo = b * T, hi = min(n, lo + T);
+    for (uint32_t k = threadIdx.x; k < BZONE_WORDS; k += blockDim.x) z[k] = 0ull;
+    __syncthreads();
+    const uint64_t ubits = (uint64_t)v.nw * 64;
+    for (uint32_t k = lo; k < hi; ++k) {
+        const uint32_t row = order[k];
+        if (v.oc_off[row] != NONE) {
+            const uint64_t* oc = v.oc + v.oc_off[row];
+            for (uint32_t w = threadIdx.x; w < v.n_occ; w += blockDim.x)
+                for (uint64_t x = oc[w]; x; x &= x - 1) {
+                    const uint64_t bin = (uint64_t)w * 64 + (uint64_t)(__ffsll((long long)x) - 1);
+                    const uint64_t cb = bin * 512 * (BZONE_WORDS * 64) / ubits;
+                    atomicOr(&z[cb >> 6], 1ull << (cb & 63));
+                }
+        } else {
+            const uint64_t s0 = v.s_off[row], len = v.s_off[row + 1] - s0;
+            const uint64_t step = len > 1024 ? len / 1024 : 1;
+            for (uint64_t e = (uint64_t)threadIdx.x * step; e < len; e += (uint64_t)blockDim.x * step) {
+                const uint64_t cb = (uint64_t)v.s_val[s0 + e] * (BZONE_WORDS * 64) / ubits;
+                atomicOr(&z[cb >> 6], 1ull << (cb & 63));
+            }
+        }
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < BZONE_WORDS; k += blockDim.x) out[(uint64_t)b * BZONE_WORDS + k] = z[k];
+}
+
 // Tile (ti, tj), ti <= tj, from a linear index over the block triangle.
 __device__ __forceinline__ void tile_decode(uint32_t nb, uint32_t t, uint32_t& ti, uint32_t& tj) {
     // rows of the block triangle: row i holds nb - i tiles
@@ -95,8 +131,9 @@ __device__ __forceinline__ void tile_decode(uint32_t nb, uint32_t t, uint32_t& t
 
 // ---------------------------------------------------------------- phase 2
 __global__ void select_tiles_kernel(const RowMetaD* __restrict__ bmeta, const uint32_t* __restrict__ het,
-                                    uint32_t nb, int policy, int fixed_cell, CostModelD model,
-                                    const float* __restrict__ mlp, MlpShape shape, TileDecision* __restrict__ dec) {
+                                    const uint64_t* __restrict__ bzone, uint32_t nb, int policy, int fixed_cell,
+                                    CostModelD model, const float* __restrict__ mlp, MlpShape shape,
+                                    TileDecision* __restrict__ dec) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t ntiles = nb * (nb + 1) / 2;
     if (t >= ntiles) return;
@@ -111,7 +148,8 @@ __global__ void select_tiles_kernel(const RowMetaD* __restrict__ bmeta, const ui
         d.cell = d.cell2 = fixed_cell;
     } else if (policy == STORM_POLICY_LEARNED && mlp != nullptr) {
         float x[MLP_MAX_F];
-        tile_features(a, b, het[ti], het[tj], x);
+        tile_features(a, b, het[ti], het[tj],
+                      zone_overlap(bzone + (uint64_t)ti * BZONE_WORDS, bzone + (uint64_t)tj * BZONE_WORDS), x);
         d.cell = d.cell2 = mlp_argmax_available(mlp, shape, x, a, b);
     } else {
         double best1 = 0.0;
@@ -357,6 +395,7 @@ struct STORM_rows_s {
     cudaStream_t stream = nullptr;
     DevBuf<uint32_t> d_order, d_het, d_out, d_tile_list;
     DevBuf<RowMetaD> d_bmeta;
+    DevBuf<uint64_t> d_bzone;
     DevBuf<TileDecision> d_dec;
     DevBuf<RowsStatsDev> d_stats;
     // tensor-core dense block
@@ -370,6 +409,11 @@ struct STORM_rows_s {
     uint32_t n_dtiles = 0;
     DevBuf<DeviceFlags> d_dflags;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // cost model of the cost-model policies and of the untrained learned
+    // selector: the reference's defaults until calibrated on this GPU
+    CostModelD model = default_cost_model();
+    bool calibrated = false;
+    double last_training[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     // learned selector
     Mlp mlp;
     // CUDA graph of the batched form, keyed by the call's shape
@@ -480,7 +524,7 @@ static void rows_run(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell,
     c.T = T;
     c.nb = nb;
     c.policy = policy;
-    c.model = default_cost_model();
+    c.model = r->model;
     // Dense block: the suffix of the density order whose rows all have a
     // bitmap and whose smallest sparse form (elements or run bounds) is
     // >= dense_min_density x universe; its pairs run on the tensor
@@ -517,7 +561,10 @@ static void rows_run(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell,
         }
     }
     const bool learned = policy == STORM_POLICY_LEARNED && r->mlp.trained;
-    if (learned) r->mlp.ensure_device(st);
+    if (learned) {
+        r->mlp.ensure_device(st);
+        r->d_bzone.reserve((uint64_t)nb * BZONE_WORDS);
+    }
 
     // slices per tile so the launch has enough CTAs
     const int sms = require_device();
@@ -538,9 +585,11 @@ static void rows_run(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell,
     auto phases_1_2 = [&]() {
         SB_CUDA(cudaMemsetAsync(r->d_stats.p, 0, sizeof(RowsStatsDev), st));
         block_meta_kernel<<<(nb + 127) / 128, 128, 0, st>>>(c.v, c.order, n, T, r->d_bmeta.p, r->d_het.p);
+        if (learned) block_zone_kernel<<<nb, 256, 0, st>>>(c.v, c.order, n, T, r->d_bzone.p);
         select_tiles_kernel<<<(ntiles + 127) / 128, 128, 0, st>>>(
-            r->d_bmeta.p, r->d_het.p, nb, learned ? policy : (policy == STORM_POLICY_LEARNED ? STORM_POLICY_PERTILE : policy),
-            fixed_cell, c.model, learned ? r->mlp.d_params.p : nullptr, r->mlp.shape, r->d_dec.p);
+            r->d_bmeta.p, r->d_het.p, learned ? r->d_bzone.p : nullptr, nb,
+            learned ? policy : (policy == STORM_POLICY_LEARNED ? STORM_POLICY_PERTILE : policy), fixed_cell, c.model,
+            learned ? r->mlp.d_params.p : nullptr, r->mlp.shape, r->d_dec.p);
         if (policy == STORM_POLICY_PROBE)
             probe_tiles_kernel<<<(ntiles * 32 + 127) / 128, 128, 0, st>>>(c, r->d_dec.p, ntiles);
     };
@@ -569,6 +618,7 @@ static void rows_run(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell,
                                            nd ? ptr(r->d_dtiles.p) : 0ull,
                                            nd ? ptr(r->d_dflags.p) : 0ull,
                                            learned ? ptr(r->mlp.d_params.p) : 0ull,
+                                           learned ? ptr(r->d_bzone.p) : 0ull,
                                            learned ? ((uint64_t)r->mlp.shape.H << 40 | (uint64_t)r->mlp.shape.F << 20 |
                                                       r->mlp.shape.C)
                                                    : 0ull};
@@ -913,75 +963,312 @@ time_cells_kernel(PairCtx c, const uint32_t* __restrict__ tiles, uint32_t n_samp
     }
 }
 
+// What the cost model sees of the pairs time_cells_kernel times (the same
+// pair sample of each tile): per (tile, cell) the reference default model's
+// predicted cost above its fixed term, summed, and the number of pairs.
+__global__ void __launch_bounds__(TK_THREADS)
+cell_predict_kernel(PairCtx c, const uint32_t* __restrict__ tiles, uint32_t n_samples, uint32_t max_pairs,
+                    double* __restrict__ pred, uint32_t* __restrict__ npairs) {
+    const uint32_t sample = blockIdx.x / P_EMPTY, cell = blockIdx.x % P_EMPTY;
+    if (sample >= n_samples) return;
+    __shared__ double s_pred;
+    __shared__ unsigned int s_np;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t ti, tj;
+    tile_decode(c.nb, tiles[sample], ti, tj);
+    const uint32_t i0 = ti * c.T, i1 = min(c.n, i0 + c.T), j0 = tj * c.T, j1 = min(c.n, j0 + c.T);
+    const uint32_t nr = i1 - i0, nc = j1 - j0, np = nr * nc;
+    const uint32_t step = np > max_pairs ? np / max_pairs : 1;
+    if (threadIdx.x == 0) {
+        s_pred = 0.0;
+        s_np = 0;
+    }
+    __syncthreads();
+    const CostModelD m = default_cost_model();
+    double acc = 0.0;
+    uint32_t cnt = 0;
+    if (lane == 0) {
+        for (uint32_t q = warp * step; q < np; q += TK_WARPS * step) {
+            const uint32_t oi = i0 + q / nc, oj = j0 + q % nc;
+            if (ti == tj && oj <= oi) continue;
+            const RowMetaD& mi = c.v.meta[c.order[oi]];
+            const RowMetaD& mj = c.v.meta[c.order[oj]];
+            if (span_disjoint(mi, mj)) continue;
+            acc += predict_cost(m, (int)cell, mi, mj) - m.ns_fixed;
+            ++cnt;
+        }
+        atomicAdd(&s_pred, acc);
+        atomicAdd(&s_np, cnt);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        pred[(uint64_t)sample * P_EMPTY + cell] = s_pred;
+        npairs[(uint64_t)sample * P_EMPTY + cell] = s_np;
+    }
+}
+
+// Timings of every cell on sampled tiles of r's density order, with the
+// tile aggregates and the cost model's view of the same pairs.
+struct TileTimings {
+    uint32_t T = 64, nb = 0;
+    std::vector<uint32_t> pick;                 // sampled tile indices
+    std::vector<unsigned long long> cyc;        // [sample][cell] min of three, ~0 = cell unavailable
+    std::vector<double> pred;                   // [sample][cell] default model, above its fixed term
+    std::vector<uint32_t> npairs;               // [sample][cell]
+    std::vector<RowMetaD> bmeta;
+    std::vector<uint32_t> het;
+    std::vector<uint64_t> bzone;                // [block][BZONE_WORDS]
+    void tile_of(uint32_t k, uint32_t& ti, uint32_t& tj) const {
+        uint64_t t = pick[k], i = 0;
+        auto S = [this](uint64_t q) { return q * nb - q * (q - 1) / 2; };
+        while (i + 1 < nb && S(i + 1) <= t) ++i;
+        ti = (uint32_t)i;
+        tj = (uint32_t)(t - S(i) + i);
+    }
+};
+
+static TileTimings time_tiles(STORM_rows_t* r, uint32_t T, uint32_t samples, uint64_t seed) {
+    rows_ensure_uploaded(r);
+    cudaStream_t st = rows_stream(r);
+    const uint32_t n = (uint32_t)(r->offs.size() - 1);
+    if (n < 2) fail(STORM_B200_EARG, "fewer than two rows");
+    TileTimings tt;
+    tt.T = T;
+    const uint32_t nb = (n + T - 1) / T;
+    tt.nb = nb;
+    if ((uint64_t)nb * (nb + 1) / 2 > 0xFFFFFFFFull) fail(STORM_B200_ELIMIT, "more than 2^32 tiles");
+    const uint32_t ntiles = nb * (nb + 1) / 2;
+    const std::vector<uint32_t> order = rows_order(r, STORM_POLICY_PERTILE);
+    r->d_order.reserve(n);
+    r->d_bmeta.reserve(nb);
+    r->d_het.reserve(nb);
+    r->d_bzone.reserve((size_t)nb * BZONE_WORDS);
+    SB_CUDA(cudaMemcpyAsync(r->d_order.p, order.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    PairCtx c;
+    c.v = r->dev.view;
+    c.order = r->d_order.p;
+    c.n = n;
+    c.T = T;
+    c.nb = nb;
+    c.policy = STORM_POLICY_PERTILE;
+    c.model = r->model;
+    block_meta_kernel<<<(nb + 127) / 128, 128, 0, st>>>(c.v, c.order, n, T, r->d_bmeta.p, r->d_het.p);
+    block_zone_kernel<<<nb, 256, 0, st>>>(c.v, c.order, n, T, r->d_bzone.p);
+    SB_CUDA(cudaGetLastError());
+    tt.bmeta.resize(nb);
+    tt.het.resize(nb);
+    tt.bzone.resize((size_t)nb * BZONE_WORDS);
+    SB_CUDA(cudaMemcpyAsync(tt.bmeta.data(), r->d_bmeta.p, nb * sizeof(RowMetaD), cudaMemcpyDeviceToHost, st));
+    SB_CUDA(cudaMemcpyAsync(tt.het.data(), r->d_het.p, nb * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    SB_CUDA(cudaMemcpyAsync(tt.bzone.data(), r->d_bzone.p, tt.bzone.size() * sizeof(uint64_t),
+                            cudaMemcpyDeviceToHost, st));
+    // sample tiles (all of them when there are few)
+    uint64_t s = seed ? seed : 0x5E1EC7;
+    auto rnd = [&s]() {
+        uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    };
+    if (samples == 0 || samples >= ntiles) {
+        tt.pick.resize(ntiles);
+        std::iota(tt.pick.begin(), tt.pick.end(), 0u);
+    } else {
+        std::vector<uint32_t> all(ntiles);
+        std::iota(all.begin(), all.end(), 0u);
+        for (uint32_t k = 0; k < samples; ++k) std::swap(all[k], all[k + rnd() % (ntiles - k)]);
+        tt.pick.assign(all.begin(), all.begin() + samples);
+    }
+    const uint32_t ns = (uint32_t)tt.pick.size();
+    DevBuf<uint32_t> dpick, dnp;
+    DevBuf<unsigned long long> dcyc;
+    DevBuf<double> dpred;
+    dpick.reserve(ns);
+    dcyc.reserve((size_t)ns * P_EMPTY);
+    dpred.reserve((size_t)ns * P_EMPTY);
+    dnp.reserve((size_t)ns * P_EMPTY);
+    SB_CUDA(cudaMemcpyAsync(dpick.p, tt.pick.data(), ns * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    tt.cyc.assign((size_t)ns * P_EMPTY, ~0ull);
+    std::vector<unsigned long long> tmp((size_t)ns * P_EMPTY);
+    for (int rep = 0; rep < 3; ++rep) {   // min of three timings per (tile, cell)
+        time_cells_kernel<<<ns * P_EMPTY, TK_THREADS, 0, st>>>(c, dpick.p, ns, 256, dcyc.p);
+        SB_CUDA(cudaGetLastError());
+        SB_CUDA(cudaMemcpyAsync(tmp.data(), dcyc.p, tmp.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                st));
+        SB_CUDA(cudaStreamSynchronize(st));
+        for (size_t k = 0; k < tt.cyc.size(); ++k) tt.cyc[k] = std::min(tt.cyc[k], tmp[k]);
+    }
+    cell_predict_kernel<<<ns * P_EMPTY, TK_THREADS, 0, st>>>(c, dpick.p, ns, 256, dpred.p, dnp.p);
+    SB_CUDA(cudaGetLastError());
+    tt.pred.resize((size_t)ns * P_EMPTY);
+    tt.npairs.resize((size_t)ns * P_EMPTY);
+    SB_CUDA(cudaMemcpyAsync(tt.pred.data(), dpred.p, tt.pred.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    SB_CUDA(cudaMemcpyAsync(tt.npairs.data(), dnp.p, tt.npairs.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                            st));
+    SB_CUDA(cudaStreamSynchronize(st));
+    return tt;
+}
+
+// The reference's calibration (calibrate / calibrate_on_rows,
+// storm_cost.cpp:556-769, 779-895) fits, per cell, time / work on pairs it
+// times, plus a per-pair fixed term; here the timings are this GPU's, of the
+// container's own sampled tiles (time_cells_kernel), and the model keeps the
+// reference's work formulas: cycles(tile, cell) ~ a_cell x (the default
+// model's prediction above its fixed term) + f x pairs, solved as one
+// weighted least-squares problem (relative error) over the samples `use`.
+// Returns the fitted model in SM cycles (the selector compares predictions,
+// so the unit is free) and the fit's relative RMS error.
+static CostModelD fit_cost_model(const TileTimings& tt, const std::vector<uint32_t>& use, double* rms_out) {
+    constexpr int K = P_EMPTY + 1;               // a_0 .. a_9, f
+    double A[K][K] = {}, B[K] = {};
+    std::vector<int> seen(P_EMPTY, 0);
+    for (uint32_t k : use)
+        for (int cl = 0; cl < P_EMPTY; ++cl) {
+            const size_t e = (size_t)k * P_EMPTY + cl;
+            if (tt.cyc[e] == ~0ull || tt.npairs[e] == 0) continue;
+            const double y = (double)tt.cyc[e], w = 1.0 / (y * y);
+            const double xa = tt.pred[e], xf = (double)tt.npairs[e];
+            A[cl][cl] += w * xa * xa;
+            A[cl][K - 1] += w * xa * xf;
+            A[K - 1][cl] += w * xa * xf;
+            A[K - 1][K - 1] += w * xf * xf;
+            B[cl] += w * xa * y;
+            B[K - 1] += w * xf * y;
+            seen[cl] = 1;
+        }
+    for (int cl = 0; cl < P_EMPTY; ++cl)
+        if (!seen[cl]) A[cl][cl] = 1.0;          // unfitted cell: a = 0 for now
+    double M[K][K + 1];
+    for (int i = 0; i < K; ++i) {
+        for (int j = 0; j < K; ++j) M[i][j] = A[i][j];
+        M[i][K] = B[i];
+    }
+    bool ok = true;
+    for (int col = 0; col < K && ok; ++col) {    // Gaussian elimination, partial pivoting
+        int piv = col;
+        for (int i = col + 1; i < K; ++i)
+            if (std::fabs(M[i][col]) > std::fabs(M[piv][col])) piv = i;
+        if (std::fabs(M[piv][col]) < 1e-300) {
+            ok = false;
+            break;
+        }
+        for (int j = 0; j <= K; ++j) std::swap(M[col][j], M[piv][j]);
+        for (int i = 0; i < K; ++i) {
+            if (i == col) continue;
+            const double f = M[i][col] / M[col][col];
+            for (int j = col; j <= K; ++j) M[i][j] -= f * M[col][j];
+        }
+    }
+    double a[K];
+    for (int i = 0; i < K; ++i) a[i] = ok ? M[i][K] / M[i][i] : 0.0;
+    if (!ok || a[K - 1] < 0.0) {                 // no fixed term: per-cell ratios
+        a[K - 1] = 0.0;
+        for (int cl = 0; cl < P_EMPTY; ++cl) {
+            double sy = 0, sx = 0;
+            for (uint32_t k : use) {
+                const size_t e = (size_t)k * P_EMPTY + cl;
+                if (tt.cyc[e] == ~0ull || tt.npairs[e] == 0) continue;
+                sy += (double)tt.cyc[e];
+                sx += tt.pred[e];
+            }
+            a[cl] = sx > 0 ? sy / sx : 0.0;
+        }
+    }
+    // cells with no sample (or a non-positive fit) take the mean scale of the others
+    double mean = 0;
+    int nf = 0;
+    for (int cl = 0; cl < P_EMPTY; ++cl)
+        if (seen[cl] && a[cl] > 0) {
+            mean += a[cl];
+            ++nf;
+        }
+    mean = nf ? mean / nf : 1.0;
+    for (int cl = 0; cl < P_EMPTY; ++cl)
+        if (!seen[cl] || a[cl] <= 0) a[cl] = mean;
+    const CostModelD d = default_cost_model();
+    CostModelD m = d;
+    for (int cl = 0; cl < P_EMPTY; ++cl) m.ns_per_unit[cl] = a[cl] * d.ns_per_unit[cl];
+    m.ns_fixed = a[K - 1];
+    m.ns_per_occ_word = a[P_BB] * d.ns_per_occ_word;
+    m.ns_probe_hot = m.ns_probe_cold = 0.0;
+    double se = 0;
+    size_t cnt = 0;
+    for (uint32_t k : use)
+        for (int cl = 0; cl < P_EMPTY; ++cl) {
+            const size_t e = (size_t)k * P_EMPTY + cl;
+            if (tt.cyc[e] == ~0ull || tt.npairs[e] == 0) continue;
+            const double y = (double)tt.cyc[e];
+            const double p = a[cl] * tt.pred[e] + a[K - 1] * tt.npairs[e];
+            se += (p - y) * (p - y) / (y * y);
+            ++cnt;
+        }
+    if (rms_out) *rms_out = cnt ? std::sqrt(se / cnt) : 0.0;
+    return m;
+}
+
+static void drop_graph(STORM_rows_t* r) {
+    if (r->graph) {
+        cudaGraphExecDestroy(r->graph);
+        r->graph = nullptr;
+    }
+}
+
 }  // namespace sb200
 
 extern "C" {
+
+int STORM_rows_calibrate(STORM_rows_t* r, uint32_t tile, uint32_t samples, uint64_t seed, double* model_out) {
+    if (r == NULL) return STORM_B200_ENULL;
+    return guard([&]() -> int {
+        const TileTimings tt = time_tiles(r, tile ? tile : 64, samples, seed);
+        std::vector<uint32_t> use(tt.pick.size());
+        std::iota(use.begin(), use.end(), 0u);
+        double rms = 0;
+        r->model = fit_cost_model(tt, use, &rms);
+        r->calibrated = true;
+        drop_graph(r);
+        if (model_out) {
+            for (int cl = 0; cl < P_COUNT; ++cl) model_out[cl] = r->model.ns_per_unit[cl];
+            model_out[P_COUNT] = r->model.ns_fixed;
+            model_out[P_COUNT + 1] = r->model.ns_per_occ_word;
+            model_out[P_COUNT + 2] = rms;
+        }
+        return 0;
+    });
+}
+
+int STORM_rows_cost_model(STORM_rows_t* r, double* model, int set) {
+    if (r == NULL) return STORM_B200_ENULL;
+    if (set) {
+        if (model == NULL) {
+            r->model = default_cost_model();
+            r->calibrated = false;
+        } else {
+            for (int cl = 0; cl < P_COUNT; ++cl) r->model.ns_per_unit[cl] = model[cl];
+            r->model.ns_fixed = model[P_COUNT];
+            r->model.ns_per_occ_word = model[P_COUNT + 1];
+            r->model.ns_probe_hot = r->model.ns_probe_cold = 0.0;
+            r->calibrated = true;
+        }
+        drop_graph(r);
+        return 0;
+    }
+    if (model == NULL) return STORM_B200_EVALUES;
+    for (int cl = 0; cl < P_COUNT; ++cl) model[cl] = r->model.ns_per_unit[cl];
+    model[P_COUNT] = r->model.ns_fixed;
+    model[P_COUNT + 1] = r->model.ns_per_occ_word;
+    return r->calibrated ? 1 : 0;
+}
 
 int STORM_rows_train_selector(STORM_rows_t* r, uint32_t tile, uint32_t samples, uint32_t epochs, uint64_t seed,
                               double* stats) {
     if (r == NULL) return STORM_B200_ENULL;
     return guard([&]() -> int {
-        rows_ensure_uploaded(r);
-        cudaStream_t st = rows_stream(r);
-        const uint32_t n = (uint32_t)(r->offs.size() - 1);
-        if (n < 2) return STORM_B200_EARG;
         const uint32_t T = tile ? tile : 64;
+        const TileTimings tt = time_tiles(r, T, samples, seed);
         r->trained_tile = T;
-        const uint32_t nb = (n + T - 1) / T;
-        if ((uint64_t)nb * (nb + 1) / 2 > 0xFFFFFFFFull) return STORM_B200_ELIMIT;
-        const uint32_t ntiles = nb * (nb + 1) / 2;
-        const std::vector<uint32_t> order = rows_order(r, STORM_POLICY_PERTILE);
-        r->d_order.reserve(n);
-        r->d_bmeta.reserve(nb);
-        r->d_het.reserve(nb);
-        SB_CUDA(cudaMemcpyAsync(r->d_order.p, order.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-        PairCtx c;
-        c.v = r->dev.view;
-        c.order = r->d_order.p;
-        c.n = n;
-        c.T = T;
-        c.nb = nb;
-        c.policy = STORM_POLICY_PERTILE;
-        c.model = default_cost_model();
-        block_meta_kernel<<<(nb + 127) / 128, 128, 0, st>>>(c.v, c.order, n, T, r->d_bmeta.p, r->d_het.p);
-        std::vector<RowMetaD> bmeta(nb);
-        std::vector<uint32_t> het(nb);
-        SB_CUDA(cudaMemcpyAsync(bmeta.data(), r->d_bmeta.p, nb * sizeof(RowMetaD), cudaMemcpyDeviceToHost, st));
-        SB_CUDA(cudaMemcpyAsync(het.data(), r->d_het.p, nb * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        // sample tiles (all of them when there are few)
-        uint64_t s = seed ? seed : 0x5E1EC7;
-        auto rnd = [&s]() {
-            uint64_t z = (s += 0x9E3779B97F4A7C15ull);
-            z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-            z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-            return z ^ (z >> 31);
-        };
-        std::vector<uint32_t> pick;
-        if (samples == 0 || samples >= ntiles) {
-            pick.resize(ntiles);
-            std::iota(pick.begin(), pick.end(), 0u);
-        } else {
-            std::vector<uint32_t> all(ntiles);
-            std::iota(all.begin(), all.end(), 0u);
-            for (uint32_t k = 0; k < samples; ++k) std::swap(all[k], all[k + rnd() % (ntiles - k)]);
-            pick.assign(all.begin(), all.begin() + samples);
-        }
-        const uint32_t ns = (uint32_t)pick.size();
-        DevBuf<uint32_t> dpick;
-        DevBuf<unsigned long long> dcyc;
-        dpick.reserve(ns);
-        dcyc.reserve((size_t)ns * P_EMPTY);
-        SB_CUDA(cudaMemcpyAsync(dpick.p, pick.data(), ns * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-        std::vector<unsigned long long> cyc((size_t)ns * P_EMPTY, ~0ull), tmp((size_t)ns * P_EMPTY);
-        for (int rep = 0; rep < 3; ++rep) {   // min of three timings per (tile, cell)
-            time_cells_kernel<<<ns * P_EMPTY, TK_THREADS, 0, st>>>(c, dpick.p, ns, 256, dcyc.p);
-            SB_CUDA(cudaGetLastError());
-            SB_CUDA(cudaMemcpyAsync(tmp.data(), dcyc.p, tmp.size() * sizeof(unsigned long long),
-                                    cudaMemcpyDeviceToHost, st));
-            SB_CUDA(cudaStreamSynchronize(st));
-            for (size_t k = 0; k < cyc.size(); ++k) cyc[k] = std::min(cyc[k], tmp[k]);
-        }
-        // features, labels, the cost model's choice
+        const uint32_t ns = (uint32_t)tt.pick.size();
+        // features, labels
         const MlpShape sh = r->mlp.shape;
         std::vector<float> X;
         std::vector<int32_t> Y;
@@ -990,21 +1277,18 @@ int STORM_rows_train_selector(STORM_rows_t* r, uint32_t tile, uint32_t samples, 
             uint32_t best = P_EMPTY;
             unsigned long long bc = ~0ull;
             for (uint32_t cl = 0; cl < P_EMPTY; ++cl)
-                if (cyc[(size_t)k * P_EMPTY + cl] < bc) {
-                    bc = cyc[(size_t)k * P_EMPTY + cl];
+                if (tt.cyc[(size_t)k * P_EMPTY + cl] < bc) {
+                    bc = tt.cyc[(size_t)k * P_EMPTY + cl];
                     best = cl;
                 }
             if (best == P_EMPTY) continue;
             uint32_t ti, tj;
-            {   // host copy of tile_decode
-                uint64_t t = pick[k], i = 0;
-                auto S = [nb](uint64_t q) { return q * nb - q * (q - 1) / 2; };
-                while (i + 1 < nb && S(i + 1) <= t) ++i;
-                ti = (uint32_t)i;
-                tj = (uint32_t)(t - S(i) + i);
-            }
+            tt.tile_of(k, ti, tj);
             float x[MLP_MAX_F];
-            tile_features(bmeta[ti], bmeta[tj], het[ti], het[tj], x);
+            tile_features(tt.bmeta[ti], tt.bmeta[tj], tt.het[ti], tt.het[tj],
+                          zone_overlap(tt.bzone.data() + (size_t)ti * BZONE_WORDS,
+                                       tt.bzone.data() + (size_t)tj * BZONE_WORDS),
+                          x);
             X.insert(X.end(), x, x + sh.F);
             Y.push_back((int32_t)best);
             idx.push_back(k);
@@ -1014,17 +1298,23 @@ int STORM_rows_train_selector(STORM_rows_t* r, uint32_t tile, uint32_t samples, 
         // 80 / 20 split, deterministic by sample position
         std::vector<float> Xtr, Xte;
         std::vector<int32_t> Ytr, Yte;
-        std::vector<uint32_t> te_idx;
+        std::vector<uint32_t> tr_idx, te_idx;
         for (uint32_t k = 0; k < nl; ++k) {
             const bool test = (k % 5) == 4;
             (test ? Xte : Xtr).insert((test ? Xte : Xtr).end(), X.begin() + (size_t)k * sh.F,
                                       X.begin() + (size_t)(k + 1) * sh.F);
             (test ? Yte : Ytr).push_back(Y[k]);
-            if (test) te_idx.push_back(idx[k]);
+            (test ? te_idx : tr_idx).push_back(idx[k]);
         }
+        // The cost model calibrated on the training tiles' timings becomes
+        // this container's model: the fallback of the learned policy and the
+        // model of the cost-model policies.
+        double rms = 0;
+        r->model = fit_cost_model(tt, tr_idx, &rms);
+        r->calibrated = true;
         mlp_init(r->mlp, seed ^ 0xA5A5A5A5ull);
         r->mlp.dirty = true;
-        const float loss = mlp_train(r->mlp, Xtr, Ytr, epochs ? epochs : 400, st);
+        const float loss = mlp_train(r->mlp, Xtr, Ytr, epochs ? epochs : 400, rows_stream(r));
         r->mlp.trained = true;
         // accuracy on the training split
         uint32_t correct = 0;
@@ -1036,43 +1326,54 @@ int STORM_rows_train_selector(STORM_rows_t* r, uint32_t tile, uint32_t samples, 
                 if (lg[cl] > lg[am]) am = cl;
             correct += (am == (uint32_t)Ytr[k]);
         }
-        // regret on the held-out tiles: sum of chosen cycles / sum of best - 1
-        const CostModelD model = default_cost_model();
-        double best_sum = 0, mlp_sum = 0, cost_sum = 0;
+        // regret on the held-out tiles: sum of chosen cycles / sum of best - 1,
+        // for the MLP, the calibrated model and the reference's default model
+        const CostModelD dflt = default_cost_model();
+        double best_sum = 0, mlp_sum = 0, cal_sum = 0, def_sum = 0;
         for (size_t q = 0; q < te_idx.size(); ++q) {
             const uint32_t k = te_idx[q];
             uint32_t ti, tj;
-            {
-                uint64_t t = pick[k], i = 0;
-                auto S = [nb](uint64_t z) { return z * nb - z * (z - 1) / 2; };
-                while (i + 1 < nb && S(i + 1) <= t) ++i;
-                ti = (uint32_t)i;
-                tj = (uint32_t)(t - S(i) + i);
-            }
-            const unsigned long long* cy = cyc.data() + (size_t)k * P_EMPTY;
+            tt.tile_of(k, ti, tj);
+            const unsigned long long* cy = tt.cyc.data() + (size_t)k * P_EMPTY;
             const int y = Yte[q];
-            const int m_cell = mlp_argmax_available(r->mlp.params.data(), sh, Xte.data() + q * sh.F, bmeta[ti], bmeta[tj]);
-            int c_cell = select_pairing_d(model, bmeta[ti], bmeta[tj], nullptr);
-            if (c_cell == P_EMPTY) c_cell = (bmeta[ti].has_bm && bmeta[tj].has_bm) ? P_BB : P_SS;
+            const RowMetaD& a = tt.bmeta[ti];
+            const RowMetaD& b = tt.bmeta[tj];
+            const int m_cell = mlp_argmax_available(r->mlp.params.data(), sh, Xte.data() + q * sh.F, a, b);
+            auto model_cell = [&](const CostModelD& mm) {
+                int cl = select_pairing_d(mm, a, b, nullptr);
+                if (cl == P_EMPTY) cl = (a.has_bm && b.has_bm) ? P_BB : P_SS;
+                return cl;
+            };
             auto cost = [&](int cl) { return cy[cl] == ~0ull ? (double)cy[y] * 4.0 : (double)cy[cl]; };
             best_sum += (double)cy[y];
             mlp_sum += cost(m_cell);
-            cost_sum += cost(c_cell);
+            cal_sum += cost(model_cell(r->model));
+            def_sum += cost(model_cell(dflt));
         }
+        const double reg_mlp = best_sum > 0 ? mlp_sum / best_sum - 1.0 : 0.0;
+        const double reg_cal = best_sum > 0 ? cal_sum / best_sum - 1.0 : 0.0;
+        const double reg_def = best_sum > 0 ? def_sum / best_sum - 1.0 : 0.0;
         if (stats) {
             stats[0] = ns;
             stats[1] = epochs ? epochs : 400;
             stats[2] = loss;
             stats[3] = Ytr.empty() ? 0.0 : (double)correct / Ytr.size();
-            stats[4] = best_sum > 0 ? mlp_sum / best_sum - 1.0 : 0.0;
-            stats[5] = best_sum > 0 ? cost_sum / best_sum - 1.0 : 0.0;
+            stats[4] = reg_mlp;
+            stats[5] = reg_cal;
         }
-        if (r->graph) {
-            cudaGraphExecDestroy(r->graph);
-            r->graph = nullptr;
-        }
+        const double rep[8] = {reg_mlp, reg_cal, reg_def, (double)te_idx.size(), (double)tr_idx.size(), rms,
+                               r->model.ns_fixed, (double)ns};
+        std::copy(rep, rep + 8, r->last_training);
+        drop_graph(r);
         return 0;
     });
+}
+
+int STORM_rows_last_training(const STORM_rows_t* r, double* out8) {
+    if (r == NULL) return STORM_B200_ENULL;
+    if (out8 == NULL) return STORM_B200_EVALUES;
+    std::copy(r->last_training, r->last_training + 8, out8);
+    return 0;
 }
 
 int STORM_rows_reset_selector(STORM_rows_t* r) {

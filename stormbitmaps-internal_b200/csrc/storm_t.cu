@@ -17,6 +17,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <atomic>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
@@ -25,6 +26,7 @@
 #include <cmath>
 #include "chunk_engine.cuh"
 #include "dense.cuh"
+#include "oneshot.cuh"
 
 namespace sb200 {
 
@@ -117,24 +119,23 @@ static void ensure_packed(const STORM_t* s, StormDev* d) {
     d->shape = shape;
 }
 
-// One-shot engine for calls that compare a few chunks or rows.
-struct AdHoc {
-    ChunkPack pack;
-    ChunkDev dev;
-    ChunkEngine engine;
-    cudaStream_t st = nullptr;
-    AdHoc() {
-        require_device();
-        SB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+// This thread's reusable context for the calls that compare a few chunks or
+// rows (kept across calls: one stream and the engine's buffers per device).
+OneShot& one_shot() {
+    require_device();
+    int dev = 0;
+    SB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) fail(STORM_B200_ECUDA, "device ordinal out of range");
+    thread_local std::unique_ptr<OneShot> per_device[64];
+    std::unique_ptr<OneShot>& h = per_device[dev];
+    if (!h) {
+        std::unique_ptr<OneShot> fresh(new OneShot());
+        SB_CUDA(cudaStreamCreateWithFlags(&fresh->st, cudaStreamNonBlocking));
+        h = std::move(fresh);
     }
-    ~AdHoc() {
-        if (st) cudaStreamDestroy(st);
-    }
-    uint64_t rect(uint64_t n1, uint64_t n2) {
-        dev.upload(pack, st);
-        return engine.run(dev, PAIRS_RECT, n1, n2, nullptr, st);
-    }
-};
+    h->pack.clear();
+    return *h;
+}
 
 }  // namespace sb200
 
@@ -301,7 +302,7 @@ uint64_t STORM_bitmap_intersect_cardinality(STORM_bitmap_t* STORM_RESTRICT b1, S
     if (b1->id != b2->id) return 0;
     uint64_t r = 0;
     guard([&]() -> int {
-        AdHoc h;
+        OneShot& h = one_shot();
         h.pack.add_chunk(b1->id, *b1);
         h.pack.end_row();
         h.pack.add_chunk(b2->id, *b2);
@@ -413,7 +414,7 @@ uint64_t STORM_bitmap_cont_intersect_cardinality(const STORM_bitmap_cont_t* STOR
     if (c1->n_bitmaps == 0 || c2->n_bitmaps == 0) return 0;
     uint64_t r = 0;
     guard([&]() -> int {
-        AdHoc h;
+        OneShot& h = one_shot();
         h.pack.add_row(c1);
         h.pack.add_row(c2);
         r = h.rect(1, 1);
@@ -611,7 +612,7 @@ uint64_t STORM_intersect_cardinality_square(const STORM_t* STORM_RESTRICT s1, co
     if (s1 == NULL || s2 == NULL) return 0;
     uint64_t r = 0;
     guard([&]() -> int {
-        AdHoc h;
+        OneShot& h = one_shot();
         h.pack.add_rows(s1->conts, s1->n_conts);
         h.pack.add_rows(s2->conts, s2->n_conts);
         r = h.rect(s1->n_conts, s2->n_conts);
