@@ -85,6 +85,9 @@ typedef void (*STORM_tile_callback)(uint32_t i0, uint32_t j0, uint32_t nr, uint3
 #define STORM_B200_KERNEL_MMA_DB 4  /* tcgen05 kind::i8, A in TMEM, 128 x 192 tiles
                                        with two accumulators drained by their own
                                        warps while the next tile computes        */
+#define STORM_B200_KERNEL_MMA_2CTA 5 /* tcgen05 kind::i8 on CTA pairs (cta_group::2):
+                                       256 x 256 tiles, each CTA expanding half of
+                                       the B rows                                */
 
 /* Append n_rows rows given as packed little-endian bitmaps of
  * words_per_row 64-bit words each, in host memory or (unified addressing)

@@ -36,7 +36,7 @@ u32p = C.POINTER(C.c_uint32)
 u64p = C.POINTER(C.c_uint64)
 TILE_CB = C.CFUNCTYPE(None, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, u32p, C.c_void_p)
 
-KERNEL_AUTO, KERNEL_POPC, KERNEL_MMA, KERNEL_MMA_SS, KERNEL_MMA_DB = 0, 1, 2, 3, 4
+KERNEL_AUTO, KERNEL_POPC, KERNEL_MMA, KERNEL_MMA_SS, KERNEL_MMA_DB, KERNEL_MMA_2CTA = 0, 1, 2, 3, 4, 5
 SCHED_AUTO, SCHED_TILES, SCHED_STREAM_K = 0, 1, 2
 OK, ENULL, EVALUES, EARG, ENOMEM, ECUDA, ETIMEOUT, ESIZE, ELIMIT = 0, -1, -2, -3, -4, -5, -6, -7, -8
 

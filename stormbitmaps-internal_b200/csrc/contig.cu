@@ -225,7 +225,7 @@ int STORM_contig_clear(STORM_contiguous_t* bitmap) {
 
 int STORM_contig_set_kernel(STORM_contiguous_t* c, int kernel) {
     if (c == NULL) return STORM_B200_ENULL;
-    if (kernel < STORM_B200_KERNEL_AUTO || kernel > STORM_B200_KERNEL_MMA_DB) return STORM_B200_EARG;
+    if (kernel < STORM_B200_KERNEL_AUTO || kernel > STORM_B200_KERNEL_MMA_2CTA) return STORM_B200_EARG;
     c->kernel_pref = kernel;
     return 0;
 }

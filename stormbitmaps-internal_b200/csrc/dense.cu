@@ -4,6 +4,7 @@
 #include "bb_mma.cuh"
 #include "bb_mma_ts.cuh"
 #include "bb_mma_ts2.cuh"
+#include "bb_mma_2cta.cuh"
 
 #include <algorithm>
 #include <mutex>
@@ -41,17 +42,29 @@ static uint32_t ts_schedule(uint32_t n_tiles, int sms, uint32_t w_pad, uint32_t&
 
 constexpr uint64_t DB_AUTO_MAX_BITS = 1ull << 17;
 
+// Rows per A block and per B block of a kernel's tiles.
+uint64_t tile_rows_a(int kind) {
+    return kind == STORM_B200_KERNEL_POPC ? POPC_BM : kind == STORM_B200_KERNEL_MMA_2CTA ? C2_BM : MMA_BM;
+}
+uint64_t tile_rows_b(int kind) {
+    return kind == STORM_B200_KERNEL_POPC     ? POPC_BM
+           : kind == STORM_B200_KERNEL_MMA_DB ? T2_BN
+           : kind == STORM_B200_KERNEL_MMA_2CTA ? C2_BN
+                                                : MMA_BN;
+}
+
 void build_tiles(std::vector<uint2>& t, uint64_t n, int kind) {
     t.clear();
     // tile indices and counts are 32-bit (the kernels' work lists); bound the
     // count by the full block grid before building anything
-    const uint64_t bm = (kind == STORM_B200_KERNEL_POPC) ? POPC_BM : MMA_BM;
-    const uint64_t bn = (kind == STORM_B200_KERNEL_POPC)     ? POPC_BM
-                        : (kind == STORM_B200_KERNEL_MMA_DB) ? T2_BN
-                                                             : MMA_BN;
+    const uint64_t bm = tile_rows_a(kind), bn = tile_rows_b(kind);
     if (((n + bm - 1) / bm) * ((n + bn - 1) / bn) > 0xFFFFFFFFull)
         fail(STORM_B200_ELIMIT, "more than 2^32 tiles: split the rows into several containers");
-    if (kind == STORM_B200_KERNEL_MMA || kind == STORM_B200_KERNEL_MMA_SS) {
+    if (kind == STORM_B200_KERNEL_MMA_2CTA) {
+        const uint64_t nb = (n + C2_BM - 1) / C2_BM;
+        for (uint64_t bi = 0; bi < nb; ++bi)
+            for (uint64_t bj = bi; bj < nb; ++bj) t.push_back(make_uint2((uint32_t)bi, (uint32_t)bj));
+    } else if (kind == STORM_B200_KERNEL_MMA || kind == STORM_B200_KERNEL_MMA_SS) {
         const uint64_t nbi = (n + MMA_BM - 1) / MMA_BM, nbj = (n + MMA_BN - 1) / MMA_BN;
         // Tile (bi, bj) holds a pair with i <= j iff 128 bi <= 256 bj + 255,
         // i.e. bj >= floor(bi / 2).
@@ -81,7 +94,8 @@ int DenseEngine::prepare(uint64_t n, uint64_t row_bits, int kernel_pref, cudaStr
         kind = row_bits <= DB_AUTO_MAX_BITS    ? STORM_B200_KERNEL_MMA_DB
                : row_bits <= MMA_MAX_BITS_W4 ? STORM_B200_KERNEL_MMA
                                              : STORM_B200_KERNEL_POPC;
-    if ((kind == STORM_B200_KERNEL_MMA || kind == STORM_B200_KERNEL_MMA_DB) && row_bits > MMA_MAX_BITS_W4)
+    if ((kind == STORM_B200_KERNEL_MMA || kind == STORM_B200_KERNEL_MMA_DB || kind == STORM_B200_KERNEL_MMA_2CTA) &&
+        row_bits > MMA_MAX_BITS_W4)
         fail(STORM_B200_ELIMIT, "tensor-core kernel is exact only for rows of at most 2^27 bits");
     if (kind == STORM_B200_KERNEL_MMA_SS && row_bits > MMA_MAX_BITS)
         fail(STORM_B200_ELIMIT, "shared-memory tensor-core kernel is exact only for rows of at most 2^23 bits");
@@ -148,6 +162,31 @@ void DenseEngine::launch(int kind, const uint64_t* dX, uint32_t n, uint32_t w_pa
         else
             bb_mma_ts2_long_kernel<<<grid, T2_THREADS, T2_SMEM_BYTES, st>>>(dX, n, w_pad, d_tiles.p + t0, count,
                                                                            d_out, d_flags.p, ks);
+    } else if (kind == STORM_B200_KERNEL_MMA_2CTA) {
+        // CTA pairs (clusters of 2), one per two SMs, whole tiles round robin
+        static std::atomic<uint64_t> done_a{0}, done_b{0};
+        smem_attr_once(bb_mma_2cta_kernel, (int)C2_SMEM_BYTES, done_a);
+        smem_attr_once(bb_mma_2cta_long_kernel, (int)C2_SMEM_BYTES, done_b);
+        const uint32_t pairs = std::max<uint32_t>(1u, std::min<uint32_t>(count, (uint32_t)sms / 2));
+        const uint32_t smem = (uint64_t)w_pad * 64 <= TS_COALESCE_MAX_BITS ? C2_SMEM_BYTES
+                                                                          : C2_SMEM_BYTES - C2_EPI_BYTES;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(2 * pairs, 1, 1);
+        cfg.blockDim = dim3(C2_THREADS, 1, 1);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        const uint2* tl = d_tiles.p + t0;
+        if ((uint64_t)w_pad * 64 <= MMA_MAX_BITS)
+            SB_CUDA(cudaLaunchKernelEx(&cfg, bb_mma_2cta_kernel, dX, n, w_pad, tl, count, d_out, d_flags.p));
+        else
+            SB_CUDA(cudaLaunchKernelEx(&cfg, bb_mma_2cta_long_kernel, dX, n, w_pad, tl, count, d_out, d_flags.p));
     } else if (kind == STORM_B200_KERNEL_MMA_SS) {
         static std::atomic<uint64_t> done{0};
         smem_attr_once(bb_mma_kernel, (int)MMA_SMEM_BYTES, done);
@@ -284,11 +323,10 @@ uint64_t DenseEngine::panels_to_host(const uint64_t* dX, uint64_t n, uint32_t w_
                                      uint32_t* host_out, cudaStream_t st, cudaStream_t copy_st,
                                      uint64_t chunk_rows) {
     const int sms = require_device();
-    const uint64_t bm = (kind == STORM_B200_KERNEL_POPC) ? POPC_BM : MMA_BM;
-    const uint64_t bn = (kind == STORM_B200_KERNEL_POPC)     ? POPC_BM
-                        : (kind == STORM_B200_KERNEL_MMA_DB) ? T2_BN
-                                                             : MMA_BN;
-    const uint32_t wave = (kind == STORM_B200_KERNEL_POPC) ? 2u * (uint32_t)sms : (uint32_t)sms;
+    const uint64_t bm = tile_rows_a(kind), bn = tile_rows_b(kind);
+    const uint32_t wave = kind == STORM_B200_KERNEL_POPC        ? 2u * (uint32_t)sms
+                          : kind == STORM_B200_KERNEL_MMA_2CTA ? (uint32_t)sms / 2
+                                                               : (uint32_t)sms;
     const auto panels = host_panels(n_tiles, wave);
     // first tile of each A block (the list is ordered by A block)
     std::vector<uint32_t> first_tile((size_t)h_tiles.back().x + 1, 0);
@@ -410,7 +448,7 @@ extern "C" int STORM_contig_pairw_intersect_matrix_noalloc(const uint64_t* d_row
     {
         std::lock_guard<std::mutex> lock(mu);
         if (scratch_of[dev] == nullptr) {
-            int major = 0, sms = 0;
+            int major = 0;
             if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess || major != 10)
                 return STORM_B200_ECUDA;
             void* p = nullptr;
@@ -418,7 +456,6 @@ extern "C" int STORM_contig_pairw_intersect_matrix_noalloc(const uint64_t* d_row
             if (cudaFuncSetAttribute(bb_mma_ts_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)TS_SMEM_BYTES) != cudaSuccess)
                 return STORM_B200_ECUDA;
-            (void)sms;
             scratch_of[dev] = p;
         }
         scratch = static_cast<NoAllocScratch*>(scratch_of[dev]);

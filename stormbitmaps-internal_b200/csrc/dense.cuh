@@ -76,6 +76,9 @@ void build_mma_tiles(std::vector<uint2>& t, uint64_t n);
 // (tcgen05), 128 x 192 (double-buffered tcgen05) or 128 x 128 (POPC) tiles
 // covering every pair i <= j < n once, ordered by A block.
 void build_tiles(std::vector<uint2>& t, uint64_t n, int kind);
+// Rows per A block / per B block of a kernel's tiles.
+uint64_t tile_rows_a(int kind);
+uint64_t tile_rows_b(int kind);
 // Panels of the host-output forms over a tile list of n_tiles, in processing
 // order (the end of the list first), each a whole number of waves but the
 // last.

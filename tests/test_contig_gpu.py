@@ -12,11 +12,12 @@ import oracle_lib as ol
 
 pytestmark = pytest.mark.gpu
 
-KERNELS = ("popc", "mma", "mma_ss", "mma_db")
+KERNELS = ("popc", "mma", "mma_ss", "mma_db", "mma_2cta")
 
 
 def _kernel(sb, name):
-    return {"popc": sb.KERNEL_POPC, "mma": sb.KERNEL_MMA, "mma_ss": sb.KERNEL_MMA_SS, "mma_db": sb.KERNEL_MMA_DB}[name]
+    return {"popc": sb.KERNEL_POPC, "mma": sb.KERNEL_MMA, "mma_ss": sb.KERNEL_MMA_SS, "mma_db": sb.KERNEL_MMA_DB,
+            "mma_2cta": sb.KERNEL_MMA_2CTA}[name]
 
 
 def contig_from_words(sb, words, m, kernel):
@@ -55,7 +56,7 @@ def test_edge_shapes_match_oracle(sb, kernel, n, m, p):
     np.testing.assert_array_equal(mat, want)
 
 
-@pytest.mark.parametrize("kernel", ("mma", "mma_db"))
+@pytest.mark.parametrize("kernel", ("mma", "mma_db", "mma_2cta"))
 def test_long_rows_tensor_kernel(sb, kernel):
     """Rows past 2^23 bits take the 4-byte weight cycle (D = 8 x count):
     random rows, and all-ones rows of 2^26 bits (count 2^26, D = 2^29)."""
@@ -226,7 +227,7 @@ def _check_full_size(sb, n, m, p, seed, kernels, every_pair=False):
 def test_config1_full_size_every_pair(sb):
     """4096 rows x 65536 bits, Bernoulli(0.5): all 8,390,656 pairs against the
     reference's own kernel, and the four bitmap x bitmap kernels bit for bit."""
-    _check_full_size(sb, 4096, 65536, 0.5, 101, ["mma", "mma_db", "mma_ss", "popc"], every_pair=True)
+    _check_full_size(sb, 4096, 65536, 0.5, 101, ["mma", "mma_db", "mma_ss", "mma_2cta", "popc"], every_pair=True)
 
 
 def test_config5a_haplotypes_full_size(sb):
@@ -266,7 +267,7 @@ def test_config2_full_size_tensor_and_popc_kernels(sb):
     tensor-core kernel against the CUDA-core AND + POPC kernel -- an
     independent code path -- on all 2,147,516,416 pairs, plus sampled rows
     against the oracle, the diagonal and the sum identity."""
-    _check_full_size(sb, 65536, 262144, (0.05, 0.5), 202, ["mma", "popc"])
+    _check_full_size(sb, 65536, 262144, (0.05, 0.5), 202, ["mma", "mma_2cta", "popc"])
 
 
 def test_device_pointer_ingest_orders_after_producer(sb):
