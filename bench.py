@@ -963,13 +963,16 @@ def autotune_config1(sb, device):
         raise sb.StormError(rc, "STORM_contig_add_bitmaps")
     k, sched, times = c.autotune()
     names = ("tcgen05_ts_tiles", "tcgen05_ts_stream_k", "tcgen05_db_tiles", "tcgen05_db_stream_k", "tcgen05_ss",
-             "popc")
+             "popc", "tcgen05_cta_pair_tiles")
     c.close()
+    cand = [(sb.KERNEL_MMA, sb.SCHED_TILES), (sb.KERNEL_MMA, sb.SCHED_STREAM_K), (sb.KERNEL_MMA_DB, sb.SCHED_TILES),
+            (sb.KERNEL_MMA_DB, sb.SCHED_STREAM_K), (sb.KERNEL_MMA_SS, sb.SCHED_AUTO), (sb.KERNEL_POPC, sb.SCHED_AUTO),
+            (sb.KERNEL_MMA_2CTA, sb.SCHED_TILES)]
+    tops = {nm: round(2.0 * 4096 * 4097 / 2 * 65536 / (t * 1e-3) / 1e12, 1) for nm, t in zip(names, times) if t > 0}
     return {"workload": "4096 rows x 65536 bits, Bernoulli(0.5)",
             "candidates_ms": {nm: round(t, 4) for nm, t in zip(names, times)},
-            "kept": names[[(sb.KERNEL_MMA, sb.SCHED_TILES), (sb.KERNEL_MMA, sb.SCHED_STREAM_K),
-                           (sb.KERNEL_MMA_DB, sb.SCHED_TILES), (sb.KERNEL_MMA_DB, sb.SCHED_STREAM_K),
-                           (sb.KERNEL_MMA_SS, sb.SCHED_AUTO), (sb.KERNEL_POPC, sb.SCHED_AUTO)].index((k, sched))]}
+            "candidates_tops_int8": tops,
+            "kept": names[cand.index((k, sched))] if (k, sched) in cand else f"kernel {k} schedule {sched}"}
 
 
 def config45_forms(device):

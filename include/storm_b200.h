@@ -117,10 +117,11 @@ int STORM_contig_set_schedule(STORM_contiguous_t* c, int schedule);
  * all-pairs call on the GPU with each bitmap x bitmap kernel that is exact
  * for its row length -- tcgen05 with A in tensor memory (128 x 256 tiles,
  * then 128 x 192 double-buffered tiles), each under whole-tile and stream-K
- * schedules; tcgen05 with both operands in shared memory; CUDA-core POPC --
- * best of two calls each, and keeps the fastest kernel and schedule for
- * later calls.  times_ms (6 entries in that order, -1 when skipped) and the
- * choice are reported when non-NULL.  Counts do not depend on it. */
+ * schedules; tcgen05 with both operands in shared memory; CUDA-core POPC;
+ * tcgen05 on CTA pairs (whole tiles) -- best of two calls each, and keeps
+ * the fastest kernel and schedule for later calls.  times_ms (7 entries in
+ * that order, -1 when skipped) and the choice are reported when non-NULL.
+ * Counts do not depend on it. */
 int STORM_contig_autotune(STORM_contiguous_t* c, int* best_kernel, int* best_schedule, double* times_ms);
 /* Pack the rows into HBM now (otherwise done by the first all-pairs call). */
 int STORM_contig_upload(STORM_contiguous_t* c);

@@ -288,8 +288,8 @@ class StormContig:
 
     def autotune(self):
         """Time every exact kernel/schedule on these rows and keep the fastest:
-        (kernel, schedule, times_ms[6])."""
-        k, sc, t = C.c_int(0), C.c_int(0), (C.c_double * 6)()
+        (kernel, schedule, times_ms[7])."""
+        k, sc, t = C.c_int(0), C.c_int(0), (C.c_double * 7)()
         _check(_lib.STORM_contig_autotune(self.h, C.byref(k), C.byref(sc), t), "STORM_contig_autotune")
         return k.value, sc.value, list(t)
 

@@ -212,6 +212,199 @@ void ChunkDev::upload(const ChunkPack& p, cudaStream_t st) {
     SB_CUDA(cudaStreamSynchronize(st));
 }
 
+PinnedStage::~PinnedStage() {
+    for (int k = 0; k < 2; ++k) {
+        if (done[k]) {
+            cudaEventSynchronize(done[k]);
+            cudaEventDestroy(done[k]);
+        }
+        if (buf[k]) cudaFreeHost(buf[k]);
+    }
+}
+
+void PinnedStage::ensure() {
+    for (int k = 0; k < 2; ++k) {
+        if (!buf[k]) SB_CUDA(cudaHostAlloc((void**)&buf[k], BYTES, cudaHostAllocDefault));
+        if (!done[k]) SB_CUDA(cudaEventCreateWithFlags(&done[k], cudaEventDisableTiming));
+    }
+}
+
+// Splits [0, n) into at most `parts` contiguous ranges of about equal weight
+// (prefix[r] = weight of rows before r) and runs fn(r0, r1) on each, one
+// host thread per range.
+template <class F>
+static void parallel_rows(uint64_t n, const std::vector<uint64_t>& prefix, unsigned parts, F fn) {
+    if (n == 0) return;
+    const uint64_t total = prefix[n];
+    const uint64_t k = std::max<uint64_t>(1, std::min<uint64_t>({(uint64_t)parts, n, 1 + total / (4u << 20)}));
+    if (k <= 1) {
+        fn((uint64_t)0, n);
+        return;
+    }
+    std::vector<uint64_t> cut{0};
+    for (uint64_t r = 0; r < n && cut.size() < k; ++r)
+        if (prefix[r + 1] * k >= total * cut.size()) cut.push_back(r + 1);
+    if (cut.back() != n) cut.push_back(n);
+    std::vector<std::thread> th;
+    for (size_t t = 0; t + 1 < cut.size(); ++t)
+        if (cut[t] < cut[t + 1]) th.emplace_back(fn, cut[t], cut[t + 1]);
+    for (auto& t : th) t.join();
+}
+
+void ChunkDev::upload_rows(const STORM_bitmap_cont_t* rows, uint64_t n, cudaStream_t st, PinnedStage& stage) {
+    const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    auto live = [&](uint64_t r) { return rows[r].bitmaps && rows[r].block_ids ? rows[r].n_bitmaps : 0u; };
+    // Pass 1: per row its chunk count, bitmap words, list slots (each list on
+    // a multiple of 8 entries, as ChunkPack places them) and facts.
+    std::vector<uint64_t> c_base(n + 1, 0), b_base(n + 1, 0), l_base(n + 1, 0), l_used(n, 0), w1(n + 1, 0);
+    std::vector<uint8_t> has_list(n, 0);
+    std::vector<uint32_t> row_max(n, 0);
+    facts.assign(n, ChunkRowFacts{});
+    for (uint64_t r = 0; r < n; ++r) w1[r + 1] = w1[r] + 1 + live(r);
+    parallel_rows(n, w1, hw, [&](uint64_t r0, uint64_t r1) {
+        for (uint64_t r = r0; r < r1; ++r) {
+            ChunkRowFacts f;
+            uint64_t nb = 0, pos = 0;
+            uint32_t mx = 0;
+            const uint32_t k_n = live(r);
+            for (uint32_t k = 0; k < k_n; ++k) {
+                const STORM_bitmap_t& b = rows[r].bitmaps[k];
+                const uint32_t id = rows[r].block_ids[k];
+                ++f.chunks;
+                if (k > 0 && id <= rows[r].block_ids[k - 1]) f.plain = false;
+                if (b.n_bitmap) {
+                    ++nb;
+                    if (b.n_bitmap != CHUNK_WORDS || b.data == NULL) f.plain = false;
+                    f.card += b.n_bits_set;
+                    ++f.bitmap_chunks;
+                } else {
+                    const uint32_t ns = b.scalar ? b.n_scalar : 0;
+                    pos = (pos + 7) / 8 * 8 + ns;
+                    has_list[r] = 1;
+                    for (uint32_t e = 1; e < ns; ++e)
+                        if (b.scalar[e] <= b.scalar[e - 1]) {
+                            f.plain = false;
+                            break;
+                        }
+                    f.card += ns;
+                    f.list_entries += ns;
+                }
+                if (id > mx) mx = id;
+            }
+            facts[r] = f;
+            row_max[r] = mx;
+            c_base[r + 1] = k_n;
+            b_base[r + 1] = nb * CHUNK_WORDS;
+            l_used[r] = pos;
+            l_base[r + 1] = (pos + 7) / 8 * 8;
+        }
+    });
+    max_cid = 0;
+    for (uint64_t r = 0; r < n; ++r) {
+        c_base[r + 1] += c_base[r];
+        b_base[r + 1] += b_base[r];
+        l_base[r + 1] += l_base[r];
+        max_cid = std::max(max_cid, row_max[r]);
+    }
+    n_rows = n;
+    const uint64_t nc = c_base[n], nbw = b_base[n], nl = l_base[n];
+    // Pass 2: chunk metadata on host threads, then to the device.
+    std::vector<uint64_t> h_row_off(n + 1);
+    std::vector<uint32_t, NoInitAlloc<uint32_t>> h_cid(nc), h_ckl(nc);
+    std::vector<uint64_t, NoInitAlloc<uint64_t>> h_coff(nc);
+    for (uint64_t r = 0; r <= n; ++r) h_row_off[r] = c_base[r];
+    parallel_rows(n, w1, hw, [&](uint64_t r0, uint64_t r1) {
+        for (uint64_t r = r0; r < r1; ++r) {
+            uint64_t c = c_base[r], w = b_base[r], pos = 0;
+            const uint32_t k_n = live(r);
+            for (uint32_t k = 0; k < k_n; ++k, ++c) {
+                const STORM_bitmap_t& b = rows[r].bitmaps[k];
+                h_cid[c] = rows[r].block_ids[k];
+                if (b.n_bitmap) {
+                    h_coff[c] = w;
+                    h_ckl[c] = CK_BITMAP | (b.n_bitmap < CHUNK_WORDS ? b.n_bitmap : CHUNK_WORDS);
+                    w += CHUNK_WORDS;
+                } else {
+                    const uint32_t ns = b.scalar ? b.n_scalar : 0;
+                    pos = (pos + 7) / 8 * 8;
+                    h_coff[c] = l_base[r] + pos;
+                    uint32_t flags = ns & CK_LEN;
+                    for (uint32_t e = 1; e < ns; ++e)
+                        if (b.scalar[e] <= b.scalar[e - 1]) {
+                            flags |= CK_DUP;
+                            break;
+                        }
+                    h_ckl[c] = flags;
+                    pos += ns;
+                }
+            }
+        }
+    });
+    row_off.reserve(n + 1);
+    cid.reserve(nc ? nc : 1);
+    ckl.reserve(nc ? nc : 1);
+    coff.reserve(nc ? nc : 1);
+    bm.reserve(nbw ? nbw : 1);
+    lst.reserve(nl ? nl : 1);
+    SB_CUDA(cudaMemcpyAsync(row_off.p, h_row_off.data(), (n + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    if (nc) {
+        SB_CUDA(cudaMemcpyAsync(cid.p, h_cid.data(), nc * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        SB_CUDA(cudaMemcpyAsync(ckl.p, h_ckl.data(), nc * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        SB_CUDA(cudaMemcpyAsync(coff.p, h_coff.data(), nc * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    }
+    // Pass 3: payload slices (bitmaps, then lists, of consecutive rows)
+    // gathered into pinned buffers in turn, each copied while the next fills.
+    stage.ensure();
+    std::vector<uint64_t> pb(n + 1, 0);   // payload bytes of rows before r
+    for (uint64_t r = 0; r < n; ++r)
+        pb[r + 1] = pb[r] + (b_base[r + 1] - b_base[r]) * 8 + (l_base[r + 1] - l_base[r]) * 2;
+    uint64_t r0 = 0;
+    int k = 0;
+    while (r0 < n) {
+        uint64_t r1 = r0 + 1;
+        while (r1 < n && pb[r1 + 1] - pb[r0] <= PinnedStage::BYTES) ++r1;
+        const uint64_t bw = b_base[r1] - b_base[r0], lw = l_base[r1] - l_base[r0];
+        if (bw * 8 + lw * 2 > PinnedStage::BYTES) fail(STORM_B200_ELIMIT, "a row larger than the staging buffer");
+        if (stage.used[k]) SB_CUDA(cudaEventSynchronize(stage.done[k]));
+        unsigned char* sb = stage.buf[k];
+        uint64_t* sbm = reinterpret_cast<uint64_t*>(sb);
+        uint16_t* slst = reinterpret_cast<uint16_t*>(sb + bw * 8);
+        std::vector<uint64_t> wr(r1 - r0 + 1);
+        for (uint64_t r = r0; r <= r1; ++r) wr[r - r0] = pb[r] - pb[r0];
+        parallel_rows(r1 - r0, wr, hw, [&](uint64_t q0, uint64_t q1) {
+            for (uint64_t r = r0 + q0; r < r0 + q1; ++r) {
+                uint64_t w = b_base[r] - b_base[r0];
+                uint16_t* lr = slst + (l_base[r] - l_base[r0]);
+                std::memset(lr, 0, (l_base[r + 1] - l_base[r]) * sizeof(uint16_t));
+                uint64_t pos = 0;
+                const uint32_t k_n = live(r);
+                for (uint32_t q = 0; q < k_n; ++q) {
+                    const STORM_bitmap_t& b = rows[r].bitmaps[q];
+                    if (b.n_bitmap) {
+                        const uint32_t nw = b.n_bitmap < CHUNK_WORDS ? b.n_bitmap : CHUNK_WORDS;
+                        const uint32_t copied = b.data ? nw : 0;
+                        if (copied) std::memcpy(sbm + w, b.data, copied * sizeof(uint64_t));
+                        std::memset(sbm + w + copied, 0, (CHUNK_WORDS - copied) * sizeof(uint64_t));
+                        w += CHUNK_WORDS;
+                    } else {
+                        const uint32_t ns = b.scalar ? b.n_scalar : 0;
+                        pos = (pos + 7) / 8 * 8;
+                        if (ns) std::memcpy(lr + pos, b.scalar, ns * sizeof(uint16_t));
+                        pos += ns;
+                    }
+                }
+            }
+        });
+        if (bw) SB_CUDA(cudaMemcpyAsync(bm.p + b_base[r0], sbm, bw * 8, cudaMemcpyHostToDevice, st));
+        if (lw) SB_CUDA(cudaMemcpyAsync(lst.p + l_base[r0], slst, lw * 2, cudaMemcpyHostToDevice, st));
+        SB_CUDA(cudaEventRecord(stage.done[k], st));
+        stage.used[k] = true;
+        k ^= 1;
+        r0 = r1;
+    }
+    SB_CUDA(cudaStreamSynchronize(st));
+}
+
 template <class T>
 __device__ __forceinline__ uint32_t lower_bound_dev(const T* a, uint32_t n, T x) {
     uint32_t lo = 0, hi = n;

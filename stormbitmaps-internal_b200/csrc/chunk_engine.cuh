@@ -103,6 +103,17 @@ struct ChunkPack {
     void end_row() { row_off.push_back(cid.size()); }
 };
 
+// Pinned host staging for the pipelined upload: two buffers the packer
+// fills in turn while the other one's copy to the device runs.
+struct PinnedStage {
+    static constexpr uint64_t BYTES = 64ull << 20;   // per buffer; holds any one row (<= 16 MiB)
+    unsigned char* buf[2] = {nullptr, nullptr};
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    bool used[2] = {false, false};
+    ~PinnedStage();
+    void ensure();
+};
+
 struct ChunkDev {
     DevBuf<uint64_t> row_off, coff, bm;
     DevBuf<uint32_t> cid, ckl;
@@ -111,6 +122,12 @@ struct ChunkDev {
     std::vector<ChunkRowFacts> facts;   // host copy of the per-row facts
     uint32_t max_cid = 0;
     void upload(const ChunkPack& p, cudaStream_t st);
+    // The same layout as upload(ChunkPack::add_rows(rows, n)), without the
+    // host copy of the payload: the rows' chunk metadata is built on host
+    // threads, and their bitmaps and lists are gathered on host threads
+    // straight into pinned staging slices whose copies to the device run
+    // while the next slice is gathered.
+    void upload_rows(const STORM_bitmap_cont_t* rows, uint64_t n, cudaStream_t st, PinnedStage& stage);
     ChunkView view() const {
         return ChunkView{row_off.p, cid.p, ckl.p, coff.p, bm.p, lst.p};
     }

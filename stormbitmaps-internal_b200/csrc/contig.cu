@@ -246,17 +246,22 @@ int STORM_contig_autotune(STORM_contiguous_t* c, int* best_kernel, int* best_sch
         const uint64_t bits = c->vector_length;
         // tcgen05 (A in TMEM) with 128 x 256 tiles and with 128 x 192 double-
         // buffered tiles, each under both schedules; tcgen05 with both
-        // operands in shared memory; CUDA-core POPC -- each where it is exact.
-        const int kern[6] = {STORM_B200_KERNEL_MMA,    STORM_B200_KERNEL_MMA,    STORM_B200_KERNEL_MMA_DB,
-                             STORM_B200_KERNEL_MMA_DB, STORM_B200_KERNEL_MMA_SS, STORM_B200_KERNEL_POPC};
-        const int sched[6] = {STORM_B200_SCHED_TILES, STORM_B200_SCHED_STREAM_K, STORM_B200_SCHED_TILES,
-                              STORM_B200_SCHED_STREAM_K, STORM_B200_SCHED_AUTO, STORM_B200_SCHED_AUTO};
-        const bool ok[6] = {bits <= TC_MAX_ROW_BITS, bits <= TC_MAX_ROW_BITS, bits <= TC_MAX_ROW_BITS,
-                            bits <= TC_MAX_ROW_BITS, bits <= TC_SS_MAX_ROW_BITS, true};
+        // operands in shared memory; CUDA-core POPC; tcgen05 on CTA pairs --
+        // each where it is exact.
+        constexpr int NK = 7;
+        const int kern[NK] = {STORM_B200_KERNEL_MMA,    STORM_B200_KERNEL_MMA,    STORM_B200_KERNEL_MMA_DB,
+                              STORM_B200_KERNEL_MMA_DB, STORM_B200_KERNEL_MMA_SS, STORM_B200_KERNEL_POPC,
+                              STORM_B200_KERNEL_MMA_2CTA};
+        const int sched[NK] = {STORM_B200_SCHED_TILES,    STORM_B200_SCHED_STREAM_K, STORM_B200_SCHED_TILES,
+                               STORM_B200_SCHED_STREAM_K, STORM_B200_SCHED_AUTO,     STORM_B200_SCHED_AUTO,
+                               STORM_B200_SCHED_TILES};
+        const bool ok[NK] = {bits <= TC_MAX_ROW_BITS, bits <= TC_MAX_ROW_BITS,    bits <= TC_MAX_ROW_BITS,
+                             bits <= TC_MAX_ROW_BITS, bits <= TC_SS_MAX_ROW_BITS, true,
+                             bits <= TC_MAX_ROW_BITS};
         const int keep_sched = c->engine.schedule;
         double best = -1.0;
         int bk = c->kernel_pref, bs = keep_sched;
-        for (int k = 0; k < 6; ++k) {
+        for (int k = 0; k < NK; ++k) {
             if (times_ms) times_ms[k] = -1.0;
             if (!ok[k] || n == 0) continue;
             c->engine.schedule = sched[k];

@@ -40,6 +40,7 @@ static void* aligned_alloc64(size_t bytes) {
 // room for it).  Invalidated by every mutating call through this library.
 struct StormDev {
     ChunkDev dev;
+    PinnedStage stage;
     ChunkEngine engine;
     cudaStream_t stream = nullptr;
     DevBuf<uint32_t> d_out;
@@ -112,9 +113,7 @@ static uint64_t row_shape(const STORM_t* s) {
 static void ensure_packed(const STORM_t* s, StormDev* d) {
     const uint64_t shape = row_shape(s);
     if (d->valid && d->shape == shape) return;
-    ChunkPack p;
-    p.add_rows(s->conts, s->n_conts);
-    d->dev.upload(p, stream_of(d));
+    d->dev.upload_rows(s->conts, s->n_conts, stream_of(d), d->stage);
     d->valid = true;
     d->shape = shape;
 }
