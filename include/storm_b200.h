@@ -300,6 +300,22 @@ uint64_t STORM_last_postings_rows(const STORM_t* s);
 int STORM_set_panel(STORM_t* s, int mode);
 /* Rows the last per-pair call stored in the transposed panel. */
 uint64_t STORM_last_panel_rows(const STORM_t* s);
+/* Per engine of the last per-pair call -- out8[0..3]: device ms of the
+ * tensor cores, the chunk kernel, the transposed panel and the postings
+ * (with their histogram); out8[4..7]: the planner's predicted ms for the work
+ * it gave each (0 for the chunk kernel, which it does not price). */
+int STORM_last_engine_ms(const STORM_t* s, double* out8);
+/* GPU calibration of the planner (no counterpart in the reference's C ABI;
+ * its calibrate_on_rows fits the kernel layer's constants on the host,
+ * storm_cost.cpp:779-895): on a strided sample of up to sample_rows rows (0:
+ * 2048) every plain row is counted on the tensor cores, then in the
+ * transposed panel, then the list rows by postings; each engine's constants
+ * are scaled by its measured / predicted device time, and later plans of s
+ * use them.  out (4 entries, may be NULL): the tensor, panel and postings
+ * scales and the sample's row count.  Counts never depend on it. */
+int STORM_calibrate(STORM_t* s, uint32_t sample_rows, double* out);
+/* Back to the planner's built-in constants. */
+int STORM_reset_cost_model(STORM_t* s);
 
 #ifdef __cplusplus
 } /* extern "C" */

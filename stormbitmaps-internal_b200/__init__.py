@@ -114,6 +114,9 @@ _sig("STORM_last_dense_panels", C.c_uint64, [C.c_void_p])
 _sig("STORM_set_sparse_postings", C.c_int, [C.c_void_p, C.c_int])
 _sig("STORM_last_postings_rows", C.c_uint64, [C.c_void_p])
 _sig("STORM_set_panel", C.c_int, [C.c_void_p, C.c_int])
+_sig("STORM_last_engine_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_double)])
+_sig("STORM_calibrate", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_double)])
+_sig("STORM_reset_cost_model", C.c_int, [C.c_void_p])
 _sig("STORM_last_panel_rows", C.c_uint64, [C.c_void_p])
 
 
@@ -479,6 +482,21 @@ class Storm:
 
     def last_postings_rows(self) -> int:
         return int(_lib.STORM_last_postings_rows(self.h))
+
+    def last_engine_ms(self):
+        """{engine: (device ms, predicted ms)} of the last per-pair call."""
+        o = (C.c_double * 8)()
+        _check(_lib.STORM_last_engine_ms(self.h, o), "STORM_last_engine_ms")
+        return {k: (o[i], o[4 + i]) for i, k in enumerate(("tensor", "chunk", "panel", "postings"))}
+
+    def calibrate(self, sample_rows: int = 0):
+        """GPU calibration of the planner: (tensor, panel, postings) scales and sample rows."""
+        o = (C.c_double * 4)()
+        _check(_lib.STORM_calibrate(self.h, sample_rows, o), "STORM_calibrate")
+        return list(o)
+
+    def reset_cost_model(self):
+        _check(_lib.STORM_reset_cost_model(self.h), "STORM_reset_cost_model")
 
     def set_panel(self, mode: int):
         _check(_lib.STORM_set_panel(self.h, int(mode)), "STORM_set_panel")

@@ -1211,6 +1211,28 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         if (d_out) SB_CUDA(cudaMemsetAsync(d_out, 0, tri_size(n) * sizeof(uint32_t), st));
     }
 
+    // ---- predicted device time of each engine for this plan
+    for (int k = 0; k < 4; ++k) last_engine_ms[k] = last_engine_pred_ms[k] = 0.0;
+    for (cudaEvent_t& e : ev_eng)
+        if (!e) SB_CUDA(cudaEventCreate(&e));
+    {
+        const double dd = (double)nd, tqn = (double)tq.size();
+        last_engine_pred_ms[0] = 1e-6 * tc_ns * (dd * (dd + 1.0) / 2.0 + dd * tqn);
+        if (panel_plan && (nm || nd) && (nq + nm)) {
+            const double npw = (double)(nm + nd), nb = std::ceil(npw / PANEL_ROWS);
+            double vb = 0.0, pairs = 0.0;
+            for (uint64_t w = nc; w < nc + nq + nm; ++w) {
+                const double after = (double)(n - 1 - w) < npw ? (double)(n - 1 - w) : npw;   // panel rows after it
+                vb += (double)d.facts[h_perm[w]].card * std::ceil(after / PANEL_ROWS);
+                pairs += after;
+            }
+            last_engine_pred_ms[2] = 1e-6 * (cost.ns_per_panel_value * vb + cost.ns_per_panel_pair * pairs +
+                                             nb * 3.0 * PANEL_ROWS * (double)W * 8.0 * cost.ns_per_panel_byte);
+        }
+        if (nq) last_engine_pred_ms[3] = 1e-6 * post_ns((double)ps.pairs, nq);
+    }
+    SB_CUDA(cudaEventRecord(ev_eng[0], st));   // the postings' histogram and the set-up precede it
+
     // ---- tensor cores: H x H and H x tq, panel by panel
     if (nd) {
         std::vector<uint32_t> emap(nd_pad + tq.size(), ~0u);   // expanded row -> stored row (~0: padding)
@@ -1267,8 +1289,10 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         last_dense_rows = nd;
         last_dense_panels = npan;
     }
+    SB_CUDA(cudaEventRecord(ev_eng[1], st));
     // ---- chunk kernel: every pair with a C row (the walk's triangle prefix)
     chunk_launch(PAIRS_TRIANGLE, nc * n - (nc * (nc - 1)) / 2 * (nc ? 1 : 0), perm, 0, 0, n, 0);
+    SB_CUDA(cudaEventRecord(ev_eng[2], st));
     // ---- transposed panel: (L u M) x (M u H), blocks of PANEL_ROWS panel rows
     if (panel_plan && (nm || nd) && (nq + nm)) {
         const uint64_t pw0 = nc + nq;                      // walk position of the first panel row
@@ -1322,6 +1346,7 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         last_panel_rows = npw;
         last_panel_queries = nq + nm;
     }
+    SB_CUDA(cudaEventRecord(ev_eng[3], st));
     // ---- L x L by postings
     uint64_t q_sum = 0;
     if (nq) {
@@ -1364,7 +1389,18 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         SB_CUDA(cudaGetLastError());
         ++launches;
     }
-    return finish(q_sum);
+    const uint64_t total = finish(q_sum);
+    float t_pre = 0, t_tc = 0, t_ch = 0, t_pa = 0, t_po = 0;
+    SB_CUDA(cudaEventElapsedTime(&t_pre, log.ev0, ev_eng[0]));
+    SB_CUDA(cudaEventElapsedTime(&t_tc, ev_eng[0], ev_eng[1]));
+    SB_CUDA(cudaEventElapsedTime(&t_ch, ev_eng[1], ev_eng[2]));
+    SB_CUDA(cudaEventElapsedTime(&t_pa, ev_eng[2], ev_eng[3]));
+    SB_CUDA(cudaEventElapsedTime(&t_po, ev_eng[3], log.ev1));
+    last_engine_ms[0] = t_tc;
+    last_engine_ms[1] = t_ch;
+    last_engine_ms[2] = t_pa;
+    last_engine_ms[3] = t_po + (nq ? t_pre : 0.f);
+    return total;
 }
 
 }  // namespace sb200

@@ -197,6 +197,12 @@ struct ChunkEngine {
                                        // 2 every plain row in it
     uint64_t last_dense_rows = 0, last_dense_panels = 0, last_postings_rows = 0;
     uint64_t last_panel_rows = 0, last_panel_queries = 0;
+    // Per engine of the last per-pair triangle call -- tensor cores, chunk
+    // kernel, transposed panel, postings (with the histograms): device ms
+    // (events between the engines on the stream) and the cost model's
+    // prediction for the work it gave each.
+    double last_engine_ms[4] = {0, 0, 0, 0}, last_engine_pred_ms[4] = {0, 0, 0, 0};
+    cudaEvent_t ev_eng[4] = {nullptr, nullptr, nullptr, nullptr};
     DevBuf<uint64_t> d_pX, d_DT;       // panel block: expanded rows, transposed
     DevBuf<uint32_t> d_xorder, d_pmap, d_mrows;
     DevBuf<unsigned long long> d_ctr;
@@ -206,7 +212,11 @@ struct ChunkEngine {
     DevBuf<PostingsStats> d_pstats;
     DevBuf<uint64_t> d_panel;
     DevBuf<uint2> d_tiles;
-    ~ChunkEngine() { log.destroy(); }
+    ~ChunkEngine() {
+        log.destroy();
+        for (cudaEvent_t e : ev_eng)
+            if (e) cudaEventDestroy(e);
+    }
     // Returns the sum over i < j (triangle) or over all (i, j) (rect).
     uint64_t run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_t n2, uint32_t* d_out,
                  cudaStream_t st);

@@ -775,6 +775,81 @@ int STORM_set_sparse_postings(STORM_t* s, int mode) {
 
 uint64_t STORM_last_postings_rows(const STORM_t* s) { return s ? state_of(s)->engine.last_postings_rows : 0; }
 
+int STORM_last_engine_ms(const STORM_t* s, double* out8) {
+    if (s == NULL) return STORM_B200_ENULL;
+    if (out8 == NULL) return STORM_B200_EVALUES;
+    const ChunkEngine& e = state_of(s)->engine;
+    for (int k = 0; k < 4; ++k) {
+        out8[k] = e.last_engine_ms[k];
+        out8[4 + k] = e.last_engine_pred_ms[k];
+    }
+    return 0;
+}
+
+// The planner's constants fitted to this GPU on a sample of the rows (the
+// reference's calibrate_on_rows, storm_cost.cpp:779-895, samples the
+// caller's pairs the same way: strided, not the first rows): every plain row
+// of the sample on the tensor cores, then in the transposed panel, then the
+// list rows by postings; per engine the ratio of measured to predicted
+// device time (best of two) scales that engine's constants.
+int STORM_calibrate(STORM_t* s, uint32_t sample_rows, double* out) {
+    if (s == NULL) return STORM_B200_ENULL;
+    return guard([&]() -> int {
+        StormDev* d = state_of(s);
+        const uint64_t n = s->n_conts;
+        const uint64_t m = std::min<uint64_t>(n, sample_rows ? sample_rows : 2048);
+        if (m < 2) return STORM_B200_EARG;
+        ChunkPack p;
+        for (uint64_t k = 0; k < m; ++k) p.add_row(&s->conts[k * n / m]);
+        cudaStream_t st = stream_of(d);
+        ChunkDev cd;
+        cd.upload(p, st);
+        ChunkEngine e;
+        e.cost = d->engine.cost;
+        DevBuf<uint32_t> out_buf;
+        out_buf.reserve(tri_size(m));
+        // engine k: (dense_min_density, postings_mode, panel_mode) forcing it
+        const double dens[3] = {1e-12, 0.0, 0.0};
+        const int post[3] = {0, -1, 1}, pan[3] = {0, 2, 0}, eng[3] = {0, 2, 3};
+        double scale[3] = {1.0, 1.0, 1.0};
+        for (int k = 0; k < 3; ++k) {
+            e.dense_min_density = dens[k];
+            e.postings_mode = post[k];
+            e.panel_mode = pan[k];
+            double meas = -1.0, pred = 0.0;
+            for (int rep = 0; rep < 2; ++rep) {
+                e.run(cd, PAIRS_TRIANGLE, m, 0, out_buf.p, st);
+                const double ms = e.last_engine_ms[eng[k]];
+                meas = meas < 0 ? ms : std::min(meas, ms);
+                pred = e.last_engine_pred_ms[eng[k]];
+            }
+            if (pred > 1e-4 && meas > 0) scale[k] = meas / pred;
+        }
+        ChunkCostModel& c = d->engine.cost;
+        c.ns_per_tensor_bit *= scale[0];
+        c.ns_per_panel_value *= scale[1];
+        c.ns_per_panel_pair *= scale[1];
+        c.ns_per_panel_byte *= scale[1];
+        c.ns_per_posting_pair *= scale[2];
+        c.ns_per_posting_pair_hbm *= scale[2];
+        c.ns_per_posting_sweep *= scale[2];
+        c.ns_per_sweep_row_pair *= scale[2];
+        if (out) {
+            out[0] = scale[0];
+            out[1] = scale[1];
+            out[2] = scale[2];
+            out[3] = (double)m;
+        }
+        return 0;
+    });
+}
+
+int STORM_reset_cost_model(STORM_t* s) {
+    if (s == NULL) return STORM_B200_ENULL;
+    state_of(s)->engine.cost = ChunkCostModel{};
+    return 0;
+}
+
 int STORM_set_panel(STORM_t* s, int mode) {
     if (s == NULL) return STORM_B200_ENULL;
     if (mode < -1 || mode > 2) return STORM_B200_EARG;

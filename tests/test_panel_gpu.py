@@ -84,3 +84,27 @@ def test_panel_beside_chunk_rows(sb):
     strict = iu[0] != iu[1]
     np.testing.assert_array_equal(mat[strict], want[strict])
     assert s.pairw_intersect_cardinality() == ws
+
+
+def test_planner_calibration_keeps_counts(sb):
+    """STORM_calibrate scales the planner's constants by the measured /
+    predicted device time of each engine on a strided row sample; the plans
+    it leads to give the oracle's counts, and every engine's time of the
+    last call is reported beside its prediction."""
+    sets = gen.zipf_sets(700, 1 << 20, 1.1, 16, 1 << 17, 304)
+    s = build_storm(sb, sets)
+    vals, offs = gen.to_csr(sets)
+    want, ws = ol.sets_matrix(vals, offs)
+    scales = s.calibrate(256)
+    assert scales[3] == 256
+    assert all(x > 0 for x in scales[:3]), scales
+    mat, ssum = s.matrix()
+    assert ssum == ws
+    np.testing.assert_array_equal(mat, want)
+    eng = s.last_engine_ms()
+    assert all(v[0] >= 0 for v in eng.values())
+    assert sum(v[0] for v in eng.values()) > 0
+    s.reset_cost_model()
+    mat, ssum = s.matrix()
+    assert ssum == ws
+    np.testing.assert_array_equal(mat, want)
