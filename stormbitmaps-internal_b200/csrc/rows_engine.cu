@@ -79,10 +79,20 @@ __global__ void block_meta_kernel(RowsView v, const uint32_t* __restrict__ order
     het_x1000[b] = mean > 0 ? (uint32_t)fmin(4e9, 1000.0 * (double)mx / mean) : 1000u;
 }
 
-// Block zone maps (one CTA per row block of the traversal order): the bins
-// of the block's values, from each row's zone map where it has one, else from
-// up to 1024 of its values (evenly strided; the overlap is a selection
-// feature, not a count).
+// Block zone maps (one CTA per row block of the traversal order): a
+// superset of the coarse bins holding the block's values -- from each row's
+// zone map where it has one (storm_repr.cpp:47-59: 512-value bins), from its
+// values when it has at most ZONE_EXACT_MAX of them, else every bin of its
+// [first, last] span.  Two blocks whose maps share no bin share no value:
+// every pair of their tile is empty (the tile-granular form of the zone-map
+// transpose of bench/bench_tile.cpp:224-264); their overlap is also a
+// feature of the learned selector.
+constexpr uint64_t ZONE_EXACT_MAX = 16384;
+
+__device__ __forceinline__ void zone_set_range(unsigned long long* z, uint64_t c0, uint64_t c1) {
+    for (uint64_t cb = c0; cb <= c1; ++cb) atomicOr(&z[cb >> 6], 1ull << (cb & 63));
+}
+
 __global__ void __launch_bounds__(256)
 block_zone_kernel(RowsView v, const uint32_t* __restrict__ order, uint32_t n, uint32_t T,
                   uint64_t* __restrict__ out) {
@@ -92,27 +102,39 @@ block_zone_kernel(RowsView v, const uint32_t* __restrict__ order, uint32_t n, ui
     for (uint32_t k = threadIdx.x; k < BZONE_WORDS; k += blockDim.x) z[k] = 0ull;
     __syncthreads();
     const uint64_t ubits = (uint64_t)v.nw * 64;
+    const uint64_t nbins = BZONE_WORDS * 64;
+    auto bin_of = [&](uint64_t x) { return x * nbins / ubits; };
     for (uint32_t k = lo; k < hi; ++k) {
         const uint32_t row = order[k];
+        const RowMetaD& m = v.meta[row];
+        if (m.card == 0) continue;
+        const uint64_t s0 = v.s_off[row], len = v.s_off[row + 1] - s0;
         if (v.oc_off[row] != NONE) {
             const uint64_t* oc = v.oc + v.oc_off[row];
             for (uint32_t w = threadIdx.x; w < v.n_occ; w += blockDim.x)
                 for (uint64_t x = oc[w]; x; x &= x - 1) {
                     const uint64_t bin = (uint64_t)w * 64 + (uint64_t)(__ffsll((long long)x) - 1);
-                    const uint64_t cb = bin * 512 * (BZONE_WORDS * 64) / ubits;
-                    atomicOr(&z[cb >> 6], 1ull << (cb & 63));
+                    const uint64_t first = bin * 512, last = min(first + 511, ubits - 1);
+                    zone_set_range(z, bin_of(first), bin_of(last));
                 }
-        } else {
-            const uint64_t s0 = v.s_off[row], len = v.s_off[row + 1] - s0;
-            const uint64_t step = len > 1024 ? len / 1024 : 1;
-            for (uint64_t e = (uint64_t)threadIdx.x * step; e < len; e += (uint64_t)blockDim.x * step) {
-                const uint64_t cb = (uint64_t)v.s_val[s0 + e] * (BZONE_WORDS * 64) / ubits;
+        } else if (len <= ZONE_EXACT_MAX) {
+            for (uint64_t e = threadIdx.x; e < len; e += blockDim.x) {
+                const uint64_t cb = bin_of(v.s_val[s0 + e]);
                 atomicOr(&z[cb >> 6], 1ull << (cb & 63));
             }
+        } else {
+            const uint64_t c0 = bin_of(m.first), c1 = bin_of(m.last);
+            for (uint64_t cb = c0 + threadIdx.x; cb <= c1; cb += blockDim.x) atomicOr(&z[cb >> 6], 1ull << (cb & 63));
         }
     }
     __syncthreads();
     for (uint32_t k = threadIdx.x; k < BZONE_WORDS; k += blockDim.x) out[(uint64_t)b * BZONE_WORDS + k] = z[k];
+}
+
+__device__ __forceinline__ bool zones_disjoint(const uint64_t* za, const uint64_t* zb) {
+    for (uint32_t k = 0; k < BZONE_WORDS; ++k)
+        if (za[k] & zb[k]) return false;
+    return true;
 }
 
 // Tile (ti, tj), ti <= tj, from a linear index over the block triangle.
@@ -142,6 +164,13 @@ __global__ void select_tiles_kernel(const RowMetaD* __restrict__ bmeta, const ui
     const RowMetaD& a = bmeta[ti];
     const RowMetaD& b = bmeta[tj];
     TileDecision d{P_BB, P_BB};
+    // Whole-tile rejection: blocks whose zone maps do not meet hold no
+    // common value, so every pair of the tile is empty.
+    if (policy != STORM_POLICY_ALLBITMAP && bzone != nullptr && ti != tj &&
+        zones_disjoint(bzone + (uint64_t)ti * BZONE_WORDS, bzone + (uint64_t)tj * BZONE_WORDS)) {
+        dec[t] = TileDecision{P_EMPTY, P_EMPTY};
+        return;
+    }
     if (policy == STORM_POLICY_ALLBITMAP) {
         d.cell = d.cell2 = P_BB;
     } else if (policy == STORM_POLICY_FIXED) {
@@ -218,6 +247,10 @@ __device__ __forceinline__ uint32_t pair_count(const PairCtx& c, uint32_t oi, ui
     if (ri == rj) {
         used = -1;
         return lane == 0 ? mi.card : 0u;
+    }
+    if (td.cell == P_EMPTY) {   // the whole tile was rejected by its blocks' zone maps
+        used = P_EMPTY;
+        return 0;
     }
     const bool i_dense = mi.card >= mj.card;
     const uint32_t d = i_dense ? ri : rj, s = i_dense ? rj : ri;
@@ -561,10 +594,9 @@ static void rows_run(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell,
         }
     }
     const bool learned = policy == STORM_POLICY_LEARNED && r->mlp.trained;
-    if (learned) {
-        r->mlp.ensure_device(st);
-        r->d_bzone.reserve((uint64_t)nb * BZONE_WORDS);
-    }
+    if (learned) r->mlp.ensure_device(st);
+    const bool zones = policy != STORM_POLICY_ALLBITMAP;   // tile rejection and the learned feature
+    if (zones) r->d_bzone.reserve((uint64_t)nb * BZONE_WORDS);
 
     // slices per tile so the launch has enough CTAs
     const int sms = require_device();
@@ -585,9 +617,9 @@ static void rows_run(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell,
     auto phases_1_2 = [&]() {
         SB_CUDA(cudaMemsetAsync(r->d_stats.p, 0, sizeof(RowsStatsDev), st));
         block_meta_kernel<<<(nb + 127) / 128, 128, 0, st>>>(c.v, c.order, n, T, r->d_bmeta.p, r->d_het.p);
-        if (learned) block_zone_kernel<<<nb, 256, 0, st>>>(c.v, c.order, n, T, r->d_bzone.p);
+        if (zones) block_zone_kernel<<<nb, 256, 0, st>>>(c.v, c.order, n, T, r->d_bzone.p);
         select_tiles_kernel<<<(ntiles + 127) / 128, 128, 0, st>>>(
-            r->d_bmeta.p, r->d_het.p, learned ? r->d_bzone.p : nullptr, nb,
+            r->d_bmeta.p, r->d_het.p, zones ? r->d_bzone.p : nullptr, nb,
             learned ? policy : (policy == STORM_POLICY_LEARNED ? STORM_POLICY_PERTILE : policy), fixed_cell, c.model,
             learned ? r->mlp.d_params.p : nullptr, r->mlp.shape, r->d_dec.p);
         if (policy == STORM_POLICY_PROBE)
@@ -618,7 +650,7 @@ static void rows_run(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell,
                                            nd ? ptr(r->d_dtiles.p) : 0ull,
                                            nd ? ptr(r->d_dflags.p) : 0ull,
                                            learned ? ptr(r->mlp.d_params.p) : 0ull,
-                                           learned ? ptr(r->d_bzone.p) : 0ull,
+                                           zones ? ptr(r->d_bzone.p) : 0ull,
                                            learned ? ((uint64_t)r->mlp.shape.H << 40 | (uint64_t)r->mlp.shape.F << 20 |
                                                       r->mlp.shape.C)
                                                    : 0ull};
