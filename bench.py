@@ -782,6 +782,31 @@ def triangle_row_sums(d_tri, n):
     return got, diag
 
 
+def engine_roofline(eng, device):
+    """Per STORM_t engine of the last call: device ms, the planner's
+    prediction, and the engine's roofline -- the tensor cores against the
+    measured 8-bit tensor peak, the panel and the postings (bytes they must
+    move) against the measured HBM bandwidth."""
+    peaks, src = measured_peaks()
+    tpk, _ = tensor_peak_tops(device)
+    out = {}
+    for name, (ms, pred, work) in eng.items():
+        if ms <= 0 and work <= 0:
+            continue
+        e = {"ms": round(ms, 3), "predicted_ms": round(pred, 3)}
+        if ms > 0 and work > 0:
+            if name == "tensor":
+                e.update({"tops_int8": work / (ms * 1e-3) / 1e12, "frac_of_tensor_peak": work / (ms * 1e-3) / 1e12 / tpk})
+            elif name in ("panel", "postings"):
+                gbs = work / (ms * 1e-3) / 1e9
+                e.update({"alg_bytes": work, "GBps": gbs, "frac_of_hbm": gbs / peaks["hbm_gbs"],
+                          "hbm_peak_source": src})
+            else:
+                e.update({"pairs": work})
+        out[name] = e
+    return out
+
+
 def storm_t_full(device, names=tuple(FULL_CORPORA), cpu_seconds=2.0):
     """The sparse and mixed-density configurations at full size through
     STORM_t: rows generated on the GPU and appended from host memory
@@ -833,7 +858,9 @@ def storm_t_full(device, names=tuple(FULL_CORPORA), cpu_seconds=2.0):
             ms = st.last_kernel_ms()
             best = ms if best is None else min(best, ms)
         r["device"] = {"ms": round(best, 2), "pairs_per_s": tri / (best * 1e-3), "ns_per_pair": best * 1e6 / tri,
-                       "tensor_rows": st.last_dense()[0], "postings_rows": st.last_postings_rows()}
+                       "tensor_rows": st.last_dense()[0], "postings_rows": st.last_postings_rows(),
+                       "panel_rows": st.last_panel_rows()}
+        r["engines"] = engine_roofline(st.last_engine_ms(), device)
         got_row, diag = triangle_row_sums(d_tri, n)
         ok = (bool(torch.equal(diag.cpu(), torch.as_tensor(cards))) and
               int((got_row != res["want_row"]).sum().item()) == 0 and sums == {want_sum})

@@ -300,11 +300,17 @@ uint64_t STORM_last_postings_rows(const STORM_t* s);
 int STORM_set_panel(STORM_t* s, int mode);
 /* Rows the last per-pair call stored in the transposed panel. */
 uint64_t STORM_last_panel_rows(const STORM_t* s);
-/* Per engine of the last per-pair call -- out8[0..3]: device ms of the
+/* Per engine of the last per-pair call -- out12[0..3]: device ms of the
  * tensor cores, the chunk kernel, the transposed panel and the postings
- * (with their histogram); out8[4..7]: the planner's predicted ms for the work
- * it gave each (0 for the chunk kernel, which it does not price). */
-int STORM_last_engine_ms(const STORM_t* s, double* out8);
+ * (with their histogram); out12[4..7]: the planner's predicted ms for the
+ * work it gave each (0 for the chunk kernel, which it does not price);
+ * out12[8..11]: that work -- tensor cores in int8 operations (2 x pairs x
+ * universe bits), chunk kernel in pairs, panel and postings in the bytes
+ * they must move (panel: a 256-byte transposed line per query value and
+ * 2048-row block, the expanded and transposed blocks, 4 bytes per count;
+ * postings: 8 bytes per value, per list entry and per increment, and the
+ * universe-sized histogram). */
+int STORM_last_engine_ms(const STORM_t* s, double* out12);
 /* GPU calibration of the planner (no counterpart in the reference's C ABI;
  * its calibrate_on_rows fits the kernel layer's constants on the host,
  * storm_cost.cpp:779-895): on a strided sample of up to sample_rows rows (0:

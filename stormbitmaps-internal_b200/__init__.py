@@ -484,10 +484,12 @@ class Storm:
         return int(_lib.STORM_last_postings_rows(self.h))
 
     def last_engine_ms(self):
-        """{engine: (device ms, predicted ms)} of the last per-pair call."""
-        o = (C.c_double * 8)()
+        """{engine: (device ms, predicted ms, work)} of the last per-pair call
+        (work: int8 ops for the tensor cores, pairs for the chunk kernel,
+        bytes for the panel and the postings)."""
+        o = (C.c_double * 12)()
         _check(_lib.STORM_last_engine_ms(self.h, o), "STORM_last_engine_ms")
-        return {k: (o[i], o[4 + i]) for i, k in enumerate(("tensor", "chunk", "panel", "postings"))}
+        return {k: (o[i], o[4 + i], o[8 + i]) for i, k in enumerate(("tensor", "chunk", "panel", "postings"))}
 
     def calibrate(self, sample_rows: int = 0):
         """GPU calibration of the planner: (tensor, panel, postings) scales and sample rows."""

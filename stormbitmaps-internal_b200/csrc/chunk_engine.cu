@@ -1212,12 +1212,14 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
     }
 
     // ---- predicted device time of each engine for this plan
-    for (int k = 0; k < 4; ++k) last_engine_ms[k] = last_engine_pred_ms[k] = 0.0;
+    for (int k = 0; k < 4; ++k) last_engine_ms[k] = last_engine_pred_ms[k] = last_engine_work[k] = 0.0;
     for (cudaEvent_t& e : ev_eng)
         if (!e) SB_CUDA(cudaEventCreate(&e));
     {
         const double dd = (double)nd, tqn = (double)tq.size();
         last_engine_pred_ms[0] = 1e-6 * tc_ns * (dd * (dd + 1.0) / 2.0 + dd * tqn);
+        last_engine_work[0] = 2.0 * (dd * (dd + 1.0) / 2.0 + dd * tqn) * (double)U;
+        last_engine_work[1] = (double)(nc * n - (nc * (nc - 1)) / 2 * (nc ? 1 : 0));
         if (panel_plan && (nm || nd) && (nq + nm)) {
             const double npw = (double)(nm + nd), nb = std::ceil(npw / PANEL_ROWS);
             double vb = 0.0, pairs = 0.0;
@@ -1228,8 +1230,14 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
             }
             last_engine_pred_ms[2] = 1e-6 * (cost.ns_per_panel_value * vb + cost.ns_per_panel_pair * pairs +
                                              nb * 3.0 * PANEL_ROWS * (double)W * 8.0 * cost.ns_per_panel_byte);
+            last_engine_work[2] = 256.0 * vb + 4.0 * pairs + nb * 3.0 * PANEL_ROWS * (double)W * 8.0;
         }
-        if (nq) last_engine_pred_ms[3] = 1e-6 * post_ns((double)ps.pairs, nq);
+        if (nq) {
+            last_engine_pred_ms[3] = 1e-6 * post_ns((double)ps.pairs, nq);
+            double vals = 0.0;
+            for (uint32_t r : qrows) vals += (double)d.facts[r].card;
+            last_engine_work[3] = 8.0 * vals + 8.0 * (double)ps.entries + 8.0 * (double)ps.pairs + 8.0 * (double)U;
+        }
     }
     SB_CUDA(cudaEventRecord(ev_eng[0], st));   // the postings' histogram and the set-up precede it
 

@@ -202,6 +202,13 @@ struct ChunkEngine {
     // (events between the engines on the stream) and the cost model's
     // prediction for the work it gave each.
     double last_engine_ms[4] = {0, 0, 0, 0}, last_engine_pred_ms[4] = {0, 0, 0, 0};
+    // ... and the algorithmic work of each: tensor cores in int8 operations
+    // (2 x pairs x universe bits), chunk kernel in pairs, the panel and the
+    // postings in bytes they must move (panel: one 256-byte transposed line
+    // per query value and block, the expanded and transposed blocks, 4 bytes
+    // per count written; postings: the histogram and list entries, 8 bytes
+    // per increment -- a read and a write of its count).
+    double last_engine_work[4] = {0, 0, 0, 0};
     cudaEvent_t ev_eng[4] = {nullptr, nullptr, nullptr, nullptr};
     DevBuf<uint64_t> d_pX, d_DT;       // panel block: expanded rows, transposed
     DevBuf<uint32_t> d_xorder, d_pmap, d_mrows;

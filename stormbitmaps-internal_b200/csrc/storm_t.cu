@@ -775,13 +775,14 @@ int STORM_set_sparse_postings(STORM_t* s, int mode) {
 
 uint64_t STORM_last_postings_rows(const STORM_t* s) { return s ? state_of(s)->engine.last_postings_rows : 0; }
 
-int STORM_last_engine_ms(const STORM_t* s, double* out8) {
+int STORM_last_engine_ms(const STORM_t* s, double* out12) {
     if (s == NULL) return STORM_B200_ENULL;
-    if (out8 == NULL) return STORM_B200_EVALUES;
+    if (out12 == NULL) return STORM_B200_EVALUES;
     const ChunkEngine& e = state_of(s)->engine;
     for (int k = 0; k < 4; ++k) {
-        out8[k] = e.last_engine_ms[k];
-        out8[4 + k] = e.last_engine_pred_ms[k];
+        out12[k] = e.last_engine_ms[k];
+        out12[4 + k] = e.last_engine_pred_ms[k];
+        out12[8 + k] = e.last_engine_work[k];
     }
     return 0;
 }
