@@ -370,11 +370,6 @@ def mixed_density_forms(sb, device, n=4096, universe=1 << 20, tile=64):
     out = {"workload": f"{n} rows over 2^{universe.bit_length() - 1}, card ~ Zipf(1.1) on [16, 2^"
                        f"{(universe // 4).bit_length() - 1}], uniform w/o replacement; tile {tile}",
            "pairs": pairs, "generate_s": round(t_gen, 2)}
-    t0 = time.perf_counter()
-    sel = r.train_selector(tile=tile, samples=1024, epochs=400, seed=7)
-    out["train_s"] = round(time.perf_counter() - t0, 2)
-    out["selector"] = {k: (round(v, 4) if isinstance(v, float) else v) for k, v in sel.items()}
-
     def best_of(policy, exec_, reps=3, tile=tile):
         times, s = [], None
         for _ in range(reps):
@@ -383,7 +378,17 @@ def mixed_density_forms(sb, device, n=4096, universe=1 << 20, tile=64):
         return s, min(times), st
 
     forms = {}
-    ref_sum = None
+    # the reference's default constants (Apple M4, storm_cost.cpp:482-496) before any calibration
+    r.set_dense_block(0.0)
+    s0, ns0, st0 = best_of(sb.POLICY_PERTILE, sb.EXEC_PER_TILE)
+    forms["plain_per_tile_default_model"] = {"pairs_per_s": pairs / (ns0 * 1e-9), "ms": ns0 * 1e-6,
+                                             "launches": st0["launches"], "cell_pairs": st0["cell_pairs"]}
+    t0 = time.perf_counter()
+    sel = r.train_selector(tile=tile, samples=1024, epochs=400, seed=7)   # also calibrates the cost model
+    out["train_s"] = round(time.perf_counter() - t0, 2)
+    out["selector"] = {k: (round(v, 4) if isinstance(v, float) else v) for k, v in sel.items()}
+    out["selector"].update({k: round(v, 4) for k, v in r.last_training().items()})
+    ref_sum = s0
     for name, pol, ex, dense in (("plain_per_tile_cost_model", sb.POLICY_PERTILE, sb.EXEC_PER_TILE, 0.0),
                                  ("batched_cost_model", sb.POLICY_PERTILE, sb.EXEC_BATCHED, 0.0),
                                  ("batched_learned", sb.POLICY_LEARNED, sb.EXEC_BATCHED, 0.0),
@@ -409,8 +414,11 @@ def mixed_density_forms(sb, device, n=4096, universe=1 << 20, tile=64):
         forms[name] = {"pairs_per_s": pairs / (ns * 1e-9), "ms": ns * 1e-6, "launches": st["launches"],
                        "tile": t_tile, "dense_block_min_density": t_dens, "cell_pairs": st["cell_pairs"]}
     out["forms"] = forms
+    out["plain_per_tile_cost_model_is"] = "the cost model calibrated on this GPU's cell timings (training split)"
     out["learned_autotuned_over_plain"] = (forms["batched_learned_autotuned"]["pairs_per_s"] /
                                            forms["plain_per_tile_cost_model"]["pairs_per_s"])
+    out["calibrated_over_default_per_tile"] = (forms["plain_per_tile_cost_model"]["pairs_per_s"] /
+                                               forms["plain_per_tile_default_model"]["pairs_per_s"])
     out["learned_over_plain"] = forms["batched_learned"]["pairs_per_s"] / forms["plain_per_tile_cost_model"]["pairs_per_s"]
     out["learned_tensor_block_over_plain"] = (forms["batched_learned_tensor_block"]["pairs_per_s"] /
                                               forms["plain_per_tile_cost_model"]["pairs_per_s"])
@@ -920,8 +928,11 @@ def forms_on(sb, sets, universe, tile=64, samples=1024, with_plain=True):
     n = len(sets)
     pairs = n * (n - 1) // 2
     sel = r.train_selector(tile=tile, samples=samples, epochs=400, seed=7)
+    lt = r.last_training()
     res = {"rows": n, "pairs": pairs,
-           "regret_learned": round(sel["regret_mlp"], 4), "regret_cost_model": round(sel["regret_cost_model"], 4),
+           "regret_learned": round(sel["regret_mlp"], 4),
+           "regret_cost_model_calibrated": round(lt["regret_calibrated_model"], 4),
+           "regret_cost_model_default": round(lt["regret_default_model"], 4),
            "train_accuracy": round(sel["train_accuracy"], 3)}
     sums = set()
     dflt = DENSE_BLOCK_DEFAULT
@@ -1206,6 +1217,60 @@ def storm_t_forms(device, cpu_seconds=2.0, only=None):
     return out
 
 
+def north_star_summary(line):
+    """The figures the target names, compactly: the tensor-core kernel's
+    fraction of the measured 8-bit peak on the headline workload and on the
+    4096 x 65536 configuration; learned-batched vs plain per-tile vs the
+    reference CPU driver on the mixed-density corpus, with the selectors'
+    regret; each full-size STORM_t configuration's device rate, CPU rate and
+    identity check."""
+    def g(d, *path):
+        for k in path:
+            if not isinstance(d, dict) or k not in d:
+                return None
+            d = d[k]
+        return d
+
+    def r3(x):
+        return None if x is None else float(f"{x:.4g}")
+
+    ns = {"headline_frac": r3(g(line, "roofline", "frac")), "headline_e2e_pairs_per_s": r3(g(line, "e2e", "value"))}
+    at = line.get("autotune_config1")
+    if isinstance(at, dict) and "candidates_tops_int8" in at:
+        peak = g(line, "roofline", "peak")
+        best = max(at["candidates_tops_int8"].values()) if at["candidates_tops_int8"] else None
+        ns["config1_best_tops"] = r3(best)
+        ns["config1_frac"] = r3(best / peak) if best and peak else None
+        ns["config1_kept"] = at.get("kept")
+    md = line.get("mixed_density")
+    if isinstance(md, dict) and "forms" in md:
+        f = md["forms"]
+        ns["mixed_density"] = {
+            "learned_batched": r3(g(f, "batched_learned_tensor_block", "pairs_per_s")),
+            "learned_batched_autotuned": r3(g(f, "batched_learned_autotuned", "pairs_per_s")),
+            "plain_per_tile_calibrated": r3(g(f, "plain_per_tile_cost_model", "pairs_per_s")),
+            "plain_per_tile_default": r3(g(f, "plain_per_tile_default_model", "pairs_per_s")),
+            "cpu_reference": r3(g(md, "cpu_reference_per_tile", "pairs_per_s")),
+            "regret_mlp": g(md, "selector", "regret_mlp"),
+            "regret_calibrated": g(md, "selector", "regret_calibrated_model"),
+            "regret_default": g(md, "selector", "regret_default_model")}
+    full = line.get("storm_t_full")
+    if isinstance(full, dict):
+        for name, r in full.items():
+            if isinstance(r, dict) and "device" in r:
+                ns[name] = {"device_pairs_per_s": r3(g(r, "device", "pairs_per_s")),
+                            "ms": g(r, "device", "ms"),
+                            "cpu_1core": r3(g(r, "cpu_reference", "pairs_per_s")),
+                            "cpu_all": r3(g(r, "cpu_reference_all_threads", "pairs_per_s")),
+                            "exact": g(r, "checked", "identities_hold")}
+            elif isinstance(r, dict):
+                ns[name] = r
+    c5 = line.get("config5a_full")
+    if isinstance(c5, dict) and "pairs_per_s" in c5:
+        ns["config5a"] = {"pairs_per_s": r3(c5["pairs_per_s"]), "frac": r3(g(c5, "roofline", "frac"))}
+    return ns
+
+
 # ------------------------------------------------------------------ arms
 def run_reference_arm(args):
     rank, world, local = dist_env()
@@ -1474,6 +1539,7 @@ def run_b200_arm(args):
         except Exception as e:
             line["config5a_full"] = {"error": f"{type(e).__name__}: {e}"}
     if rank == 0:
+        line["north_star"] = north_star_summary(line)   # last, so that the tail of the line keeps it
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
