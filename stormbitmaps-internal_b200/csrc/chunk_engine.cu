@@ -850,6 +850,8 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
     log.launches = 0;
     log.last_ms = 0.f;
     last_dense_rows = last_dense_panels = last_postings_rows = 0;
+    last_panel_rows = last_panel_queries = 0;
+    for (int k = 0; k < 4; ++k) last_engine_ms[k] = last_engine_pred_ms[k] = last_engine_work[k] = 0.0;
     if (n_pairs_all == 0) return 0;
     d_flags.reserve(1);
     SB_CUDA(cudaMemsetAsync(d_flags.p, 0, sizeof(DeviceFlags), st));
