@@ -150,7 +150,7 @@ int64_t STORM_rows_cell(STORM_rows_t* r, int pairing, uint64_t row_a, uint64_t r
 
 /* ---- learned selector ---------------------------------------------------
  * Features per tile pair (row tiles of the density-sorted order) -> scores
- * per cell; argmax is the cell.  STORM_rows_train_selector times every
+ * per cell (the reference's ten and C x B); argmax is the cell.  STORM_rows_train_selector times every
  * applicable cell on sampled tiles of `r` on the GPU (the labels), trains the
  * MLP with the device forward/backward kernels, and installs it in `r`.
  * Returns 0; stats[0..5] = samples, epochs, final loss, train accuracy,
@@ -178,13 +178,18 @@ int STORM_rows_reset_selector(STORM_rows_t* r);
  * reference default model's prediction above its fixed term) + f x pairs,
  * one weighted least-squares fit (relative error).  The result replaces r's
  * cost model (the cost-model policies and the untrained learned policy use
- * it; counts never depend on it).  model_out (14 entries, may be NULL):
- * ns_per_unit[11] and the fixed and zone-map-word terms in SM cycles, then
- * the fit's relative RMS error.  No counterpart in the reference's C ABI. */
+ * it; counts never depend on it).  The complement cell C x B
+ * (STORM_PAIRING_CB, kernels/cell_comp.cpp), which the reference never
+ * selects, is timed too and becomes a candidate of the calibrated model
+ * (priced per complement position) when it was timed.  model_out (15
+ * entries, may be NULL): ns_per_unit[11], the fixed and zone-map-word terms
+ * and C x B's price per complement position, in SM cycles, then the fit's
+ * relative RMS error.  No counterpart in the reference's C ABI. */
 int STORM_rows_calibrate(STORM_rows_t* r, uint32_t tile, uint32_t samples, uint64_t seed, double* model_out);
-/* r's cost model: set = 0 copies it into model[13] (ns_per_unit[11], fixed,
- * zone-map word) and returns 1 when calibrated, 0 for the reference default;
- * set = 1 installs model[13], or the reference default when model is NULL. */
+/* r's cost model: set = 0 copies it into model[14] (ns_per_unit[11], fixed,
+ * zone-map word, C x B per complement position -- 0: never chosen) and
+ * returns 1 when calibrated, 0 for the reference default; set = 1 installs
+ * model[14], or the reference default when model is NULL. */
 int STORM_rows_cost_model(STORM_rows_t* r, double* model, int set);
 /* Parameters out/in (so a trained selector can be saved and loaded):
  * n_params floats.  Returns the parameter count when params is NULL. */

@@ -1,6 +1,7 @@
 // mlp.cuh -- the learned cell selector: a two-layer MLP over tile features.
 //
-//   x (16 tile features) -> h = relu(W1 x + b1) (32) -> logits = W2 h + b2 (10 cells)
+//   x (16 tile features) -> h = relu(W1 x + b1) (32) -> logits = W2 h + b2 (11 cell slots:
+//   the reference's ten cells and C x B)
 //
 // The features are the tile aggregates the cost model reads (storm_cost.cpp:
 // work_units inputs: cardinality, runs, non-zero words, universe words, the
@@ -23,7 +24,7 @@ constexpr int MLP_MAX_H = 64;
 constexpr int MLP_MAX_C = 16;
 
 struct MlpShape {
-    uint32_t F = 16, H = 32, C = 10;
+    uint32_t F = 16, H = 32, C = 11;   // C: cell slots (slot_cell)
     __host__ __device__ uint32_t n_params() const { return H * F + H + C * H + C; }
 };
 
@@ -130,11 +131,11 @@ __host__ __device__ inline int mlp_argmax_available(const float* p, const MlpSha
     const RowMetaD& s = a_dense ? b : a;
     int best = P_SS;
     float bs = -3.0e38f;
-    for (uint32_t c = 0; c < sh.C && c < (uint32_t)P_EMPTY; ++c) {
-        if (!cell_available((int)c, d, s)) continue;
+    for (uint32_t c = 0; c < sh.C && c < (uint32_t)N_SLOTS; ++c) {
+        if (!cell_available(slot_cell((int)c), d, s)) continue;
         if (lg[c] > bs) {
             bs = lg[c];
-            best = (int)c;
+            best = slot_cell((int)c);
         }
     }
     return best;

@@ -354,6 +354,7 @@ __device__ __forceinline__ uint32_t run_cell(const RowsView& v, int p, uint32_t 
         case P_RR: return cell_rr(v, d, s, lane);
         case P_RW: return cell_rw(v, s, d, lane);
         case P_WW: return cell_ww(v, d, s, lane);
+        case P_CB: return cell_cb(v, d, s, lane);   // the denser row's complement, the other's bitmap
         default: return 0;
     }
 }

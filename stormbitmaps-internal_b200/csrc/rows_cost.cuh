@@ -28,7 +28,19 @@ struct RowMetaD {
 struct CostModelD {
     double ns_per_unit[P_COUNT];
     double ns_fixed, ns_per_occ_word, ns_probe_hot, ns_probe_cold;
+    // C x B (|A & B| = |B| - |A' & B|, one probe per complement position):
+    // not among the reference's candidates, so 0 (never chosen) in its
+    // default model; a calibrated model prices it from its own timings.
+    double ns_per_unit_cb;
 };
+
+// Cells the selectors choose among, as slots: the reference's ten
+// (P_BB .. P_WW) and C x B.
+constexpr int N_SLOTS = P_EMPTY + 1;
+__host__ __device__ inline int slot_cell(int slot) { return slot < P_EMPTY ? slot : P_CB; }
+// The default model's price of one complement probe, the unit C x B's
+// calibrated constant scales (a probe per entry, as B x S's is).
+constexpr double CB_UNIT_REF = 0.30;
 
 __host__ __device__ inline CostModelD default_cost_model() {
     CostModelD m{};
@@ -47,6 +59,7 @@ __host__ __device__ inline CostModelD default_cost_model() {
     m.ns_per_occ_word = 0.30;
     m.ns_probe_hot = 0.0;
     m.ns_probe_cold = 0.0;
+    m.ns_per_unit_cb = 0.0;
     return m;
 }
 
@@ -109,8 +122,16 @@ __host__ __device__ inline double work_units(int p, const RowMetaD& a, const Row
     }
 }
 
+// Complement positions of the denser row (the probes of C x B).
+__host__ __device__ inline double cb_work(const RowMetaD& a, const RowMetaD& b) {
+    const RowMetaD& d = a.card >= b.card ? a : b;
+    const double u = (double)d.nw * 64.0;
+    return u > (double)d.card ? u - (double)d.card : 0.0;
+}
+
 __host__ __device__ inline double predict_cost(const CostModelD& m, int p, const RowMetaD& a, const RowMetaD& b) {
     if (p == P_EMPTY) return 0.0;
+    if (p == P_CB) return m.ns_fixed + m.ns_per_unit_cb * cb_work(a, b);
     const double mw = (double)(a.nw > b.nw ? a.nw : b.nw);
     if (p == P_BB && !(a.has_occ && b.has_occ)) return m.ns_fixed + m.ns_per_unit[P_BB] * mw;
     double c = m.ns_fixed + m.ns_per_unit[p] * work_units(p, a, b) * (p == P_RR ? RR_SCALE : 1.0);
@@ -137,6 +158,7 @@ __host__ __device__ inline bool cell_available(int p, const RowMetaD& d, const R
             const bool swap = (double)d.runs * BR_ORIENT_MARGIN <= (double)s.runs;
             return swap ? s.has_bm : d.has_bm;
         }
+        case P_CB: return d.has_comp && s.has_bm;
         default: return p >= 0 && p < P_EMPTY;
     }
 }
@@ -160,6 +182,13 @@ __host__ __device__ inline int select_pairing_d(const CostModelD& m, const RowMe
         if (c < bestc) {
             bestc = c;
             best = i;
+        }
+    }
+    if (m.ns_per_unit_cb > 0.0 && cell_available(P_CB, d, s)) {
+        const double c = predict_cost(m, P_CB, a, b);
+        if (c < bestc) {
+            bestc = c;
+            best = P_CB;
         }
     }
     if (predicted) *predicted = bestc;

@@ -53,12 +53,13 @@ __global__ void block_meta_kernel(RowsView v, const uint32_t* __restrict__ order
     m.last = 0;
     uint64_t card = 0, runs = 0, nnz = 0;
     uint32_t mx = 0;
-    m.has_rank = m.has_occ = m.has_bm = 1;
+    m.has_rank = m.has_occ = m.has_bm = m.has_comp = 1;
     for (uint32_t k = lo; k < hi; ++k) {
         const RowMetaD& r = v.meta[order[k]];
         m.has_rank &= r.has_rank;
         m.has_occ &= r.has_occ;
         m.has_bm &= r.has_bm;
+        m.has_comp &= r.has_comp;
         card += r.card;
         runs += r.runs;
         nnz += r.nnz;
@@ -950,7 +951,8 @@ namespace sb200 {
 __global__ void __launch_bounds__(TK_THREADS)
 time_cells_kernel(PairCtx c, const uint32_t* __restrict__ tiles, uint32_t n_samples, uint32_t max_pairs,
                   unsigned long long* __restrict__ cycles) {
-    const uint32_t sample = blockIdx.x / P_EMPTY, cell = blockIdx.x % P_EMPTY;
+    const uint32_t sample = blockIdx.x / N_SLOTS, slot = blockIdx.x % N_SLOTS;
+    const int cell = slot_cell((int)slot);
     if (sample >= n_samples) return;
     __shared__ int s_missing;
     __shared__ long long s_t0;
@@ -979,18 +981,18 @@ time_cells_kernel(PairCtx c, const uint32_t* __restrict__ tiles, uint32_t n_samp
         const RowMetaD& md = idn ? mi : mj;
         const RowMetaD& ms = idn ? mj : mi;
         if (span_disjoint(md, ms)) continue;
-        if (!cell_available((int)cell, md, ms)) {
+        if (!cell_available(cell, md, ms)) {
             s_missing = 1;
             continue;
         }
-        sink += run_cell(c.v, (int)cell, idn ? ri : rj, idn ? rj : ri, lane, true);
+        sink += run_cell(c.v, cell, idn ? ri : rj, idn ? rj : ri, lane, true);
     }
     sink = warp_sum_u32(sink);
     if (lane == 0) atomicAdd(&s_sink, sink);
     __syncthreads();
     if (threadIdx.x == 0) {
         const long long dt = clock64() - s_t0;
-        cycles[(uint64_t)sample * P_EMPTY + cell] =
+        cycles[(uint64_t)sample * N_SLOTS + slot] =
             s_missing ? ~0ull : (unsigned long long)dt + (s_sink == 0xFFFFFFFFu ? 1ull : 0ull);
     }
 }
@@ -1001,7 +1003,8 @@ time_cells_kernel(PairCtx c, const uint32_t* __restrict__ tiles, uint32_t n_samp
 __global__ void __launch_bounds__(TK_THREADS)
 cell_predict_kernel(PairCtx c, const uint32_t* __restrict__ tiles, uint32_t n_samples, uint32_t max_pairs,
                     double* __restrict__ pred, uint32_t* __restrict__ npairs) {
-    const uint32_t sample = blockIdx.x / P_EMPTY, cell = blockIdx.x % P_EMPTY;
+    const uint32_t sample = blockIdx.x / N_SLOTS, slot = blockIdx.x % N_SLOTS;
+    const int cell = slot_cell((int)slot);
     if (sample >= n_samples) return;
     __shared__ double s_pred;
     __shared__ unsigned int s_np;
@@ -1026,7 +1029,8 @@ cell_predict_kernel(PairCtx c, const uint32_t* __restrict__ tiles, uint32_t n_sa
             const RowMetaD& mi = c.v.meta[c.order[oi]];
             const RowMetaD& mj = c.v.meta[c.order[oj]];
             if (span_disjoint(mi, mj)) continue;
-            acc += predict_cost(m, (int)cell, mi, mj) - m.ns_fixed;
+            // C x B, absent from the default model, priced as a probe per complement position
+            acc += cell == P_CB ? CB_UNIT_REF * cb_work(mi, mj) : predict_cost(m, cell, mi, mj) - m.ns_fixed;
             ++cnt;
         }
         atomicAdd(&s_pred, acc);
@@ -1034,8 +1038,8 @@ cell_predict_kernel(PairCtx c, const uint32_t* __restrict__ tiles, uint32_t n_sa
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        pred[(uint64_t)sample * P_EMPTY + cell] = s_pred;
-        npairs[(uint64_t)sample * P_EMPTY + cell] = s_np;
+        pred[(uint64_t)sample * N_SLOTS + slot] = s_pred;
+        npairs[(uint64_t)sample * N_SLOTS + slot] = s_np;
     }
 }
 
@@ -1044,9 +1048,9 @@ cell_predict_kernel(PairCtx c, const uint32_t* __restrict__ tiles, uint32_t n_sa
 struct TileTimings {
     uint32_t T = 64, nb = 0;
     std::vector<uint32_t> pick;                 // sampled tile indices
-    std::vector<unsigned long long> cyc;        // [sample][cell] min of three, ~0 = cell unavailable
-    std::vector<double> pred;                   // [sample][cell] default model, above its fixed term
-    std::vector<uint32_t> npairs;               // [sample][cell]
+    std::vector<unsigned long long> cyc;        // [sample][slot] min of three, ~0 = cell unavailable
+    std::vector<double> pred;                   // [sample][slot] default model, above its fixed term
+    std::vector<uint32_t> npairs;               // [sample][slot]
     std::vector<RowMetaD> bmeta;
     std::vector<uint32_t> het;
     std::vector<uint64_t> bzone;                // [block][BZONE_WORDS]
@@ -1116,24 +1120,24 @@ static TileTimings time_tiles(STORM_rows_t* r, uint32_t T, uint32_t samples, uin
     DevBuf<unsigned long long> dcyc;
     DevBuf<double> dpred;
     dpick.reserve(ns);
-    dcyc.reserve((size_t)ns * P_EMPTY);
-    dpred.reserve((size_t)ns * P_EMPTY);
-    dnp.reserve((size_t)ns * P_EMPTY);
+    dcyc.reserve((size_t)ns * N_SLOTS);
+    dpred.reserve((size_t)ns * N_SLOTS);
+    dnp.reserve((size_t)ns * N_SLOTS);
     SB_CUDA(cudaMemcpyAsync(dpick.p, tt.pick.data(), ns * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-    tt.cyc.assign((size_t)ns * P_EMPTY, ~0ull);
-    std::vector<unsigned long long> tmp((size_t)ns * P_EMPTY);
+    tt.cyc.assign((size_t)ns * N_SLOTS, ~0ull);
+    std::vector<unsigned long long> tmp((size_t)ns * N_SLOTS);
     for (int rep = 0; rep < 3; ++rep) {   // min of three timings per (tile, cell)
-        time_cells_kernel<<<ns * P_EMPTY, TK_THREADS, 0, st>>>(c, dpick.p, ns, 256, dcyc.p);
+        time_cells_kernel<<<ns * N_SLOTS, TK_THREADS, 0, st>>>(c, dpick.p, ns, 256, dcyc.p);
         SB_CUDA(cudaGetLastError());
         SB_CUDA(cudaMemcpyAsync(tmp.data(), dcyc.p, tmp.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                                 st));
         SB_CUDA(cudaStreamSynchronize(st));
         for (size_t k = 0; k < tt.cyc.size(); ++k) tt.cyc[k] = std::min(tt.cyc[k], tmp[k]);
     }
-    cell_predict_kernel<<<ns * P_EMPTY, TK_THREADS, 0, st>>>(c, dpick.p, ns, 256, dpred.p, dnp.p);
+    cell_predict_kernel<<<ns * N_SLOTS, TK_THREADS, 0, st>>>(c, dpick.p, ns, 256, dpred.p, dnp.p);
     SB_CUDA(cudaGetLastError());
-    tt.pred.resize((size_t)ns * P_EMPTY);
-    tt.npairs.resize((size_t)ns * P_EMPTY);
+    tt.pred.resize((size_t)ns * N_SLOTS);
+    tt.npairs.resize((size_t)ns * N_SLOTS);
     SB_CUDA(cudaMemcpyAsync(tt.pred.data(), dpred.p, tt.pred.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
     SB_CUDA(cudaMemcpyAsync(tt.npairs.data(), dnp.p, tt.npairs.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost,
                             st));
@@ -1151,13 +1155,13 @@ static TileTimings time_tiles(STORM_rows_t* r, uint32_t T, uint32_t samples, uin
 // Returns the fitted model in SM cycles (the selector compares predictions,
 // so the unit is free) and the fit's relative RMS error.
 static CostModelD fit_cost_model(const TileTimings& tt, const std::vector<uint32_t>& use, double* rms_out) {
-    constexpr int K = P_EMPTY + 1;               // a_0 .. a_9, f
+    constexpr int K = N_SLOTS + 1;               // a per cell slot, f
     double A[K][K] = {}, B[K] = {};
-    std::vector<int> seen(P_EMPTY, 0);
+    std::vector<int> seen(N_SLOTS, 0);
     for (uint32_t k : use)
-        for (int cl = 0; cl < P_EMPTY; ++cl) {
-            const size_t e = (size_t)k * P_EMPTY + cl;
-            if (tt.cyc[e] == ~0ull || tt.npairs[e] == 0) continue;
+        for (int cl = 0; cl < N_SLOTS; ++cl) {
+            const size_t e = (size_t)k * N_SLOTS + cl;
+            if (tt.cyc[e] == ~0ull || tt.npairs[e] == 0 || tt.pred[e] <= 0.0) continue;
             const double y = (double)tt.cyc[e], w = 1.0 / (y * y);
             const double xa = tt.pred[e], xf = (double)tt.npairs[e];
             A[cl][cl] += w * xa * xa;
@@ -1168,14 +1172,14 @@ static CostModelD fit_cost_model(const TileTimings& tt, const std::vector<uint32
             B[K - 1] += w * xf * y;
             seen[cl] = 1;
         }
-    for (int cl = 0; cl < P_EMPTY; ++cl)
+    for (int cl = 0; cl < N_SLOTS; ++cl)
         if (!seen[cl]) A[cl][cl] = 1.0;          // unfitted cell: a = 0 for now
     double M[K][K + 1];
     for (int i = 0; i < K; ++i) {
         for (int j = 0; j < K; ++j) M[i][j] = A[i][j];
         M[i][K] = B[i];
     }
-    bool ok = true;
+    bool ok = A[K - 1][K - 1] > 0.0;
     for (int col = 0; col < K && ok; ++col) {    // Gaussian elimination, partial pivoting
         int piv = col;
         for (int i = col + 1; i < K; ++i)
@@ -1195,10 +1199,10 @@ static CostModelD fit_cost_model(const TileTimings& tt, const std::vector<uint32
     for (int i = 0; i < K; ++i) a[i] = ok ? M[i][K] / M[i][i] : 0.0;
     if (!ok || a[K - 1] < 0.0) {                 // no fixed term: per-cell ratios
         a[K - 1] = 0.0;
-        for (int cl = 0; cl < P_EMPTY; ++cl) {
+        for (int cl = 0; cl < N_SLOTS; ++cl) {
             double sy = 0, sx = 0;
             for (uint32_t k : use) {
-                const size_t e = (size_t)k * P_EMPTY + cl;
+                const size_t e = (size_t)k * N_SLOTS + cl;
                 if (tt.cyc[e] == ~0ull || tt.npairs[e] == 0) continue;
                 sy += (double)tt.cyc[e];
                 sx += tt.pred[e];
@@ -1206,7 +1210,8 @@ static CostModelD fit_cost_model(const TileTimings& tt, const std::vector<uint32
             a[cl] = sx > 0 ? sy / sx : 0.0;
         }
     }
-    // cells with no sample (or a non-positive fit) take the mean scale of the others
+    // reference cells with no sample (or a non-positive fit) take the mean
+    // scale of the others; C x B stays unpriced (never chosen) without one
     double mean = 0;
     int nf = 0;
     for (int cl = 0; cl < P_EMPTY; ++cl)
@@ -1220,15 +1225,16 @@ static CostModelD fit_cost_model(const TileTimings& tt, const std::vector<uint32
     const CostModelD d = default_cost_model();
     CostModelD m = d;
     for (int cl = 0; cl < P_EMPTY; ++cl) m.ns_per_unit[cl] = a[cl] * d.ns_per_unit[cl];
+    m.ns_per_unit_cb = (seen[P_EMPTY] && a[P_EMPTY] > 0) ? a[P_EMPTY] * CB_UNIT_REF : 0.0;
     m.ns_fixed = a[K - 1];
     m.ns_per_occ_word = a[P_BB] * d.ns_per_occ_word;
     m.ns_probe_hot = m.ns_probe_cold = 0.0;
     double se = 0;
     size_t cnt = 0;
     for (uint32_t k : use)
-        for (int cl = 0; cl < P_EMPTY; ++cl) {
-            const size_t e = (size_t)k * P_EMPTY + cl;
-            if (tt.cyc[e] == ~0ull || tt.npairs[e] == 0) continue;
+        for (int cl = 0; cl < N_SLOTS; ++cl) {
+            const size_t e = (size_t)k * N_SLOTS + cl;
+            if (tt.cyc[e] == ~0ull || tt.npairs[e] == 0 || tt.pred[e] <= 0.0) continue;
             const double y = (double)tt.cyc[e];
             const double p = a[cl] * tt.pred[e] + a[K - 1] * tt.npairs[e];
             se += (p - y) * (p - y) / (y * y);
@@ -1263,7 +1269,8 @@ int STORM_rows_calibrate(STORM_rows_t* r, uint32_t tile, uint32_t samples, uint6
             for (int cl = 0; cl < P_COUNT; ++cl) model_out[cl] = r->model.ns_per_unit[cl];
             model_out[P_COUNT] = r->model.ns_fixed;
             model_out[P_COUNT + 1] = r->model.ns_per_occ_word;
-            model_out[P_COUNT + 2] = rms;
+            model_out[P_COUNT + 2] = r->model.ns_per_unit_cb;
+            model_out[P_COUNT + 3] = rms;
         }
         return 0;
     });
@@ -1279,6 +1286,7 @@ int STORM_rows_cost_model(STORM_rows_t* r, double* model, int set) {
             for (int cl = 0; cl < P_COUNT; ++cl) r->model.ns_per_unit[cl] = model[cl];
             r->model.ns_fixed = model[P_COUNT];
             r->model.ns_per_occ_word = model[P_COUNT + 1];
+            r->model.ns_per_unit_cb = model[P_COUNT + 2];
             r->model.ns_probe_hot = r->model.ns_probe_cold = 0.0;
             r->calibrated = true;
         }
@@ -1289,6 +1297,7 @@ int STORM_rows_cost_model(STORM_rows_t* r, double* model, int set) {
     for (int cl = 0; cl < P_COUNT; ++cl) model[cl] = r->model.ns_per_unit[cl];
     model[P_COUNT] = r->model.ns_fixed;
     model[P_COUNT + 1] = r->model.ns_per_occ_word;
+    model[P_COUNT + 2] = r->model.ns_per_unit_cb;
     return r->calibrated ? 1 : 0;
 }
 
@@ -1306,14 +1315,14 @@ int STORM_rows_train_selector(STORM_rows_t* r, uint32_t tile, uint32_t samples, 
         std::vector<int32_t> Y;
         std::vector<uint32_t> idx;
         for (uint32_t k = 0; k < ns; ++k) {
-            uint32_t best = P_EMPTY;
+            uint32_t best = N_SLOTS;
             unsigned long long bc = ~0ull;
-            for (uint32_t cl = 0; cl < P_EMPTY; ++cl)
-                if (tt.cyc[(size_t)k * P_EMPTY + cl] < bc) {
-                    bc = tt.cyc[(size_t)k * P_EMPTY + cl];
+            for (uint32_t cl = 0; cl < (uint32_t)N_SLOTS; ++cl)
+                if (tt.cyc[(size_t)k * N_SLOTS + cl] < bc) {
+                    bc = tt.cyc[(size_t)k * N_SLOTS + cl];
                     best = cl;
                 }
-            if (best == P_EMPTY) continue;
+            if (best == (uint32_t)N_SLOTS) continue;
             uint32_t ti, tj;
             tt.tile_of(k, ti, tj);
             float x[MLP_MAX_F];
@@ -1366,7 +1375,7 @@ int STORM_rows_train_selector(STORM_rows_t* r, uint32_t tile, uint32_t samples, 
             const uint32_t k = te_idx[q];
             uint32_t ti, tj;
             tt.tile_of(k, ti, tj);
-            const unsigned long long* cy = tt.cyc.data() + (size_t)k * P_EMPTY;
+            const unsigned long long* cy = tt.cyc.data() + (size_t)k * N_SLOTS;
             const int y = Yte[q];
             const RowMetaD& a = tt.bmeta[ti];
             const RowMetaD& b = tt.bmeta[tj];
@@ -1376,7 +1385,10 @@ int STORM_rows_train_selector(STORM_rows_t* r, uint32_t tile, uint32_t samples, 
                 if (cl == P_EMPTY) cl = (a.has_bm && b.has_bm) ? P_BB : P_SS;
                 return cl;
             };
-            auto cost = [&](int cl) { return cy[cl] == ~0ull ? (double)cy[y] * 4.0 : (double)cy[cl]; };
+            auto cost = [&](int cl) {   // a cell's timed slot (C x B is the last)
+                const int sl = cl == P_CB ? P_EMPTY : cl;
+                return cy[sl] == ~0ull ? (double)cy[y] * 4.0 : (double)cy[sl];
+            };
             best_sum += (double)cy[y];
             mlp_sum += cost(m_cell);
             cal_sum += cost(model_cell(r->model));

@@ -110,7 +110,7 @@ def test_gpu_calibration_of_the_cost_model(sb):
     for s in sets:
         r.add(s)
     model, rms = r.calibrate(tile=32, samples=0, seed=5)
-    assert len(model) == 13 and all(x >= 0 for x in model)
+    assert len(model) == 14 and all(x >= 0 for x in model)
     assert 0.0 <= rms < 10.0
     got, cal = r.cost_model()
     assert cal and np.allclose(got, model)
@@ -123,4 +123,31 @@ def test_gpu_calibration_of_the_cost_model(sb):
     got, cal = r.cost_model()
     assert not cal
     mat, st = r.allpairs_matrix(sb.POLICY_PERTILE, 32)
+    np.testing.assert_array_equal(mat, want)
+
+
+def test_complement_cell_as_a_candidate(sb):
+    """C x B (|A & B| = |B| - |A' & B|, kernels/cell_comp.cpp) is a candidate
+    of a calibrated cost model: with a model that prices it cheaply, pairs of
+    rows denser than one half with rows that have bitmaps run on it, and the
+    counts stay the oracle's; the reference's default model never picks it."""
+    u = 1 << 16
+    sets = gen.bernoulli_sets(60, u, 0.9, 71) + gen.bernoulli_sets(60, u, 0.05, 72)
+    r = sb.StormRows(u)
+    for s in sets:
+        r.add(s)
+    vals, offs = gen.to_csr(sets)
+    want, ws = ol.sets_matrix(vals, offs)
+    mat, st = r.allpairs_matrix(sb.POLICY_PERPAIR, 32)
+    np.testing.assert_array_equal(mat, want)
+    assert st["cell_pairs"].get("CB", 0) == 0
+    model, _ = r.cost_model()
+    model[13] = 1e-6                     # C x B nearly free
+    r.cost_model(set_to=model)
+    for pol in (sb.POLICY_PERPAIR, sb.POLICY_PERTILE):
+        mat, st = r.allpairs_matrix(pol, 32)
+        np.testing.assert_array_equal(mat, want)
+        assert st["cell_pairs"].get("CB", 0) > 0, (pol, st["cell_pairs"])
+    model, rms = r.calibrate(tile=32, samples=0, seed=9)
+    mat, st = r.allpairs_matrix(sb.POLICY_PERPAIR, 32)
     np.testing.assert_array_equal(mat, want)
