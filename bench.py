@@ -336,19 +336,14 @@ def reference_sample(host_rows: np.ndarray, target_s: float, threads: int):
 # ------------------------------------------------- mixed-density forms
 def zipf_sets_gpu(n, universe, s, lo, hi, seed, device):
     """Rows with cardinality P(k) ~ k^-s on [lo, hi], elements uniform without
-    replacement, sorted u32 (generated on the GPU, returned as numpy)."""
-    import torch
-    g = np.random.Generator(np.random.PCG64(seed))
-    ks = np.arange(lo, hi + 1, dtype=np.float64)
-    pk = ks ** (-s)
-    pk /= pk.sum()
-    cards = g.choice(ks.astype(np.int64), size=n, p=pk)
-    tg = torch.Generator(device=device)
-    tg.manual_seed(seed)
+    replacement, sorted u32 (generated on the GPU in batches, returned as
+    numpy arrays)."""
+    cards = zipf_cards(n, s, lo, hi, seed)
     out = []
-    for k in cards:
-        perm = torch.randperm(universe, generator=tg, device=device)[: int(k)]
-        out.append(torch.sort(perm).values.to(torch.int64).cpu().numpy().astype(np.uint32))
+    for b, (r0, r1) in enumerate(batch_plan(cards, 1 << 27)):
+        vals, offs = uniform_rows_batch(cards[r0:r1], universe, seed * 1000003 + b, device)
+        host = vals.cpu().numpy().view(np.uint32)
+        out.extend(host[int(offs[k]):int(offs[k + 1])].copy() for k in range(r1 - r0))
     return out
 
 
@@ -1015,8 +1010,9 @@ def autotune_config1(sb, device):
 
 def config45_forms(device):
     """Config-4-shaped run-clustered rows and the config-5b density sweep
-    (reduced N), each with the learned selector's held-out regret against
-    the measured-best cell, beside the cost model's."""
+    (N = 20000 up to density 1e-3, fewer rows above), each with the learned
+    selector's held-out regret against the measured-best cell, beside the
+    calibrated and the reference default cost model's."""
     import importlib
     sb = importlib.import_module("stormbitmaps-internal_b200")
     out = {}
@@ -1025,8 +1021,11 @@ def config45_forms(device):
     out["runs_2^26"] = forms_on(sb, sets, 1 << 26)
     out["runs_2^26"]["workload"] = "2048 rows over 2^26, Poisson(200) runs of Geometric(mean 256) length"
     sweep = {}
-    for d, n in ((1e-6, 4096), (1e-5, 4096), (1e-4, 2048), (1e-3, 1024), (1e-2, 512), (0.17, 256)):
-        sets = bernoulli_sets_gpu(n, 1 << 24, d, int(1e7 * d) + 5, device)
+    # N = 20000 (config 5b's row count) where the kernel layer's host packing
+    # of every representation stays within seconds; fewer rows beyond
+    for d, n in ((1e-6, 20000), (1e-5, 20000), (1e-4, 20000), (1e-3, 20000), (1e-2, 1024), (0.17, 256)):
+        sets = (sparse_bernoulli_sets_gpu(n, 1 << 24, d, int(1e7 * d) + 5, device) if d <= 1e-3 else
+                bernoulli_sets_gpu(n, 1 << 24, d, int(1e7 * d) + 5, device))
         sweep[f"{d:g}"] = forms_on(sb, sets, 1 << 24, samples=512, with_plain=False)
     out["density_sweep_2^24"] = sweep
     out["seconds"] = round(time.perf_counter() - t0, 1)
@@ -1516,6 +1515,7 @@ def run_b200_arm(args):
     if rank == 0 and world == 1 and args.forms:
         try:
             line["mixed_density"] = mixed_density_forms(sb, device)
+            line["mixed_density_2^24"] = mixed_density_forms(sb, device, n=4096, universe=1 << 24)
         except Exception as e:   # reported, never silently dropped
             line["mixed_density"] = {"error": f"{type(e).__name__}: {e}"}
         try:
