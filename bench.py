@@ -908,6 +908,49 @@ def storm_t_full(device, names=tuple(FULL_CORPORA), cpu_seconds=2.0):
     return out
 
 
+ENGINE_CASES = ("default", "panel", "postings", "tensor")
+
+
+def engine_case(engine, device, n=4096, universe=1 << 24, calls=3):
+    """One STORM_t engine on its own, for profiling and for its roofline: a
+    config-3-shaped corpus (n rows over `universe`, Zipf(1.1) cards on [16,
+    universe / 4]) with every plain row given to `engine` (panel: all in the
+    transposed panel; postings: the list rows by postings, rows with bitmap
+    chunks on the chunk kernel; tensor: all on the tensor cores) or the
+    default plan; per call the device time and each engine's measured and
+    predicted time and algorithmic work."""
+    import torch
+    import importlib
+    sb = importlib.import_module("stormbitmaps-internal_b200")
+    sets = zipf_sets_gpu(n, universe, 1.1, 16, universe // 4, 0xC0F3, device)
+    st = sb.Storm()
+    vals = np.ascontiguousarray(np.concatenate(sets), dtype=np.uint32)
+    offs = np.zeros(n + 1, np.uint64)
+    offs[1:] = np.cumsum([len(v) for v in sets])
+    st.add_rows(vals, offs)
+    if engine == "panel":
+        st.set_panel(2)
+    elif engine == "postings":
+        st.set_dense_block(0.0)
+        st.set_sparse_postings(1)
+        st.set_panel(0)
+    elif engine == "tensor":
+        st.set_dense_block(1e-12)
+        st.set_sparse_postings(0)
+        st.set_panel(0)
+    tri = n * (n + 1) // 2
+    d_tri = torch.empty(tri, dtype=torch.int32, device=device)
+    res = {"engine": engine, "workload": f"{n} rows over 2^{universe.bit_length() - 1}, Zipf(1.1) on [16, "
+                                         f"2^{(universe // 4).bit_length() - 1}]", "calls": []}
+    sums = set()
+    for _ in range(calls):
+        sums.add(st.matrix_device(d_tri.data_ptr(), tri))
+        res["calls"].append({"ms": round(st.last_kernel_ms(), 3), "engines": engine_roofline(st.last_engine_ms(), device)})
+    res["same_sum"] = len(sums) == 1
+    st.close()
+    return res
+
+
 # The library's default tensor-core dense-block threshold (rows whose sparse
 # form is at least 2^-14 of the universe).
 DENSE_BLOCK_DEFAULT = 1.0 / 16384
@@ -1569,6 +1612,8 @@ def main():
                     help="run only this STORM_t corpus of the forms (one JSON line) and exit")
     ap.add_argument("--storm-t-full", default=None, choices=tuple(FULL_CORPORA),
                     help="run only this full-size STORM_t configuration (one JSON line) and exit")
+    ap.add_argument("--engine-case", default=None, choices=ENGINE_CASES,
+                    help="run one STORM_t engine on a config-3-shaped corpus (one JSON line) and exit")
     ap.add_argument("--mixed-density-only", action="store_true",
                     help="run only the kernel layer's mixed-density forms (one JSON line) and exit")
     ap.add_argument("--mixed-density-batched", action="store_true",
@@ -1593,6 +1638,10 @@ def main():
         import torch
         sb = importlib.import_module("stormbitmaps-internal_b200")
         print(json.dumps({"mixed_density": mixed_density_forms(sb, torch.device("cuda", 0))}), flush=True)
+        return 0
+    if args.engine_case:
+        import torch
+        print(json.dumps({"engine_case": engine_case(args.engine_case, torch.device("cuda", 0))}), flush=True)
         return 0
     if args.storm_t_full:
         import torch
