@@ -640,6 +640,13 @@ class FullCorpus:
         vals, offs = uniform_rows_batch(self.cards[r0:r1], self.universe, self.seed * 1000003 + b, self.device)
         return r0, r1, vals, offs
 
+    def batch_of(self, row):
+        """Index of the batch holding `row`."""
+        for b, (r0, r1) in enumerate(self.plan):
+            if r0 <= row < r1:
+                return b
+        raise IndexError(row)
+
 
 def full_corpus(name, device):
     """The full-size configurations run through STORM_t."""

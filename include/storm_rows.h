@@ -164,7 +164,8 @@ int STORM_rows_train_selector(STORM_rows_t* r, uint32_t tile, uint32_t samples, 
  * calibrated model.  STORM_rows_last_training reports the last training:
  * out8 = regret of the MLP, of the calibrated model and of the reference's
  * default model on the held-out tiles, held-out and training tile counts,
- * the calibration's relative RMS error, its fixed term, sampled tiles. */
+ * the calibration's relative RMS error, its mean fixed cost per pair over
+ * the reference's ten cells, sampled tiles. */
 int STORM_rows_last_training(const STORM_rows_t* r, double* out8);
 /* Reset to the untrained (cost-model fallback) selector. */
 int STORM_rows_reset_selector(STORM_rows_t* r);
@@ -174,22 +175,27 @@ int STORM_rows_reset_selector(STORM_rows_t* r);
  * on the host CPU): every cell is timed on this GPU (SM clock) on sampled
  * tiles of r's own rows -- tile rows of the density order, `samples` tiles
  * (0: all), seeded -- and the model keeps the reference's work formulas with
- * constants fitted to those timings: cycles(tile, cell) ~ a_cell x (the
+ * constants fitted to those timings: per cell, cycles(tile) ~ a x (the
  * reference default model's prediction above its fixed term) + f x pairs,
- * one weighted least-squares fit (relative error).  The result replaces r's
- * cost model (the cost-model policies and the untrained learned policy use
- * it; counts never depend on it).  The complement cell C x B
+ * a weighted least-squares fit (relative error) giving the cell's
+ * ns_per_unit and its own fixed cost per pair.  The result replaces r's cost
+ * model (the cost-model policies and the untrained learned policy use it;
+ * counts never depend on it).  The complement cell C x B
  * (STORM_PAIRING_CB, kernels/cell_comp.cpp), which the reference never
  * selects, is timed too and becomes a candidate of the calibrated model
- * (priced per complement position) when it was timed.  model_out (15
- * entries, may be NULL): ns_per_unit[11], the fixed and zone-map-word terms
- * and C x B's price per complement position, in SM cycles, then the fit's
- * relative RMS error.  No counterpart in the reference's C ABI. */
+ * (priced per complement position) when it was timed.  model_out (27
+ * entries, may be NULL): the model as STORM_rows_cost_model lays it out,
+ * then the fit's relative RMS error.  No counterpart in the reference's C
+ * ABI. */
 int STORM_rows_calibrate(STORM_rows_t* r, uint32_t tile, uint32_t samples, uint64_t seed, double* model_out);
-/* r's cost model: set = 0 copies it into model[14] (ns_per_unit[11], fixed,
- * zone-map word, C x B per complement position -- 0: never chosen) and
- * returns 1 when calibrated, 0 for the reference default; set = 1 installs
- * model[14], or the reference default when model is NULL. */
+/* r's cost model: set = 0 copies it into model[26] -- ns_per_unit[11]
+ * (by pairing, STORM_PAIRING_EMPTY's unused), the fixed and zone-map-word
+ * terms, C x B's price per complement position (0: never chosen), then the
+ * fixed cost per pair of each pairing 0 .. STORM_PAIRING_CB (12 entries, 0
+ * in the reference's model) -- and returns 1 when calibrated, 0 for the
+ * reference default; set = 1 installs model[26], or the reference default
+ * when model is NULL.  Units are those of the model (SM cycles once
+ * calibrated). */
 int STORM_rows_cost_model(STORM_rows_t* r, double* model, int set);
 /* Parameters out/in (so a trained selector can be saved and loaded):
  * n_params floats.  Returns the parameter count when params is NULL. */

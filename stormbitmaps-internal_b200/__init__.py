@@ -697,21 +697,22 @@ class StormRows:
     def calibrate(self, tile=64, samples=0, seed=1):
         """GPU calibration of the cost model on these rows; returns the model
         (ns_per_unit[11], fixed, zone-map word, C x B per complement position,
-        in SM cycles) and the fit's relative RMS error."""
-        out = (C.c_double * 15)()
+        fixed cost per pair of each pairing [12], in SM cycles) and the fit's
+        relative RMS error."""
+        out = (C.c_double * 27)()
         _check(_lib.STORM_rows_calibrate(self.h, tile, samples, seed, out), "STORM_rows_calibrate")
-        return list(out)[:14], float(out[14])
+        return list(out)[:26], float(out[26])
 
     def cost_model(self, set_to=None, reset=False):
-        """Read the cost model ((model[14], calibrated)) or install one / the default."""
+        """Read the cost model ((model[26], calibrated)) or install one / the default."""
         if reset:
             _check(_lib.STORM_rows_cost_model(self.h, None, 1), "STORM_rows_cost_model")
             return None
         if set_to is not None:
-            m = (C.c_double * 14)(*[float(x) for x in set_to])
+            m = (C.c_double * 26)(*[float(x) for x in set_to])
             _check(_lib.STORM_rows_cost_model(self.h, m, 1), "STORM_rows_cost_model")
             return None
-        m = (C.c_double * 14)()
+        m = (C.c_double * 26)()
         rc = _check(_lib.STORM_rows_cost_model(self.h, m, 0), "STORM_rows_cost_model")
         return list(m), bool(rc)
 

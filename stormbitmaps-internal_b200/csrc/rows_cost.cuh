@@ -32,6 +32,10 @@ struct CostModelD {
     // not among the reference's candidates, so 0 (never chosen) in its
     // default model; a calibrated model prices it from its own timings.
     double ns_per_unit_cb;
+    // Per-cell fixed cost per pair on top of ns_fixed, indexed by pairing
+    // (P_CB included): 0 in the reference's model, fitted by the GPU
+    // calibration, where each warp-cooperative cell has its own overhead.
+    double ns_fixed_cell[P_CB + 1];
 };
 
 // Cells the selectors choose among, as slots: the reference's ten
@@ -60,6 +64,7 @@ __host__ __device__ inline CostModelD default_cost_model() {
     m.ns_probe_hot = 0.0;
     m.ns_probe_cold = 0.0;
     m.ns_per_unit_cb = 0.0;
+    for (int p = 0; p <= P_CB; ++p) m.ns_fixed_cell[p] = 0.0;
     return m;
 }
 
@@ -131,10 +136,10 @@ __host__ __device__ inline double cb_work(const RowMetaD& a, const RowMetaD& b) 
 
 __host__ __device__ inline double predict_cost(const CostModelD& m, int p, const RowMetaD& a, const RowMetaD& b) {
     if (p == P_EMPTY) return 0.0;
-    if (p == P_CB) return m.ns_fixed + m.ns_per_unit_cb * cb_work(a, b);
+    if (p == P_CB) return m.ns_fixed + m.ns_fixed_cell[P_CB] + m.ns_per_unit_cb * cb_work(a, b);
     const double mw = (double)(a.nw > b.nw ? a.nw : b.nw);
-    if (p == P_BB && !(a.has_occ && b.has_occ)) return m.ns_fixed + m.ns_per_unit[P_BB] * mw;
-    double c = m.ns_fixed + m.ns_per_unit[p] * work_units(p, a, b) * (p == P_RR ? RR_SCALE : 1.0);
+    if (p == P_BB && !(a.has_occ && b.has_occ)) return m.ns_fixed + m.ns_fixed_cell[P_BB] + m.ns_per_unit[P_BB] * mw;
+    double c = m.ns_fixed + m.ns_fixed_cell[p] + m.ns_per_unit[p] * work_units(p, a, b) * (p == P_RR ? RR_SCALE : 1.0);
     if (p == P_BS && m.ns_probe_cold > m.ns_probe_hot) {
         const double touches = (a.card <= b.card) ? (double)a.nnz : (double)b.nnz;
         c += (m.ns_probe_cold - m.ns_probe_hot) * PROBE_SCALE * touches;

@@ -1149,84 +1149,69 @@ static TileTimings time_tiles(STORM_rows_t* r, uint32_t T, uint32_t samples, uin
 // storm_cost.cpp:556-769, 779-895) fits, per cell, time / work on pairs it
 // times, plus a per-pair fixed term; here the timings are this GPU's, of the
 // container's own sampled tiles (time_cells_kernel), and the model keeps the
-// reference's work formulas: cycles(tile, cell) ~ a_cell x (the default
-// model's prediction above its fixed term) + f x pairs, solved as one
-// weighted least-squares problem (relative error) over the samples `use`.
-// Returns the fitted model in SM cycles (the selector compares predictions,
-// so the unit is free) and the fit's relative RMS error.
+// reference's work formulas: per cell slot, cycles(tile) ~ a x (the default
+// model's prediction above its fixed term) + f x pairs, a weighted
+// least-squares fit (relative error) of both, because each warp-cooperative
+// cell has its own per-pair overhead on the GPU.  Returns the fitted model
+// in SM cycles (the selector compares predictions, so the unit is free) and
+// the fit's relative RMS error.
 static CostModelD fit_cost_model(const TileTimings& tt, const std::vector<uint32_t>& use, double* rms_out) {
-    constexpr int K = N_SLOTS + 1;               // a per cell slot, f
-    double A[K][K] = {}, B[K] = {};
-    std::vector<int> seen(N_SLOTS, 0);
-    for (uint32_t k : use)
-        for (int cl = 0; cl < N_SLOTS; ++cl) {
+    double a[N_SLOTS], f[N_SLOTS];
+    bool fitted[N_SLOTS];
+    for (int cl = 0; cl < N_SLOTS; ++cl) {
+        double sxx = 0, sxp = 0, spp = 0, sxy = 0, spy = 0, sy = 0, sx = 0;
+        int cnt = 0;
+        for (uint32_t k : use) {
             const size_t e = (size_t)k * N_SLOTS + cl;
             if (tt.cyc[e] == ~0ull || tt.npairs[e] == 0 || tt.pred[e] <= 0.0) continue;
             const double y = (double)tt.cyc[e], w = 1.0 / (y * y);
-            const double xa = tt.pred[e], xf = (double)tt.npairs[e];
-            A[cl][cl] += w * xa * xa;
-            A[cl][K - 1] += w * xa * xf;
-            A[K - 1][cl] += w * xa * xf;
-            A[K - 1][K - 1] += w * xf * xf;
-            B[cl] += w * xa * y;
-            B[K - 1] += w * xf * y;
-            seen[cl] = 1;
+            const double x = tt.pred[e], q = (double)tt.npairs[e];
+            sxx += w * x * x;
+            sxp += w * x * q;
+            spp += w * q * q;
+            sxy += w * x * y;
+            spy += w * q * y;
+            sy += y;
+            sx += x;
+            ++cnt;
         }
-    for (int cl = 0; cl < N_SLOTS; ++cl)
-        if (!seen[cl]) A[cl][cl] = 1.0;          // unfitted cell: a = 0 for now
-    double M[K][K + 1];
-    for (int i = 0; i < K; ++i) {
-        for (int j = 0; j < K; ++j) M[i][j] = A[i][j];
-        M[i][K] = B[i];
-    }
-    bool ok = A[K - 1][K - 1] > 0.0;
-    for (int col = 0; col < K && ok; ++col) {    // Gaussian elimination, partial pivoting
-        int piv = col;
-        for (int i = col + 1; i < K; ++i)
-            if (std::fabs(M[i][col]) > std::fabs(M[piv][col])) piv = i;
-        if (std::fabs(M[piv][col]) < 1e-300) {
-            ok = false;
-            break;
+        fitted[cl] = cnt > 0;
+        a[cl] = f[cl] = 0.0;
+        if (!cnt) continue;
+        const double det = sxx * spp - sxp * sxp;
+        if (cnt >= 3 && det > 1e-12 * sxx * spp) {
+            a[cl] = (sxy * spp - spy * sxp) / det;
+            f[cl] = (sxx * spy - sxp * sxy) / det;
         }
-        for (int j = 0; j <= K; ++j) std::swap(M[col][j], M[piv][j]);
-        for (int i = 0; i < K; ++i) {
-            if (i == col) continue;
-            const double f = M[i][col] / M[col][col];
-            for (int j = col; j <= K; ++j) M[i][j] -= f * M[col][j];
-        }
-    }
-    double a[K];
-    for (int i = 0; i < K; ++i) a[i] = ok ? M[i][K] / M[i][i] : 0.0;
-    if (!ok || a[K - 1] < 0.0) {                 // no fixed term: per-cell ratios
-        a[K - 1] = 0.0;
-        for (int cl = 0; cl < N_SLOTS; ++cl) {
-            double sy = 0, sx = 0;
-            for (uint32_t k : use) {
-                const size_t e = (size_t)k * N_SLOTS + cl;
-                if (tt.cyc[e] == ~0ull || tt.npairs[e] == 0) continue;
-                sy += (double)tt.cyc[e];
-                sx += tt.pred[e];
-            }
+        if (!(a[cl] > 0.0) || f[cl] < 0.0) {     // degenerate or unphysical: time / work
             a[cl] = sx > 0 ? sy / sx : 0.0;
+            f[cl] = 0.0;
         }
     }
-    // reference cells with no sample (or a non-positive fit) take the mean
-    // scale of the others; C x B stays unpriced (never chosen) without one
+    // reference cells with no sample take the mean scale of the others;
+    // C x B stays unpriced (never chosen) without one
     double mean = 0;
     int nf = 0;
     for (int cl = 0; cl < P_EMPTY; ++cl)
-        if (seen[cl] && a[cl] > 0) {
+        if (fitted[cl] && a[cl] > 0) {
             mean += a[cl];
             ++nf;
         }
     mean = nf ? mean / nf : 1.0;
-    for (int cl = 0; cl < P_EMPTY; ++cl)
-        if (!seen[cl] || a[cl] <= 0) a[cl] = mean;
     const CostModelD d = default_cost_model();
     CostModelD m = d;
-    for (int cl = 0; cl < P_EMPTY; ++cl) m.ns_per_unit[cl] = a[cl] * d.ns_per_unit[cl];
-    m.ns_per_unit_cb = (seen[P_EMPTY] && a[P_EMPTY] > 0) ? a[P_EMPTY] * CB_UNIT_REF : 0.0;
-    m.ns_fixed = a[K - 1];
+    m.ns_fixed = 0.0;
+    for (int cl = 0; cl < P_EMPTY; ++cl) {
+        if (!fitted[cl] || !(a[cl] > 0)) {
+            a[cl] = mean;
+            f[cl] = 0.0;
+        }
+        m.ns_per_unit[cl] = a[cl] * d.ns_per_unit[cl];
+        m.ns_fixed_cell[cl] = f[cl];
+    }
+    const bool cb = fitted[P_EMPTY] && a[P_EMPTY] > 0;
+    m.ns_per_unit_cb = cb ? a[P_EMPTY] * CB_UNIT_REF : 0.0;
+    m.ns_fixed_cell[P_CB] = cb ? f[P_EMPTY] : 0.0;
     m.ns_per_occ_word = a[P_BB] * d.ns_per_occ_word;
     m.ns_probe_hot = m.ns_probe_cold = 0.0;
     double se = 0;
@@ -1236,7 +1221,7 @@ static CostModelD fit_cost_model(const TileTimings& tt, const std::vector<uint32
             const size_t e = (size_t)k * N_SLOTS + cl;
             if (tt.cyc[e] == ~0ull || tt.npairs[e] == 0 || tt.pred[e] <= 0.0) continue;
             const double y = (double)tt.cyc[e];
-            const double p = a[cl] * tt.pred[e] + a[K - 1] * tt.npairs[e];
+            const double p = a[cl] * tt.pred[e] + f[cl] * tt.npairs[e];
             se += (p - y) * (p - y) / (y * y);
             ++cnt;
         }
@@ -1270,7 +1255,8 @@ int STORM_rows_calibrate(STORM_rows_t* r, uint32_t tile, uint32_t samples, uint6
             model_out[P_COUNT] = r->model.ns_fixed;
             model_out[P_COUNT + 1] = r->model.ns_per_occ_word;
             model_out[P_COUNT + 2] = r->model.ns_per_unit_cb;
-            model_out[P_COUNT + 3] = rms;
+            for (int p = 0; p <= P_CB; ++p) model_out[P_COUNT + 3 + p] = r->model.ns_fixed_cell[p];
+            model_out[P_COUNT + 3 + P_CB + 1] = rms;
         }
         return 0;
     });
@@ -1287,6 +1273,7 @@ int STORM_rows_cost_model(STORM_rows_t* r, double* model, int set) {
             r->model.ns_fixed = model[P_COUNT];
             r->model.ns_per_occ_word = model[P_COUNT + 1];
             r->model.ns_per_unit_cb = model[P_COUNT + 2];
+            for (int p = 0; p <= P_CB; ++p) r->model.ns_fixed_cell[p] = model[P_COUNT + 3 + p];
             r->model.ns_probe_hot = r->model.ns_probe_cold = 0.0;
             r->calibrated = true;
         }
@@ -1298,6 +1285,7 @@ int STORM_rows_cost_model(STORM_rows_t* r, double* model, int set) {
     model[P_COUNT] = r->model.ns_fixed;
     model[P_COUNT + 1] = r->model.ns_per_occ_word;
     model[P_COUNT + 2] = r->model.ns_per_unit_cb;
+    for (int p = 0; p <= P_CB; ++p) model[P_COUNT + 3 + p] = r->model.ns_fixed_cell[p];
     return r->calibrated ? 1 : 0;
 }
 
@@ -1405,8 +1393,10 @@ int STORM_rows_train_selector(STORM_rows_t* r, uint32_t tile, uint32_t samples, 
             stats[4] = reg_mlp;
             stats[5] = reg_cal;
         }
+        double fixed_mean = 0.0;
+        for (int cl = 0; cl < P_EMPTY; ++cl) fixed_mean += r->model.ns_fixed_cell[cl] / P_EMPTY;
         const double rep[8] = {reg_mlp, reg_cal, reg_def, (double)te_idx.size(), (double)tr_idx.size(), rms,
-                               r->model.ns_fixed, (double)ns};
+                               r->model.ns_fixed + fixed_mean, (double)ns};
         std::copy(rep, rep + 8, r->last_training);
         drop_graph(r);
         return 0;

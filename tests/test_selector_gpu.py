@@ -110,7 +110,7 @@ def test_gpu_calibration_of_the_cost_model(sb):
     for s in sets:
         r.add(s)
     model, rms = r.calibrate(tile=32, samples=0, seed=5)
-    assert len(model) == 14 and all(x >= 0 for x in model)
+    assert len(model) == 26 and all(x >= 0 for x in model)
     assert 0.0 <= rms < 10.0
     got, cal = r.cost_model()
     assert cal and np.allclose(got, model)
