@@ -871,6 +871,7 @@ def storm_t_full(device, names=tuple(FULL_CORPORA), cpu_seconds=2.0):
                        "tensor_rows": st.last_dense()[0], "postings_rows": st.last_postings_rows(),
                        "panel_rows": st.last_panel_rows()}
         r["engines"] = engine_roofline(st.last_engine_ms(), device)
+        r["engines"]["plan_ms"] = round(st.last_plan_ms(), 3)
         got_row, diag = triangle_row_sums(d_tri, n)
         ok = (bool(torch.equal(diag.cpu(), torch.as_tensor(cards))) and
               int((got_row != res["want_row"]).sum().item()) == 0 and sums == {want_sum})
@@ -952,7 +953,10 @@ def engine_case(engine, device, n=4096, universe=1 << 24, calls=3):
     sums = set()
     for _ in range(calls):
         sums.add(st.matrix_device(d_tri.data_ptr(), tri))
-        res["calls"].append({"ms": round(st.last_kernel_ms(), 3), "engines": engine_roofline(st.last_engine_ms(), device)})
+        res["calls"].append({"ms": round(st.last_kernel_ms(), 3), "plan_ms": round(st.last_plan_ms(), 3),
+                             "rows": {"tensor": st.last_dense()[0], "panel": st.last_panel_rows(),
+                                      "postings": st.last_postings_rows()},
+                             "engines": engine_roofline(st.last_engine_ms(), device)})
     res["same_sum"] = len(sums) == 1
     st.close()
     return res
@@ -977,6 +981,7 @@ def forms_on(sb, sets, universe, tile=64, samples=1024, with_plain=True):
     res = {"rows": n, "pairs": pairs,
            "regret_learned": round(sel["regret_mlp"], 4),
            "regret_cost_model_calibrated": round(lt["regret_calibrated_model"], 4),
+           "fallback_model": "calibrated" if lt["kept_calibrated_model"] else "reference default",
            "regret_cost_model_default": round(lt["regret_default_model"], 4),
            "train_accuracy": round(sel["train_accuracy"], 3)}
     sums = set()
@@ -1380,7 +1385,7 @@ def run_b200_arm(args):
     w = rows_d.shape[1]
     c = sb.StormContig(m)
     c.set_kernel({"auto": sb.KERNEL_AUTO, "popc": sb.KERNEL_POPC, "mma": sb.KERNEL_MMA,
-                  "mma_ss": sb.KERNEL_MMA_SS, "mma_db": sb.KERNEL_MMA_DB}[args.kernel])
+                  "mma_ss": sb.KERNEL_MMA_SS, "mma_db": sb.KERNEL_MMA_DB, "mma_2cta": sb.KERNEL_MMA_2CTA}[args.kernel])
     c.set_schedule({"auto": sb.SCHED_AUTO, "tiles": sb.SCHED_TILES, "stream_k": sb.SCHED_STREAM_K}[args.schedule])
     rc = sb.lib().STORM_contig_add_bitmaps(c.h, C.cast(rows_d.data_ptr(), sb.u64p), n, w)
     if rc < 0:
@@ -1427,7 +1432,8 @@ def run_b200_arm(args):
     elapsed_ms = max_over_ranks(elapsed_ms, dist, device)
     launches = args.steps * c.last_launches()
     kernel_used = {sb.KERNEL_POPC: "bb_popc_kernel", sb.KERNEL_MMA: "bb_mma_ts_kernel",
-                   sb.KERNEL_MMA_SS: "bb_mma_kernel", sb.KERNEL_MMA_DB: "bb_mma_ts2_kernel"}.get(c.last_kernel(), "?")
+                   sb.KERNEL_MMA_SS: "bb_mma_kernel", sb.KERNEL_MMA_DB: "bb_mma_ts2_kernel",
+                   sb.KERNEL_MMA_2CTA: "bb_mma_2cta_kernel"}.get(c.last_kernel(), "?")
     ms_per_step = elapsed_ms / args.steps
     value = world * tri / (ms_per_step / 1e3)
 
@@ -1603,7 +1609,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma", "mma_ss", "mma_db"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma", "mma_ss", "mma_db", "mma_2cta"])
     ap.add_argument("--schedule", default="auto", choices=["auto", "tiles", "stream_k"],
                     help="tensor-core work schedule (whole tiles or stream-K; auto picks per launch)")
     ap.add_argument("--rows", type=int, default=N_ROWS)

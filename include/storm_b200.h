@@ -164,8 +164,9 @@ int STORM_contig_last_kernel(const STORM_contiguous_t* c);
  * service that reserves all of HBM for its own pool at start-up and forbids
  * cudaMalloc afterwards, or a framework whose allocator owns every device
  * buffer.  The caller owns both buffers:
- *   d_rows  row r at d_rows + r * row_pitch_words (pitch a multiple of 8
- *           words); ceil(n_rows / 256) * 256 rows must be readable, the
+ *   d_rows  32-byte aligned (STORM_B200_EARG otherwise; any cudaMalloc
+ *           pointer is), row r at d_rows + r * row_pitch_words (pitch a
+ *           multiple of 8 words); ceil(n_rows / 256) * 256 rows must be readable, the
  *           rows from n_rows on must be zero, and so must every bit of a row
  *           at or past row_bits (up to the pitch);
  *   d_out   n_rows*(n_rows+1)/2 u32, packed upper triangle (may be NULL for
@@ -311,6 +312,11 @@ uint64_t STORM_last_panel_rows(const STORM_t* s);
  * postings: 8 bytes per value, per list entry and per increment, and the
  * universe-sized histogram). */
 int STORM_last_engine_ms(const STORM_t* s, double* out12);
+/* The rest of the last per-pair call's device time before its first engine:
+ * the planner's host work while the GPU waits (after the postings' histogram
+ * statistics are read back), the row order's upload and the output's
+ * clearing, in ms; -1.0 for a NULL handle. */
+double STORM_last_plan_ms(const STORM_t* s);
 /* GPU calibration of the planner (no counterpart in the reference's C ABI;
  * its calibrate_on_rows fits the kernel layer's constants on the host,
  * storm_cost.cpp:779-895): on a strided sample of up to sample_rows rows (0:

@@ -157,16 +157,19 @@ int64_t STORM_rows_cell(STORM_rows_t* r, int pairing, uint64_t row_a, uint64_t r
  * regret of the MLP on held-out tiles, regret of the cost model there. */
 int STORM_rows_train_selector(STORM_rows_t* r, uint32_t tile, uint32_t samples, uint32_t epochs,
                               uint64_t seed, double* stats);
-/* The selector's training also fits this container's cost model to the
- * cell timings of its training tiles (as STORM_rows_calibrate does), so
- * the cost-model policies and the untrained/fallback selector price cells
- * with this GPU's constants from then on; stats[5] is the regret of that
- * calibrated model.  STORM_rows_last_training reports the last training:
- * out8 = regret of the MLP, of the calibrated model and of the reference's
- * default model on the held-out tiles, held-out and training tile counts,
- * the calibration's relative RMS error, its mean fixed cost per pair over
- * the reference's ten cells, sampled tiles. */
-int STORM_rows_last_training(const STORM_rows_t* r, double* out8);
+/* The selector's training also fits a cost model to the cell timings of
+ * its training tiles (as STORM_rows_calibrate does) and keeps, as this
+ * container's model from then on (the cost-model policies and the
+ * untrained/fallback selector), whichever of that fitted model and the
+ * reference's default model has the lower regret on the training tiles;
+ * stats[5] is the regret of the fitted model on the held-out tiles.
+ * STORM_rows_last_training reports the last training: out9 = regret of the
+ * MLP, of the fitted model and of the reference's default model on the
+ * held-out tiles, held-out and training tile counts, the fit's relative RMS
+ * error, the kept model's mean fixed cost per pair over the reference's ten
+ * cells, sampled tiles, and 1 if the fitted model was kept (0: the default
+ * model). */
+int STORM_rows_last_training(const STORM_rows_t* r, double* out9);
 /* Reset to the untrained (cost-model fallback) selector. */
 int STORM_rows_reset_selector(STORM_rows_t* r);
 

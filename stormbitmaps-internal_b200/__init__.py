@@ -115,6 +115,7 @@ _sig("STORM_set_sparse_postings", C.c_int, [C.c_void_p, C.c_int])
 _sig("STORM_last_postings_rows", C.c_uint64, [C.c_void_p])
 _sig("STORM_set_panel", C.c_int, [C.c_void_p, C.c_int])
 _sig("STORM_last_engine_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_double)])
+_sig("STORM_last_plan_ms", C.c_double, [C.c_void_p])
 _sig("STORM_calibrate", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_double)])
 _sig("STORM_reset_cost_model", C.c_int, [C.c_void_p])
 _sig("STORM_last_panel_rows", C.c_uint64, [C.c_void_p])
@@ -491,6 +492,11 @@ class Storm:
         _check(_lib.STORM_last_engine_ms(self.h, o), "STORM_last_engine_ms")
         return {k: (o[i], o[4 + i], o[8 + i]) for i, k in enumerate(("tensor", "chunk", "panel", "postings"))}
 
+    def last_plan_ms(self) -> float:
+        """Device time of the last per-pair call spent before its engines on
+        planning (host), the row order's upload and clearing the output."""
+        return float(_lib.STORM_last_plan_ms(self.h))
+
     def calibrate(self, sample_rows: int = 0):
         """GPU calibration of the planner: (tensor, panel, postings) scales and sample rows."""
         o = (C.c_double * 4)()
@@ -688,10 +694,10 @@ class StormRows:
         return dict(zip(keys, list(stats)))
 
     def last_training(self):
-        out = (C.c_double * 8)()
+        out = (C.c_double * 9)()
         _check(_lib.STORM_rows_last_training(self.h, out), "STORM_rows_last_training")
         keys = ["regret_mlp", "regret_calibrated_model", "regret_default_model", "test_tiles", "train_tiles",
-                "calibration_rms", "calibrated_fixed_cycles", "sampled_tiles"]
+                "calibration_rms", "calibrated_fixed_cycles", "sampled_tiles", "kept_calibrated_model"]
         return dict(zip(keys, list(out)))
 
     def calibrate(self, tile=64, samples=0, seed=1):

@@ -201,22 +201,19 @@ __device__ __forceinline__ void c2_body(const uint64_t* __restrict__ X, uint32_t
             const uint64_t i0 = (uint64_t)tiles[t].x * C2_BM + 128u * rank;
             const uint64_t j0 = (uint64_t)tiles[t].y * C2_BN;
             const uint64_t* src = X + (is_a ? i0 + prow : j0 + 128u * rank + prow) * (uint64_t)w_pad;
-            uint4 v0 = __ldg(reinterpret_cast<const uint4*>(src));
-            uint4 v1 = __ldg(reinterpret_cast<const uint4*>(src) + 1);
+            // loads run two stages ahead of the expansion
+            Row32 v = ldg_row32(src), nv{};
+            if (1 < nk) nv = ldg_row32(src + 4);
             for (uint32_t kb = 0; kb < nk; ++kb, ++g) {
                 const uint32_t s = g % C2_STAGES;
                 const uint32_t round = g / C2_STAGES;
-                uint4 n0 = make_uint4(0, 0, 0, 0), n1 = n0;
-                if (kb + 1 < nk) {
-                    n0 = __ldg(reinterpret_cast<const uint4*>(src + 4 * (kb + 1)));
-                    n1 = __ldg(reinterpret_cast<const uint4*>(src + 4 * (kb + 1)) + 1);
-                }
+                Row32 nnv{};
+                if (kb + 2 < nk) nnv = ldg_row32(src + 4 * (kb + 2));
                 if (!c2_wait<true>(smem_u32(&ctl->empty[s]), (round & 1) ^ 1, ctl, flags, ERR_C2_PROD_EMPTY)) {
                     ok = false;
                     break;
                 }
-                const uint64_t w[4] = {((uint64_t)v0.y << 32) | v0.x, ((uint64_t)v0.w << 32) | v0.z,
-                                       ((uint64_t)v1.y << 32) | v1.x, ((uint64_t)v1.w << 32) | v1.z};
+                const uint64_t (&w)[4] = v.w;
                 if (is_a) {
                     const uint32_t taddr = tmem_base + ((uint32_t)(warp & 3) * 32u << 16) + C2_A_COL0 + 64u * s;
 #pragma unroll
@@ -237,8 +234,8 @@ __device__ __forceinline__ void c2_body(const uint64_t* __restrict__ X, uint32_t
                 }
                 __syncwarp();
                 if (lane == 0) mbar_arrive_cluster(lead_full0 + 8u * s);
-                v0 = n0;
-                v1 = n1;
+                v = nv;
+                nv = nnv;
             }
             if (!ok) break;
             // ---- epilogue: this CTA's 128 x 256 accumulator

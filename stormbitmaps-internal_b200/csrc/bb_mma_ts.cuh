@@ -214,22 +214,19 @@ __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t
             const uint64_t i0 = (uint64_t)tiles[t].x * TS_BM;
             const uint64_t j0 = (uint64_t)tiles[t].y * TS_BN;
             const uint64_t* src = X + (is_a ? i0 + prow : j0 + prow) * (uint64_t)w_pad;
-            uint4 v0 = __ldg(reinterpret_cast<const uint4*>(src + 4 * kb0));
-            uint4 v1 = __ldg(reinterpret_cast<const uint4*>(src + 4 * kb0) + 1);
+            // loads run two stages ahead of the expansion
+            Row32 v = ldg_row32(src + 4 * kb0), nv{};
+            if (kb0 + 1 < kb1) nv = ldg_row32(src + 4 * (kb0 + 1));
             for (uint32_t kb = kb0; kb < kb1; ++kb, ++g) {
                 const uint32_t s = g % TS_STAGES;
                 const uint32_t round = g / TS_STAGES;
-                uint4 n0 = make_uint4(0, 0, 0, 0), n1 = n0;
-                if (kb + 1 < kb1) {
-                    n0 = __ldg(reinterpret_cast<const uint4*>(src + 4 * (kb + 1)));
-                    n1 = __ldg(reinterpret_cast<const uint4*>(src + 4 * (kb + 1)) + 1);
-                }
+                Row32 nnv{};
+                if (kb + 2 < kb1) nnv = ldg_row32(src + 4 * (kb + 2));
                 if (!ts_wait(smem_u32(&ctl->empty[s]), (round & 1) ^ 1, ctl, flags, ERR_PROD_EMPTY)) {
                     ok = false;
                     break;
                 }
-                const uint64_t w[4] = {((uint64_t)v0.y << 32) | v0.x, ((uint64_t)v0.w << 32) | v0.z,
-                                       ((uint64_t)v1.y << 32) | v1.x, ((uint64_t)v1.w << 32) | v1.z};
+                const uint64_t (&w)[4] = v.w;
                 if (is_a) {
                     // lanes 32*(warp%4).. ; columns A_COL0 + 64 s + [0, 64)
                     const uint32_t taddr = tmem_base + ((uint32_t)(warp & 3) * 32u << 16) + TS_A_COL0 + 64u * s;
@@ -253,8 +250,8 @@ __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t
                     fence_proxy_async_smem();
                 }
                 mbar_arrive(smem_u32(&ctl->full[s]));
-                v0 = n0;
-                v1 = n1;
+                v = nv;
+                nv = nnv;
             }
             if (!ok) break;
             if (warp >= 8) continue;   // warps 8-11 do not take part in the epilogue

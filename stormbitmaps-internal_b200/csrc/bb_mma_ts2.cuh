@@ -113,23 +113,20 @@ __device__ __forceinline__ void ts2_body(const uint64_t* __restrict__ X, uint32_
             const uint64_t row = is_a ? (uint64_t)tiles[t].x * T2_BM + prow : (uint64_t)tiles[t].y * T2_BN + prow;
             const bool live = row < n;
             const uint64_t* src = X + (live ? row : 0) * (uint64_t)w_pad;
-            const uint4 z = make_uint4(0, 0, 0, 0);
-            uint4 v0 = live ? __ldg(reinterpret_cast<const uint4*>(src + 4 * kb0)) : z;
-            uint4 v1 = live ? __ldg(reinterpret_cast<const uint4*>(src + 4 * kb0) + 1) : z;
+            // loads run two stages ahead of the expansion
+            Row32 v{}, nv{};
+            if (live) v = ldg_row32(src + 4 * kb0);
+            if (live && kb0 + 1 < kb1) nv = ldg_row32(src + 4 * (kb0 + 1));
             for (uint32_t kb = kb0; kb < kb1; ++kb, ++g) {
                 const uint32_t s = g % T2_STAGES;
                 const uint32_t round = g / T2_STAGES;
-                uint4 n0 = z, n1 = z;
-                if (live && kb + 1 < kb1) {
-                    n0 = __ldg(reinterpret_cast<const uint4*>(src + 4 * (kb + 1)));
-                    n1 = __ldg(reinterpret_cast<const uint4*>(src + 4 * (kb + 1)) + 1);
-                }
+                Row32 nnv{};
+                if (live && kb + 2 < kb1) nnv = ldg_row32(src + 4 * (kb + 2));
                 if (!t2_wait(smem_u32(&ctl->empty[s]), (round & 1) ^ 1, ctl, flags, ERR_PROD_EMPTY)) {
                     ok = false;
                     break;
                 }
-                const uint64_t w[4] = {((uint64_t)v0.y << 32) | v0.x, ((uint64_t)v0.w << 32) | v0.z,
-                                       ((uint64_t)v1.y << 32) | v1.x, ((uint64_t)v1.w << 32) | v1.z};
+                const uint64_t (&w)[4] = v.w;
                 if (is_a) {
                     const uint32_t taddr = tmem_base + ((uint32_t)(warp & 3) * 32u << 16) + t2_a_col(s);
 #pragma unroll
@@ -150,8 +147,8 @@ __device__ __forceinline__ void ts2_body(const uint64_t* __restrict__ X, uint32_
                     fence_proxy_async_smem();
                 }
                 mbar_arrive(smem_u32(&ctl->full[s]));
-                v0 = n0;
-                v1 = n1;
+                v = nv;
+                nv = nnv;
             }
         }
     } else if (warp == T2_MMA_WARP) {

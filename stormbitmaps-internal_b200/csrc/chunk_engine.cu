@@ -923,6 +923,8 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
     const bool post_ok = postings_mode != 0 && U <= POSTINGS_MAX_UNIVERSE && facts_ok;
     const double tc_ns = tensor_pair_ns(cost, slots);
     std::vector<uint8_t> cls(n, 0);                        // 0 C, 1 L, 2 M, 3 H
+    if (!ev_hist) SB_CUDA(cudaEventCreate(&ev_hist));
+    bool hist_ran = false;
     last_panel_rows = last_panel_queries = 0;
 
     SB_CUDA(cudaEventRecord(log.ev0, st));
@@ -938,6 +940,8 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         postings_hist_kernel<<<gq, 256, 0, st>>>(d.view(), d_qrows.p, (uint32_t)rows.size(), d_counts.p);
         postings_stats_kernel<<<sms * 8, 256, 0, st>>>(d_counts.p, U, d_pstats.p);
         SB_CUDA(cudaGetLastError());
+        SB_CUDA(cudaEventRecord(ev_hist, st));
+        hist_ran = true;
         launches += 2;
         PostingsStats h{};
         SB_CUDA(cudaMemcpyAsync(&h, d_pstats.p, sizeof(h), cudaMemcpyDeviceToHost, st));
@@ -1307,21 +1311,67 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
     if (panel_plan && (nm || nd) && (nq + nm)) {
         const uint64_t pw0 = nc + nq;                      // walk position of the first panel row
         const uint64_t npw = nm + nd;
-        // query rows (walk positions of L and M), heaviest first
-        std::vector<uint32_t> xo;
-        xo.reserve(nq + nm);
+        // Work items over the query rows (walk positions of L and M),
+        // heaviest first: a row with more than `seg` values is split into
+        // ranges of its chunks (about seg values each), so that the warps
+        // finish together; seg is sized for ~64 items per SM and at least
+        // PANEL_MIN_SEG values (the per-item epilogue costs about as much as
+        // a few hundred values), and doubled until the split rows' scratch
+        // slots fit PANEL_MAX_SLOTS.
         uint64_t max_card = 0;
+        double total = 0.0;
         for (uint64_t w = nc; w < nc + nq + nm; ++w) {
-            xo.push_back((uint32_t)w);
-            max_card = std::max<uint64_t>(max_card, d.facts[h_perm[w]].card);
+            const uint64_t c = d.facts[h_perm[w]].card;
+            max_card = std::max<uint64_t>(max_card, c);
+            total += (double)c;
         }
-        std::stable_sort(xo.begin(), xo.end(), [&](uint32_t x, uint32_t y) {
-            return d.facts[h_perm[x]].card > d.facts[h_perm[y]].card;
-        });
-        d_xorder.reserve(xo.size());
+        std::vector<PanelItem> items;
+        std::vector<PanelSplit> splits;
+        std::vector<double> weight;
+        uint32_t nslots = 0;
+        for (uint64_t seg = std::max<uint64_t>(PANEL_MIN_SEG, (uint64_t)(total / (64.0 * sms)));; seg *= 2) {
+            items.clear();
+            splits.clear();
+            weight.clear();
+            nslots = 0;
+            for (uint64_t w = nc; w < nc + nq + nm; ++w) {
+                const ChunkRowFacts& f = d.facts[h_perm[w]];
+                const uint32_t ns =
+                    f.card > seg && f.chunks > 1 ? (uint32_t)std::min<uint64_t>(f.chunks, (f.card + seg - 1) / seg) : 1u;
+                if (ns == 1) {
+                    items.push_back(PanelItem{(uint32_t)w, 0u, f.chunks, PANEL_NO_VALUE});
+                    weight.push_back((double)f.card);
+                    continue;
+                }
+                splits.push_back(PanelSplit{(uint32_t)w, nslots, ns, 0u});
+                for (uint32_t k = 0; k < ns; ++k) {
+                    const uint32_t lo = (uint32_t)((uint64_t)f.chunks * k / ns);
+                    const uint32_t hi = (uint32_t)((uint64_t)f.chunks * (k + 1) / ns);
+                    items.push_back(PanelItem{(uint32_t)w, lo, hi, nslots + k});
+                    weight.push_back((double)f.card * (double)(hi - lo) / (double)f.chunks);
+                }
+                nslots += ns;
+            }
+            if (nslots <= PANEL_MAX_SLOTS) break;
+        }
+        {
+            std::vector<uint32_t> ord(items.size());
+            for (uint32_t k = 0; k < ord.size(); ++k) ord[k] = k;
+            std::stable_sort(ord.begin(), ord.end(), [&](uint32_t x, uint32_t y) { return weight[x] > weight[y]; });
+            std::vector<PanelItem> sorted(items.size());
+            for (uint32_t k = 0; k < ord.size(); ++k) sorted[k] = items[ord[k]];
+            items.swap(sorted);
+        }
+        d_items.reserve(items.size());
         d_ctr.reserve(1);
         d_pmap.reserve(PANEL_ROWS);
-        SB_CUDA(cudaMemcpyAsync(d_xorder.p, xo.data(), xo.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        SB_CUDA(cudaMemcpyAsync(d_items.p, items.data(), items.size() * sizeof(PanelItem), cudaMemcpyHostToDevice, st));
+        if (!splits.empty()) {
+            d_splits.reserve(splits.size());
+            d_pscratch.reserve((uint64_t)nslots * PANEL_ROWS);
+            SB_CUDA(cudaMemcpyAsync(d_splits.p, splits.data(), splits.size() * sizeof(PanelSplit),
+                                    cudaMemcpyHostToDevice, st));
+        }
         static std::atomic<uint64_t> t_done{0};
         smem_attr_once(panel_transpose_kernel, (int)PANEL_T_SMEM, t_done);
         std::vector<uint32_t> bmap(PANEL_ROWS);
@@ -1334,24 +1384,24 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
                                  st>>>(d.view(), d_pmap.p, PANEL_ROWS, (uint32_t)W, d_pX.p);
             panel_transpose_kernel<<<(uint32_t)(W / PANEL_T_WORDS), 1024, PANEL_T_SMEM, st>>>(d_pX.p, W, d_DT.p);
             SB_CUDA(cudaMemsetAsync(d_ctr.p, 0, sizeof(unsigned long long), st));
-            const uint32_t nx = (uint32_t)xo.size();
-            if (max_card < (1ull << 11))
-                panel_query_kernel<8><<<qgrid, PANEL_Q_WARPS * 32, 0, st>>>(d.view(), perm, d_xorder.p, nx, pw0 + b0,
-                                                                            prows, d_DT.p, n, d_out, d_flags.p, d_ctr.p);
-            else if (max_card < (1ull << 15))
-                panel_query_kernel<12><<<qgrid, PANEL_Q_WARPS * 32, 0, st>>>(d.view(), perm, d_xorder.p, nx, pw0 + b0,
-                                                                             prows, d_DT.p, n, d_out, d_flags.p, d_ctr.p);
-            else if (max_card < (1ull << 19))
-                panel_query_kernel<16><<<qgrid, PANEL_Q_WARPS * 32, 0, st>>>(d.view(), perm, d_xorder.p, nx, pw0 + b0,
-                                                                             prows, d_DT.p, n, d_out, d_flags.p, d_ctr.p);
-            else if (max_card < (1ull << 23))
-                panel_query_kernel<20><<<qgrid, PANEL_Q_WARPS * 32, 0, st>>>(d.view(), perm, d_xorder.p, nx, pw0 + b0,
-                                                                             prows, d_DT.p, n, d_out, d_flags.p, d_ctr.p);
-            else
-                panel_query_kernel<24><<<qgrid, PANEL_Q_WARPS * 32, 0, st>>>(d.view(), perm, d_xorder.p, nx, pw0 + b0,
-                                                                             prows, d_DT.p, n, d_out, d_flags.p, d_ctr.p);
-            SB_CUDA(cudaGetLastError());
+            const uint32_t ni = (uint32_t)items.size();
+            uint32_t* scr = splits.empty() ? nullptr : d_pscratch.p;
+#define SB_PANEL_QUERY(NP)                                                                                      \
+    panel_query_kernel<NP><<<qgrid, PANEL_Q_WARPS * 32, 0, st>>>(d.view(), perm, d_items.p, ni, pw0 + b0, prows, \
+                                                                 d_DT.p, n, d_out, scr, d_flags.p, d_ctr.p)
+            if (max_card < (1ull << 11)) SB_PANEL_QUERY(8);
+            else if (max_card < (1ull << 15)) SB_PANEL_QUERY(12);
+            else if (max_card < (1ull << 19)) SB_PANEL_QUERY(16);
+            else if (max_card < (1ull << 23)) SB_PANEL_QUERY(20);
+            else SB_PANEL_QUERY(24);
+#undef SB_PANEL_QUERY
             launches += 3;
+            if (scr && d_out) {
+                panel_reduce_kernel<<<(uint32_t)std::min<uint64_t>(splits.size(), (uint64_t)sms * 8), 256, 0, st>>>(
+                    perm, d_splits.p, (uint32_t)splits.size(), pw0 + b0, prows, scr, n, d_out);
+                ++launches;
+            }
+            SB_CUDA(cudaGetLastError());
         }
         last_panel_rows = npw;
         last_panel_queries = nq + nm;
@@ -1400,8 +1450,9 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         ++launches;
     }
     const uint64_t total = finish(q_sum);
-    float t_pre = 0, t_tc = 0, t_ch = 0, t_pa = 0, t_po = 0;
+    float t_pre = 0, t_hist = 0, t_tc = 0, t_ch = 0, t_pa = 0, t_po = 0;
     SB_CUDA(cudaEventElapsedTime(&t_pre, log.ev0, ev_eng[0]));
+    if (hist_ran) SB_CUDA(cudaEventElapsedTime(&t_hist, log.ev0, ev_hist));
     SB_CUDA(cudaEventElapsedTime(&t_tc, ev_eng[0], ev_eng[1]));
     SB_CUDA(cudaEventElapsedTime(&t_ch, ev_eng[1], ev_eng[2]));
     SB_CUDA(cudaEventElapsedTime(&t_pa, ev_eng[2], ev_eng[3]));
@@ -1409,7 +1460,11 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
     last_engine_ms[0] = t_tc;
     last_engine_ms[1] = t_ch;
     last_engine_ms[2] = t_pa;
-    last_engine_ms[3] = t_po + (nq ? t_pre : 0.f);
+    last_engine_ms[3] = t_po + (nq ? t_hist : 0.f);
+    // the rest of the time before the engines: planning on the host while
+    // the GPU waits (after the histogram's statistics were read back), the
+    // row order's upload and the output's clearing
+    last_plan_ms = nq ? t_pre - t_hist : t_pre;
     return total;
 }
 

@@ -135,6 +135,20 @@ struct ChunkDev {
 
 struct PostingsStats;   // chunk_engine.cu
 
+// Work item of the transposed-panel engine (panel.cuh): the query row's walk
+// position, the range [c_lo, c_hi) of its chunks (indices within the row),
+// and its scratch slot (0xFFFFFFFF: the item is the whole row and writes the
+// triangle itself).
+struct PanelItem {
+    uint32_t xw, c_lo, c_hi, slot;
+};
+
+// A query row split into work items: its walk position and its scratch
+// slots [slot0, slot0 + nslots).
+struct PanelSplit {
+    uint32_t xw, slot0, nslots, pad;
+};
+
 // Pair spaces the chunk kernel walks.
 enum PairMode : uint32_t {
     PAIRS_TRIANGLE = 0,   // i <= j < n, packed output
@@ -210,8 +224,12 @@ struct ChunkEngine {
     // per increment -- a read and a write of its count).
     double last_engine_work[4] = {0, 0, 0, 0};
     cudaEvent_t ev_eng[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev_hist = nullptr;     // after the postings' histogram
+    double last_plan_ms = 0.0;         // time before the first engine that is not the histogram
     DevBuf<uint64_t> d_pX, d_DT;       // panel block: expanded rows, transposed
-    DevBuf<uint32_t> d_xorder, d_pmap, d_mrows;
+    DevBuf<PanelItem> d_items;
+    DevBuf<PanelSplit> d_splits;
+    DevBuf<uint32_t> d_pscratch, d_pmap, d_mrows;
     DevBuf<unsigned long long> d_ctr;
     DevBuf<uint32_t> d_perm, d_map;
     DevBuf<uint32_t> d_qrows, d_counts, d_start, d_post;
@@ -223,6 +241,7 @@ struct ChunkEngine {
         log.destroy();
         for (cudaEvent_t e : ev_eng)
             if (e) cudaEventDestroy(e);
+        if (ev_hist) cudaEventDestroy(ev_hist);
     }
     // Returns the sum over i < j (triangle) or over all (i, j) (rect).
     uint64_t run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_t n2, uint32_t* d_out,

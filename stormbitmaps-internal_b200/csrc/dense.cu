@@ -428,6 +428,7 @@ extern "C" int STORM_contig_pairw_intersect_matrix_noalloc(const uint64_t* d_row
     using namespace sb200;
     if (d_rows == NULL) return STORM_B200_EVALUES;
     if (n_rows == 0 || n_rows > 0xFFFFFFFFull) return STORM_B200_EARG;
+    if ((uintptr_t)d_rows % 32 != 0) return STORM_B200_EARG;   // the kernel reads rows 32 bytes at a time
     if (row_pitch_words == 0 || row_pitch_words % 8 != 0 || (uint64_t)row_pitch_words * 64 < row_bits)
         return STORM_B200_EARG;
     if (row_bits > MMA_MAX_BITS) return STORM_B200_ELIMIT;

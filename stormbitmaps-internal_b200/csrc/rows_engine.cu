@@ -447,7 +447,7 @@ struct STORM_rows_s {
     // selector: the reference's defaults until calibrated on this GPU
     CostModelD model = default_cost_model();
     bool calibrated = false;
-    double last_training[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double last_training[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     // learned selector
     Mlp mlp;
     // CUDA graph of the batched form, keyed by the call's shape
@@ -1019,7 +1019,10 @@ cell_predict_kernel(PairCtx c, const uint32_t* __restrict__ tiles, uint32_t n_sa
         s_np = 0;
     }
     __syncthreads();
-    const CostModelD m = default_cost_model();
+    // the default model without the per-pair terms the fitted model drops
+    // (its fixed term, and the B x S probe's cold/hot difference)
+    CostModelD m = default_cost_model();
+    m.ns_probe_cold = m.ns_probe_hot = 0.0;
     double acc = 0.0;
     uint32_t cnt = 0;
     if (lane == 0) {
@@ -1178,14 +1181,38 @@ static CostModelD fit_cost_model(const TileTimings& tt, const std::vector<uint32
         fitted[cl] = cnt > 0;
         a[cl] = f[cl] = 0.0;
         if (!cnt) continue;
+        // The least-squares optimum under a > 0, f >= 0: the free optimum if
+        // it is inside, else the best point on the boundary -- f = 0 (time
+        // in proportion to work) or a at a floor (time per pair).
+        const double a_only = sxx > 0 ? sxy / sxx : 0.0;
         const double det = sxx * spp - sxp * sxp;
+        bool inside = false;
         if (cnt >= 3 && det > 1e-12 * sxx * spp) {
             a[cl] = (sxy * spp - spy * sxp) / det;
             f[cl] = (sxx * spy - sxp * sxy) / det;
+            inside = a[cl] > 0.0 && f[cl] >= 0.0;
         }
-        if (!(a[cl] > 0.0) || f[cl] < 0.0) {     // degenerate or unphysical: time / work
-            a[cl] = sx > 0 ? sy / sx : 0.0;
-            f[cl] = 0.0;
+        if (!inside) {
+            auto err = [&](double aa, double ff) {   // sum of squared relative errors
+                double e2 = 0;
+                for (uint32_t k : use) {
+                    const size_t e = (size_t)k * N_SLOTS + cl;
+                    if (tt.cyc[e] == ~0ull || tt.npairs[e] == 0 || tt.pred[e] <= 0.0) continue;
+                    const double y = (double)tt.cyc[e];
+                    const double r = (aa * tt.pred[e] + ff * (double)tt.npairs[e] - y) / y;
+                    e2 += r * r;
+                }
+                return e2;
+            };
+            const double a_floor = 1e-6 * (a_only > 0 ? a_only : (sx > 0 ? sy / sx : 1.0));
+            const double f_only = spp > 0 ? std::max(0.0, (spy - a_floor * sxp) / spp) : 0.0;
+            if (a_only > 0 && err(a_only, 0.0) <= err(a_floor, f_only)) {
+                a[cl] = a_only;
+                f[cl] = 0.0;
+            } else {
+                a[cl] = a_floor;
+                f[cl] = f_only;
+            }
         }
     }
     // reference cells with no sample take the mean scale of the others;
@@ -1335,12 +1362,37 @@ int STORM_rows_train_selector(STORM_rows_t* r, uint32_t tile, uint32_t samples, 
             (test ? Yte : Ytr).push_back(Y[k]);
             (test ? te_idx : tr_idx).push_back(idx[k]);
         }
-        // The cost model calibrated on the training tiles' timings becomes
-        // this container's model: the fallback of the learned policy and the
-        // model of the cost-model policies.
+        // Regret of a cost model on a set of sampled tiles: the measured
+        // cycles of the cell it picks (from the tile's block meta, as the
+        // per-tile policy does), summed, over the sum of the best cell's - 1.
+        auto model_regret = [&](const CostModelD& mm, const std::vector<uint32_t>& tiles) {
+            double best_sum = 0, got_sum = 0;
+            for (uint32_t k : tiles) {
+                uint32_t ti, tj;
+                tt.tile_of(k, ti, tj);
+                const unsigned long long* cy = tt.cyc.data() + (size_t)k * N_SLOTS;
+                int y = 0;
+                for (int cl = 1; cl < N_SLOTS; ++cl)
+                    if (cy[cl] < cy[y]) y = cl;
+                const RowMetaD& a = tt.bmeta[ti];
+                const RowMetaD& b = tt.bmeta[tj];
+                int cl = select_pairing_d(mm, a, b, nullptr);
+                if (cl == P_EMPTY) cl = (a.has_bm && b.has_bm) ? P_BB : P_SS;
+                const int sl = cl == P_CB ? P_EMPTY : cl;
+                best_sum += (double)cy[y];
+                got_sum += cy[sl] == ~0ull ? (double)cy[y] * 4.0 : (double)cy[sl];
+            }
+            return best_sum > 0 ? got_sum / best_sum - 1.0 : 0.0;
+        };
+        // The cost model calibrated on the training tiles' timings, or the
+        // reference's default model where that picks better cells on the
+        // same tiles, becomes this container's model: the fallback of the
+        // learned policy and the model of the cost-model policies.
         double rms = 0;
-        r->model = fit_cost_model(tt, tr_idx, &rms);
-        r->calibrated = true;
+        const CostModelD fitted = fit_cost_model(tt, tr_idx, &rms);
+        const bool keep_fit = model_regret(fitted, tr_idx) <= model_regret(default_cost_model(), tr_idx);
+        r->model = keep_fit ? fitted : default_cost_model();
+        r->calibrated = keep_fit;
         mlp_init(r->mlp, seed ^ 0xA5A5A5A5ull);
         r->mlp.dirty = true;
         const float loss = mlp_train(r->mlp, Xtr, Ytr, epochs ? epochs : 400, rows_stream(r));
@@ -1379,7 +1431,7 @@ int STORM_rows_train_selector(STORM_rows_t* r, uint32_t tile, uint32_t samples, 
             };
             best_sum += (double)cy[y];
             mlp_sum += cost(m_cell);
-            cal_sum += cost(model_cell(r->model));
+            cal_sum += cost(model_cell(fitted));
             def_sum += cost(model_cell(dflt));
         }
         const double reg_mlp = best_sum > 0 ? mlp_sum / best_sum - 1.0 : 0.0;
@@ -1395,18 +1447,18 @@ int STORM_rows_train_selector(STORM_rows_t* r, uint32_t tile, uint32_t samples, 
         }
         double fixed_mean = 0.0;
         for (int cl = 0; cl < P_EMPTY; ++cl) fixed_mean += r->model.ns_fixed_cell[cl] / P_EMPTY;
-        const double rep[8] = {reg_mlp, reg_cal, reg_def, (double)te_idx.size(), (double)tr_idx.size(), rms,
-                               r->model.ns_fixed + fixed_mean, (double)ns};
-        std::copy(rep, rep + 8, r->last_training);
+        const double rep[9] = {reg_mlp, reg_cal, reg_def, (double)te_idx.size(), (double)tr_idx.size(), rms,
+                               r->model.ns_fixed + fixed_mean, (double)ns, keep_fit ? 1.0 : 0.0};
+        std::copy(rep, rep + 9, r->last_training);
         drop_graph(r);
         return 0;
     });
 }
 
-int STORM_rows_last_training(const STORM_rows_t* r, double* out8) {
+int STORM_rows_last_training(const STORM_rows_t* r, double* out9) {
     if (r == NULL) return STORM_B200_ENULL;
-    if (out8 == NULL) return STORM_B200_EVALUES;
-    std::copy(r->last_training, r->last_training + 8, out8);
+    if (out9 == NULL) return STORM_B200_EVALUES;
+    std::copy(r->last_training, r->last_training + 9, out9);
     return 0;
 }
 

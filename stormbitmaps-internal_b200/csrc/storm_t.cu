@@ -787,6 +787,11 @@ int STORM_last_engine_ms(const STORM_t* s, double* out12) {
     return 0;
 }
 
+double STORM_last_plan_ms(const STORM_t* s) {
+    if (s == NULL) return -1.0;
+    return state_of(s)->engine.last_plan_ms;
+}
+
 // The planner's constants fitted to this GPU on a sample of the rows (the
 // reference's calibrate_on_rows, storm_cost.cpp:779-895, samples the
 // caller's pairs the same way: strided, not the first rows): every plain row

@@ -130,6 +130,20 @@ __device__ __forceinline__ void tmem_st_32x32b_x32(uint32_t taddr, const uint32_
         "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31])
         : "memory");
 }
+// One 256-bit stage of a packed row (4 words, 32-byte aligned) in a single
+// load instruction: the 32 lanes of a producer warp read 32 rows, and each
+// row costs one L1 wavefront instead of two for a pair of 128-bit loads.
+struct Row32 {
+    uint64_t w[4];
+};
+__device__ __forceinline__ Row32 ldg_row32(const uint64_t* p) {
+    Row32 r;
+    asm volatile("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];"
+                 : "=l"(r.w[0]), "=l"(r.w[1]), "=l"(r.w[2]), "=l"(r.w[3])
+                 : "l"(p));
+    return r;
+}
+
 __device__ __forceinline__ void tmem_st_wait() {
     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }

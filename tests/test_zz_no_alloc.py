@@ -71,6 +71,7 @@ def test_noalloc_rejects_what_it_cannot_do(sb):
     s = C.c_uint64(0)
     assert f(None, 10, 8, 512, None, 0, C.byref(s), None) == sb.EVALUES
     assert f(d.data_ptr(), 10, 7, 448, None, 0, C.byref(s), None) == sb.EARG       # pitch not a multiple of 8
+    assert f(d.data_ptr() + 16, 10, 8, 512, None, 0, C.byref(s), None) == sb.EARG  # rows not 32-byte aligned
     big = (1 << 23) + 64                                                           # rows too long to stay exact
     assert f(d.data_ptr(), 10, (big // 64 + 7) // 8 * 8, big, None, 0, C.byref(s), None) == sb.ELIMIT
     assert f(d.data_ptr(), 46081, 8, 512, None, 0, C.byref(s), None) == sb.ELIMIT  # tile list over its maximum
