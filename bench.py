@@ -1271,6 +1271,9 @@ def storm_t_forms(device, cpu_seconds=2.0, only=None):
     return out
 
 
+TENSOR_KERNELS = ("bb_mma_kernel", "bb_mma_ts_kernel", "bb_mma_ts2_kernel", "bb_mma_2cta_kernel")
+
+
 def north_star_summary(line):
     """The figures the target names, compactly: the tensor-core kernel's
     fraction of the measured 8-bit peak on the headline workload and on the
@@ -1514,7 +1517,7 @@ def run_b200_arm(args):
 
     # ---- roofline of the dominant kernel ----
     k_ms = statistics.median(kernel_ms)
-    if kernel_used in ("bb_mma_kernel", "bb_mma_ts_kernel", "bb_mma_ts2_kernel"):
+    if kernel_used in TENSOR_KERNELS:
         ops = 2.0 * tri * m                      # u8 MACs = pairs x row bits, 2 ops each
         achieved = ops / (k_ms / 1e3) / 1e12
         peak, peak_src = tensor_peak_tops(device)
@@ -1535,7 +1538,7 @@ def run_b200_arm(args):
         "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "ns_per_pair": 1e9 / (value / world),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8 (tcgen05 kind::i8, s32 acc)"
-        if kernel_used in ("bb_mma_kernel", "bb_mma_ts_kernel", "bb_mma_ts2_kernel") else "u64 (AND + POPC)",
+        if kernel_used in TENSOR_KERNELS else "u64 (AND + POPC)",
         "data": "synthetic (seeded Bernoulli rows generated on the GPU)",
         "config": {"workload": f"dense all-bitmap XX^T: {n} rows x {m} bits, p~U[0.05,0.5], u32 i<=j out",
                    "rows": n, "bits": m, "pairs_per_gpu": tri, "kernel": kernel_used, "schedule": args.schedule,

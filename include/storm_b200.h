@@ -257,7 +257,9 @@ float STORM_last_kernel_ms(const STORM_t* s);
  * pair (which grows with the universe); min_density > 0: when its value
  * count is >= min_density x universe; 0 disables the block.
  * budget_bytes bounds the expanded rows held at once (0: 60 % of free device
- * memory); larger sets run in panels.  Applies to later all-pairs calls. */
+ * memory), each row taking (universe / 65536) x 8256 bytes (its 8 KiB
+ * chunk slots 64 bytes apart); larger sets run in panels.  Applies to later
+ * all-pairs calls. */
 int STORM_set_dense_block(STORM_t* s, double min_density, uint64_t budget_bytes);
 /* Rows / panels the last all-pairs call on s gave to the dense block. */
 uint64_t STORM_last_dense_rows(const STORM_t* s);

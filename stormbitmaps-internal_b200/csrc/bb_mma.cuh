@@ -114,7 +114,7 @@ __device__ __forceinline__ void expand_store(uint8_t* op_base, uint32_t r, uint3
 
 // tiles[t] = (bi, bj): rows [128 bi, +128) x rows [256 bj, +256).
 __global__ void __launch_bounds__(MMA_THREADS, 1)
-bb_mma_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad,
+bb_mma_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, uint64_t pitch,
               const uint2* __restrict__ tiles, uint32_t n_tiles,
               uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags) {
     extern __shared__ __align__(1024) unsigned char mma_smem[];
@@ -164,7 +164,7 @@ bb_mma_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad,
                 trow[q] = task >> 1;
                 thalf[q] = task & 1;
                 const uint64_t grow = trow[q] < MMA_BM ? i0 + trow[q] : j0 + (trow[q] - MMA_BM);
-                src[q] = X + grow * (uint64_t)w_pad + thalf[q];
+                src[q] = X + grow * pitch + thalf[q];
             }
             uint64_t v[3];
 #pragma unroll

@@ -148,7 +148,7 @@ __device__ __forceinline__ bool c2_wait(uint32_t bar, uint32_t parity, C2Ctl* ct
 }
 
 template <bool kW4>
-__device__ __forceinline__ void c2_body(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad,
+__device__ __forceinline__ void c2_body(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, RowLayout lay,
                                         const uint2* __restrict__ tiles, uint32_t n_tiles,
                                         uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags) {
     extern __shared__ __align__(1024) unsigned char c2_smem[];
@@ -200,15 +200,15 @@ __device__ __forceinline__ void c2_body(const uint64_t* __restrict__ X, uint32_t
         for (uint32_t t = cid; ok && t < n_tiles; t += n_clusters, ++tcount) {
             const uint64_t i0 = (uint64_t)tiles[t].x * C2_BM + 128u * rank;
             const uint64_t j0 = (uint64_t)tiles[t].y * C2_BN;
-            const uint64_t* src = X + (is_a ? i0 + prow : j0 + 128u * rank + prow) * (uint64_t)w_pad;
+            const uint64_t* src = X + (is_a ? i0 + prow : j0 + 128u * rank + prow) * lay.pitch;
             // loads run two stages ahead of the expansion
             Row32 v = ldg_row32(src), nv{};
-            if (1 < nk) nv = ldg_row32(src + 4);
+            if (1 < nk) nv = ldg_row32(stage_ptr(src, 1, lay.kstride));
             for (uint32_t kb = 0; kb < nk; ++kb, ++g) {
                 const uint32_t s = g % C2_STAGES;
                 const uint32_t round = g / C2_STAGES;
                 Row32 nnv{};
-                if (kb + 2 < nk) nnv = ldg_row32(src + 4 * (kb + 2));
+                if (kb + 2 < nk) nnv = ldg_row32(stage_ptr(src, kb + 2, lay.kstride));
                 if (!c2_wait<true>(smem_u32(&ctl->empty[s]), (round & 1) ^ 1, ctl, flags, ERR_C2_PROD_EMPTY)) {
                     ok = false;
                     break;
@@ -347,15 +347,15 @@ __device__ __forceinline__ void c2_body(const uint64_t* __restrict__ X, uint32_t
 }
 
 __global__ void __launch_bounds__(C2_THREADS, 1)
-bb_mma_2cta_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, const uint2* __restrict__ tiles,
+bb_mma_2cta_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, RowLayout lay, const uint2* __restrict__ tiles,
                    uint32_t n_tiles, uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags) {
-    c2_body<false>(X, n, w_pad, tiles, n_tiles, out, flags);
+    c2_body<false>(X, n, w_pad, lay, tiles, n_tiles, out, flags);
 }
 
 __global__ void __launch_bounds__(C2_THREADS, 1)
-bb_mma_2cta_long_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, const uint2* __restrict__ tiles,
+bb_mma_2cta_long_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, RowLayout lay, const uint2* __restrict__ tiles,
                         uint32_t n_tiles, uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags) {
-    c2_body<true>(X, n, w_pad, tiles, n_tiles, out, flags);
+    c2_body<true>(X, n, w_pad, lay, tiles, n_tiles, out, flags);
 }
 
 }  // namespace sb200

@@ -158,7 +158,7 @@ struct TsThresh {
 };
 
 template <bool kRowMap, bool kW4, bool kThresh = false>
-__device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad,
+__device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, RowLayout lay,
                                         const uint2* __restrict__ tiles, uint32_t n_tiles,
                                         uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags,
                                         const uint32_t* __restrict__ row_map, uint64_t n_out, uint32_t k_splits,
@@ -213,15 +213,15 @@ __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t
         for (; ok && sched.next(t, kb0, kb1, partial); ++tcount) {
             const uint64_t i0 = (uint64_t)tiles[t].x * TS_BM;
             const uint64_t j0 = (uint64_t)tiles[t].y * TS_BN;
-            const uint64_t* src = X + (is_a ? i0 + prow : j0 + prow) * (uint64_t)w_pad;
+            const uint64_t* src = X + (is_a ? i0 + prow : j0 + prow) * lay.pitch;
             // loads run two stages ahead of the expansion
-            Row32 v = ldg_row32(src + 4 * kb0), nv{};
-            if (kb0 + 1 < kb1) nv = ldg_row32(src + 4 * (kb0 + 1));
+            Row32 v = ldg_row32(stage_ptr(src, kb0, lay.kstride)), nv{};
+            if (kb0 + 1 < kb1) nv = ldg_row32(stage_ptr(src, kb0 + 1, lay.kstride));
             for (uint32_t kb = kb0; kb < kb1; ++kb, ++g) {
                 const uint32_t s = g % TS_STAGES;
                 const uint32_t round = g / TS_STAGES;
                 Row32 nnv{};
-                if (kb + 2 < kb1) nnv = ldg_row32(src + 4 * (kb + 2));
+                if (kb + 2 < kb1) nnv = ldg_row32(stage_ptr(src, kb + 2, lay.kstride));
                 if (!ts_wait(smem_u32(&ctl->empty[s]), (round & 1) ^ 1, ctl, flags, ERR_PROD_EMPTY)) {
                     ok = false;
                     break;
@@ -411,48 +411,48 @@ __device__ __forceinline__ void ts_body(const uint64_t* __restrict__ X, uint32_t
 // > 1 = that many K slices per tile; 0 = stream-K. For any value but 1 the
 // partial counts are added into out with atomics (out zeroed beforehand).
 __global__ void __launch_bounds__(TS_THREADS, 1)
-bb_mma_ts_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, const uint2* __restrict__ tiles,
+bb_mma_ts_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, RowLayout lay, const uint2* __restrict__ tiles,
                  uint32_t n_tiles, uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags, uint32_t k_splits) {
-    ts_body<false, false>(X, n, w_pad, tiles, n_tiles, out, flags, nullptr, 0, k_splits);
+    ts_body<false, false>(X, n, w_pad, lay, tiles, n_tiles, out, flags, nullptr, 0, k_splits);
 }
 
 // Rows of 2^23 .. 2^27 bits: the 4-byte weight cycle keeps D = 8 x count < 2^31.
 __global__ void __launch_bounds__(TS_THREADS, 1)
-bb_mma_ts_long_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, const uint2* __restrict__ tiles,
+bb_mma_ts_long_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, RowLayout lay, const uint2* __restrict__ tiles,
                       uint32_t n_tiles, uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags,
                       uint32_t k_splits) {
-    ts_body<false, true>(X, n, w_pad, tiles, n_tiles, out, flags, nullptr, 0, k_splits);
+    ts_body<false, true>(X, n, w_pad, lay, tiles, n_tiles, out, flags, nullptr, 0, k_splits);
 }
 
 // Same kernel over a gathered subset of rows, writing into the triangle of
 // the full row set through row_map (the kernel layer's dense block).
 __global__ void __launch_bounds__(TS_THREADS, 1)
-bb_mma_ts_rows_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, const uint2* __restrict__ tiles,
+bb_mma_ts_rows_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, RowLayout lay, const uint2* __restrict__ tiles,
                       uint32_t n_tiles, uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags,
                       const uint32_t* __restrict__ row_map, uint64_t n_out, uint32_t k_splits) {
-    ts_body<true, false>(X, n, w_pad, tiles, n_tiles, out, flags, row_map, n_out, k_splits);
+    ts_body<true, false>(X, n, w_pad, lay, tiles, n_tiles, out, flags, row_map, n_out, k_splits);
 }
 
 __global__ void __launch_bounds__(TS_THREADS, 1)
-bb_mma_ts_rows_long_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad,
+bb_mma_ts_rows_long_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, RowLayout lay,
                            const uint2* __restrict__ tiles, uint32_t n_tiles, uint32_t* __restrict__ out,
                            DeviceFlags* __restrict__ flags, const uint32_t* __restrict__ row_map, uint64_t n_out,
                            uint32_t k_splits) {
-    ts_body<true, true>(X, n, w_pad, tiles, n_tiles, out, flags, row_map, n_out, k_splits);
+    ts_body<true, true>(X, n, w_pad, lay, tiles, n_tiles, out, flags, row_map, n_out, k_splits);
 }
 
 // Thresholded form over contiguous rows (whole tiles round robin).
 __global__ void __launch_bounds__(TS_THREADS, 1)
-bb_mma_ts_thresh_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, const uint2* __restrict__ tiles,
+bb_mma_ts_thresh_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, RowLayout lay, const uint2* __restrict__ tiles,
                         uint32_t n_tiles, DeviceFlags* __restrict__ flags, TsThresh th) {
-    ts_body<false, false, true>(X, n, w_pad, tiles, n_tiles, nullptr, flags, nullptr, 0, 1u, th);
+    ts_body<false, false, true>(X, n, w_pad, lay, tiles, n_tiles, nullptr, flags, nullptr, 0, 1u, th);
 }
 
 __global__ void __launch_bounds__(TS_THREADS, 1)
-bb_mma_ts_thresh_long_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad,
+bb_mma_ts_thresh_long_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, RowLayout lay,
                              const uint2* __restrict__ tiles, uint32_t n_tiles, DeviceFlags* __restrict__ flags,
                              TsThresh th) {
-    ts_body<false, true, true>(X, n, w_pad, tiles, n_tiles, nullptr, flags, nullptr, 0, 1u, th);
+    ts_body<false, true, true>(X, n, w_pad, lay, tiles, n_tiles, nullptr, flags, nullptr, 0, 1u, th);
 }
 
 }  // namespace sb200

@@ -62,7 +62,7 @@ __device__ __forceinline__ bool t2_wait(uint32_t bar, uint32_t parity, T2Ctl* ct
 // tiles[t] = (bi, bj): rows [128 bi, +128) x rows [192 bj, +192). Rows at or
 // past n read as zero (no padding needed beyond the rows' own buffer).
 template <bool kW4>
-__device__ __forceinline__ void ts2_body(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad,
+__device__ __forceinline__ void ts2_body(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, RowLayout lay,
                                          const uint2* __restrict__ tiles, uint32_t n_tiles,
                                          uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags,
                                          uint32_t k_splits) {
@@ -112,16 +112,16 @@ __device__ __forceinline__ void ts2_body(const uint64_t* __restrict__ X, uint32_
         while (ok && sched.next(t, kb0, kb1, partial)) {
             const uint64_t row = is_a ? (uint64_t)tiles[t].x * T2_BM + prow : (uint64_t)tiles[t].y * T2_BN + prow;
             const bool live = row < n;
-            const uint64_t* src = X + (live ? row : 0) * (uint64_t)w_pad;
+            const uint64_t* src = X + (live ? row : 0) * lay.pitch;
             // loads run two stages ahead of the expansion
             Row32 v{}, nv{};
-            if (live) v = ldg_row32(src + 4 * kb0);
-            if (live && kb0 + 1 < kb1) nv = ldg_row32(src + 4 * (kb0 + 1));
+            if (live) v = ldg_row32(stage_ptr(src, kb0, lay.kstride));
+            if (live && kb0 + 1 < kb1) nv = ldg_row32(stage_ptr(src, kb0 + 1, lay.kstride));
             for (uint32_t kb = kb0; kb < kb1; ++kb, ++g) {
                 const uint32_t s = g % T2_STAGES;
                 const uint32_t round = g / T2_STAGES;
                 Row32 nnv{};
-                if (live && kb + 2 < kb1) nnv = ldg_row32(src + 4 * (kb + 2));
+                if (live && kb + 2 < kb1) nnv = ldg_row32(stage_ptr(src, kb + 2, lay.kstride));
                 if (!t2_wait(smem_u32(&ctl->empty[s]), (round & 1) ^ 1, ctl, flags, ERR_PROD_EMPTY)) {
                     ok = false;
                     break;
@@ -248,16 +248,16 @@ __device__ __forceinline__ void ts2_body(const uint64_t* __restrict__ X, uint32_
 }
 
 __global__ void __launch_bounds__(T2_THREADS, 1)
-bb_mma_ts2_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, const uint2* __restrict__ tiles,
+bb_mma_ts2_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, RowLayout lay, const uint2* __restrict__ tiles,
                   uint32_t n_tiles, uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags, uint32_t k_splits) {
-    ts2_body<false>(X, n, w_pad, tiles, n_tiles, out, flags, k_splits);
+    ts2_body<false>(X, n, w_pad, lay, tiles, n_tiles, out, flags, k_splits);
 }
 
 __global__ void __launch_bounds__(T2_THREADS, 1)
-bb_mma_ts2_long_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, const uint2* __restrict__ tiles,
+bb_mma_ts2_long_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, RowLayout lay, const uint2* __restrict__ tiles,
                        uint32_t n_tiles, uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags,
                        uint32_t k_splits) {
-    ts2_body<true>(X, n, w_pad, tiles, n_tiles, out, flags, k_splits);
+    ts2_body<true>(X, n, w_pad, lay, tiles, n_tiles, out, flags, k_splits);
 }
 
 }  // namespace sb200

@@ -35,13 +35,13 @@ struct PopcSmem {
 // Stage one K chunk of a 128-row panel into smem, k-major.
 __device__ __forceinline__ void popc_stage(uint64_t (*dst)[POPC_BM + POPC_PAD],
                                            const uint64_t* __restrict__ X, uint64_t row0,
-                                           uint32_t w_pad, uint32_t k0, int tid) {
+                                           uint64_t pitch, uint32_t k0, int tid) {
     // 128 rows x 8 words = 512 uint4 (2 words each); 2 per thread.
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
         const int idx = tid + q * POPC_THREADS;
         const int r = idx >> 2, part = idx & 3;
-        const uint4 v = *reinterpret_cast<const uint4*>(X + (row0 + r) * (uint64_t)w_pad + k0 + 2 * part);
+        const uint4 v = *reinterpret_cast<const uint4*>(X + (row0 + r) * pitch + k0 + 2 * part);
         dst[2 * part][r] = ((uint64_t)v.y << 32) | v.x;
         dst[2 * part + 1][r] = ((uint64_t)v.w << 32) | v.z;
     }
@@ -49,7 +49,7 @@ __device__ __forceinline__ void popc_stage(uint64_t (*dst)[POPC_BM + POPC_PAD],
 
 // tiles[t] = (bi, bj) in units of 128 rows, bi <= bj, covering the triangle.
 __global__ void __launch_bounds__(POPC_THREADS, 1)
-bb_popc_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad,
+bb_popc_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad, uint64_t pitch,
                const uint2* __restrict__ tiles, uint32_t n_tiles,
                uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags) {
     extern __shared__ __align__(16) unsigned char popc_smem[];
@@ -68,15 +68,15 @@ bb_popc_kernel(const uint64_t* __restrict__ X, uint32_t n, uint32_t w_pad,
             for (int b = 0; b < 8; ++b) acc[a][b] = 0;
 
         __syncthreads();   // previous tile's readers are done with both buffers
-        popc_stage(sm.a[0], X, i0, w_pad, 0, tid);
-        popc_stage(sm.b[0], X, j0, w_pad, 0, tid);
+        popc_stage(sm.a[0], X, i0, pitch, 0, tid);
+        popc_stage(sm.b[0], X, j0, pitch, 0, tid);
         __syncthreads();
 
         for (uint32_t kb = 0; kb < nk; ++kb) {
             const int cur = kb & 1;
             if (kb + 1 < nk) {
-                popc_stage(sm.a[cur ^ 1], X, i0, w_pad, (kb + 1) * POPC_BK, tid);
-                popc_stage(sm.b[cur ^ 1], X, j0, w_pad, (kb + 1) * POPC_BK, tid);
+                popc_stage(sm.a[cur ^ 1], X, i0, pitch, (kb + 1) * POPC_BK, tid);
+                popc_stage(sm.b[cur ^ 1], X, j0, pitch, (kb + 1) * POPC_BK, tid);
             }
 #pragma unroll
             for (int k = 0; k < POPC_BK; ++k) {

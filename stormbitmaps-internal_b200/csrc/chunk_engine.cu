@@ -474,29 +474,35 @@ __device__ __forceinline__ void tri_decode(uint64_t n, uint64_t p, uint64_t& i, 
 }
 
 // Expands plain rows into contiguous bitmaps: local row r of X (W words,
-// W = 1024 x chunk slots) is row rows[r]. One CTA per row, a warp per chunk
-// slot: absent chunks become zeros, bitmap chunks are copied, list chunks
-// are set bit by bit in a shared-memory copy of the chunk and written out.
+// W = 1024 x chunk slots, in layout `lay`: chunk slot s of row r -- one
+// 1024-word block -- at X + r x pitch + s x kstride) is row rows[r]. One CTA
+// per row, a warp per chunk slot: absent chunks and padding rows (~0) become
+// zeros, bitmap chunks are copied, list chunks are set bit by bit in a
+// shared-memory copy of the chunk and written out.
 constexpr int EXPAND_WARPS = 4;
 
+// Expanded rows for the tensor cores are stored block-major: chunk slot s of
+// all the panel's rows together, rows PANEL_PITCH words (8 KiB + 64 bytes)
+// apart within it.  A tile's 384 rows at one K stage then lie in about 3 MiB
+// instead of on 384 pages of 2 MiB (rows of 2^24 bits row-major), and no two
+// rows share a pitch that is a power of two.
+constexpr uint64_t PANEL_PITCH = CHUNK_WORDS + 8;
+inline uint64_t panel_row_words(uint64_t W) { return W / CHUNK_WORDS * PANEL_PITCH; }
+
 __global__ void __launch_bounds__(EXPAND_WARPS * 32)
-expand_rows_kernel(ChunkView v, const uint32_t* __restrict__ rows, uint32_t m, uint32_t W,
+expand_rows_kernel(ChunkView v, const uint32_t* __restrict__ rows, uint32_t m, uint32_t W, RowLayout lay,
                    uint64_t* __restrict__ X) {
     __shared__ __align__(16) unsigned long long chunk[EXPAND_WARPS][CHUNK_WORDS];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t slots = W / CHUNK_WORDS;
     for (uint32_t r = blockIdx.x; r < m; r += gridDim.x) {
         const uint32_t row = rows[r];
-        uint4* dst_row = reinterpret_cast<uint4*>(X + (uint64_t)r * W);
-        if (row == ~0u) {   // padding row: zeros
-            for (uint64_t q = threadIdx.x; q < (uint64_t)W / 2; q += blockDim.x) dst_row[q] = make_uint4(0, 0, 0, 0);
-            continue;
-        }
-        const uint64_t c0 = v.row_off[row], c1 = v.row_off[row + 1];
+        uint64_t* dst_row = X + (uint64_t)r * lay.pitch;
+        const uint64_t c0 = row == ~0u ? 0 : v.row_off[row], c1 = row == ~0u ? 0 : v.row_off[row + 1];
         uint64_t pos = c0;
         for (uint32_t s = warp; s < slots; s += EXPAND_WARPS) {
             while (pos < c1 && v.cid[pos] < s) ++pos;   // ids ascend: a forward walk
-            uint4* dst = dst_row + (uint64_t)s * (CHUNK_WORDS / 2);
+            uint4* dst = reinterpret_cast<uint4*>(dst_row + (uint64_t)s * lay.kstride);
             if (pos >= c1 || v.cid[pos] != s) {
                 for (uint32_t q = lane; q < CHUNK_WORDS / 2; q += 32) dst[q] = make_uint4(0, 0, 0, 0);
                 continue;
@@ -1191,7 +1197,7 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
             SB_CUDA(cudaMemGetInfo(&fr, &tot));
             budget = (uint64_t)(0.6 * (double)(fr + d_panel.n * sizeof(uint64_t)));
         }
-        const uint64_t cap_rows = budget / (W * sizeof(uint64_t));
+        const uint64_t cap_rows = budget / (panel_row_words(W) * sizeof(uint64_t));
         P = round_up(ne, 256) <= cap_rows ? round_up(ne, 256) : cap_rows / 2 / 256 * 256;
         if (P == 0) {   // not even two panels fit: the H rows go to the chunk kernel (or the panel)
             if (panel_plan) mrows.insert(mrows.end(), dense.begin(), dense.end());
@@ -1255,7 +1261,10 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         const uint64_t ne2 = emap.size();
         const bool single = P >= round_up(ne2, 256);
         const uint64_t rows_alloc = single ? P : 2 * P;
-        d_panel.reserve(rows_alloc * W);
+        // Block-major panels: chunk slot s of every expanded row together,
+        // rows PANEL_PITCH words apart within it (see panel_row_words).
+        const RowLayout lay{PANEL_PITCH, rows_alloc * PANEL_PITCH};
+        d_panel.reserve(rows_alloc * panel_row_words(W));
         d_map.reserve(rows_alloc);
         d_tiles.reserve((P / 128) * (2 * P / 256 + 1));
         const uint64_t npan = single ? 1 : (ne2 + P - 1) / P;
@@ -1266,14 +1275,14 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
                                     cudaMemcpyHostToDevice, st));
             const uint32_t grid = (uint32_t)std::min<uint64_t>(m, (uint64_t)sms * 16);
             expand_rows_kernel<<<grid, EXPAND_WARPS * 32, 0, st>>>(d.view(), d_map.p + slot, (uint32_t)m,
-                                                                   (uint32_t)W, d_panel.p + slot * W);
+                                                                   (uint32_t)W, lay, d_panel.p + slot * lay.pitch);
             SB_CUDA(cudaGetLastError());
             ++launches;
         };
         auto tensor = [&](uint64_t n_local) {
             if (tl.empty()) return;
             SB_CUDA(cudaMemcpyAsync(d_tiles.p, tl.data(), tl.size() * sizeof(uint2), cudaMemcpyHostToDevice, st));
-            launch_ts_rows(d_panel.p, (uint32_t)n_local, (uint32_t)W, d_tiles.p, (uint32_t)tl.size(), d_out,
+            launch_ts_rows(d_panel.p, (uint32_t)n_local, (uint32_t)W, lay, d_tiles.p, (uint32_t)tl.size(), d_out,
                            d_flags.p, d_map.p, n, st, /*out_zeroed=*/true);
             ++launches;
         };
@@ -1381,7 +1390,7 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
             for (uint32_t t = 0; t < PANEL_ROWS; ++t) bmap[t] = t < prows ? h_perm[pw0 + b0 + t] : ~0u;
             SB_CUDA(cudaMemcpyAsync(d_pmap.p, bmap.data(), PANEL_ROWS * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
             expand_rows_kernel<<<(uint32_t)std::min<uint64_t>(PANEL_ROWS, (uint64_t)sms * 16), EXPAND_WARPS * 32, 0,
-                                 st>>>(d.view(), d_pmap.p, PANEL_ROWS, (uint32_t)W, d_pX.p);
+                                 st>>>(d.view(), d_pmap.p, PANEL_ROWS, (uint32_t)W, row_major(W), d_pX.p);
             panel_transpose_kernel<<<(uint32_t)(W / PANEL_T_WORDS), 1024, PANEL_T_SMEM, st>>>(d_pX.p, W, d_DT.p);
             SB_CUDA(cudaMemsetAsync(d_ctr.p, 0, sizeof(unsigned long long), st));
             const uint32_t ni = (uint32_t)items.size();

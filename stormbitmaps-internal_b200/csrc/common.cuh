@@ -127,6 +127,18 @@ inline void smem_attr_once(K* kernel, int bytes, std::atomic<uint64_t>& done) {
     done.fetch_or(bit);
 }
 
+// Where the rows of an all-pairs launch are in device memory: word k of row
+// r at X[r * pitch + (k >> 10) * kstride + (k & 1023)].  Row-major rows have
+// kstride = 1024 (a row's 1024-word blocks follow each other); block-major
+// panels keep block b of every row together (kstride = the words one block
+// of all the panel's rows takes), so that the rows a tile reads at one K
+// stage lie within a few pages instead of one page per row.
+struct RowLayout {
+    uint64_t pitch = 0;
+    uint64_t kstride = 1024;
+};
+inline RowLayout row_major(uint64_t pitch) { return RowLayout{pitch, 1024}; }
+
 }  // namespace sb200
 
 // ---------------------------------------------------------------------------
@@ -134,6 +146,12 @@ inline void smem_attr_once(K* kernel, int bytes, std::atomic<uint64_t>& done) {
 // ---------------------------------------------------------------------------
 #ifdef __CUDACC__
 namespace sb200 {
+
+// The first word of 256-bit stage kb (4 words, never across a 1024-word
+// block) of the row that starts at `row`.
+__device__ __forceinline__ const uint64_t* stage_ptr(const uint64_t* row, uint32_t kb, uint64_t kstride) {
+    return row + (uint64_t)(kb >> 8) * kstride + ((kb & 255u) << 2);
+}
 
 // Packed upper-triangle index, i <= j.
 __device__ __forceinline__ uint64_t tri_index(uint64_t n, uint64_t i, uint64_t j) {

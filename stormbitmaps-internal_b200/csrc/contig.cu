@@ -8,8 +8,10 @@
 // CPU speed trick with the same result, so here every pair goes through the
 // bitmap x bitmap tile kernels.
 //
-// HBM layout: [n_pad][w_pad] u64, w_pad = roundup(ceil(len/64), 8),
-// n_pad = roundup(n, 256), zero padded.  Rows added with STORM_contig_add are
+// HBM layout: [n_pad][pitch] u64, w_pad = roundup(ceil(len/64), 8) words of
+// each row read by the kernels, pitch = dense_pitch(w_pad) (64 bytes more
+// when w_pad words are a multiple of 4 KiB), n_pad = roundup(n, 256), zero
+// padded.  Rows added with STORM_contig_add are
 // staged in host memory and flushed in one copy at the next device call;
 // STORM_contig_add_bitmaps copies straight into HBM.
 #include <algorithm>
@@ -22,7 +24,8 @@
 struct STORM_contiguous_s {
     uint64_t vector_length = 0;
     uint32_t n_words = 0;   // ceil(len / 64)
-    uint32_t w_pad = 0;     // HBM row pitch in words
+    uint32_t w_pad = 0;     // words of a row the kernels read
+    uint64_t pitch = 0;     // HBM row pitch in words, dense_pitch(w_pad)
     uint64_t n_rows = 0;    // rows on the device + staged
     uint64_t dev_rows = 0;  // rows already in HBM
     uint64_t cap_rows = 0;  // HBM capacity in rows
@@ -46,7 +49,7 @@ struct STORM_contiguous_s {
 
 namespace sb200 {
 
-__global__ void mask_tail_kernel(uint64_t* last_word, uint64_t rows, uint32_t pitch, uint64_t keep) {
+__global__ void mask_tail_kernel(uint64_t* last_word, uint64_t rows, uint64_t pitch, uint64_t keep) {
     for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < rows; r += (uint64_t)gridDim.x * blockDim.x)
         last_word[r * pitch] &= keep;
 }
@@ -64,20 +67,20 @@ static void contig_grow(STORM_contiguous_t* c, uint64_t rows) {
     uint64_t cap = std::max<uint64_t>(need, c->cap_rows * 2);
     cudaStream_t st = contig_stream(c);
     uint64_t* np = nullptr;
-    cudaError_t e = cudaMalloc((void**)&np, cap * c->w_pad * sizeof(uint64_t));
+    cudaError_t e = cudaMalloc((void**)&np, cap * c->pitch * sizeof(uint64_t));
     if (e != cudaSuccess && cap > need) {
         cudaGetLastError();
         cap = need;
-        e = cudaMalloc((void**)&np, cap * c->w_pad * sizeof(uint64_t));
+        e = cudaMalloc((void**)&np, cap * c->pitch * sizeof(uint64_t));
     }
     SB_CUDA(e);
     if (c->dev_rows)
-        SB_CUDA(cudaMemcpyAsync(np, c->d_rows.p, c->dev_rows * c->w_pad * sizeof(uint64_t),
+        SB_CUDA(cudaMemcpyAsync(np, c->d_rows.p, c->dev_rows * c->pitch * sizeof(uint64_t),
                                 cudaMemcpyDeviceToDevice, st));
     SB_CUDA(cudaStreamSynchronize(st));
     c->d_rows.release();
     c->d_rows.p = np;
-    c->d_rows.n = cap * c->w_pad;
+    c->d_rows.n = cap * c->pitch;
     c->cap_rows = cap;
 }
 
@@ -86,10 +89,10 @@ static void contig_append_device(STORM_contiguous_t* c, const uint64_t* host, ui
     if (rows == 0) return;
     contig_grow(c, c->dev_rows + rows);
     cudaStream_t st = contig_stream(c);
-    uint64_t* dst = c->d_rows.p + c->dev_rows * c->w_pad;
+    uint64_t* dst = c->d_rows.p + c->dev_rows * c->pitch;
     if (wpr != c->w_pad)
-        SB_CUDA(cudaMemsetAsync(dst, 0, rows * c->w_pad * sizeof(uint64_t), st));
-    SB_CUDA(cudaMemcpy2DAsync(dst, c->w_pad * sizeof(uint64_t), host, wpr * sizeof(uint64_t),
+        SB_CUDA(cudaMemsetAsync(dst, 0, rows * c->pitch * sizeof(uint64_t), st));
+    SB_CUDA(cudaMemcpy2DAsync(dst, c->pitch * sizeof(uint64_t), host, wpr * sizeof(uint64_t),
                               wpr * sizeof(uint64_t), rows, cudaMemcpyDefault, st));
     SB_CUDA(cudaStreamSynchronize(st));
     c->dev_rows += rows;
@@ -106,8 +109,8 @@ static void contig_flush(STORM_contiguous_t* c) {
     const uint64_t n_pad = round_up(std::max<uint64_t>(c->dev_rows, 1), 256);
     cudaStream_t st = contig_stream(c);
     if (n_pad > c->dev_rows)
-        SB_CUDA(cudaMemsetAsync(c->d_rows.p + c->dev_rows * c->w_pad, 0,
-                                (n_pad - c->dev_rows) * c->w_pad * sizeof(uint64_t), st));
+        SB_CUDA(cudaMemsetAsync(c->d_rows.p + c->dev_rows * c->pitch, 0,
+                                (n_pad - c->dev_rows) * c->pitch * sizeof(uint64_t), st));
 }
 
 // Sum over i < j; packed triangle into d_out when non-null.
@@ -142,6 +145,7 @@ STORM_contiguous_t* STORM_contig_new(size_t vector_length) {
         c->vector_length = vector_length;
         c->n_words = (uint32_t)((vector_length + 63) / 64);
         c->w_pad = (uint32_t)round_up(c->n_words ? c->n_words : 1, 8);
+        c->pitch = dense_pitch(c->w_pad);
         set_last_status(0);
         return c;
     } catch (...) {
@@ -201,8 +205,8 @@ int STORM_contig_add_bitmaps(STORM_contiguous_t* c, const uint64_t* words, uint3
         if (on_device && c->vector_length % 64 && n_rows) {
             // Device input is not inspected on the host: clear bits past the row end.
             const uint32_t grid = (uint32_t)std::min<uint64_t>((n_rows + 255) / 256, 65535);
-            mask_tail_kernel<<<grid, 256, 0, contig_stream(c)>>>(c->d_rows.p + first * c->w_pad + (c->n_words - 1),
-                                                                 n_rows, c->w_pad,
+            mask_tail_kernel<<<grid, 256, 0, contig_stream(c)>>>(c->d_rows.p + first * c->pitch + (c->n_words - 1),
+                                                                 n_rows, c->pitch,
                                                                  ~0ull >> (64 - c->vector_length % 64));
             SB_CUDA(cudaGetLastError());
             SB_CUDA(cudaStreamSynchronize(contig_stream(c)));

@@ -133,6 +133,7 @@ void DenseEngine::launch(int kind, const uint64_t* dX, uint32_t n, uint32_t w_pa
                          uint32_t* d_out, cudaStream_t st) {
     const int sms = require_device();
     if (count == 0) return;
+    const RowLayout lay = row_major(dense_pitch(w_pad));
     if (kind == STORM_B200_KERNEL_MMA) {
         static std::atomic<uint64_t> done_a{0}, done_b{0};
         smem_attr_once(bb_mma_ts_kernel, (int)TS_SMEM_BYTES, done_a);
@@ -144,10 +145,10 @@ void DenseEngine::launch(int kind, const uint64_t* dX, uint32_t n, uint32_t w_pa
         if (ks != 1 && d_out) zero_stream_k_rows(d_out, n, grid, st);
         const uint32_t smem = (uint64_t)w_pad * 64 <= TS_COALESCE_MAX_BITS ? TS_SMEM_BYTES : TS_SMEM_BYTES_LEAN;
         if ((uint64_t)w_pad * 64 <= MMA_MAX_BITS)
-            bb_mma_ts_kernel<<<grid, TS_THREADS, smem, st>>>(dX, n, w_pad, d_tiles.p + t0, count, d_out, d_flags.p,
+            bb_mma_ts_kernel<<<grid, TS_THREADS, smem, st>>>(dX, n, w_pad, lay, d_tiles.p + t0, count, d_out, d_flags.p,
                                                              ks);
         else
-            bb_mma_ts_long_kernel<<<grid, TS_THREADS, smem, st>>>(dX, n, w_pad, d_tiles.p + t0, count, d_out,
+            bb_mma_ts_long_kernel<<<grid, TS_THREADS, smem, st>>>(dX, n, w_pad, lay, d_tiles.p + t0, count, d_out,
                                                                   d_flags.p, ks);
     } else if (kind == STORM_B200_KERNEL_MMA_DB) {
         static std::atomic<uint64_t> done_a{0}, done_b{0};
@@ -157,10 +158,10 @@ void DenseEngine::launch(int kind, const uint64_t* dX, uint32_t n, uint32_t w_pa
         const uint32_t ks = (t0 == 0 && count == n_tiles) ? ts_schedule(count, sms, w_pad, grid, schedule) : 1;
         if (ks != 1 && d_out) zero_stream_k_rows(d_out, n, grid, st);
         if ((uint64_t)w_pad * 64 <= MMA_MAX_BITS)
-            bb_mma_ts2_kernel<<<grid, T2_THREADS, T2_SMEM_BYTES, st>>>(dX, n, w_pad, d_tiles.p + t0, count, d_out,
+            bb_mma_ts2_kernel<<<grid, T2_THREADS, T2_SMEM_BYTES, st>>>(dX, n, w_pad, lay, d_tiles.p + t0, count, d_out,
                                                                       d_flags.p, ks);
         else
-            bb_mma_ts2_long_kernel<<<grid, T2_THREADS, T2_SMEM_BYTES, st>>>(dX, n, w_pad, d_tiles.p + t0, count,
+            bb_mma_ts2_long_kernel<<<grid, T2_THREADS, T2_SMEM_BYTES, st>>>(dX, n, w_pad, lay, d_tiles.p + t0, count,
                                                                            d_out, d_flags.p, ks);
     } else if (kind == STORM_B200_KERNEL_MMA_2CTA) {
         // CTA pairs (clusters of 2), one per two SMs, whole tiles round robin
@@ -184,14 +185,14 @@ void DenseEngine::launch(int kind, const uint64_t* dX, uint32_t n, uint32_t w_pa
         cfg.numAttrs = 1;
         const uint2* tl = d_tiles.p + t0;
         if ((uint64_t)w_pad * 64 <= MMA_MAX_BITS)
-            SB_CUDA(cudaLaunchKernelEx(&cfg, bb_mma_2cta_kernel, dX, n, w_pad, tl, count, d_out, d_flags.p));
+            SB_CUDA(cudaLaunchKernelEx(&cfg, bb_mma_2cta_kernel, dX, n, w_pad, lay, tl, count, d_out, d_flags.p));
         else
-            SB_CUDA(cudaLaunchKernelEx(&cfg, bb_mma_2cta_long_kernel, dX, n, w_pad, tl, count, d_out, d_flags.p));
+            SB_CUDA(cudaLaunchKernelEx(&cfg, bb_mma_2cta_long_kernel, dX, n, w_pad, lay, tl, count, d_out, d_flags.p));
     } else if (kind == STORM_B200_KERNEL_MMA_SS) {
         static std::atomic<uint64_t> done{0};
         smem_attr_once(bb_mma_kernel, (int)MMA_SMEM_BYTES, done);
         const uint32_t grid = count < (uint32_t)sms ? count : (uint32_t)sms;
-        bb_mma_kernel<<<grid, MMA_THREADS, MMA_SMEM_BYTES, st>>>(dX, n, w_pad, d_tiles.p + t0, count, d_out,
+        bb_mma_kernel<<<grid, MMA_THREADS, MMA_SMEM_BYTES, st>>>(dX, n, w_pad, lay.pitch, d_tiles.p + t0, count, d_out,
                                                                   d_flags.p);
     } else {
         const size_t smem = sizeof(PopcSmem);
@@ -199,7 +200,7 @@ void DenseEngine::launch(int kind, const uint64_t* dX, uint32_t n, uint32_t w_pa
         smem_attr_once(bb_popc_kernel, (int)smem, done);
         const uint32_t cap = (uint32_t)sms * 2;
         const uint32_t grid = count < cap ? count : cap;
-        bb_popc_kernel<<<grid, POPC_THREADS, smem, st>>>(dX, n, w_pad, d_tiles.p + t0, count, d_out, d_flags.p);
+        bb_popc_kernel<<<grid, POPC_THREADS, smem, st>>>(dX, n, w_pad, lay.pitch, d_tiles.p + t0, count, d_out, d_flags.p);
     }
     SB_CUDA(cudaGetLastError());
 }
@@ -285,11 +286,11 @@ uint64_t DenseEngine::run_host_to_host(uint64_t* dX, uint64_t n, uint32_t w_pad,
     const int kind = prepare(n, row_bits, kernel_pref, st);
     // What the copies do not cover reads as zero: the row pitch's padding
     // words and the rows [n, n_pad) that whole 128 x 256 tiles read.
-    const uint64_t n_pad = round_up(n, 256);
+    const uint64_t n_pad = round_up(n, 256), pitch = dense_pitch(w_pad);
     if (host_wpr != w_pad)
-        SB_CUDA(cudaMemsetAsync(dX, 0, n_pad * w_pad * sizeof(uint64_t), h2d_st));
+        SB_CUDA(cudaMemsetAsync(dX, 0, n_pad * pitch * sizeof(uint64_t), h2d_st));
     else if (n_pad > n)
-        SB_CUDA(cudaMemsetAsync(dX + n * w_pad, 0, (n_pad - n) * w_pad * sizeof(uint64_t), h2d_st));
+        SB_CUDA(cudaMemsetAsync(dX + n * pitch, 0, (n_pad - n) * pitch * sizeof(uint64_t), h2d_st));
     const uint64_t chunk_rows = round_up(std::max<uint64_t>(1, (n + 31) / 32), 128);
     const uint64_t chunks = (n + chunk_rows - 1) / chunk_rows;
     while (h2d_ev.size() < chunks) {
@@ -301,7 +302,7 @@ uint64_t DenseEngine::run_host_to_host(uint64_t* dX, uint64_t n, uint32_t w_pad,
     // [c x chunk_rows, n) (and the zeroing) as resident.
     for (uint64_t c = chunks; c-- > 0;) {
         const uint64_t r0 = c * chunk_rows, r1 = std::min(n, r0 + chunk_rows);
-        SB_CUDA(cudaMemcpy2DAsync(dX + r0 * w_pad, (size_t)w_pad * sizeof(uint64_t), host_rows + r0 * host_wpr,
+        SB_CUDA(cudaMemcpy2DAsync(dX + r0 * pitch, (size_t)pitch * sizeof(uint64_t), host_rows + r0 * host_wpr,
                                   (size_t)host_wpr * sizeof(uint64_t), (size_t)host_wpr * sizeof(uint64_t),
                                   r1 - r0, cudaMemcpyHostToDevice, h2d_st));
         SB_CUDA(cudaEventRecord(h2d_ev[c], h2d_st));
@@ -474,7 +475,8 @@ extern "C" int STORM_contig_pairw_intersect_matrix_noalloc(const uint64_t* d_row
     // TS_COALESCE_MAX_BITS stage their counts through shared memory.
     const uint32_t smem =
         (uint64_t)row_pitch_words * 64 <= TS_COALESCE_MAX_BITS ? TS_SMEM_BYTES : TS_SMEM_BYTES_LEAN;
-    bb_mma_ts_kernel<<<grid, TS_THREADS, smem, st>>>(d_rows, (uint32_t)n_rows, row_pitch_words, scratch->tiles,
+    bb_mma_ts_kernel<<<grid, TS_THREADS, smem, st>>>(d_rows, (uint32_t)n_rows, row_pitch_words,
+                                                      row_major(row_pitch_words), scratch->tiles,
                                                       (uint32_t)n_tiles, d_out, &scratch->flags, 1u);
     if (cudaGetLastError() != cudaSuccess) {
         cudaStreamSynchronize(st);   // nothing already queued may still write d_out after the return
@@ -559,13 +561,13 @@ extern "C" int STORM_b200_wait_selftest(uint32_t limit_us) {
 namespace sb200 {
 
 // |Xi| of each row: warp per row.
-__global__ void row_popcount_kernel(const uint64_t* __restrict__ X, uint64_t n, uint32_t w_pad,
+__global__ void row_popcount_kernel(const uint64_t* __restrict__ X, uint64_t n, uint32_t w_pad, uint64_t pitch,
                                     uint32_t* __restrict__ card) {
     const int lane = threadIdx.x & 31;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += nw) {
         uint32_t c = 0;
-        for (uint32_t w = lane; w < w_pad; w += 32) c += __popcll(X[r * w_pad + w]);
+        for (uint32_t w = lane; w < w_pad; w += 32) c += __popcll(X[r * pitch + w]);
         c = warp_sum_u32(c);
         if (lane == 0) card[r] = c;
     }
@@ -681,15 +683,16 @@ uint64_t DenseEngine::run_threshold(const uint64_t* dX, uint64_t n, uint32_t w_p
         smem_attr_once(bb_mma_ts_thresh_long_kernel, (int)TS_SMEM_BYTES, done_b);
         SB_CUDA(cudaMemsetAsync(d_found.p, 0, sizeof(unsigned long long), st));
         row_popcount_kernel<<<(uint32_t)std::min<uint64_t>((n + 7) / 8, (uint64_t)sms * 16), 256, 0, st>>>(
-            dX, n, w_pad, d_card.p);
+            dX, n, w_pad, dense_pitch(w_pad), d_card.p);
         const TsThresh th{d_card.p, t, d_pairs, d_cnts, (unsigned long long)cap, d_found.p};
         const uint32_t grid = n_tiles < (uint32_t)sms ? n_tiles : (uint32_t)sms;
+        const RowLayout lay = row_major(dense_pitch(w_pad));
         if ((uint64_t)w_pad * 64 <= MMA_MAX_BITS)
-            bb_mma_ts_thresh_kernel<<<grid, TS_THREADS, TS_SMEM_BYTES_LEAN, st>>>(dX, (uint32_t)n, w_pad, d_tiles.p,
+            bb_mma_ts_thresh_kernel<<<grid, TS_THREADS, TS_SMEM_BYTES_LEAN, st>>>(dX, (uint32_t)n, w_pad, lay, d_tiles.p,
                                                                                    n_tiles, d_flags.p, th);
         else
             bb_mma_ts_thresh_long_kernel<<<grid, TS_THREADS, TS_SMEM_BYTES_LEAN, st>>>(
-                dX, (uint32_t)n, w_pad, d_tiles.p, n_tiles, d_flags.p, th);
+                dX, (uint32_t)n, w_pad, lay, d_tiles.p, n_tiles, d_flags.p, th);
         SB_CUDA(cudaGetLastError());
         unsigned long long h = 0;
         SB_CUDA(cudaMemcpyAsync(&h, d_found.p, sizeof(h), cudaMemcpyDeviceToHost, st));
@@ -723,8 +726,8 @@ namespace sb200 {
 
 void build_mma_tiles(std::vector<uint2>& t, uint64_t n) { build_tiles(t, n, STORM_B200_KERNEL_MMA); }
 
-void launch_ts_rows(const uint64_t* X, uint32_t n, uint32_t w_pad, const uint2* tiles, uint32_t n_tiles,
-                    uint32_t* out, DeviceFlags* flags, const uint32_t* row_map, uint64_t n_out, cudaStream_t st,
+void launch_ts_rows(const uint64_t* X, uint32_t n, uint32_t w_pad, RowLayout lay, const uint2* tiles,
+                    uint32_t n_tiles, uint32_t* out, DeviceFlags* flags, const uint32_t* row_map, uint64_t n_out, cudaStream_t st,
                     bool out_zeroed) {
     const int sms = require_device();
     if (n_tiles == 0) return;
@@ -739,10 +742,10 @@ void launch_ts_rows(const uint64_t* X, uint32_t n, uint32_t w_pad, const uint2* 
     if (ks != 1 && out && !out_zeroed) SB_CUDA(cudaMemsetAsync(out, 0, tri_size(n_out) * sizeof(uint32_t), st));
     const uint32_t smem = (uint64_t)w_pad * 64 <= TS_COALESCE_MAX_BITS ? TS_SMEM_BYTES : TS_SMEM_BYTES_LEAN;
     if ((uint64_t)w_pad * 64 <= MMA_MAX_BITS)
-        bb_mma_ts_rows_kernel<<<grid, TS_THREADS, smem, st>>>(X, n, w_pad, tiles, n_tiles, out, flags, row_map, n_out,
+        bb_mma_ts_rows_kernel<<<grid, TS_THREADS, smem, st>>>(X, n, w_pad, lay, tiles, n_tiles, out, flags, row_map, n_out,
                                                               ks);
     else
-        bb_mma_ts_rows_long_kernel<<<grid, TS_THREADS, smem, st>>>(X, n, w_pad, tiles, n_tiles, out, flags, row_map,
+        bb_mma_ts_rows_long_kernel<<<grid, TS_THREADS, smem, st>>>(X, n, w_pad, lay, tiles, n_tiles, out, flags, row_map,
                                                                    n_out, ks);
     SB_CUDA(cudaGetLastError());
 }

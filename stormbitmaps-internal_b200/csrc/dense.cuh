@@ -8,8 +8,18 @@
 
 namespace sb200 {
 
-// Device rows: X is [n_pad][w_pad] u64, zero padded, n_pad % 256 == 0 and
-// w_pad % 8 == 0.
+// Row pitch (words) of the dense engine's device rows of w_pad words: a
+// pitch that is a multiple of 4 KiB gets 64 bytes more.  With a power-of-two
+// pitch the same K stage of the 384 rows a tile reads falls on the same
+// memory partitions, and their loads queue there; measured on B200 with the
+// tensor-core kernel (ms, same rows): 65536 x 2^18 bits 368.6 -> 353.8,
+// 16384 x 2^18 23.7 -> 21.6, 4096 x 2^16 0.484 -> 0.468, 4096 x 2^23 48.2
+// -> 46.4.  (256 bytes more was slower than none at 2^18: 395.1.)
+inline uint64_t dense_pitch(uint32_t w_pad) { return w_pad % 512 == 0 ? (uint64_t)w_pad + 8 : (uint64_t)w_pad; }
+
+// Device rows: X is [n_pad][dense_pitch(w_pad)] u64, of which each row's
+// first w_pad words are read (zero past the row's bits), n_pad % 256 == 0
+// and w_pad % 8 == 0.
 struct DenseEngine {
     int schedule = STORM_B200_SCHED_AUTO;   // tensor-core work schedule
     DevBuf<uint2> d_tiles;
@@ -38,7 +48,7 @@ struct DenseEngine {
                          uint32_t* host_out, int kernel_pref, cudaStream_t st, cudaStream_t copy_st);
 
     // run_to_host with the rows also coming from the host: host_rows (n x
-    // host_wpr words, host memory) are copied into dX ([n_pad][w_pad],
+    // host_wpr words, host memory) are copied into dX ([n_pad][pitch],
     // zero padded here) on h2d_st, last rows first, and each panel waits
     // only for the rows its tiles read, so the upload, the tiles and the
     // copy back overlap.
@@ -88,13 +98,14 @@ constexpr uint64_t TC_MAX_ROW_BITS = 1ull << 27;
 // ... and the shared-memory form (8-byte weight cycle only).
 constexpr uint64_t TC_SS_MAX_ROW_BITS = 1ull << 23;
 
-// Tensor-core kernel over n gathered rows X ([>= roundup(n, 256)][w_pad]);
-// count (i, j) lands at the packed index of (row_map[i], row_map[j]) in a
+// Tensor-core kernel over n gathered rows X (>= roundup(n, 256) rows of
+// w_pad words in layout `lay`); count (i, j) lands at the packed index of
+// (row_map[i], row_map[j]) in a
 // triangle of n_out rows; the sum over i < j accumulates into flags->sum.
 // With few tiles the K range is split and partial counts are added into
 // out: out_zeroed says the caller has zeroed the triangle already, else it
 // is zeroed here when a split is taken.  Asynchronous on st.
-void launch_ts_rows(const uint64_t* X, uint32_t n, uint32_t w_pad, const uint2* tiles, uint32_t n_tiles,
+void launch_ts_rows(const uint64_t* X, uint32_t n, uint32_t w_pad, RowLayout lay, const uint2* tiles, uint32_t n_tiles,
                     uint32_t* out, DeviceFlags* flags, const uint32_t* row_map, uint64_t n_out, cudaStream_t st,
                     bool out_zeroed = false);
 

@@ -68,11 +68,11 @@ __global__ void rect_sum_kernel(const uint32_t* __restrict__ tri, uint64_t n, ui
 static void upload_dense(DevBuf<uint64_t>& d, const uint64_t* rows, uint64_t n, uint32_t n_ints, uint32_t& w_pad,
                          cudaStream_t st) {
     w_pad = (uint32_t)round_up(n_ints ? n_ints : 1, 8);
-    const uint64_t n_pad = round_up(n ? n : 1, 256);
-    d.reserve(n_pad * w_pad);
-    SB_CUDA(cudaMemsetAsync(d.p, 0, n_pad * w_pad * sizeof(uint64_t), st));
+    const uint64_t n_pad = round_up(n ? n : 1, 256), pitch = dense_pitch(w_pad);
+    d.reserve(n_pad * pitch);
+    SB_CUDA(cudaMemsetAsync(d.p, 0, n_pad * pitch * sizeof(uint64_t), st));
     if (n && n_ints)
-        SB_CUDA(cudaMemcpy2DAsync(d.p, w_pad * sizeof(uint64_t), rows, n_ints * sizeof(uint64_t),
+        SB_CUDA(cudaMemcpy2DAsync(d.p, pitch * sizeof(uint64_t), rows, n_ints * sizeof(uint64_t),
                                   n_ints * sizeof(uint64_t), n, cudaMemcpyHostToDevice, st));
 }
 

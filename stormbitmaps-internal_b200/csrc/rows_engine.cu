@@ -223,12 +223,12 @@ struct PairCtx {
 // Gather the bitmaps of the dense block (sorted positions [from, n)) into a
 // zero-padded [nd_pad][w_pad] matrix for the tensor-core kernel.
 __global__ void gather_dense_kernel(RowsView v, const uint32_t* __restrict__ order, uint32_t from, uint32_t nd,
-                                    uint32_t nd_pad, uint32_t w_pad, uint64_t* __restrict__ X,
+                                    uint32_t nd_pad, uint64_t pitch, uint64_t* __restrict__ X,
                                     uint32_t* __restrict__ row_map) {
-    const uint64_t total = (uint64_t)nd_pad * w_pad;
+    const uint64_t total = (uint64_t)nd_pad * pitch;
     for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < total;
          e += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t r = (uint32_t)(e / w_pad), w = (uint32_t)(e % w_pad);
+        const uint32_t r = (uint32_t)(e / pitch), w = (uint32_t)(e % pitch);
         uint64_t x = 0;
         if (r < nd) {
             const uint32_t row = order[from + r];
@@ -580,8 +580,9 @@ static void rows_run(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell,
     const uint32_t nd = n - D;
     const uint32_t w_pad_d = (uint32_t)round_up(((uint64_t)r->universe + 63) / 64, 8);
     const uint32_t nd_pad = (uint32_t)round_up(nd ? nd : 1, 256);
+    const uint64_t pitch_d = dense_pitch(w_pad_d);
     if (nd) {
-        r->d_dense.reserve((uint64_t)nd_pad * w_pad_d);
+        r->d_dense.reserve((uint64_t)nd_pad * pitch_d);
         r->d_dmap.reserve(nd);
         r->d_dflags.reserve(1);
         if (r->dtiles_n != nd) {
@@ -609,11 +610,11 @@ static void rows_run(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell,
     auto dense_phase = [&]() {
         if (!nd) return;
         SB_CUDA(cudaMemsetAsync(r->d_dflags.p, 0, sizeof(DeviceFlags), st));
-        const uint64_t total = (uint64_t)nd_pad * w_pad_d;
+        const uint64_t total = (uint64_t)nd_pad * pitch_d;
         const uint32_t gg = (uint32_t)std::min<uint64_t>((total + 255) / 256, (uint64_t)sms * 32);
-        gather_dense_kernel<<<gg, 256, 0, st>>>(c.v, c.order, D, nd, nd_pad, w_pad_d, r->d_dense.p, r->d_dmap.p);
-        launch_ts_rows(r->d_dense.p, nd, w_pad_d, r->d_dtiles.p, r->n_dtiles, d_out, r->d_dflags.p, r->d_dmap.p, n,
-                       st);
+        gather_dense_kernel<<<gg, 256, 0, st>>>(c.v, c.order, D, nd, nd_pad, pitch_d, r->d_dense.p, r->d_dmap.p);
+        launch_ts_rows(r->d_dense.p, nd, w_pad_d, row_major(pitch_d), r->d_dtiles.p, r->n_dtiles, d_out,
+                       r->d_dflags.p, r->d_dmap.p, n, st);
     };
     auto phases_1_2 = [&]() {
         SB_CUDA(cudaMemsetAsync(r->d_stats.p, 0, sizeof(RowsStatsDev), st));

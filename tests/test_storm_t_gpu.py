@@ -161,7 +161,7 @@ def test_tensor_dense_block_in_panels(sb):
     sets = _dense_corpus(700, 60, universe, 500, 4000, 92)
     s = build_storm(sb, sets)
     s.set_sparse_postings(0)                # the dense block alone (postings tested below)
-    row_bytes = universe // 8
+    row_bytes = universe // 65536 * 8256          # an expanded row: its 8 KiB chunk slots 64 bytes apart
     s.set_dense_block(1.0 / 16384, 2 * 256 * row_bytes + 4096)
     vals, offs = gen.to_csr(sets)
     want, ws = ol.sets_matrix(vals, offs)
@@ -283,7 +283,7 @@ def test_tensor_rows_with_postings_in_panels(sb):
     sets += [gen.uniform_set(g, int(g.integers(5, 50)), universe) for _ in range(300)]
     sets = [sets[k] for k in g.permutation(len(sets))]
     s = build_storm(sb, sets)
-    s.set_dense_block(1.0 / 1024, 2 * 256 * (universe // 8) + 4096)
+    s.set_dense_block(1.0 / 1024, 2 * 256 * (universe // 65536 * 8256) + 4096)
     vals, offs = gen.to_csr(sets)
     want, ws = ol.sets_matrix(vals, offs)
     for mode in (2, 3):
