@@ -347,7 +347,7 @@ def zipf_sets_gpu(n, universe, s, lo, hi, seed, device):
     return out
 
 
-def mixed_density_forms(sb, device, n=4096, universe=1 << 20, tile=64):
+def mixed_density_forms(sb, device, n=4096, universe=1 << 20, tile=64, samples=1024):
     """Config-3-shaped corpus (Zipf(1.1) cardinalities, clipped like the full
     configuration relative to the universe: [16, universe/4]) through the kernel
     layer: plain per-tile GPU launches with the reference's cost model, the
@@ -379,7 +379,7 @@ def mixed_density_forms(sb, device, n=4096, universe=1 << 20, tile=64):
     forms["plain_per_tile_default_model"] = {"pairs_per_s": pairs / (ns0 * 1e-9), "ms": ns0 * 1e-6,
                                              "launches": st0["launches"], "cell_pairs": st0["cell_pairs"]}
     t0 = time.perf_counter()
-    sel = r.train_selector(tile=tile, samples=1024, epochs=400, seed=7)   # also calibrates the cost model
+    sel = r.train_selector(tile=tile, samples=samples, epochs=400, seed=7)   # also calibrates the cost model
     out["train_s"] = round(time.perf_counter() - t0, 2)
     out["selector"] = {k: (round(v, 4) if isinstance(v, float) else v) for k, v in sel.items()}
     out["selector"].update({k: round(v, 4) for k, v in r.last_training().items()})
@@ -1063,7 +1063,7 @@ def autotune_config1(sb, device):
             "kept": names[cand.index((k, sched))] if (k, sched) in cand else f"kernel {k} schedule {sched}"}
 
 
-def config45_forms(device):
+def config45_forms(device, full_sweep=False):
     """Config-4-shaped run-clustered rows and the config-5b density sweep
     (N = 20000 up to density 1e-3, fewer rows above), each with the learned
     selector's held-out regret against the measured-best cell, beside the
@@ -1078,10 +1078,14 @@ def config45_forms(device):
     sweep = {}
     # N = 20000 (config 5b's row count) where the kernel layer's host packing
     # of every representation stays within seconds; fewer rows beyond
-    for d, n in ((1e-6, 20000), (1e-5, 20000), (1e-4, 20000), (1e-3, 20000), (1e-2, 1024), (0.17, 256)):
+    # (the default run keeps 1e-5 and 1e-3 at N = 20000 and 1e-2; --all-forms runs every density)
+    grid = ((1e-6, 20000), (1e-5, 20000), (1e-4, 20000), (1e-3, 20000), (1e-2, 1024), (0.17, 256))
+    for d, n in (grid if full_sweep else ((1e-5, 20000), (1e-3, 20000), (1e-2, 1024))):
+        t1 = time.perf_counter()
         sets = (sparse_bernoulli_sets_gpu(n, 1 << 24, d, int(1e7 * d) + 5, device) if d <= 1e-3 else
                 bernoulli_sets_gpu(n, 1 << 24, d, int(1e7 * d) + 5, device))
         sweep[f"{d:g}"] = forms_on(sb, sets, 1 << 24, samples=512, with_plain=False)
+        sweep[f"{d:g}"]["seconds"] = round(time.perf_counter() - t1, 1)
     out["density_sweep_2^24"] = sweep
     out["seconds"] = round(time.perf_counter() - t0, 1)
     return out
@@ -1136,6 +1140,8 @@ def sparse_bernoulli_sets_gpu(n, universe, density, seed, device, chunk_rows=204
 STORM_T_CASES = ("zipf_2^24", "runs_2^26", "haplotypes_20000", "bernoulli_1e-06_2^24_N20000",
                  "bernoulli_1e-05_2^24_N20000", "bernoulli_0.0001_2^24_N20000", "bernoulli_0.001_2^24_N20000",
                  "bernoulli_0.01_2^24", "bernoulli_0.17_2^24")
+STORM_T_DEFAULT_CASES = ("zipf_2^24", "bernoulli_1e-06_2^24_N20000", "bernoulli_1e-05_2^24_N20000",
+                         "bernoulli_0.0001_2^24_N20000", "bernoulli_0.001_2^24_N20000")
 
 
 def storm_t_forms(device, cpu_seconds=2.0, only=None):
@@ -1173,7 +1179,7 @@ def storm_t_forms(device, cpu_seconds=2.0, only=None):
     assert [c[0] for c in corpora] == list(STORM_T_CASES)
     out = {}
     for name, make, desc in corpora:
-        if only is not None and name != only:
+        if only is not None and name not in ((only,) if isinstance(only, str) else only):
             continue
         t0 = time.perf_counter()
         sets = make()
@@ -1572,31 +1578,30 @@ def run_b200_arm(args):
     if thresh is not None:
         line["threshold_form"] = thresh
     if rank == 0 and world == 1 and args.forms:
-        try:
-            line["mixed_density"] = mixed_density_forms(sb, device)
-            line["mixed_density_2^24"] = mixed_density_forms(sb, device, n=4096, universe=1 << 24)
-        except Exception as e:   # reported, never silently dropped
-            line["mixed_density"] = {"error": f"{type(e).__name__}: {e}"}
-        try:
-            line["configs_4_5"] = config45_forms(device)
-        except Exception as e:
-            line["configs_4_5"] = {"error": f"{type(e).__name__}: {e}"}
-        try:
-            line["storm_t"] = storm_t_forms(device)
-        except Exception as e:
-            line["storm_t"] = {"error": f"{type(e).__name__}: {e}"}
-        try:
-            line["storm_t_full"] = storm_t_full(device)
-        except Exception as e:
-            line["storm_t_full"] = {"error": f"{type(e).__name__}: {e}"}
-        try:
-            line["autotune_config1"] = autotune_config1(sb, device)
-        except Exception as e:
-            line["autotune_config1"] = {"error": f"{type(e).__name__}: {e}"}
-        try:
-            line["config5a_full"] = config5a_full(sb, device)
-        except Exception as e:
-            line["config5a_full"] = {"error": f"{type(e).__name__}: {e}"}
+        # Characterisation forms, each timed (wall seconds in form_seconds).
+        # The default run keeps them to a few minutes: the STORM_t table keeps
+        # config 5b's densities at N = 20000 and the config-3-shaped corpus
+        # (the full-size configurations have their own entries); --all-forms
+        # adds the reduced-size duplicates and the whole density sweep.
+        secs = {}
+
+        def form(key, fn):
+            t1 = time.perf_counter()
+            try:
+                line[key] = fn()
+            except Exception as e:   # reported, never silently dropped
+                line[key] = {"error": f"{type(e).__name__}: {e}"}
+            secs[key] = round(time.perf_counter() - t1, 1)
+
+        form("mixed_density", lambda: mixed_density_forms(sb, device))
+        form("mixed_density_2^24", lambda: mixed_density_forms(sb, device, n=4096, universe=1 << 24,
+                                                               samples=1024 if args.all_forms else 256))
+        form("configs_4_5", lambda: config45_forms(device, full_sweep=args.all_forms))
+        form("storm_t", lambda: storm_t_forms(device, only=None if args.all_forms else STORM_T_DEFAULT_CASES))
+        form("storm_t_full", lambda: storm_t_full(device))
+        form("autotune_config1", lambda: autotune_config1(sb, device))
+        form("config5a_full", lambda: config5a_full(sb, device))
+        line["form_seconds"] = secs
     if rank == 0:
         line["north_star"] = north_star_summary(line)   # last, so that the tail of the line keeps it
         print(json.dumps(line), flush=True)
@@ -1620,6 +1625,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--all-forms", action="store_true",
+                    help="also the reduced-size STORM_t corpora and the whole density sweep (longer run)")
     ap.add_argument("--no-forms", dest="forms", action="store_false",
                     help="skip the mixed-density learned/plain/CPU comparison")
     ap.add_argument("--traffic", type=float, default=None,

@@ -315,9 +315,9 @@ uint64_t STORM_last_panel_rows(const STORM_t* s);
  * universe-sized histogram). */
 int STORM_last_engine_ms(const STORM_t* s, double* out12);
 /* The rest of the last per-pair call's device time before its first engine:
- * the planner's host work while the GPU waits (after the postings' histogram
- * statistics are read back), the row order's upload and the output's
- * clearing, in ms; -1.0 for a NULL handle. */
+ * the planner's host work while the GPU waits (before the postings'
+ * histogram and after its statistics are read back), the row order's upload
+ * and the output's clearing, in ms; -1.0 for a NULL handle. */
 double STORM_last_plan_ms(const STORM_t* s);
 /* GPU calibration of the planner (no counterpart in the reference's C ABI;
  * its calibrate_on_rows fits the kernel layer's constants on the host,

@@ -930,6 +930,7 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
     const double tc_ns = tensor_pair_ns(cost, slots);
     std::vector<uint8_t> cls(n, 0);                        // 0 C, 1 L, 2 M, 3 H
     if (!ev_hist) SB_CUDA(cudaEventCreate(&ev_hist));
+    if (!ev_hist0) SB_CUDA(cudaEventCreate(&ev_hist0));
     bool hist_ran = false;
     last_panel_rows = last_panel_queries = 0;
 
@@ -937,6 +938,7 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
     PostingsStats ps{};
     auto histogram = [&](const std::vector<uint32_t>& rows) {
         d_qrows.reserve(rows.size());
+        SB_CUDA(cudaEventRecord(ev_hist0, st));
         SB_CUDA(cudaMemcpyAsync(d_qrows.p, rows.data(), rows.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
         d_counts.reserve(U);
         d_pstats.reserve(1);
@@ -1461,7 +1463,7 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
     const uint64_t total = finish(q_sum);
     float t_pre = 0, t_hist = 0, t_tc = 0, t_ch = 0, t_pa = 0, t_po = 0;
     SB_CUDA(cudaEventElapsedTime(&t_pre, log.ev0, ev_eng[0]));
-    if (hist_ran) SB_CUDA(cudaEventElapsedTime(&t_hist, log.ev0, ev_hist));
+    if (hist_ran) SB_CUDA(cudaEventElapsedTime(&t_hist, ev_hist0, ev_hist));
     SB_CUDA(cudaEventElapsedTime(&t_tc, ev_eng[0], ev_eng[1]));
     SB_CUDA(cudaEventElapsedTime(&t_ch, ev_eng[1], ev_eng[2]));
     SB_CUDA(cudaEventElapsedTime(&t_pa, ev_eng[2], ev_eng[3]));
@@ -1471,8 +1473,8 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
     last_engine_ms[2] = t_pa;
     last_engine_ms[3] = t_po + (nq ? t_hist : 0.f);
     // the rest of the time before the engines: planning on the host while
-    // the GPU waits (after the histogram's statistics were read back), the
-    // row order's upload and the output's clearing
+    // the GPU waits (before the histogram and after its statistics are read
+    // back), the row order's upload and the output's clearing
     last_plan_ms = nq ? t_pre - t_hist : t_pre;
     return total;
 }

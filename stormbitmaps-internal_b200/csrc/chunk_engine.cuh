@@ -224,7 +224,7 @@ struct ChunkEngine {
     // per increment -- a read and a write of its count).
     double last_engine_work[4] = {0, 0, 0, 0};
     cudaEvent_t ev_eng[4] = {nullptr, nullptr, nullptr, nullptr};
-    cudaEvent_t ev_hist = nullptr;     // after the postings' histogram
+    cudaEvent_t ev_hist0 = nullptr, ev_hist = nullptr;   // around the postings' histogram
     double last_plan_ms = 0.0;         // time before the first engine that is not the histogram
     DevBuf<uint64_t> d_pX, d_DT;       // panel block: expanded rows, transposed
     DevBuf<PanelItem> d_items;
@@ -242,6 +242,7 @@ struct ChunkEngine {
         for (cudaEvent_t e : ev_eng)
             if (e) cudaEventDestroy(e);
         if (ev_hist) cudaEventDestroy(ev_hist);
+        if (ev_hist0) cudaEventDestroy(ev_hist0);
     }
     // Returns the sum over i < j (triangle) or over all (i, j) (rect).
     uint64_t run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_t n2, uint32_t* d_out,
