@@ -360,11 +360,14 @@ def mixed_density_forms(sb, device, n=4096, universe=1 << 20, tile=64, samples=1
     r = sb.StormRows(universe)
     for v in sets:
         r.add(v)
-    r.upload()
+    t_up = time.perf_counter()
+    r.upload()   # positions to HBM, every representation built on the device
+    t_up = time.perf_counter() - t_up
     pairs = n * (n - 1) // 2
     out = {"workload": f"{n} rows over 2^{universe.bit_length() - 1}, card ~ Zipf(1.1) on [16, 2^"
                        f"{(universe // 4).bit_length() - 1}], uniform w/o replacement; tile {tile}",
-           "pairs": pairs, "generate_s": round(t_gen, 2)}
+           "pairs": pairs, "generate_s": round(t_gen, 2), "upload_and_device_build_s": round(t_up, 4),
+           "values": int(sum(len(v) for v in sets))}
     def best_of(policy, exec_, reps=3, tile=tile):
         times, s = [], None
         for _ in range(reps):
@@ -973,12 +976,14 @@ def forms_on(sb, sets, universe, tile=64, samples=1024, with_plain=True):
     r = sb.StormRows(universe)
     for v in sets:
         r.add(v)
-    r.upload()
+    t_up = time.perf_counter()
+    r.upload()   # positions to HBM, every representation built on the device
+    t_up = time.perf_counter() - t_up
     n = len(sets)
     pairs = n * (n - 1) // 2
     sel = r.train_selector(tile=tile, samples=samples, epochs=400, seed=7)
     lt = r.last_training()
-    res = {"rows": n, "pairs": pairs,
+    res = {"rows": n, "pairs": pairs, "upload_and_device_build_s": round(t_up, 4),
            "regret_learned": round(sel["regret_mlp"], 4),
            "regret_cost_model_calibrated": round(lt["regret_calibrated_model"], 4),
            "fallback_model": "calibrated" if lt["kept_calibrated_model"] else "reference default",

@@ -112,6 +112,24 @@ int STORM_rows_set_dense_block(STORM_rows_t* r, double min_density);
  * plus a 9th word of representation flags (bit 0 bitmap, 1 complement). */
 int STORM_rows_meta(STORM_rows_t* r, uint64_t row, uint32_t* meta9);
 
+/* Forms of one row's stored representation, as STORM_rows_repr copies them
+ * (storm::Row, storm_repr.h:112-276, built on the device by
+ * storm::build_row's rules, storm_repr.cpp:25-207). */
+#define STORM_REPR_RUN_START  0   /* u32 run starts, ascending */
+#define STORM_REPR_RUN_END    1   /* u32 run ends (exclusive) */
+#define STORM_REPR_EWAH       2   /* u64 EWAH-64 stream (storm_repr.h:28-31) */
+#define STORM_REPR_MARKERS    3   /* u32 pairs: stream position of each marker, first word it decodes */
+#define STORM_REPR_BITMAP     4   /* u64 words, n_words of them */
+#define STORM_REPR_RANK       5   /* u64 rank9 directory, 2 x (n_words / 8 rounded up + 1) */
+#define STORM_REPR_OCC        6   /* u64 zone map, one bit per 8 words */
+#define STORM_REPR_COMPLEMENT 7   /* u32 positions not in the row, ascending */
+/* Copies one form of one row to host memory (no counterpart in the
+ * reference, whose Row is a host struct the caller reads directly): returns
+ * the form's element count (pairs for STORM_REPR_MARKERS; 0 for a form the
+ * row does not have) and, when out is non-NULL, copies min(count, cap)
+ * elements into it. */
+int64_t STORM_rows_repr(STORM_rows_t* r, uint64_t row, int kind, void* out, uint64_t cap);
+
 /* Autotuner (no counterpart in the reference, which fixes its tile at 64):
  * times this container's own all-pairs sum on the GPU for every tile in
  * {32, 64, 128, 256} x tensor dense-block threshold in {0, 2^-16, 2^-14,

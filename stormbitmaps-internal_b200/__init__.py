@@ -520,6 +520,7 @@ class Storm:
 # --- kernel layer (include/storm_rows.h) ---------------------------------
 POLICY_ALLBITMAP, POLICY_PERPAIR, POLICY_PERTILE, POLICY_ORACLE, POLICY_FIXED, POLICY_PROBE, POLICY_REFINE, \
     POLICY_LEARNED = range(8)
+REPR_RUN_START, REPR_RUN_END, REPR_EWAH, REPR_MARKERS, REPR_BITMAP, REPR_RANK, REPR_OCC, REPR_COMPLEMENT = range(8)
 POLICY_NAMES = ["all-bitmap", "per-pair", "per-tile", "oracle", "fixed-cell", "probe", "refine", "learned"]
 PAIRINGS = ["BB", "BS", "BR", "BW", "SS", "SR", "SW", "RR", "RW", "WW", "EMPTY", "CB"]
 (P_BB, P_BS, P_BR, P_BW, P_SS, P_SR, P_SW, P_RR, P_RW, P_WW, P_EMPTY, P_CB) = range(12)
@@ -547,6 +548,7 @@ _sig("STORM_rows_set_bitmap_budget", C.c_int, [C.c_void_p, C.c_uint64])
 _sig("STORM_rows_upload", C.c_int, [C.c_void_p])
 _sig("STORM_rows_set_dense_block", C.c_int, [C.c_void_p, C.c_double])
 _sig("STORM_rows_meta", C.c_int, [C.c_void_p, C.c_uint64, u32p])
+_sig("STORM_rows_repr", C.c_int64, [C.c_void_p, C.c_uint64, C.c_int, C.c_void_p, C.c_uint64])
 _sig("STORM_rows_allpairs_sum", C.c_int, [C.c_void_p, C.c_int, C.c_uint32, C.c_int, C.c_int, C.POINTER(AllPairsStats)])
 _sig("STORM_rows_allpairs_matrix", C.c_int, [C.c_void_p, C.c_int, C.c_uint32, C.c_int, C.c_int, u32p, C.c_uint64,
                                              C.POINTER(AllPairsStats)])
@@ -661,6 +663,17 @@ class StormRows:
         m = np.zeros(9, dtype=np.uint32)
         _check(_lib.STORM_rows_meta(self.h, row, _p(m, u32p)), "STORM_rows_meta")
         return m
+
+    def repr(self, row: int, kind: int) -> np.ndarray:
+        """One stored form of one row (REPR_*), copied from the device;
+        markers come as an (m, 2) array of (stream position, first word)."""
+        n = _check(_lib.STORM_rows_repr(self.h, row, kind, None, 0), "STORM_rows_repr")
+        dt = np.uint32 if kind in (REPR_RUN_START, REPR_RUN_END, REPR_COMPLEMENT) else \
+            np.uint64 if kind != REPR_MARKERS else np.uint32
+        out = np.zeros(n * (2 if kind == REPR_MARKERS else 1), dt)
+        if n:
+            _check(_lib.STORM_rows_repr(self.h, row, kind, out.ctypes.data, n), "STORM_rows_repr")
+        return out.reshape(-1, 2) if kind == REPR_MARKERS else out
 
     def allpairs_sum(self, policy, tile=64, fixed_cell=P_BS, exec_=EXEC_BATCHED):
         st = AllPairsStats()

@@ -424,7 +424,6 @@ struct STORM_rows_s {
     std::vector<uint64_t> offs{0};
     uint64_t bitmap_budget = 0;
     bool dirty = true;
-    RowsPack pack;
     RowsDev dev;
     cudaStream_t stream = nullptr;
     DevBuf<uint32_t> d_order, d_het, d_out, d_tile_list;
@@ -495,8 +494,7 @@ void rows_ensure_uploaded(STORM_rows_t* r) {
         const uint64_t fit = budget / row_bytes;
         for (uint64_t k = 0; k < n && k < fit; ++k) bm_rows[ord[k]] = 1;
     }
-    pack_rows(r->vals, r->offs, r->universe, bm_rows, r->pack);
-    upload_rows(r->pack, r->universe, r->dev, st);
+    build_rows(r->vals, r->offs, r->universe, bm_rows, r->dev, st);
     r->dirty = false;
     if (r->graph) {
         cudaGraphExecDestroy(r->graph);
@@ -516,7 +514,7 @@ std::vector<uint32_t> rows_order(const STORM_rows_t* r, int policy) {
     std::iota(o.begin(), o.end(), 0u);
     if (sorted_order_policy(policy))
         std::stable_sort(o.begin(), o.end(), [&](uint32_t a, uint32_t b) {
-            return r->pack.meta[a].card < r->pack.meta[b].card;
+            return r->dev.h_meta[a].card < r->dev.h_meta[b].card;
         });
     return o;
 }
@@ -534,7 +532,7 @@ static void rows_run(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell,
     STORM_allpairs_stats S{};
     if (policy == STORM_POLICY_ALLBITMAP)
         for (uint32_t i = 0; i < n; ++i)
-            if (!r->pack.meta[i].has_bm) fail(STORM_B200_ELIMIT, "all-bitmap policy needs a bitmap for every row");
+            if (!r->dev.h_meta[i].has_bm) fail(STORM_B200_ELIMIT, "all-bitmap policy needs a bitmap for every row");
     if (n == 0) {
         if (st_out) *st_out = S;
         return;
@@ -569,7 +567,7 @@ static void rows_run(STORM_rows_t* r, int policy, uint32_t tile, int fixed_cell,
     if (sorted_pol && r->dense_min_density > 0.0 && r->universe <= (1u << 27)) {
         const double min_size = r->dense_min_density * (double)r->universe;
         auto joins = [&](uint32_t row) {
-            const RowMetaD& m = r->pack.meta[row];
+            const RowMetaD& m = r->dev.h_meta[row];
             const double sparse = std::min<double>((double)m.card, 2.0 * m.runs);
             return m.has_bm && sparse >= min_size;
         };
@@ -789,8 +787,8 @@ int STORM_rows_meta(STORM_rows_t* r, uint64_t row, uint32_t* meta9) {
     if (meta9 == NULL) return STORM_B200_EVALUES;
     return guard([&]() -> int {
         rows_ensure_uploaded(r);
-        if (row >= r->pack.meta.size()) return STORM_B200_EARG;
-        const RowMetaD& m = r->pack.meta[row];
+        if (row >= r->dev.h_meta.size()) return STORM_B200_EARG;
+        const RowMetaD& m = r->dev.h_meta[row];
         const uint32_t w[9] = {m.card, m.runs, m.nw, m.nnz, m.first, m.last, m.has_rank, m.has_occ,
                                (uint32_t)(m.has_bm ? 1 : 0) | (uint32_t)(m.has_comp ? 2 : 0)};
         std::copy(w, w + 9, meta9);
@@ -922,8 +920,8 @@ int64_t STORM_rows_cell(STORM_rows_t* r, int pairing, uint64_t a, uint64_t b) {
         rows_ensure_uploaded(r);
         const uint64_t n = r->offs.size() - 1;
         if (a >= n || b >= n || pairing < 0 || pairing > P_CB || pairing == P_EMPTY) return STORM_B200_EARG;
-        const RowMetaD& ma = r->pack.meta[a];
-        const RowMetaD& mb = r->pack.meta[b];
+        const RowMetaD& ma = r->dev.h_meta[a];
+        const RowMetaD& mb = r->dev.h_meta[b];
         const bool need_a_bm = pairing == P_BB || pairing == P_BS || pairing == P_BR || pairing == P_BW;
         if ((need_a_bm && !ma.has_bm) || (pairing == P_BB && !mb.has_bm)) return STORM_B200_ELIMIT;
         if (pairing == P_CB && (!ma.has_comp || !mb.has_bm)) return STORM_B200_ELIMIT;
@@ -936,6 +934,89 @@ int64_t STORM_rows_cell(STORM_rows_t* r, int pairing, uint64_t a, uint64_t b) {
         SB_CUDA(cudaMemcpyAsync(&h, d.p, sizeof(h), cudaMemcpyDeviceToHost, st));
         SB_CUDA(cudaStreamSynchronize(st));
         res = (int64_t)h;
+        return 0;
+    });
+    return rc < 0 ? rc : res;
+}
+
+int64_t STORM_rows_repr(STORM_rows_t* r, uint64_t row, int kind, void* out, uint64_t cap) {
+    if (r == NULL) return STORM_B200_ENULL;
+    int64_t res = 0;
+    int rc = guard([&]() -> int {
+        rows_ensure_uploaded(r);
+        const uint64_t n = r->offs.size() - 1;
+        if (row >= n || kind < STORM_REPR_RUN_START || kind > STORM_REPR_COMPLEMENT) return STORM_B200_EARG;
+        const RowMetaD& m = r->dev.h_meta[row];
+        const RowsDev& d = r->dev;
+        const uint32_t nblk = (m.nw + 7) / 8;
+        auto span = [&](const DevBuf<uint64_t>& off) {
+            uint64_t h[2];
+            SB_CUDA(cudaMemcpy(h, off.p + row, sizeof(h), cudaMemcpyDeviceToHost));
+            return std::make_pair(h[0], h[1] - h[0]);
+        };
+        auto start = [&](const DevBuf<uint64_t>& off) {
+            uint64_t h = 0;
+            SB_CUDA(cudaMemcpy(&h, off.p + row, sizeof(h), cudaMemcpyDeviceToHost));
+            return h;
+        };
+        const void* src = nullptr;
+        size_t elem = 0;
+        uint64_t count = 0;
+        switch (kind) {
+            case STORM_REPR_RUN_START:
+            case STORM_REPR_RUN_END: {
+                const auto s = span(d.r_off);
+                src = (kind == STORM_REPR_RUN_START ? d.r_start.p : d.r_end.p) + s.first;
+                elem = 4;
+                count = s.second;
+                break;
+            }
+            case STORM_REPR_EWAH: {
+                const auto s = span(d.w_off);
+                src = d.w_buf.p + s.first;
+                elem = 8;
+                count = s.second;
+                break;
+            }
+            case STORM_REPR_MARKERS: {
+                const auto s = span(d.m_off);
+                src = d.m_tab.p + s.first;
+                elem = 8;
+                count = s.second;
+                break;
+            }
+            case STORM_REPR_BITMAP:
+                if (m.has_bm) {
+                    src = d.bm.p + start(d.b_off);
+                    elem = 8;
+                    count = m.nw;
+                }
+                break;
+            case STORM_REPR_RANK:
+                if (m.has_rank) {
+                    src = d.rk.p + start(d.rk_off);
+                    elem = 8;
+                    count = 2 * (uint64_t)(nblk + 1);
+                }
+                break;
+            case STORM_REPR_OCC:
+                if (m.has_occ) {
+                    src = d.oc.p + start(d.oc_off);
+                    elem = 8;
+                    count = r->dev.view.n_occ;
+                }
+                break;
+            default: {   // complement
+                const auto s = span(d.c_off);
+                src = d.c_val.p + s.first;
+                elem = 4;
+                count = s.second;
+                break;
+            }
+        }
+        if (out && count && cap)
+            SB_CUDA(cudaMemcpy(out, src, std::min<uint64_t>(count, cap) * elem, cudaMemcpyDeviceToHost));
+        res = (int64_t)count;
         return 0;
     });
     return rc < 0 ? rc : res;

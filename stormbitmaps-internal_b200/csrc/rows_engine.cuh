@@ -42,38 +42,22 @@ struct RowsView {
     const uint32_t* c_val;
 };
 
-// Host-side packed form (built once per upload).
-struct RowsPack {
-    std::vector<RowMetaD> meta;
-    std::vector<uint64_t> s_off{0}, r_off{0}, w_off{0}, m_off{0}, c_off{0};
-    std::vector<uint32_t> s_val, r_start, r_end, c_val;
-    std::vector<uint64_t> w_buf, bm, rk, oc;
-    std::vector<uint2> m_tab;
-    std::vector<uint64_t> b_off, rk_off, oc_off;
-};
-
-template <class T>
-struct DevVec {
-    DevBuf<T> buf;
-    void put(const std::vector<T>& h, cudaStream_t st) {
-        buf.reserve(h.size() ? h.size() : 1);
-        if (!h.empty())
-            SB_CUDA(cudaMemcpyAsync(buf.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
-    }
-};
-
+// Every representation of the rows, in HBM, and a host copy of the
+// per-row metadata (the host orders rows and checks policies with it).
 struct RowsDev {
-    DevVec<RowMetaD> meta;
-    DevVec<uint64_t> s_off, r_off, w_off, m_off, c_off, b_off, rk_off, oc_off, w_buf, bm, rk, oc;
-    DevVec<uint32_t> s_val, r_start, r_end, c_val;
-    DevVec<uint2> m_tab;
+    DevBuf<RowMetaD> meta;
+    DevBuf<uint64_t> s_off, r_off, w_off, m_off, c_off, b_off, rk_off, oc_off, w_buf, bm, rk, oc;
+    DevBuf<uint32_t> s_val, r_start, r_end, c_val;
+    DevBuf<uint2> m_tab;
+    DevBuf<uint4> counts;              // per-row sizes, scratch of the build
+    std::vector<RowMetaD> h_meta;
     RowsView view{};
 };
 
-// Build every representation of the rows (host, O(total size + bitmap words
-// of the rows that get a bitmap)).  `bm_rows` marks the rows that get B.
-void pack_rows(const std::vector<uint32_t>& vals, const std::vector<uint64_t>& offs, uint32_t universe,
-               const std::vector<uint8_t>& bm_rows, RowsPack& p);
-void upload_rows(const RowsPack& p, uint32_t universe, RowsDev& d, cudaStream_t st);
+// Uploads the rows' sorted positions and builds every representation from
+// them on the device (rows_pack.cu). `bm_rows` marks the rows that get B
+// (empty: every row). Synchronous on `st`.
+void build_rows(const std::vector<uint32_t>& vals, const std::vector<uint64_t>& offs, uint32_t universe,
+                const std::vector<uint8_t>& bm_rows, RowsDev& d, cudaStream_t st);
 
 }  // namespace sb200
