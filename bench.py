@@ -862,7 +862,8 @@ def storm_t_full(device, names=tuple(FULL_CORPORA), cpu_seconds=2.0):
         _, s_e2e = st.matrix(host_out.numpy().view(np.uint32))
         r["e2e"] = {"first_matrix_call_s": round(time.perf_counter() - t1, 3),
                     "pairs_per_s": tri / (time.perf_counter() - t1), "d2h_bytes": tri * 4,
-                    "call": "STORM_pairw_intersect_matrix (pack + upload + all pairs + copy back)"}
+                    "call": "STORM_pairw_intersect_matrix (pack + upload + all pairs + copy back)",
+                    "transfers": st.last_transfer_ms()}
         del host_out
         d_tri = torch.empty(tri, dtype=torch.int32, device=device)
         best, sums = None, {s_e2e}
@@ -1209,7 +1210,7 @@ def storm_t_forms(device, cpu_seconds=2.0, only=None):
         sums.add(v)
         res["e2e"] = {"STORM_add_s": round(t_add, 3), "first_matrix_call_s": round(t_e2e, 3),
                       "pairs_per_s_incl_pack_upload_download": pairs / t_e2e,
-                      "d2h_bytes": pairs * 4}
+                      "d2h_bytes": pairs * 4, "transfers": s.last_transfer_ms()}
         res["setup_s"] = round(time.perf_counter() - t0, 1)
         for form, thr, post in forms:
             s.set_dense_block(thr)

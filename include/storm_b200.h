@@ -319,6 +319,13 @@ int STORM_last_engine_ms(const STORM_t* s, double* out12);
  * histogram and after its statistics are read back), the row order's upload
  * and the output's clearing, in ms; -1.0 for a NULL handle. */
 double STORM_last_plan_ms(const STORM_t* s);
+/* Host-side transfers of the last all-pairs call (no counterpart in the
+ * reference, which has no device): out4[0] wall ms of packing and uploading
+ * the rows (0 when they were already on the device), out4[1] the payload
+ * bytes uploaded (bitmaps and lists), out4[2] wall ms of copying the
+ * per-pair triangle into the caller's host buffer (0 for calls without
+ * one), out4[3] its bytes. */
+int STORM_last_transfer_ms(const STORM_t* s, double* out4);
 /* GPU calibration of the planner (no counterpart in the reference's C ABI;
  * its calibrate_on_rows fits the kernel layer's constants on the host,
  * storm_cost.cpp:779-895): on a strided sample of up to sample_rows rows (0:

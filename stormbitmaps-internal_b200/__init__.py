@@ -116,6 +116,7 @@ _sig("STORM_last_postings_rows", C.c_uint64, [C.c_void_p])
 _sig("STORM_set_panel", C.c_int, [C.c_void_p, C.c_int])
 _sig("STORM_last_engine_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_double)])
 _sig("STORM_last_plan_ms", C.c_double, [C.c_void_p])
+_sig("STORM_last_transfer_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_double)])
 _sig("STORM_calibrate", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_double)])
 _sig("STORM_reset_cost_model", C.c_int, [C.c_void_p])
 _sig("STORM_last_panel_rows", C.c_uint64, [C.c_void_p])
@@ -491,6 +492,14 @@ class Storm:
         o = (C.c_double * 12)()
         _check(_lib.STORM_last_engine_ms(self.h, o), "STORM_last_engine_ms")
         return {k: (o[i], o[4 + i], o[8 + i]) for i, k in enumerate(("tensor", "chunk", "panel", "postings"))}
+
+    def last_transfer_ms(self) -> dict:
+        """Host-side transfers of the last all-pairs call: packing and upload
+        of the rows (ms, payload bytes; 0 when they were on the device), and
+        the copy of the triangle into host memory (ms, bytes)."""
+        o = (C.c_double * 4)()
+        _check(_lib.STORM_last_transfer_ms(self.h, o), "STORM_last_transfer_ms")
+        return {"upload_ms": o[0], "upload_bytes": o[1], "copy_back_ms": o[2], "copy_back_bytes": o[3]}
 
     def last_plan_ms(self) -> float:
         """Device time of the last per-pair call spent before its engines on

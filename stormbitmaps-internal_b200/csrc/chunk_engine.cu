@@ -3,6 +3,8 @@
 #include <cmath>
 #include <cstring>
 #include <algorithm>
+#include <exception>
+#include <mutex>
 #include <thread>
 #include "chunk_engine.cuh"
 #include "dense.cuh"
@@ -153,7 +155,7 @@ void ChunkPack::add_rows(const STORM_bitmap_cont_t* rows, uint64_t n) {
         }
     };
     const uint64_t work = b_base[n] * 8 + l_base[n] * 2 + c_base[n] * 16;
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned hw = host_threads();
     const uint64_t n_thr = std::min<uint64_t>({(uint64_t)std::min(hw, 32u), n, 1 + work / (8u << 20)});
     if (n_thr <= 1) {
         fill(0, n);
@@ -213,20 +215,53 @@ void ChunkDev::upload(const ChunkPack& p, cudaStream_t st) {
 }
 
 PinnedStage::~PinnedStage() {
-    for (int k = 0; k < 2; ++k) {
-        if (done[k]) {
-            cudaEventSynchronize(done[k]);
-            cudaEventDestroy(done[k]);
+    for (Lane& l : lanes) {
+        if (l.st) {
+            cudaStreamSynchronize(l.st);
+            cudaStreamDestroy(l.st);
         }
-        if (buf[k]) cudaFreeHost(buf[k]);
+        for (cudaEvent_t e : l.done)
+            if (e) cudaEventDestroy(e);
     }
+    if (ready) cudaEventDestroy(ready);
+    if (pool) cudaFreeHost(pool);
 }
 
 void PinnedStage::ensure() {
-    for (int k = 0; k < 2; ++k) {
-        if (!buf[k]) SB_CUDA(cudaHostAlloc((void**)&buf[k], BYTES, cudaHostAllocDefault));
-        if (!done[k]) SB_CUDA(cudaEventCreateWithFlags(&done[k], cudaEventDisableTiming));
+    if (pool) return;
+    const unsigned w = std::max(1u, std::min(64u, host_threads()));
+    SB_CUDA(cudaHostAlloc((void**)&pool, TOTAL, cudaHostAllocDefault));
+    lane_bytes = TOTAL / (2 * w) / 4096 * 4096;   // >= 1 MiB: any chunk's payload fits
+    lanes.resize(w);
+    for (unsigned t = 0; t < w; ++t) {
+        Lane& l = lanes[t];
+        l.buf[0] = pool + (2 * (uint64_t)t) * lane_bytes;
+        l.buf[1] = l.buf[0] + lane_bytes;
+        SB_CUDA(cudaStreamCreateWithFlags(&l.st, cudaStreamNonBlocking));
+        for (cudaEvent_t& e : l.done) SB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
+    SB_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+}
+
+// Runs fn(t) for t in [0, workers) on that many host threads (t = 0 on the
+// calling thread) and rethrows the first failure after all have ended.
+template <class F>
+static void run_workers(unsigned workers, F fn) {
+    std::mutex mu;
+    std::exception_ptr first;
+    auto body = [&](unsigned t) {
+        try {
+            fn(t);
+        } catch (...) {
+            std::lock_guard<std::mutex> lock(mu);
+            if (!first) first = std::current_exception();
+        }
+    };
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < workers; ++t) th.emplace_back(body, t);
+    body(0);
+    for (auto& t : th) t.join();
+    if (first) std::rethrow_exception(first);
 }
 
 // Splits [0, n) into at most `parts` contiguous ranges of about equal weight
@@ -245,19 +280,47 @@ static void parallel_rows(uint64_t n, const std::vector<uint64_t>& prefix, unsig
     for (uint64_t r = 0; r < n && cut.size() < k; ++r)
         if (prefix[r + 1] * k >= total * cut.size()) cut.push_back(r + 1);
     if (cut.back() != n) cut.push_back(n);
-    std::vector<std::thread> th;
-    for (size_t t = 0; t + 1 < cut.size(); ++t)
-        if (cut[t] < cut[t + 1]) th.emplace_back(fn, cut[t], cut[t + 1]);
-    for (auto& t : th) t.join();
+    run_workers((unsigned)(cut.size() - 1), [&](unsigned t) { fn(cut[t], cut[t + 1]); });
+}
+
+// Lists are not necessarily strictly increasing in the public layout (a
+// repeated value, or values added out of order): one warp per list chunk
+// tests its entries, flags the chunk CK_DUP and marks its row.
+__global__ void list_order_kernel(const uint64_t* __restrict__ row_off, uint64_t n_rows, uint32_t* __restrict__ ckl,
+                                  const uint64_t* __restrict__ coff, const uint16_t* __restrict__ lst, uint64_t nc,
+                                  uint8_t* __restrict__ row_dup) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    for (uint64_t c = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < nc; c += warps) {
+        const uint32_t k = ckl[c];
+        if (k & CK_BITMAP) continue;
+        const uint32_t len = k & CK_LEN;
+        const uint16_t* l = lst + coff[c];
+        bool bad = false;
+        for (uint32_t e0 = 1; e0 < len && !bad; e0 += 32) {
+            const uint32_t e = e0 + lane;
+            bad = __any_sync(0xffffffffu, e < len && l[e] <= l[e - 1]);
+        }
+        if (bad && lane == 0) {
+            ckl[c] = k | CK_DUP;
+            uint64_t lo = 0, hi = n_rows;   // the row r with row_off[r] <= c < row_off[r + 1]
+            while (lo + 1 < hi) {
+                const uint64_t mid = (lo + hi) >> 1;
+                if (row_off[mid] <= c) lo = mid;
+                else hi = mid;
+            }
+            row_dup[lo] = 1;
+        }
+    }
 }
 
 void ChunkDev::upload_rows(const STORM_bitmap_cont_t* rows, uint64_t n, cudaStream_t st, PinnedStage& stage) {
-    const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    const unsigned hw = std::max(1u, std::min(64u, host_threads()));
     auto live = [&](uint64_t r) { return rows[r].bitmaps && rows[r].block_ids ? rows[r].n_bitmaps : 0u; };
     // Pass 1: per row its chunk count, bitmap words, list slots (each list on
-    // a multiple of 8 entries, as ChunkPack places them) and facts.
-    std::vector<uint64_t> c_base(n + 1, 0), b_base(n + 1, 0), l_base(n + 1, 0), l_used(n, 0), w1(n + 1, 0);
-    std::vector<uint8_t> has_list(n, 0);
+    // a multiple of 8 entries, as ChunkPack places them) and facts; the
+    // lists' order is tested on the device below.
+    std::vector<uint64_t> c_base(n + 1, 0), b_base(n + 1, 0), l_base(n + 1, 0), w1(n + 1, 0);
     std::vector<uint32_t> row_max(n, 0);
     facts.assign(n, ChunkRowFacts{});
     for (uint64_t r = 0; r < n; ++r) w1[r + 1] = w1[r] + 1 + live(r);
@@ -280,12 +343,6 @@ void ChunkDev::upload_rows(const STORM_bitmap_cont_t* rows, uint64_t n, cudaStre
                 } else {
                     const uint32_t ns = b.scalar ? b.n_scalar : 0;
                     pos = (pos + 7) / 8 * 8 + ns;
-                    has_list[r] = 1;
-                    for (uint32_t e = 1; e < ns; ++e)
-                        if (b.scalar[e] <= b.scalar[e - 1]) {
-                            f.plain = false;
-                            break;
-                        }
                     f.card += ns;
                     f.list_entries += ns;
                 }
@@ -295,7 +352,6 @@ void ChunkDev::upload_rows(const STORM_bitmap_cont_t* rows, uint64_t n, cudaStre
             row_max[r] = mx;
             c_base[r + 1] = k_n;
             b_base[r + 1] = nb * CHUNK_WORDS;
-            l_used[r] = pos;
             l_base[r + 1] = (pos + 7) / 8 * 8;
         }
     });
@@ -308,6 +364,7 @@ void ChunkDev::upload_rows(const STORM_bitmap_cont_t* rows, uint64_t n, cudaStre
     }
     n_rows = n;
     const uint64_t nc = c_base[n], nbw = b_base[n], nl = l_base[n];
+    payload_bytes = nbw * 8 + nl * 2;
     // Pass 2: chunk metadata on host threads, then to the device.
     std::vector<uint64_t> h_row_off(n + 1);
     std::vector<uint32_t, NoInitAlloc<uint32_t>> h_cid(nc), h_ckl(nc);
@@ -328,13 +385,7 @@ void ChunkDev::upload_rows(const STORM_bitmap_cont_t* rows, uint64_t n, cudaStre
                     const uint32_t ns = b.scalar ? b.n_scalar : 0;
                     pos = (pos + 7) / 8 * 8;
                     h_coff[c] = l_base[r] + pos;
-                    uint32_t flags = ns & CK_LEN;
-                    for (uint32_t e = 1; e < ns; ++e)
-                        if (b.scalar[e] <= b.scalar[e - 1]) {
-                            flags |= CK_DUP;
-                            break;
-                        }
-                    h_ckl[c] = flags;
+                    h_ckl[c] = ns & CK_LEN;
                     pos += ns;
                 }
             }
@@ -352,57 +403,150 @@ void ChunkDev::upload_rows(const STORM_bitmap_cont_t* rows, uint64_t n, cudaStre
         SB_CUDA(cudaMemcpyAsync(ckl.p, h_ckl.data(), nc * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
         SB_CUDA(cudaMemcpyAsync(coff.p, h_coff.data(), nc * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
     }
-    // Pass 3: payload slices (bitmaps, then lists, of consecutive rows)
-    // gathered into pinned buffers in turn, each copied while the next fills.
+    // Pass 3: the payload. Each worker takes a range of rows of about equal
+    // bytes and moves it in slices of whole chunks: bitmaps (1024 words,
+    // short ones zero-filled) at the front of its buffer, list slots (the
+    // list, zero padding to a multiple of 8 entries) behind them, two copies
+    // per slice on the worker's stream while it fills its other buffer.
     stage.ensure();
     std::vector<uint64_t> pb(n + 1, 0);   // payload bytes of rows before r
     for (uint64_t r = 0; r < n; ++r)
         pb[r + 1] = pb[r] + (b_base[r + 1] - b_base[r]) * 8 + (l_base[r + 1] - l_base[r]) * 2;
-    uint64_t r0 = 0;
-    int k = 0;
-    while (r0 < n) {
-        uint64_t r1 = r0 + 1;
-        while (r1 < n && pb[r1 + 1] - pb[r0] <= PinnedStage::BYTES) ++r1;
-        const uint64_t bw = b_base[r1] - b_base[r0], lw = l_base[r1] - l_base[r0];
-        if (bw * 8 + lw * 2 > PinnedStage::BYTES) fail(STORM_B200_ELIMIT, "a row larger than the staging buffer");
-        if (stage.used[k]) SB_CUDA(cudaEventSynchronize(stage.done[k]));
-        unsigned char* sb = stage.buf[k];
-        uint64_t* sbm = reinterpret_cast<uint64_t*>(sb);
-        uint16_t* slst = reinterpret_cast<uint16_t*>(sb + bw * 8);
-        std::vector<uint64_t> wr(r1 - r0 + 1);
-        for (uint64_t r = r0; r <= r1; ++r) wr[r - r0] = pb[r] - pb[r0];
-        parallel_rows(r1 - r0, wr, hw, [&](uint64_t q0, uint64_t q1) {
-            for (uint64_t r = r0 + q0; r < r0 + q1; ++r) {
-                uint64_t w = b_base[r] - b_base[r0];
-                uint16_t* lr = slst + (l_base[r] - l_base[r0]);
-                std::memset(lr, 0, (l_base[r + 1] - l_base[r]) * sizeof(uint16_t));
-                uint64_t pos = 0;
-                const uint32_t k_n = live(r);
-                for (uint32_t q = 0; q < k_n; ++q) {
-                    const STORM_bitmap_t& b = rows[r].bitmaps[q];
-                    if (b.n_bitmap) {
-                        const uint32_t nw = b.n_bitmap < CHUNK_WORDS ? b.n_bitmap : CHUNK_WORDS;
-                        const uint32_t copied = b.data ? nw : 0;
-                        if (copied) std::memcpy(sbm + w, b.data, copied * sizeof(uint64_t));
-                        std::memset(sbm + w + copied, 0, (CHUNK_WORDS - copied) * sizeof(uint64_t));
-                        w += CHUNK_WORDS;
-                    } else {
-                        const uint32_t ns = b.scalar ? b.n_scalar : 0;
-                        pos = (pos + 7) / 8 * 8;
-                        if (ns) std::memcpy(lr + pos, b.scalar, ns * sizeof(uint16_t));
-                        pos += ns;
-                    }
+    const unsigned workers =
+        (unsigned)std::max<uint64_t>(1, std::min<uint64_t>({(uint64_t)stage.lanes.size(), n, 1 + pb[n] / (4u << 20)}));
+    std::vector<uint64_t> cut{0};
+    for (uint64_t r = 0; r < n && cut.size() < workers; ++r)
+        if (pb[r + 1] * workers >= pb[n] * cut.size()) cut.push_back(r + 1);
+    while (cut.size() <= workers) cut.push_back(n);
+    SB_CUDA(cudaEventRecord(stage.ready, st));   // the metadata copies and earlier work on st
+    const uint64_t cap = stage.lane_bytes;
+    run_workers(workers, [&](unsigned t) {
+        PinnedStage::Lane& L = stage.lanes[t];
+        SB_CUDA(cudaStreamWaitEvent(L.st, stage.ready, 0));
+        uint64_t r = cut[t], k = 0;
+        const uint64_t r_end = cut[t + 1];
+        bool used[2] = {false, false};
+        int which = 0;
+        auto advance = [&]() {
+            ++k;
+            while (r < r_end && k >= live(r)) {
+                ++r;
+                k = 0;
+            }
+        };
+        while (r < r_end && k >= live(r)) {
+            ++r;
+            k = 0;
+        }
+        while (r < r_end) {
+            // the slice: whole chunks from (r, k) while they fit
+            uint64_t sr = r, sk = k, bw = 0, ls = 0;
+            uint64_t b0 = ~0ull, l0 = ~0ull;
+            while (r < r_end) {
+                const STORM_bitmap_t& b = rows[r].bitmaps[k];
+                const uint64_t c = c_base[r] + k;
+                uint64_t nb = 0, nls = 0;
+                if (b.n_bitmap) nb = CHUNK_WORDS;
+                else nls = ((uint64_t)(h_ckl[c] & CK_LEN) + 7) / 8 * 8;
+                if ((bw + nb) * 8 + (ls + nls) * 2 > cap) {
+                    if (bw || ls) break;
+                    // a list longer than a buffer (the public layout allows
+                    // any length): straight from its own memory
+                    const uint64_t ns = h_ckl[c] & CK_LEN;
+                    if (ns) SB_CUDA(cudaMemcpyAsync(lst.p + h_coff[c], b.scalar, ns * 2, cudaMemcpyHostToDevice, L.st));
+                    if (nls > ns) SB_CUDA(cudaMemsetAsync(lst.p + h_coff[c] + ns, 0, (nls - ns) * 2, L.st));
+                    advance();
+                    sr = r;
+                    sk = k;
+                    continue;
+                }
+                if (nb && b0 == ~0ull) b0 = h_coff[c];
+                if (nls && l0 == ~0ull) l0 = h_coff[c];
+                bw += nb;
+                ls += nls;
+                advance();
+            }
+            if (used[which]) SB_CUDA(cudaEventSynchronize(L.done[which]));
+            uint64_t* sbm = reinterpret_cast<uint64_t*>(L.buf[which]);
+            uint16_t* slst = reinterpret_cast<uint16_t*>(L.buf[which] + bw * 8);
+            uint64_t w = 0, p = 0;
+            for (uint64_t q = sr, qk = sk; q < r || (q == r && qk < k);) {
+                const STORM_bitmap_t& b = rows[q].bitmaps[qk];
+                if (b.n_bitmap) {
+                    const uint32_t nw = b.n_bitmap < CHUNK_WORDS ? b.n_bitmap : CHUNK_WORDS;
+                    const uint32_t copied = b.data ? nw : 0;
+                    if (copied) std::memcpy(sbm + w, b.data, copied * sizeof(uint64_t));
+                    std::memset(sbm + w + copied, 0, (CHUNK_WORDS - copied) * sizeof(uint64_t));
+                    w += CHUNK_WORDS;
+                } else {
+                    const uint32_t ns = b.scalar ? b.n_scalar : 0;
+                    const uint64_t slot = ((uint64_t)ns + 7) / 8 * 8;
+                    if (ns) std::memcpy(slst + p, b.scalar, ns * sizeof(uint16_t));
+                    std::memset(slst + p + ns, 0, (slot - ns) * sizeof(uint16_t));
+                    p += slot;
+                }
+                ++qk;
+                while (q < r_end && qk >= live(q)) {
+                    ++q;
+                    qk = 0;
                 }
             }
-        });
-        if (bw) SB_CUDA(cudaMemcpyAsync(bm.p + b_base[r0], sbm, bw * 8, cudaMemcpyHostToDevice, st));
-        if (lw) SB_CUDA(cudaMemcpyAsync(lst.p + l_base[r0], slst, lw * 2, cudaMemcpyHostToDevice, st));
-        SB_CUDA(cudaEventRecord(stage.done[k], st));
-        stage.used[k] = true;
-        k ^= 1;
-        r0 = r1;
+            if (bw) SB_CUDA(cudaMemcpyAsync(bm.p + b0, sbm, bw * 8, cudaMemcpyHostToDevice, L.st));
+            if (ls) SB_CUDA(cudaMemcpyAsync(lst.p + l0, slst, ls * 2, cudaMemcpyHostToDevice, L.st));
+            SB_CUDA(cudaEventRecord(L.done[which], L.st));
+            used[which] = true;
+            which ^= 1;
+        }
+        SB_CUDA(cudaStreamSynchronize(L.st));
+    });
+    // The lists' order, on the device.
+    d_row_dup.reserve(n ? n : 1);
+    SB_CUDA(cudaMemsetAsync(d_row_dup.p, 0, n ? n : 1, st));
+    if (nc && nl) {
+        const uint64_t blocks = std::min<uint64_t>((nc + 7) / 8, 148ull * 16);
+        list_order_kernel<<<(unsigned)blocks, 256, 0, st>>>(row_off.p, n, ckl.p, coff.p, lst.p, nc, d_row_dup.p);
+        SB_CUDA(cudaGetLastError());
     }
+    std::vector<uint8_t> dup(n ? n : 1);
+    SB_CUDA(cudaMemcpyAsync(dup.data(), d_row_dup.p, n ? n : 1, cudaMemcpyDeviceToHost, st));
     SB_CUDA(cudaStreamSynchronize(st));
+    for (uint64_t r = 0; r < n; ++r)
+        if (dup[r]) facts[r].plain = false;
+}
+
+void copy_to_host(uint32_t* out, const uint32_t* d_src, uint64_t count, cudaStream_t st, PinnedStage& stage) {
+    const uint64_t bytes = count * sizeof(uint32_t);
+    if (bytes == 0) return;
+    cudaPointerAttributes a{};
+    const bool pinned = cudaPointerGetAttributes(&a, out) == cudaSuccess && a.type == cudaMemoryTypeHost;
+    cudaGetLastError();   // an attribute query of plain host memory may leave an error behind
+    if (pinned || bytes < (32u << 20)) {
+        SB_CUDA(cudaMemcpyAsync(out, d_src, bytes, cudaMemcpyDeviceToHost, st));
+        SB_CUDA(cudaStreamSynchronize(st));
+        return;
+    }
+    stage.ensure();
+    const uint64_t cap = stage.lane_bytes / sizeof(uint32_t);
+    const unsigned workers =
+        (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(stage.lanes.size(), bytes / (8u << 20)));
+    SB_CUDA(cudaEventRecord(stage.ready, st));
+    run_workers(workers, [&](unsigned t) {
+        PinnedStage::Lane& L = stage.lanes[t];
+        SB_CUDA(cudaStreamWaitEvent(L.st, stage.ready, 0));
+        const uint64_t lo = count * t / workers, hi = count * (t + 1) / workers;
+        auto issue = [&](uint64_t x, int b) {
+            const uint64_t len = std::min(cap, hi - x);
+            SB_CUDA(cudaMemcpyAsync(L.buf[b], d_src + x, len * sizeof(uint32_t), cudaMemcpyDeviceToHost, L.st));
+            SB_CUDA(cudaEventRecord(L.done[b], L.st));
+        };
+        if (lo < hi) issue(lo, 0);
+        int b = 0;
+        for (uint64_t x = lo; x < hi; x += cap, b ^= 1) {
+            if (x + cap < hi) issue(x + cap, b ^ 1);   // its buffer was drained in the last round
+            SB_CUDA(cudaEventSynchronize(L.done[b]));
+            std::memcpy(out + x, L.buf[b], std::min(cap, hi - x) * sizeof(uint32_t));
+        }
+    });
 }
 
 template <class T>

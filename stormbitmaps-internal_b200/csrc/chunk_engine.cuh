@@ -103,16 +103,34 @@ struct ChunkPack {
     void end_row() { row_off.push_back(cid.size()); }
 };
 
-// Pinned host staging for the pipelined upload: two buffers the packer
-// fills in turn while the other one's copy to the device runs.
+// Pinned host staging for copies between pageable host memory and the
+// device: one lane per host worker thread, each with two pinned buffers
+// (one filled or drained by its thread while the other one's copy runs),
+// its own stream and two events. Allocated once per handle.
 struct PinnedStage {
-    static constexpr uint64_t BYTES = 64ull << 20;   // per buffer; holds any one row (<= 16 MiB)
-    unsigned char* buf[2] = {nullptr, nullptr};
-    cudaEvent_t done[2] = {nullptr, nullptr};
-    bool used[2] = {false, false};
+    static constexpr uint64_t TOTAL = 128ull << 20;   // pinned bytes per handle
+    struct Lane {
+        unsigned char* buf[2] = {nullptr, nullptr};
+        cudaEvent_t done[2] = {nullptr, nullptr};
+        cudaStream_t st = nullptr;
+    };
+    unsigned char* pool = nullptr;
+    std::vector<Lane> lanes;
+    uint64_t lane_bytes = 0;   // bytes of each of a lane's two buffers
+    cudaEvent_t ready = nullptr;
+    PinnedStage() = default;
+    PinnedStage(const PinnedStage&) = delete;
+    PinnedStage& operator=(const PinnedStage&) = delete;
     ~PinnedStage();
-    void ensure();
+    void ensure();   // min(64, host threads) lanes
 };
+
+// Copies `count` u32 from device memory to host memory `out` once the work
+// already queued on `st` is done, and returns when they are there: one copy
+// when `out` is pinned or small, else through the stage's lanes, each host
+// worker draining its share of `out` while the next slice of that share
+// crosses PCIe.
+void copy_to_host(uint32_t* out, const uint32_t* d_src, uint64_t count, cudaStream_t st, PinnedStage& stage);
 
 struct ChunkDev {
     DevBuf<uint64_t> row_off, coff, bm;
@@ -121,13 +139,17 @@ struct ChunkDev {
     uint64_t n_rows = 0;
     std::vector<ChunkRowFacts> facts;   // host copy of the per-row facts
     uint32_t max_cid = 0;
+    uint64_t payload_bytes = 0;         // bitmap and list bytes of the last upload
     void upload(const ChunkPack& p, cudaStream_t st);
     // The same layout as upload(ChunkPack::add_rows(rows, n)), without the
     // host copy of the payload: the rows' chunk metadata is built on host
-    // threads, and their bitmaps and lists are gathered on host threads
-    // straight into pinned staging slices whose copies to the device run
-    // while the next slice is gathered.
+    // threads; their bitmaps and lists are gathered by host workers, each
+    // over its own range of chunks, straight into its pinned lane, whose
+    // copies to the device run while the worker fills its other buffer; the
+    // lists' order (the CK_DUP flag and the rows' "plain" fact) is tested on
+    // the device after the upload.
     void upload_rows(const STORM_bitmap_cont_t* rows, uint64_t n, cudaStream_t st, PinnedStage& stage);
+    DevBuf<uint8_t> d_row_dup;
     ChunkView view() const {
         return ChunkView{row_off.p, cid.p, ckl.p, coff.p, bm.p, lst.p};
     }

@@ -60,6 +60,10 @@ int guard(F&& body) {
     }
 }
 
+// Host threads this process may run on (its CPU affinity set; at least 1):
+// the width of the library's host-side packing and copying.
+unsigned host_threads();
+
 // Current device must be an sm_100 part (the kernels are built for sm_100a
 // only).  Returns its SM count; throws ECUDA otherwise.
 int require_device();

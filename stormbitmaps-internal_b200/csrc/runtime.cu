@@ -1,13 +1,30 @@
 // runtime.cu -- device discovery, status strings, thread-local status.
 #include "common.cuh"
 
+#include <sched.h>
+
 #include <mutex>
+#include <thread>
 
 namespace sb200 {
 
 static thread_local int g_last_status = 0;
 void set_last_status(int s) { g_last_status = s; }
 int last_status() { return g_last_status; }
+
+unsigned host_threads() {
+    static const unsigned n = [] {
+        cpu_set_t set;
+        CPU_ZERO(&set);
+        if (sched_getaffinity(0, sizeof(set), &set) == 0) {
+            const int c = CPU_COUNT(&set);
+            if (c > 0) return (unsigned)c;
+        }
+        const unsigned h = std::thread::hardware_concurrency();
+        return h ? h : 1u;
+    }();
+    return n;
+}
 
 int require_device() {
     int dev = 0;

@@ -18,6 +18,7 @@
 #include <cstring>
 #include <atomic>
 #include <memory>
+#include <chrono>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
@@ -49,6 +50,7 @@ struct StormDev {
     DevBuf<unsigned long long> d_found;
     bool valid = false;
     uint64_t shape = 0;    // row_shape() of the rows last packed
+    double xfer[4] = {0, 0, 0, 0};   // STORM_last_transfer_ms
     ~StormDev() {
         if (stream) cudaStreamDestroy(stream);
     }
@@ -110,10 +112,18 @@ static uint64_t row_shape(const STORM_t* s) {
     return h;
 }
 
+static double wall_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 static void ensure_packed(const STORM_t* s, StormDev* d) {
     const uint64_t shape = row_shape(s);
+    for (double& x : d->xfer) x = 0.0;
     if (d->valid && d->shape == shape) return;
+    const double t0 = wall_ms();
     d->dev.upload_rows(s->conts, s->n_conts, stream_of(d), d->stage);
+    d->xfer[0] = wall_ms() - t0;
+    d->xfer[1] = (double)d->dev.payload_bytes;
     d->valid = true;
     d->shape = shape;
 }
@@ -504,7 +514,7 @@ int64_t STORM_add_rows(STORM_t* s, const uint32_t* values, const uint64_t* offse
         }
     };
     const uint64_t total = offsets[n_rows] - offsets[0];
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned hw = host_threads();
     const uint64_t n_thr = std::min<uint64_t>({(uint64_t)std::min(hw, 64u), n_rows, 1 + total / (1u << 20)});
     if (n_thr <= 1) {
         fill(0, n_rows);
@@ -556,7 +566,7 @@ int64_t STORM_add_bitmap_rows(STORM_t* s, const uint64_t* words, uint64_t n_rows
                 failed.store(1);
         }
     };
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned hw = host_threads();
     const uint64_t n_thr = std::min<uint64_t>({(uint64_t)std::min(hw, 64u), n_rows,
                                                1 + n_rows * words_per_row / (1u << 17)});
     if (n_thr <= 1) {
@@ -639,8 +649,10 @@ int STORM_pairw_intersect_matrix(STORM_t* s, uint32_t* out, uint64_t out_len, ui
         d->d_out.reserve(need ? need : 1);
         const uint64_t r = d->engine.run(d->dev, PAIRS_TRIANGLE, s->n_conts, 0, d->d_out.p, st);
         if (need) {
-            SB_CUDA(cudaMemcpyAsync(out, d->d_out.p, need * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-            SB_CUDA(cudaStreamSynchronize(st));
+            const double t0 = wall_ms();
+            copy_to_host(out, d->d_out.p, need, st, d->stage);
+            d->xfer[2] = wall_ms() - t0;
+            d->xfer[3] = (double)need * sizeof(uint32_t);
         }
         if (sum) *sum = r;
         return 0;
@@ -784,6 +796,14 @@ int STORM_last_engine_ms(const STORM_t* s, double* out12) {
         out12[4 + k] = e.last_engine_pred_ms[k];
         out12[8 + k] = e.last_engine_work[k];
     }
+    return 0;
+}
+
+int STORM_last_transfer_ms(const STORM_t* s, double* out4) {
+    if (s == NULL) return STORM_B200_ENULL;
+    if (out4 == NULL) return STORM_B200_EVALUES;
+    const StormDev* d = state_of(s);
+    for (int k = 0; k < 4; ++k) out4[k] = d->xfer[k];
     return 0;
 }
 

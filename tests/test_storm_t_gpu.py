@@ -494,3 +494,104 @@ def test_repeated_and_unordered_list_values_match_reference(sb):
                 want1 = ol.oracle().oracle_list16_blocked(la.ctypes.data_as(C.POINTER(C.c_uint16)),
                                                           lb.ctypes.data_as(C.POINTER(C.c_uint16)), la.size, lb.size)
                 assert sb.intersect_vector16(la, lb) == want1, (seed, a, b)
+
+
+
+def test_list_longer_than_a_staging_buffer(sb):
+    """A list chunk can be longer than one upload worker's pinned buffer (the
+    public layout sets no limit: STORM_bitmap_add_scalar_only appends to a
+    chunk's list without one, repeats included); such a list goes to the
+    device straight from its own memory. Every pair against the reference's
+    per-chunk rules (storm.cpp:652-690) computed here from the rows' lists:
+    list x list by the oracle's restatement of the blocked SSE4.2 count
+    (pinned to the reference by test_list16_cpu.py), bitmap x list one probe
+    per list entry, bitmap x bitmap AND + POPC."""
+    import ctypes as C
+    from test_ingest_cpu import StormT
+    L = sb.lib()
+    L.STORM_bitmap_add_scalar_only.argtypes = [C.c_void_p, sb.u32p, C.c_uint32]
+    g = np.random.default_rng(77)
+    rows = [np.array([5, 10, 20, 70000], np.uint32),                               # list chunks 0 and 1
+            np.sort(g.choice(65536, 3000, replace=False)).astype(np.uint32),       # list
+            np.sort(g.choice(65536, 5000, replace=False)).astype(np.uint32),       # bitmap
+            np.sort(g.choice(np.arange(65536, 131072), 2000, replace=False)).astype(np.uint32),
+            np.array([1, 2, 3], np.uint32)]
+    # (row, chunk index) -> values STORM_bitmap_add_scalar_only appends
+    longs = {(0, 0): g.integers(0, 65536, 9_000_000).astype(np.uint32),   # 18 MB: longer than a lane buffer (>= 4 host threads)
+             (0, 1): g.integers(65536, 131072, 700_000).astype(np.uint32),
+             (4, 0): np.sort(g.integers(0, 65536, 1_200_000)).astype(np.uint32)}
+    st = sb.Storm()
+    for v in rows:
+        st.add(v)
+    s = C.cast(st.h, C.POINTER(StormT)).contents
+    for (r, k), v in longs.items():
+        assert L.STORM_bitmap_add_scalar_only(C.addressof(s.conts[r].bitmaps[k]), v.ctypes.data_as(sb.u32p),
+                                              v.size) == v.size
+    # the rows' chunks as the reference sees them: id -> ("list", u16 entries) or ("bitmap", words)
+    chunks = []
+    for r, v in enumerate(rows):
+        ids = np.unique(v >> 16)
+        row = {}
+        for k, cid in enumerate(ids):
+            part = (v[(v >> 16) == cid] & 0xFFFF).astype(np.uint16)
+            if (r, k) in longs:
+                part = np.concatenate([part, (longs[(r, k)] & 0xFFFF).astype(np.uint16)])
+            if part.size >= 4096 and (r, k) not in longs:
+                row[int(cid)] = ("bitmap", gen.sets_to_rows([part.astype(np.uint32)], 65536)[0])
+            else:
+                row[int(cid)] = ("list", np.ascontiguousarray(part))
+        chunks.append(row)
+    O = ol.oracle()
+
+    def pair(a, b):
+        total = 0
+        for cid in sorted(set(a) & set(b)):
+            (ka, xa), (kb, xb) = a[cid], b[cid]
+            if ka == "list" and kb == "list":
+                total += O.oracle_list16_blocked(xa.ctypes.data_as(ol.u16p), xb.ctypes.data_as(ol.u16p),
+                                                 xa.size, xb.size)
+            elif ka == "bitmap" and kb == "bitmap":
+                total += int(np.unpackbits((xa & xb).view(np.uint8)).sum())
+            else:
+                words, lst = (xa, xb) if ka == "bitmap" else (xb, xa)
+                total += int(((words[lst >> 6] >> (lst & 63).astype(np.uint64)) & np.uint64(1)).sum())
+        return total
+
+    n = len(rows)
+    want = {(i, j): pair(chunks[i], chunks[j]) for i in range(n) for j in range(i + 1, n)}
+    assert st.pairw_intersect_cardinality() == sum(want.values())
+    mat, ssum = st.matrix()
+    assert ssum == sum(want.values())
+    k = 0
+    for i in range(n):
+        for j in range(i, n):
+            if j > i:
+                assert mat[k] == want[(i, j)], (i, j, int(mat[k]), want[(i, j)])
+            k += 1
+    st.close()
+
+
+def test_triangle_into_pageable_host_memory(sb):
+    """A per-pair triangle of more than 32 MiB copied into pageable host
+    memory goes through the handle's pinned lanes, one host worker per share
+    of the output: equal, entry for entry, to the triangle the same call
+    writes into device memory, for row counts that split unevenly."""
+    import torch
+    for n, seed in ((4100, 31), (5003, 32)):
+        sets = gen.bernoulli_sets(n, 1 << 20, 1e-3, seed)
+        vals, offs = gen.to_csr(sets)
+        st = sb.Storm()
+        st.add_rows(vals, offs)
+        tri = n * (n + 1) // 2
+        host = np.full(tri, 0xFFFFFFFF, np.uint32)   # pageable
+        got, s1 = st.matrix(host)
+        d = torch.empty(tri, dtype=torch.int32, device="cuda")
+        s2 = st.matrix_device(d.data_ptr(), tri)
+        assert s1 == s2
+        assert np.array_equal(got, d.cpu().numpy().view(np.uint32)), n
+        xf = st.last_transfer_ms()
+        assert xf["copy_back_ms"] == 0.0   # the device form copies nothing back
+        st.matrix(host)
+        xf = st.last_transfer_ms()
+        assert xf["upload_ms"] == 0.0 and xf["copy_back_bytes"] == tri * 4
+        st.close()
