@@ -274,10 +274,21 @@ uint64_t STORM_last_dense_panels(const STORM_t* s);
  * two forms: the increments go list by list into the output, or -- for
  * outputs larger than L2, at most 51200 postings rows, and when predicted
  * faster from the exact increment count -- a row sweep counts each row's
- * partners in shared memory and writes its slice once.  Modes 2
- * and 3 force the rows in and pick the list-by-list or the row-sweep form.
+ * partners in shared memory and writes its slice once.  A third per-pair
+ * form indexes runs instead of values (at most 51200 postings rows): the
+ * universe is cut into bins of a power of two near the rows' mean run
+ * length, each row's maximal runs into pieces per bin, and a row sweep adds
+ * the overlaps of a row's pieces with the pieces of later rows in the same
+ * bins -- rows made of long runs then cost per run, not per value; it is
+ * used when its exact entry count (from a histogram of pieces per bin)
+ * predicts less time than the value form.  Modes 2, 3 and 4 force the rows
+ * in and pick the list-by-list, the row-sweep or the run-sweep form.
  * Counts are identical. */
 int STORM_set_sparse_postings(STORM_t* s, int mode);
+/* The per-pair form the last all-pairs call on s used for its postings
+ * rows: 0 list by list, 1 row sweep, 2 run sweep, -1 none (no postings
+ * rows, or a sum-only call). */
+int STORM_last_postings_form(const STORM_t* s);
 /* Autotuner (no counterpart in the reference): times the per-pair all-pairs
  * call on the GPU with the tensor-core rows on (cost rule) or off, crossed
  * with the postings on (cost rule) or off, best of two calls each, and keeps

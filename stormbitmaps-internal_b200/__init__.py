@@ -116,6 +116,7 @@ _sig("STORM_last_postings_rows", C.c_uint64, [C.c_void_p])
 _sig("STORM_set_panel", C.c_int, [C.c_void_p, C.c_int])
 _sig("STORM_last_engine_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_double)])
 _sig("STORM_last_plan_ms", C.c_double, [C.c_void_p])
+_sig("STORM_last_postings_form", C.c_int, [C.c_void_p])
 _sig("STORM_last_transfer_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_double)])
 _sig("STORM_calibrate", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_double)])
 _sig("STORM_reset_cost_model", C.c_int, [C.c_void_p])
@@ -492,6 +493,11 @@ class Storm:
         o = (C.c_double * 12)()
         _check(_lib.STORM_last_engine_ms(self.h, o), "STORM_last_engine_ms")
         return {k: (o[i], o[4 + i], o[8 + i]) for i, k in enumerate(("tensor", "chunk", "panel", "postings"))}
+
+    def last_postings_form(self) -> int:
+        """Per-pair form of the last call's postings: 0 list by list, 1 row
+        sweep, 2 run sweep, -1 none."""
+        return int(_lib.STORM_last_postings_form(self.h))
 
     def last_transfer_ms(self) -> dict:
         """Host-side transfers of the last all-pairs call: packing and upload

@@ -13,6 +13,19 @@
 
 namespace sb200 {
 
+// Maximal runs of set bits of a bitmap chunk (its words as stored).
+static uint64_t bitmap_runs(const STORM_bitmap_t& b) {
+    if (!b.data) return 0;
+    const uint32_t nw = b.n_bitmap < CHUNK_WORDS ? b.n_bitmap : CHUNK_WORDS;
+    uint64_t runs = 0, carry = 0;
+    for (uint32_t w = 0; w < nw; ++w) {
+        const uint64_t x = b.data[w];
+        runs += (uint64_t)__builtin_popcountll(x & ~((x << 1) | carry));
+        carry = x >> 63;
+    }
+    return runs;
+}
+
 void ChunkPack::add_chunk(uint32_t id, const STORM_bitmap_t& b) {
     cid.push_back(id);
     if (b.n_bitmap) {
@@ -48,11 +61,13 @@ void ChunkPack::add_row(const STORM_bitmap_cont_t* c) {
                 if (b.n_bitmap != CHUNK_WORDS || b.data == NULL) f.plain = false;
                 f.card += b.n_bits_set;
                 ++f.bitmap_chunks;
+                f.runs += bitmap_runs(b);
             } else {
                 if (ckl.back() & CK_DUP) f.plain = false;
                 const uint32_t ns = b.scalar ? b.n_scalar : 0;
                 f.card += ns;
                 f.list_entries += ns;
+                for (uint32_t e = 0; e < ns; ++e) f.runs += e == 0 || b.scalar[e] != b.scalar[e - 1] + 1;
             }
             if (id > max_cid) max_cid = id;
         }
@@ -131,16 +146,16 @@ void ChunkPack::add_rows(const STORM_bitmap_cont_t* rows, uint64_t n) {
                     if (b.n_bitmap != CHUNK_WORDS || b.data == NULL) f.plain = false;
                     f.card += b.n_bits_set;
                     ++f.bitmap_chunks;
+                    f.runs += bitmap_runs(b);
                 } else {
                     const uint32_t ns = b.scalar ? b.n_scalar : 0;
                     pos = (pos + 7) / 8 * 8;
                     coff[c] = lb + pos;
                     uint32_t flags = ns & CK_LEN;
-                    for (uint32_t e = 1; e < ns; ++e)
-                        if (b.scalar[e] <= b.scalar[e - 1]) {
-                            flags |= CK_DUP;
-                            break;
-                        }
+                    for (uint32_t e = 0; e < ns; ++e) {
+                        if (e && b.scalar[e] <= b.scalar[e - 1]) flags |= CK_DUP;
+                        f.runs += e == 0 || b.scalar[e] != b.scalar[e - 1] + 1;
+                    }
                     ckl[c] = flags;
                     if (ns) std::memcpy(lst.data() + lb + pos, b.scalar, ns * sizeof(uint16_t));
                     pos += ns;
@@ -284,32 +299,54 @@ static void parallel_rows(uint64_t n, const std::vector<uint64_t>& prefix, unsig
 }
 
 // Lists are not necessarily strictly increasing in the public layout (a
-// repeated value, or values added out of order): one warp per list chunk
-// tests its entries, flags the chunk CK_DUP and marks its row.
+// repeated value, or values added out of order): one warp per chunk tests a
+// list's entries, flags the chunk CK_DUP and marks its row; and counts the
+// chunk's maximal runs of consecutive values into its row.
 __global__ void list_order_kernel(const uint64_t* __restrict__ row_off, uint64_t n_rows, uint32_t* __restrict__ ckl,
-                                  const uint64_t* __restrict__ coff, const uint16_t* __restrict__ lst, uint64_t nc,
-                                  uint8_t* __restrict__ row_dup) {
+                                  const uint64_t* __restrict__ coff, const uint16_t* __restrict__ lst,
+                                  const uint64_t* __restrict__ bm, uint64_t nc, uint8_t* __restrict__ row_dup,
+                                  uint32_t* __restrict__ row_runs) {
     const int lane = threadIdx.x & 31;
     const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
     for (uint64_t c = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < nc; c += warps) {
         const uint32_t k = ckl[c];
-        if (k & CK_BITMAP) continue;
         const uint32_t len = k & CK_LEN;
-        const uint16_t* l = lst + coff[c];
+        if (len == 0) continue;
         bool bad = false;
-        for (uint32_t e0 = 1; e0 < len && !bad; e0 += 32) {
-            const uint32_t e = e0 + lane;
-            bad = __any_sync(0xffffffffu, e < len && l[e] <= l[e - 1]);
+        uint32_t runs = 0;   // maximal runs of consecutive values (the run sweep's pieces)
+        if (k & CK_BITMAP) {
+            // run starts: set bits whose lower neighbour is clear
+            const uint64_t* wd = bm + coff[c];
+            uint64_t carry = 0;
+            for (uint32_t w0 = 0; w0 < len; w0 += 32) {
+                const uint32_t wi = w0 + lane;
+                const uint64_t x = wi < len ? wd[wi] : 0ull;
+                const uint64_t prev = __shfl_up_sync(0xffffffffu, x, 1);
+                const uint64_t cin = lane ? prev >> 63 : carry;
+                carry = __shfl_sync(0xffffffffu, x, 31) >> 63;
+                runs += warp_sum_u32((uint32_t)__popcll(x & ~((x << 1) | cin)));
+            }
+        } else {
+            const uint16_t* l = lst + coff[c];
+            for (uint32_t e0 = 0; e0 < len; e0 += 32) {
+                const uint32_t e = e0 + lane;
+                const bool in = e < len;
+                bad |= __any_sync(0xffffffffu, in && e > 0 && l[e] <= l[e - 1]);
+                runs += __popc(__ballot_sync(0xffffffffu, in && (e == 0 || l[e] != l[e - 1] + 1)));
+            }
         }
-        if (bad && lane == 0) {
-            ckl[c] = k | CK_DUP;
+        if (lane == 0) {
             uint64_t lo = 0, hi = n_rows;   // the row r with row_off[r] <= c < row_off[r + 1]
             while (lo + 1 < hi) {
                 const uint64_t mid = (lo + hi) >> 1;
                 if (row_off[mid] <= c) lo = mid;
                 else hi = mid;
             }
-            row_dup[lo] = 1;
+            if (bad) {
+                ckl[c] = k | CK_DUP;
+                row_dup[lo] = 1;
+            }
+            atomicAdd(&row_runs[lo], runs);
         }
     }
 }
@@ -499,19 +536,26 @@ void ChunkDev::upload_rows(const STORM_bitmap_cont_t* rows, uint64_t n, cudaStre
         }
         SB_CUDA(cudaStreamSynchronize(L.st));
     });
-    // The lists' order, on the device.
+    // The lists' order and runs, on the device.
     d_row_dup.reserve(n ? n : 1);
+    d_row_runs.reserve(n ? n : 1);
     SB_CUDA(cudaMemsetAsync(d_row_dup.p, 0, n ? n : 1, st));
-    if (nc && nl) {
+    SB_CUDA(cudaMemsetAsync(d_row_runs.p, 0, (n ? n : 1) * sizeof(uint32_t), st));
+    if (nc) {
         const uint64_t blocks = std::min<uint64_t>((nc + 7) / 8, 148ull * 16);
-        list_order_kernel<<<(unsigned)blocks, 256, 0, st>>>(row_off.p, n, ckl.p, coff.p, lst.p, nc, d_row_dup.p);
+        list_order_kernel<<<(unsigned)blocks, 256, 0, st>>>(row_off.p, n, ckl.p, coff.p, lst.p, bm.p, nc,
+                                                            d_row_dup.p, d_row_runs.p);
         SB_CUDA(cudaGetLastError());
     }
     std::vector<uint8_t> dup(n ? n : 1);
+    std::vector<uint32_t> runs(n ? n : 1);
     SB_CUDA(cudaMemcpyAsync(dup.data(), d_row_dup.p, n ? n : 1, cudaMemcpyDeviceToHost, st));
+    SB_CUDA(cudaMemcpyAsync(runs.data(), d_row_runs.p, (n ? n : 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     SB_CUDA(cudaStreamSynchronize(st));
-    for (uint64_t r = 0; r < n; ++r)
+    for (uint64_t r = 0; r < n; ++r) {
         if (dup[r]) facts[r].plain = false;
+        facts[r].runs = runs[r];
+    }
 }
 
 void copy_to_host(uint32_t* out, const uint32_t* d_src, uint64_t count, cudaStream_t st, PinnedStage& stage) {
@@ -813,8 +857,9 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x, int lane) {
 }
 
 // Gives every value held by >= 2 rows a slot range in the postings array
-// (start) and a list record; other values get start = ~0. One atomic per
-// warp per 32 values.
+// (start) and, when `lists` is given, a list record; other values get
+// start = ~0. One atomic per warp per 32 values. (The run postings use it
+// for bins.)
 __global__ void postings_alloc_kernel(const uint32_t* __restrict__ counts, uint64_t U, uint32_t* __restrict__ start,
                                       uint2* __restrict__ lists, PostingsStats* st) {
     const int lane = threadIdx.x & 31;
@@ -836,7 +881,7 @@ __global__ void postings_alloc_kernel(const uint32_t* __restrict__ counts, uint6
             if (want) {
                 const uint32_t s = (uint32_t)(e0 + n_incl - c);
                 start[x] = s;
-                lists[l0 + __popc(b & ((1u << lane) - 1u))] = make_uint2(s, c);
+                if (lists) lists[l0 + __popc(b & ((1u << lane) - 1u))] = make_uint2(s, c);
             } else {
                 start[x] = ~0u;
             }
@@ -959,6 +1004,279 @@ postings_rows_kernel(ChunkView v, const uint32_t* __restrict__ qrows, uint32_t n
     }
 }
 
+// ---- run postings: L x L by overlaps of runs, bin by bin ----------------
+// The universe is cut into bins of 2^wlog values (16 .. 32768, so that no
+// bin straddles a chunk); a piece is a maximal run of a row's values inside
+// one bin. A row's pieces are disjoint, so |Xa & Xb| is the sum over bins of
+// the overlaps of a's pieces with b's pieces there: rows made of long runs
+// cost per piece instead of per value. Each bin held by >= 2 pieces gets a
+// list of (row, start, end) entries (offsets inside the bin), built like the
+// value postings (histogram, allocation, scatter); then a row sweep: a CTA
+// per row, for each of its pieces the entries of the piece's bin, overlaps
+// with rows after it added in shared memory, its triangle slice written once.
+constexpr uint32_t RUN_SWEEP_BATCH = 2048;   // pieces prefixed in shared memory at once
+
+__device__ __forceinline__ bool run_piece_start(const uint16_t* l, uint32_t e, uint32_t wmask) {
+    return e == 0 || l[e] != l[e - 1] + 1 || (l[e] & wmask) == 0;
+}
+
+__device__ __forceinline__ bool run_piece_last(const uint16_t* l, uint32_t e, uint32_t nl, uint32_t wmask) {
+    return e + 1 == nl || l[e + 1] != l[e] + 1 || ((l[e] + 1u) & wmask) == 0;
+}
+
+// In a bitmap chunk, per word (index `word` inside the chunk): the bits
+// where a bin starts and where one ends (bins of 2^wlog >= 16 bits).
+__device__ __forceinline__ uint64_t run_bin_first_bits(uint32_t word, uint32_t wlog) {
+    if (wlog >= 6) return ((word << 6) & ((1u << wlog) - 1u)) == 0 ? 1ull : 0ull;
+    return wlog == 4 ? 0x0001000100010001ull : 0x0000000100000001ull;
+}
+
+__device__ __forceinline__ uint64_t run_bin_last_bits(uint32_t word, uint32_t wlog) {
+    if (wlog >= 6) return (((word + 1) << 6) & ((1u << wlog) - 1u)) == 0 ? (1ull << 63) : 0ull;
+    return wlog == 4 ? 0x8000800080008000ull : 0x8000000080000000ull;
+}
+
+// Word wi of a bitmap chunk held by this lane (a warp walks the chunk 32
+// words at a time, `carry` = bit 63 of the word before the warp's first):
+// the bits that start a piece and the bits that end one.
+__device__ __forceinline__ void run_bitmap_word(const uint64_t* wd, uint32_t nwc, uint32_t w0, int lane,
+                                                uint32_t wlog, uint64_t& carry, uint64_t& starts, uint64_t& lasts) {
+    const uint32_t wi = w0 + lane;
+    const uint64_t x = wi < nwc ? wd[wi] : 0ull;
+    const uint64_t prev = __shfl_up_sync(0xffffffffu, x, 1);
+    const uint64_t next = __shfl_down_sync(0xffffffffu, x, 1);
+    const uint64_t cin = lane ? prev >> 63 : carry;
+    const uint64_t nin = lane < 31 ? next & 1ull : (w0 + 32 < nwc ? wd[w0 + 32] & 1ull : 0ull);
+    carry = __shfl_sync(0xffffffffu, x, 31) >> 63;
+    starts = (x & ~((x << 1) | cin)) | (x & run_bin_first_bits(wi, wlog));
+    lasts = (x & ~((x >> 1) | (nin << 63))) | (x & run_bin_last_bits(wi, wlog));
+}
+
+// Pieces per row and per bin; warp per row.
+__global__ void run_count_kernel(ChunkView v, const uint32_t* __restrict__ rows, uint32_t nq, uint32_t wlog,
+                                 uint32_t* __restrict__ pieces, uint32_t* __restrict__ bins) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t wmask = (1u << wlog) - 1u;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nq; r += nw) {
+        const uint32_t row = rows[r];
+        uint32_t cnt = 0;
+        for (uint64_t c = v.row_off[row]; c < v.row_off[row + 1]; ++c) {
+            const uint32_t base = v.cid[c] << 16;
+            const uint32_t k = v.ckl[c];
+            if (k & CK_BITMAP) {
+                const uint64_t* wd = v.bm + v.coff[c];
+                const uint32_t nwc = k & CK_LEN;
+                uint64_t carry = 0, starts, lasts;
+                for (uint32_t w0 = 0; w0 < nwc; w0 += 32) {
+                    run_bitmap_word(wd, nwc, w0, lane, wlog, carry, starts, lasts);
+                    cnt += __popcll(starts);
+                    for (uint64_t x = starts; x; x &= x - 1)
+                        atomicAdd(&bins[(base + ((w0 + lane) << 6) + (uint32_t)(__ffsll((long long)x) - 1)) >> wlog],
+                                  1u);
+                }
+            } else {
+                const uint16_t* l = v.lst + v.coff[c];
+                const uint32_t nl = k & CK_LEN;
+                for (uint32_t e = lane; e < nl; e += 32)
+                    if (run_piece_start(l, e, wmask)) {
+                        ++cnt;
+                        atomicAdd(&bins[(base | l[e]) >> wlog], 1u);
+                    }
+            }
+        }
+        cnt = warp_sum_u32(cnt);
+        if (lane == 0) pieces[r] = cnt;
+    }
+}
+
+// Over the bins held by >= 2 pieces: st[0] += their pieces (list entries),
+// st[1] += pieces^2 (the sweep's entry reads).
+__global__ void run_stats_kernel(const uint32_t* __restrict__ bins, uint64_t nb, unsigned long long* __restrict__ st) {
+    unsigned long long e = 0, q = 0;
+    for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < nb; x += (uint64_t)gridDim.x * blockDim.x) {
+        const unsigned long long c = bins[x];
+        if (c >= 2) {
+            e += c;
+            q += c * c;
+        }
+    }
+    e = warp_sum_u64(e);
+    q = warp_sum_u64(q);
+    if ((threadIdx.x & 31) == 0 && e) {
+        atomicAdd(&st[0], e);
+        atomicAdd(&st[1], q);
+    }
+}
+
+// The rows' pieces in row order: pieces[poff[r] + k] = (first value, end),
+// the k-th start and the k-th last value of the row paired by rank (list
+// entries, or set bits of bitmap chunks).
+__global__ void run_fill_kernel(ChunkView v, const uint32_t* __restrict__ rows, uint32_t nq, uint32_t wlog,
+                                const uint64_t* __restrict__ poff, uint2* __restrict__ pieces) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t wmask = (1u << wlog) - 1u;
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nq; r += nw) {
+        const uint32_t row = rows[r];
+        uint2* out = pieces + poff[r];
+        uint32_t ks = 0, kl = 0;
+        for (uint64_t c = v.row_off[row]; c < v.row_off[row + 1]; ++c) {
+            const uint32_t base = v.cid[c] << 16;
+            const uint32_t k = v.ckl[c];
+            if (k & CK_BITMAP) {
+                const uint64_t* wd = v.bm + v.coff[c];
+                const uint32_t nwc = k & CK_LEN;
+                uint64_t carry = 0, starts, lasts;
+                for (uint32_t w0 = 0; w0 < nwc; w0 += 32) {
+                    run_bitmap_word(wd, nwc, w0, lane, wlog, carry, starts, lasts);
+                    const uint32_t ns = (uint32_t)__popcll(starts), nls = (uint32_t)__popcll(lasts);
+                    uint32_t xs = ns, xl = nls;   // inclusive scans over the lanes (words in order)
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const uint32_t ys = __shfl_up_sync(0xffffffffu, xs, o), yl = __shfl_up_sync(0xffffffffu, xl, o);
+                        if (lane >= o) {
+                            xs += ys;
+                            xl += yl;
+                        }
+                    }
+                    const uint32_t at = base + ((w0 + lane) << 6);
+                    uint32_t j = ks + xs - ns;
+                    for (uint64_t x = starts; x; x &= x - 1) out[j++].x = at + (uint32_t)(__ffsll((long long)x) - 1);
+                    j = kl + xl - nls;
+                    for (uint64_t x = lasts; x; x &= x - 1) out[j++].y = at + (uint32_t)__ffsll((long long)x);
+                    ks += __shfl_sync(0xffffffffu, xs, 31);
+                    kl += __shfl_sync(0xffffffffu, xl, 31);
+                }
+            } else {
+                const uint16_t* l = v.lst + v.coff[c];
+                const uint32_t nl = k & CK_LEN;
+                for (uint32_t e0 = 0; e0 < nl; e0 += 32) {
+                    const uint32_t e = e0 + lane;
+                    const bool in = e < nl;
+                    const bool st = in && run_piece_start(l, e, wmask);
+                    const bool la = in && run_piece_last(l, e, nl, wmask);
+                    const uint32_t bs = __ballot_sync(0xffffffffu, st), bl = __ballot_sync(0xffffffffu, la);
+                    if (st) out[ks + __popc(bs & lt)].x = base | l[e];
+                    if (la) out[kl + __popc(bl & lt)].y = (base | l[e]) + 1u;
+                    ks += __popc(bs);
+                    kl += __popc(bl);
+                }
+            }
+        }
+    }
+}
+
+// Each piece of a bin held by >= 2 pieces into the bin's list: (row, start
+// | end << 16), offsets inside the bin; start[b] advances to the list's end.
+__global__ void run_scatter_kernel(uint32_t nq, uint32_t wlog, const uint64_t* __restrict__ poff,
+                                   const uint2* __restrict__ pieces, uint32_t* __restrict__ start,
+                                   uint2* __restrict__ list) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t wmask = (1u << wlog) - 1u;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nq; r += nw)
+        for (uint64_t p = poff[r] + lane; p < poff[r + 1]; p += 32) {
+            const uint2 pc = pieces[p];
+            const uint32_t bin = pc.x >> wlog;
+            if (start[bin] == ~0u) continue;
+            list[atomicAdd(&start[bin], 1u)] = make_uint2(r, (pc.x & wmask) | ((pc.y - (bin << wlog)) << 16));
+        }
+}
+
+// The row sweep over pieces: CTA per row a; the (piece, bin entry) pairs of
+// a batch of a's pieces are split evenly over the threads (a shared-memory
+// prefix of the pieces' bin lengths maps work index -> piece). Shared
+// memory: nq counters, then RUN_SWEEP_BATCH + 1 prefix words. Bin b's list
+// is [end[b] - bins[b], end[b]). Adds the sum over a's partners after it to
+// flags->sum.
+__global__ void __launch_bounds__(POST_SWEEP_THREADS)
+run_sweep_kernel(const uint32_t* __restrict__ qrows, uint32_t nq, const uint64_t* __restrict__ poff,
+                 const uint2* __restrict__ pieces, uint32_t wlog, const uint32_t* __restrict__ bins,
+                 const uint32_t* __restrict__ end, const uint2* __restrict__ list, uint64_t n,
+                 uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags) {
+    extern __shared__ uint32_t cnt[];
+    uint32_t* pref = cnt + nq;
+    __shared__ uint32_t warp_tot[POST_SWEEP_THREADS / 32];
+    __shared__ unsigned long long row_card;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (uint32_t a = blockIdx.x; a < nq; a += gridDim.x) {
+        const uint32_t row = qrows[a];
+        for (uint32_t b = threadIdx.x; b < nq; b += blockDim.x) cnt[b] = 0;
+        if (threadIdx.x == 0) row_card = 0;
+        const uint64_t p0 = poff[a], np = poff[a + 1] - p0;
+        unsigned long long card = 0;
+        for (uint64_t pb = 0; pb < np; pb += RUN_SWEEP_BATCH) {
+            const uint32_t m = (uint32_t)(np - pb < RUN_SWEEP_BATCH ? np - pb : RUN_SWEEP_BATCH);
+            // pref[k] = entries of the bins of pieces pb .. pb + k - 1: each
+            // thread sums a contiguous segment, then a block scan of the sums
+            const uint32_t seg = (m + POST_SWEEP_THREADS - 1) / POST_SWEEP_THREADS;
+            const uint32_t k0 = threadIdx.x * seg, k1 = k0 + seg < m ? k0 + seg : m;
+            uint32_t mine = 0;
+            for (uint32_t k = k0; k < k1; ++k) {
+                const uint2 pc = pieces[p0 + pb + k];
+                card += pc.y - pc.x;
+                const uint32_t c = bins[pc.x >> wlog];
+                mine += c >= 2 ? c : 0u;
+            }
+            uint32_t inc = mine;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += y;
+            }
+            __syncthreads();   // the previous batch is done with pref and warp_tot
+            if (lane == 31) warp_tot[wid] = inc;
+            __syncthreads();
+            uint32_t before = 0, total = 0;
+            for (int w = 0; w < POST_SWEEP_THREADS / 32; ++w) {
+                if (w < wid) before += warp_tot[w];
+                total += warp_tot[w];
+            }
+            uint32_t acc = before + inc - mine;
+            for (uint32_t k = k0; k < k1; ++k) {
+                pref[k] = acc;
+                const uint32_t c = bins[pieces[p0 + pb + k].x >> wlog];
+                acc += c >= 2 ? c : 0u;
+            }
+            if (threadIdx.x == 0) pref[m] = total;
+            __syncthreads();
+            for (uint32_t t = threadIdx.x; t < total; t += blockDim.x) {
+                uint32_t lo = 0, hi = m;           // last piece k with pref[k] <= t
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (pref[mid] <= t) lo = mid;
+                    else hi = mid;
+                }
+                const uint2 pc = pieces[p0 + pb + lo];
+                const uint32_t bin = pc.x >> wlog;
+                const uint2 E = list[end[bin] - bins[bin] + (t - pref[lo])];
+                if (E.x > a) {
+                    const uint32_t b0 = bin << wlog;
+                    const uint32_t s2 = b0 + (E.y & 0xFFFFu), e2 = b0 + (E.y >> 16);
+                    const uint32_t s = pc.x > s2 ? pc.x : s2, e = pc.y < e2 ? pc.y : e2;
+                    if (e > s) atomicAdd(&cnt[E.x], e - s);
+                }
+            }
+        }
+        card = warp_sum_u64(card);
+        if (lane == 0 && card) atomicAdd(&row_card, card);
+        __syncthreads();
+        const uint64_t base = tri_index(n, row, row) - row;   // out index of (row, j) is base + j
+        unsigned long long sum = 0;
+        for (uint32_t b = a + 1 + threadIdx.x; b < nq; b += blockDim.x) {
+            const uint32_t gb = qrows[b];
+            out[gb > row ? base + gb : tri_index(n, gb, row)] = cnt[b];
+            sum += cnt[b];
+        }
+        sum = warp_sum_u64(sum);
+        if (lane == 0 && sum) atomicAdd(&flags->sum, sum);
+        if (threadIdx.x == 0) out[base + row] = (uint32_t)row_card;
+        __syncthreads();
+    }
+}
+
 // Diagonal of rows with bitmap chunks too (warp per row): each row's value
 // count, set bits of its bitmap chunks plus its list entries.
 __global__ void row_card_diag_kernel(ChunkView v, const uint32_t* __restrict__ rows, uint32_t m, uint64_t n,
@@ -1001,6 +1319,7 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
     log.last_ms = 0.f;
     last_dense_rows = last_dense_panels = last_postings_rows = 0;
     last_panel_rows = last_panel_queries = 0;
+    last_postings_form = -1;
     for (int k = 0; k < 4; ++k) last_engine_ms[k] = last_engine_pred_ms[k] = last_engine_work[k] = 0.0;
     if (n_pairs_all == 0) return 0;
     d_flags.reserve(1);
@@ -1100,6 +1419,54 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         SB_CUDA(cudaStreamSynchronize(st));
         return h;
     };
+    // Run postings (run_sweep_kernel): bins of 2^rwlog values, the mean run
+    // length of the plain list rows rounded to a power of two in [16, 32768]
+    // (a run of length l spans about 1 + l / bin bins; the sweep's entry
+    // reads, pieces^2 x bin / U for uniform rows, are least at bin = l).
+    uint32_t rwlog = 4;
+    if (facts_ok) {
+        double sc = 0.0, sr = 0.0;
+        for (uint64_t r = 0; r < n; ++r) {
+            const ChunkRowFacts& f = d.facts[r];
+            if (f.plain && f.bitmap_chunks == 0) {
+                sc += (double)f.card;
+                sr += (double)f.runs;
+            }
+        }
+        const double ml = sr > 0.0 ? sc / sr : 1.0;
+        rwlog = (uint32_t)std::min(15.0, std::max(4.0, std::round(std::log2(std::max(ml, 1.0)))));
+    }
+    const double RW = (double)(1u << rwlog);
+    const uint64_t n_bins = U >> rwlog;
+    auto pieces_est = [&](const ChunkRowFacts& f) { return (double)f.runs + (double)f.card / RW; };
+    unsigned long long run_entries = 0, run_checks = 0;   // exact, from the piece histogram
+    std::vector<uint32_t> h_rpieces;
+    bool use_run = false;
+    auto run_histogram = [&](const std::vector<uint32_t>& rows) {
+        const uint64_t q = rows.size();
+        d_qrows.reserve(q);
+        SB_CUDA(cudaEventRecord(ev_hist0, st));
+        SB_CUDA(cudaMemcpyAsync(d_qrows.p, rows.data(), q * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        d_rbins.reserve(n_bins);
+        d_rpieces.reserve(q);
+        d_rstats.reserve(2);
+        SB_CUDA(cudaMemsetAsync(d_rbins.p, 0, n_bins * sizeof(uint32_t), st));
+        SB_CUDA(cudaMemsetAsync(d_rstats.p, 0, 2 * sizeof(unsigned long long), st));
+        const uint32_t gq = (uint32_t)std::min<uint64_t>((q + 7) / 8, (uint64_t)sms * 16);
+        run_count_kernel<<<gq, 256, 0, st>>>(d.view(), d_qrows.p, (uint32_t)q, rwlog, d_rpieces.p, d_rbins.p);
+        run_stats_kernel<<<sms * 8, 256, 0, st>>>(d_rbins.p, n_bins, d_rstats.p);
+        SB_CUDA(cudaGetLastError());
+        SB_CUDA(cudaEventRecord(ev_hist, st));
+        hist_ran = true;
+        launches += 2;
+        unsigned long long h[2] = {0, 0};
+        h_rpieces.resize(q);
+        SB_CUDA(cudaMemcpyAsync(h, d_rstats.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+        SB_CUDA(cudaMemcpyAsync(h_rpieces.data(), d_rpieces.p, q * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        SB_CUDA(cudaStreamSynchronize(st));
+        run_entries = h[0];
+        run_checks = h[1];
+    };
     auto finish = [&](uint64_t extra_sum) {
         SB_CUDA(cudaEventRecord(log.ev1, st));
         DeviceFlags f;
@@ -1157,7 +1524,52 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         const double per_pair = sweep_form(incr, q) ? sweep_ns(incr, q) : incr * c_list;
         return (d_out ? per_pair : 0.0) + (double)U * cost.ns_per_universe_value;
     };
+    // ns of the run sweep with `checks` entry reads for q rows (per pair only)
+    auto run_ns = [&](double checks, uint64_t q) {
+        return (double)q * (double)q * cost.ns_per_sweep_row_pair + checks * cost.ns_per_run_check +
+               (double)n_bins * cost.ns_per_universe_value;
+    };
+    auto run_ok = [&](uint64_t q) {
+        return d_out != nullptr && q <= POST_SWEEP_MAX_ROWS && postings_mode != 2 && postings_mode != 3;
+    };
     std::vector<uint32_t> qrows, dense, mrows;             // L, H, M
+    // L x L for `rest` (plain rows without bitmap chunks) by postings when
+    // predicted faster than `alt` ns (or when forced): the run sweep when its
+    // estimate beats the value postings' and its exact count (the piece
+    // histogram) beats `alt`, else the value postings on their exact count
+    // (the value histogram).
+    auto decide = [&](const std::vector<uint32_t>& rest, double alt) -> bool {
+        const uint64_t q = rest.size();
+        if (q < 2) return false;
+        bool lists_only = true;   // the value postings index list chunks only
+        for (uint32_t r : rest) lists_only = lists_only && d.facts[r].bitmap_chunks == 0;
+        if (run_ok(q)) {
+            double P = 0.0, C1 = 0.0, C2 = 0.0;
+            for (uint32_t r : rest) {
+                const ChunkRowFacts& f = d.facts[r];
+                P += pieces_est(f);
+                C1 += (double)f.card;
+                C2 += (double)f.card * (double)f.card;
+            }
+            const double run_e = run_ns(P * P * RW / (double)U, q);
+            const double val_e = post_ns((C1 * C1 - C2) / (2.0 * (double)U), q);
+            if (postings_mode == 4 || run_e < val_e || !lists_only) {
+                run_histogram(rest);
+                if (postings_mode == 4 || postings_mode == 1 || run_ns((double)run_checks, q) < alt) {
+                    use_run = true;
+                    qrows = rest;
+                    return true;
+                }
+            }
+        }
+        if (!lists_only) return false;
+        ps = histogram(rest);
+        if (ps.entries < (1ull << 32) && (postings_mode > 0 || post_ns((double)ps.pairs, q) < alt)) {
+            qrows = rest;
+            return true;
+        }
+        return false;
+    };
     bool panel_plan = false;
     // The panel needs a block of expanded rows and its transpose in HBM.
     const uint64_t panel_bytes = 2ull * PANEL_ROWS * W * sizeof(uint64_t);
@@ -1189,11 +1601,7 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
                 chunk_rest += chunk_self_pair_ns(cost, f, slots);
             }
         }
-        if (rest.size() >= 2) {
-            ps = histogram(rest);
-            const double alt = 0.5 * ((double)rest.size() - 1.0) * chunk_rest;
-            if (ps.entries < (1ull << 32) && (postings_mode > 0 || post_ns((double)ps.pairs, rest.size()) < alt)) qrows = rest;
-        }
+        if (rest.size() >= 2) decide(rest, 0.5 * ((double)rest.size() - 1.0) * chunk_rest);
     } else if (tc_ok && post_ok) {
         // Plain rows, heaviest first.  Plan A (no panel): rows with bitmap
         // chunks go to H, list rows join H while that lowers tensor time (H x
@@ -1207,24 +1615,32 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         std::stable_sort(pl.begin(), pl.end(),
                          [&](uint32_t x, uint32_t y) { return d.facts[x].card > d.facts[y].card; });
         const uint64_t np = pl.size();
-        std::vector<double> S1(np + 1, 0.0), S2(np + 1, 0.0);
+        std::vector<double> S1(np + 1, 0.0), S2(np + 1, 0.0), S3(np + 1, 0.0);
         uint64_t lb = 0;                                   // rows [0, lb) hold every bitmap-chunk row
         for (uint64_t t = 0; t < np; ++t) {
             const double c = (double)d.facts[pl[t]].card;
             S1[t + 1] = S1[t] + c;
             S2[t + 1] = S2[t] + c * c;
+            S3[t + 1] = S3[t] + pieces_est(d.facts[pl[t]]);
             if (d.facts[pl[t]].bitmap_chunks) lb = t + 1;
         }
-        auto post_est = [&](uint64_t from) {   // postings ns of the rows [from, np)
+        // postings ns of the rows [from, np): the value form (rows without
+        // bitmap chunks: from >= lb) or the run form (any plain rows)
+        auto post_est = [&](uint64_t from) {
             const uint64_t q = np - from;
             if (q < 2) return 0.0;
             const double r1 = S1[np] - S1[from], r2 = S2[np] - S2[from];
-            return post_ns((r1 * r1 - r2) / (2.0 * (double)U), q);
+            double v = from >= lb ? post_ns((r1 * r1 - r2) / (2.0 * (double)U), q) : HUGE_VAL;
+            if (run_ok(q)) {
+                const double P = S3[np] - S3[from];
+                v = std::min(v, run_ns(P * P * RW / (double)U, q));
+            }
+            return v;
         };
-        // Plan A: H = [0, k) for k >= lb.
+        // Plan A: H = [0, k); the rows below k by postings.
         uint64_t best_k = lb;
         double best_a = -1.0;
-        for (uint64_t k = lb; k <= np; ++k) {
+        for (uint64_t k = 0; k <= np; ++k) {
             const double kk = (double)k;
             const double v = tc_ns * (kk * (kk - 1.0) / 2.0 + kk * (double)(np - k)) + post_est(k);
             if (best_a < 0 || v < best_a) {
@@ -1232,7 +1648,8 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
                 best_k = k;
             }
         }
-        if (postings_mode > 0) best_k = lb;                // forced: every list row to the postings
+        if (postings_mode == 4) best_k = 0;                // forced: every plain row to the run sweep
+        else if (postings_mode > 0) best_k = lb;           // forced: every list row to the postings
         // Plan B over candidate cuts (h, m).
         uint64_t best_h = 0, best_m = 0;
         double best_b = -1.0;
@@ -1244,7 +1661,7 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
             const double build_ns = 3.0 * (double)PANEL_ROWS * (double)W * 8.0 * cost.ns_per_panel_byte;
             for (uint64_t h : cand) {
                 for (uint64_t e : cand) {                  // e = h + m
-                    if (e < h || e < lb || e > np || e == 0) continue;
+                    if (e < h || e > np || e == 0) continue;   // rows past e: postings (value or run form)
                     if (panel_mode > 0 && e == h) continue;    // forced: some rows in M
                     const double m = (double)(e - h), hh = (double)h, nl = (double)(np - e);
                     const double nb = std::ceil((double)e / PANEL_ROWS);
@@ -1274,7 +1691,6 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         }
         std::sort(rest.begin(), rest.end());               // stored order: ascending output writes
         if (rest.size() >= 2) {
-            ps = histogram(rest);
             // The estimate assumes independent rows; correlated rows share
             // more. With the exact count, keep the postings only if they beat
             // the alternative on these pairs: the panel (the rows queried
@@ -1284,8 +1700,7 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
                                                 (0.5 * std::ceil(q / PANEL_ROWS) + 0.5) +
                                                 cost.ns_per_panel_pair * q * (q - 1.0) / 2.0
                                           : tc_ns * (q * (q - 1.0) / 2.0);
-            if (ps.entries < (1ull << 32) && (postings_mode > 0 || post_ns((double)ps.pairs, rest.size()) < alt)) {
-                qrows = rest;
+            if (decide(rest, alt)) {
             } else if (panel_plan) {
                 mrows.insert(mrows.end(), rest.begin(), rest.end());
             } else {
@@ -1313,11 +1728,7 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
                 chunk_rest += chunk_self_pair_ns(cost, f, slots);
             }
         }
-        if (rest.size() >= 2) {
-            ps = histogram(rest);
-            const double alt = 0.5 * ((double)rest.size() - 1.0) * chunk_rest;
-            if (ps.entries < (1ull << 32) && (postings_mode > 0 || post_ns((double)ps.pairs, rest.size()) < alt)) qrows = rest;
-        }
+        if (rest.size() >= 2) decide(rest, 0.5 * ((double)rest.size() - 1.0) * chunk_rest);
     }
     if (panel_plan && mrows.empty() && dense.empty()) panel_plan = false;
     // Rows the tensor cores expand behind the H rows: the L rows in the plan
@@ -1390,7 +1801,15 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
                                              nb * 3.0 * PANEL_ROWS * (double)W * 8.0 * cost.ns_per_panel_byte);
             last_engine_work[2] = 256.0 * vb + 4.0 * pairs + nb * 3.0 * PANEL_ROWS * (double)W * 8.0;
         }
-        if (nq) {
+        if (nq && use_run) {
+            // run sweep: the pieces (8 B each, written and read), the bin
+            // entries each piece reads (8 B), 4 B per count of the slice
+            last_engine_pred_ms[3] = 1e-6 * run_ns((double)run_checks, nq);
+            double pcs = 0.0;
+            for (uint32_t k : h_rpieces) pcs += (double)k;
+            last_engine_work[3] = 16.0 * pcs + 8.0 * (double)run_entries + 8.0 * (double)run_checks +
+                                  4.0 * (double)nq * ((double)nq + 1.0) / 2.0 + 4.0 * (double)n_bins;
+        } else if (nq) {
             last_engine_pred_ms[3] = 1e-6 * post_ns((double)ps.pairs, nq);
             double vals = 0.0;
             for (uint32_t r : qrows) vals += (double)d.facts[r].card;
@@ -1564,9 +1983,36 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
     SB_CUDA(cudaEventRecord(ev_eng[3], st));
     // ---- L x L by postings
     uint64_t q_sum = 0;
-    if (nq) {
+    last_postings_form = -1;
+    if (nq && use_run) {
+        // run sweep (the sum over these pairs is added by the kernel)
+        last_postings_form = 2;
+        std::vector<uint64_t> poff(nq + 1, 0);
+        for (uint64_t k = 0; k < nq; ++k) poff[k + 1] = poff[k] + h_rpieces[k];
+        d_rpoff.reserve(nq + 1);
+        SB_CUDA(cudaMemcpyAsync(d_rpoff.p, poff.data(), (nq + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+        d_pieces.reserve(poff[nq] ? poff[nq] : 1);
+        d_rstart.reserve(n_bins);
+        d_rlist.reserve(run_entries ? run_entries : 1);
+        d_pstats.reserve(1);
+        SB_CUDA(cudaMemsetAsync(d_pstats.p, 0, sizeof(PostingsStats), st));
+        const uint32_t gq = (uint32_t)std::min<uint64_t>((nq + 7) / 8, (uint64_t)sms * 16);
+        run_fill_kernel<<<gq, 256, 0, st>>>(d.view(), d_qrows.p, (uint32_t)nq, rwlog, d_rpoff.p, d_pieces.p);
+        postings_alloc_kernel<<<sms * 8, 256, 0, st>>>(d_rbins.p, n_bins, d_rstart.p, nullptr, d_pstats.p);
+        run_scatter_kernel<<<gq, 256, 0, st>>>((uint32_t)nq, rwlog, d_rpoff.p, d_pieces.p, d_rstart.p, d_rlist.p);
+        static std::atomic<uint64_t> done{0};
+        smem_attr_once(run_sweep_kernel, (int)((POST_SWEEP_MAX_ROWS + RUN_SWEEP_BATCH + 1) * sizeof(uint32_t)), done);
+        const uint32_t smem = (uint32_t)((nq + RUN_SWEEP_BATCH + 1) * sizeof(uint32_t));
+        const uint32_t gr = (uint32_t)std::min<uint64_t>(nq, (uint64_t)sms * 8);
+        run_sweep_kernel<<<gr, POST_SWEEP_THREADS, smem, st>>>(d_qrows.p, (uint32_t)nq, d_rpoff.p, d_pieces.p, rwlog,
+                                                               d_rbins.p, d_rstart.p, d_rlist.p, n, d_out, d_flags.p);
+        SB_CUDA(cudaGetLastError());
+        launches += 4;
+        last_postings_rows = nq;
+    } else if (nq) {
         q_sum = ps.pairs;
         const bool sweep = sweep_form((double)ps.pairs, nq);
+        last_postings_form = sweep ? 1 : 0;
         if (d_out) {
             d_start.reserve(U);
             d_lists.reserve(ps.lists ? ps.lists : 1);

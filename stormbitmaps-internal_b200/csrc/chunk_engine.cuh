@@ -74,6 +74,7 @@ struct NoInitAlloc : std::allocator<T> {
 
 struct ChunkRowFacts {
     uint64_t card = 0, list_entries = 0;
+    uint64_t runs = 0;   // maximal runs of consecutive values inside the list chunks
     uint32_t chunks = 0, bitmap_chunks = 0;
     bool plain = true;
 };
@@ -150,6 +151,7 @@ struct ChunkDev {
     // the device after the upload.
     void upload_rows(const STORM_bitmap_cont_t* rows, uint64_t n, cudaStream_t st, PinnedStage& stage);
     DevBuf<uint8_t> d_row_dup;
+    DevBuf<uint32_t> d_row_runs;
     ChunkView view() const {
         return ChunkView{row_off.p, cid.p, ckl.p, coff.p, bm.p, lst.p};
     }
@@ -205,6 +207,7 @@ struct ChunkCostModel {
     double ns_per_panel_value = 0.05;        // transposed panel: one query value against one 2048-row block
     double ns_per_panel_pair = 0.005;        // transposed panel: one count written
     double ns_per_panel_byte = 1.0 / 6000.0; // transposed panel: expansion and transpose traffic
+    double ns_per_run_check = 0.02;          // run sweep: one bin entry read against one piece
 };
 double chunk_self_pair_ns(const ChunkCostModel& m, const ChunkRowFacts& f, uint64_t slots);
 double tensor_pair_ns(const ChunkCostModel& m, uint64_t slots);
@@ -228,11 +231,18 @@ struct ChunkEngine {
     ChunkCostModel cost;
     uint64_t dense_budget_bytes = 0;   // 0: 60 % of free device memory
     int postings_mode = -1;            // -1 by cost, 0 never, 1 always (when the rows qualify);
-                                       // 2 / 3 always, per-pair form list by list / row sweep
+                                       // 2 / 3 / 4 always, per-pair form list by list / row sweep /
+                                       // run sweep
     int panel_mode = -1;               // transposed panel: -1 by cost, 0 never, 1 whenever it can run,
                                        // 2 every plain row in it
     uint64_t last_dense_rows = 0, last_dense_panels = 0, last_postings_rows = 0;
     uint64_t last_panel_rows = 0, last_panel_queries = 0;
+    int last_postings_form = -1;       // per-pair form of the last call's postings: 0 list by list,
+                                       // 1 row sweep, 2 run sweep (-1: none)
+    DevBuf<uint32_t> d_rpieces, d_rbins, d_rstart;
+    DevBuf<uint64_t> d_rpoff;
+    DevBuf<uint2> d_pieces, d_rlist;
+    DevBuf<unsigned long long> d_rstats;
     // Per engine of the last per-pair triangle call -- tensor cores, chunk
     // kernel, transposed panel, postings (with the histograms): device ms
     // (events between the engines on the stream) and the cost model's

@@ -780,12 +780,17 @@ int STORM_autotune(STORM_t* s, double* best_min_density, int* best_postings, dou
 
 int STORM_set_sparse_postings(STORM_t* s, int mode) {
     if (s == NULL) return STORM_B200_ENULL;
-    if (mode < -1 || mode > 3) return STORM_B200_EARG;
+    if (mode < -1 || mode > 4) return STORM_B200_EARG;
     state_of(s)->engine.postings_mode = mode;
     return 0;
 }
 
 uint64_t STORM_last_postings_rows(const STORM_t* s) { return s ? state_of(s)->engine.last_postings_rows : 0; }
+
+int STORM_last_postings_form(const STORM_t* s) {
+    if (s == NULL) return STORM_B200_ENULL;
+    return state_of(s)->engine.last_postings_form;
+}
 
 int STORM_last_engine_ms(const STORM_t* s, double* out12) {
     if (s == NULL) return STORM_B200_ENULL;
@@ -838,6 +843,7 @@ int STORM_calibrate(STORM_t* s, uint32_t sample_rows, double* out) {
         const double dens[3] = {1e-12, 0.0, 0.0};
         const int post[3] = {0, -1, 1}, pan[3] = {0, 2, 0}, eng[3] = {0, 2, 3};
         double scale[3] = {1.0, 1.0, 1.0};
+        int post_form = -1;
         for (int k = 0; k < 3; ++k) {
             e.dense_min_density = dens[k];
             e.postings_mode = post[k];
@@ -850,15 +856,20 @@ int STORM_calibrate(STORM_t* s, uint32_t sample_rows, double* out) {
                 pred = e.last_engine_pred_ms[eng[k]];
             }
             if (pred > 1e-4 && meas > 0) scale[k] = meas / pred;
+            if (k == 2) post_form = e.last_postings_form;
         }
         ChunkCostModel& c = d->engine.cost;
         c.ns_per_tensor_bit *= scale[0];
         c.ns_per_panel_value *= scale[1];
         c.ns_per_panel_pair *= scale[1];
         c.ns_per_panel_byte *= scale[1];
-        c.ns_per_posting_pair *= scale[2];
-        c.ns_per_posting_pair_hbm *= scale[2];
-        c.ns_per_posting_sweep *= scale[2];
+        if (post_form == 2) {   // the postings ran as the run sweep: its constant
+            c.ns_per_run_check *= scale[2];
+        } else {
+            c.ns_per_posting_pair *= scale[2];
+            c.ns_per_posting_pair_hbm *= scale[2];
+            c.ns_per_posting_sweep *= scale[2];
+        }
         c.ns_per_sweep_row_pair *= scale[2];
         if (out) {
             out[0] = scale[0];

@@ -47,7 +47,7 @@ static void compare(const char* name, const ChunkPack& a, const ChunkPack& b) {
         for (size_t r = 0; r < a.facts.size(); ++r) {
             const auto &x = a.facts[r], &y = b.facts[r];
             if (x.card != y.card || x.list_entries != y.list_entries || x.chunks != y.chunks ||
-                x.bitmap_chunks != y.bitmap_chunks || x.plain != y.plain) {
+                x.bitmap_chunks != y.bitmap_chunks || x.plain != y.plain || x.runs != y.runs) {
                 std::printf("facts: row %zu differs\n", r);
                 ++g_fail;
                 break;

@@ -595,3 +595,95 @@ def test_triangle_into_pageable_host_memory(sb):
         xf = st.last_transfer_ms()
         assert xf["upload_ms"] == 0.0 and xf["copy_back_bytes"] == tri * 4
         st.close()
+
+
+@pytest.mark.parametrize("universe,mean_len", [(1 << 20, 64), (1 << 24, 256), (1 << 26, 700)])
+def test_run_sweep_matches_oracle(sb, universe, mean_len):
+    """The run form of the postings (pieces of runs per bin, overlaps summed
+    in a row sweep), forced, on run-clustered rows plus rows that reach its
+    edge cases -- empty rows, single values, runs across chunk and bin
+    boundaries, scattered values, a row equal to another -- against the
+    oracle, every pair and the sum."""
+    sets = gen.run_sets(160, universe, 40, mean_len, universe % 1009)
+    g = gen.rng(universe % 97)
+    sets += [np.zeros(0, np.uint32), np.array([0], np.uint32), np.array([universe - 1], np.uint32),
+             np.arange(65536 - 300, 65536 + 300, dtype=np.uint32),
+             np.arange(0, min(universe, 1 << 18), 3, dtype=np.uint32),
+             np.unique(g.integers(0, universe, 4000)).astype(np.uint32), sets[3].copy()]
+    vals, offs = gen.to_csr(sets)
+    want, ws = ol.sets_matrix(vals, offs)
+    st = sb.Storm()
+    st.add_rows(vals, offs)
+    st.set_dense_block(0.0)
+    st.set_panel(0)
+    st.set_sparse_postings(4)
+    got, s = st.matrix()
+    assert st.last_postings_form() == 2
+    assert st.last_postings_rows() >= len(sets) // 2
+    assert s == ws
+    np.testing.assert_array_equal(got, want)
+    assert st.pairw_intersect_cardinality() == ws
+    st.close()
+
+
+def test_default_plan_takes_the_run_sweep_on_run_clustered_rows(sb):
+    """Config-4-shaped rows (Poisson runs of Geometric(256) length over 2^26):
+    the planner's own choice indexes runs, and the counts match the value
+    postings' forced on the same rows and the oracle on sampled rows."""
+    sets = gen.run_sets(1200, 1 << 26, 120, 256, 4242)
+    vals, offs = gen.to_csr(sets)
+    st = sb.Storm()
+    st.add_rows(vals, offs)
+    got, s = st.matrix()
+    assert st.last_postings_form() == 2
+    st.set_sparse_postings(3)
+    ref, s3 = st.matrix()
+    assert st.last_postings_form() == 1
+    assert s == s3
+    np.testing.assert_array_equal(got, ref)
+    n = len(sets)
+    pick = [0, 1, 599, n - 1]
+    sub_vals, sub_offs = gen.to_csr([sets[i] for i in pick])
+    want, _ = ol.sets_matrix(sub_vals, sub_offs)
+    iu = np.triu_indices(len(pick))
+    for k, (a, b) in enumerate(zip(iu[0], iu[1])):
+        i, j = pick[a], pick[b]
+        assert got[i * n - i * (i - 1) // 2 + (j - i)] == want[k], (i, j)
+    st.close()
+
+
+@pytest.mark.parametrize("universe", [1 << 20, 1 << 24])
+def test_run_sweep_with_bitmap_chunks(sb, universe):
+    """The run form over rows that also hold bitmap chunks (runs of set bits
+    cut at bin and word boundaries): long runs, half-dense chunks, a full
+    chunk, runs ending on a chunk's last bit, beside list rows -- every plain
+    row forced into the run sweep, against the oracle."""
+    g = gen.rng(universe % 101)
+    sets = gen.run_sets(90, universe, 30, 300, universe % 1013)
+    extra = []
+    for k in range(30):
+        v = set()
+        for _ in range(int(g.integers(1, 4))):
+            s0 = int(g.integers(0, universe - 9000))
+            v.update(range(s0, s0 + int(g.integers(4096, 9000))))          # a bitmap chunk or two
+        if k % 3 == 0:
+            c0 = int(g.integers(0, universe // 65536)) * 65536
+            v.update((c0 + np.flatnonzero(g.random(65536) < 0.5)).tolist())   # half-dense chunk
+        if k % 5 == 0:
+            c0 = int(g.integers(0, universe // 65536)) * 65536
+            v.update(range(c0, c0 + 65536))                                  # full chunk
+        if k % 7 == 0:
+            v.update(range(65536 - 5000, 65536 + 37))                         # ends past a chunk's last bit
+        extra.append(np.array(sorted(v), np.uint32))
+    sets += extra
+    vals, offs = gen.to_csr(sets)
+    want, ws = ol.sets_matrix(vals, offs)
+    st = sb.Storm()
+    st.add_rows(vals, offs)
+    st.set_sparse_postings(4)
+    got, s = st.matrix()
+    assert st.last_postings_form() == 2
+    assert st.last_postings_rows() == len(sets)
+    assert s == ws
+    np.testing.assert_array_equal(got, want)
+    st.close()
