@@ -198,7 +198,7 @@ enum PairMode : uint32_t {
 struct ChunkCostModel {
     double ns_per_shared_chunk = 0.086;
     double ns_per_lane_iteration = 0.0228;
-    double ns_per_tensor_bit = 1.3e-6;
+    double ns_per_tensor_bit = 0.7e-6;
     double ns_per_posting_pair = 0.05;       // one (pair, shared value) increment, output in L2
     double ns_per_posting_pair_hbm = 0.042;  // the same, output larger than L2
     double ns_per_posting_sweep = 0.016;     // the same in the row sweep (shared memory)
@@ -207,7 +207,7 @@ struct ChunkCostModel {
     double ns_per_panel_value = 0.05;        // transposed panel: one query value against one 2048-row block
     double ns_per_panel_pair = 0.005;        // transposed panel: one count written
     double ns_per_panel_byte = 1.0 / 6000.0; // transposed panel: expansion and transpose traffic
-    double ns_per_run_check = 0.02;          // run sweep: one bin entry read against one piece
+    double ns_per_run_check = 0.03;          // run sweep: one bin entry read against one piece
 };
 double chunk_self_pair_ns(const ChunkCostModel& m, const ChunkRowFacts& f, uint64_t slots);
 double tensor_pair_ns(const ChunkCostModel& m, uint64_t slots);
