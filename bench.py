@@ -1093,8 +1093,8 @@ def config45_forms(device, full_sweep=False):
     out["runs_2^26"] = forms_on(sb, sets, 1 << 26)
     out["runs_2^26"]["workload"] = "2048 rows over 2^26, Poisson(200) runs of Geometric(mean 256) length"
     sweep = {}
-    # N = 20000 (config 5b's row count) where the kernel layer's host packing
-    # of every representation stays within seconds; fewer rows beyond
+    # N = 20000 (config 5b's row count) where the kernel layer's per-pair
+    # cells finish within a minute; fewer rows beyond
     # (the default run keeps 1e-5 and 1e-3 at N = 20000 and 1e-2; --all-forms runs every density)
     grid = ((1e-6, 20000), (1e-5, 20000), (1e-4, 20000), (1e-3, 20000), (1e-2, 1024), (0.17, 256))
     for d, n in (grid if full_sweep else ((1e-5, 20000), (1e-3, 20000), (1e-2, 1024))):
