@@ -1240,6 +1240,32 @@ def storm_t_forms(device, cpu_seconds=2.0, only=None):
             ms = s.last_kernel_ms()
             best = ms if best is None else min(best, ms)
         res["gpu_default_sum_only_ms"] = round(best, 3)
+        # The planner against single-engine plans on the same rows: regret =
+        # default / the fastest plan measured - 1 (chunk kernel alone only
+        # where it finishes in seconds).
+        plans = {"tensor_rows_only": (1e-12, 0, 0), "panel_only": (-1.0, -1, 2), "postings_only": (0.0, 1, 0)}
+        if n <= 4096:
+            plans["chunk_kernel_only"] = (0.0, 0, 0)
+        plan_ms = {"default": res["gpu_default"]["ms"]}
+        for pname, (thr, post, pan) in plans.items():
+            s.set_dense_block(thr)
+            s.set_sparse_postings(post)
+            s.set_panel(pan)
+            best = None
+            for _ in range(2):
+                _, v = s.matrix(buf)
+                sums.add(v)
+                ms = s.last_kernel_ms()
+                best = ms if best is None else min(best, ms)
+                if best > 2000:
+                    break
+            plan_ms[pname] = round(best, 3)
+        s.set_dense_block(-1.0)
+        s.set_sparse_postings(-1)
+        s.set_panel(-1)
+        fastest = min(plan_ms, key=plan_ms.get)
+        res["plans"] = {"ms": plan_ms, "fastest": fastest,
+                        "default_regret": round(plan_ms["default"] / plan_ms[fastest] - 1.0, 4)}
         s.close()
         if len(sums) != 1:
             raise RuntimeError(f"{name}: forms disagree {sums}")

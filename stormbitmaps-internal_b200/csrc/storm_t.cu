@@ -554,16 +554,53 @@ int64_t STORM_add_bitmap_rows(STORM_t* s, const uint64_t* words, uint64_t n_rows
     }
     const uint32_t first = s->n_conts;
     std::atomic<int> failed{0};
+    // Chunk by chunk, what STORM_bitmap_cont_add builds from the row's set
+    // positions: no chunk without a set bit; a list below
+    // STORM_DEFAULT_SCALAR_THRESHOLD set bits (their positions); otherwise
+    // a bitmap, taken as the words themselves (STORM_bitmap_add on a fresh
+    // chunk sets exactly these bits and counts them).
     auto fill = [&](uint64_t r0, uint64_t r1) {
         std::vector<uint32_t> pos;
         for (uint64_t r = r0; r < r1; ++r) {
             const uint64_t* w = words + r * words_per_row;
-            pos.clear();
-            for (uint64_t k = 0; k < words_per_row; ++k)
-                for (uint64_t x = w[k]; x; x &= x - 1) pos.push_back((uint32_t)(k * 64 + __builtin_ctzll(x)));
-            if (STORM_bitmap_cont_add(&s->conts[first + r], pos.empty() ? nullptr : pos.data(),
-                                      (uint32_t)pos.size()) < 0 && !pos.empty())
-                failed.store(1);
+            STORM_bitmap_cont_t* c = &s->conts[first + r];
+            for (uint64_t k0 = 0; k0 < words_per_row; k0 += CHUNK_WORDS) {
+                const uint64_t kw = std::min<uint64_t>(CHUNK_WORDS, words_per_row - k0);
+                uint64_t cnt = 0, last_k = 0;
+                for (uint64_t k = 0; k < kw; ++k)
+                    if (w[k0 + k]) {
+                        cnt += (uint64_t)__builtin_popcountll(w[k0 + k]);
+                        last_k = k;
+                    }
+                if (cnt == 0) continue;
+                const uint32_t id = (uint32_t)(k0 / CHUNK_WORDS);
+                if (!cont_reserve(c, c->n_bitmaps + 1)) {
+                    failed.store(1);
+                    return;
+                }
+                STORM_bitmap_t* x = &c->bitmaps[c->n_bitmaps];
+                x->id = id;
+                c->block_ids[c->n_bitmaps] = id;
+                if (cnt < STORM_DEFAULT_SCALAR_THRESHOLD) {
+                    pos.clear();
+                    for (uint64_t k = 0; k < kw; ++k)
+                        for (uint64_t y = w[k0 + k]; y; y &= y - 1)
+                            pos.push_back((uint32_t)((k0 + k) * 64 + __builtin_ctzll(y)));
+                    if (STORM_bitmap_add_scalar_only(x, pos.data(), (uint32_t)pos.size()) < 0) {
+                        failed.store(1);
+                        return;
+                    }
+                } else {
+                    if (!ensure_data(x)) {
+                        failed.store(1);
+                        return;
+                    }
+                    std::memcpy(x->data, w + k0, kw * sizeof(uint64_t));
+                    x->n_bits_set += (uint32_t)cnt;
+                }
+                ++c->n_bitmaps;
+                c->prev_inserted_value = (uint32_t)((k0 + last_k) * 64 + 63 - __builtin_clzll(w[k0 + last_k]));
+            }
         }
     };
     const unsigned hw = host_threads();
