@@ -272,11 +272,12 @@ uint64_t STORM_last_dense_panels(const STORM_t* s);
  * used when the exact increment count predicts less time than the chunk
  * kernel; 1: whenever rows qualify; 0: never.  Per-pair counts take one of
  * two forms: the increments go list by list into the output, or -- for
- * outputs larger than L2, at most 51200 postings rows, and when predicted
- * faster from the exact increment count -- a row sweep counts each row's
- * partners in shared memory and writes its slice once.  A third per-pair
- * form indexes runs instead of values (at most 51200 postings rows): the
- * universe is cut into bins of a power of two near the rows' mean run
+ * outputs larger than L2, and when predicted faster from the exact
+ * increment count -- a row sweep counts each row's partners in shared
+ * memory (in blocks of 51200 partner rows, reading the row's lists once per
+ * block) and writes its slice once.  A third per-pair form indexes runs
+ * instead of values: the universe is cut into bins of a power of two near
+ * the rows' mean run
  * length, each row's maximal runs into pieces per bin, and a row sweep adds
  * the overlaps of a row's pieces with the pieces of later rows in the same
  * bins -- rows made of long runs then cost per run, not per value; it is

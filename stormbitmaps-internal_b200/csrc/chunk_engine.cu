@@ -949,7 +949,11 @@ __global__ void postings_pairs_kernel(const uint2* __restrict__ lists, uint64_t 
 // ascending order. The row's entries are split evenly over the threads (a
 // shared-memory prefix of its chunk lengths maps entry -> chunk), so rows of
 // one long chunk and rows of many short ones both keep every thread busy.
-// Shared memory: nq counters, then up to POST_SWEEP_MAX_CHUNKS + 1 prefix
+// Partners are counted for one block of local indices [pb0, pb0 + pbn) per
+// launch (at most POST_SWEEP_MAX_ROWS, the counters shared memory holds):
+// more postings rows take one launch per block, each reading a row's lists
+// again; the launch of block 0 writes the diagonal.
+// Shared memory: pbn counters, then up to POST_SWEEP_MAX_CHUNKS + 1 prefix
 // words. Lists hold local indices, list x is [end[x] - counts[x], end[x]).
 constexpr uint32_t POST_SWEEP_THREADS = 256;
 constexpr uint32_t POST_SWEEP_MAX_CHUNKS = 2048;  // universe <= 2^27
@@ -958,14 +962,16 @@ constexpr uint32_t POST_SWEEP_MAX_ROWS = 51200;   // 200 KiB of counters + 8 KiB
 __global__ void __launch_bounds__(POST_SWEEP_THREADS)
 postings_rows_kernel(ChunkView v, const uint32_t* __restrict__ qrows, uint32_t nq, const uint32_t* __restrict__ counts,
                      const uint32_t* __restrict__ end, const uint32_t* __restrict__ post, uint64_t n,
-                     uint32_t* __restrict__ out) {
+                     uint32_t* __restrict__ out, uint32_t pb0, uint32_t pbn) {
     extern __shared__ uint32_t cnt[];
-    uint32_t* pref = cnt + nq;                 // pref[k] = entries of the row's chunks before chunk k
+    uint32_t* pref = cnt + pbn;                // pref[k] = entries of the row's chunks before chunk k
+    const uint32_t pb1 = pb0 + pbn;
     for (uint32_t a = blockIdx.x; a < nq; a += gridDim.x) {
+        if (a + 1 >= pb1 && pb0 > 0) continue;     // no partner after a in this block, diagonal not here
         const uint32_t row = qrows[a];
         const uint64_t c0 = v.row_off[row];
         const uint32_t nc = (uint32_t)(v.row_off[row + 1] - c0);   // <= POST_SWEEP_MAX_CHUNKS (plain rows)
-        for (uint32_t b = threadIdx.x; b < nq; b += blockDim.x) cnt[b] = 0;
+        for (uint32_t b = threadIdx.x; b < pbn; b += blockDim.x) cnt[b] = 0;
         if (threadIdx.x == 0) {
             uint32_t acc = 0;
             for (uint32_t k = 0; k < nc; ++k) {
@@ -976,7 +982,8 @@ postings_rows_kernel(ChunkView v, const uint32_t* __restrict__ qrows, uint32_t n
         }
         __syncthreads();
         const uint32_t total = pref[nc];
-        for (uint32_t e = threadIdx.x; e < total; e += blockDim.x) {
+        const uint32_t work = a + 1 < pb1 ? total : 0u;   // no partner in the block: the diagonal only
+        for (uint32_t e = threadIdx.x; e < work; e += blockDim.x) {
             uint32_t lo = 0, hi = nc;              // last chunk k with pref[k] <= e
             while (hi - lo > 1) {
                 const uint32_t mid = (lo + hi) >> 1;
@@ -990,16 +997,16 @@ postings_rows_kernel(ChunkView v, const uint32_t* __restrict__ qrows, uint32_t n
             const uint32_t e1 = end[x];
             for (uint32_t k = e1 - len; k < e1; ++k) {
                 const uint32_t b = post[k];
-                if (b > a) atomicAdd(&cnt[b], 1u);
+                if (b > a && b >= pb0 && b < pb1) atomicAdd(&cnt[b - pb0], 1u);
             }
         }
         __syncthreads();
         const uint64_t base = tri_index(n, row, row) - row;   // out index of (row, j) is base + j
-        for (uint32_t b = a + 1 + threadIdx.x; b < nq; b += blockDim.x) {
+        for (uint32_t b = (a + 1 > pb0 ? a + 1 : pb0) + threadIdx.x; b < pb1; b += blockDim.x) {
             const uint32_t gb = qrows[b];   // ascending: gb > row (the other order kept exact too)
-            out[gb > row ? base + gb : tri_index(n, gb, row)] = cnt[b];
+            out[gb > row ? base + gb : tri_index(n, gb, row)] = cnt[b - pb0];
         }
-        if (threadIdx.x == 0) out[base + row] = total;
+        if (threadIdx.x == 0 && pb0 == 0) out[base + row] = total;
         __syncthreads();
     }
 }
@@ -1187,23 +1194,26 @@ __global__ void run_scatter_kernel(uint32_t nq, uint32_t wlog, const uint64_t* _
 
 // The row sweep over pieces: CTA per row a; the (piece, bin entry) pairs of
 // a batch of a's pieces are split evenly over the threads (a shared-memory
-// prefix of the pieces' bin lengths maps work index -> piece). Shared
-// memory: nq counters, then RUN_SWEEP_BATCH + 1 prefix words. Bin b's list
-// is [end[b] - bins[b], end[b]). Adds the sum over a's partners after it to
-// flags->sum.
+// prefix of the pieces' bin lengths maps work index -> piece). Partners in
+// one block of local indices [pb0, pb0 + pbn) per launch, as in
+// postings_rows_kernel. Shared memory: pbn counters, then RUN_SWEEP_BATCH + 1
+// prefix words. Bin b's list is [end[b] - bins[b], end[b]). Adds the sum
+// over a's partners after it (in the block) to flags->sum.
 __global__ void __launch_bounds__(POST_SWEEP_THREADS)
 run_sweep_kernel(const uint32_t* __restrict__ qrows, uint32_t nq, const uint64_t* __restrict__ poff,
                  const uint2* __restrict__ pieces, uint32_t wlog, const uint32_t* __restrict__ bins,
                  const uint32_t* __restrict__ end, const uint2* __restrict__ list, uint64_t n,
-                 uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags) {
+                 uint32_t* __restrict__ out, DeviceFlags* __restrict__ flags, uint32_t pb0, uint32_t pbn) {
     extern __shared__ uint32_t cnt[];
-    uint32_t* pref = cnt + nq;
+    uint32_t* pref = cnt + pbn;
+    const uint32_t pb1 = pb0 + pbn;
     __shared__ uint32_t warp_tot[POST_SWEEP_THREADS / 32];
     __shared__ unsigned long long row_card;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (uint32_t a = blockIdx.x; a < nq; a += gridDim.x) {
+        if (a + 1 >= pb1 && pb0 > 0) continue;     // no partner after a in this block, diagonal not here
         const uint32_t row = qrows[a];
-        for (uint32_t b = threadIdx.x; b < nq; b += blockDim.x) cnt[b] = 0;
+        for (uint32_t b = threadIdx.x; b < pbn; b += blockDim.x) cnt[b] = 0;
         if (threadIdx.x == 0) row_card = 0;
         const uint64_t p0 = poff[a], np = poff[a + 1] - p0;
         unsigned long long card = 0;
@@ -1242,7 +1252,8 @@ run_sweep_kernel(const uint32_t* __restrict__ qrows, uint32_t nq, const uint64_t
             }
             if (threadIdx.x == 0) pref[m] = total;
             __syncthreads();
-            for (uint32_t t = threadIdx.x; t < total; t += blockDim.x) {
+            const uint32_t work = a + 1 < pb1 ? total : 0u;   // no partner in the block: the diagonal only
+            for (uint32_t t = threadIdx.x; t < work; t += blockDim.x) {
                 uint32_t lo = 0, hi = m;           // last piece k with pref[k] <= t
                 while (hi - lo > 1) {
                     const uint32_t mid = (lo + hi) >> 1;
@@ -1252,11 +1263,11 @@ run_sweep_kernel(const uint32_t* __restrict__ qrows, uint32_t nq, const uint64_t
                 const uint2 pc = pieces[p0 + pb + lo];
                 const uint32_t bin = pc.x >> wlog;
                 const uint2 E = list[end[bin] - bins[bin] + (t - pref[lo])];
-                if (E.x > a) {
+                if (E.x > a && E.x >= pb0 && E.x < pb1) {
                     const uint32_t b0 = bin << wlog;
                     const uint32_t s2 = b0 + (E.y & 0xFFFFu), e2 = b0 + (E.y >> 16);
                     const uint32_t s = pc.x > s2 ? pc.x : s2, e = pc.y < e2 ? pc.y : e2;
-                    if (e > s) atomicAdd(&cnt[E.x], e - s);
+                    if (e > s) atomicAdd(&cnt[E.x - pb0], e - s);
                 }
             }
         }
@@ -1265,14 +1276,14 @@ run_sweep_kernel(const uint32_t* __restrict__ qrows, uint32_t nq, const uint64_t
         __syncthreads();
         const uint64_t base = tri_index(n, row, row) - row;   // out index of (row, j) is base + j
         unsigned long long sum = 0;
-        for (uint32_t b = a + 1 + threadIdx.x; b < nq; b += blockDim.x) {
+        for (uint32_t b = (a + 1 > pb0 ? a + 1 : pb0) + threadIdx.x; b < pb1; b += blockDim.x) {
             const uint32_t gb = qrows[b];
-            out[gb > row ? base + gb : tri_index(n, gb, row)] = cnt[b];
-            sum += cnt[b];
+            out[gb > row ? base + gb : tri_index(n, gb, row)] = cnt[b - pb0];
+            sum += cnt[b - pb0];
         }
         sum = warp_sum_u64(sum);
         if (lane == 0 && sum) atomicAdd(&flags->sum, sum);
-        if (threadIdx.x == 0) out[base + row] = (uint32_t)row_card;
+        if (threadIdx.x == 0 && pb0 == 0) out[base + row] = (uint32_t)row_card;
         __syncthreads();
     }
 }
@@ -1511,11 +1522,14 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
     // (partners counted in shared memory, each output written once).
     const bool big_out = tri_size(n) * sizeof(uint32_t) > L2_BYTES_B200;
     const double c_list = big_out ? cost.ns_per_posting_pair_hbm : cost.ns_per_posting_pair;
+    // The row sweeps count partners in blocks of POST_SWEEP_MAX_ROWS rows,
+    // reading each row's lists (or bins) once per block.
+    auto sweep_blocks = [&](uint64_t q) { return (double)((q + POST_SWEEP_MAX_ROWS - 1) / POST_SWEEP_MAX_ROWS); };
     auto sweep_ns = [&](double incr, uint64_t q) {
-        return (double)q * (double)q * cost.ns_per_sweep_row_pair + incr * cost.ns_per_posting_sweep;
+        return (double)q * (double)q * cost.ns_per_sweep_row_pair + incr * cost.ns_per_posting_sweep * sweep_blocks(q);
     };
     auto sweep_form = [&](double incr, uint64_t q) {
-        if (q > POST_SWEEP_MAX_ROWS || postings_mode == 2) return false;
+        if (postings_mode == 2) return false;
         return postings_mode == 3 || (big_out && sweep_ns(incr, q) < incr * c_list);
     };
     // ns of the postings for a set of q rows with incr increments (sums need
@@ -1526,11 +1540,11 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
     };
     // ns of the run sweep with `checks` entry reads for q rows (per pair only)
     auto run_ns = [&](double checks, uint64_t q) {
-        return (double)q * (double)q * cost.ns_per_sweep_row_pair + checks * cost.ns_per_run_check +
+        return (double)q * (double)q * cost.ns_per_sweep_row_pair + checks * cost.ns_per_run_check * sweep_blocks(q) +
                (double)n_bins * cost.ns_per_universe_value;
     };
     auto run_ok = [&](uint64_t q) {
-        return d_out != nullptr && q <= POST_SWEEP_MAX_ROWS && postings_mode != 2 && postings_mode != 3;
+        return d_out != nullptr && q >= 2 && postings_mode != 2 && postings_mode != 3;
     };
     std::vector<uint32_t> qrows, dense, mrows;             // L, H, M
     // L x L for `rest` (plain rows without bitmap chunks) by postings when
@@ -2002,12 +2016,17 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
         run_scatter_kernel<<<gq, 256, 0, st>>>((uint32_t)nq, rwlog, d_rpoff.p, d_pieces.p, d_rstart.p, d_rlist.p);
         static std::atomic<uint64_t> done{0};
         smem_attr_once(run_sweep_kernel, (int)((POST_SWEEP_MAX_ROWS + RUN_SWEEP_BATCH + 1) * sizeof(uint32_t)), done);
-        const uint32_t smem = (uint32_t)((nq + RUN_SWEEP_BATCH + 1) * sizeof(uint32_t));
         const uint32_t gr = (uint32_t)std::min<uint64_t>(nq, (uint64_t)sms * 8);
-        run_sweep_kernel<<<gr, POST_SWEEP_THREADS, smem, st>>>(d_qrows.p, (uint32_t)nq, d_rpoff.p, d_pieces.p, rwlog,
-                                                               d_rbins.p, d_rstart.p, d_rlist.p, n, d_out, d_flags.p);
+        for (uint64_t pb0 = 0; pb0 < nq; pb0 += POST_SWEEP_MAX_ROWS) {
+            const uint32_t pbn = (uint32_t)std::min<uint64_t>(POST_SWEEP_MAX_ROWS, nq - pb0);
+            const uint32_t smem = (uint32_t)((pbn + RUN_SWEEP_BATCH + 1) * sizeof(uint32_t));
+            run_sweep_kernel<<<gr, POST_SWEEP_THREADS, smem, st>>>(d_qrows.p, (uint32_t)nq, d_rpoff.p, d_pieces.p,
+                                                                   rwlog, d_rbins.p, d_rstart.p, d_rlist.p, n, d_out,
+                                                                   d_flags.p, (uint32_t)pb0, pbn);
+            ++launches;
+        }
         SB_CUDA(cudaGetLastError());
-        launches += 4;
+        launches += 3;
         last_postings_rows = nq;
     } else if (nq) {
         q_sum = ps.pairs;
@@ -2021,14 +2040,18 @@ uint64_t ChunkEngine::run(const ChunkDev& d, PairMode mode, uint64_t n1, uint64_
             const uint32_t gq = (uint32_t)std::min<uint64_t>((nq + 7) / 8, (uint64_t)sms * 16);
             postings_scatter_kernel<<<gq, 256, 0, st>>>(d.view(), d_qrows.p, (uint32_t)nq, d_start.p, d_post.p);
             if (sweep) {
-                const uint32_t smem = (uint32_t)((nq + POST_SWEEP_MAX_CHUNKS + 1) * sizeof(uint32_t));
                 static std::atomic<uint64_t> done{0};
                 smem_attr_once(postings_rows_kernel,
                                (int)((POST_SWEEP_MAX_ROWS + POST_SWEEP_MAX_CHUNKS + 1) * sizeof(uint32_t)), done);
                 const uint32_t gr = (uint32_t)std::min<uint64_t>(nq, (uint64_t)sms * 8);
-                postings_rows_kernel<<<gr, POST_SWEEP_THREADS, smem, st>>>(d.view(), d_qrows.p, (uint32_t)nq,
-                                                                           d_counts.p, d_start.p, d_post.p, n, d_out);
-                launches += 3;
+                for (uint64_t pb0 = 0; pb0 < nq; pb0 += POST_SWEEP_MAX_ROWS) {
+                    const uint32_t pbn = (uint32_t)std::min<uint64_t>(POST_SWEEP_MAX_ROWS, nq - pb0);
+                    const uint32_t smem = (uint32_t)((pbn + POST_SWEEP_MAX_CHUNKS + 1) * sizeof(uint32_t));
+                    postings_rows_kernel<<<gr, POST_SWEEP_THREADS, smem, st>>>(
+                        d.view(), d_qrows.p, (uint32_t)nq, d_counts.p, d_start.p, d_post.p, n, d_out, (uint32_t)pb0, pbn);
+                    ++launches;
+                }
+                launches += 2;
             } else {
                 const uint32_t gp = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((ps.lists + 255) / 256,
                                                                                        (uint64_t)sms * 16));

@@ -687,3 +687,44 @@ def test_run_sweep_with_bitmap_chunks(sb, universe):
     assert s == ws
     np.testing.assert_array_equal(got, want)
     st.close()
+
+
+def test_row_sweeps_beyond_one_partner_block(sb):
+    """More postings rows than the row sweeps' shared-memory counters hold
+    (51200): partners are counted block by block. 60000 sparse rows (about
+    168 values each over 2^24, plus empty rows) by the value row sweep, the
+    run sweep and the list-by-list form -- three independent code paths --
+    agree on every pair; the diagonal is the cardinalities and the sum the
+    value-histogram identity."""
+    import torch
+    n, U = 60000, 1 << 24
+    g = np.random.default_rng(60000)
+    cards = g.binomial(U, 1e-5, size=n)
+    cards[::997] = 0
+    draws = g.integers(0, U, size=int(cards.sum()), dtype=np.uint64).astype(np.uint32)
+    ends = np.cumsum(cards)
+    sets = [np.unique(draws[e - c:e]) for c, e in zip(cards, ends)]
+    vals, offs = gen.to_csr(sets)
+    st = sb.Storm()
+    st.add_rows(vals, offs)
+    st.set_dense_block(0.0)
+    st.set_panel(0)
+    tri = n * (n + 1) // 2
+    got = {}
+    for mode, form in ((3, 1), (4, 2), (2, 0)):
+        st.set_sparse_postings(mode)
+        d = torch.full((tri,), -1, dtype=torch.int32, device="cuda")
+        s = st.matrix_device(d.data_ptr(), tri)
+        assert st.last_postings_form() == form
+        assert st.last_postings_rows() == n
+        got[mode] = (s, d)
+    hist = np.bincount(vals, minlength=U).astype(np.int64)
+    want_sum = int((hist * (hist - 1) // 2).sum())
+    for mode in (3, 4, 2):
+        assert got[mode][0] == want_sum, mode
+    assert torch.equal(got[3][1], got[2][1])
+    assert torch.equal(got[4][1], got[2][1])
+    ii = torch.arange(n, device="cuda", dtype=torch.int64)
+    diag = got[2][1][ii * n - ii * (ii - 1) // 2].cpu().numpy()
+    np.testing.assert_array_equal(diag, [len(x) for x in sets])
+    st.close()
