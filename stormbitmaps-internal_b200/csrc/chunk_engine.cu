@@ -10,6 +10,7 @@
 #include "dense.cuh"
 #include "list16_ref.cuh"
 #include "panel.cuh"
+#include "run_pieces.cuh"
 
 namespace sb200 {
 
@@ -1021,27 +1022,8 @@ postings_rows_kernel(ChunkView v, const uint32_t* __restrict__ qrows, uint32_t n
 // value postings (histogram, allocation, scatter); then a row sweep: a CTA
 // per row, for each of its pieces the entries of the piece's bin, overlaps
 // with rows after it added in shared memory, its triangle slice written once.
+// The piece rules: run_pieces.cuh.
 constexpr uint32_t RUN_SWEEP_BATCH = 2048;   // pieces prefixed in shared memory at once
-
-__device__ __forceinline__ bool run_piece_start(const uint16_t* l, uint32_t e, uint32_t wmask) {
-    return e == 0 || l[e] != l[e - 1] + 1 || (l[e] & wmask) == 0;
-}
-
-__device__ __forceinline__ bool run_piece_last(const uint16_t* l, uint32_t e, uint32_t nl, uint32_t wmask) {
-    return e + 1 == nl || l[e + 1] != l[e] + 1 || ((l[e] + 1u) & wmask) == 0;
-}
-
-// In a bitmap chunk, per word (index `word` inside the chunk): the bits
-// where a bin starts and where one ends (bins of 2^wlog >= 16 bits).
-__device__ __forceinline__ uint64_t run_bin_first_bits(uint32_t word, uint32_t wlog) {
-    if (wlog >= 6) return ((word << 6) & ((1u << wlog) - 1u)) == 0 ? 1ull : 0ull;
-    return wlog == 4 ? 0x0001000100010001ull : 0x0000000100000001ull;
-}
-
-__device__ __forceinline__ uint64_t run_bin_last_bits(uint32_t word, uint32_t wlog) {
-    if (wlog >= 6) return (((word + 1) << 6) & ((1u << wlog) - 1u)) == 0 ? (1ull << 63) : 0ull;
-    return wlog == 4 ? 0x8000800080008000ull : 0x8000000080000000ull;
-}
 
 // Word wi of a bitmap chunk held by this lane (a warp walks the chunk 32
 // words at a time, `carry` = bit 63 of the word before the warp's first):
@@ -1055,8 +1037,7 @@ __device__ __forceinline__ void run_bitmap_word(const uint64_t* wd, uint32_t nwc
     const uint64_t cin = lane ? prev >> 63 : carry;
     const uint64_t nin = lane < 31 ? next & 1ull : (w0 + 32 < nwc ? wd[w0 + 32] & 1ull : 0ull);
     carry = __shfl_sync(0xffffffffu, x, 31) >> 63;
-    starts = (x & ~((x << 1) | cin)) | (x & run_bin_first_bits(wi, wlog));
-    lasts = (x & ~((x >> 1) | (nin << 63))) | (x & run_bin_last_bits(wi, wlog));
+    run_word_masks(x, cin, nin, wi, wlog, starts, lasts);
 }
 
 // Pieces per row and per bin; warp per row.
