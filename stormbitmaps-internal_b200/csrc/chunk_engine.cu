@@ -259,6 +259,14 @@ void PinnedStage::ensure() {
     SB_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
 }
 
+// Waits for a lane's stream when a worker leaves, also by an exception, so
+// that no copy of a failed call still reads or writes the lane's buffers
+// when the next call fills them.
+struct LaneSync {
+    cudaStream_t st;
+    ~LaneSync() { cudaStreamSynchronize(st); }
+};
+
 // Runs fn(t) for t in [0, workers) on that many host threads (t = 0 on the
 // calling thread) and rethrows the first failure after all have ended.
 template <class F>
@@ -460,6 +468,7 @@ void ChunkDev::upload_rows(const STORM_bitmap_cont_t* rows, uint64_t n, cudaStre
     const uint64_t cap = stage.lane_bytes;
     run_workers(workers, [&](unsigned t) {
         PinnedStage::Lane& L = stage.lanes[t];
+        const LaneSync lane_sync{L.st};
         SB_CUDA(cudaStreamWaitEvent(L.st, stage.ready, 0));
         uint64_t r = cut[t], k = 0;
         const uint64_t r_end = cut[t + 1];
@@ -563,8 +572,10 @@ void copy_to_host(uint32_t* out, const uint32_t* d_src, uint64_t count, cudaStre
     const uint64_t bytes = count * sizeof(uint32_t);
     if (bytes == 0) return;
     cudaPointerAttributes a{};
-    const bool pinned = cudaPointerGetAttributes(&a, out) == cudaSuccess && a.type == cudaMemoryTypeHost;
+    const bool known = cudaPointerGetAttributes(&a, out) == cudaSuccess;
     cudaGetLastError();   // an attribute query of plain host memory may leave an error behind
+    if (known && a.type == cudaMemoryTypeDevice) fail(STORM_B200_EARG, "the host output buffer is device memory");
+    const bool pinned = known && a.type == cudaMemoryTypeHost;
     if (pinned || bytes < (32u << 20)) {
         SB_CUDA(cudaMemcpyAsync(out, d_src, bytes, cudaMemcpyDeviceToHost, st));
         SB_CUDA(cudaStreamSynchronize(st));
@@ -577,6 +588,7 @@ void copy_to_host(uint32_t* out, const uint32_t* d_src, uint64_t count, cudaStre
     SB_CUDA(cudaEventRecord(stage.ready, st));
     run_workers(workers, [&](unsigned t) {
         PinnedStage::Lane& L = stage.lanes[t];
+        const LaneSync lane_sync{L.st};
         SB_CUDA(cudaStreamWaitEvent(L.st, stage.ready, 0));
         const uint64_t lo = count * t / workers, hi = count * (t + 1) / workers;
         auto issue = [&](uint64_t x, int b) {

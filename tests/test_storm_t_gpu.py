@@ -728,3 +728,25 @@ def test_row_sweeps_beyond_one_partner_block(sb):
     diag = got[2][1][ii * n - ii * (ii - 1) // 2].cpu().numpy()
     np.testing.assert_array_equal(diag, [len(x) for x in sets])
     st.close()
+
+
+def test_host_output_call_refuses_device_memory(sb):
+    """The per-pair call that copies the triangle into host memory returns
+    STORM_B200_EARG, without writing, when the buffer it is given is device
+    memory (the device form is STORM_pairw_intersect_matrix_device)."""
+    import ctypes as C
+    import torch
+    sets = gen.zipf_sets(300, 1 << 20, 1.1, 16, 1 << 15, 5)
+    vals, offs = gen.to_csr(sets)
+    st = sb.Storm()
+    st.add_rows(vals, offs)
+    tri = 300 * 301 // 2
+    d = torch.zeros(tri, dtype=torch.int32, device="cuda")
+    s = C.c_uint64(0)
+    rc = sb.lib().STORM_pairw_intersect_matrix(st.h, C.cast(d.data_ptr(), sb.u32p), tri, C.byref(s))
+    assert rc == sb.EARG
+    assert int(d.abs().sum().item()) == 0
+    got, _ = st.matrix()   # the container still works
+    want, _ = ol.sets_matrix(vals, offs)
+    np.testing.assert_array_equal(got, want)
+    st.close()
