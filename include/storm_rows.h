@@ -88,6 +88,9 @@ uint32_t STORM_rows_universe(const STORM_rows_t* r);
  * memory).  Rows that do not get a bitmap behave like the reference's
  * sparse_only rows (storm_repr.h:280-291): no B, no rank, no zone map. */
 int STORM_rows_set_bitmap_budget(STORM_rows_t* r, uint64_t bytes);
+/* Copies the rows' positions to the device and builds every representation
+ * there (storm::build_row's rules, storm_repr.cpp:25-207); the all-pairs
+ * calls do it themselves after rows change. */
 int STORM_rows_upload(STORM_rows_t* r);
 /* A new STORM_rows_t (universe = the file's n_bits) holding the rows of a
  * STORMBIN corpus file; same format, stride and max_rows rules and errors
