@@ -215,3 +215,37 @@ def test_oracle_catches_a_planted_mistake(golden):
     words[3, 5] ^= np.uint64(1 << 17)
     mat, _ = ol.contig_matrix(words)
     assert not np.array_equal(mat, golden["contig/dense_1024/matrix"])
+
+
+@pytest.mark.parametrize("shape", ["runs_2^20", "runs_2^24_long", "runs_across_chunks", "zipf_2^20", "mixed"])
+def test_oracle_sets_fuzzed_against_reference_build(shape):
+    """Beyond the golden vectors: the oracle's per-pair set counts (the
+    checker of every STORM_t engine, the run postings included) against the
+    reference built here from its sources (oracle/_ref, STORM_t through its
+    own STORM_add and STORM_pairw_intersect_cardinality per pair) on seeded
+    run-clustered, Zipf and mixed corpora. Skipped without oracle/_ref."""
+    R = ol.reference()
+    if R is None:
+        pytest.skip("reference library not built (oracle/_ref)")
+    seed = sum(map(ord, shape))
+    if shape == "runs_2^20":
+        sets = gen.run_sets(60, 1 << 20, 20, 64, seed)
+    elif shape == "runs_2^24_long":
+        sets = gen.run_sets(40, 1 << 24, 30, 2000, seed)
+    elif shape == "runs_across_chunks":
+        g = gen.rng(seed)
+        sets = [np.arange(65536 * k - int(g.integers(1, 5000)), 65536 * k + int(g.integers(1, 5000)),
+                          dtype=np.uint32) for k in range(1, 30)]
+    elif shape == "zipf_2^20":
+        sets = gen.zipf_sets(60, 1 << 20, 1.1, 16, 1 << 18, seed)
+    else:
+        sets = (gen.run_sets(20, 1 << 22, 10, 500, seed) + gen.zipf_sets(20, 1 << 22, 1.1, 16, 1 << 16, seed) +
+                [np.zeros(0, np.uint32), np.array([0], np.uint32)])
+    vals, offs = gen.to_csr(sets)
+    n = len(sets)
+    want, ws = ol.sets_matrix(vals, offs)
+    ref = np.zeros(n * (n + 1) // 2, np.uint32)
+    assert R.ref_storm_matrix(P(vals, ol.u32p), P(offs, ol.u64p), n, P(ref, ol.u32p)) == ws
+    iu = np.triu_indices(n)
+    strict = iu[0] != iu[1]
+    np.testing.assert_array_equal(want[strict], ref[strict])
