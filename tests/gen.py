@@ -152,3 +152,28 @@ def repeat_corpus(seed: int):
             v = uniform_set(g, int(g.integers(13000, 30000)), 3 << 16)
         sets.append(np.asarray(v, dtype=np.uint32))
     return sets
+
+
+def segmentation_rows(u: int, g):
+    """Rows over [0, u) that reach each EWAH-64 segmentation case (empty and
+    full rows, full words at the first and last word, full runs beside
+    literals and zero gaps, partial last words, several densities, runs)."""
+    nw = (u + 63) // 64
+    full = lambda w: list(range(64 * w, min(64 * w + 64, u)))
+    rows = [[], list(range(u)), [0], [u - 1], full(0), full(nw - 1) if u % 64 == 0 else [u - 1, u - 2],
+            full(0) + [70, 80] + full(3) + full(4) + [64 * 6 + 1] + full(7)]
+    # alternating full words, literals and gaps, at random
+    v = []
+    for w in range(nw):
+        t = g.integers(0, 4)
+        if t == 1:
+            v += full(w)
+        elif t == 2:
+            v += sorted(set(int(x) for x in g.integers(64 * w, min(64 * w + 64, u), size=5)))
+    rows.append(v)
+    # long runs of full words ending in literals and the partial last word
+    rows.append(list(range(0, min(u, 64 * 40 + 17))) + list(range(max(0, u - 100), u)))
+    for d in (0.0005, 0.02, 0.3, 0.5, 0.9, 0.999):
+        rows.append(np.flatnonzero(g.random(u) < d).tolist())
+    rows += [x.tolist() for x in run_sets(6, u, 30, 600, int(g.integers(1 << 30)))]
+    return [np.array(sorted(set(x for x in r if 0 <= x < u)), np.uint32) for r in rows]

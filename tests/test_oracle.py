@@ -249,3 +249,57 @@ def test_oracle_sets_fuzzed_against_reference_build(shape):
     iu = np.triu_indices(n)
     strict = iu[0] != iu[1]
     np.testing.assert_array_equal(want[strict], ref[strict])
+
+
+@pytest.mark.parametrize("u", [64, 100, 4103, 65536, (1 << 20) + 13])
+def test_oracle_representations_fuzzed_against_reference_build(u):
+    """The oracle's builders (runs, EWAH-64, rank9, zone map, complement,
+    RowMeta) -- the checker of the device-built representations -- against
+    the reference's own storm::build_row (oracle/_ref) on rows that reach
+    every EWAH segmentation case, beyond the golden rows. Skipped without
+    oracle/_ref."""
+    R = ol.reference()
+    if R is None:
+        pytest.skip("reference library not built (oracle/_ref)")
+    O = ol.oracle()
+    nw = (u + 63) // 64
+    for v in gen.segmentation_rows(u, gen.rng(u + 7)):
+        v = np.ascontiguousarray(v, np.uint32)
+        rs = np.zeros(v.size + 1, np.uint32)
+        re = np.zeros(v.size + 1, np.uint32)
+        ew = np.zeros(2 * nw + 2, np.uint64)
+        rk = np.zeros(2 * ((nw + 7) // 8 + 1) + 2, np.uint64)
+        oc = np.zeros((((nw + 7) // 8) + 63) // 64 + 1, np.uint64)
+        cp = np.zeros(max(u, 1), np.uint32)
+        sizes = np.zeros(6, np.uint64)
+        meta = np.zeros(8, np.uint32)
+        R.ref_build_row(P(v, ol.u32p), v.size, u, P(rs, ol.u32p), P(re, ol.u32p), P(ew, ol.u64p), P(rk, ol.u64p),
+                        P(oc, ol.u64p), P(cp, ol.u32p), P(sizes, ol.u64p), P(meta, ol.u32p))
+        tag = f"u={u} card={v.size}"
+        ors = np.zeros(v.size + 1, np.uint32)
+        ore = np.zeros(v.size + 1, np.uint32)
+        k = O.oracle_runs(P(v, ol.u32p), v.size, P(ors, ol.u32p), P(ore, ol.u32p))
+        assert k == sizes[0], tag
+        np.testing.assert_array_equal(ors[:k], rs[:k], err_msg=tag)
+        np.testing.assert_array_equal(ore[:k], re[:k], err_msg=tag)
+        bm = gen.sets_to_rows([v], u)[0][:nw].copy()
+        oew = np.zeros(2 * nw + 2, np.uint64)
+        kw = O.oracle_ewah(P(bm, ol.u64p), nw, P(oew, ol.u64p))
+        assert kw == sizes[1], tag
+        np.testing.assert_array_equal(oew[:kw], ew[:kw], err_msg=tag)
+        om = np.zeros(8, np.uint32)
+        O.oracle_row_meta(P(v, ol.u32p), v.size, u, P(om, ol.u32p))
+        np.testing.assert_array_equal(om, meta, err_msg=tag)
+        if sizes[2]:
+            ork = np.zeros(2 * ((nw + 7) // 8 + 1), np.uint64)
+            O.oracle_rank9(P(bm, ol.u64p), nw, P(ork, ol.u64p))
+            np.testing.assert_array_equal(ork, rk[:int(sizes[2])], err_msg=tag)
+        if sizes[3]:
+            ooc = np.zeros(int(sizes[3]), np.uint64)
+            O.oracle_occ(P(bm, ol.u64p), nw, 8, P(ooc, ol.u64p))
+            np.testing.assert_array_equal(ooc, oc[:int(sizes[3])], err_msg=tag)
+        if sizes[4]:
+            ocp = np.zeros(max(u, 1), np.uint32)
+            kc = O.oracle_complement(P(v, ol.u32p), v.size, u, P(ocp, ol.u32p))
+            assert kc == sizes[4], tag
+            np.testing.assert_array_equal(ocp[:kc], cp[:kc], err_msg=tag)

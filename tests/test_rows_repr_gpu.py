@@ -107,33 +107,10 @@ def test_device_build_matches_reference_build_row(sb, golden):
         r.close()
 
 
-def _segmentation_rows(u, g):
-    """Rows that reach each EWAH case at universe u."""
-    nw = (u + 63) // 64
-    full = lambda w: list(range(64 * w, min(64 * w + 64, u)))
-    rows = [[], list(range(u)), [0], [u - 1], full(0), full(nw - 1) if u % 64 == 0 else [u - 1, u - 2],
-            full(0) + [70, 80] + full(3) + full(4) + [64 * 6 + 1] + full(7)]
-    # alternating full words, literals and gaps, at random
-    v = []
-    for w in range(nw):
-        t = g.integers(0, 4)
-        if t == 1:
-            v += full(w)
-        elif t == 2:
-            v += sorted(set(int(x) for x in g.integers(64 * w, min(64 * w + 64, u), size=5)))
-    rows.append(v)
-    # long runs of full words ending in literals and the partial last word
-    rows.append(list(range(0, min(u, 64 * 40 + 17))) + list(range(max(0, u - 100), u)))
-    for d in (0.0005, 0.02, 0.3, 0.5, 0.9, 0.999):
-        rows.append(np.flatnonzero(g.random(u) < d).tolist())
-    rows += [x.tolist() for x in gen.run_sets(6, u, 30, 600, int(g.integers(1 << 30)))]
-    return [np.array(sorted(set(x for x in r if 0 <= x < u)), np.uint32) for r in rows]
-
-
 @pytest.mark.parametrize("u", [64, 100, 4103, 65536, (1 << 20) + 13])
 def test_device_build_matches_oracle(sb, u):
     g = gen.rng(u + 7)
-    rows = _segmentation_rows(u, g)
+    rows = gen.segmentation_rows(u, g)
     r = sb.StormRows(u)
     for v in rows:
         r.add(v)
