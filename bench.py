@@ -1374,6 +1374,12 @@ def north_star_summary(line):
     c5 = line.get("config5a_full")
     if isinstance(c5, dict) and "pairs_per_s" in c5:
         ns["config5a"] = {"pairs_per_s": r3(c5["pairs_per_s"]), "frac": r3(g(c5, "roofline", "frac"))}
+    stf = line.get("storm_t")
+    if isinstance(stf, dict):
+        regret = {name: g(r, "plans", "default_regret") for name, r in stf.items() if isinstance(r, dict)}
+        regret = {k: v for k, v in regret.items() if v is not None}
+        if regret:
+            ns["storm_t_plan_regret"] = regret
     return ns
 
 
